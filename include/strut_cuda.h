@@ -1,0 +1,272 @@
+/*
+ * strut_cuda.h -- C ABI of the B200 (sm_100a) nonlinear-transient hot path of Strut.
+ *
+ * Everything here is plain C11: integer status codes, plain pointers and sizes, FP64
+ * mechanics.  The caller owns every host buffer it passes; the library copies what it needs
+ * into device memory and never keeps a caller pointer past the call.
+ *
+ * The entry points replace the per-Newton-iteration block and the step-level calls of Strut's
+ * transient nonlinear driver (reference paths are relative to the Strut project root):
+ *
+ *   strut_gpu_create          <- model set-up done by src/mojo/solver/run_case/loader.mojo
+ *                                (material defs 963-1100, per-element state 1700-1830,
+ *                                DOF numbering 2393-2450) and
+ *                                analysis/transient_nonlinear.mojo:830-1160
+ *   strut_gpu_run_steps       <- analysis/transient_nonlinear.mojo:1698-3110 (step loop:
+ *                                Newmark predictor, Newton loop, commit, post-step update)
+ *   strut_gpu_state_determination
+ *                             <- assemble_global_stiffness_and_internal_soa
+ *                                (solver/assembly/stiffness_internal.mojo:1293-1460) followed
+ *                                by load_reduced_matrix/add_reduced_matrix
+ *                                (solver/run_case/linear_solver_backend.mojo:1877-1983)
+ *   strut_gpu_factor_solve    <- factorize_loaded + solve
+ *                                (linear_solver_backend.mojo:2174-2199, 2277-2305)
+ *   strut_gpu_commit / revert <- fiber_section2d_commit_runtime_all /
+ *                                fiber_section2d_revert_trial_runtime_all
+ *                                (sections/fiber2d.mojo:4191-4252) and
+ *                                _sync_force_beam_column2d_committed_basic_states
+ *                                (solver/run_case/helpers.mojo:1832-1883)
+ *   strut_gpu_section_path    <- src/mojo/section_path.mojo:354-560 (known-answer driver)
+ *   strut_gpu_material_path   <- src/mojo/material_path.mojo:233-262 (known-answer driver)
+ *   strut_gpu_section_eval_batch
+ *                             <- fiber_section2d_set_trial_from_offset
+ *                                (sections/fiber2d.mojo:3982-4024) over many section
+ *                                instances at once (the fiber-state micro-benchmark path of
+ *                                src/mojo/benchmarks_micro.mojo:234)
+ *
+ * Tag values follow src/mojo/tag_types.mojo so a Strut host can pass its own tags through.
+ */
+#ifndef STRUT_CUDA_H
+#define STRUT_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STRUT_ABI_VERSION 1
+#define STRUT_MAX_INT_PTS 10
+
+/* Status codes.  No entry point aborts the process. */
+enum {
+    STRUT_OK = 0,
+    STRUT_NONCONVERGED = 1,   /* Newton (global) ran out of iterations at some step      */
+    STRUT_SINGULAR = 2,       /* zero / tiny pivot, or a non-positive Cholesky diagonal  */
+    STRUT_NAN = 3,            /* non-finite value in the state                           */
+    STRUT_BAD_ARG = 4,        /* invalid input, sizes out of range                       */
+    STRUT_CUDA_ERROR = 5,     /* a CUDA runtime call failed                              */
+    STRUT_UNSUPPORTED = 6,    /* valid Strut input that this library does not implement  */
+    STRUT_ELEMENT_FAILED = 7  /* forceBeamColumn final tangent recovery failed           */
+};
+
+/* UniMaterialTypeTag (tag_types.mojo:136-141). */
+enum { STRUT_MAT_ELASTIC = 0, STRUT_MAT_STEEL01 = 1, STRUT_MAT_CONCRETE01 = 2,
+       STRUT_MAT_STEEL02 = 3, STRUT_MAT_CONCRETE02 = 4 };
+
+/* ElementTypeTag (tag_types.mojo:1-14). */
+enum { STRUT_ELEM_FORCE_BEAM_COLUMN_2D = 2, STRUT_ELEM_DISP_BEAM_COLUMN_2D = 3 };
+
+/* geomTransf. */
+enum { STRUT_GEOM_LINEAR = 0, STRUT_GEOM_PDELTA = 1 };
+
+/* AnalysisSystemTag (tag_types.mojo:43-51). */
+enum { STRUT_SYSTEM_BAND_GENERAL = 1, STRUT_SYSTEM_BAND_SPD = 2 };
+
+/* Transient test modes (transient_nonlinear.mojo:671-684). */
+enum { STRUT_TEST_MAX_DISP_INCR = 0, STRUT_TEST_NORM_DISP_INCR = 1,
+       STRUT_TEST_NORM_UNBALANCE = 2, STRUT_TEST_ENERGY_INCR = 3 };
+
+/* Uniaxial material definition: UniMaterialDef (materials/uniaxial/core.mojo:48-118).
+ * p[] holds p0..p10 exactly as Strut's loader fills them (loader.mojo:913-1100):
+ *   Elastic    p0=E
+ *   Steel01    p0=Fy p1=E0 p2=b
+ *   Steel02    p0=Fy p1=E0 p2=b p3=R0 p4=cR1 p5=cR2 p6=a1 p7=a2 p8=a3 p9=a4 p10=sigInit
+ *   Concrete02 p0=fc p1=epsc0 p2=fcu p3=epscu p4=rat p5=ft p6=Ets  (compression negative) */
+typedef struct StrutUniMaterial {
+    int32_t type;
+    int32_t reserved;
+    double p[11];
+} StrutUniMaterial;
+
+/* One fiber cell as discretised from patches / layers / direct fibers (fiber2d.mojo:37-56):
+ * raw coordinates (not centroid-relative), area and an index into the material table. */
+typedef struct StrutFiber {
+    double y;
+    double z;
+    double area;
+    int32_t material;
+    int32_t reserved;
+} StrutFiber;
+
+/* A FiberSection2d: a contiguous run of fibers[] (append_fiber_section2d_from_input,
+ * fiber2d.mojo:3881-3944). */
+typedef struct StrutFiberSection {
+    int32_t fiber_offset;
+    int32_t fiber_count;
+} StrutFiberSection;
+
+/* Beam integration rule, already mapped to xi in [0,1] and weights x0.5
+ * (beam_integration_rule, elements/beam_integration.mojo:224-243). */
+typedef struct StrutBeamIntegration {
+    int32_t num_int_pts;
+    int32_t reserved;
+    double xi[STRUT_MAX_INT_PTS];
+    double w[STRUT_MAX_INT_PTS];
+} StrutBeamIntegration;
+
+/* A 2D frame element (forceBeamColumn2d / dispBeamColumn2d). */
+typedef struct StrutFrameElement {
+    int32_t type;          /* STRUT_ELEM_*                                      */
+    int32_t node_i;        /* node indices, 0-based                             */
+    int32_t node_j;
+    int32_t section;       /* index into sections[]                             */
+    int32_t geom;          /* STRUT_GEOM_*                                      */
+    int32_t integration;   /* index into integrations[]                         */
+    int32_t dof[6];        /* global dof indices node*ndf + (d-1)               */
+} StrutFrameElement;
+
+/* A uniform excitation (pattern UniformExcitation + Path time series with dt,
+ * time_series.mojo:61-90; transient_nonlinear.mojo:1823-1852).  direction is 1-based; a model
+ * may carry up to two (the second one is an extension beyond Strut's single pattern). */
+typedef struct StrutExcitation {
+    int32_t direction;     /* 0 = unused                                        */
+    int32_t count;         /* number of samples in values                       */
+    const double* values;
+    double dt;             /* Path dt                                           */
+    double factor;
+    double start_time;
+    int32_t use_last;
+    int32_t reserved;
+} StrutExcitation;
+
+/* One analysis instance (one frame + one record). */
+typedef struct StrutModelDesc {
+    int32_t ndm;                 /* must be 2                                            */
+    int32_t ndf;                 /* must be 3                                            */
+    int32_t num_nodes;
+    int32_t num_dofs;            /* num_nodes * ndf                                      */
+    const double* node_coords;   /* num_nodes * 2 : x, y                                 */
+    int32_t num_materials;
+    int32_t num_fibers;
+    const StrutUniMaterial* materials;
+    const StrutFiber* fibers;
+    int32_t num_sections;
+    int32_t num_integrations;
+    const StrutFiberSection* sections;
+    const StrutBeamIntegration* integrations;
+    int32_t num_elements;
+    int32_t num_free;
+    const StrutFrameElement* elements;
+    const int32_t* free_index;   /* num_dofs : free equation number or -1                */
+    const double* mass;          /* num_dofs : M_total (lumped)                          */
+    const double* mass_rayleigh; /* num_dofs : M_rayleigh_total                          */
+    const double* f_const;       /* num_dofs : constant nodal loads (may be NULL)        */
+    double alpha_m, beta_k, beta_k_init, beta_k_comm;   /* rayleigh                      */
+    double dt, gamma, beta;      /* Newmark                                              */
+    double tol;
+    int32_t max_iters;
+    int32_t test_type;           /* STRUT_TEST_*                                         */
+    int32_t system;              /* STRUT_SYSTEM_*                                       */
+    int32_t num_excitations;     /* 0..2                                                 */
+    StrutExcitation excitation[2];
+    /* recorders: displacement history of these dofs, global end forces of these elements */
+    int32_t num_record_dofs;
+    int32_t num_record_elements;
+    const int32_t* record_dofs;
+    const int32_t* record_elements;
+} StrutModelDesc;
+
+/* Per-run statistics (RuntimeProfileMetrics counters, solver/profile.mojo:37-74). */
+typedef struct StrutStepStats {
+    int64_t global_newton_iterations;  /* summed over instances                      */
+    int64_t local_element_iterations;  /* forceBeamColumn corrector iterations       */
+    int64_t section_evaluations;       /* section (integration point) evaluations    */
+    int64_t fiber_updates;             /* fiber trial-state updates                  */
+    int64_t factorizations;
+    int32_t steps_done;
+    int32_t failed_instance;           /* first instance with a non-OK status, or -1 */
+    int32_t failed_step;
+    int32_t status;
+} StrutStepStats;
+
+typedef struct StrutHandle StrutHandle;
+
+/* ---- library ----------------------------------------------------------------------- */
+int strut_gpu_abi_version(void);
+/* Human readable text of the last error on this thread (never NULL). */
+const char* strut_gpu_last_error(void);
+
+/* ---- batched transient analysis ---------------------------------------------------- */
+/* Copies num_instances model descriptions into device memory, performs the initial
+ * assembly (K_init for betaKInit) and leaves every instance at step 0.  device < 0 keeps the
+ * current device. */
+int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_t device,
+                     StrutHandle** out);
+int strut_gpu_destroy(StrutHandle* h);
+int strut_gpu_num_instances(const StrutHandle* h);
+/* Runs n_steps Newmark steps for every instance (predictor, Newton to the test tolerance,
+ * commit, Newmark update).  Stops at the first step where an instance fails. */
+int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats);
+/* Copies recorder histories of one instance for steps [0, steps_done):
+ * disp: steps x num_record_dofs, eforce: steps x num_record_elements x 6,
+ * iters: Newton iterations per step.  Any pointer may be NULL. */
+int strut_gpu_get_history(StrutHandle* h, int32_t instance, double* disp, double* eforce,
+                          int32_t* iters);
+/* Same for all instances at once, instance-major, each block sized as for one instance
+ * with that instance's recorder counts; offsets are the prefix sums of those sizes. */
+int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int32_t* iters);
+/* Current free displacement / velocity / acceleration vectors of one instance. */
+int strut_gpu_get_state(StrutHandle* h, int32_t instance, double* u_free, double* v_free,
+                        double* a_free);
+
+/* ---- single-iteration entries (parity tests) --------------------------------------- */
+/* Sets the trial free displacements of every instance (concatenated in instance order),
+ * runs element state determination + assembly and returns, concatenated per instance,
+ * F_int at the free dofs and the effective band matrix (K + a1*C + a0*M in band storage,
+ * n_free x (2*bw+1) for BandGeneral, n_free x (bw+1) for BandSPD).  Outputs may be NULL. */
+int strut_gpu_state_determination(StrutHandle* h, const double* u_free, double* f_int_free,
+                                  double* band_out);
+/* Band width / storage width of one instance (so the caller can size band_out). */
+int strut_gpu_band_info(const StrutHandle* h, int32_t instance, int32_t* half_bw,
+                        int32_t* row_width);
+/* Factors the effective matrix from the last state determination and solves K du = rhs
+ * (rhs / du concatenated per instance). */
+int strut_gpu_factor_solve(StrutHandle* h, const double* rhs, double* du);
+/* trial -> committed for every fiber and element (fiber2d.mojo:4191; helpers.mojo:1832). */
+int strut_gpu_commit(StrutHandle* h);
+/* committed -> trial (fiber2d.mojo:4222). */
+int strut_gpu_revert(StrutHandle* h);
+
+/* ---- known-answer drivers ---------------------------------------------------------- */
+/* section_path: one FiberSection2d, a path of (eps0, kappa) pairs; after each point the
+ * section is committed.  out: n_points x 5 = N, Mz, k11, k12, k22. */
+int strut_gpu_section_path(const StrutUniMaterial* materials, int32_t num_materials,
+                           const StrutFiber* fibers, int32_t num_fibers,
+                           const double* eps0_kappa, int32_t n_points, double* out);
+/* material_path: one uniaxial material, a strain history, commit after each strain (the
+ * scalar uniaxial path of materials/uniaxial/ops.mojo:117-174). out: n x 2 stress, tangent. */
+int strut_gpu_material_path(const StrutUniMaterial* material, const double* strains,
+                            int32_t n, double* out);
+/* Batched section evaluation: n_inst instances of one FiberSection2d, each with its own
+ * fiber history.  Evaluates every instance at its (eps0, kappa) from committed state and
+ * writes N, Mz, k11, k12, k22 per instance; if commit != 0 the trial state becomes the
+ * committed state.  Repeated calls continue the same histories (state lives in the handle). */
+typedef struct StrutSectionBatch StrutSectionBatch;
+int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t num_materials,
+                                   const StrutFiber* fibers, int32_t num_fibers,
+                                   int32_t n_inst, StrutSectionBatch** out);
+int strut_gpu_section_batch_destroy(StrutSectionBatch* b);
+/* eps0_kappa_dev / resp_dev are DEVICE pointers (n_inst x 2 and n_inst x 5). */
+int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_dev,
+                                 double* resp_dev, int32_t commit, void* stream);
+/* Copies the committed fiber state of one instance to the host in the section's family
+ * order (Steel02 then Concrete02 then the others, 16 doubles per fiber, see DESIGN). */
+int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double* out,
+                                  int32_t* n_fibers);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STRUT_CUDA_H */

@@ -1,0 +1,126 @@
+"""ctypes binding of the CPU oracle (liboracle.so) -- test infrastructure only.
+
+Imported by tests/, by ``__graft_entry__.smoke()`` as the checker and by ``bench.py``'s CPU
+baseline leg.  The product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from strut_b200 import _abi as A
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def build(force: bool = False) -> Path:
+    srcs = list(HERE.glob("*.c")) + list(HERE.glob("*.h")) + [HERE.parent / "include" / "strut_cuda.h"]
+    if force or not LIB_PATH.exists() or any(p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in srcs):
+        subprocess.check_call(["make", "-s", "-C", str(HERE), "liboracle.so"])
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        L.oracle_set_simd_width.argtypes = [C.c_int]
+        L.oracle_get_simd_width.restype = C.c_int
+        L.oracle_material_path.argtypes = [C.POINTER(A.StrutUniMaterial), _dp, C.c_int, _dp]
+        L.oracle_section_path.argtypes = [C.POINTER(A.StrutUniMaterial), C.c_int,
+                                          C.POINTER(A.StrutFiber), C.c_int, _dp, C.c_int, _dp]
+        L.oracle_section_batch_path.argtypes = [C.POINTER(A.StrutUniMaterial), C.c_int,
+                                                C.POINTER(A.StrutFiber), C.c_int, C.c_int, _dp,
+                                                C.c_int, _dp]
+        L.oracle_run_transient.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _ip, _ip]
+        L.oracle_state_determination.argtypes = [C.POINTER(A.StrutModelDesc), _dp, _dp, _dp, _ip]
+        L.oracle_run_transient_batch.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, C.c_int,
+                                                 C.c_int, _ip]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def set_simd_width(w: int):
+    lib().oracle_set_simd_width(int(w))
+
+
+def material_path(mat: A.StrutUniMaterial, strains) -> np.ndarray:
+    s = np.ascontiguousarray(strains, dtype=np.float64)
+    out = np.zeros((len(s), 2))
+    lib().oracle_material_path(C.byref(mat), _d(s), len(s), _d(out))
+    return out
+
+
+def section_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
+    ek = np.ascontiguousarray(eps0_kappa, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros((len(ek), 5))
+    rc = lib().oracle_section_path(mats, nmat, fibs, nfib, _d(ek), len(ek), _d(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_section_path failed: {A.STATUS_NAMES.get(rc, rc)}")
+    return out
+
+
+def section_batch_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
+    """eps0_kappa: (npts, n_inst, 2) -> (npts, n_inst, 5)"""
+    ek = np.ascontiguousarray(eps0_kappa, dtype=np.float64)
+    npts, n_inst = ek.shape[0], ek.shape[1]
+    out = np.zeros((npts, n_inst, 5))
+    rc = lib().oracle_section_batch_path(mats, nmat, fibs, nfib, n_inst, _d(ek), npts, _d(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_section_batch_path failed: {A.STATUS_NAMES.get(rc, rc)}")
+    return out
+
+
+def run_transient(model, steps: int):
+    """(disp (steps, nrec), eforce (steps, nrece, 6), iters (steps,), rc, failed_step)"""
+    d = model.desc()
+    nrec = d.num_record_dofs
+    nrece = d.num_record_elements
+    disp = np.zeros((steps, max(nrec, 1)))
+    ef = np.zeros((steps, max(nrece, 1), 6))
+    iters = np.zeros(steps, dtype=np.int32)
+    failed = C.c_int(-1)
+    rc = lib().oracle_run_transient(C.byref(d), steps, _d(disp), _d(ef),
+                                    iters.ctypes.data_as(_ip), C.byref(failed))
+    return disp[:, :nrec], ef[:, :nrece], iters, rc, failed.value
+
+
+def state_determination(model, u_free):
+    d = model.desc()
+    u = np.ascontiguousarray(u_free, dtype=np.float64)
+    f = np.zeros(model.num_free)
+    bw = C.c_int(0)
+    # first call with band_out NULL to learn the band width
+    rc = lib().oracle_state_determination(C.byref(d), _d(u), _d(f), None, C.byref(bw))
+    if rc != 0:
+        raise RuntimeError(f"oracle_state_determination failed: {A.STATUS_NAMES.get(rc, rc)}")
+    rw = bw.value + 1 if model.system == A.SYSTEM_BAND_SPD else 2 * bw.value + 1
+    band = np.zeros((model.num_free, rw))
+    rc = lib().oracle_state_determination(C.byref(d), _d(u), _d(f), _d(band), C.byref(bw))
+    return f, band, bw.value
+
+
+def run_batch(models, steps: int, nthreads: int):
+    descs = (A.StrutModelDesc * len(models))()
+    for i, m in enumerate(models):
+        descs[i] = m.desc()
+    tot = C.c_int(0)
+    rc = lib().oracle_run_transient_batch(descs, len(models), steps, nthreads, C.byref(tot))
+    return rc, tot.value

@@ -1,0 +1,761 @@
+/*
+ * ORACLE -- test infrastructure only.  Newmark-Newton transient driver, assembly and band
+ * linear systems restated from Strut (paths relative to the Strut project root):
+ *   Newmark constants / kernels   src/mojo/solver/run_case/analysis/transient_nonlinear.mojo:
+ *                                 496-648, 1052-1055
+ *   initial assembly (K_init)     transient_nonlinear.mojo:1207-1453
+ *   step loop                     transient_nonlinear.mojo:1698-3110 (predictor 1766,
+ *                                 ground motion 1823-1852, Newton 1959-2847, residual with
+ *                                 dense dot products 2341-2356, band load 2400-2411,
+ *                                 NormDispIncr test 2539 / 2798-2811, commit 3081-3108)
+ *   element scatter               src/mojo/solver/assembly/stiffness_internal_frame2d.mojo:
+ *                                 594-619 (element order)
+ *   band slots / load / add       src/mojo/solver/run_case/linear_solver_backend.mojo:363-440,
+ *                                 1877-1983; bandwidth 1481-1507
+ *   BandGeneral factor / solve    linear_solver_backend.mojo:631-680 (+ dense partial-pivot
+ *                                 fallback 175-240, 612-629), 735-770
+ *   BandSPD factor / solve        linear_solver_backend.mojo:689-726, 772-812
+ *   basic-state sync at commit    src/mojo/solver/run_case/helpers.mojo:1832-1883
+ *   Path time series (dt form)    src/mojo/solver/time_series.mojo:61-90
+ */
+#include "oracle_internal.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct OModel {
+    const StrutModelDesc* d;
+    int n, bw, rw; /* free count, half band width, general row width 2bw+1 */
+    int spd;
+    OSection* secs;
+    OElement* elems;
+    int* efree; /* num_elements x 6 free equation numbers */
+    double *K, *Kinit, *Kcomm, *C, *Keff, *Kspd;
+    double *Mff, *Mrff;
+    double *dense;
+    int* piv;
+    int dense_mode;
+    double *u, *u_f, *v_f, *a_f, *u_n, *v_n, *a_n, *Fint, *Fext, *P_f, *R_f, *du, *at, *vt,
+        *work;
+    double a0, a1, a2, a3;
+    int has_damping;
+    long newton_iters, factorizations;
+} OModel;
+
+static double path_eval(const StrutExcitation* x, double t) {
+    /* eval_time_series_input, Path with dt (time_series.mojo:71-90) */
+    int n = x->count;
+    if (n == 0) return 0.0;
+    if (t < x->start_time) return 0.0;
+    double incr = (t - x->start_time) / x->dt;
+    int incr1 = (int)floor(incr);
+    int incr2 = incr1 + 1;
+    if (incr2 >= n) {
+        if (x->use_last) return x->factor * x->values[n - 1];
+        return 0.0;
+    }
+    double v1 = x->values[incr1], v2 = x->values[incr2];
+    return x->factor * (v1 + (v2 - v1) * (incr - (double)incr1));
+}
+
+static int gslot(const OModel* m, int row, int col) {
+    int off = col - row + m->bw;
+    if (off < 0 || off > 2 * m->bw) return -1;
+    return row * m->rw + off;
+}
+
+static void model_free(OModel* m) {
+    if (m->elems) {
+        for (int e = 0; e < m->d->num_elements; ++e) {
+            if (!m->elems[e].sst) continue;
+            for (int ip = 0; ip < m->elems[e].nip; ++ip)
+                oracle_section_state_free(&m->elems[e].sst[ip]);
+            free(m->elems[e].sst);
+        }
+        free(m->elems);
+    }
+    if (m->secs) {
+        for (int s = 0; s < m->d->num_sections; ++s) oracle_section_free(&m->secs[s]);
+        free(m->secs);
+    }
+    free(m->efree);
+    free(m->K); free(m->Kinit); free(m->Kcomm); free(m->C); free(m->Keff); free(m->Kspd);
+    free(m->Mff); free(m->Mrff); free(m->dense); free(m->piv);
+    free(m->u); free(m->u_f); free(m->v_f); free(m->a_f); free(m->u_n); free(m->v_n);
+    free(m->a_n); free(m->Fint); free(m->Fext); free(m->P_f); free(m->R_f); free(m->du);
+    free(m->at); free(m->vt); free(m->work);
+    memset(m, 0, sizeof(*m));
+}
+
+static int model_build(OModel* m, const StrutModelDesc* d) {
+    memset(m, 0, sizeof(*m));
+    m->d = d;
+    if (d->ndm != 2 || d->ndf != 3) return STRUT_UNSUPPORTED;
+    if (d->num_free <= 0 || d->num_elements <= 0) return STRUT_BAD_ARG;
+    if (d->system != STRUT_SYSTEM_BAND_GENERAL && d->system != STRUT_SYSTEM_BAND_SPD)
+        return STRUT_UNSUPPORTED;
+    m->spd = d->system == STRUT_SYSTEM_BAND_SPD;
+    m->n = d->num_free;
+    m->secs = (OSection*)calloc(d->num_sections, sizeof(OSection));
+    for (int s = 0; s < d->num_sections; ++s) {
+        int rc = oracle_section_build(&m->secs[s], d->materials, d->num_materials, d->fibers,
+                                      d->sections[s].fiber_offset, d->sections[s].fiber_count);
+        if (rc != STRUT_OK) return rc;
+    }
+    m->elems = (OElement*)calloc(d->num_elements, sizeof(OElement));
+    m->efree = (int*)malloc(sizeof(int) * 6 * d->num_elements);
+    int bw = 0;
+    for (int e = 0; e < d->num_elements; ++e) {
+        const StrutFrameElement* ed = &d->elements[e];
+        OElement* el = &m->elems[e];
+        if (ed->type != STRUT_ELEM_FORCE_BEAM_COLUMN_2D && ed->type != STRUT_ELEM_DISP_BEAM_COLUMN_2D)
+            return STRUT_UNSUPPORTED;
+        el->desc = ed;
+        el->sec = &m->secs[ed->section];
+        const StrutBeamIntegration* r = &d->integrations[ed->integration];
+        el->nip = r->num_int_pts;
+        for (int ip = 0; ip < el->nip; ++ip) {
+            el->xi[ip] = r->xi[ip];
+            el->w[ip] = r->w[ip];
+        }
+        double x1 = d->node_coords[2 * ed->node_i], y1 = d->node_coords[2 * ed->node_i + 1];
+        double x2 = d->node_coords[2 * ed->node_j], y2 = d->node_coords[2 * ed->node_j + 1];
+        double dx = x2 - x1, dy = y2 - y1;
+        el->L = hypot(dx, dy);
+        if (el->L == 0.0) return STRUT_BAD_ARG;
+        double inv_L = 1.0 / el->L;
+        el->c = dx * inv_L;
+        el->s = dy * inv_L;
+        el->c_div = dx / el->L;
+        el->s_div = dy / el->L;
+        el->L_sync = sqrt(dx * dx + dy * dy);
+        el->c_sync = dx / el->L_sync;
+        el->s_sync = dy / el->L_sync;
+        el->sst = (OSecState*)calloc(el->nip, sizeof(OSecState));
+        for (int ip = 0; ip < el->nip; ++ip) oracle_section_state_alloc(el->sec, &el->sst[ip]);
+        for (int a = 0; a < 6; ++a) {
+            int dof = ed->dof[a];
+            m->efree[6 * e + a] = (dof >= 0 && dof < d->num_dofs) ? d->free_index[dof] : -1;
+        }
+        for (int a = 0; a < 6; ++a) {
+            int ia = m->efree[6 * e + a];
+            if (ia < 0) continue;
+            for (int b = a + 1; b < 6; ++b) {
+                int ib = m->efree[6 * e + b];
+                if (ib < 0) continue;
+                int diff = ia > ib ? ia - ib : ib - ia;
+                if (diff > bw) bw = diff;
+            }
+        }
+    }
+    m->bw = bw;
+    m->rw = 2 * bw + 1;
+    int n = m->n;
+    size_t bsz = (size_t)n * m->rw;
+    m->K = (double*)calloc(bsz, sizeof(double));
+    m->Kinit = (double*)calloc(bsz, sizeof(double));
+    m->Kcomm = (double*)calloc(bsz, sizeof(double));
+    m->C = (double*)calloc(bsz, sizeof(double));
+    m->Keff = (double*)calloc(bsz, sizeof(double));
+    m->Kspd = (double*)calloc((size_t)n * (bw + 1), sizeof(double));
+    m->Mff = (double*)calloc(n, sizeof(double));
+    m->Mrff = (double*)calloc(n, sizeof(double));
+    int nd = d->num_dofs;
+    m->u = (double*)calloc(nd, sizeof(double));
+    m->Fint = (double*)calloc(nd, sizeof(double));
+    m->Fext = (double*)calloc(nd, sizeof(double));
+    m->u_f = (double*)calloc(n, sizeof(double));
+    m->v_f = (double*)calloc(n, sizeof(double));
+    m->a_f = (double*)calloc(n, sizeof(double));
+    m->u_n = (double*)calloc(n, sizeof(double));
+    m->v_n = (double*)calloc(n, sizeof(double));
+    m->a_n = (double*)calloc(n, sizeof(double));
+    m->P_f = (double*)calloc(n, sizeof(double));
+    m->R_f = (double*)calloc(n, sizeof(double));
+    m->du = (double*)calloc(n, sizeof(double));
+    m->at = (double*)calloc(n, sizeof(double));
+    m->vt = (double*)calloc(n, sizeof(double));
+    m->work = (double*)calloc(n, sizeof(double));
+    int has_mass = 0;
+    for (int dof = 0; dof < nd; ++dof) {
+        int fi = d->free_index[dof];
+        if (fi < 0) continue;
+        if (d->mass[dof] != 0.0) {
+            m->Mff[fi] += d->mass[dof] * 1.0 * 1.0;
+            has_mass = 1;
+        }
+        if (d->mass_rayleigh && d->mass_rayleigh[dof] != 0.0)
+            m->Mrff[fi] += d->mass_rayleigh[dof] * 1.0 * 1.0;
+    }
+    if (!has_mass) return STRUT_BAD_ARG;
+    double beta = d->beta, gamma = d->gamma, dt = d->dt;
+    if (beta <= 0.0 || dt <= 0.0) return STRUT_BAD_ARG;
+    m->a0 = 1.0 / (beta * dt * dt);
+    m->a1 = gamma / (beta * dt);
+    m->a2 = 1.0 / (beta * dt);
+    m->a3 = 1.0 / (2.0 * beta) - 1.0;
+    m->has_damping = d->alpha_m != 0.0 || d->beta_k != 0.0 || d->beta_k_init != 0.0 ||
+                     d->beta_k_comm != 0.0;
+    return STRUT_OK;
+}
+
+/* assemble_global_stiffness_and_internal_soa: zero K and F_int, then every element in order */
+static int assemble(OModel* m, double* ek_out, double* ef_out) {
+    const StrutModelDesc* d = m->d;
+    memset(m->K, 0, sizeof(double) * (size_t)m->n * m->rw);
+    memset(m->Fint, 0, sizeof(double) * d->num_dofs);
+    for (int e = 0; e < d->num_elements; ++e) {
+        OElement* el = &m->elems[e];
+        double ug[6], k[36], f[6];
+        for (int a = 0; a < 6; ++a) ug[a] = m->u[el->desc->dof[a]];
+        int rc = el->desc->type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D ? oracle_fbc2d(el, ug, k, f)
+                                                                   : oracle_dbc2d(el, ug, k, f);
+        if (rc != STRUT_OK) return rc;
+        if (ek_out) memcpy(ek_out + 36 * e, k, sizeof(k));
+        if (ef_out) memcpy(ef_out + 6 * e, f, sizeof(f));
+        for (int a = 0; a < 6; ++a) {
+            int ia = m->efree[6 * e + a];
+            if (ia >= 0) {
+                for (int b = 0; b < 6; ++b) {
+                    int ib = m->efree[6 * e + b];
+                    if (ib < 0) continue;
+                    int sl = gslot(m, ia, ib);
+                    if (sl >= 0) m->K[sl] += k[a * 6 + b];
+                }
+            }
+            m->Fint[el->desc->dof[a]] += f[a];
+        }
+    }
+    return STRUT_OK;
+}
+
+/* dense dot of a band row against x with Strut's chunked reduction order */
+static double band_row_dot(const OModel* m, const double* band, int i, const double* x) {
+    int W = oracle_get_simd_width();
+    int n = m->n;
+    double sum = 0.0;
+    double lane[16];
+    int j0 = i - m->bw < 0 ? 0 : i - m->bw;
+    int j1 = i + m->bw > n - 1 ? n - 1 : i + m->bw;
+    int full_end = (n / W) * W;
+    for (int c = (j0 / W) * W; c < full_end && c <= j1; c += W) {
+        for (int l = 0; l < W; ++l) {
+            int j = c + l;
+            double aij = (j >= j0 && j <= j1) ? band[i * m->rw + (j - i + m->bw)] : 0.0;
+            lane[l] = (aij * x[j]) * 1.0;
+        }
+        sum += oracle_tree_reduce(lane, W);
+    }
+    int start = full_end > j0 ? full_end : j0;
+    for (int j = start; j <= j1; ++j) sum += (band[i * m->rw + (j - i + m->bw)] * x[j]) * 1.0;
+    return sum;
+}
+
+static double diag_dot(const OModel* m, const double* diag, int i, const double* x) {
+    /* M_ff rows are diagonal: every chunk but the one holding i reduces to zero */
+    (void)m;
+    return (diag[i] * x[i]) * 1.0;
+}
+
+static int dense_lu(OModel* m) {
+    int n = m->n;
+    double* A = m->dense;
+    for (int i = 0; i < n; ++i) m->piv[i] = i;
+    double eps = 1.0e-14;
+    for (int col = 0; col < n; ++col) {
+        int prow = col;
+        double pabs = fabs(A[(size_t)col * n + col]);
+        for (int row = col + 1; row < n; ++row) {
+            double cand = fabs(A[(size_t)row * n + col]);
+            if (cand > pabs) {
+                pabs = cand;
+                prow = row;
+            }
+        }
+        if (pabs <= eps) return STRUT_SINGULAR;
+        if (prow != col) {
+            for (int j = 0; j < n; ++j) {
+                double t = A[(size_t)col * n + j];
+                A[(size_t)col * n + j] = A[(size_t)prow * n + j];
+                A[(size_t)prow * n + j] = t;
+            }
+            int t = m->piv[col];
+            m->piv[col] = m->piv[prow];
+            m->piv[prow] = t;
+        }
+        double diag = A[(size_t)col * n + col];
+        if (fabs(diag) <= eps) return STRUT_SINGULAR;
+        for (int row = col + 1; row < n; ++row) {
+            double factor = A[(size_t)row * n + col] / diag;
+            A[(size_t)row * n + col] = factor;
+            if (factor == 0.0) continue;
+            for (int j = col + 1; j < n; ++j) A[(size_t)row * n + j] -= factor * A[(size_t)col * n + j];
+        }
+    }
+    return STRUT_OK;
+}
+
+static int band_general_factor(OModel* m) {
+    int n = m->n, bw = m->bw;
+    double* B = m->Keff;
+    double tol = 1.0e-14;
+    double* orig = (double*)malloc(sizeof(double) * (size_t)n * m->rw);
+    memcpy(orig, B, sizeof(double) * (size_t)n * m->rw);
+    m->dense_mode = 0;
+    int rc = STRUT_OK;
+    for (int k = 0; k < n; ++k) {
+        int i1 = k + bw > n - 1 ? n - 1 : k + bw;
+        int prow = k;
+        double pabs = 0.0;
+        for (int row = k; row <= i1; ++row) {
+            int sl = gslot(m, row, k);
+            if (sl < 0) continue;
+            double cand = fabs(B[sl]);
+            if (cand > pabs) {
+                pabs = cand;
+                prow = row;
+            }
+        }
+        if (pabs <= tol) {
+            rc = STRUT_SINGULAR;
+            break;
+        }
+        if (prow != k) {
+            if (!m->dense) {
+                m->dense = (double*)malloc(sizeof(double) * (size_t)n * n);
+                m->piv = (int*)malloc(sizeof(int) * n);
+            }
+            memset(m->dense, 0, sizeof(double) * (size_t)n * n);
+            for (int row = 0; row < n; ++row) {
+                int c0 = row - bw < 0 ? 0 : row - bw;
+                int c1 = row + bw > n - 1 ? n - 1 : row + bw;
+                for (int col = c0; col <= c1; ++col) m->dense[(size_t)row * n + col] = orig[gslot(m, row, col)];
+            }
+            rc = dense_lu(m);
+            m->dense_mode = 1;
+            break;
+        }
+        double diag = B[gslot(m, k, k)];
+        if (fabs(diag) <= tol) {
+            rc = STRUT_SINGULAR;
+            break;
+        }
+        int j1 = k + bw > n - 1 ? n - 1 : k + bw;
+        for (int i = k + 1; i <= i1; ++i) {
+            int ik = gslot(m, i, k);
+            if (ik < 0) continue;
+            double factor = B[ik] / diag;
+            B[ik] = factor;
+            if (factor == 0.0) continue;
+            for (int j = k + 1; j <= j1; ++j) {
+                int kj = gslot(m, k, j), ij = gslot(m, i, j);
+                if (ij < 0 || kj < 0) continue;
+                B[ij] -= factor * B[kj];
+            }
+        }
+    }
+    free(orig);
+    return rc;
+}
+
+static int band_general_solve(OModel* m, const double* rhs, double* x) {
+    int n = m->n, bw = m->bw;
+    if (m->dense_mode) {
+        double* A = m->dense;
+        for (int i = 0; i < n; ++i) {
+            double s = rhs[m->piv[i]];
+            for (int j = 0; j < i; ++j) s -= A[(size_t)i * n + j] * m->work[j];
+            m->work[i] = s;
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double s = m->work[i];
+            for (int j = i + 1; j < n; ++j) s -= A[(size_t)i * n + j] * x[j];
+            x[i] = s / A[(size_t)i * n + i];
+        }
+        return STRUT_OK;
+    }
+    const double* B = m->Keff;
+    for (int i = 0; i < n; ++i) {
+        double sum = rhs[i];
+        int j0 = i - bw < 0 ? 0 : i - bw;
+        for (int j = j0; j < i; ++j) sum -= B[gslot(m, i, j)] * m->work[j];
+        m->work[i] = sum;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double sum = m->work[i];
+        int j1 = i + bw > n - 1 ? n - 1 : i + bw;
+        for (int j = i + 1; j <= j1; ++j) sum -= B[gslot(m, i, j)] * x[j];
+        double diag = B[gslot(m, i, i)];
+        if (diag == 0.0) return STRUT_SINGULAR;
+        x[i] = sum / diag;
+    }
+    return STRUT_OK;
+}
+
+#define SSLOT(bw, row, col) ((row) * ((bw) + 1) + ((row) - (col)))
+
+static int band_spd_factor(OModel* m) {
+    int n = m->n, bw = m->bw;
+    double* S = m->Kspd;
+    for (int row = 0; row < n; ++row) {
+        int first = row - bw < 0 ? 0 : row - bw;
+        for (int col = first; col < row; ++col) {
+            double sum = S[SSLOT(bw, row, col)];
+            int k0 = first;
+            int cf = col - bw < 0 ? 0 : col - bw;
+            if (cf > k0) k0 = cf;
+            for (int k = k0; k < col; ++k) sum -= S[SSLOT(bw, row, k)] * S[SSLOT(bw, col, k)];
+            double diag = S[SSLOT(bw, col, col)];
+            if (diag == 0.0) return STRUT_SINGULAR;
+            S[SSLOT(bw, row, col)] = sum / diag;
+        }
+        double ds = S[SSLOT(bw, row, row)];
+        for (int k = first; k < row; ++k) {
+            double v = S[SSLOT(bw, row, k)];
+            ds -= v * v;
+        }
+        if (ds <= 0.0) return STRUT_SINGULAR;
+        S[SSLOT(bw, row, row)] = sqrt(ds);
+    }
+    return STRUT_OK;
+}
+
+static int band_spd_solve(OModel* m, const double* rhs, double* x) {
+    int n = m->n, bw = m->bw;
+    const double* S = m->Kspd;
+    for (int row = 0; row < n; ++row) {
+        int first = row - bw < 0 ? 0 : row - bw;
+        double sum = rhs[row];
+        for (int col = first; col < row; ++col) sum -= S[SSLOT(bw, row, col)] * m->work[col];
+        double diag = S[SSLOT(bw, row, row)];
+        if (diag == 0.0) return STRUT_SINGULAR;
+        m->work[row] = sum / diag;
+    }
+    for (int i = 0; i < n; ++i) x[i] = m->work[i];
+    for (int row = n - 1; row >= 0; --row) {
+        double diag = S[SSLOT(bw, row, row)];
+        if (diag == 0.0) return STRUT_SINGULAR;
+        x[row] /= diag;
+        double xv = x[row];
+        int first = row - bw < 0 ? 0 : row - bw;
+        for (int col = first; col < row; ++col) x[col] -= S[SSLOT(bw, row, col)] * xv;
+    }
+    return STRUT_OK;
+}
+
+/* C_ff rebuild (transient_nonlinear.mojo:2302-2335) and the effective band
+ * (load_reduced_matrix K_ff, add_reduced_matrix C_ff*a1, add_reduced_matrix M_ff*a0). */
+static int build_keff(OModel* m) {
+    const StrutModelDesc* d = m->d;
+    int n = m->n, bw = m->bw;
+    size_t bsz = (size_t)n * m->rw;
+    if (m->has_damping) {
+        for (size_t i = 0; i < bsz; ++i) m->C[i] = 0.0;
+        if (d->alpha_m != 0.0) {
+            for (int i = 0; i < n; ++i) {
+                for (int j = i - bw; j <= i + bw; ++j) {
+                    if (j < 0 || j >= n) continue;
+                    m->C[gslot(m, i, j)] = d->alpha_m * (i == j ? m->Mrff[i] : 0.0);
+                }
+            }
+        }
+        for (size_t i = 0; i < bsz; ++i) {
+            if (d->beta_k != 0.0) m->C[i] += d->beta_k * m->K[i];
+            if (d->beta_k_init != 0.0) m->C[i] += d->beta_k_init * m->Kinit[i];
+            if (d->beta_k_comm != 0.0) m->C[i] += d->beta_k_comm * m->Kcomm[i];
+        }
+    }
+    if (!m->spd) {
+        for (size_t i = 0; i < bsz; ++i) m->Keff[i] = m->K[i];
+        if (m->has_damping && m->a1 != 0.0)
+            for (size_t i = 0; i < bsz; ++i) m->Keff[i] += m->a1 * m->C[i];
+        if (m->a0 != 0.0)
+            for (int i = 0; i < n; ++i) m->Keff[gslot(m, i, i)] += m->a0 * m->Mff[i];
+        /* off-diagonal entries of a0 * M_ff add 0.0 */
+        return STRUT_OK;
+    }
+    /* BandSPD: lower triangle with the 1e-10 symmetry check (linear_solver_backend.mojo:
+     * 266-271, 1936-1948) */
+    for (int i = 0; i < n; ++i) {
+        int j0 = i - bw < 0 ? 0 : i - bw;
+        for (int j = j0; j <= i; ++j) {
+            double lo = m->K[gslot(m, i, j)], up = m->K[gslot(m, j, i)];
+            if (fabs(lo - up) > 1.0e-10) return STRUT_BAD_ARG;
+            m->Kspd[SSLOT(bw, i, j)] = lo;
+        }
+    }
+    if (m->has_damping && m->a1 != 0.0) {
+        for (int i = 0; i < n; ++i) {
+            int j0 = i - bw < 0 ? 0 : i - bw;
+            for (int j = j0; j <= i; ++j) {
+                double lo = m->C[gslot(m, i, j)], up = m->C[gslot(m, j, i)];
+                if (fabs(lo - up) > 1.0e-10) return STRUT_BAD_ARG;
+                m->Kspd[SSLOT(bw, i, j)] += m->a1 * lo;
+            }
+        }
+    }
+    for (int i = 0; i < n; ++i) m->Kspd[SSLOT(bw, i, i)] += m->a0 * m->Mff[i];
+    return STRUT_OK;
+}
+
+static void scatter_u(OModel* m) {
+    const StrutModelDesc* d = m->d;
+    for (int dof = 0; dof < d->num_dofs; ++dof) {
+        int fi = d->free_index[dof];
+        if (fi >= 0) m->u[dof] = m->u_f[fi];
+    }
+}
+
+static int initial_assembly(OModel* m) {
+    int rc = assemble(m, 0, 0);
+    if (rc != STRUT_OK) return rc;
+    size_t bsz = (size_t)m->n * m->rw;
+    if (m->d->beta_k_init != 0.0) memcpy(m->Kinit, m->K, sizeof(double) * bsz);
+    if (m->d->beta_k_comm != 0.0) memcpy(m->Kcomm, m->K, sizeof(double) * bsz);
+    for (int e = 0; e < m->d->num_elements; ++e)
+        for (int ip = 0; ip < m->elems[e].nip; ++ip) oracle_section_revert(&m->elems[e].sst[ip]);
+    return STRUT_OK;
+}
+
+static double simd_sumsq(const double* x, int n) { return oracle_simd_dot(x, x, n); }
+
+static void record_step(OModel* m, int step, double* disp_hist, double* eforce_hist) {
+    const StrutModelDesc* d = m->d;
+    if (disp_hist)
+        for (int j = 0; j < d->num_record_dofs; ++j)
+            disp_hist[(size_t)step * d->num_record_dofs + j] = m->u[d->record_dofs[j]];
+    if (eforce_hist) {
+        for (int j = 0; j < d->num_record_elements; ++j) {
+            OElement* el = &m->elems[d->record_elements[j]];
+            double ug[6], f[6], k[36];
+            for (int a = 0; a < 6; ++a) ug[a] = m->u[el->desc->dof[a]];
+            if (el->desc->type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D)
+                oracle_fbc2d_force_from_basic(el, ug, f);
+            else
+                oracle_dbc2d(el, ug, k, f);
+            memcpy(eforce_hist + ((size_t)step * d->num_record_elements + j) * 6, f, sizeof(f));
+        }
+    }
+}
+
+static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_hist,
+                     int* iters_hist, int* failed_step) {
+    const StrutModelDesc* d = m->d;
+    int n = m->n;
+    double dt = d->dt, beta = d->beta, gamma = d->gamma;
+    double coeff = dt * dt * (0.5 - beta);
+    if (failed_step) *failed_step = -1;
+    for (int step = 0; step < steps; ++step) {
+        memcpy(m->u_n, m->u_f, sizeof(double) * n);
+        memcpy(m->v_n, m->v_f, sizeof(double) * n);
+        memcpy(m->a_n, m->a_f, sizeof(double) * n);
+        for (int i = 0; i < n; ++i) m->u_f[i] = m->u_n[i] + dt * m->v_n[i] + coeff * m->a_n[i];
+        scatter_u(m);
+        double t = (double)(step + 1) * dt;
+        for (int dof = 0; dof < d->num_dofs; ++dof) m->Fext[dof] = d->f_const ? d->f_const[dof] : 0.0;
+        for (int x = 0; x < d->num_excitations; ++x) {
+            const StrutExcitation* ex = &d->excitation[x];
+            if (ex->direction < 1) continue;
+            double ag = path_eval(ex, t);
+            for (int dof = 0; dof < d->num_dofs; ++dof) {
+                if ((dof % d->ndf) + 1 == ex->direction) {
+                    double load = 0.0;
+                    load += -d->mass[dof] * ag;
+                    m->Fext[dof] += load;
+                }
+            }
+        }
+        for (int dof = 0; dof < d->num_dofs; ++dof) {
+            int fi = d->free_index[dof];
+            if (fi >= 0) m->P_f[fi] = m->Fext[dof];
+        }
+        int converged = 0;
+        int it;
+        for (it = 0; it < d->max_iters; ++it) {
+            m->newton_iters++;
+            int rc = assemble(m, 0, 0);
+            if (rc != STRUT_OK) {
+                if (failed_step) *failed_step = step;
+                return rc;
+            }
+            rc = build_keff(m);
+            if (rc != STRUT_OK) {
+                if (failed_step) *failed_step = step;
+                return rc;
+            }
+            for (int i = 0; i < n; ++i) {
+                double an = m->a0 * (m->u_f[i] - m->u_n[i]) - m->a2 * m->v_n[i] - m->a3 * m->a_n[i];
+                m->at[i] = an;
+                m->vt[i] = m->v_n[i] + dt * ((1.0 - gamma) * m->a_n[i] + gamma * an);
+            }
+            int ndofs = d->num_dofs;
+            (void)ndofs;
+            for (int dof = 0; dof < d->num_dofs; ++dof) {
+                int i = d->free_index[dof];
+                if (i < 0) continue;
+                double damping = 0.0;
+                if (m->has_damping) damping = band_row_dot(m, m->C, i, m->vt);
+                double inertia = diag_dot(m, m->Mff, i, m->at);
+                m->R_f[i] = m->P_f[i] - m->Fint[dof] - 0.0 - damping - inertia;
+            }
+            if (d->test_type == STRUT_TEST_NORM_UNBALANCE) {
+                if (sqrt(simd_sumsq(m->R_f, n)) <= d->tol) {
+                    converged = 1;
+                    break;
+                }
+            }
+            rc = m->spd ? band_spd_factor(m) : band_general_factor(m);
+            if (rc != STRUT_OK) {
+                if (failed_step) *failed_step = step;
+                return rc;
+            }
+            m->factorizations++;
+            rc = m->spd ? band_spd_solve(m, m->R_f, m->du) : band_general_solve(m, m->R_f, m->du);
+            if (rc != STRUT_OK) {
+                if (failed_step) *failed_step = step;
+                return rc;
+            }
+            double max_diff = 0.0;
+            for (int i = 0; i < n; ++i)
+                if (fabs(m->du[i]) > max_diff) max_diff = fabs(m->du[i]);
+            double norm = sqrt(simd_sumsq(m->du, n));
+            double energy = fabs(oracle_simd_dot(m->du, m->R_f, n));
+            for (int i = 0; i < n; ++i) m->u_f[i] += m->du[i];
+            scatter_u(m);
+            if (!isfinite(norm)) {
+                if (failed_step) *failed_step = step;
+                return STRUT_NAN;
+            }
+            if (d->test_type == STRUT_TEST_NORM_DISP_INCR && norm <= d->tol) {
+                converged = 1;
+                break;
+            }
+            if (d->test_type == STRUT_TEST_ENERGY_INCR && energy <= d->tol) {
+                converged = 1;
+                break;
+            }
+            if (d->test_type == STRUT_TEST_MAX_DISP_INCR && max_diff <= d->tol) {
+                converged = 1;
+                break;
+            }
+        }
+        if (iters_hist) iters_hist[step] = converged ? it + 1 : d->max_iters;
+        if (!converged) {
+            if (failed_step) *failed_step = step;
+            return STRUT_NONCONVERGED;
+        }
+        /* commit: fibers, then the forceBeamColumn2d basic deformation sync */
+        for (int e = 0; e < d->num_elements; ++e) {
+            OElement* el = &m->elems[e];
+            for (int ip = 0; ip < el->nip; ++ip) oracle_section_commit(&el->sst[ip]);
+            if (el->desc->type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D) {
+                double ug[6], ul[6];
+                for (int a = 0; a < 6; ++a) ug[a] = m->u[el->desc->dof[a]];
+                double c = el->c_sync, s = el->s_sync;
+                ul[0] = c * ug[0] + s * ug[1];
+                ul[1] = -s * ug[0] + c * ug[1];
+                ul[2] = ug[2];
+                ul[3] = c * ug[3] + s * ug[4];
+                ul[4] = -s * ug[3] + c * ug[4];
+                ul[5] = ug[5];
+                double chord = (ul[4] - ul[1]) / el->L_sync;
+                el->v[0] = ul[3] - ul[0];
+                el->v[1] = ul[2] - chord;
+                el->v[2] = ul[5] - chord;
+            }
+        }
+        for (int i = 0; i < n; ++i) {
+            double an = m->a0 * (m->u_f[i] - m->u_n[i]) - m->a2 * m->v_n[i] - m->a3 * m->a_n[i];
+            double vn = m->v_n[i] + dt * ((1.0 - gamma) * m->a_n[i] + gamma * an);
+            m->a_f[i] = an;
+            m->v_f[i] = vn;
+        }
+        record_step(m, step, disp_hist, eforce_hist);
+    }
+    return STRUT_OK;
+}
+
+int oracle_run_transient(const StrutModelDesc* d, int steps, double* disp_hist,
+                         double* eforce_hist, int* iters_hist, int* failed_step) {
+    OModel m;
+    int rc = model_build(&m, d);
+    if (rc == STRUT_OK) rc = initial_assembly(&m);
+    if (rc == STRUT_OK) rc = run_steps(&m, steps, disp_hist, eforce_hist, iters_hist, failed_step);
+    model_free(&m);
+    return rc;
+}
+
+int oracle_state_determination(const StrutModelDesc* d, const double* u_free,
+                               double* f_int_free, double* band_out, int* half_bw) {
+    OModel m;
+    int rc = model_build(&m, d);
+    if (rc == STRUT_OK) rc = initial_assembly(&m);
+    if (rc == STRUT_OK) {
+        memcpy(m.u_f, u_free, sizeof(double) * m.n);
+        scatter_u(&m);
+        rc = assemble(&m, 0, 0);
+    }
+    if (rc == STRUT_OK) rc = build_keff(&m);
+    if (rc == STRUT_OK) {
+        if (half_bw) *half_bw = m.bw;
+        if (f_int_free)
+            for (int dof = 0; dof < d->num_dofs; ++dof)
+                if (d->free_index[dof] >= 0) f_int_free[d->free_index[dof]] = m.Fint[dof];
+        if (band_out) {
+            if (m.spd)
+                memcpy(band_out, m.Kspd, sizeof(double) * (size_t)m.n * (m.bw + 1));
+            else
+                memcpy(band_out, m.Keff, sizeof(double) * (size_t)m.n * m.rw);
+        }
+    }
+    model_free(&m);
+    return rc;
+}
+
+typedef struct {
+    const StrutModelDesc* models;
+    int n, steps, next, total_iters, rc;
+    pthread_mutex_t lock;
+} BatchJob;
+
+static void* batch_worker(void* arg) {
+    BatchJob* job = (BatchJob*)arg;
+    for (;;) {
+        pthread_mutex_lock(&job->lock);
+        int i = job->next++;
+        pthread_mutex_unlock(&job->lock);
+        if (i >= job->n) break;
+        const StrutModelDesc* d = &job->models[i];
+        int* iters = (int*)calloc(job->steps, sizeof(int));
+        int failed = -1;
+        int rc = oracle_run_transient(d, job->steps, 0, 0, iters, &failed);
+        int tot = 0;
+        for (int s = 0; s < job->steps; ++s) tot += iters[s];
+        free(iters);
+        pthread_mutex_lock(&job->lock);
+        job->total_iters += tot;
+        if (rc != STRUT_OK && job->rc == STRUT_OK) job->rc = rc;
+        pthread_mutex_unlock(&job->lock);
+    }
+    return 0;
+}
+
+int oracle_run_transient_batch(const StrutModelDesc* models, int n, int steps, int nthreads,
+                               int* total_iters) {
+    BatchJob job;
+    memset(&job, 0, sizeof(job));
+    job.models = models;
+    job.n = n;
+    job.steps = steps;
+    pthread_mutex_init(&job.lock, 0);
+    if (nthreads < 1) nthreads = 1;
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+    for (int i = 0; i < nthreads; ++i) pthread_create(&th[i], 0, batch_worker, &job);
+    for (int i = 0; i < nthreads; ++i) pthread_join(th[i], 0);
+    free(th);
+    pthread_mutex_destroy(&job.lock);
+    if (total_iters) *total_iters = job.total_iters;
+    return job.rc;
+}

@@ -1,0 +1,259 @@
+"""Synthetic RC-frame workloads in Strut's JSON schema (seeded, no external data).
+
+* ``rc_frame_case``: a 2D reinforced-concrete moment frame of forceBeamColumn2d elements with
+  fiber sections (confined Concrete02 core, unconfined Concrete02 cover, Steel02 bars), lumped
+  floor masses, Rayleigh damping fitted to two modes of the initial stiffness, Newmark
+  (gamma 0.5, beta 0.25), Newton with NormDispIncr, BandGeneral.
+* ``kanai_tajimi_record``: Gaussian white noise through the Kanai-Tajimi filter
+  H(s) = (wg^2 + 2 zg wg s) / (s^2 + 2 zg wg s + wg^2) (bilinear transform), a trapezoid
+  envelope (rise, hold, decay) and scaling to a target peak ground acceleration.
+* ``batched_frames``: the 256-frame batch (stories U{3..12}, bays U{2..5}, wg U(8, 25) rad/s,
+  PGA U(0.2, 0.6) g, record i seeded with 1000 + i).
+
+Builder choices that the workload description leaves open (recorded here): cover 0.04 m; the
+cover concrete is fpc -30 MPa, epsc0 -0.002, fpcu 0, epscu -0.004 with the core's rat, ft and
+Ets; masses act on both translational dofs of every floor node; Rayleigh is written as
+``{alphaM, betaKInit}``; no gravity load.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .integration import beam_integration_rule
+
+G = 9.81
+
+CORE = {"fpc": -30.0e6, "epsc0": -0.002, "fpcu": -6.0e6, "epscu": -0.006,
+        "rat": 0.1, "ft": 3.0e6, "Ets": 1500.0e6}
+COVER = {"fpc": -30.0e6, "epsc0": -0.002, "fpcu": 0.0, "epscu": -0.004,
+         "rat": 0.1, "ft": 3.0e6, "Ets": 1500.0e6}
+STEEL = {"Fy": 420.0e6, "E0": 200.0e9, "b": 0.01, "R0": 18.0, "cR1": 0.925, "cR2": 0.15}
+BAR_AREA = 500.0e-6
+COVER_T = 0.04
+
+
+def rc_section(sec_id: int, width: float, depth: float, core_mat=1, cover_mat=2, steel_mat=3):
+    """10x10 confined core, two 20-fiber cover layers, 2 x 4 bars: 148 fibers."""
+    h2, b2, c = 0.5 * depth, 0.5 * width, COVER_T
+    return {
+        "id": sec_id,
+        "type": "FiberSection2d",
+        "params": {
+            "patches": [
+                {"type": "rect", "material": core_mat, "num_subdiv_y": 10, "num_subdiv_z": 10,
+                 "y_i": -(h2 - c), "z_i": -(b2 - c), "y_j": h2 - c, "z_j": b2 - c},
+                {"type": "rect", "material": cover_mat, "num_subdiv_y": 1, "num_subdiv_z": 20,
+                 "y_i": h2 - c, "z_i": -b2, "y_j": h2, "z_j": b2},
+                {"type": "rect", "material": cover_mat, "num_subdiv_y": 1, "num_subdiv_z": 20,
+                 "y_i": -h2, "z_i": -b2, "y_j": -(h2 - c), "z_j": b2},
+            ],
+            "layers": [
+                {"type": "straight", "material": steel_mat, "num_bars": 4, "bar_area": BAR_AREA,
+                 "y_start": h2 - c, "z_start": -(b2 - c), "y_end": h2 - c, "z_end": b2 - c},
+                {"type": "straight", "material": steel_mat, "num_bars": 4, "bar_area": BAR_AREA,
+                 "y_start": -(h2 - c), "z_start": -(b2 - c), "y_end": -(h2 - c), "z_end": b2 - c},
+            ],
+        },
+    }
+
+
+def kanai_tajimi_record(seed: int, n: int, dt: float, wg: float = 15.0, zg: float = 0.6,
+                        pga_g: float = 0.35, rise: float = 2.0, hold: float = 10.0,
+                        decay: float = 8.0) -> np.ndarray:
+    """Ground acceleration samples [m/s^2], n samples at dt."""
+    from scipy import signal
+
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(n)
+    b_s = [2.0 * zg * wg, wg * wg]
+    a_s = [1.0, 2.0 * zg * wg, wg * wg]
+    bz, az = signal.bilinear(b_s, a_s, fs=1.0 / dt)
+    ag = signal.lfilter(bz, az, w)
+    t = np.arange(n) * dt
+    env = np.where(t < rise, t / rise,
+                   np.where(t < rise + hold, 1.0,
+                            np.clip(1.0 - (t - rise - hold) / decay, 0.0, 1.0)))
+    ag = ag * env
+    peak = np.max(np.abs(ag))
+    if peak > 0.0:
+        ag = ag * (pga_g * G / peak)
+    return ag
+
+
+def _section_initial_props(sec: dict, mats: dict):
+    """EA, ES, EI about the area centroid from the fibers' initial tangents."""
+    from .model import discretize_section
+
+    cells = discretize_section(sec["params"])
+    area = sum(c[2] for c in cells)
+    ybar = sum(c[2] * c[0] for c in cells) / area
+    EA = ES = EI = 0.0
+    for (y, _z, a, m) in cells:
+        mat = mats[m]
+        if mat["type"] == "Concrete02":
+            E = 2.0 * mat["params"]["fpc"] / mat["params"]["epsc0"]
+        elif mat["type"] in ("Steel02", "Steel01"):
+            E = mat["params"]["E0"]
+        else:
+            E = mat["params"]["E"]
+        yr = y - ybar
+        EA += E * a
+        ES += -E * a * yr
+        EI += E * a * yr * yr
+    return EA, ES, EI
+
+
+def initial_stiffness(case: dict) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Dense initial K_ff, lumped M_ff diagonal and free map of a frame case (numpy)."""
+    nodes = case["nodes"]
+    idx = {n["id"]: i for i, n in enumerate(nodes)}
+    ndof = 3 * len(nodes)
+    fixed = np.zeros(ndof, dtype=bool)
+    for i, n in enumerate(nodes):
+        for d in n.get("constraints", []) or []:
+            fixed[3 * i + d - 1] = True
+    free = np.where(~fixed)[0]
+    mats = {m["id"]: m for m in case["materials"]}
+    secs = {s["id"]: _section_initial_props(s, mats) for s in case["sections"]}
+    K = np.zeros((ndof, ndof))
+    for e in case["elements"]:
+        ni, nj = idx[e["nodes"][0]], idx[e["nodes"][1]]
+        x1, y1 = nodes[ni]["x"], nodes[ni]["y"]
+        x2, y2 = nodes[nj]["x"], nodes[nj]["y"]
+        L = math.hypot(x2 - x1, y2 - y1)
+        c, s = (x2 - x1) / L, (y2 - y1) / L
+        EA, ES, EI = secs[e["section"]]
+        fs = np.linalg.inv(np.array([[EA, ES], [ES, EI]]))
+        xis, ws = beam_integration_rule(e.get("integration", "Lobatto"), e.get("num_int_pts", 3))
+        F = np.zeros((3, 3))
+        for xi, w in zip(xis, ws):
+            b = np.array([[1.0, 0.0, 0.0], [0.0, xi - 1.0, xi]])
+            F += w * L * b.T @ fs @ b
+        kb = np.linalg.inv(F)
+        a = np.array([[-1, 0, 0, 1, 0, 0],
+                      [0, 1 / L, 1, 0, -1 / L, 0],
+                      [0, 1 / L, 0, 0, -1 / L, 1]], dtype=float)
+        kl = a.T @ kb @ a
+        T = np.zeros((6, 6))
+        for o in (0, 3):
+            T[o:o + 2, o:o + 2] = [[c, s], [-s, c]]
+            T[o + 2, o + 2] = 1.0
+        kg = T.T @ kl @ T
+        dofs = [3 * ni, 3 * ni + 1, 3 * ni + 2, 3 * nj, 3 * nj + 1, 3 * nj + 2]
+        K[np.ix_(dofs, dofs)] += kg
+    M = np.zeros(ndof)
+    for m in case.get("masses", []):
+        M[3 * idx[m["node"]] + m["dof"] - 1] += m["value"]
+    return K[np.ix_(free, free)], M[free], free
+
+
+def rayleigh_from_modes(case: dict, zeta: float = 0.05, modes=(1, 3)):
+    """alphaM, betaK giving ``zeta`` in the two given modes of the initial system."""
+    from scipy import linalg
+
+    K, M, _free = initial_stiffness(case)
+    m_idx = np.where(M > 0.0)[0]
+    z_idx = np.where(M == 0.0)[0]
+    if len(z_idx):
+        Kmm = K[np.ix_(m_idx, m_idx)]
+        Kmz = K[np.ix_(m_idx, z_idx)]
+        Kzz = K[np.ix_(z_idx, z_idx)]
+        Kc = Kmm - Kmz @ np.linalg.solve(Kzz, Kmz.T)
+    else:
+        Kc = K
+    lam = linalg.eigh(Kc, np.diag(M[m_idx]), eigvals_only=True)
+    w = np.sqrt(np.sort(lam))
+    wi, wj = w[modes[0] - 1], w[modes[1] - 1]
+    alpha = 2.0 * zeta * wi * wj / (wi + wj)
+    beta = 2.0 * zeta / (wi + wj)
+    return float(alpha), float(beta), w
+
+
+def rc_frame_case(stories: int = 3, bays: int = 3, story_h: float = 3.6, bay_w: float = 6.0,
+                  nip: int = 5, floor_mass: float = 60.0e3, dt: float = 0.01, steps: int = 2000,
+                  seed: int = 1000, wg: float = 15.0, zg: float = 0.6, pga_g: float = 0.35,
+                  tol: float = 1.0e-8, max_iters: int = 20, element: str = "forceBeamColumn2d",
+                  system: str = "BandGeneral", zeta: float = 0.05, record=None,
+                  geom: str = "Linear") -> dict:
+    nodes = []
+    nid = 1
+    grid = {}
+    for i in range(stories + 1):
+        for j in range(bays + 1):
+            n = {"id": nid, "x": j * bay_w, "y": i * story_h}
+            if i == 0:
+                n["constraints"] = [1, 2, 3]
+            nodes.append(n)
+            grid[(i, j)] = nid
+            nid += 1
+    elements = []
+    eid = 1
+    for i in range(stories):
+        for j in range(bays + 1):
+            elements.append({"id": eid, "type": element, "nodes": [grid[(i, j)], grid[(i + 1, j)]],
+                             "section": 1, "geomTransf": geom, "integration": "Lobatto",
+                             "num_int_pts": nip})
+            eid += 1
+    for i in range(1, stories + 1):
+        for j in range(bays):
+            elements.append({"id": eid, "type": element, "nodes": [grid[(i, j)], grid[(i, j + 1)]],
+                             "section": 2, "geomTransf": geom, "integration": "Lobatto",
+                             "num_int_pts": nip})
+            eid += 1
+    masses = []
+    for i in range(1, stories + 1):
+        for j in range(bays + 1):
+            masses.append({"node": grid[(i, j)], "dof": 1, "value": floor_mass})
+            masses.append({"node": grid[(i, j)], "dof": 2, "value": floor_mass})
+    n_samples = steps + 1
+    if record is None:
+        record = kanai_tajimi_record(seed, n_samples, dt, wg=wg, zg=zg, pga_g=pga_g)
+    case = {
+        "schema_version": "1.0",
+        "metadata": {"name": f"rc_frame_{stories}s{bays}b_seed{seed}", "units": "SI"},
+        "model": {"ndm": 2, "ndf": 3},
+        "nodes": nodes,
+        "materials": [
+            {"id": 1, "type": "Concrete02", "params": dict(CORE)},
+            {"id": 2, "type": "Concrete02", "params": dict(COVER)},
+            {"id": 3, "type": "Steel02", "params": dict(STEEL)},
+        ],
+        "sections": [rc_section(1, 0.5, 0.5), rc_section(2, 0.4, 0.6)],
+        "elements": elements,
+        "masses": masses,
+        "time_series": [{"type": "Path", "tag": 1, "dt": dt, "values": [float(v) for v in record]}],
+        "pattern": {"type": "UniformExcitation", "tag": 1, "direction": 1, "accel": 1},
+        "analysis": {"type": "transient_nonlinear", "steps": steps, "dt": dt,
+                     "integrator": {"type": "Newmark", "gamma": 0.5, "beta": 0.25},
+                     "algorithm": "Newton", "test_type": "NormDispIncr", "tol": tol,
+                     "max_iters": max_iters, "system": system, "numberer": "RCM"},
+        "recorders": [
+            {"type": "node_displacement", "nodes": [grid[(stories, 0)]], "dofs": [1, 2, 3],
+             "output": "roof"},
+            {"type": "element_force", "elements": [1], "output": "base_col"},
+        ],
+    }
+    alpha, beta, _w = rayleigh_from_modes(case, zeta=zeta)
+    case["rayleigh"] = {"alphaM": alpha, "betaKInit": beta}
+    return case
+
+
+def batched_frame_params(n: int = 256, base_seed: int = 1000):
+    out = []
+    for i in range(n):
+        rng = np.random.default_rng(base_seed + i)
+        stories = int(rng.integers(3, 13))
+        bays = int(rng.integers(2, 6))
+        wg = float(rng.uniform(8.0, 25.0))
+        pga = float(rng.uniform(0.2, 0.6))
+        out.append(dict(stories=stories, bays=bays, wg=wg, pga_g=pga, seed=base_seed + i))
+    return out
+
+
+def batched_frames(n: int = 256, steps: int = 2000, dt: float = 0.01, base_seed: int = 1000,
+                   **kw):
+    return [rc_frame_case(stories=p["stories"], bays=p["bays"], wg=p["wg"], pga_g=p["pga_g"],
+                          seed=p["seed"], steps=steps, dt=dt, **kw)
+            for p in batched_frame_params(n, base_seed)]
