@@ -1,0 +1,1018 @@
+// Fused element state determination for forceBeamColumn2d / dispBeamColumn2d on sm_100a.
+//
+// One CTA per element, one warp per integration point (section).  The element's committed
+// fiber history (all of its sections, all families) is staged into shared memory with
+// cp.async.bulk (the TMA unit's bulk copy) completing on an mbarrier; every section evaluation
+// of the element-level flexibility iteration then reads shared memory only.  Each lane walks
+// the fibers of its warp's section, computes trial stress/tangent in registers and the warp
+// reduces the section resultants and tangent (N, Mz, k11, k12, k22) with shuffles.  Thread 0
+// runs the element-level algebra (3x3 flexibility inverse, work-norm test, subdivision and
+// scheme fallbacks); decisions are broadcast through shared memory so control stays uniform.
+//
+// Algorithm (paths relative to the Strut project root):
+//   src/mojo/elements/force_beam_column2d.mojo:223-272 (3x3 inverse), 608-801 (exact elastic,
+//   initial basic tangent), 804-1189 (_force_beam_column2d_try_increment), 1418-1920 (entry:
+//   schemes x subdivisions, basic -> local -> global); src/mojo/sections/fiber2d.mojo:3042-3086
+//   (section flexibility); src/mojo/elements/disp_beam_column2d.mojo:114-254.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace strut {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// cp.async.bulk global -> shared, completing transaction bytes on the mbarrier.
+// dst/src 16-byte aligned, bytes a multiple of 16.  No multicast.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, "
+        "1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after a fixed number of polls (each try_wait itself suspends for a
+// hardware time slice), reports it, and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+    for (int i = 0; i < (1 << 20); ++i)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+enum { ELEM_ERR_NONE = 0, ELEM_ERR_TMA_TIMEOUT = 1, ELEM_ERR_FAILED = 2 };
+
+// element-level scratch in shared memory
+struct ElemScratch {
+    double q[3], acc_q[3], acc_v[3], v[3], rem[3], att[3], tv[3], zero3[3];
+    double svs_e[kMaxIp], svs_k[kMaxIp];  // accepted section deformations
+    double vs_e[kMaxIp], vs_k[kMaxIp];    // element state section deformations
+    double pt_e[kMaxIp], pt_k[kMaxIp];    // points to evaluate
+    double resp[kMaxIp][5];
+    double sub_e[kMaxIp], sub_k[kMaxIp], ssr_n[kMaxIp], ssr_m[kMaxIp];
+    double fs00[kMaxIp], fs01[kMaxIp], fs11[kMaxIp];
+    double best[10];
+    double ul[6];
+    double k[36];
+    double f[6];
+    int best_ok;
+    int flag;
+    int loop_ctrl;
+    int local_iters;
+    int section_evals;
+};
+
+// Family views of the element's committed history in shared memory.
+struct StageView {
+    const double* c2;  // 5 fields x c2_blk
+    const double* s2;  // 10 fields x s2_blk
+    const int* kon;    // s2_blk
+    const double* s1;  // 5 fields x s1_blk
+    int c2_blk, s2_blk, s1_blk;
+};
+
+// Warp-level section evaluation of section `ip` of the element at (eps0, kappa).
+// Lanes stride over each family's fibers; results are reduced with shuffles and returned in
+// every lane.  hist == nullptr evaluates elastic-only sections.
+__device__ __forceinline__ void section_eval_warp(const Geo& g, const DevSection& sd,
+                                                  const StageView& sv, int ip, double eps0,
+                                                  double kappa, int lane, double out[5]) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a3el = 0.0;
+    int base = sd.geo_off;
+    for (int j = lane; j < sd.n_s2; j += 32) {
+        const int idx = ip * sd.n_s2 + j;
+        S2State c;
+        const int B = sv.s2_blk;
+        c.eps = sv.s2[0 * B + idx];
+        c.sig = sv.s2[1 * B + idx];
+        c.tan = sv.s2[2 * B + idx];
+        c.epsmin = sv.s2[3 * B + idx];
+        c.epsmax = sv.s2[4 * B + idx];
+        c.epspl = sv.s2[5 * B + idx];
+        c.epss0 = sv.s2[6 * B + idx];
+        c.sigs0 = sv.s2[7 * B + idx];
+        c.epsr = sv.s2[8 * B + idx];
+        c.sigr = sv.s2[9 * B + idx];
+        c.kon = sv.kon[idx];
+        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+        S2State t;
+        steel02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+        const double fs = t.sig * A, ks = t.tan * A;
+        a0 += fs;
+        a1 += -fs * y;
+        a2 += ks;
+        a3 += -ks * y;
+        a4 += ks * y * y;
+    }
+    base += sd.n_s2;
+    for (int j = lane; j < sd.n_c2; j += 32) {
+        const int idx = ip * sd.n_c2 + j;
+        const int B = sv.c2_blk;
+        C2State c;
+        c.eps = sv.c2[0 * B + idx];
+        c.sig = sv.c2[1 * B + idx];
+        c.tan = sv.c2[2 * B + idx];
+        c.ecmin = sv.c2[3 * B + idx];
+        c.dept = sv.c2[4 * B + idx];
+        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+        C2State t;
+        concrete02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+        const double fs = t.sig * A, ks = t.tan * A;
+        a0 += fs;
+        a1 += -fs * y;
+        a2 += ks;
+        a3 += -ks * y;
+        a4 += ks * y * y;
+    }
+    base += sd.n_c2;
+    for (int j = lane; j < sd.n_s1; j += 32) {
+        const int idx = ip * sd.n_s1 + j;
+        const int B = sv.s1_blk;
+        S1State c;
+        c.eps = sv.s1[0 * B + idx];
+        c.sig = sv.s1[1 * B + idx];
+        c.tan = sv.s1[2 * B + idx];
+        c.epsp = sv.s1[3 * B + idx];
+        c.alpha = sv.s1[4 * B + idx];
+        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+        S1State t;
+        steel01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+        const double fs = t.sig * A, ks = t.tan * A;
+        a0 += fs;
+        a1 += -fs * y;
+        a2 += ks;
+        a3 += -ks * y;
+        a4 += ks * y * y;
+    }
+    base += sd.n_s1;
+    for (int j = lane; j < sd.n_el; j += 32) {
+        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+        const double E = g.mats[__ldg(g.m + base + j)].p[0];
+        const double ks = E * A;
+        const double fs = ks * (eps0 - y * kappa);
+        a0 += fs;
+        a1 += -fs * y;
+        a2 += ks;
+        a3el += -ks * y;
+        a4 += ks * y * y;
+    }
+    out[0] = warp_sum(a0);
+    out[1] = warp_sum(a1);
+    out[2] = warp_sum(a2);
+    // fiber2d.mojo:3491-3499: a section whose elastic fibers share one modulus reports no
+    // elastic k12 contribution.
+    const double k12el = warp_sum(a3el);
+    out[3] = warp_sum(a3) + (sd.el_uniform ? 0.0 : k12el);
+    out[4] = warp_sum(a4);
+}
+
+__device__ __forceinline__ bool invert3(const double* F, double* k) {
+    const double a = F[0], b = F[1], c = F[2], d = F[3], e = F[4], f = F[5], g = F[6],
+                 h = F[7], i = F[8];
+    const double co00 = e * i - f * h;
+    const double co01 = -(d * i - f * g);
+    const double co02 = d * h - e * g;
+    const double co10 = -(b * i - c * h);
+    const double co11 = a * i - c * g;
+    const double co12 = -(a * h - b * g);
+    const double co20 = b * f - c * e;
+    const double co21 = -(a * f - c * d);
+    const double co22 = a * e - b * d;
+    const double det = a * co00 + b * co01 + c * co02;
+    if (fabs(det) <= 1.0e-40) return false;
+    const double inv_det = 1.0 / det;
+    k[0] = co00 * inv_det;
+    k[1] = co10 * inv_det;
+    k[2] = co20 * inv_det;
+    k[3] = co01 * inv_det;
+    k[4] = co11 * inv_det;
+    k[5] = co21 * inv_det;
+    k[6] = co02 * inv_det;
+    k[7] = co12 * inv_det;
+    k[8] = co22 * inv_det;
+    return true;
+}
+
+__device__ __forceinline__ void flex_accum(double* F, double wL, double bmi, double bmj,
+                                           double f00, double f01, double f11) {
+    const double f10 = f01;
+    F[0] += wL * f00;
+    F[1] += wL * f01 * bmi;
+    F[2] += wL * f01 * bmj;
+    F[3] += wL * bmi * f10;
+    F[4] += wL * bmi * f11 * bmi;
+    F[5] += wL * bmi * f11 * bmj;
+    F[6] += wL * bmj * f10;
+    F[7] += wL * bmj * f11 * bmi;
+    F[8] += wL * bmj * f11 * bmj;
+}
+
+// All warps with warp < nip evaluate their section at S.pt; lane 0 stores S.resp.
+__device__ __forceinline__ void eval_points(const Geo& g, const DevSection& sd,
+                                            const StageView& sv, const DevElem& E,
+                                            ElemScratch& S) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < E.nip) {
+        double r[5];
+        section_eval_warp(g, sd, sv, warp, S.pt_e[warp], S.pt_k[warp], lane, r);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < 5; ++c) S.resp[warp][c] = r[c];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) S.section_evals += E.nip;
+}
+
+// Section flexibility of every evaluated point in ip order, stopping at the first singular
+// one (fiber_section2d_batch_eval_same_def).  Thread 0 only.
+__device__ __forceinline__ bool flex_of_resp(const ElemScratch& S, int nip, double* f00,
+                                             double* f01, double* f11) {
+    for (int ip = 0; ip < nip; ++ip) {
+        const double k11 = S.resp[ip][2], k12 = S.resp[ip][3], k22 = S.resp[ip][4];
+        const double det = k11 * k22 - k12 * k12;
+        if (fabs(det) <= 1.0e-40) return false;
+        const double inv_det = 1.0 / det;
+        f00[ip] = k22 * inv_det;
+        f01[ip] = -k12 * inv_det;
+        f11[ip] = k11 * inv_det;
+    }
+    return true;
+}
+
+// _force_beam_column2d_try_increment, executed collectively.  Starting state: S.q, S.vs_*.
+// On success S.q / S.vs_* hold the converged state and S.best the result.
+__device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const StageView& sv,
+                                  const DevElem& E, ElemScratch& S, const double* base,
+                                  const double* dv, int scheme) {
+    const int tid = threadIdx.x;
+    const int nip = E.nip;
+    if (!sd.init_valid) return false;
+    if (tid == 0) {
+        for (int ip = 0; ip < nip; ++ip) {
+            S.pt_e[ip] = S.vs_e[ip];
+            S.pt_k[ip] = S.vs_k[ip];
+        }
+    }
+    __syncthreads();
+    eval_points(g, sd, sv, E, S);
+    if (tid == 0) {
+        int ok = flex_of_resp(S, nip, S.fs00, S.fs01, S.fs11) ? 1 : 0;
+        if (ok) {
+            double P[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int ip = 0; ip < nip; ++ip) {
+                S.ssr_n[ip] = S.resp[ip][0];
+                S.ssr_m[ip] = S.resp[ip][1];
+                S.sub_e[ip] = S.vs_e[ip];
+                S.sub_k[ip] = S.vs_k[ip];
+                const double xi = E.xi[ip], wL = E.w[ip] * E.L;
+                flex_accum(P, wL, xi - 1.0, xi, S.fs00[ip], S.fs01[ip], S.fs11[ip]);
+            }
+            double pk[9];
+            if (invert3(P, pk)) {
+                S.q[0] += (pk[0] * dv[0] + pk[1] * dv[1] + pk[2] * dv[2]);
+                S.q[1] += (pk[3] * dv[0] + pk[4] * dv[1] + pk[5] * dv[2]);
+                S.q[2] += (pk[6] * dv[0] + pk[7] * dv[1] + pk[8] * dv[2]);
+            }
+        }
+        S.flag = ok;
+    }
+    __syncthreads();
+    if (!S.flag) return false;
+    const int num_iters = scheme == 1 ? 100 : 10;
+    for (int it = 0; it < num_iters; ++it) {
+        if (tid == 0) {
+            S.local_iters++;
+            const bool use_init = scheme == 1 || (scheme == 2 && it == 0);
+            for (int ip = 0; ip < nip; ++ip) {
+                const double xi = E.xi[ip];
+                const double bmi = xi - 1.0, bmj = xi;
+                const double ss0 = S.q[0] + 0.0;
+                const double ss1 = bmi * S.q[1] + bmj * S.q[2] + 0.0;
+                const double dss0 = ss0 - S.ssr_n[ip];
+                const double dss1 = ss1 - S.ssr_m[ip];
+                const double a00 = use_init ? sd.f00 : S.fs00[ip];
+                const double a01 = use_init ? sd.f01 : S.fs01[ip];
+                const double a11 = use_init ? sd.f11 : S.fs11[ip];
+                S.pt_e[ip] = S.sub_e[ip] + (a00 * dss0 + a01 * dss1);
+                S.pt_k[ip] = S.sub_k[ip] + (a01 * dss0 + a11 * dss1);
+            }
+        }
+        __syncthreads();
+        eval_points(g, sd, sv, E, S);
+        if (tid == 0) {
+            double n00[kMaxIp], n01[kMaxIp], n11[kMaxIp];
+            int res = 0;
+            if (flex_of_resp(S, nip, n00, n01, n11)) {
+                double F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                double vr0 = 0.0, vr1 = 0.0, vr2 = 0.0;
+                for (int ip = 0; ip < nip; ++ip) {
+                    const double xi = E.xi[ip], wL = E.w[ip] * E.L;
+                    const double bmi = xi - 1.0, bmj = xi;
+                    const double ss0 = S.q[0] + 0.0;
+                    const double ss1 = bmi * S.q[1] + bmj * S.q[2] + 0.0;
+                    S.sub_e[ip] = S.pt_e[ip];
+                    S.sub_k[ip] = S.pt_k[ip];
+                    S.ssr_n[ip] = S.resp[ip][0];
+                    S.ssr_m[ip] = S.resp[ip][1];
+                    S.fs00[ip] = n00[ip];
+                    S.fs01[ip] = n01[ip];
+                    S.fs11[ip] = n11[ip];
+                    const double dr0 = ss0 - S.ssr_n[ip];
+                    const double dr1 = ss1 - S.ssr_m[ip];
+                    const double dvr0 = n00[ip] * dr0 + n01[ip] * dr1;
+                    const double dvr1 = n01[ip] * dr0 + n11[ip] * dr1;
+                    flex_accum(F, wL, bmi, bmj, n00[ip], n01[ip], n11[ip]);
+                    vr0 += wL * (S.pt_e[ip] + dvr0);
+                    vr1 += wL * bmi * (S.pt_k[ip] + dvr1);
+                    vr2 += wL * bmj * (S.pt_k[ip] + dvr1);
+                }
+                double k[9];
+                if (invert3(F, k)) {
+                    const double r0 = (base[0] + dv[0]) - vr0;
+                    const double r1 = (base[1] + dv[1]) - vr1;
+                    const double r2 = (base[2] + dv[2]) - vr2;
+                    const double dq0 = k[0] * r0 + k[1] * r1 + k[2] * r2;
+                    const double dq1 = k[3] * r0 + k[4] * r1 + k[5] * r2;
+                    const double dq2 = k[6] * r0 + k[7] * r1 + k[8] * r2;
+                    const double work = fabs(r0 * dq0 + r1 * dq1 + r2 * dq2);
+                    S.q[0] += dq0;
+                    S.q[1] += dq1;
+                    S.q[2] += dq2;
+                    res = 1;
+                    if (work < 1.0e-12) {
+                        res = 2;
+                        for (int ip = 0; ip < nip; ++ip) {
+                            S.vs_e[ip] = S.sub_e[ip];
+                            S.vs_k[ip] = S.sub_k[ip];
+                        }
+                        S.best[0] = S.q[0];
+                        S.best[1] = S.q[1];
+                        S.best[2] = S.q[2];
+                        S.best[3] = k[0];
+                        S.best[4] = k[1];
+                        S.best[5] = k[2];
+                        S.best[6] = k[3];
+                        S.best[7] = k[4];
+                        S.best[8] = k[5];
+                        S.best[9] = k[8];
+                    }
+                }
+            }
+            S.flag = res;
+        }
+        __syncthreads();
+        const int f = S.flag;
+        if (f == 0) return false;
+        if (f == 2) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ double max_abs3(const double* v) {
+    double m = fabs(v[0]);
+    if (fabs(v[1]) > m) m = fabs(v[1]);
+    if (fabs(v[2]) > m) m = fabs(v[2]);
+    return m;
+}
+
+__device__ __forceinline__ void u_to_local(double c, double s, const double* ug, double* ul) {
+    ul[0] = c * ug[0] + s * ug[1];
+    ul[1] = -s * ug[0] + c * ug[1];
+    ul[2] = ug[2];
+    ul[3] = c * ug[3] + s * ug[4];
+    ul[4] = -s * ug[3] + c * ug[4];
+    ul[5] = ug[5];
+}
+
+__device__ __forceinline__ void k_to_global(double* k, double c, double s) {
+    for (int i = 0; i < 6; ++i) {
+        const double k0 = k[i * 6 + 0], k1 = k[i * 6 + 1], k3 = k[i * 6 + 3], k4 = k[i * 6 + 4];
+        k[i * 6 + 0] = c * k0 - s * k1;
+        k[i * 6 + 1] = s * k0 + c * k1;
+        k[i * 6 + 3] = c * k3 - s * k4;
+        k[i * 6 + 4] = s * k3 + c * k4;
+    }
+    for (int r0 = 0; r0 <= 3; r0 += 3) {
+        const int r1 = r0 + 1;
+        for (int j = 0; j < 6; ++j) {
+            const double a = k[r0 * 6 + j], b = k[r1 * 6 + j];
+            k[r0 * 6 + j] = c * a - s * b;
+            k[r1 * 6 + j] = s * a + c * b;
+        }
+    }
+}
+
+__device__ __forceinline__ void f_to_global(double* f, double c, double s) {
+    const double f0 = f[0], f1 = f[1], f3 = f[3], f4 = f[4];
+    f[0] = c * f0 - s * f1;
+    f[1] = s * f0 + c * f1;
+    f[3] = c * f3 - s * f4;
+    f[4] = s * f3 + c * f4;
+}
+
+__device__ __forceinline__ void basic_map(int col, double inv_L, double* a) {
+    a[0] = a[1] = a[2] = 0.0;
+    switch (col) {
+        case 0: a[0] = -1.0; break;
+        case 1: a[1] = inv_L; a[2] = inv_L; break;
+        case 2: a[1] = 1.0; break;
+        case 3: a[0] = 1.0; break;
+        case 4: a[1] = -inv_L; a[2] = -inv_L; break;
+        default: a[2] = 1.0; break;
+    }
+}
+
+__device__ __forceinline__ double curv_shape(int idx, double inv_L, double inv_L_sq, double xi) {
+    switch (idx) {
+        case 1: return (-6.0 + 12.0 * xi) * inv_L_sq;
+        case 2: return (-4.0 + 6.0 * xi) * inv_L;
+        case 4: return (6.0 - 12.0 * xi) * inv_L_sq;
+        case 5: return (-2.0 + 6.0 * xi) * inv_L;
+        default: return 0.0;
+    }
+}
+
+__device__ __forceinline__ double axial_shape(int idx, double inv_L) {
+    if (idx == 0) return -inv_L;
+    if (idx == 3) return inv_L;
+    return 0.0;
+}
+
+// Copies a POD struct from global to shared memory with 4-byte words.
+template <typename T>
+__device__ __forceinline__ void copy_struct(T* dst, const T* src) {
+    static_assert(sizeof(T) % 4 == 0, "4-byte multiple");
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) d[i] = s[i];
+}
+
+// Stages the element's committed fiber history into shared memory.  Returns false (and sets
+// *err) if the bulk copy did not complete within the bounded wait.
+__device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState& fs,
+                                              double* sm, uint64_t* bar, StageView& sv,
+                                              int* err) {
+    double* c2 = sm;
+    double* s2 = c2 + 5 * E.c2_blk;
+    double* s1 = s2 + 10 * E.s2_blk;
+    int* kon = reinterpret_cast<int*>(s1 + 5 * E.s1_blk);
+    sv.c2 = c2;
+    sv.s2 = s2;
+    sv.s1 = s1;
+    sv.kon = kon;
+    sv.c2_blk = E.c2_blk;
+    sv.s2_blk = E.s2_blk;
+    sv.s1_blk = E.s1_blk;
+    const uint32_t bytes = (uint32_t)(8 * (5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) +
+                                      4 * E.s2_blk);
+    if (bytes == 0) return true;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(bar, bytes);
+        for (int f = 0; f < 5 && E.c2_blk; ++f)
+            bulk_g2s(c2 + f * E.c2_blk, fs.c2 + f * fs.c2_n + E.c2_off, 8u * E.c2_blk, bar);
+        for (int f = 0; f < 10 && E.s2_blk; ++f)
+            bulk_g2s(s2 + f * E.s2_blk, fs.s2 + f * fs.s2_n + E.s2_off, 8u * E.s2_blk, bar);
+        if (E.s2_blk) bulk_g2s(kon, fs.s2_kon + E.s2_off, 4u * E.s2_blk, bar);
+        for (int f = 0; f < 5 && E.s1_blk; ++f)
+            bulk_g2s(s1 + f * E.s1_blk, fs.s1 + f * fs.s1_n + E.s1_off, 8u * E.s1_blk, bar);
+    }
+    if (!mbar_wait_bounded(bar, 0)) {
+        if (threadIdx.x == 0) *err = ELEM_ERR_TMA_TIMEOUT;
+        // let the copies land before the CTA exits (second bounded wait)
+        mbar_wait_bounded(bar, 0);
+        return false;
+    }
+    return true;
+}
+
+// mode 0: state determination (writes k, f and the element state)
+__global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
+    const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
+    double* __restrict__ estate, double* __restrict__ ek, double* __restrict__ ef,
+    const int* __restrict__ active, int* __restrict__ status, int* __restrict__ elem_err,
+    unsigned long long* __restrict__ counters) {
+    extern __shared__ __align__(128) double smem_fib[];
+    __shared__ DevElem E;
+    __shared__ DevSection sd;
+    __shared__ ElemScratch S;
+    __shared__ __align__(8) uint64_t bar;
+    const int e = blockIdx.x;
+    const int tid = threadIdx.x;
+    copy_struct(&E, elems + e);
+    __syncthreads();
+    if (!active[E.inst]) return;
+    copy_struct(&sd, g.secs + E.sec);
+    if (tid == 0) {
+        S.local_iters = 0;
+        S.section_evals = 0;
+        for (int i = 0; i < 3; ++i) {
+            S.q[i] = estate[(size_t)e * kEStride + kEq + i];
+            S.acc_v[i] = estate[(size_t)e * kEStride + kEv + i];
+            S.zero3[i] = 0.0;
+        }
+        for (int ip = 0; ip < E.nip; ++ip) {
+            S.vs_e[ip] = estate[(size_t)e * kEStride + kEe + ip];
+            S.vs_k[ip] = estate[(size_t)e * kEStride + kEk + ip];
+        }
+        double ug[6];
+        for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
+        if (E.type == 2)
+            u_to_local(E.c, E.s, ug, S.ul);
+        else
+            u_to_local(E.c_div, E.s_div, ug, S.ul);
+    }
+    StageView sv;
+    int err = ELEM_ERR_NONE;
+    const bool staged = stage_element(E, fs, smem_fib, &bar, sv, &err);
+    __syncthreads();
+    if (!staged) {
+        if (tid == 0) {
+            elem_err[e] = err;
+            status[E.inst] = 5;
+        }
+        return;
+    }
+    const int nip = E.nip;
+    if (E.type == 3) {
+        // ---------------- dispBeamColumn2d ----------------
+        const int warp = tid >> 5, lane = tid & 31;
+        const double L = E.L, inv_L = 1.0 / L, inv_L_sq = inv_L * inv_L;
+        if (warp < nip) {
+            const double xi = E.xi[warp];
+            const double b1 = curv_shape(1, inv_L, inv_L_sq, xi);
+            const double b2 = curv_shape(2, inv_L, inv_L_sq, xi);
+            const double b4 = curv_shape(4, inv_L, inv_L_sq, xi);
+            const double b5 = curv_shape(5, inv_L, inv_L_sq, xi);
+            const double eps0 = (-inv_L) * S.ul[0] + inv_L * S.ul[3];
+            const double kappa = b1 * S.ul[1] + b2 * S.ul[2] + b4 * S.ul[4] + b5 * S.ul[5];
+            double r[5];
+            section_eval_warp(g, sd, sv, warp, eps0, kappa, lane, r);
+            if (lane == 0) {
+                for (int c = 0; c < 5; ++c) S.resp[warp][c] = r[c];
+                S.vs_e[warp] = eps0;
+                S.vs_k[warp] = kappa;
+            }
+        }
+        __syncthreads();
+        if (tid < 36) {
+            const int a = tid / 6, b = tid % 6;
+            double kab = 0.0;
+            for (int ip = 0; ip < nip; ++ip) {
+                const double xi = E.xi[ip], wL = E.w[ip] * L;
+                const double ban = axial_shape(a, inv_L), bam = curv_shape(a, inv_L, inv_L_sq, xi);
+                const double bbn = axial_shape(b, inv_L), bbm = curv_shape(b, inv_L, inv_L_sq, xi);
+                const double dN = S.resp[ip][2] * bbn + S.resp[ip][3] * bbm;
+                const double dM = S.resp[ip][3] * bbn + S.resp[ip][4] * bbm;
+                kab += wL * (ban * dN + bam * dM);
+            }
+            S.k[tid] = kab;
+        } else if (tid < 42) {
+            const int a = tid - 36;
+            double fa = 0.0;
+            for (int ip = 0; ip < nip; ++ip) {
+                const double xi = E.xi[ip], wL = E.w[ip] * L;
+                const double ban = axial_shape(a, inv_L), bam = curv_shape(a, inv_L, inv_L_sq, xi);
+                fa += wL * (ban * S.resp[ip][0] + bam * S.resp[ip][1]);
+            }
+            S.f[a] = fa;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (E.geom == 1) {
+                double avg = 0.0;
+                for (int ip = 0; ip < nip; ++ip) avg += E.w[ip] * S.resp[ip][0];
+                const double al = avg / L;
+                S.k[1 * 6 + 1] += al;
+                S.k[4 * 6 + 4] += al;
+                S.k[1 * 6 + 4] -= al;
+                S.k[4 * 6 + 1] -= al;
+                const double ps = (S.ul[1] - S.ul[4]) * al;
+                S.f[1] += ps;
+                S.f[4] -= ps;
+            }
+            k_to_global(S.k, E.c_div, E.s_div);
+            f_to_global(S.f, E.c_div, E.s_div);
+            for (int ip = 0; ip < nip; ++ip) {
+                estate[(size_t)e * kEStride + kEe + ip] = S.vs_e[ip];
+                estate[(size_t)e * kEStride + kEk + ip] = S.vs_k[ip];
+            }
+        }
+        __syncthreads();
+        if (tid < 36) ek[(size_t)e * 36 + tid] = S.k[tid];
+        else if (tid < 42) ef[(size_t)e * 6 + tid - 36] = S.f[tid - 36];
+        if (tid == 0) {
+            atomicAdd(&counters[1], (unsigned long long)nip);
+            atomicAdd(&counters[2], (unsigned long long)nip *
+                                        (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
+        }
+        return;
+    }
+    // ---------------- forceBeamColumn2d ----------------
+    const double L = E.L;
+    const double inv_L = E.inv_L;
+    if (tid == 0) {
+        const double chord = (S.ul[4] - S.ul[1]) / L;
+        S.v[0] = S.ul[3] - S.ul[0];
+        S.v[1] = S.ul[2] - chord;
+        S.v[2] = S.ul[5] - chord;
+        for (int i = 0; i < 3; ++i) {
+            S.acc_q[i] = S.q[i];
+            S.rem[i] = S.v[i] - S.acc_v[i];
+            S.att[i] = S.rem[i];
+        }
+        for (int ip = 0; ip < nip; ++ip) {
+            S.svs_e[ip] = S.vs_e[ip];
+            S.svs_k[ip] = S.vs_k[ip];
+        }
+        S.best_ok = 0;
+        S.loop_ctrl = 0;
+    }
+    __syncthreads();
+    int converged = 0;
+    if (sd.all_elastic) {
+        // _force_beam_column2d_exact_elastic_state (section evaluations there only set trial
+        // fiber state, which this design does not store)
+        if (tid == 0) {
+            int ok = 0;
+            if (sd.init_valid) {
+                double F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                double vl0 = 0.0, vl1 = 0.0, vl2 = 0.0;
+                for (int ip = 0; ip < nip; ++ip) {
+                    const double xi = E.xi[ip], wL = E.w[ip] * L;
+                    const double bmi = xi - 1.0, bmj = xi;
+                    flex_accum(F, wL, bmi, bmj, sd.f00, sd.f01, sd.f11);
+                    vl0 += wL * (sd.f00 * 0.0 + sd.f01 * 0.0);
+                    vl1 += wL * bmi * (sd.f01 * 0.0 + sd.f11 * 0.0);
+                    vl2 += wL * bmj * (sd.f01 * 0.0 + sd.f11 * 0.0);
+                }
+                double k[9];
+                if (invert3(F, k)) {
+                    const double r0 = S.v[0] - vl0, r1 = S.v[1] - vl1, r2 = S.v[2] - vl2;
+                    const double q0 = k[0] * r0 + k[1] * r1 + k[2] * r2;
+                    const double q1 = k[3] * r0 + k[4] * r1 + k[5] * r2;
+                    const double q2 = k[6] * r0 + k[7] * r1 + k[8] * r2;
+                    for (int ip = 0; ip < nip; ++ip) {
+                        const double xi = E.xi[ip];
+                        const double axial = q0 + 0.0;
+                        const double moment = (xi - 1.0) * q1 + xi * q2 + 0.0;
+                        S.vs_e[ip] = sd.f00 * axial + sd.f01 * moment;
+                        S.vs_k[ip] = sd.f01 * axial + sd.f11 * moment;
+                        S.svs_e[ip] = S.vs_e[ip];
+                        S.svs_k[ip] = S.vs_k[ip];
+                    }
+                    S.q[0] = q0;
+                    S.q[1] = q1;
+                    S.q[2] = q2;
+                    for (int i = 0; i < 3; ++i) {
+                        S.acc_v[i] = S.v[i];
+                        S.acc_q[i] = S.q[i];
+                        S.rem[i] = 0.0;
+                    }
+                    S.best[0] = q0;
+                    S.best[1] = q1;
+                    S.best[2] = q2;
+                    for (int i = 0; i < 6; ++i) S.best[3 + i] = k[i];
+                    S.best[9] = k[8];
+                    S.best_ok = 1;
+                    ok = 1;
+                }
+            }
+            S.flag = ok;
+        }
+        __syncthreads();
+        converged = S.flag;
+    }
+    if (!converged) {
+        if (max_abs3(S.rem) <= 1.0e-16) {
+            for (int scheme = 0; scheme < 3; ++scheme) {
+                if (tid == 0) {
+                    for (int i = 0; i < 3; ++i) S.q[i] = S.acc_q[i];
+                    for (int ip = 0; ip < nip; ++ip) {
+                        S.vs_e[ip] = S.svs_e[ip];
+                        S.vs_k[ip] = S.svs_k[ip];
+                    }
+                }
+                __syncthreads();
+                if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.zero3, scheme)) continue;
+                if (tid == 0) S.best_ok = 1;
+                converged = 1;
+                break;
+            }
+        } else {
+            int num_subdivide = 1;
+            int guard = 0;
+            while (num_subdivide <= 4 && guard < 1000) {
+                ++guard;
+                int scheme_success = 0;
+                if (tid == 0)
+                    for (int i = 0; i < 3; ++i) S.tv[i] = S.acc_v[i] + S.att[i];
+                __syncthreads();
+                for (int scheme = 0; scheme < 3; ++scheme) {
+                    if (tid == 0) {
+                        for (int i = 0; i < 3; ++i) S.q[i] = S.acc_q[i];
+                        for (int ip = 0; ip < nip; ++ip) {
+                            S.vs_e[ip] = S.svs_e[ip];
+                            S.vs_k[ip] = S.svs_k[ip];
+                        }
+                    }
+                    __syncthreads();
+                    if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme)) continue;
+                    if (tid == 0) {
+                        for (int i = 0; i < 3; ++i) {
+                            S.acc_v[i] = S.tv[i];
+                            S.acc_q[i] = S.best[i];
+                        }
+                        for (int ip = 0; ip < nip; ++ip) {
+                            S.svs_e[ip] = S.vs_e[ip];
+                            S.svs_k[ip] = S.vs_k[ip];
+                        }
+                        S.best_ok = 1;
+                        for (int i = 0; i < 3; ++i) S.rem[i] = S.v[i] - S.acc_v[i];
+                        if (max_abs3(S.rem) <= 1.0e-12) {
+                            S.loop_ctrl = 1;
+                        } else {
+                            for (int i = 0; i < 3; ++i) S.att[i] = S.rem[i];
+                            S.loop_ctrl = 0;
+                        }
+                    }
+                    __syncthreads();
+                    scheme_success = 1;
+                    if (S.loop_ctrl == 1) converged = 1;
+                    else num_subdivide = 1;
+                    break;
+                }
+                if (converged) break;
+                if (scheme_success) continue;
+                if (tid == 0)
+                    for (int i = 0; i < 3; ++i) S.att[i] /= 10.0;
+                __syncthreads();
+                num_subdivide += 1;
+            }
+        }
+    }
+    if (tid == 0) {
+        int fail = 0;
+        if (!converged) {
+            for (int i = 0; i < 3; ++i) S.q[i] = S.acc_q[i];
+            for (int ip = 0; ip < nip; ++ip) {
+                S.vs_e[ip] = S.svs_e[ip];
+                S.vs_k[ip] = S.svs_k[ip];
+            }
+        }
+        if (!S.best_ok) {
+            // _force_beam_column2d_initial_basic_tangent fallback
+            double F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int ip = 0; ip < nip; ++ip) {
+                const double xi = E.xi[ip], wL = E.w[ip] * L;
+                flex_accum(F, wL, xi - 1.0, xi, sd.f00, sd.f01, sd.f11);
+            }
+            double k[9];
+            if (sd.init_valid && invert3(F, k)) {
+                S.best[0] = S.q[0];
+                S.best[1] = S.q[1];
+                S.best[2] = S.q[2];
+                for (int i = 0; i < 6; ++i) S.best[3 + i] = k[i];
+                S.best[9] = k[8];
+            } else {
+                fail = 1;
+            }
+        }
+        S.flag = fail;
+        // element state: q, section deformations, accepted basic deformation
+        for (int i = 0; i < 3; ++i) {
+            estate[(size_t)e * kEStride + kEq + i] = S.q[i];
+            estate[(size_t)e * kEStride + kEv + i] = S.acc_v[i];
+        }
+        for (int ip = 0; ip < nip; ++ip) {
+            estate[(size_t)e * kEStride + kEe + ip] = S.vs_e[ip];
+            estate[(size_t)e * kEStride + kEk + ip] = S.vs_k[ip];
+        }
+    }
+    __syncthreads();
+    if (S.flag) {
+        if (tid == 0) {
+            elem_err[e] = ELEM_ERR_FAILED;
+            status[E.inst] = 7;
+        }
+        return;
+    }
+    if (tid < 36) {
+        const int a = tid / 6, b = tid % 6;
+        const double* B = S.best;
+        const double kb[9] = {B[3], B[4], B[5], B[6], B[7], B[8], B[5], B[8], B[9]};
+        double av[3], bv[3];
+        basic_map(a, inv_L, av);
+        basic_map(b, inv_L, bv);
+        S.k[tid] = av[0] * (kb[0] * bv[0] + kb[1] * bv[1] + kb[2] * bv[2]) +
+                   av[1] * (kb[3] * bv[0] + kb[4] * bv[1] + kb[5] * bv[2]) +
+                   av[2] * (kb[6] * bv[0] + kb[7] * bv[1] + kb[8] * bv[2]);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const double q0 = S.best[0], q1 = S.best[1], q2 = S.best[2];
+        if (E.geom == 1) {
+            const double ql = q0 * inv_L;
+            S.k[1 * 6 + 1] += ql;
+            S.k[4 * 6 + 4] += ql;
+            S.k[1 * 6 + 4] -= ql;
+            S.k[4 * 6 + 1] -= ql;
+        }
+        S.f[0] = -q0 + 0.0;
+        S.f[1] = (q1 + q2) * inv_L + 0.0;
+        S.f[2] = q1;
+        S.f[3] = q0;
+        S.f[4] = -(q1 + q2) * inv_L + 0.0;
+        S.f[5] = q2;
+        if (E.geom == 1) {
+            const double ps = (S.ul[1] - S.ul[4]) * q0 * inv_L;
+            S.f[1] += ps;
+            S.f[4] -= ps;
+        }
+        k_to_global(S.k, E.c, E.s);
+        f_to_global(S.f, E.c, E.s);
+        atomicAdd(&counters[0], (unsigned long long)S.local_iters);
+        atomicAdd(&counters[1], (unsigned long long)S.section_evals);
+        atomicAdd(&counters[2], (unsigned long long)S.section_evals *
+                                    (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
+    }
+    __syncthreads();
+    if (tid < 36) ek[(size_t)e * 36 + tid] = S.k[tid];
+    else if (tid < 42) ef[(size_t)e * 6 + tid - 36] = S.f[tid - 36];
+}
+
+// Commit: recompute each fiber's trial state at the section deformation stored in the element
+// state and write it over the committed state (fiber2d.mojo:4191-4221); then the
+// forceBeamColumn2d basic-deformation sync from the converged displacements
+// (helpers.mojo:1832-1883) and, for recorded elements, the global end forces
+// (helpers.mojo:1500-1600 for forceBeamColumn2d; a section evaluation at the converged
+// displacements from the new committed state for dispBeamColumn2d).
+__global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
+    const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
+    double* __restrict__ estate, const int* __restrict__ status, double* __restrict__ rec_out,
+    const int* __restrict__ rece_base) {
+    __shared__ DevElem E;
+    __shared__ DevSection sd;
+    __shared__ double resp[kMaxIp][5];
+    __shared__ double ul[6];
+    const int e = blockIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    copy_struct(&E, elems + e);
+    __syncthreads();
+    if (status[E.inst] != 0) return;
+    copy_struct(&sd, g.secs + E.sec);
+    __syncthreads();
+    const int nip = E.nip;
+    if (warp < nip) {
+        const double eps0 = estate[(size_t)e * kEStride + kEe + warp];
+        const double kappa = estate[(size_t)e * kEStride + kEk + warp];
+        int base = sd.geo_off;
+        for (int j = lane; j < sd.n_s2; j += 32) {
+            const long long idx = E.s2_off + warp * sd.n_s2 + j;
+            double* F = fs.s2 + idx;
+            const long long N = fs.s2_n;
+            S2State c, t;
+            c.eps = F[0 * N]; c.sig = F[1 * N]; c.tan = F[2 * N]; c.epsmin = F[3 * N];
+            c.epsmax = F[4 * N]; c.epspl = F[5 * N]; c.epss0 = F[6 * N]; c.sigs0 = F[7 * N];
+            c.epsr = F[8 * N]; c.sigr = F[9 * N]; c.kon = fs.s2_kon[idx];
+            const double y = __ldg(g.y + base + j);
+            steel02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            F[0 * N] = t.eps; F[1 * N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.epsmin;
+            F[4 * N] = t.epsmax; F[5 * N] = t.epspl; F[6 * N] = t.epss0; F[7 * N] = t.sigs0;
+            F[8 * N] = t.epsr; F[9 * N] = t.sigr; fs.s2_kon[idx] = t.kon;
+        }
+        base += sd.n_s2;
+        for (int j = lane; j < sd.n_c2; j += 32) {
+            const long long idx = E.c2_off + warp * sd.n_c2 + j;
+            double* F = fs.c2 + idx;
+            const long long N = fs.c2_n;
+            C2State c, t;
+            c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.ecmin = F[3 * N]; c.dept = F[4 * N];
+            const double y = __ldg(g.y + base + j);
+            concrete02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.ecmin; F[4 * N] = t.dept;
+        }
+        base += sd.n_c2;
+        for (int j = lane; j < sd.n_s1; j += 32) {
+            const long long idx = E.s1_off + warp * sd.n_s1 + j;
+            double* F = fs.s1 + idx;
+            const long long N = fs.s1_n;
+            S1State c, t;
+            c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.epsp = F[3 * N]; c.alpha = F[4 * N];
+            const double y = __ldg(g.y + base + j);
+            steel01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.epsp; F[4 * N] = t.alpha;
+        }
+    }
+    if (tid == 0) {
+        double ug[6];
+        for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
+        if (E.type == 2) {
+            u_to_local(E.c_sync, E.s_sync, ug, ul);
+            const double chord = (ul[4] - ul[1]) / E.L_sync;
+            estate[(size_t)e * kEStride + kEv + 0] = ul[3] - ul[0];
+            estate[(size_t)e * kEStride + kEv + 1] = ul[2] - chord;
+            estate[(size_t)e * kEStride + kEv + 2] = ul[5] - chord;
+            if (E.rec >= 0 && rec_out) {
+                const double inv_L = 1.0 / E.L_sync;
+                const double q0 = estate[(size_t)e * kEStride + 0];
+                const double q1 = estate[(size_t)e * kEStride + 1];
+                const double q2 = estate[(size_t)e * kEStride + 2];
+                const double shear = (q1 + q2) * inv_L;
+                double f[6] = {-q0 + 0.0, shear + 0.0, q1, q0, -shear + 0.0, q2};
+                if (E.geom == 1) {
+                    const double ps = (ul[1] - ul[4]) * q0 * inv_L;
+                    f[1] += ps;
+                    f[4] -= ps;
+                }
+                f_to_global(f, E.c_sync, E.s_sync);
+                double* out = rec_out + ((size_t)rece_base[E.inst] + E.rec) * 6;
+                for (int i = 0; i < 6; ++i) out[i] = f[i];
+            }
+        } else {
+            u_to_local(E.c_div, E.s_div, ug, ul);
+        }
+    }
+    if (E.type != 3 || E.rec < 0 || !rec_out) return;
+    __syncthreads();
+    // dispBeamColumn2d recorder: section evaluation at the converged displacements from the
+    // just-committed state (each lane reads back exactly the fibers it wrote)
+    const double L = E.L, inv_L = 1.0 / L, inv_L_sq = inv_L * inv_L;
+    if (warp < nip) {
+        const double xi = E.xi[warp];
+        const double eps0 = (-inv_L) * ul[0] + inv_L * ul[3];
+        const double kappa = curv_shape(1, inv_L, inv_L_sq, xi) * ul[1] +
+                             curv_shape(2, inv_L, inv_L_sq, xi) * ul[2] +
+                             curv_shape(4, inv_L, inv_L_sq, xi) * ul[4] +
+                             curv_shape(5, inv_L, inv_L_sq, xi) * ul[5];
+        // StageView over global memory: field stride = family length
+        StageView gv;
+        gv.c2 = fs.c2 + E.c2_off;
+        gv.s2 = fs.s2 + E.s2_off;
+        gv.kon = fs.s2_kon + E.s2_off;
+        gv.s1 = fs.s1 + E.s1_off;
+        gv.c2_blk = (int)fs.c2_n;
+        gv.s2_blk = (int)fs.s2_n;
+        gv.s1_blk = (int)fs.s1_n;
+        double r[5];
+        section_eval_warp(g, sd, gv, warp, eps0, kappa, lane, r);
+        if (lane == 0)
+            for (int c = 0; c < 5; ++c) resp[warp][c] = r[c];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double f[6] = {0, 0, 0, 0, 0, 0};
+        double avg = 0.0;
+        for (int ip = 0; ip < nip; ++ip) {
+            const double xi = E.xi[ip], wL = E.w[ip] * L;
+            avg += E.w[ip] * resp[ip][0];
+            for (int a = 0; a < 6; ++a)
+                f[a] += wL * (axial_shape(a, inv_L) * resp[ip][0] +
+                              curv_shape(a, inv_L, inv_L_sq, xi) * resp[ip][1]);
+        }
+        if (E.geom == 1) {
+            const double ps = (ul[1] - ul[4]) * (avg / L);
+            f[1] += ps;
+            f[4] -= ps;
+        }
+        f_to_global(f, E.c_div, E.s_div);
+        double* out = rec_out + ((size_t)rece_base[E.inst] + E.rec) * 6;
+        for (int i = 0; i < 6; ++i) out[i] = f[i];
+    }
+}
+
+}  // namespace strut

@@ -1,0 +1,166 @@
+// Known-answer drivers and the batched section kernel.
+//
+//   material_path_kernel   the scalar uniaxial path of Strut's material_path driver
+//                          (src/mojo/material_path.mojo:233-262; ops.mojo:117-174: an unchanged
+//                          trial strain returns the previous trial state)
+//   section_path_kernel    Strut's section_path driver (src/mojo/section_path.mojo:354-470):
+//                          evaluate the FiberSection2d at each (eps0, kappa), then commit
+//   section_batch_kernel   many section instances, one warp each, reading committed history
+//                          and writing trial (commit != 0: written over committed); the
+//                          fiber-state throughput kernel
+#pragma once
+
+#include "kernels.cuh"
+
+namespace strut {
+
+__global__ void material_path_kernel(DevMat m, const double* __restrict__ strains, int n,
+                                     double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (m.type == 4) {
+        C2State c{0.0, 0.0, m.k[C2K_EC0], 0.0, 0.0};
+        C2State t = c;
+        for (int i = 0; i < n; ++i) {
+            const double eps = strains[i];
+            if (eps != t.eps) concrete02_trial(m, c, eps, t);
+            out[2 * i] = t.sig;
+            out[2 * i + 1] = t.tan;
+            c = t;
+        }
+    } else if (m.type == 3) {
+        S2State c{};
+        c.tan = m.p[1];
+        c.epsmax = m.k[S2K_EPSY];
+        c.epsmin = -m.k[S2K_EPSY];
+        if (m.p[10] != 0.0) {
+            c.eps = m.k[S2K_SIGINI_E0];
+            c.sig = m.p[10];
+        }
+        S2State t = c;
+        for (int i = 0; i < n; ++i) {
+            const double eps = strains[i];
+            if (eps != t.eps) steel02_trial(m, c, eps, t);
+            out[2 * i] = t.sig;
+            out[2 * i + 1] = t.tan;
+            c = t;
+        }
+    } else if (m.type == 1) {
+        S1State c{0.0, 0.0, m.p[1], 0.0, 0.0};
+        S1State t = c;
+        for (int i = 0; i < n; ++i) {
+            const double eps = strains[i];
+            if (eps != t.eps) steel01_trial(m, c, eps, t);
+            out[2 * i] = t.sig;
+            out[2 * i + 1] = t.tan;
+            c = t;
+        }
+    } else {
+        double teps = 0.0, tsig = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double eps = strains[i];
+            if (eps != teps) {
+                teps = eps;
+                tsig = m.p[0] * eps;
+            }
+            out[2 * i] = tsig;
+            out[2 * i + 1] = m.p[0];
+        }
+    }
+}
+
+// Batched section evaluation.  State of instance i, family field f, fiber j at
+//   base_f + f * (n_inst * n_fam) + i * n_fam + j
+// (field-major, then instance, then fiber) so a warp's loads are contiguous.
+struct BatchState {
+    double* c2;
+    double* s2;
+    int* kon;
+    double* s1;
+    long long n_inst;
+};
+
+__global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd, BatchState bs,
+                                                            const double* __restrict__ ek,
+                                                            double* __restrict__ resp,
+                                                            int commit) {
+    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp_global >= bs.n_inst) return;
+    const long long i = warp_global;
+    const double eps0 = ek[2 * i], kappa = ek[2 * i + 1];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a3el = 0.0;
+    int base = sd.geo_off;
+    {
+        const long long N = bs.n_inst * sd.n_s2;
+        for (int j = lane; j < sd.n_s2; j += 32) {
+            double* F = bs.s2 + i * sd.n_s2 + j;
+            int* K = bs.kon + i * sd.n_s2 + j;
+            S2State c, t;
+            c.eps = F[0 * N]; c.sig = F[1 * N]; c.tan = F[2 * N]; c.epsmin = F[3 * N];
+            c.epsmax = F[4 * N]; c.epspl = F[5 * N]; c.epss0 = F[6 * N]; c.sigs0 = F[7 * N];
+            c.epsr = F[8 * N]; c.sigr = F[9 * N]; c.kon = *K;
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            steel02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            if (commit) {
+                F[0 * N] = t.eps; F[1 * N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.epsmin;
+                F[4 * N] = t.epsmax; F[5 * N] = t.epspl; F[6 * N] = t.epss0;
+                F[7 * N] = t.sigs0; F[8 * N] = t.epsr; F[9 * N] = t.sigr; *K = t.kon;
+            }
+            const double fs = t.sig * A, ks = t.tan * A;
+            a0 += fs; a1 += -fs * y; a2 += ks; a3 += -ks * y; a4 += ks * y * y;
+        }
+    }
+    base += sd.n_s2;
+    {
+        const long long N = bs.n_inst * sd.n_c2;
+        for (int j = lane; j < sd.n_c2; j += 32) {
+            double* F = bs.c2 + i * sd.n_c2 + j;
+            C2State c, t;
+            c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.ecmin = F[3 * N]; c.dept = F[4 * N];
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            concrete02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            if (commit) {
+                F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.ecmin;
+                F[4 * N] = t.dept;
+            }
+            const double fs = t.sig * A, ks = t.tan * A;
+            a0 += fs; a1 += -fs * y; a2 += ks; a3 += -ks * y; a4 += ks * y * y;
+        }
+    }
+    base += sd.n_c2;
+    {
+        const long long N = bs.n_inst * sd.n_s1;
+        for (int j = lane; j < sd.n_s1; j += 32) {
+            double* F = bs.s1 + i * sd.n_s1 + j;
+            S1State c, t;
+            c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.epsp = F[3 * N]; c.alpha = F[4 * N];
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            steel01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            if (commit) {
+                F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.epsp;
+                F[4 * N] = t.alpha;
+            }
+            const double fs = t.sig * A, ks = t.tan * A;
+            a0 += fs; a1 += -fs * y; a2 += ks; a3 += -ks * y; a4 += ks * y * y;
+        }
+    }
+    base += sd.n_s1;
+    for (int j = lane; j < sd.n_el; j += 32) {
+        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+        const double ks = g.mats[__ldg(g.m + base + j)].p[0] * A;
+        const double fs = ks * (eps0 - y * kappa);
+        a0 += fs; a1 += -fs * y; a2 += ks; a3el += -ks * y; a4 += ks * y * y;
+    }
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
+    const double k12el = warp_sum(a3el);
+    a3 = warp_sum(a3) + (sd.el_uniform ? 0.0 : k12el);
+    a4 = warp_sum(a4);
+    if (lane == 0) {
+        double* r = resp + 5 * i;
+        r[0] = a0; r[1] = a1; r[2] = a2; r[3] = a3; r[4] = a4;
+    }
+}
+
+}  // namespace strut

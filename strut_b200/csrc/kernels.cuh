@@ -1,0 +1,81 @@
+// Device data layout and kernels of the batched transient hot path (sm_100a, FP64).
+//
+// HBM layout (all instances concatenated, instance-major):
+//   fiber geometry   per section definition, families contiguous: Steel02 | Concrete02 |
+//                    Steel01 | Elastic; y relative to the area centroid, area, material index
+//   fiber history    structure-of-arrays per family, committed state only.  Element e owns
+//                    one block per family: [ip0 fibers | ip1 fibers | ...] padded to 4 entries,
+//                    so every field block is a 32-byte aligned contiguous run that one
+//                    cp.async.bulk moves into shared memory.
+//   element state    32 doubles per element: q0..q2 | eps0[10] | kappa[10] | v0..v2
+//                    (the forceBeamColumn "force_basic_q" block of loader.mojo:1757-1771; for
+//                    dispBeamColumn the section deformations of the last state determination)
+//   element output   k (6x6 global) and f (6) per element
+//   instance arrays  free-dof vectors, band Kinit, gather lists for band slots and F_int
+//
+// Trial fiber state is never written to HBM: a fiber's trial state is a pure function of its
+// committed state and strain, so the commit kernel recomputes it from the section deformations
+// stored in the element state and writes it over the committed state.
+#pragma once
+
+#include <cstdint>
+
+#include "fiber_device.cuh"
+
+namespace strut {
+
+constexpr int kMaxIp = 10;
+constexpr int kEStride = 32;  // doubles of element state
+constexpr int kEq = 0, kEe = 3, kEk = 13, kEv = 23;
+
+struct DevSection {
+    int n_s2, n_c2, n_s1, n_el;
+    int geo_off;
+    int el_uniform;
+    int init_valid;
+    int all_elastic;
+    double f00, f01, f11;
+};
+
+struct DevElem {
+    int type, geom, nip, sec;
+    int inst, rec;              // rec: recorder slot of this element in its instance or -1
+    int dof[6];                 // absolute indices into the concatenated full u vector
+    int s2_off, c2_off, s1_off; // block offsets into family arrays
+    int s2_blk, c2_blk, s1_blk; // block lengths (multiples of 4)
+    double L, inv_L, c, s, c_div, s_div, L_sync, c_sync, s_sync;
+    double xi[kMaxIp], w[kMaxIp];
+};
+
+struct DevInst {
+    int n, bw, rw, num_dofs;
+    int u_off, f_off;
+    long long band_off;
+    long long slot_ptr_off;  // slot_ptr has n*rw + 1 entries per instance
+    int fint_ptr_off;        // fint_ptr has n + 1 entries per instance
+    int max_iters, test_type, spd, has_damping;
+    int rec_off, n_rec, rece_off, n_rece;
+    double a0, a1, a2, a3, dt, gamma, beta, coeff, tol;
+    double alpha_m, beta_k, beta_k_init, beta_k_comm;
+};
+
+struct FiberState {
+    // family arrays: field f of family X lives at X + f * X_n
+    double* c2;
+    long long c2_n;
+    double* s2;
+    int* s2_kon;
+    long long s2_n;
+    double* s1;
+    long long s1_n;
+};
+
+struct Geo {
+    const double* y;
+    const double* a;
+    const int* m;
+    const DevMat* mats;
+    const DevSection* secs;
+};
+
+}  // namespace strut

@@ -1,0 +1,449 @@
+// Per-instance Newton kernels: assembly gather, Rayleigh damping, residual, band factor/solve,
+// displacement update and the convergence test, fused into one CTA per instance with the
+// effective band matrix resident in shared memory.  Plus the Newmark predictor and post-step
+// update over all free dofs.
+//
+// Algorithm (paths relative to the Strut project root):
+//   element scatter order     src/mojo/solver/assembly/stiffness_internal_frame2d.mojo:594-619
+//                             (contributions are gathered per band slot in element order, so
+//                             every K entry is summed exactly as Strut's scatter sums it)
+//   C_ff and residual         src/mojo/solver/run_case/analysis/transient_nonlinear.mojo:
+//                             2302-2356
+//   effective matrix          linear_solver_backend.mojo:1877-1983 (K + a1 C + a0 M)
+//   BandGeneral factor/solve  linear_solver_backend.mojo:631-680, 735-770 (unpivoted Doolittle;
+//                             the dense partial-pivot fallback of 175-240 is reported as
+//                             STRUT_UNSUPPORTED for now)
+//   BandSPD factor/solve      linear_solver_backend.mojo:689-726, 772-812
+//   Newmark                   transient_nonlinear.mojo:496-648, 1052-1055
+//   tests                     nonlinear_convergence.mojo:8-20, transient_nonlinear.mojo:2798-2811
+#pragma once
+
+#include "kernels.cuh"
+
+namespace strut {
+
+enum { INST_MODE_NEWTON = 0, INST_MODE_EXPORT = 1, INST_MODE_SOLVE_EXPORTED = 2 };
+
+struct InstArrays {
+    double *u_f, *v_f, *a_f, *u_n, *v_n, *a_n, *P_f, *du, *R;
+    const double *Mff, *Mrff, *fconst;
+    double* u_full;
+    const int* free_dof;  // absolute index of each free dof in u_full
+    const double* Kinit;  // band, per instance at band_off
+    const long long* slot_ptr;
+    const int* slot_contrib;
+    const int* fint_ptr;
+    const int* fint_contrib;
+    const double* ek;
+    const double* ef;
+    int* active;
+    int* status;
+    int* iters;
+    int* nactive;
+    int* hist_iters;  // this step's row (n_inst entries) or null
+    double* export_band;  // band per instance (BandGeneral rw / BandSPD bw+1 layout)
+    double* export_f;     // F_int at free dofs
+    const double* rhs_in; // INST_MODE_SOLVE_EXPORTED
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) s += red[w];
+    return s;
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) s = fmax(s, red[w]);
+    return s;
+}
+
+// Right-looking band LU without pivoting on the n x (2bw+1) band in shared memory.  Step k
+// updates the trailing bw x bw block with multipliers a_ik / a_kk computed in place and writes
+// the multipliers of column k-1 (no longer read).  Returns 0 ok, 2 singular, 6 pivoting needed.
+__device__ int band_lu_smem(double* B, int n, int bw, int rw, int* flag) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int k = 0; k < n; ++k) {
+        const int m = min(bw, n - 1 - k);
+        // pivot check (linear_solver_backend.mojo:637-657), every thread reads the column
+        const double akk = B[k * rw + bw];
+        double cmax = fabs(akk);
+        bool swap = false;
+        for (int i = k + 1; i <= k + m; ++i) {
+            const double c = fabs(B[i * rw + (k - i + bw)]);
+            if (c > cmax) {
+                cmax = c;
+                swap = true;
+            }
+        }
+        if (cmax <= 1.0e-14) return 2;
+        if (swap) return 6;
+        if (fabs(akk) <= 1.0e-14) return 2;
+        // multipliers of the previous column
+        if (k > 0) {
+            const int mp = min(bw, n - k);  // rows k .. k-1+bw below pivot k-1
+            const double apk = B[(k - 1) * rw + bw];
+            for (int t = tid; t < mp; t += nt) {
+                const int i = k + t;
+                const int sl = i * rw + (k - 1 - i + bw);
+                B[sl] = B[sl] / apk;
+            }
+        }
+        // trailing update (reads column k, row k, writes the block; multiplier slots of
+        // column k are rewritten only at step k+1)
+        for (int t = tid; t < m * m; t += nt) {
+            const int i = k + 1 + t / m;
+            const int j = k + 1 + t % m;
+            const double factor = B[i * rw + (k - i + bw)] / akk;
+            if (factor != 0.0) B[i * rw + (j - i + bw)] -= factor * B[k * rw + (j - k + bw)];
+        }
+        __syncthreads();
+    }
+    (void)flag;
+    return 0;
+}
+
+// Row-oriented band Cholesky (L L^T) on the lower band stored in general layout: right-looking
+// variant with the same arithmetic per entry as the row-oriented reference up to summation
+// order.  Returns 0 ok, 2 not positive definite.
+__device__ int band_chol_smem(double* B, int n, int bw, int rw) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int k = 0; k < n; ++k) {
+        const int m = min(bw, n - 1 - k);
+        const double dkk = B[k * rw + bw];
+        if (!(dkk > 0.0)) return 2;
+        const double lkk = sqrt(dkk);
+        // column k of L (rows k+1..k+m) and the trailing lower update
+        for (int t = tid; t < m * m; t += nt) {
+            const int i = k + 1 + t / m;
+            const int j = k + 1 + t % m;
+            if (j > i) continue;
+            const double lik = B[i * rw + (k - i + bw)] / lkk;
+            const double ljk = B[j * rw + (k - j + bw)] / lkk;
+            B[i * rw + (j - i + bw)] -= lik * ljk;
+        }
+        __syncthreads();
+        for (int t = tid; t < m; t += nt) {
+            const int i = k + 1 + t;
+            B[i * rw + (k - i + bw)] = B[i * rw + (k - i + bw)] / lkk;
+        }
+        if (tid == 0) B[k * rw + bw] = lkk;
+        __syncthreads();
+    }
+    return 0;
+}
+
+// Forward/back substitution with one warp (rows are sequential; each row's band dot product
+// is split over the lanes).
+__device__ void band_solve_lu_warp(const double* B, int n, int bw, int rw, const double* rhs,
+                                   double* w, double* x) {
+    const int lane = threadIdx.x & 31;
+    for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        const int j0 = max(0, i - bw);
+        for (int j = j0 + lane; j < i; j += 32) s += B[i * rw + (j - i + bw)] * w[j];
+        s = warp_sum(s);
+        if (lane == 0) w[i] = rhs[i] - s;
+        __syncwarp();
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = 0.0;
+        const int j1 = min(n - 1, i + bw);
+        for (int j = i + 1 + lane; j <= j1; j += 32) s += B[i * rw + (j - i + bw)] * x[j];
+        s = warp_sum(s);
+        if (lane == 0) x[i] = (w[i] - s) / B[i * rw + bw];
+        __syncwarp();
+    }
+}
+
+__device__ void band_solve_chol_warp(const double* B, int n, int bw, int rw, const double* rhs,
+                                     double* w, double* x) {
+    const int lane = threadIdx.x & 31;
+    for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        const int j0 = max(0, i - bw);
+        for (int j = j0 + lane; j < i; j += 32) s += B[i * rw + (j - i + bw)] * w[j];
+        s = warp_sum(s);
+        if (lane == 0) w[i] = (rhs[i] - s) / B[i * rw + bw];
+        __syncwarp();
+    }
+    // L^T x = w : x_i = (w_i - sum_{j>i} L_ji x_j) / L_ii
+    for (int i = n - 1; i >= 0; --i) {
+        double s = 0.0;
+        const int j1 = min(n - 1, i + bw);
+        for (int j = i + 1 + lane; j <= j1; j += 32) s += B[j * rw + (i - j + bw)] * x[j];
+        s = warp_sum(s);
+        if (lane == 0) x[i] = (w[i] - s) / B[i * rw + bw];
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ double gather_slot(const InstArrays& A, long long sp0, int slot) {
+    const long long c0 = A.slot_ptr[sp0 + slot], c1 = A.slot_ptr[sp0 + slot + 1];
+    double K = 0.0;
+    for (long long c = c0; c < c1; ++c) K += A.ek[A.slot_contrib[c]];
+    return K;
+}
+
+__global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __restrict__ insts,
+                                                              InstArrays A, int mode, int step) {
+    extern __shared__ __align__(16) double smem_inst[];
+    __shared__ DevInst I;
+    __shared__ double red[32];
+    __shared__ int ctrl;
+    const int inst = blockIdx.x;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    {
+        const uint32_t* s = reinterpret_cast<const uint32_t*>(insts + inst);
+        uint32_t* d = reinterpret_cast<uint32_t*>(&I);
+        for (int i = tid; i < (int)(sizeof(DevInst) / 4); i += nt) d[i] = s[i];
+    }
+    __syncthreads();
+    if (mode == INST_MODE_NEWTON && !A.active[inst]) return;
+    const int n = I.n, bw = I.bw, rw = I.rw;
+    double* Kb = smem_inst;        // n * rw
+    double* vt = Kb + (size_t)n * rw;
+    double* R = vt + n;
+    double* w = R + n;
+    double* du = w + n;
+    const int f0 = I.f_off;
+    int rc = 0;
+    if (mode == INST_MODE_SOLVE_EXPORTED) {
+        for (int t = tid; t < n * rw; t += nt) Kb[t] = A.export_band[I.band_off + t];
+        for (int i = tid; i < n; i += nt) R[i] = A.rhs_in[f0 + i];
+        __syncthreads();
+    } else {
+        if (mode == INST_MODE_NEWTON && tid == 0) A.iters[inst] += 1;
+        // v_trial, a_trial (transient_nonlinear.mojo:496-531)
+        for (int i = tid; i < n; i += nt) {
+            const int gi = f0 + i;
+            const double an =
+                I.a0 * (A.u_f[gi] - A.u_n[gi]) - I.a2 * A.v_n[gi] - I.a3 * A.a_n[gi];
+            vt[i] = A.v_n[gi] + I.dt * ((1.0 - I.gamma) * A.a_n[gi] + I.gamma * an);
+            w[i] = an;
+        }
+        __syncthreads();
+        // rows: gather K (element order), C, effective band; residual
+        const long long sp0 = I.slot_ptr_off;
+        const double* Kinit = A.Kinit + I.band_off;
+        int bad_sym = 0;
+        for (int i = tid; i < n; i += nt) {
+            double cv = 0.0;
+            for (int o = 0; o < rw; ++o) {
+                const int j = i + o - bw;
+                const int slot = i * rw + o;
+                if (j < 0 || j >= n) {
+                    Kb[slot] = 0.0;
+                    continue;
+                }
+                const double K = gather_slot(A, sp0, slot);
+                double C = 0.0;
+                if (I.has_damping) {
+                    C = I.alpha_m * (i == j ? A.Mrff[f0 + i] : 0.0);
+                    if (I.beta_k != 0.0) C += I.beta_k * K;
+                    if (I.beta_k_init != 0.0) C += I.beta_k_init * Kinit[slot];
+                    cv += C * vt[j];
+                }
+                if (I.spd && j < i) {
+                    // BandSPD takes the lower triangle after checking symmetry to 1e-10
+                    // (linear_solver_backend.mojo:266-271, 1936-1948)
+                    const int mslot = j * rw + (i - j + bw);
+                    const double Kt = gather_slot(A, sp0, mslot);
+                    if (fabs(K - Kt) > 1.0e-10) bad_sym = 1;
+                    if (I.has_damping && I.a1 != 0.0) {
+                        double Ct = 0.0;
+                        if (I.beta_k != 0.0) Ct += I.beta_k * Kt;
+                        if (I.beta_k_init != 0.0) Ct += I.beta_k_init * Kinit[mslot];
+                        if (fabs(C - Ct) > 1.0e-10) bad_sym = 1;
+                    }
+                }
+                double keff = K;
+                if (I.has_damping && I.a1 != 0.0) keff += I.a1 * C;
+                if (i == j) keff += I.a0 * A.Mff[f0 + i];
+                Kb[slot] = keff;
+            }
+            const int q0 = A.fint_ptr[I.fint_ptr_off + i], q1 = A.fint_ptr[I.fint_ptr_off + i + 1];
+            double F = 0.0;
+            for (int q = q0; q < q1; ++q) F += A.ef[A.fint_contrib[q]];
+            const double ma = A.Mff[f0 + i] * w[i];
+            R[i] = A.P_f[f0 + i] - F - 0.0 - cv - ma;
+            A.R[f0 + i] = R[i];
+            if (mode == INST_MODE_EXPORT) A.export_f[f0 + i] = F;
+        }
+        if (tid == 0) ctrl = 0;
+        __syncthreads();
+        if (bad_sym) ctrl = 1;
+        __syncthreads();
+        if (ctrl) {
+            if (tid == 0) {
+                A.status[inst] = 4;
+                if (mode == INST_MODE_NEWTON && A.active[inst]) {
+                    A.active[inst] = 0;
+                    atomicSub(A.nactive, 1);
+                }
+            }
+            return;
+        }
+        if (mode == INST_MODE_EXPORT) {
+            for (int t = tid; t < n * rw; t += nt) A.export_band[I.band_off + t] = Kb[t];
+            return;
+        }
+        if (I.test_type == 2) {  // NormUnbalance before the solve
+            double s = 0.0;
+            for (int i = tid; i < n; i += nt) s += R[i] * R[i];
+            s = block_sum(s, red);
+            if (sqrt(s) <= I.tol) {
+                if (tid == 0) {
+                    A.active[inst] = 0;
+                    atomicSub(A.nactive, 1);
+                    if (A.hist_iters) A.hist_iters[inst] = A.iters[inst];
+                }
+                return;
+            }
+        }
+    }
+    if (I.spd)
+        rc = band_chol_smem(Kb, n, bw, rw);
+    else
+        rc = band_lu_smem(Kb, n, bw, rw, nullptr);
+    if (rc != 0) {
+        if (tid == 0) {
+            A.status[inst] = rc;
+            if (mode == INST_MODE_NEWTON && A.active[inst]) {
+                A.active[inst] = 0;
+                atomicSub(A.nactive, 1);
+            }
+        }
+        return;
+    }
+    // multipliers of the last column were written in the loop except column n-1 (none below)
+    __syncthreads();
+    if (tid < 32) {
+        if (I.spd)
+            band_solve_chol_warp(Kb, n, bw, rw, R, w, du);
+        else
+            band_solve_lu_warp(Kb, n, bw, rw, R, w, du);
+    }
+    __syncthreads();
+    if (mode == INST_MODE_SOLVE_EXPORTED) {
+        for (int i = tid; i < n; i += nt) A.du[f0 + i] = du[i];
+        return;
+    }
+    double ss = 0.0, en = 0.0, mx = 0.0;
+    for (int i = tid; i < n; i += nt) {
+        const int gi = f0 + i;
+        const double d = du[i];
+        ss += d * d;
+        en += d * R[i];
+        mx = fmax(mx, fabs(d));
+        A.du[gi] = d;
+        const double un = A.u_f[gi] + d;
+        A.u_f[gi] = un;
+        A.u_full[A.free_dof[gi]] = un;
+    }
+    const double norm = sqrt(block_sum(ss, red));
+    const double energy = fabs(block_sum(en, red));
+    const double maxd = block_max(mx, red);
+    if (tid == 0) {
+        bool conv = false;
+        if (I.test_type == 1) conv = norm <= I.tol;
+        else if (I.test_type == 3) conv = energy <= I.tol;
+        else if (I.test_type == 0) conv = maxd <= I.tol;
+        if (!isfinite(norm)) {
+            A.status[inst] = 3;
+            conv = true;
+        }
+        if (conv) {
+            A.active[inst] = 0;
+            atomicSub(A.nactive, 1);
+            if (A.hist_iters) A.hist_iters[inst] = A.iters[inst];
+        } else if (A.iters[inst] >= I.max_iters) {
+            A.status[inst] = 1;
+            A.active[inst] = 0;
+            atomicSub(A.nactive, 1);
+            if (A.hist_iters) A.hist_iters[inst] = A.iters[inst];
+        }
+    }
+}
+
+// Newmark predictor over every free dof (transient_nonlinear.mojo:553-590), the excitation
+// load P_f = F_const + (-M ag) on the excitation direction (1823-1852), and per-instance
+// activation for the Newton loop.
+__global__ void predictor_kernel(const DevInst* __restrict__ insts, InstArrays A,
+                                 const int* __restrict__ free_inst,
+                                 const int* __restrict__ free_dir, const double* __restrict__ ag,
+                                 int n_free_total, int n_inst) {
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi < n_inst) {
+        const bool ok = A.status[gi] == 0;
+        A.active[gi] = ok ? 1 : 0;
+        A.iters[gi] = 0;
+        if (ok) atomicAdd(A.nactive, 1);
+    }
+    if (gi >= n_free_total) return;
+    const int inst = free_inst[gi];
+    const DevInst& I = insts[inst];
+    const double un = A.u_f[gi], vn = A.v_f[gi], an = A.a_f[gi];
+    A.u_n[gi] = un;
+    A.v_n[gi] = vn;
+    A.a_n[gi] = an;
+    const double up = un + I.dt * vn + I.coeff * an;
+    A.u_f[gi] = up;
+    A.u_full[A.free_dof[gi]] = up;
+    double p = A.fconst[gi];
+    // ag holds, per instance, the ground acceleration of each excitation direction at this
+    // step followed by a has-excitation flag per direction.  Strut adds -M*ag onto a zero load
+    // vector first (uniform_inertia_load), then onto F_const.
+    const int dir = free_dir[gi];
+    if (dir == 1 || dir == 2) {
+        const double agv = ag[4 * inst + (dir - 1)];
+        if (ag[4 * inst + 2 + (dir - 1)] != 0.0) {
+            double load = 0.0;
+            load += -A.Mff[gi] * agv;
+            p += load;
+        }
+    }
+    A.P_f[gi] = p;
+}
+
+// Newmark update after convergence (transient_nonlinear.mojo:594-647).
+__global__ void post_step_kernel(const DevInst* __restrict__ insts, InstArrays A,
+                                 const int* __restrict__ free_inst, int n_free_total) {
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= n_free_total) return;
+    const int inst = free_inst[gi];
+    if (A.status[inst] != 0) return;
+    const DevInst& I = insts[inst];
+    const double an = I.a0 * (A.u_f[gi] - A.u_n[gi]) - I.a2 * A.v_n[gi] - I.a3 * A.a_n[gi];
+    const double vn = A.v_n[gi] + I.dt * ((1.0 - I.gamma) * A.a_n[gi] + I.gamma * an);
+    A.a_f[gi] = an;
+    A.v_f[gi] = vn;
+}
+
+__global__ void record_disp_kernel(const double* __restrict__ u_full,
+                                   const int* __restrict__ rec_dof, int n_rec_total,
+                                   double* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_rec_total) out[t] = u_full[rec_dof[t]];
+}
+
+__global__ void scatter_free_kernel(const double* __restrict__ u_f, const int* __restrict__ free_dof,
+                                    double* __restrict__ u_full, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) u_full[free_dof[t]] = u_f[t];
+}
+
+}  // namespace strut

@@ -1,0 +1,1166 @@
+// Host side of libstrut_cuda.so: packs Strut model descriptions into the device layout
+// described in kernels.cuh, drives the Newmark-Newton loop and implements the C ABI of
+// include/strut_cuda.h.
+//
+// Step loop (src/mojo/solver/run_case/analysis/transient_nonlinear.mojo:1698-3110):
+//   predictor_kernel            Newmark predictor + ground-motion load, activate instances
+//   repeat (Newton):
+//     element_state_kernel      every element of every still-active instance
+//     instance_newton_kernel    assembly gather, residual, band factor/solve, update, test
+//     (host reads the number of still-active instances)
+//   commit_kernel               fiber commit, basic-deformation sync, element-force records
+//   post_step_kernel            Newmark velocity / acceleration update
+//   record_disp_kernel          displacement records
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "strut_cuda.h"
+#include "element_kernels.cuh"
+#include "kat_kernels.cuh"
+#include "solver_kernels.cuh"
+
+using namespace strut;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(STRUT_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+inline int round4(int x) { return (x + 3) & ~3; }
+
+DevMat make_devmat(const StrutUniMaterial& m) {
+    DevMat d;
+    std::memset(&d, 0, sizeof(d));
+    d.type = m.type;
+    for (int i = 0; i < 11; ++i) d.p[i] = m.p[i];
+    const double* p = m.p;
+    if (m.type == STRUT_MAT_CONCRETE02) {
+        const double fc = p[0], epsc0 = p[1], fcu = p[2], epscu = p[3], rat = p[4], ft = p[5],
+                     Ets = p[6];
+        const double Ec0 = (2.0 * fc) / epsc0;
+        d.k[C2K_EC0] = Ec0;
+        d.k[C2K_EPSR] = (fcu - rat * Ec0 * epscu) / (Ec0 * (1.0 - rat));
+        d.k[C2K_SIGMR] = Ec0 * d.k[C2K_EPSR];
+        d.k[C2K_EPS0T] = ft / Ec0;
+        d.k[C2K_EPSUT] = ft * (1.0 / Ets + 1.0 / Ec0);
+    } else if (m.type == STRUT_MAT_STEEL02) {
+        const double Fy = p[0], E0 = p[1], b = p[2], a2 = p[7], a4 = p[9];
+        const double Esh = b * E0, epsy = Fy / E0;
+        d.k[S2K_ESH] = Esh;
+        d.k[S2K_EPSY] = epsy;
+        d.k[S2K_SIGINI_E0] = p[10] / E0;
+        d.k[S2K_DPOS] = 2.0 * (a4 * epsy);
+        d.k[S2K_DNEG] = 2.0 * (a2 * epsy);
+        d.k[S2K_E0MESH] = E0 - Esh;
+        d.k[S2K_ESHEPSY] = Esh * epsy;
+    } else if (m.type == STRUT_MAT_STEEL01) {
+        const double E0 = p[1], b = p[2];
+        const double H = (b * E0) / (1.0 - b);
+        d.k[S1K_H] = H;
+        d.k[S1K_EH] = (E0 * H) / (E0 + H);
+        d.k[S1K_E0PH] = E0 + H;
+    }
+    return d;
+}
+
+double initial_tangent(const StrutUniMaterial& m) {
+    switch (m.type) {
+        case STRUT_MAT_ELASTIC: return m.p[0];
+        case STRUT_MAT_STEEL01: return m.p[1];
+        case STRUT_MAT_CONCRETE01: return (2.0 * m.p[0]) / m.p[1];
+        case STRUT_MAT_STEEL02: return m.p[1];
+        case STRUT_MAT_CONCRETE02: return (2.0 * m.p[0]) / m.p[1];
+        default: return 0.0;
+    }
+}
+
+// Host image of the fiber geometry and section definitions.
+struct SectionPack {
+    std::vector<DevSection> secs;
+    std::vector<double> y, a;
+    std::vector<int> m;
+};
+
+// Builds one FiberSection2d definition (fiber2d.mojo:3323-3455): area centroid, families,
+// initial flexibility.  mat_base offsets material indices into the global table.
+int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fibers, int off,
+                 int count, int mat_base, SectionPack& sp) {
+    if (count <= 0) return fail(STRUT_BAD_ARG, "section without fibers");
+    double area_sum = 0.0, qz_sum = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const StrutFiber& f = fibers[off + i];
+        if (f.material < 0 || f.material >= nmat) return fail(STRUT_BAD_ARG, "fiber material out of range");
+        const int t = mats[f.material].type;
+        if (t != STRUT_MAT_ELASTIC && t != STRUT_MAT_STEEL01 && t != STRUT_MAT_STEEL02 &&
+            t != STRUT_MAT_CONCRETE02)
+            return fail(STRUT_UNSUPPORTED, "fiber material type not implemented on this path");
+        area_sum += f.area;
+        qz_sum += f.area * f.y;
+    }
+    if (!(area_sum > 0.0)) return fail(STRUT_BAD_ARG, "section total area must be > 0");
+    const double y_bar = qz_sum / area_sum;
+    DevSection sd;
+    std::memset(&sd, 0, sizeof(sd));
+    sd.geo_off = (int)sp.y.size();
+    double ik11 = 0.0, ik12 = 0.0, ik22 = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const StrutFiber& f = fibers[off + i];
+        const double y_rel = f.y - y_bar;
+        const double ks = initial_tangent(mats[f.material]) * f.area;
+        ik11 += ks;
+        ik12 += -ks * y_rel;
+        ik22 += ks * y_rel * y_rel;
+    }
+    const int order[4] = {STRUT_MAT_STEEL02, STRUT_MAT_CONCRETE02, STRUT_MAT_STEEL01,
+                          STRUT_MAT_ELASTIC};
+    int counts[4] = {0, 0, 0, 0};
+    for (int fam = 0; fam < 4; ++fam) {
+        for (int i = 0; i < count; ++i) {
+            const StrutFiber& f = fibers[off + i];
+            if (mats[f.material].type != order[fam]) continue;
+            sp.y.push_back(f.y - y_bar);
+            sp.a.push_back(f.area);
+            sp.m.push_back(mat_base + f.material);
+            counts[fam]++;
+        }
+    }
+    sd.n_s2 = counts[0];
+    sd.n_c2 = counts[1];
+    sd.n_s1 = counts[2];
+    sd.n_el = counts[3];
+    sd.all_elastic = (sd.n_s2 + sd.n_c2 + sd.n_s1) == 0;
+    sd.el_uniform = 0;
+    if (sd.n_el > 0) {
+        sd.el_uniform = 1;
+        double E0 = -1.0;
+        for (int i = 0; i < count; ++i) {
+            const StrutFiber& f = fibers[off + i];
+            if (mats[f.material].type != STRUT_MAT_ELASTIC) continue;
+            const double E = mats[f.material].p[0];
+            if (E0 < 0.0) E0 = E;
+            else if (E != E0) sd.el_uniform = 0;
+        }
+    }
+    const double det = ik11 * ik22 - ik12 * ik12;
+    if (std::fabs(det) > 1.0e-40) {
+        const double inv_det = 1.0 / det;
+        sd.init_valid = 1;
+        sd.f00 = ik22 * inv_det;
+        sd.f01 = -ik12 * inv_det;
+        sd.f11 = ik11 * inv_det;
+    }
+    sp.secs.push_back(sd);
+    return STRUT_OK;
+}
+
+double path_eval(const StrutExcitation& x, double t) {
+    // eval_time_series_input, Path with dt (src/mojo/solver/time_series.mojo:71-90)
+    const int n = x.count;
+    if (n == 0) return 0.0;
+    if (t < x.start_time) return 0.0;
+    const double incr = (t - x.start_time) / x.dt;
+    const int incr1 = (int)std::floor(incr);
+    const int incr2 = incr1 + 1;
+    if (incr2 >= n) {
+        if (x.use_last) return x.factor * x.values[n - 1];
+        return 0.0;
+    }
+    const double v1 = x.values[incr1], v2 = x.values[incr2];
+    return x.factor * (v1 + (v2 - v1) * (incr - (double)incr1));
+}
+
+template <typename T>
+int upload(T** dptr, const std::vector<T>& h, std::vector<void*>& allocs) {
+    const size_t n = std::max<size_t>(h.size(), 1);
+    CK(cudaMalloc((void**)dptr, n * sizeof(T)));
+    allocs.push_back(*dptr);
+    if (!h.empty()) CK(cudaMemcpy(*dptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return STRUT_OK;
+}
+
+template <typename T>
+int dzeros(T** dptr, size_t n, std::vector<void*>& allocs) {
+    n = std::max<size_t>(n, 1);
+    CK(cudaMalloc((void**)dptr, n * sizeof(T)));
+    allocs.push_back(*dptr);
+    CK(cudaMemset(*dptr, 0, n * sizeof(T)));
+    return STRUT_OK;
+}
+
+#define TRY(x)                       \
+    do {                             \
+        int rc_ = (x);               \
+        if (rc_ != STRUT_OK) return rc_; \
+    } while (0)
+
+}  // namespace
+
+struct ExcHost {
+    int num;
+    StrutExcitation x[2];
+    std::vector<double> vals[2];
+};
+
+struct StrutHandle {
+    int n_inst = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    std::vector<DevInst> insts;
+    std::vector<ExcHost> exc;
+    std::vector<int> rec_off, n_rec, rece_off, n_rece;
+    std::vector<std::vector<int>> rece_map;  // record entry -> unique element record slot
+    int n_rec_total = 0, n_rece_slots = 0;
+    int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
+    long long band_total = 0;
+    int max_nip = 1;
+    size_t elem_smem = 0, inst_smem = 0;
+    int max_iters_global = 1;
+    std::vector<int> max_fibers_per_section;
+    // device
+    DevElem* d_elems = nullptr;
+    DevInst* d_insts = nullptr;
+    Geo geo;
+    FiberState fs;
+    double* d_estate = nullptr;
+    double* d_ek = nullptr;
+    double* d_ef = nullptr;
+    InstArrays A;
+    int* d_free_inst = nullptr;
+    int* d_free_dir = nullptr;
+    int* d_rec_dof = nullptr;
+    int* d_rece_base = nullptr;
+    int* d_elem_err = nullptr;
+    unsigned long long* d_counters = nullptr;
+    double* d_ag = nullptr;
+    int ag_cap = 0;
+    double* d_hist_disp = nullptr;
+    double* d_hist_ef = nullptr;
+    int* d_hist_iters = nullptr;
+    int hist_cap = 0;
+    int steps_done = 0;
+    int* h_ctrl = nullptr;  // pinned: nactive
+    bool state_determined = false;
+    double* d_rhs = nullptr;
+    std::vector<long long> elem_fibers;  // fibers per element (all families)
+    ~StrutHandle() {
+        for (void* p : allocs) cudaFree(p);
+        if (d_hist_disp) cudaFree(d_hist_disp);
+        if (d_hist_ef) cudaFree(d_hist_ef);
+        if (d_hist_iters) cudaFree(d_hist_iters);
+        if (d_ag) cudaFree(d_ag);
+        if (h_ctrl) cudaFreeHost(h_ctrl);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+static int launch_elements(StrutHandle* h) {
+    element_state_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), h->elem_smem, h->stream>>>(
+        h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->d_ek, h->d_ef, h->A.active,
+        h->A.status, h->d_elem_err, h->d_counters);
+    CK(cudaGetLastError());
+    return STRUT_OK;
+}
+
+static int launch_instances(StrutHandle* h, int mode, int step) {
+    InstArrays A = h->A;
+    A.hist_iters = (mode == INST_MODE_NEWTON && step >= 0) ? h->d_hist_iters + (size_t)step * h->n_inst
+                                                           : nullptr;
+    instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(h->d_insts, A, mode, step);
+    CK(cudaGetLastError());
+    return STRUT_OK;
+}
+
+static int ensure_history(StrutHandle* h, int need) {
+    if (need <= h->hist_cap) return STRUT_OK;
+    int cap = std::max(need, std::max(64, 2 * h->hist_cap));
+    double* nd = nullptr;
+    double* ne = nullptr;
+    int* ni = nullptr;
+    CK(cudaMalloc((void**)&nd, (size_t)cap * std::max(h->n_rec_total, 1) * sizeof(double)));
+    CK(cudaMalloc((void**)&ne, (size_t)cap * std::max(h->n_rece_slots, 1) * 6 * sizeof(double)));
+    CK(cudaMalloc((void**)&ni, (size_t)cap * h->n_inst * sizeof(int)));
+    CK(cudaMemset(ni, 0, (size_t)cap * h->n_inst * sizeof(int)));
+    if (h->hist_cap > 0 && h->steps_done > 0) {
+        CK(cudaMemcpy(nd, h->d_hist_disp, (size_t)h->steps_done * std::max(h->n_rec_total, 1) * sizeof(double),
+                      cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(ne, h->d_hist_ef, (size_t)h->steps_done * std::max(h->n_rece_slots, 1) * 6 * sizeof(double),
+                      cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(ni, h->d_hist_iters, (size_t)h->steps_done * h->n_inst * sizeof(int),
+                      cudaMemcpyDeviceToDevice));
+    }
+    if (h->d_hist_disp) cudaFree(h->d_hist_disp);
+    if (h->d_hist_ef) cudaFree(h->d_hist_ef);
+    if (h->d_hist_iters) cudaFree(h->d_hist_iters);
+    h->d_hist_disp = nd;
+    h->d_hist_ef = ne;
+    h->d_hist_iters = ni;
+    h->hist_cap = cap;
+    return STRUT_OK;
+}
+
+extern "C" {
+
+int strut_gpu_abi_version(void) { return STRUT_ABI_VERSION; }
+
+const char* strut_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_t device,
+                     StrutHandle** out) {
+    if (!models || num_instances <= 0 || !out) return fail(STRUT_BAD_ARG, "bad arguments");
+    *out = nullptr;
+    if (device >= 0) CK(cudaSetDevice(device));
+    StrutHandle* h = new StrutHandle();
+    int rc = STRUT_OK;
+    auto bail = [&](int code) {
+        delete h;
+        return code;
+    };
+    CK(cudaGetDevice(&h->device));
+    h->n_inst = num_instances;
+    std::vector<DevMat> mats;
+    SectionPack sp;
+    std::vector<DevElem> elems;
+    std::vector<double> Mff, Mrff, fconst;
+    std::vector<int> free_dof, free_inst, free_dir, rec_dof, rece_base;
+    std::vector<long long> slot_ptr(1, 0);
+    std::vector<int> slot_contrib;
+    std::vector<int> fint_ptr(1, 0), fint_contrib;
+    long long c2_total = 0, s2_total = 0, s1_total = 0;
+    std::vector<int> sec_base(num_instances);
+    int u_off = 0, f_off = 0;
+    long long band_off = 0;
+    h->insts.resize(num_instances);
+    h->exc.resize(num_instances);
+    h->rec_off.resize(num_instances);
+    h->n_rec.resize(num_instances);
+    h->rece_off.resize(num_instances);
+    h->n_rece.resize(num_instances);
+    h->rece_map.resize(num_instances);
+    for (int inst = 0; inst < num_instances; ++inst) {
+        const StrutModelDesc& d = models[inst];
+        if (d.ndm != 2 || d.ndf != 3) return bail(fail(STRUT_UNSUPPORTED, "only 2D frames (ndm 2, ndf 3)"));
+        if (d.num_free <= 0 || d.num_elements <= 0 || d.num_dofs != d.num_nodes * d.ndf)
+            return bail(fail(STRUT_BAD_ARG, "inconsistent model sizes"));
+        if (d.system != STRUT_SYSTEM_BAND_GENERAL && d.system != STRUT_SYSTEM_BAND_SPD)
+            return bail(fail(STRUT_UNSUPPORTED, "only BandGeneral and BandSPD"));
+        if (d.beta_k_comm != 0.0)
+            return bail(fail(STRUT_UNSUPPORTED, "rayleigh betaKComm is not implemented on this path"));
+        if (!(d.beta > 0.0) || !(d.dt > 0.0)) return bail(fail(STRUT_BAD_ARG, "Newmark beta and dt must be > 0"));
+        if (d.max_iters <= 0) return bail(fail(STRUT_BAD_ARG, "max_iters must be > 0"));
+        const int mat_base = (int)mats.size();
+        for (int i = 0; i < d.num_materials; ++i) mats.push_back(make_devmat(d.materials[i]));
+        sec_base[inst] = (int)sp.secs.size();
+        for (int s = 0; s < d.num_sections; ++s) {
+            rc = pack_section(d.materials, d.num_materials, d.fibers, d.sections[s].fiber_offset,
+                              d.sections[s].fiber_count, mat_base, sp);
+            if (rc != STRUT_OK) return bail(rc);
+        }
+        // free numbering / masses
+        int nf = d.num_free;
+        std::vector<int> free_of_dof(d.num_dofs);
+        bool has_mass = false;
+        std::vector<double> mff(nf, 0.0), mrff(nf, 0.0), fcf(nf, 0.0);
+        std::vector<int> fdof(nf, -1);
+        for (int dof = 0; dof < d.num_dofs; ++dof) {
+            const int fi = d.free_index[dof];
+            free_of_dof[dof] = fi;
+            if (fi < 0) continue;
+            if (fi >= nf) return bail(fail(STRUT_BAD_ARG, "free index out of range"));
+            fdof[fi] = dof;
+            if (d.mass[dof] != 0.0) {
+                mff[fi] += d.mass[dof] * 1.0 * 1.0;
+                has_mass = true;
+            }
+            if (d.mass_rayleigh && d.mass_rayleigh[dof] != 0.0) mrff[fi] += d.mass_rayleigh[dof] * 1.0 * 1.0;
+            if (d.f_const) fcf[fi] = d.f_const[dof];
+        }
+        if (!has_mass) return bail(fail(STRUT_BAD_ARG, "transient_nonlinear requires masses on free dofs"));
+        for (int fi = 0; fi < nf; ++fi) {
+            if (fdof[fi] < 0) return bail(fail(STRUT_BAD_ARG, "free numbering has holes"));
+            Mff.push_back(mff[fi]);
+            Mrff.push_back(mrff[fi]);
+            fconst.push_back(fcf[fi]);
+            free_dof.push_back(u_off + fdof[fi]);
+            free_inst.push_back(inst);
+            free_dir.push_back((fdof[fi] % d.ndf) + 1);
+        }
+        // elements
+        const int e0 = (int)elems.size();
+        int bw = 0;
+        std::vector<int> efree(6 * d.num_elements);
+        std::vector<int> rec_slot(d.num_elements, -1);
+        std::vector<int>& rmap = h->rece_map[inst];
+        int nslots = 0;
+        for (int j = 0; j < d.num_record_elements; ++j) {
+            const int re = d.record_elements[j];
+            if (re < 0 || re >= d.num_elements) return bail(fail(STRUT_BAD_ARG, "recorded element out of range"));
+            if (rec_slot[re] < 0) rec_slot[re] = nslots++;
+            rmap.push_back(rec_slot[re]);
+        }
+        for (int e = 0; e < d.num_elements; ++e) {
+            const StrutFrameElement& ed = d.elements[e];
+            if (ed.type != STRUT_ELEM_FORCE_BEAM_COLUMN_2D && ed.type != STRUT_ELEM_DISP_BEAM_COLUMN_2D)
+                return bail(fail(STRUT_UNSUPPORTED, "element type not implemented on this path"));
+            if (ed.geom != STRUT_GEOM_LINEAR && ed.geom != STRUT_GEOM_PDELTA)
+                return bail(fail(STRUT_UNSUPPORTED, "geomTransf must be Linear or PDelta"));
+            if (ed.section < 0 || ed.section >= d.num_sections || ed.integration < 0 ||
+                ed.integration >= d.num_integrations)
+                return bail(fail(STRUT_BAD_ARG, "element section / integration out of range"));
+            const StrutBeamIntegration& r = d.integrations[ed.integration];
+            if (r.num_int_pts < 1 || r.num_int_pts > kMaxIp)
+                return bail(fail(STRUT_BAD_ARG, "num_int_pts out of range"));
+            DevElem E;
+            std::memset(&E, 0, sizeof(E));
+            E.type = ed.type;
+            E.geom = ed.geom;
+            E.nip = r.num_int_pts;
+            E.sec = sec_base[inst] + ed.section;
+            E.inst = inst;
+            E.rec = rec_slot[e];
+            for (int a = 0; a < 6; ++a) {
+                if (ed.dof[a] < 0 || ed.dof[a] >= d.num_dofs) return bail(fail(STRUT_BAD_ARG, "element dof out of range"));
+                E.dof[a] = u_off + ed.dof[a];
+                efree[6 * e + a] = free_of_dof[ed.dof[a]];
+            }
+            const double x1 = d.node_coords[2 * ed.node_i], y1 = d.node_coords[2 * ed.node_i + 1];
+            const double x2 = d.node_coords[2 * ed.node_j], y2 = d.node_coords[2 * ed.node_j + 1];
+            const double dx = x2 - x1, dy = y2 - y1;
+            E.L = std::hypot(dx, dy);
+            if (E.L == 0.0) return bail(fail(STRUT_BAD_ARG, "zero-length element"));
+            E.inv_L = 1.0 / E.L;
+            E.c = dx * E.inv_L;
+            E.s = dy * E.inv_L;
+            E.c_div = dx / E.L;
+            E.s_div = dy / E.L;
+            E.L_sync = std::sqrt(dx * dx + dy * dy);
+            E.c_sync = dx / E.L_sync;
+            E.s_sync = dy / E.L_sync;
+            for (int ip = 0; ip < E.nip; ++ip) {
+                E.xi[ip] = r.xi[ip];
+                E.w[ip] = r.w[ip];
+            }
+            const DevSection& sd = sp.secs[E.sec];
+            E.s2_off = (int)s2_total;
+            E.s2_blk = round4(E.nip * sd.n_s2);
+            s2_total += E.s2_blk;
+            E.c2_off = (int)c2_total;
+            E.c2_blk = round4(E.nip * sd.n_c2);
+            c2_total += E.c2_blk;
+            E.s1_off = (int)s1_total;
+            E.s1_blk = round4(E.nip * sd.n_s1);
+            s1_total += E.s1_blk;
+            h->max_nip = std::max(h->max_nip, E.nip);
+            const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) + 4 * (size_t)E.s2_blk;
+            h->elem_smem = std::max(h->elem_smem, smem);
+            h->elem_fibers.push_back((long long)E.nip * (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
+            elems.push_back(E);
+            for (int a = 0; a < 6; ++a) {
+                const int ia = efree[6 * e + a];
+                if (ia < 0) continue;
+                for (int b = a + 1; b < 6; ++b) {
+                    const int ib = efree[6 * e + b];
+                    if (ib < 0) continue;
+                    bw = std::max(bw, std::abs(ia - ib));
+                }
+            }
+        }
+        const int rw = 2 * bw + 1;
+        // band slot contributions, element order (stiffness_internal_frame2d.mojo:594-619)
+        std::vector<std::vector<int>> slots((size_t)nf * rw);
+        std::vector<std::vector<int>> fcontr(nf);
+        for (int e = 0; e < d.num_elements; ++e) {
+            for (int a = 0; a < 6; ++a) {
+                const int ia = efree[6 * e + a];
+                if (ia < 0) continue;
+                for (int b = 0; b < 6; ++b) {
+                    const int ib = efree[6 * e + b];
+                    if (ib < 0) continue;
+                    slots[(size_t)ia * rw + (ib - ia + bw)].push_back((e0 + e) * 36 + a * 6 + b);
+                }
+                fcontr[ia].push_back((e0 + e) * 6 + a);
+            }
+        }
+        for (auto& v : slots) {
+            slot_contrib.insert(slot_contrib.end(), v.begin(), v.end());
+            slot_ptr.push_back((long long)slot_contrib.size());
+        }
+        for (auto& v : fcontr) {
+            fint_contrib.insert(fint_contrib.end(), v.begin(), v.end());
+            fint_ptr.push_back((int)fint_contrib.size());
+        }
+        DevInst I;
+        std::memset(&I, 0, sizeof(I));
+        I.n = nf;
+        I.bw = bw;
+        I.rw = rw;
+        I.num_dofs = d.num_dofs;
+        I.u_off = u_off;
+        I.f_off = f_off;
+        I.band_off = band_off;
+        I.slot_ptr_off = band_off;
+        I.fint_ptr_off = f_off;
+        I.max_iters = d.max_iters;
+        I.test_type = d.test_type;
+        I.spd = d.system == STRUT_SYSTEM_BAND_SPD;
+        I.has_damping = d.alpha_m != 0.0 || d.beta_k != 0.0 || d.beta_k_init != 0.0 || d.beta_k_comm != 0.0;
+        I.dt = d.dt;
+        I.gamma = d.gamma;
+        I.beta = d.beta;
+        I.a0 = 1.0 / (d.beta * d.dt * d.dt);
+        I.a1 = d.gamma / (d.beta * d.dt);
+        I.a2 = 1.0 / (d.beta * d.dt);
+        I.a3 = 1.0 / (2.0 * d.beta) - 1.0;
+        I.coeff = d.dt * d.dt * (0.5 - d.beta);
+        I.tol = d.tol;
+        I.alpha_m = d.alpha_m;
+        I.beta_k = d.beta_k;
+        I.beta_k_init = d.beta_k_init;
+        I.beta_k_comm = d.beta_k_comm;
+        I.rec_off = h->n_rec_total;
+        I.n_rec = d.num_record_dofs;
+        I.rece_off = h->n_rece_slots;
+        I.n_rece = nslots;
+        h->rec_off[inst] = h->n_rec_total;
+        h->n_rec[inst] = d.num_record_dofs;
+        h->rece_off[inst] = h->n_rece_slots;
+        h->n_rece[inst] = nslots;
+        rece_base.push_back(h->n_rece_slots);
+        for (int j = 0; j < d.num_record_dofs; ++j) {
+            if (d.record_dofs[j] < 0 || d.record_dofs[j] >= d.num_dofs) return bail(fail(STRUT_BAD_ARG, "record dof out of range"));
+            rec_dof.push_back(u_off + d.record_dofs[j]);
+        }
+        h->n_rec_total += d.num_record_dofs;
+        h->n_rece_slots += nslots;
+        const size_t ismem = ((size_t)nf * rw + 5 * (size_t)nf) * sizeof(double);
+        if (ismem > 220 * 1024)
+            return bail(fail(STRUT_UNSUPPORTED, "instance band does not fit in shared memory (n x (2bw+1) too large)"));
+        h->inst_smem = std::max(h->inst_smem, ismem);
+        h->max_iters_global = std::max(h->max_iters_global, d.max_iters);
+        h->insts[inst] = I;
+        // excitations
+        ExcHost& ex = h->exc[inst];
+        ex.num = d.num_excitations;
+        if (ex.num < 0 || ex.num > 2) return bail(fail(STRUT_BAD_ARG, "num_excitations must be 0..2"));
+        for (int x = 0; x < ex.num; ++x) {
+            ex.x[x] = d.excitation[x];
+            if (ex.x[x].direction < 1 || ex.x[x].direction > 2) return bail(fail(STRUT_BAD_ARG, "excitation direction must be 1 or 2"));
+            if (ex.x[x].count > 0 && !(ex.x[x].dt > 0.0)) return bail(fail(STRUT_BAD_ARG, "Path time series dt must be > 0"));
+            ex.vals[x].assign(ex.x[x].values, ex.x[x].values + ex.x[x].count);
+            ex.x[x].values = ex.vals[x].data();
+        }
+        if (ex.num == 2 && ex.x[0].direction == ex.x[1].direction)
+            return bail(fail(STRUT_BAD_ARG, "two excitations must act in different directions"));
+        u_off += d.num_dofs;
+        f_off += nf;
+        band_off += (long long)nf * rw;
+    }
+    h->n_free_total = f_off;
+    h->n_dofs_total = u_off;
+    h->n_elem = (int)elems.size();
+    h->band_total = band_off;
+    if (h->elem_smem > 200 * 1024) return bail(fail(STRUT_UNSUPPORTED, "element fiber history exceeds shared memory"));
+    h->elem_smem = std::max<size_t>(h->elem_smem, 16);
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaFuncSetAttribute(element_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->elem_smem));
+    CK(cudaFuncSetAttribute(instance_newton_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)std::max<size_t>(h->inst_smem, 16)));
+    auto& al = h->allocs;
+    // geometry and definitions
+    DevMat* d_mats;
+    DevSection* d_secs;
+    double *d_y, *d_a;
+    int* d_m;
+    if ((rc = upload(&d_mats, mats, al)) || (rc = upload(&d_secs, sp.secs, al)) ||
+        (rc = upload(&d_y, sp.y, al)) || (rc = upload(&d_a, sp.a, al)) || (rc = upload(&d_m, sp.m, al)) ||
+        (rc = upload(&h->d_elems, elems, al)) || (rc = upload(&h->d_insts, h->insts, al)))
+        return bail(rc);
+    h->geo.y = d_y;
+    h->geo.a = d_a;
+    h->geo.m = d_m;
+    h->geo.mats = d_mats;
+    h->geo.secs = d_secs;
+    // fiber history: committed state initialised from each material (core.mojo:203-263)
+    {
+        const long long c2n = round4((int)std::max<long long>(c2_total, 4));
+        const long long s2n = round4((int)std::max<long long>(s2_total, 4));
+        const long long s1n = round4((int)std::max<long long>(s1_total, 4));
+        std::vector<double> c2(5 * c2n, 0.0), s2(10 * s2n, 0.0), s1(5 * s1n, 0.0);
+        std::vector<int> kon(s2n, 0);
+        for (const DevElem& E : elems) {
+            const DevSection& sd = sp.secs[E.sec];
+            for (int ip = 0; ip < E.nip; ++ip) {
+                int base = sd.geo_off;
+                for (int j = 0; j < sd.n_s2; ++j) {
+                    const DevMat& m = mats[sp.m[base + j]];
+                    const long long idx = E.s2_off + ip * sd.n_s2 + j;
+                    s2[2 * s2n + idx] = m.p[1];
+                    s2[4 * s2n + idx] = m.k[S2K_EPSY];
+                    s2[3 * s2n + idx] = -m.k[S2K_EPSY];
+                    if (m.p[10] != 0.0) {
+                        s2[0 * s2n + idx] = m.k[S2K_SIGINI_E0];
+                        s2[1 * s2n + idx] = m.p[10];
+                    }
+                }
+                base += sd.n_s2;
+                for (int j = 0; j < sd.n_c2; ++j) {
+                    const DevMat& m = mats[sp.m[base + j]];
+                    c2[2 * c2n + E.c2_off + ip * sd.n_c2 + j] = m.k[C2K_EC0];
+                }
+                base += sd.n_c2;
+                for (int j = 0; j < sd.n_s1; ++j) {
+                    const DevMat& m = mats[sp.m[base + j]];
+                    s1[2 * s1n + E.s1_off + ip * sd.n_s1 + j] = m.p[1];
+                }
+            }
+        }
+        if ((rc = upload(&h->fs.c2, c2, al)) || (rc = upload(&h->fs.s2, s2, al)) ||
+            (rc = upload(&h->fs.s2_kon, kon, al)) || (rc = upload(&h->fs.s1, s1, al)))
+            return bail(rc);
+        h->fs.c2_n = c2n;
+        h->fs.s2_n = s2n;
+        h->fs.s1_n = s1n;
+    }
+    InstArrays& A = h->A;
+    std::memset(&A, 0, sizeof(A));
+    const size_t nF = h->n_free_total;
+    if ((rc = dzeros(&h->d_estate, (size_t)h->n_elem * kEStride, al)) ||
+        (rc = dzeros(&h->d_ek, (size_t)h->n_elem * 36, al)) ||
+        (rc = dzeros(&h->d_ef, (size_t)h->n_elem * 6, al)) || (rc = dzeros(&A.u_f, nF, al)) ||
+        (rc = dzeros(&A.v_f, nF, al)) || (rc = dzeros(&A.a_f, nF, al)) ||
+        (rc = dzeros(&A.u_n, nF, al)) || (rc = dzeros(&A.v_n, nF, al)) ||
+        (rc = dzeros(&A.a_n, nF, al)) || (rc = dzeros(&A.P_f, nF, al)) ||
+        (rc = dzeros(&A.du, nF, al)) || (rc = dzeros(&A.R, nF, al)) ||
+        (rc = dzeros(&A.u_full, (size_t)h->n_dofs_total, al)) ||
+        (rc = dzeros(&A.active, (size_t)h->n_inst, al)) ||
+        (rc = dzeros(&A.status, (size_t)h->n_inst, al)) ||
+        (rc = dzeros(&A.iters, (size_t)h->n_inst, al)) || (rc = dzeros(&A.nactive, 4, al)) ||
+        (rc = dzeros(&A.export_band, (size_t)h->band_total, al)) ||
+        (rc = dzeros(&A.export_f, nF, al)) || (rc = dzeros(&h->d_rhs, nF, al)) ||
+        (rc = dzeros(&h->d_elem_err, (size_t)h->n_elem, al)) ||
+        (rc = dzeros(&h->d_counters, 8, al)))
+        return bail(rc);
+    double* d_Mff;
+    double* d_Mrff;
+    double* d_fconst;
+    int* d_free_dof;
+    long long* d_slot_ptr;
+    int* d_slot_contrib;
+    int* d_fint_ptr;
+    int* d_fint_contrib;
+    double* d_Kinit;
+    if ((rc = upload(&d_Mff, Mff, al)) || (rc = upload(&d_Mrff, Mrff, al)) ||
+        (rc = upload(&d_fconst, fconst, al)) || (rc = upload(&d_free_dof, free_dof, al)) ||
+        (rc = upload(&h->d_free_inst, free_inst, al)) || (rc = upload(&h->d_free_dir, free_dir, al)) ||
+        (rc = upload(&d_slot_ptr, slot_ptr, al)) || (rc = upload(&d_slot_contrib, slot_contrib, al)) ||
+        (rc = upload(&d_fint_ptr, fint_ptr, al)) || (rc = upload(&d_fint_contrib, fint_contrib, al)) ||
+        (rc = upload(&h->d_rec_dof, rec_dof, al)) || (rc = upload(&h->d_rece_base, rece_base, al)) ||
+        (rc = dzeros(&d_Kinit, (size_t)h->band_total, al)))
+        return bail(rc);
+    A.Mff = d_Mff;
+    A.Mrff = d_Mrff;
+    A.fconst = d_fconst;
+    A.free_dof = d_free_dof;
+    A.slot_ptr = d_slot_ptr;
+    A.slot_contrib = d_slot_contrib;
+    A.fint_ptr = d_fint_ptr;
+    A.fint_contrib = d_fint_contrib;
+    A.ek = h->d_ek;
+    A.ef = h->d_ef;
+    A.Kinit = d_Kinit;
+    CK(cudaMallocHost((void**)&h->h_ctrl, 4 * sizeof(int)));
+    // initial assembly at the initial displacements (transient_nonlinear.mojo:1207-1453): K_init
+    // for betaKInit; the trial fiber state it produces is discarded (revert) by construction.
+    {
+        std::vector<int> ones(h->n_inst, 1);
+        CK(cudaMemcpy(A.active, ones.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice));
+        if ((rc = launch_elements(h)) != STRUT_OK) return bail(rc);
+        // Kinit = K gathered in element order; the export path of the instance kernel with
+        // a0 = a1 = 0 and no damping would equal K, but a dedicated gather keeps it exact.
+        std::vector<DevInst> tmp = h->insts;
+        for (auto& I : tmp) {
+            I.a0 = 0.0;
+            I.a1 = 0.0;
+            I.has_damping = 0;
+            I.spd = 0;
+        }
+        DevInst* d_tmp;
+        if ((rc = upload(&d_tmp, tmp, al))) return bail(rc);
+        InstArrays B = A;
+        B.export_band = d_Kinit;
+        instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(d_tmp, B, INST_MODE_EXPORT, -1);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+        std::vector<int> st(h->n_inst);
+        CK(cudaMemcpy(st.data(), A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < h->n_inst; ++i)
+            if (st[i] != 0) return bail(fail(st[i], "initial assembly failed for instance " + std::to_string(i)));
+    }
+    *out = h;
+    return STRUT_OK;
+}
+
+int strut_gpu_destroy(StrutHandle* h) {
+    if (!h) return STRUT_BAD_ARG;
+    cudaStreamSynchronize(h->stream);
+    delete h;
+    return STRUT_OK;
+}
+
+int strut_gpu_num_instances(const StrutHandle* h) { return h ? h->n_inst : 0; }
+
+int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) {
+    if (!h || n_steps < 0) return fail(STRUT_BAD_ARG, "bad arguments");
+    StrutStepStats st;
+    std::memset(&st, 0, sizeof(st));
+    st.failed_instance = -1;
+    st.failed_step = -1;
+    TRY(ensure_history(h, h->steps_done + n_steps));
+    // ground accelerations of every step of this call: per instance 2 values + 2 flags
+    if (h->ag_cap < n_steps) {
+        if (h->d_ag) cudaFree(h->d_ag);
+        h->d_ag = nullptr;
+        CK(cudaMalloc((void**)&h->d_ag, (size_t)n_steps * 4 * h->n_inst * sizeof(double)));
+        h->ag_cap = n_steps;
+    }
+    {
+        std::vector<double> ag((size_t)n_steps * 4 * h->n_inst, 0.0);
+        for (int s = 0; s < n_steps; ++s) {
+            const int step = h->steps_done + s;
+            for (int i = 0; i < h->n_inst; ++i) {
+                const double t = (double)(step + 1) * h->insts[i].dt;
+                double* row = &ag[((size_t)s * h->n_inst + i) * 4];
+                for (int x = 0; x < h->exc[i].num; ++x) {
+                    const int dir = h->exc[i].x[x].direction;
+                    row[dir - 1] = path_eval(h->exc[i].x[x], t);
+                    row[2 + dir - 1] = 1.0;
+                }
+            }
+        }
+        if (n_steps > 0)
+            CK(cudaMemcpyAsync(h->d_ag, ag.data(), ag.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    CK(cudaMemsetAsync(h->d_counters, 0, 8 * sizeof(unsigned long long), h->stream));
+    const int nF = h->n_free_total;
+    const int tb = 256;
+    int rc = STRUT_OK;
+    for (int s = 0; s < n_steps; ++s) {
+        const int step = h->steps_done;
+        CK(cudaMemsetAsync(h->A.nactive, 0, 4 * sizeof(int), h->stream));
+        const int npred = std::max(nF, h->n_inst);
+        predictor_kernel<<<(npred + tb - 1) / tb, tb, 0, h->stream>>>(
+            h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag + (size_t)s * 4 * h->n_inst, nF, h->n_inst);
+        CK(cudaGetLastError());
+        for (int it = 0; it < h->max_iters_global; ++it) {
+            TRY(launch_elements(h));
+            TRY(launch_instances(h, INST_MODE_NEWTON, step));
+            CK(cudaMemcpyAsync(h->h_ctrl, h->A.nactive, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            if (h->h_ctrl[0] <= 0) break;
+        }
+        std::vector<int> status(h->n_inst);
+        CK(cudaMemcpy(status.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < h->n_inst; ++i) {
+            if (status[i] != 0) {
+                st.failed_instance = i;
+                st.failed_step = step;
+                rc = status[i];
+                break;
+            }
+        }
+        if (rc != STRUT_OK) break;
+        commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
+            h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status,
+            h->d_hist_ef + (size_t)step * std::max(h->n_rece_slots, 1) * 6, h->d_rece_base);
+        CK(cudaGetLastError());
+        post_step_kernel<<<(nF + tb - 1) / tb, tb, 0, h->stream>>>(h->d_insts, h->A, h->d_free_inst, nF);
+        CK(cudaGetLastError());
+        if (h->n_rec_total > 0) {
+            record_disp_kernel<<<(h->n_rec_total + tb - 1) / tb, tb, 0, h->stream>>>(
+                h->A.u_full, h->d_rec_dof, h->n_rec_total, h->d_hist_disp + (size_t)step * h->n_rec_total);
+            CK(cudaGetLastError());
+        }
+        h->steps_done++;
+        st.steps_done++;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    unsigned long long cnt[8];
+    CK(cudaMemcpy(cnt, h->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+    st.local_element_iterations = (int64_t)cnt[0];
+    st.section_evaluations = (int64_t)cnt[1];
+    {
+        const int first = h->steps_done - st.steps_done;
+        if (st.steps_done > 0) {
+            std::vector<int> it((size_t)st.steps_done * h->n_inst);
+            CK(cudaMemcpy(it.data(), h->d_hist_iters + (size_t)first * h->n_inst, it.size() * sizeof(int),
+                          cudaMemcpyDeviceToHost));
+            long long tot = 0;
+            for (int v : it) tot += v;
+            st.global_newton_iterations = tot;
+            st.factorizations = tot;
+        }
+    }
+    // fiber updates: per section evaluation, the section's fiber count
+    st.fiber_updates = (int64_t)cnt[2];
+    st.status = rc;
+    if (rc != STRUT_OK) {
+        std::vector<int> ee(h->n_elem);
+        CK(cudaMemcpy(ee.data(), h->d_elem_err, sizeof(int) * h->n_elem, cudaMemcpyDeviceToHost));
+        g_last_error = "instance " + std::to_string(st.failed_instance) + " failed at step " +
+                       std::to_string(st.failed_step) + " with status " + std::to_string(rc);
+        if (rc == 6) g_last_error += " (BandGeneral needs the dense partial-pivot fallback)";
+    }
+    if (stats) *stats = st;
+    return rc;
+}
+
+int strut_gpu_get_history(StrutHandle* h, int32_t instance, double* disp, double* eforce,
+                          int32_t* iters) {
+    if (!h || instance < 0 || instance >= h->n_inst) return fail(STRUT_BAD_ARG, "bad arguments");
+    const int S = h->steps_done;
+    if (S == 0) return STRUT_OK;
+    if (disp && h->n_rec[instance] > 0) {
+        std::vector<double> all((size_t)S * h->n_rec_total);
+        CK(cudaMemcpy(all.data(), h->d_hist_disp, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < S; ++s)
+            for (int j = 0; j < h->n_rec[instance]; ++j)
+                disp[(size_t)s * h->n_rec[instance] + j] = all[(size_t)s * h->n_rec_total + h->rec_off[instance] + j];
+    }
+    if (eforce && !h->rece_map[instance].empty()) {
+        const int slots = std::max(h->n_rece_slots, 1);
+        std::vector<double> all((size_t)S * slots * 6);
+        CK(cudaMemcpy(all.data(), h->d_hist_ef, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        const auto& mp = h->rece_map[instance];
+        for (int s = 0; s < S; ++s)
+            for (size_t j = 0; j < mp.size(); ++j)
+                for (int c = 0; c < 6; ++c)
+                    eforce[((size_t)s * mp.size() + j) * 6 + c] =
+                        all[((size_t)s * slots + h->rece_off[instance] + mp[j]) * 6 + c];
+    }
+    if (iters) {
+        std::vector<int> all((size_t)S * h->n_inst);
+        CK(cudaMemcpy(all.data(), h->d_hist_iters, all.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < S; ++s) iters[s] = all[(size_t)s * h->n_inst + instance];
+    }
+    return STRUT_OK;
+}
+
+int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int32_t* iters) {
+    if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
+    const int S = h->steps_done;
+    if (S == 0) return STRUT_OK;
+    if (disp && h->n_rec_total > 0) {
+        std::vector<double> all((size_t)S * h->n_rec_total);
+        CK(cudaMemcpy(all.data(), h->d_hist_disp, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        size_t o = 0;
+        for (int i = 0; i < h->n_inst; ++i)
+            for (int s = 0; s < S; ++s)
+                for (int j = 0; j < h->n_rec[i]; ++j) disp[o++] = all[(size_t)s * h->n_rec_total + h->rec_off[i] + j];
+    }
+    if (eforce) {
+        const int slots = std::max(h->n_rece_slots, 1);
+        std::vector<double> all((size_t)S * slots * 6);
+        CK(cudaMemcpy(all.data(), h->d_hist_ef, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        size_t o = 0;
+        for (int i = 0; i < h->n_inst; ++i) {
+            const auto& mp = h->rece_map[i];
+            for (int s = 0; s < S; ++s)
+                for (size_t j = 0; j < mp.size(); ++j)
+                    for (int c = 0; c < 6; ++c)
+                        eforce[o++] = all[((size_t)s * slots + h->rece_off[i] + mp[j]) * 6 + c];
+        }
+    }
+    if (iters) {
+        std::vector<int> all((size_t)S * h->n_inst);
+        CK(cudaMemcpy(all.data(), h->d_hist_iters, all.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        size_t o = 0;
+        for (int i = 0; i < h->n_inst; ++i)
+            for (int s = 0; s < S; ++s) iters[o++] = all[(size_t)s * h->n_inst + i];
+    }
+    return STRUT_OK;
+}
+
+int strut_gpu_get_state(StrutHandle* h, int32_t instance, double* u_free, double* v_free,
+                        double* a_free) {
+    if (!h || instance < 0 || instance >= h->n_inst) return fail(STRUT_BAD_ARG, "bad arguments");
+    const DevInst& I = h->insts[instance];
+    CK(cudaStreamSynchronize(h->stream));
+    if (u_free) CK(cudaMemcpy(u_free, h->A.u_f + I.f_off, I.n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (v_free) CK(cudaMemcpy(v_free, h->A.v_f + I.f_off, I.n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (a_free) CK(cudaMemcpy(a_free, h->A.a_f + I.f_off, I.n * sizeof(double), cudaMemcpyDeviceToHost));
+    return STRUT_OK;
+}
+
+int strut_gpu_band_info(const StrutHandle* h, int32_t instance, int32_t* half_bw, int32_t* row_width) {
+    if (!h || instance < 0 || instance >= h->n_inst) return fail(STRUT_BAD_ARG, "bad arguments");
+    const DevInst& I = h->insts[instance];
+    if (half_bw) *half_bw = I.bw;
+    if (row_width) *row_width = I.spd ? I.bw + 1 : I.rw;
+    return STRUT_OK;
+}
+
+int strut_gpu_state_determination(StrutHandle* h, const double* u_free, double* f_int_free,
+                                  double* band_out) {
+    if (!h || !u_free) return fail(STRUT_BAD_ARG, "bad arguments");
+    const int nF = h->n_free_total;
+    CK(cudaMemcpyAsync(h->A.u_f, u_free, nF * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    scatter_free_kernel<<<(nF + 255) / 256, 256, 0, h->stream>>>(h->A.u_f, h->A.free_dof, h->A.u_full, nF);
+    CK(cudaGetLastError());
+    std::vector<int> ones(h->n_inst, 1), zeros(h->n_inst, 0);
+    CK(cudaMemcpyAsync(h->A.active, ones.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->A.status, zeros.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));
+    TRY(launch_elements(h));
+    TRY(launch_instances(h, INST_MODE_EXPORT, -1));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int> st(h->n_inst);
+    CK(cudaMemcpy(st.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < h->n_inst; ++i)
+        if (st[i] != 0) return fail(st[i], "state determination failed for instance " + std::to_string(i));
+    if (f_int_free) CK(cudaMemcpy(f_int_free, h->A.export_f, nF * sizeof(double), cudaMemcpyDeviceToHost));
+    if (band_out) {
+        std::vector<double> band((size_t)h->band_total);
+        CK(cudaMemcpy(band.data(), h->A.export_band, band.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        size_t o = 0;
+        for (int i = 0; i < h->n_inst; ++i) {
+            const DevInst& I = h->insts[i];
+            for (int r = 0; r < I.n; ++r) {
+                if (I.spd) {
+                    for (int k = 0; k <= I.bw; ++k) {  // slot row*(bw+1) + (row - col)
+                        const int col = r - k;
+                        band_out[o++] = col >= 0 ? band[I.band_off + (size_t)r * I.rw + (col - r + I.bw)] : 0.0;
+                    }
+                } else {
+                    for (int k = 0; k < I.rw; ++k) band_out[o++] = band[I.band_off + (size_t)r * I.rw + k];
+                }
+            }
+        }
+    }
+    h->state_determined = true;
+    return STRUT_OK;
+}
+
+int strut_gpu_factor_solve(StrutHandle* h, const double* rhs, double* du) {
+    if (!h || !rhs || !du) return fail(STRUT_BAD_ARG, "bad arguments");
+    if (!h->state_determined) return fail(STRUT_BAD_ARG, "call strut_gpu_state_determination first");
+    const int nF = h->n_free_total;
+    CK(cudaMemcpyAsync(h->d_rhs, rhs, nF * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    InstArrays A = h->A;
+    A.rhs_in = h->d_rhs;
+    std::vector<int> zeros(h->n_inst, 0);
+    CK(cudaMemcpyAsync(h->A.status, zeros.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));
+    instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(h->d_insts, A, INST_MODE_SOLVE_EXPORTED, -1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int> st(h->n_inst);
+    CK(cudaMemcpy(st.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < h->n_inst; ++i)
+        if (st[i] != 0) return fail(st[i], "factorization failed for instance " + std::to_string(i));
+    CK(cudaMemcpy(du, h->A.du, nF * sizeof(double), cudaMemcpyDeviceToHost));
+    return STRUT_OK;
+}
+
+int strut_gpu_commit(StrutHandle* h) {
+    if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
+    commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate,
+                                                                 h->A.status, nullptr, h->d_rece_base);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    return STRUT_OK;
+}
+
+int strut_gpu_revert(StrutHandle* h) {
+    // Trial fiber state is never stored (it is recomputed from committed state on demand), so
+    // committed -> trial has nothing to copy.
+    if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
+    return STRUT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// known-answer drivers and batched section evaluation
+// ---------------------------------------------------------------------------------------
+struct StrutSectionBatch {
+    int n_inst = 0;
+    std::vector<void*> allocs;
+    Geo geo;
+    DevSection sd;
+    BatchState bs;
+    ~StrutSectionBatch() {
+        for (void* p : allocs) cudaFree(p);
+    }
+};
+
+extern "C" {
+
+int strut_gpu_material_path(const StrutUniMaterial* material, const double* strains, int32_t n,
+                            double* out) {
+    if (!material || (n > 0 && (!strains || !out)) || n < 0) return fail(STRUT_BAD_ARG, "bad arguments");
+    if (n == 0) return STRUT_OK;
+    DevMat m = make_devmat(*material);
+    if (m.type == STRUT_MAT_CONCRETE01) return fail(STRUT_UNSUPPORTED, "Concrete01 not implemented on this path");
+    double *d_s = nullptr, *d_o = nullptr;
+    CK(cudaMalloc((void**)&d_s, n * sizeof(double)));
+    CK(cudaMalloc((void**)&d_o, 2 * n * sizeof(double)));
+    CK(cudaMemcpy(d_s, strains, n * sizeof(double), cudaMemcpyHostToDevice));
+    material_path_kernel<<<1, 32>>>(m, d_s, n, d_o);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out, d_o, 2 * n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d_s);
+    cudaFree(d_o);
+    if (e != cudaSuccess) return fail(STRUT_CUDA_ERROR, cudaGetErrorString(e));
+    return STRUT_OK;
+}
+
+int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t num_materials,
+                                   const StrutFiber* fibers, int32_t num_fibers, int32_t n_inst,
+                                   StrutSectionBatch** out) {
+    if (!materials || !fibers || num_fibers <= 0 || n_inst <= 0 || !out) return fail(STRUT_BAD_ARG, "bad arguments");
+    *out = nullptr;
+    SectionPack sp;
+    int rc = pack_section(materials, num_materials, fibers, 0, num_fibers, 0, sp);
+    if (rc != STRUT_OK) return rc;
+    std::vector<DevMat> mats;
+    for (int i = 0; i < num_materials; ++i) mats.push_back(make_devmat(materials[i]));
+    StrutSectionBatch* b = new StrutSectionBatch();
+    b->n_inst = n_inst;
+    b->sd = sp.secs[0];
+    DevMat* d_mats;
+    DevSection* d_secs;
+    double *d_y, *d_a;
+    int* d_m;
+    auto& al = b->allocs;
+    if ((rc = upload(&d_mats, mats, al)) || (rc = upload(&d_secs, sp.secs, al)) || (rc = upload(&d_y, sp.y, al)) ||
+        (rc = upload(&d_a, sp.a, al)) || (rc = upload(&d_m, sp.m, al))) {
+        delete b;
+        return rc;
+    }
+    b->geo.y = d_y;
+    b->geo.a = d_a;
+    b->geo.m = d_m;
+    b->geo.mats = d_mats;
+    b->geo.secs = d_secs;
+    const DevSection& sd = b->sd;
+    const long long n2 = (long long)n_inst * sd.n_s2, n3 = (long long)n_inst * sd.n_c2, n1 = (long long)n_inst * sd.n_s1;
+    std::vector<double> s2(10 * std::max<long long>(n2, 1), 0.0), c2(5 * std::max<long long>(n3, 1), 0.0),
+        s1(5 * std::max<long long>(n1, 1), 0.0);
+    std::vector<int> kon(std::max<long long>(n2, 1), 0);
+    for (long long i = 0; i < n_inst; ++i) {
+        int base = sd.geo_off;
+        for (int j = 0; j < sd.n_s2; ++j) {
+            const DevMat& m = mats[sp.m[base + j]];
+            const long long idx = i * sd.n_s2 + j;
+            s2[2 * n2 + idx] = m.p[1];
+            s2[4 * n2 + idx] = m.k[S2K_EPSY];
+            s2[3 * n2 + idx] = -m.k[S2K_EPSY];
+            if (m.p[10] != 0.0) {
+                s2[idx] = m.k[S2K_SIGINI_E0];
+                s2[n2 + idx] = m.p[10];
+            }
+        }
+        base += sd.n_s2;
+        for (int j = 0; j < sd.n_c2; ++j) c2[2 * n3 + i * sd.n_c2 + j] = mats[sp.m[base + j]].k[C2K_EC0];
+        base += sd.n_c2;
+        for (int j = 0; j < sd.n_s1; ++j) s1[2 * n1 + i * sd.n_s1 + j] = mats[sp.m[base + j]].p[1];
+    }
+    if ((rc = upload(&b->bs.s2, s2, al)) || (rc = upload(&b->bs.c2, c2, al)) || (rc = upload(&b->bs.s1, s1, al)) ||
+        (rc = upload(&b->bs.kon, kon, al))) {
+        delete b;
+        return rc;
+    }
+    b->bs.n_inst = n_inst;
+    *out = b;
+    return STRUT_OK;
+}
+
+int strut_gpu_section_batch_destroy(StrutSectionBatch* b) {
+    if (!b) return STRUT_BAD_ARG;
+    cudaDeviceSynchronize();
+    delete b;
+    return STRUT_OK;
+}
+
+int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_dev, double* resp_dev,
+                                 int32_t commit, void* stream) {
+    if (!b || !eps0_kappa_dev || !resp_dev) return fail(STRUT_BAD_ARG, "bad arguments");
+    const long long threads = (long long)b->n_inst * 32;
+    const int tb = 256;
+    section_batch_kernel<<<(unsigned)((threads + tb - 1) / tb), tb, 0, (cudaStream_t)stream>>>(
+        b->geo, b->sd, b->bs, eps0_kappa_dev, resp_dev, commit ? 1 : 0);
+    CK(cudaGetLastError());
+    return STRUT_OK;
+}
+
+int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double* out, int32_t* n_fibers) {
+    if (!b || instance < 0 || instance >= b->n_inst) return fail(STRUT_BAD_ARG, "bad arguments");
+    const DevSection& sd = b->sd;
+    const int nf = sd.n_s2 + sd.n_c2 + sd.n_s1;
+    if (n_fibers) *n_fibers = nf;
+    if (!out) return STRUT_OK;
+    CK(cudaDeviceSynchronize());
+    // 16 doubles per fiber: eps, sig, tan, then the family's history fields, then kon
+    std::vector<double> o((size_t)nf * 16, 0.0);
+    const long long n2 = (long long)b->n_inst * sd.n_s2, n3 = (long long)b->n_inst * sd.n_c2,
+                    n1 = (long long)b->n_inst * sd.n_s1;
+    for (int j = 0; j < sd.n_s2; ++j) {
+        for (int f = 0; f < 10; ++f)
+            CK(cudaMemcpy(&o[(size_t)j * 16 + f], b->bs.s2 + f * n2 + (long long)instance * sd.n_s2 + j, sizeof(double),
+                          cudaMemcpyDeviceToHost));
+        int kon = 0;
+        CK(cudaMemcpy(&kon, b->bs.kon + (long long)instance * sd.n_s2 + j, sizeof(int), cudaMemcpyDeviceToHost));
+        o[(size_t)j * 16 + 15] = kon;
+    }
+    for (int j = 0; j < sd.n_c2; ++j)
+        for (int f = 0; f < 5; ++f)
+            CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + j) * 16 + f], b->bs.c2 + f * n3 + (long long)instance * sd.n_c2 + j,
+                          sizeof(double), cudaMemcpyDeviceToHost));
+    for (int j = 0; j < sd.n_s1; ++j)
+        for (int f = 0; f < 5; ++f)
+            CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + sd.n_c2 + j) * 16 + f],
+                          b->bs.s1 + f * n1 + (long long)instance * sd.n_s1 + j, sizeof(double), cudaMemcpyDeviceToHost));
+    std::memcpy(out, o.data(), o.size() * sizeof(double));
+    return STRUT_OK;
+}
+
+int strut_gpu_section_path(const StrutUniMaterial* materials, int32_t num_materials, const StrutFiber* fibers,
+                           int32_t num_fibers, const double* eps0_kappa, int32_t n_points, double* out) {
+    if (n_points < 0 || (n_points > 0 && (!eps0_kappa || !out))) return fail(STRUT_BAD_ARG, "bad arguments");
+    StrutSectionBatch* b = nullptr;
+    int rc = strut_gpu_section_batch_create(materials, num_materials, fibers, num_fibers, 1, &b);
+    if (rc != STRUT_OK) return rc;
+    double *d_ek = nullptr, *d_r = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d_ek, 2 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_r, 5 * sizeof(double));
+    for (int p = 0; p < n_points && e == cudaSuccess && rc == STRUT_OK; ++p) {
+        e = cudaMemcpy(d_ek, eps0_kappa + 2 * p, 2 * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) break;
+        rc = strut_gpu_section_eval_batch(b, d_ek, d_r, 1, nullptr);
+        if (rc != STRUT_OK) break;
+        e = cudaMemcpy(out + 5 * p, d_r, 5 * sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    if (d_ek) cudaFree(d_ek);
+    if (d_r) cudaFree(d_r);
+    strut_gpu_section_batch_destroy(b);
+    if (e != cudaSuccess) return fail(STRUT_CUDA_ERROR, cudaGetErrorString(e));
+    return rc;
+}
+
+}  // extern "C"

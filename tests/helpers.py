@@ -1,0 +1,74 @@
+"""Shared helpers for the test-suite (cases and comparisons)."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def lcg_strains(seed: int, n: int, scale: float, kind: str = "walk") -> np.ndarray:
+    """Deterministic strain scenarios in the spirit of Strut's material micro-benchmark
+    (src/mojo/material_compare_micro.mojo:288-368): a 64-bit LCG drives a random walk or a
+    cyclic ramp with growing amplitude."""
+    mask = (1 << 64) - 1
+    state = (seed * 2862933555777941757 + 3037000493) & mask
+    out = np.zeros(n)
+    x = 0.0
+    for i in range(n):
+        state = (state * 6364136223846793005 + 1442695040888963407) & mask
+        r = (state >> 11) / float(1 << 53)
+        if kind == "walk":
+            x += (r - 0.5) * scale
+        else:
+            amp = scale * (1.0 + i / n * 4.0)
+            x = amp * np.sin(2.0 * np.pi * i / 37.0) + (r - 0.5) * scale * 0.1
+        out[i] = x
+    return out
+
+
+def mixed_section_case(order):
+    """Restated from tests/unit/test_fiber_section.py:263-361 of the reference."""
+    layers = []
+    for material, y, area in order:
+        layers.append({"type": "straight", "material": material, "num_bars": 1, "bar_area": area,
+                       "y_start": y, "z_start": 0.0, "y_end": y, "z_end": 0.0})
+    return {
+        "materials": [
+            {"id": 1, "type": "Concrete02", "params": {"fpc": -32.0, "epsc0": -0.0021, "fpcu": -18.0,
+                                                        "epscu": -0.0058, "rat": 0.12, "ft": 2.8, "Ets": 180.0}},
+            {"id": 2, "type": "Concrete02", "params": {"fpc": -36.0, "epsc0": -0.0024, "fpcu": -21.0,
+                                                        "epscu": -0.0064, "rat": 0.1, "ft": 3.1, "Ets": 220.0}},
+            {"id": 3, "type": "Steel02", "params": {"Fy": 420.0, "E0": 200000.0, "b": 0.012, "R0": 18.0,
+                                                     "cR1": 0.925, "cR2": 0.15, "a1": 0.01, "a2": 1.0,
+                                                     "a3": 0.01, "a4": 1.0}},
+            {"id": 4, "type": "Steel02", "params": {"Fy": 460.0, "E0": 200000.0, "b": 0.01, "R0": 20.0,
+                                                     "cR1": 0.92, "cR2": 0.18, "a1": 0.015, "a2": 1.0,
+                                                     "a3": 0.015, "a4": 1.0}},
+        ],
+        "section": {"id": 9, "type": "FiberSection2d", "params": {"patches": [], "layers": layers}},
+        "deformation_path": [
+            {"eps0": -8.0e-4, "kappa": 6.0e-3},
+            {"eps0": -1.6e-3, "kappa": 1.0e-2},
+            {"eps0": -2.0e-4, "kappa": -4.0e-3},
+            {"eps0": 4.0e-4, "kappa": -8.0e-3},
+            {"eps0": -6.0e-4, "kappa": 5.0e-3},
+        ],
+    }
+
+
+ALTERNATING = [(1, -0.30, 0.0042), (3, -0.24, 0.00045), (2, -0.10, 0.0040), (4, -0.04, 0.00055),
+               (3, 0.04, 0.00045), (1, 0.10, 0.0042), (4, 0.24, 0.00055), (2, 0.30, 0.0040)]
+GROUPED = [(1, -0.30, 0.0042), (1, 0.10, 0.0042), (2, -0.10, 0.0040), (2, 0.30, 0.0040),
+           (3, -0.24, 0.00045), (3, 0.04, 0.00045), (4, -0.04, 0.00055), (4, 0.24, 0.00055)]
+
+
+def path_array(case):
+    return np.array([[p["eps0"], p["kappa"]] for p in case["deformation_path"]])
+
+
+def rel_err_of_peak(a, b):
+    """max |a - b| / max |b| over a history (the 'within x of peak response' measure)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    peak = np.max(np.abs(b))
+    if peak == 0.0:
+        return float(np.max(np.abs(a - b)))
+    return float(np.max(np.abs(a - b)) / peak)
