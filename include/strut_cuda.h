@@ -192,6 +192,16 @@ typedef struct StrutStepStats {
 
 typedef struct StrutHandle StrutHandle;
 
+/* Per-kernel timing of a handle's launches, measured with CUDA events on the handle's own
+ * stream while profiling is enabled (no counterpart in the reference; used for rooflines).
+ * Index: 0 element state, 1 instance Newton, 2 commit, 3 predictor, 4 post-step. */
+#define STRUT_PROF_KERNELS 8
+typedef struct StrutKernelProfile {
+    int64_t launches[STRUT_PROF_KERNELS];
+    double ms[STRUT_PROF_KERNELS];
+    double bytes[STRUT_PROF_KERNELS];   /* algorithmic HBM bytes moved by those launches */
+} StrutKernelProfile;
+
 /* ---- library ----------------------------------------------------------------------- */
 int strut_gpu_abi_version(void);
 /* Human readable text of the last error on this thread (never NULL). */
@@ -219,6 +229,12 @@ int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int3
 /* Current free displacement / velocity / acceleration vectors of one instance. */
 int strut_gpu_get_state(StrutHandle* h, int32_t instance, double* u_free, double* v_free,
                         double* a_free);
+
+/* Enables / disables per-launch event timing; enabling clears the accumulated profile. */
+int strut_gpu_set_profiling(StrutHandle* h, int32_t enabled);
+int strut_gpu_get_profile(const StrutHandle* h, StrutKernelProfile* out);
+/* The cudaStream_t every kernel of this handle is launched on (for callers' own events). */
+void* strut_gpu_stream(const StrutHandle* h);
 
 /* ---- single-iteration entries (parity tests) --------------------------------------- */
 /* Sets the trial free displacements of every instance (concatenated in instance order),

@@ -163,6 +163,21 @@ class StrutStepStats(C.Structure):
     ]
 
 
+class StrutKernelProfile(C.Structure):
+    _fields_ = [
+        ("launches", C.c_int64 * 8),
+        ("ms", C.c_double * 8),
+        ("bytes", C.c_double * 8),
+    ]
+
+
+PROF_ELEMENT = 0
+PROF_INSTANCE = 1
+PROF_COMMIT = 2
+PROF_PREDICTOR = 3
+PROF_POST = 4
+
+
 # Every function the header declares, with its ctypes signature.  Used by the binding and by
 # the test that checks the built library exports all of them.
 EXPORTS = {
@@ -178,6 +193,9 @@ EXPORTS = {
     "strut_gpu_get_history": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, _ip]),
     "strut_gpu_get_history_all": (C.c_int, [C.c_void_p, _dp, _dp, _ip]),
     "strut_gpu_get_state": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, _dp]),
+    "strut_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "strut_gpu_get_profile": (C.c_int, [C.c_void_p, C.POINTER(StrutKernelProfile)]),
+    "strut_gpu_stream": (C.c_void_p, [C.c_void_p]),
     "strut_gpu_state_determination": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "strut_gpu_band_info": (C.c_int, [C.c_void_p, C.c_int32, _ip, _ip]),
     "strut_gpu_factor_solve": (C.c_int, [C.c_void_p, _dp, _dp]),

@@ -636,6 +636,7 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
         if (tid < 36) ek[(size_t)e * 36 + tid] = S.k[tid];
         else if (tid < 42) ef[(size_t)e * 6 + tid - 36] = S.f[tid - 36];
         if (tid == 0) {
+            atomicAdd(&counters[3], (unsigned long long)E.io_bytes);
             atomicAdd(&counters[1], (unsigned long long)nip);
             atomicAdd(&counters[2], (unsigned long long)nip *
                                         (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
@@ -865,6 +866,7 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
         }
         k_to_global(S.k, E.c, E.s);
         f_to_global(S.f, E.c, E.s);
+        atomicAdd(&counters[3], (unsigned long long)E.io_bytes);
         atomicAdd(&counters[0], (unsigned long long)S.local_iters);
         atomicAdd(&counters[1], (unsigned long long)S.section_evals);
         atomicAdd(&counters[2], (unsigned long long)S.section_evals *

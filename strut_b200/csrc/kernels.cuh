@@ -45,6 +45,8 @@ struct DevElem {
     int s2_blk, c2_blk, s1_blk; // block lengths (multiples of 4)
     double L, inv_L, c, s, c_div, s_div, L_sync, c_sync, s_sync;
     double xi[kMaxIp], w[kMaxIp];
+    double io_bytes;            // algorithmic HBM bytes of one state determination
+    double commit_bytes;        // algorithmic HBM bytes of one commit
 };
 
 struct DevInst {
@@ -57,6 +59,7 @@ struct DevInst {
     int rec_off, n_rec, rece_off, n_rece;
     double a0, a1, a2, a3, dt, gamma, beta, coeff, tol;
     double alpha_m, beta_k, beta_k_init, beta_k_comm;
+    double io_bytes;  // algorithmic HBM bytes of one Newton iteration of this instance
 };
 
 struct FiberState {

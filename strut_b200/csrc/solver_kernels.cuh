@@ -44,6 +44,7 @@ struct InstArrays {
     double* export_band;  // band per instance (BandGeneral rw / BandSPD bw+1 layout)
     double* export_f;     // F_int at free dofs
     const double* rhs_in; // INST_MODE_SOLVE_EXPORTED
+    unsigned long long* bytes_counter;
 };
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -226,7 +227,10 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
         for (int i = tid; i < n; i += nt) R[i] = A.rhs_in[f0 + i];
         __syncthreads();
     } else {
-        if (mode == INST_MODE_NEWTON && tid == 0) A.iters[inst] += 1;
+        if (mode == INST_MODE_NEWTON && tid == 0) {
+            A.iters[inst] += 1;
+            if (A.bytes_counter) atomicAdd(A.bytes_counter, (unsigned long long)I.io_bytes);
+        }
         // v_trial, a_trial (transient_nonlinear.mojo:496-531)
         for (int i = tid; i < n; i += nt) {
             const int gi = f0 + i;

@@ -258,8 +258,12 @@ struct StrutHandle {
     int steps_done = 0;
     int* h_ctrl = nullptr;  // pinned: nactive
     bool state_determined = false;
+    bool prof = false;
+    StrutKernelProfile P;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double* d_rhs = nullptr;
     std::vector<long long> elem_fibers;  // fibers per element (all families)
+    double commit_bytes_total = 0.0;
     ~StrutHandle() {
         for (void* p : allocs) cudaFree(p);
         if (d_hist_disp) cudaFree(d_hist_disp);
@@ -267,15 +271,35 @@ struct StrutHandle {
         if (d_hist_iters) cudaFree(d_hist_iters);
         if (d_ag) cudaFree(d_ag);
         if (h_ctrl) cudaFreeHost(h_ctrl);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
     }
 };
 
+static int prof_begin(StrutHandle* h) {
+    if (h->prof) CK(cudaEventRecord(h->ev0, h->stream));
+    return STRUT_OK;
+}
+
+static int prof_end(StrutHandle* h, int k) {
+    if (!h->prof) return STRUT_OK;
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->P.ms[k] += ms;
+    h->P.launches[k] += 1;
+    return STRUT_OK;
+}
+
 static int launch_elements(StrutHandle* h) {
+    TRY(prof_begin(h));
     element_state_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), h->elem_smem, h->stream>>>(
         h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->d_ek, h->d_ef, h->A.active,
         h->A.status, h->d_elem_err, h->d_counters);
     CK(cudaGetLastError());
+    TRY(prof_end(h, 0));
     return STRUT_OK;
 }
 
@@ -283,8 +307,11 @@ static int launch_instances(StrutHandle* h, int mode, int step) {
     InstArrays A = h->A;
     A.hist_iters = (mode == INST_MODE_NEWTON && step >= 0) ? h->d_hist_iters + (size_t)step * h->n_inst
                                                            : nullptr;
+    A.bytes_counter = h->d_counters + 4;
+    TRY(prof_begin(h));
     instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(h->d_insts, A, mode, step);
     CK(cudaGetLastError());
+    TRY(prof_end(h, 1));
     return STRUT_OK;
 }
 
@@ -471,6 +498,15 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) + 4 * (size_t)E.s2_blk;
             h->elem_smem = std::max(h->elem_smem, smem);
             h->elem_fibers.push_back((long long)E.nip * (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
+            {
+                // committed history read once (Concrete02 / Steel01 5 doubles, Steel02 10
+                // doubles + kon), element state read + written, k and f written, 6 dofs read,
+                // the element record itself
+                const double fib = (double)E.nip * (40.0 * sd.n_c2 + 84.0 * sd.n_s2 + 40.0 * sd.n_s1);
+                const double est = 8.0 * (6 + 2 * E.nip);
+                E.io_bytes = fib + 2.0 * est + 8.0 * 42 + 8.0 * 6 + (double)sizeof(DevElem);
+                E.commit_bytes = 2.0 * fib + est + 8.0 * 6 + (double)sizeof(DevElem);
+            }
             elems.push_back(E);
             for (int a = 0; a < 6; ++a) {
                 const int ia = efree[6 * e + a];
@@ -534,6 +570,15 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         I.beta_k = d.beta_k;
         I.beta_k_init = d.beta_k_init;
         I.beta_k_comm = d.beta_k_comm;
+        {
+            // gathered element k / f entries, the band written to shared memory is not HBM;
+            // K_init band, the gather lists, and the free-dof vectors
+            long long ncontrib = 0, nfc = 0;
+            for (auto& v : slots) ncontrib += (long long)v.size();
+            for (auto& v : fcontr) nfc += (long long)v.size();
+            I.io_bytes = 12.0 * ncontrib + 12.0 * nfc + 8.0 * (double)nf * rw * (d.beta_k_init != 0.0) +
+                         8.0 * ((double)nf * rw + 1) + 8.0 * 14.0 * nf;
+        }
         I.rec_off = h->n_rec_total;
         I.n_rec = d.num_record_dofs;
         I.rece_off = h->n_rece_slots;
@@ -572,6 +617,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         f_off += nf;
         band_off += (long long)nf * rw;
     }
+    for (const DevElem& E : elems) h->commit_bytes_total += E.commit_bytes;
     h->n_free_total = f_off;
     h->n_dofs_total = u_off;
     h->n_elem = (int)elems.size();
@@ -686,6 +732,9 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     A.ef = h->d_ef;
     A.Kinit = d_Kinit;
     CK(cudaMallocHost((void**)&h->h_ctrl, 4 * sizeof(int)));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    std::memset(&h->P, 0, sizeof(h->P));
     // initial assembly at the initial displacements (transient_nonlinear.mojo:1207-1453): K_init
     // for betaKInit; the trial fiber state it produces is discarded (revert) by construction.
     {
@@ -766,9 +815,11 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
         const int step = h->steps_done;
         CK(cudaMemsetAsync(h->A.nactive, 0, 4 * sizeof(int), h->stream));
         const int npred = std::max(nF, h->n_inst);
+        TRY(prof_begin(h));
         predictor_kernel<<<(npred + tb - 1) / tb, tb, 0, h->stream>>>(
             h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag + (size_t)s * 4 * h->n_inst, nF, h->n_inst);
         CK(cudaGetLastError());
+        TRY(prof_end(h, 3));
         for (int it = 0; it < h->max_iters_global; ++it) {
             TRY(launch_elements(h));
             TRY(launch_instances(h, INST_MODE_NEWTON, step));
@@ -787,12 +838,17 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             }
         }
         if (rc != STRUT_OK) break;
+        TRY(prof_begin(h));
         commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
             h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status,
             h->d_hist_ef + (size_t)step * std::max(h->n_rece_slots, 1) * 6, h->d_rece_base);
         CK(cudaGetLastError());
+        TRY(prof_end(h, 2));
+        TRY(prof_begin(h));
         post_step_kernel<<<(nF + tb - 1) / tb, tb, 0, h->stream>>>(h->d_insts, h->A, h->d_free_inst, nF);
         CK(cudaGetLastError());
+        TRY(prof_end(h, 4));
+        if (h->prof) h->P.bytes[2] += h->commit_bytes_total;
         if (h->n_rec_total > 0) {
             record_disp_kernel<<<(h->n_rec_total + tb - 1) / tb, tb, 0, h->stream>>>(
                 h->A.u_full, h->d_rec_dof, h->n_rec_total, h->d_hist_disp + (size_t)step * h->n_rec_total);
@@ -804,6 +860,12 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
     CK(cudaStreamSynchronize(h->stream));
     unsigned long long cnt[8];
     CK(cudaMemcpy(cnt, h->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+    if (h->prof) {
+        h->P.bytes[0] += (double)cnt[3];
+        h->P.bytes[1] += (double)cnt[4];
+        h->P.bytes[3] += (double)st.steps_done * 8.0 * 12.0 * h->n_free_total;
+        h->P.bytes[4] += (double)st.steps_done * 8.0 * 8.0 * h->n_free_total;
+    }
     st.local_element_iterations = (int64_t)cnt[0];
     st.section_evaluations = (int64_t)cnt[1];
     {
@@ -908,6 +970,21 @@ int strut_gpu_get_state(StrutHandle* h, int32_t instance, double* u_free, double
     if (a_free) CK(cudaMemcpy(a_free, h->A.a_f + I.f_off, I.n * sizeof(double), cudaMemcpyDeviceToHost));
     return STRUT_OK;
 }
+
+int strut_gpu_set_profiling(StrutHandle* h, int32_t enabled) {
+    if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
+    h->prof = enabled != 0;
+    if (h->prof) std::memset(&h->P, 0, sizeof(h->P));
+    return STRUT_OK;
+}
+
+int strut_gpu_get_profile(const StrutHandle* h, StrutKernelProfile* out) {
+    if (!h || !out) return fail(STRUT_BAD_ARG, "bad arguments");
+    *out = h->P;
+    return STRUT_OK;
+}
+
+void* strut_gpu_stream(const StrutHandle* h) { return h ? (void*)h->stream : nullptr; }
 
 int strut_gpu_band_info(const StrutHandle* h, int32_t instance, int32_t* half_bw, int32_t* row_width) {
     if (!h || instance < 0 || instance >= h->n_inst) return fail(STRUT_BAD_ARG, "bad arguments");
