@@ -55,6 +55,7 @@ int oracle_run_transient(const StrutModelDesc* m, int steps, double* disp_hist,
 int oracle_state_determination(const StrutModelDesc* m, const double* u_free,
                                double* f_int_free, double* band_out, int* half_bw);
 /* Multi-instance run over nthreads host threads (CPU baseline leg). */
+long oracle_dense_fallbacks(void);
 int oracle_run_transient_batch(const StrutModelDesc* models, int n, int steps, int nthreads,
                                int* total_iters);
 

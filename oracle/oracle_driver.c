@@ -25,6 +25,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+static long g_dense_fallbacks = 0;
+long oracle_dense_fallbacks(void) { return g_dense_fallbacks; }
+
 typedef struct OModel {
     const StrutModelDesc* d;
     int n, bw, rw; /* free count, half band width, general row width 2bw+1 */
@@ -335,6 +338,7 @@ static int band_general_factor(OModel* m) {
             }
             rc = dense_lu(m);
             m->dense_mode = 1;
+            __atomic_add_fetch(&g_dense_fallbacks, 1, __ATOMIC_RELAXED);
             break;
         }
         double diag = B[gslot(m, k, k)];

@@ -60,6 +60,7 @@ struct DevInst {
     double a0, a1, a2, a3, dt, gamma, beta, coeff, tol;
     double alpha_m, beta_k, beta_k_init, beta_k_comm;
     double io_bytes;  // algorithmic HBM bytes of one Newton iteration of this instance
+    long long dense_off;  // offset of this instance's n x n fallback scratch
 };
 
 struct FiberState {

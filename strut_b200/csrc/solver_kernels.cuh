@@ -45,6 +45,9 @@ struct InstArrays {
     double* export_f;     // F_int at free dofs
     const double* rhs_in; // INST_MODE_SOLVE_EXPORTED
     unsigned long long* bytes_counter;
+    double* dense;        // per instance n x n scratch for the partial-pivot fallback
+    int* piv;             // per free dof
+    int* fallbacks;       // per instance count of dense fallbacks
 };
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -199,11 +202,126 @@ __device__ __forceinline__ double gather_slot(const InstArrays& A, long long sp0
     return K;
 }
 
+// Effective-matrix entry of band slot (i, j) exactly as the row assembly computes it
+// (load K, add a1 C, add a0 M).
+__device__ __forceinline__ double keff_slot(const DevInst& I, const InstArrays& A, long long sp0,
+                                            const double* Kinit, int i, int j, int slot) {
+    const double K = gather_slot(A, sp0, slot);
+    double C = 0.0;
+    if (I.has_damping) {
+        C = I.alpha_m * (i == j ? A.Mrff[I.f_off + i] : 0.0);
+        if (I.beta_k != 0.0) C += I.beta_k * K;
+        if (I.beta_k_init != 0.0) C += I.beta_k_init * Kinit[slot];
+    }
+    double keff = K;
+    if (I.has_damping && I.a1 != 0.0) keff += I.a1 * C;
+    if (i == j) keff += I.a0 * A.Mff[I.f_off + i];
+    return keff;
+}
+
+// Block argmax of |column| with the reference's tie rule (first row wins).
+__device__ __forceinline__ void block_argmax(double& v, int& r, double* red_v, int* red_r) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int orr = __shfl_xor_sync(0xffffffffu, r, o);
+        if (ov > v || (ov == v && orr < r)) {
+            v = ov;
+            r = orr;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+        red_v[warp] = v;
+        red_r[warp] = r;
+    }
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    v = red_v[0];
+    r = red_r[0];
+    for (int w = 1; w < nw; ++w) {
+        if (red_v[w] > v || (red_v[w] == v && red_r[w] < r)) {
+            v = red_v[w];
+            r = red_r[w];
+        }
+    }
+}
+
+// Dense LU with partial pivoting on an n x n row-major matrix in global memory
+// (_try_factorize_dense_unsymmetric_loaded, linear_solver_backend.mojo:175-215).  fac is an
+// n-entry shared scratch.  Returns 0 ok, 2 singular.
+__device__ int dense_lu_global(double* D, int* piv, int n, double* fac, double* red_v, int* red_r) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < n; i += nt) piv[i] = i;
+    __syncthreads();
+    for (int col = 0; col < n; ++col) {
+        double v = -1.0;
+        int r = n;
+        for (int row = col + tid; row < n; row += nt) {
+            const double c = fabs(D[(size_t)row * n + col]);
+            if (c > v) {
+                v = c;
+                r = row;
+            }
+        }
+        block_argmax(v, r, red_v, red_r);
+        if (v <= 1.0e-14) return 2;
+        if (r != col) {
+            for (int j = tid; j < n; j += nt) {
+                const double t = D[(size_t)col * n + j];
+                D[(size_t)col * n + j] = D[(size_t)r * n + j];
+                D[(size_t)r * n + j] = t;
+            }
+            if (tid == 0) {
+                const int t = piv[col];
+                piv[col] = piv[r];
+                piv[r] = t;
+            }
+        }
+        __syncthreads();
+        const double diag = D[(size_t)col * n + col];
+        if (fabs(diag) <= 1.0e-14) return 2;
+        for (int row = col + 1 + tid; row < n; row += nt) fac[row] = D[(size_t)row * n + col] / diag;
+        __syncthreads();
+        const int m = n - col - 1;
+        for (long long t = tid; t < (long long)m * m; t += nt) {
+            const int row = col + 1 + (int)(t / m);
+            const int j = col + 1 + (int)(t % m);
+            const double f = fac[row];
+            if (f != 0.0) D[(size_t)row * n + j] -= f * D[(size_t)col * n + j];
+        }
+        for (int row = col + 1 + tid; row < n; row += nt) D[(size_t)row * n + col] = fac[row];
+        __syncthreads();
+    }
+    return 0;
+}
+
+// _solve_dense_unsymmetric (linear_solver_backend.mojo:218-240) with one warp.
+__device__ void dense_solve_warp(const double* D, const int* piv, int n, const double* rhs,
+                                 double* w, double* x) {
+    const int lane = threadIdx.x & 31;
+    for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int j = lane; j < i; j += 32) s += D[(size_t)i * n + j] * w[j];
+        s = warp_sum(s);
+        if (lane == 0) w[i] = rhs[piv[i]] - s;
+        __syncwarp();
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = 0.0;
+        for (int j = i + 1 + lane; j < n; j += 32) s += D[(size_t)i * n + j] * x[j];
+        s = warp_sum(s);
+        if (lane == 0) x[i] = (w[i] - s) / D[(size_t)i * n + i];
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __restrict__ insts,
                                                               InstArrays A, int mode, int step) {
     extern __shared__ __align__(16) double smem_inst[];
     __shared__ DevInst I;
     __shared__ double red[32];
+    __shared__ int red_r[32];
     __shared__ int ctrl;
     const int inst = blockIdx.x;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -220,6 +338,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     double* R = vt + n;
     double* w = R + n;
     double* du = w + n;
+    double* fac = du + n;
     const int f0 = I.f_off;
     int rc = 0;
     if (mode == INST_MODE_SOLVE_EXPORTED) {
@@ -323,6 +442,33 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
         rc = band_chol_smem(Kb, n, bw, rw);
     else
         rc = band_lu_smem(Kb, n, bw, rw, nullptr);
+    bool dense = false;
+    double* D = A.dense + I.dense_off;
+    int* piv = A.piv + f0;
+    if (rc == 6) {
+        // BandGeneral: a row swap would be needed, so the whole effective matrix is factored
+        // densely with partial pivoting (linear_solver_backend.mojo:650-657, 612-629), starting
+        // again from the assembled values.
+        __syncthreads();
+        for (long long t = tid; t < (long long)n * n; t += nt) D[t] = 0.0;
+        __syncthreads();
+        if (mode == INST_MODE_SOLVE_EXPORTED) {
+            for (int t = tid; t < n * rw; t += nt) {
+                const int i = t / rw, j = i + t % rw - bw;
+                if (j >= 0 && j < n) D[(size_t)i * n + j] = A.export_band[I.band_off + t];
+            }
+        } else {
+            const double* Kinit = A.Kinit + I.band_off;
+            for (int t = tid; t < n * rw; t += nt) {
+                const int i = t / rw, j = i + t % rw - bw;
+                if (j >= 0 && j < n) D[(size_t)i * n + j] = keff_slot(I, A, I.slot_ptr_off, Kinit, i, j, t);
+            }
+        }
+        __syncthreads();
+        rc = dense_lu_global(D, piv, n, fac, red, red_r);
+        dense = true;
+        if (tid == 0 && A.fallbacks) A.fallbacks[inst] += 1;
+    }
     if (rc != 0) {
         if (tid == 0) {
             A.status[inst] = rc;
@@ -336,7 +482,9 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     // multipliers of the last column were written in the loop except column n-1 (none below)
     __syncthreads();
     if (tid < 32) {
-        if (I.spd)
+        if (dense)
+            dense_solve_warp(D, piv, n, R, w, du);
+        else if (I.spd)
             band_solve_chol_warp(Kb, n, bw, rw, R, w, du);
         else
             band_solve_lu_warp(Kb, n, bw, rw, R, w, du);

@@ -264,6 +264,7 @@ struct StrutHandle {
     double* d_rhs = nullptr;
     std::vector<long long> elem_fibers;  // fibers per element (all families)
     double commit_bytes_total = 0.0;
+    long long dense_total = 0;
     ~StrutHandle() {
         for (void* p : allocs) cudaFree(p);
         if (d_hist_disp) cudaFree(d_hist_disp);
@@ -374,6 +375,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     std::vector<int> sec_base(num_instances);
     int u_off = 0, f_off = 0;
     long long band_off = 0;
+    long long dense_off = 0;
     h->insts.resize(num_instances);
     h->exc.resize(num_instances);
     h->rec_off.resize(num_instances);
@@ -552,6 +554,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         I.f_off = f_off;
         I.band_off = band_off;
         I.slot_ptr_off = band_off;
+        I.dense_off = dense_off;
+        dense_off += (long long)nf * nf;
         I.fint_ptr_off = f_off;
         I.max_iters = d.max_iters;
         I.test_type = d.test_type;
@@ -594,7 +598,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         }
         h->n_rec_total += d.num_record_dofs;
         h->n_rece_slots += nslots;
-        const size_t ismem = ((size_t)nf * rw + 5 * (size_t)nf) * sizeof(double);
+        const size_t ismem = ((size_t)nf * rw + 6 * (size_t)nf) * sizeof(double);
         if (ismem > 220 * 1024)
             return bail(fail(STRUT_UNSUPPORTED, "instance band does not fit in shared memory (n x (2bw+1) too large)"));
         h->inst_smem = std::max(h->inst_smem, ismem);
@@ -622,6 +626,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     h->n_dofs_total = u_off;
     h->n_elem = (int)elems.size();
     h->band_total = band_off;
+    h->dense_total = dense_off;
     if (h->elem_smem > 200 * 1024) return bail(fail(STRUT_UNSUPPORTED, "element fiber history exceeds shared memory"));
     h->elem_smem = std::max<size_t>(h->elem_smem, 16);
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -701,7 +706,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         (rc = dzeros(&A.export_band, (size_t)h->band_total, al)) ||
         (rc = dzeros(&A.export_f, nF, al)) || (rc = dzeros(&h->d_rhs, nF, al)) ||
         (rc = dzeros(&h->d_elem_err, (size_t)h->n_elem, al)) ||
-        (rc = dzeros(&h->d_counters, 8, al)))
+        (rc = dzeros(&h->d_counters, 8, al)) || (rc = dzeros(&A.dense, (size_t)h->dense_total, al)) ||
+        (rc = dzeros(&A.piv, nF, al)) || (rc = dzeros(&A.fallbacks, (size_t)h->n_inst, al)))
         return bail(rc);
     double* d_Mff;
     double* d_Mrff;
@@ -888,7 +894,6 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
         CK(cudaMemcpy(ee.data(), h->d_elem_err, sizeof(int) * h->n_elem, cudaMemcpyDeviceToHost));
         g_last_error = "instance " + std::to_string(st.failed_instance) + " failed at step " +
                        std::to_string(st.failed_step) + " with status " + std::to_string(rc);
-        if (rc == 6) g_last_error += " (BandGeneral needs the dense partial-pivot fallback)";
     }
     if (stats) *stats = st;
     return rc;
