@@ -220,7 +220,7 @@ def main():
 
     if args.profile_only:
         with runtime.Analysis(models, device=device) as an:
-            an.run(min(50, args.record_steps))
+            an.run(min(50, args.record_steps), check=False)
         return 0
 
     def one_analysis(prof=False):
@@ -231,10 +231,14 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st = an.run(args.record_steps)
+        st = an.run(args.record_steps, check=False)
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
+        status = an.instance_status()
+        if st.status not in (A.STRUT_OK, A.STRUT_NONCONVERGED):
+            raise RuntimeError(f"analysis failed: status {st.status}")
+        st.completed = int((status == 0).sum())
         prof_out = None
         if prof:
             P = A.StrutKernelProfile()
@@ -263,9 +267,16 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         tot_ms = float(t.item())
     ms_per_step = tot_ms / args.steps
-    records = args.frames * world
-    value = records / (ms_per_step / 1000.0) * 3600.0
     st = stats[-1]
+    # records that ran all steps (a record whose Newton iteration fails is masked out of the
+    # batch at its failing step, as Strut would abort it; it is not counted)
+    completed = st.completed
+    if world > 1:
+        t = torch.tensor([completed], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t)
+        completed = int(t.item())
+    records = completed
+    value = records / (ms_per_step / 1000.0) * 3600.0
     newton_per_step = st.global_newton_iterations / float(args.frames * args.record_steps)
     fiber_updates_per_s = st.fiber_updates / (times[-1] / 1000.0)
 
@@ -276,7 +287,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         with runtime.Analysis(models, device=device) as an:
-            an.run(args.record_steps)
+            an.run(args.record_steps, check=False)
             disp, ef, it = an.history_all()
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
@@ -334,6 +345,8 @@ def main():
                        "fibers_per_gpu": n_fibers, "parallelism": f"replicas{world}",
                        "l2": "fiber history of the batch exceeds L2 (no flush needed)"},
             "newton_its_per_step": newton_per_step,
+            "records_completed": completed,
+            "records_failed_nonconvergence": args.frames * world - completed,
             "fiber_state_updates_per_s": fiber_updates_per_s,
             "simulated_s_per_wall_s": args.frames * args.record_steps * DT / (times[-1] / 1000.0),
             "e2e": {"value": e2e_value, "unit": "records/hour", "h2d_bytes_per_step": int(h2d),

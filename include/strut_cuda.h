@@ -216,7 +216,9 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
 int strut_gpu_destroy(StrutHandle* h);
 int strut_gpu_num_instances(const StrutHandle* h);
 /* Runs n_steps Newmark steps for every instance (predictor, Newton to the test tolerance,
- * commit, Newmark update).  Stops at the first step where an instance fails. */
+ * commit, Newmark update).  An instance that fails (non-convergence, singular matrix, ...) is
+ * masked out of the remaining steps while the others carry on; the first failure (instance,
+ * step, status) is returned.  A single-instance handle stops at its failing step. */
 int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats);
 /* Copies recorder histories of one instance for steps [0, steps_done):
  * disp: steps x num_record_dofs, eforce: steps x num_record_elements x 6,
@@ -226,6 +228,8 @@ int strut_gpu_get_history(StrutHandle* h, int32_t instance, double* disp, double
 /* Same for all instances at once, instance-major, each block sized as for one instance
  * with that instance's recorder counts; offsets are the prefix sums of those sizes. */
 int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int32_t* iters);
+/* Status of every instance (STRUT_OK or the code it failed with), n_inst entries. */
+int strut_gpu_instance_status(const StrutHandle* h, int32_t* status);
 /* Current free displacement / velocity / acceleration vectors of one instance. */
 int strut_gpu_get_state(StrutHandle* h, int32_t instance, double* u_free, double* v_free,
                         double* a_free);

@@ -193,6 +193,7 @@ EXPORTS = {
     "strut_gpu_get_history": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, _ip]),
     "strut_gpu_get_history_all": (C.c_int, [C.c_void_p, _dp, _dp, _ip]),
     "strut_gpu_get_state": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, _dp]),
+    "strut_gpu_instance_status": (C.c_int, [C.c_void_p, _ip]),
     "strut_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "strut_gpu_get_profile": (C.c_int, [C.c_void_p, C.POINTER(StrutKernelProfile)]),
     "strut_gpu_stream": (C.c_void_p, [C.c_void_p]),

@@ -81,10 +81,12 @@ struct ElemScratch {
     double sub_e[kMaxIp], sub_k[kMaxIp], ssr_n[kMaxIp], ssr_m[kMaxIp];
     double fs00[kMaxIp], fs01[kMaxIp], fs11[kMaxIp];
     double best[10];
+    double c_n[kMaxIp], c_m[kMaxIp], c_f00[kMaxIp], c_f01[kMaxIp], c_f11[kMaxIp];
     double ul[6];
     double k[36];
     double f[6];
     int best_ok;
+    int c_valid;
     int flag;
     int loop_ctrl;
     int local_iters;
@@ -284,9 +286,22 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
         }
     }
     __syncthreads();
-    eval_points(g, sd, sv, E, S);
+    const bool cached = S.c_valid != 0;
+    if (!cached) eval_points(g, sd, sv, E, S);
     if (tid == 0) {
-        int ok = flex_of_resp(S, nip, S.fs00, S.fs01, S.fs11) ? 1 : 0;
+        int ok;
+        if (cached) {
+            for (int ip = 0; ip < nip; ++ip) {
+                S.resp[ip][0] = S.c_n[ip];
+                S.resp[ip][1] = S.c_m[ip];
+                S.fs00[ip] = S.c_f00[ip];
+                S.fs01[ip] = S.c_f01[ip];
+                S.fs11[ip] = S.c_f11[ip];
+            }
+            ok = 1;
+        } else {
+            ok = flex_of_resp(S, nip, S.fs00, S.fs01, S.fs11) ? 1 : 0;
+        }
         if (ok) {
             double P[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             for (int ip = 0; ip < nip; ++ip) {
@@ -374,7 +389,13 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
                         for (int ip = 0; ip < nip; ++ip) {
                             S.vs_e[ip] = S.sub_e[ip];
                             S.vs_k[ip] = S.sub_k[ip];
+                            S.c_n[ip] = S.ssr_n[ip];
+                            S.c_m[ip] = S.ssr_m[ip];
+                            S.c_f00[ip] = S.fs00[ip];
+                            S.c_f01[ip] = S.fs01[ip];
+                            S.c_f11[ip] = S.fs11[ip];
                         }
+                        S.c_valid = 1;
                         S.best[0] = S.q[0];
                         S.best[1] = S.q[1];
                         S.best[2] = S.q[2];
@@ -545,10 +566,17 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
             S.acc_v[i] = estate[(size_t)e * kEStride + kEv + i];
             S.zero3[i] = 0.0;
         }
+        const double* es = estate + (size_t)e * kEStride;
         for (int ip = 0; ip < E.nip; ++ip) {
-            S.vs_e[ip] = estate[(size_t)e * kEStride + kEe + ip];
-            S.vs_k[ip] = estate[(size_t)e * kEStride + kEk + ip];
+            S.vs_e[ip] = es[kEe + ip];
+            S.vs_k[ip] = es[kEk + ip];
+            S.c_n[ip] = es[kEcN + ip];
+            S.c_m[ip] = es[kEcM + ip];
+            S.c_f00[ip] = es[kEc00 + ip];
+            S.c_f01[ip] = es[kEc01 + ip];
+            S.c_f11[ip] = es[kEc11 + ip];
         }
+        S.c_valid = E.type == 2 && es[kEcv] != 0.0;
         double ug[6];
         for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
         if (E.type == 2)
@@ -710,6 +738,7 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
                     for (int i = 0; i < 6; ++i) S.best[3 + i] = k[i];
                     S.best[9] = k[8];
                     S.best_ok = 1;
+                    S.c_valid = 0;
                     ok = 1;
                 }
             }
@@ -819,10 +848,17 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
             estate[(size_t)e * kEStride + kEq + i] = S.q[i];
             estate[(size_t)e * kEStride + kEv + i] = S.acc_v[i];
         }
+        double* es = estate + (size_t)e * kEStride;
         for (int ip = 0; ip < nip; ++ip) {
-            estate[(size_t)e * kEStride + kEe + ip] = S.vs_e[ip];
-            estate[(size_t)e * kEStride + kEk + ip] = S.vs_k[ip];
+            es[kEe + ip] = S.vs_e[ip];
+            es[kEk + ip] = S.vs_k[ip];
+            es[kEcN + ip] = S.c_n[ip];
+            es[kEcM + ip] = S.c_m[ip];
+            es[kEc00 + ip] = S.c_f00[ip];
+            es[kEc01 + ip] = S.c_f01[ip];
+            es[kEc11 + ip] = S.c_f11[ip];
         }
+        es[kEcv] = S.c_valid ? 1.0 : 0.0;
     }
     __syncthreads();
     if (S.flag) {
@@ -943,6 +979,10 @@ __global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
     if (tid == 0) {
         double ug[6];
         for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
+        // After commit the stored deformations evaluated from the new committed state give the
+        // same Concrete02 / Steel02 / Elastic responses bit for bit (zero strain increment);
+        // Steel01's return map may move by rounding, so its sections drop the cache.
+        if (sd.n_s1 > 0) estate[(size_t)e * kEStride + kEcv] = 0.0;
         if (E.type == 2) {
             u_to_local(E.c_sync, E.s_sync, ug, ul);
             const double chord = (ul[4] - ul[1]) / E.L_sync;

@@ -7,9 +7,10 @@
 //                    one block per family: [ip0 fibers | ip1 fibers | ...] padded to 4 entries,
 //                    so every field block is a 32-byte aligned contiguous run that one
 //                    cp.async.bulk moves into shared memory.
-//   element state    32 doubles per element: q0..q2 | eps0[10] | kappa[10] | v0..v2
-//                    (the forceBeamColumn "force_basic_q" block of loader.mojo:1757-1771; for
-//                    dispBeamColumn the section deformations of the last state determination)
+//   element state    80 doubles per element: q0..q2 | eps0[10] | kappa[10] | v0..v2 (the
+//                    forceBeamColumn "force_basic_q" block of loader.mojo:1757-1771; for
+//                    dispBeamColumn the section deformations of the last state determination),
+//                    then the cached section responses at those deformations
 //   element output   k (6x6 global) and f (6) per element
 //   instance arrays  free-dof vectors, band Kinit, gather lists for band slots and F_int
 //
@@ -25,8 +26,13 @@
 namespace strut {
 
 constexpr int kMaxIp = 10;
-constexpr int kEStride = 32;  // doubles of element state
+constexpr int kEStride = 80;  // doubles of element state
 constexpr int kEq = 0, kEe = 3, kEk = 13, kEv = 23;
+// Section responses at the stored deformations (N, Mz and the 2x2 flexibility), valid flag.
+// A forceBeamColumn state determination starts by re-evaluating every section at the stored
+// deformations (force_beam_column2d.mojo:877-925); when nothing changed since the evaluation
+// that produced them, those responses are these, bit for bit.
+constexpr int kEcv = 26, kEcN = 27, kEcM = 37, kEc00 = 47, kEc01 = 57, kEc11 = 67;
 
 struct DevSection {
     int n_s2, n_c2, n_s1, n_el;

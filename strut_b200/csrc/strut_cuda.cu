@@ -833,17 +833,21 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             CK(cudaStreamSynchronize(h->stream));
             if (h->h_ctrl[0] <= 0) break;
         }
-        std::vector<int> status(h->n_inst);
-        CK(cudaMemcpy(status.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < h->n_inst; ++i) {
-            if (status[i] != 0) {
-                st.failed_instance = i;
-                st.failed_step = step;
-                rc = status[i];
-                break;
+        // A failed instance keeps its status and is masked out of every later step; the other
+        // instances of the batch carry on.  The first failure is reported.
+        if (rc == STRUT_OK) {
+            std::vector<int> status(h->n_inst);
+            CK(cudaMemcpy(status.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < h->n_inst; ++i) {
+                if (status[i] != 0) {
+                    st.failed_instance = i;
+                    st.failed_step = step;
+                    rc = status[i];
+                    break;
+                }
             }
+            if (rc != STRUT_OK && h->n_inst == 1) break;
         }
-        if (rc != STRUT_OK) break;
         TRY(prof_begin(h));
         commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
             h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status,
@@ -962,6 +966,13 @@ int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int3
         for (int i = 0; i < h->n_inst; ++i)
             for (int s = 0; s < S; ++s) iters[o++] = all[(size_t)s * h->n_inst + i];
     }
+    return STRUT_OK;
+}
+
+int strut_gpu_instance_status(const StrutHandle* h, int32_t* status) {
+    if (!h || !status) return fail(STRUT_BAD_ARG, "bad arguments");
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(status, h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
     return STRUT_OK;
 }
 

@@ -119,6 +119,11 @@ class Analysis:
         )
         return disp, ef, it
 
+    def instance_status(self):
+        st = np.zeros(len(self.models), dtype=np.int32)
+        _check(lib().strut_gpu_instance_status(self.h, st.ctypes.data_as(_ip)), "strut_gpu_instance_status")
+        return st
+
     def state(self, instance: int = 0):
         n = self.models[instance].num_free
         u, v, a = np.zeros(n), np.zeros(n), np.zeros(n)

@@ -228,3 +228,20 @@ def test_transient_frame_with_pivoting_fallback(gpu_lib, oracle):
     case = W.rc_frame_case(stories=p["stories"], bays=p["bays"], wg=p["wg"], pga_g=p["pga_g"],
                            seed=p["seed"], steps=120)
     _transient_parity(gpu_lib, oracle, [case], 120)
+
+
+def test_failed_instance_is_masked_and_others_continue(gpu_lib):
+    """One record of a batch that cannot converge (tol 1e-30) is masked out at its failing
+    step; the other record runs every step and matches its solo run bit for bit."""
+    ok = W.rc_frame_case(stories=2, bays=2, steps=60, seed=31)
+    bad = W.rc_frame_case(stories=2, bays=1, steps=60, seed=32, tol=1e-30, max_iters=3)
+    with gpu_lib.Analysis([M.Model(bad), M.Model(ok)]) as an:
+        st = an.run(60, check=False)
+        assert an.last_status == A.STRUT_NONCONVERGED
+        assert st.failed_instance == 0 and st.failed_step == 0 and st.steps_done == 60
+        assert list(an.instance_status()) == [A.STRUT_NONCONVERGED, A.STRUT_OK]
+        d_batch, e_batch, i_batch = an.history(1)
+    with gpu_lib.Analysis([M.Model(ok)]) as solo:
+        solo.run(60)
+        d_solo, e_solo, i_solo = solo.history(0)
+    assert np.array_equal(d_batch, d_solo) and np.array_equal(i_batch, i_solo)
