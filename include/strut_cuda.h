@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define STRUT_ABI_VERSION 1
+#define STRUT_ABI_VERSION 2
 #define STRUT_MAX_INT_PTS 10
 
 /* Status codes.  No entry point aborts the process. */
@@ -65,7 +65,8 @@ enum { STRUT_MAT_ELASTIC = 0, STRUT_MAT_STEEL01 = 1, STRUT_MAT_CONCRETE01 = 2,
        STRUT_MAT_STEEL02 = 3, STRUT_MAT_CONCRETE02 = 4 };
 
 /* ElementTypeTag (tag_types.mojo:1-14). */
-enum { STRUT_ELEM_FORCE_BEAM_COLUMN_2D = 2, STRUT_ELEM_DISP_BEAM_COLUMN_2D = 3 };
+enum { STRUT_ELEM_FORCE_BEAM_COLUMN_2D = 2, STRUT_ELEM_DISP_BEAM_COLUMN_2D = 3,
+       STRUT_ELEM_FORCE_BEAM_COLUMN_3D = 11, STRUT_ELEM_DISP_BEAM_COLUMN_3D = 12 };
 
 /* geomTransf. */
 enum { STRUT_GEOM_LINEAR = 0, STRUT_GEOM_PDELTA = 1 };
@@ -99,11 +100,17 @@ typedef struct StrutFiber {
     int32_t reserved;
 } StrutFiber;
 
-/* A FiberSection2d: a contiguous run of fibers[] (append_fiber_section2d_from_input,
- * fiber2d.mojo:3881-3944). */
+/* A FiberSection2d / FiberSection3d: a contiguous run of fibers[]
+ * (append_fiber_section2d_from_input, fiber2d.mojo:3881-3944; append_fiber_section3d_from_input,
+ * fiber3d.mojo:654-720).  G and J (FiberSection3d params) give the torsional stiffness GJ/L of
+ * 3D beam-columns. */
 typedef struct StrutFiberSection {
     int32_t fiber_offset;
     int32_t fiber_count;
+    int32_t dim;           /* 2 or 3                                            */
+    int32_t reserved;
+    double G;
+    double J;
 } StrutFiberSection;
 
 /* Beam integration rule, already mapped to xi in [0,1] and weights x0.5
@@ -115,7 +122,8 @@ typedef struct StrutBeamIntegration {
     double w[STRUT_MAX_INT_PTS];
 } StrutBeamIntegration;
 
-/* A 2D frame element (forceBeamColumn2d / dispBeamColumn2d). */
+/* A frame element: forceBeamColumn2d / dispBeamColumn2d (6 dofs) or forceBeamColumn3d /
+ * dispBeamColumn3d (12 dofs, local axes from vecxz as in elements/utils.mojo:96-140). */
 typedef struct StrutFrameElement {
     int32_t type;          /* STRUT_ELEM_*                                      */
     int32_t node_i;        /* node indices, 0-based                             */
@@ -123,7 +131,10 @@ typedef struct StrutFrameElement {
     int32_t section;       /* index into sections[]                             */
     int32_t geom;          /* STRUT_GEOM_*                                      */
     int32_t integration;   /* index into integrations[]                         */
-    int32_t dof[6];        /* global dof indices node*ndf + (d-1)               */
+    int32_t dof[12];       /* global dof indices node*ndf + (d-1)               */
+    double vecxz[3];       /* 3D only                                           */
+    int32_t has_vecxz;
+    int32_t reserved;
 } StrutFrameElement;
 
 /* A uniform excitation (pattern UniformExcitation + Path time series with dt,
@@ -142,11 +153,11 @@ typedef struct StrutExcitation {
 
 /* One analysis instance (one frame + one record). */
 typedef struct StrutModelDesc {
-    int32_t ndm;                 /* must be 2                                            */
-    int32_t ndf;                 /* must be 3                                            */
+    int32_t ndm;                 /* 2 (ndf 3) or 3 (ndf 6)                               */
+    int32_t ndf;
     int32_t num_nodes;
     int32_t num_dofs;            /* num_nodes * ndf                                      */
-    const double* node_coords;   /* num_nodes * 2 : x, y                                 */
+    const double* node_coords;   /* num_nodes * ndm : x, y (, z)                         */
     int32_t num_materials;
     int32_t num_fibers;
     const StrutUniMaterial* materials;
@@ -281,7 +292,11 @@ int strut_gpu_section_batch_destroy(StrutSectionBatch* b);
 int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_dev,
                                  double* resp_dev, int32_t commit, void* stream);
 /* Copies the committed fiber state of one instance to the host in the section's family
- * order (Steel02 then Concrete02 then the others, 16 doubles per fiber, see DESIGN). */
+ * order (Steel02 fibers, then Concrete02, then Steel01), 16 doubles per fiber, unused slots 0:
+ *   Steel02:    eps sig tan epsmin epsmax epspl epss0 sigs0 epsr sigr, slot 15 = kon
+ *   Concrete02: eps sig tan ecmin dept
+ *   Steel01:    eps sig tan epsp alpha
+ * Pass out = NULL to query *n_fibers only. */
 int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double* out,
                                   int32_t* n_fibers);
 

@@ -39,6 +39,8 @@ MAT_CONCRETE02 = 4
 # ElementTypeTag (tag_types.mojo:1-14)
 ELEM_FORCE_BEAM_COLUMN_2D = 2
 ELEM_DISP_BEAM_COLUMN_2D = 3
+ELEM_FORCE_BEAM_COLUMN_3D = 11
+ELEM_DISP_BEAM_COLUMN_3D = 12
 
 GEOM_LINEAR = 0
 GEOM_PDELTA = 1
@@ -70,7 +72,14 @@ class StrutFiber(C.Structure):
 
 
 class StrutFiberSection(C.Structure):
-    _fields_ = [("fiber_offset", C.c_int32), ("fiber_count", C.c_int32)]
+    _fields_ = [
+        ("fiber_offset", C.c_int32),
+        ("fiber_count", C.c_int32),
+        ("dim", C.c_int32),
+        ("reserved", C.c_int32),
+        ("G", C.c_double),
+        ("J", C.c_double),
+    ]
 
 
 class StrutBeamIntegration(C.Structure):
@@ -90,7 +99,10 @@ class StrutFrameElement(C.Structure):
         ("section", C.c_int32),
         ("geom", C.c_int32),
         ("integration", C.c_int32),
-        ("dof", C.c_int32 * 6),
+        ("dof", C.c_int32 * 12),
+        ("vecxz", C.c_double * 3),
+        ("has_vecxz", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -921,14 +921,15 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
 // displacements from the new committed state for dispBeamColumn2d).
 __global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
-    double* __restrict__ estate, const int* __restrict__ status, double* __restrict__ rec_out,
-    const int* __restrict__ rece_base) {
+    double* __restrict__ estate, const int* __restrict__ status, double* __restrict__ rec_base,
+    const int* __restrict__ rece_base, int rec_slots, const DevCtl* __restrict__ ctl) {
     __shared__ DevElem E;
     __shared__ DevSection sd;
     __shared__ double resp[kMaxIp][5];
     __shared__ double ul[6];
     const int e = blockIdx.x;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double* rec_out = rec_base ? rec_base + (size_t)ctl->step * rec_slots * 6 : nullptr;
     copy_struct(&E, elems + e);
     __syncthreads();
     if (status[E.inst] != 0) return;

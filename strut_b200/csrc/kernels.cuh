@@ -69,6 +69,17 @@ struct DevInst {
     long long dense_off;  // offset of this instance's n x n fallback scratch
 };
 
+// Step / iteration control on the device (read by the kernels, advanced by step_end_kernel).
+struct DevCtl {
+    int step;       // absolute index of the step being computed
+    int step0;      // first step of the current run (ground-motion table row 0)
+    int n_end;      // run stops before this step
+    int iter;       // Newton iteration of the current step
+    int max_iters;  // max over instances
+    int single;     // single-instance handle: stop at the failing step
+    int pad0, pad1;
+};
+
 struct FiberState {
     // family arrays: field f of family X lives at X + f * X_n
     double* c2;

@@ -40,7 +40,8 @@ struct InstArrays {
     int* status;
     int* iters;
     int* nactive;
-    int* hist_iters;  // this step's row (n_inst entries) or null
+    int* hist_iters;  // iteration-count history (steps x n_inst) or null
+    const DevCtl* ctl;
     double* export_band;  // band per instance (BandGeneral rw / BandSPD bw+1 layout)
     double* export_f;     // F_int at free dofs
     const double* rhs_in; // INST_MODE_SOLVE_EXPORTED
@@ -332,6 +333,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     }
     __syncthreads();
     if (mode == INST_MODE_NEWTON && !A.active[inst]) return;
+    int* hrow = (A.hist_iters && A.ctl) ? A.hist_iters + (size_t)A.ctl->step * gridDim.x : nullptr;
     const int n = I.n, bw = I.bw, rw = I.rw;
     double* Kb = smem_inst;        // n * rw
     double* vt = Kb + (size_t)n * rw;
@@ -432,7 +434,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
                 if (tid == 0) {
                     A.active[inst] = 0;
                     atomicSub(A.nactive, 1);
-                    if (A.hist_iters) A.hist_iters[inst] = A.iters[inst];
+                    if (hrow) hrow[inst] = A.iters[inst];
                 }
                 return;
             }
@@ -521,12 +523,12 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
         if (conv) {
             A.active[inst] = 0;
             atomicSub(A.nactive, 1);
-            if (A.hist_iters) A.hist_iters[inst] = A.iters[inst];
+            if (hrow) hrow[inst] = A.iters[inst];
         } else if (A.iters[inst] >= I.max_iters) {
             A.status[inst] = 1;
             A.active[inst] = 0;
             atomicSub(A.nactive, 1);
-            if (A.hist_iters) A.hist_iters[inst] = A.iters[inst];
+            if (hrow) hrow[inst] = A.iters[inst];
         }
     }
 }
@@ -536,9 +538,15 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
 // activation for the Newton loop.
 __global__ void predictor_kernel(const DevInst* __restrict__ insts, InstArrays A,
                                  const int* __restrict__ free_inst,
-                                 const int* __restrict__ free_dir, const double* __restrict__ ag,
-                                 int n_free_total, int n_inst) {
+                                 const int* __restrict__ free_dir, const double* __restrict__ ag_base,
+                                 int n_free_total, int n_inst, DevCtl* ctl,
+                                 cudaGraphConditionalHandle inner, int use_cond) {
     const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    const double* ag = ag_base + (size_t)(ctl->step - ctl->step0) * 4 * n_inst;
+    if (gi == 0) {
+        ctl->iter = 0;
+        if (use_cond) cudaGraphSetConditional(inner, 1);
+    }
     if (gi < n_inst) {
         const bool ok = A.status[gi] == 0;
         A.active[gi] = ok ? 1 : 0;
@@ -587,9 +595,36 @@ __global__ void post_step_kernel(const DevInst* __restrict__ insts, InstArrays A
 
 __global__ void record_disp_kernel(const double* __restrict__ u_full,
                                    const int* __restrict__ rec_dof, int n_rec_total,
-                                   double* __restrict__ out) {
+                                   double* __restrict__ out_base, const DevCtl* __restrict__ ctl) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n_rec_total) out[t] = u_full[rec_dof[t]];
+    if (t < n_rec_total) out_base[(size_t)ctl->step * n_rec_total + t] = u_full[rec_dof[t]];
+}
+
+// End of a Newton iteration: continue while some instance is still iterating.
+__global__ void newton_check_kernel(DevCtl* ctl, const int* __restrict__ nactive,
+                                    cudaGraphConditionalHandle inner, int use_cond) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    ctl->iter += 1;
+    const int more = (*nactive > 0 && ctl->iter < ctl->max_iters) ? 1 : 0;
+    if (use_cond) cudaGraphSetConditional(inner, more);
+}
+
+// End of a step: note the step at which each instance failed, advance the step counter, reset
+// the active count, and continue while steps remain (a single-instance handle stops at its
+// failing step).
+__global__ void step_end_kernel(DevCtl* ctl, const int* __restrict__ status,
+                                int* __restrict__ fail_step, int n_inst, int* nactive,
+                                cudaGraphConditionalHandle outer, int use_cond) {
+    const int step = ctl->step;
+    for (int i = threadIdx.x; i < n_inst; i += blockDim.x)
+        if (status[i] != 0 && fail_step[i] < 0) fail_step[i] = step;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->step = step + 1;
+        *nactive = 0;
+        const bool stop = ctl->single && status[0] != 0;
+        if (use_cond) cudaGraphSetConditional(outer, (step + 1 < ctl->n_end && !stop) ? 1 : 0);
+    }
 }
 
 __global__ void scatter_free_kernel(const double* __restrict__ u_f, const int* __restrict__ free_dof,

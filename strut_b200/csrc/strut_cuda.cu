@@ -18,6 +18,8 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "strut_cuda.h"
@@ -261,6 +263,11 @@ struct StrutHandle {
     bool prof = false;
     StrutKernelProfile P;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevCtl* d_ctl = nullptr;
+    int* d_fail_step = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const void* graph_keys[4] = {nullptr, nullptr, nullptr, nullptr};
     double* d_rhs = nullptr;
     std::vector<long long> elem_fibers;  // fibers per element (all families)
     double commit_bytes_total = 0.0;
@@ -272,6 +279,8 @@ struct StrutHandle {
         if (d_hist_iters) cudaFree(d_hist_iters);
         if (d_ag) cudaFree(d_ag);
         if (h_ctrl) cudaFreeHost(h_ctrl);
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -306,8 +315,7 @@ static int launch_elements(StrutHandle* h) {
 
 static int launch_instances(StrutHandle* h, int mode, int step) {
     InstArrays A = h->A;
-    A.hist_iters = (mode == INST_MODE_NEWTON && step >= 0) ? h->d_hist_iters + (size_t)step * h->n_inst
-                                                           : nullptr;
+    A.hist_iters = (mode == INST_MODE_NEWTON && step >= 0) ? h->d_hist_iters : nullptr;
     A.bytes_counter = h->d_counters + 4;
     TRY(prof_begin(h));
     instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(h->d_insts, A, mode, step);
@@ -342,6 +350,119 @@ static int ensure_history(StrutHandle* h, int need) {
     h->d_hist_iters = ni;
     h->hist_cap = cap;
     return STRUT_OK;
+}
+
+template <typename T, size_t... I>
+static void fill_params(T& t, void** p, std::index_sequence<I...>) {
+    ((p[I] = (void*)&std::get<I>(t)), ...);
+}
+
+// Adds a kernel node with the given launch configuration and arguments (copied at creation).
+template <typename... P, typename... Q>
+static int add_kernel_node(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* deps,
+                           size_t ndeps, void (*func)(P...), dim3 grid, dim3 block, size_t smem,
+                           Q... args) {
+    std::tuple<std::decay_t<P>...> vals(args...);
+    void* params[sizeof...(P) > 0 ? sizeof...(P) : 1];
+    fill_params(vals, params, std::index_sequence_for<P...>{});
+    cudaKernelNodeParams kp;
+    std::memset(&kp, 0, sizeof(kp));
+    kp.func = (void*)func;
+    kp.gridDim = grid;
+    kp.blockDim = block;
+    kp.sharedMemBytes = (unsigned)smem;
+    kp.kernelParams = params;
+    kp.extra = nullptr;
+    CK(cudaGraphAddKernelNode(node, g, deps, ndeps, &kp));
+    return STRUT_OK;
+}
+
+static int add_while_node(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* deps,
+                          size_t ndeps, cudaGraphConditionalHandle handle, cudaGraph_t* body) {
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+    std::memset(raw, 0, sizeof(raw));
+    cudaGraphNodeParams* np = reinterpret_cast<cudaGraphNodeParams*>(raw);
+    np->type = cudaGraphNodeTypeConditional;
+    np->conditional.handle = handle;
+    np->conditional.type = cudaGraphCondTypeWhile;
+    np->conditional.size = 1;
+    CK(cudaGraphAddNode(node, g, deps, ndeps, np));
+    *body = np->conditional.phGraph_out[0];
+    return STRUT_OK;
+}
+
+// The whole step loop as one CUDA graph: an outer WHILE over steps (condition set by
+// step_end_kernel) around predictor -> inner WHILE over Newton iterations (element state
+// determination, instance Newton kernel, newton_check_kernel sets the condition) -> commit ->
+// Newmark update -> displacement records -> step_end.  The host synchronises once per run.
+static int build_graph(StrutHandle* h) {
+    if (h->gexec) {
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+    }
+    if (h->graph) {
+        cudaGraphDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    h->graph = g;
+    cudaGraphConditionalHandle outer, inner;
+    CK(cudaGraphConditionalHandleCreate(&outer, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNode_t n_outer;
+    cudaGraph_t body;
+    TRY(add_while_node(&n_outer, g, nullptr, 0, outer, &body));
+    CK(cudaGraphConditionalHandleCreate(&inner, body, 1, cudaGraphCondAssignDefault));
+    const int nF = h->n_free_total;
+    const int tb = 256;
+    const int npred = std::max(nF, h->n_inst);
+    InstArrays A = h->A;
+    A.hist_iters = h->d_hist_iters;
+    A.ctl = h->d_ctl;
+    A.bytes_counter = h->d_counters + 4;
+    cudaGraphNode_t n_pred, n_inner, n_commit, n_post, n_rec, n_end;
+    TRY(add_kernel_node(&n_pred, body, nullptr, 0, predictor_kernel, dim3((npred + tb - 1) / tb), dim3(tb), 0,
+                        (const DevInst*)h->d_insts, A, (const int*)h->d_free_inst, (const int*)h->d_free_dir,
+                        (const double*)h->d_ag, nF, h->n_inst, h->d_ctl, inner, 1));
+    cudaGraph_t ibody;
+    TRY(add_while_node(&n_inner, body, &n_pred, 1, inner, &ibody));
+    cudaGraphNode_t n_el, n_in, n_chk;
+    TRY(add_kernel_node(&n_el, ibody, nullptr, 0, element_state_kernel, dim3(h->n_elem),
+                        dim3(32 * std::max(h->max_nip, 2)), h->elem_smem, (const DevElem*)h->d_elems, h->geo,
+                        h->fs, (const double*)h->A.u_full, h->d_estate, h->d_ek, h->d_ef,
+                        (const int*)h->A.active, h->A.status, h->d_elem_err, h->d_counters));
+    TRY(add_kernel_node(&n_in, ibody, &n_el, 1, instance_newton_kernel, dim3(h->n_inst), dim3(256),
+                        h->inst_smem, (const DevInst*)h->d_insts, A, (int)INST_MODE_NEWTON, 0));
+    TRY(add_kernel_node(&n_chk, ibody, &n_in, 1, newton_check_kernel, dim3(1), dim3(32), 0, h->d_ctl,
+                        (const int*)h->A.nactive, inner, 1));
+    TRY(add_kernel_node(&n_commit, body, &n_inner, 1, commit_kernel, dim3(h->n_elem),
+                        dim3(32 * std::max(h->max_nip, 2)), 0, (const DevElem*)h->d_elems, h->geo, h->fs,
+                        (const double*)h->A.u_full, h->d_estate, (const int*)h->A.status, h->d_hist_ef,
+                        (const int*)h->d_rece_base, std::max(h->n_rece_slots, 1), (const DevCtl*)h->d_ctl));
+    TRY(add_kernel_node(&n_post, body, &n_commit, 1, post_step_kernel, dim3((nF + tb - 1) / tb), dim3(tb), 0,
+                        (const DevInst*)h->d_insts, A, (const int*)h->d_free_inst, nF));
+    cudaGraphNode_t last = n_post;
+    if (h->n_rec_total > 0) {
+        TRY(add_kernel_node(&n_rec, body, &n_post, 1, record_disp_kernel, dim3((h->n_rec_total + tb - 1) / tb),
+                            dim3(tb), 0, (const double*)h->A.u_full, (const int*)h->d_rec_dof, h->n_rec_total,
+                            h->d_hist_disp, (const DevCtl*)h->d_ctl));
+        last = n_rec;
+    }
+    TRY(add_kernel_node(&n_end, body, &last, 1, step_end_kernel, dim3(1), dim3(256), 0, h->d_ctl,
+                        (const int*)h->A.status, h->d_fail_step, h->n_inst, h->A.nactive, outer, 1));
+    CK(cudaGraphInstantiate(&h->gexec, g, 0));
+    h->graph_keys[0] = h->d_hist_disp;
+    h->graph_keys[1] = h->d_hist_ef;
+    h->graph_keys[2] = h->d_hist_iters;
+    h->graph_keys[3] = h->d_ag;
+    return STRUT_OK;
+}
+
+static int ensure_graph(StrutHandle* h) {
+    if (h->gexec && h->graph_keys[0] == h->d_hist_disp && h->graph_keys[1] == h->d_hist_ef &&
+        h->graph_keys[2] == h->d_hist_iters && h->graph_keys[3] == h->d_ag)
+        return STRUT_OK;
+    return build_graph(h);
 }
 
 extern "C" {
@@ -737,6 +858,12 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     A.ek = h->d_ek;
     A.ef = h->d_ef;
     A.Kinit = d_Kinit;
+    if ((rc = dzeros(&h->d_ctl, 1, al))) return bail(rc);
+    {
+        std::vector<int> neg(h->n_inst, -1);
+        if ((rc = upload(&h->d_fail_step, neg, al))) return bail(rc);
+    }
+    A.ctl = h->d_ctl;
     CK(cudaMallocHost((void**)&h->h_ctrl, 4 * sizeof(int)));
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
@@ -817,55 +944,85 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
     const int nF = h->n_free_total;
     const int tb = 256;
     int rc = STRUT_OK;
-    for (int s = 0; s < n_steps; ++s) {
-        const int step = h->steps_done;
+    const int step0 = h->steps_done;
+    {
+        DevCtl c;
+        std::memset(&c, 0, sizeof(c));
+        c.step = step0;
+        c.step0 = step0;
+        c.n_end = step0 + n_steps;
+        c.max_iters = h->max_iters_global;
+        c.single = h->n_inst == 1;
+        CK(cudaMemcpyAsync(h->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemsetAsync(h->A.nactive, 0, 4 * sizeof(int), h->stream));
-        const int npred = std::max(nF, h->n_inst);
-        TRY(prof_begin(h));
-        predictor_kernel<<<(npred + tb - 1) / tb, tb, 0, h->stream>>>(
-            h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag + (size_t)s * 4 * h->n_inst, nF, h->n_inst);
-        CK(cudaGetLastError());
-        TRY(prof_end(h, 3));
-        for (int it = 0; it < h->max_iters_global; ++it) {
-            TRY(launch_elements(h));
-            TRY(launch_instances(h, INST_MODE_NEWTON, step));
-            CK(cudaMemcpyAsync(h->h_ctrl, h->A.nactive, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            if (h->h_ctrl[0] <= 0) break;
-        }
-        // A failed instance keeps its status and is masked out of every later step; the other
-        // instances of the batch carry on.  The first failure is reported.
-        if (rc == STRUT_OK) {
-            std::vector<int> status(h->n_inst);
-            CK(cudaMemcpy(status.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
-            for (int i = 0; i < h->n_inst; ++i) {
-                if (status[i] != 0) {
-                    st.failed_instance = i;
-                    st.failed_step = step;
-                    rc = status[i];
-                    break;
-                }
-            }
-            if (rc != STRUT_OK && h->n_inst == 1) break;
-        }
-        TRY(prof_begin(h));
-        commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
-            h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status,
-            h->d_hist_ef + (size_t)step * std::max(h->n_rece_slots, 1) * 6, h->d_rece_base);
-        CK(cudaGetLastError());
-        TRY(prof_end(h, 2));
-        TRY(prof_begin(h));
-        post_step_kernel<<<(nF + tb - 1) / tb, tb, 0, h->stream>>>(h->d_insts, h->A, h->d_free_inst, nF);
-        CK(cudaGetLastError());
-        TRY(prof_end(h, 4));
-        if (h->prof) h->P.bytes[2] += h->commit_bytes_total;
-        if (h->n_rec_total > 0) {
-            record_disp_kernel<<<(h->n_rec_total + tb - 1) / tb, tb, 0, h->stream>>>(
-                h->A.u_full, h->d_rec_dof, h->n_rec_total, h->d_hist_disp + (size_t)step * h->n_rec_total);
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (n_steps > 0 && !h->prof) {
+        TRY(ensure_graph(h));
+        CK(cudaGraphLaunch(h->gexec, h->stream));
+    } else {
+        // host-driven loop (profiling: per-launch event timing on the launching stream)
+        cudaGraphConditionalHandle none = 0;
+        for (int s = 0; s < n_steps; ++s) {
+            const int step = step0 + s;
+            const int npred = std::max(nF, h->n_inst);
+            TRY(prof_begin(h));
+            predictor_kernel<<<(npred + tb - 1) / tb, tb, 0, h->stream>>>(
+                h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag, nF, h->n_inst, h->d_ctl, none, 0);
             CK(cudaGetLastError());
+            TRY(prof_end(h, 3));
+            for (int it = 0; it < h->max_iters_global; ++it) {
+                TRY(launch_elements(h));
+                TRY(launch_instances(h, INST_MODE_NEWTON, step));
+                CK(cudaMemcpyAsync(h->h_ctrl, h->A.nactive, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                if (h->h_ctrl[0] <= 0) break;
+            }
+            TRY(prof_begin(h));
+            commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
+                h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, h->d_hist_ef, h->d_rece_base,
+                std::max(h->n_rece_slots, 1), h->d_ctl);
+            CK(cudaGetLastError());
+            TRY(prof_end(h, 2));
+            TRY(prof_begin(h));
+            post_step_kernel<<<(nF + tb - 1) / tb, tb, 0, h->stream>>>(h->d_insts, h->A, h->d_free_inst, nF);
+            CK(cudaGetLastError());
+            TRY(prof_end(h, 4));
+            if (h->prof) h->P.bytes[2] += h->commit_bytes_total;
+            if (h->n_rec_total > 0) {
+                record_disp_kernel<<<(h->n_rec_total + tb - 1) / tb, tb, 0, h->stream>>>(
+                    h->A.u_full, h->d_rec_dof, h->n_rec_total, h->d_hist_disp, h->d_ctl);
+                CK(cudaGetLastError());
+            }
+            step_end_kernel<<<1, 256, 0, h->stream>>>(h->d_ctl, h->A.status, h->d_fail_step, h->n_inst,
+                                                      h->A.nactive, none, 0);
+            CK(cudaGetLastError());
+            if (h->n_inst == 1) {
+                int s0 = 0;
+                CK(cudaMemcpyAsync(&s0, h->A.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                if (s0 != 0) break;
+            }
         }
-        h->steps_done++;
-        st.steps_done++;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    {
+        DevCtl c;
+        CK(cudaMemcpy(&c, h->d_ctl, sizeof(c), cudaMemcpyDeviceToHost));
+        st.steps_done = c.step - step0;
+        h->steps_done = c.step;
+        std::vector<int> status(h->n_inst), fstep(h->n_inst);
+        CK(cudaMemcpy(status.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fstep.data(), h->d_fail_step, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
+        // the first failure of this run: earliest step, then lowest instance
+        for (int i = 0; i < h->n_inst; ++i) {
+            if (status[i] == 0 || fstep[i] < step0) continue;
+            if (st.failed_instance < 0 || fstep[i] < st.failed_step) {
+                st.failed_instance = i;
+                st.failed_step = fstep[i];
+                rc = status[i];
+            }
+        }
     }
     CK(cudaStreamSynchronize(h->stream));
     unsigned long long cnt[8];
@@ -1072,8 +1229,8 @@ int strut_gpu_factor_solve(StrutHandle* h, const double* rhs, double* du) {
 
 int strut_gpu_commit(StrutHandle* h) {
     if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
-    commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate,
-                                                                 h->A.status, nullptr, h->d_rece_base);
+    commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
+        h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, nullptr, h->d_rece_base, 1, h->d_ctl);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
     return STRUT_OK;
@@ -1209,7 +1366,7 @@ int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double
     if (n_fibers) *n_fibers = nf;
     if (!out) return STRUT_OK;
     CK(cudaDeviceSynchronize());
-    // 16 doubles per fiber: eps, sig, tan, then the family's history fields, then kon
+    // 16 doubles per fiber: the family's committed fields in declaration order, kon in slot 15
     std::vector<double> o((size_t)nf * 16, 0.0);
     const long long n2 = (long long)b->n_inst * sd.n_s2, n3 = (long long)b->n_inst * sd.n_c2,
                     n1 = (long long)b->n_inst * sd.n_s1;

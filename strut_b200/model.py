@@ -261,19 +261,23 @@ class Model:
         model = case.get("model", {})
         self.ndm = int(model.get("ndm", 2))
         self.ndf = int(model.get("ndf", 3))
-        if self.ndm != 2 or self.ndf != 3:
-            raise ModelError("this path implements 2D frames (ndm=2, ndf=3)")
+        if (self.ndm, self.ndf) not in ((2, 3), (3, 6)):
+            raise ModelError("this path implements frames with ndm=2, ndf=3 or ndm=3, ndf=6")
         nodes = case["nodes"]
         self.node_ids = [int(n["id"]) for n in nodes]
         self.node_index = {nid: i for i, nid in enumerate(self.node_ids)}
         nn = len(nodes)
         self.num_nodes = nn
         self.num_dofs = nn * self.ndf
-        self.coords = np.zeros(2 * nn)
+        self.coords = np.zeros(self.ndm * nn)
         constrained = np.zeros(self.num_dofs, dtype=bool)
         for i, n in enumerate(nodes):
-            self.coords[2 * i] = float(n["x"])
-            self.coords[2 * i + 1] = float(n["y"])
+            self.coords[self.ndm * i] = float(n["x"])
+            self.coords[self.ndm * i + 1] = float(n["y"])
+            if self.ndm == 3:
+                if "z" not in n:
+                    raise ModelError("z is required when ndm=3")
+                self.coords[self.ndm * i + 2] = float(n["z"])
             for d in n.get("constraints", []) or []:
                 d = int(d)
                 if d < 1 or d > self.ndf:
@@ -295,8 +299,9 @@ class Model:
         self.section_index = {}
         fibers = []
         sections = []
+        want = "FiberSection2d" if self.ndm == 2 else "FiberSection3d"
         for s in case.get("sections", []):
-            if s["type"] != "FiberSection2d":
+            if s["type"] != want:
                 raise ModelError(f"unsupported section type for this path: {s['type']}")
             cells = discretize_section(s.get("params", {}))
             off = len(fibers)
@@ -308,6 +313,13 @@ class Model:
                 fibers.append(f)
             sec = A.StrutFiberSection()
             sec.fiber_offset, sec.fiber_count = off, len(cells)
+            sec.dim = self.ndm
+            if self.ndm == 3:
+                prm = s.get("params", {})
+                sec.G = float(prm.get("G", 0.0))
+                sec.J = float(prm.get("J", 0.0))
+                if not (sec.G > 0.0 and sec.J > 0.0):
+                    raise ModelError("FiberSection3d beam-column use requires positive params.G and params.J")
             self.section_index[int(s["id"])] = len(sections)
             sections.append(sec)
         self.fibers = fibers
@@ -320,12 +332,13 @@ class Model:
         self.elem_ids = []
         for e in case.get("elements", []):
             et = e["type"]
-            if et == "forceBeamColumn2d":
-                tag = A.ELEM_FORCE_BEAM_COLUMN_2D
-            elif et == "dispBeamColumn2d":
-                tag = A.ELEM_DISP_BEAM_COLUMN_2D
-            else:
+            tags = {"forceBeamColumn2d": (A.ELEM_FORCE_BEAM_COLUMN_2D, 2),
+                    "dispBeamColumn2d": (A.ELEM_DISP_BEAM_COLUMN_2D, 2),
+                    "forceBeamColumn3d": (A.ELEM_FORCE_BEAM_COLUMN_3D, 3),
+                    "dispBeamColumn3d": (A.ELEM_DISP_BEAM_COLUMN_3D, 3)}
+            if et not in tags or tags[et][1] != self.ndm:
                 raise ModelError(f"unsupported element type for this path: {et}")
+            tag = tags[et][0]
             geom = e.get("geomTransf", "Linear")
             if geom == "Linear":
                 g = A.GEOM_LINEAR
@@ -356,9 +369,13 @@ class Model:
             el.section = self.section_index[sid]
             el.geom = g
             el.integration = rules[key]
-            for a in range(3):
+            for a in range(self.ndf):
                 el.dof[a] = ni * self.ndf + a
-                el.dof[3 + a] = nj * self.ndf + a
+                el.dof[self.ndf + a] = nj * self.ndf + a
+            if "vecxz" in e and e["vecxz"] is not None:
+                vx = [float(x) for x in e["vecxz"]]
+                el.vecxz[0], el.vecxz[1], el.vecxz[2] = vx
+                el.has_vecxz = 1
             self.elem_ids.append(int(e["id"]))
             elems.append(el)
         self.elements = elems

@@ -27,7 +27,7 @@ def test_library_exports_every_header_symbol(gpu_lib):
 
 def test_abi_version_and_error_text_without_gpu(gpu_lib):
     lib = gpu_lib.lib()
-    assert lib.strut_gpu_abi_version() == 1
+    assert lib.strut_gpu_abi_version() == 2
     assert isinstance(lib.strut_gpu_last_error(), bytes)
 
 
@@ -36,7 +36,8 @@ def test_struct_sizes_match_c_layout():
     assert C.sizeof(A.StrutUniMaterial) == 96
     assert C.sizeof(A.StrutFiber) == 32
     assert C.sizeof(A.StrutBeamIntegration) == 168
-    assert C.sizeof(A.StrutFrameElement) == 48
+    assert C.sizeof(A.StrutFrameElement) == 104
+    assert C.sizeof(A.StrutFiberSection) == 32
     assert C.sizeof(A.StrutExcitation) == 48
     assert C.sizeof(A.StrutModelDesc) == 320
     assert C.sizeof(A.StrutStepStats) == 56

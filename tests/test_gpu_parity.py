@@ -245,3 +245,19 @@ def test_failed_instance_is_masked_and_others_continue(gpu_lib):
         solo.run(60)
         d_solo, e_solo, i_solo = solo.history(0)
     assert np.array_equal(d_batch, d_solo) and np.array_equal(i_batch, i_solo)
+
+
+def test_graph_loop_equals_host_loop(gpu_lib):
+    """The CUDA-graph step loop (conditional WHILE nodes) and the host-driven loop used while
+    profiling launch the same kernels in the same order: identical histories, bit for bit."""
+    cases = [W.rc_frame_case(stories=s, bays=b, steps=50, seed=40 + s) for s, b in ((2, 1), (3, 2))]
+    out = []
+    for prof in (0, 1):
+        models = [M.Model(c) for c in cases]
+        with gpu_lib.Analysis(models) as an:
+            gpu_lib.lib().strut_gpu_set_profiling(an.h, prof)
+            an.run(20)
+            an.run(30)
+            out.append([an.history(i) for i in range(2)])
+    for (d0, e0, i0), (d1, e1, i1) in zip(out[0], out[1]):
+        assert np.array_equal(d0, d1) and np.array_equal(e0, e1) and np.array_equal(i0, i1)
