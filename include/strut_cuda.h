@@ -205,7 +205,9 @@ typedef struct StrutHandle StrutHandle;
 
 /* Per-kernel timing of a handle's launches, measured with CUDA events on the handle's own
  * stream while profiling is enabled (no counterpart in the reference; used for rooflines).
- * Index: 0 element state, 1 instance Newton, 2 commit, 3 predictor, 4 post-step. */
+ * Index: 0 element state, 1 instance Newton, 2 commit, 3 predictor, 4 post-step;
+ * 5 the element critical path: bytes[5] sums, over element launches, the largest number of
+ * forceBeamColumn local iterations one element ran in that launch (ms[5] = ms[0]). */
 #define STRUT_PROF_KERNELS 8
 typedef struct StrutKernelProfile {
     int64_t launches[STRUT_PROF_KERNELS];

@@ -48,7 +48,7 @@ def lib():
         L.oracle_run_transient.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _ip, _ip]
         L.oracle_state_determination.argtypes = [C.POINTER(A.StrutModelDesc), _dp, _dp, _dp, _ip]
         L.oracle_run_transient_batch.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, C.c_int,
-                                                 C.c_int, _ip]
+                                                 C.c_int, _ip, _ip]
         _lib = L
     return _lib
 
@@ -118,9 +118,13 @@ def state_determination(model, u_free):
 
 
 def run_batch(models, steps: int, nthreads: int):
+    """Runs every model for `steps` steps over `nthreads` host threads.  Returns
+    (first failure status or 0, total Newton iterations, per-record status array)."""
     descs = (A.StrutModelDesc * len(models))()
     for i, m in enumerate(models):
         descs[i] = m.desc()
     tot = C.c_int(0)
-    rc = lib().oracle_run_transient_batch(descs, len(models), steps, nthreads, C.byref(tot))
-    return rc, tot.value
+    st = np.zeros(len(models), dtype=np.int32)
+    rc = lib().oracle_run_transient_batch(descs, len(models), steps, nthreads, C.byref(tot),
+                                          st.ctypes.data_as(_ip))
+    return rc, tot.value, st

@@ -54,10 +54,12 @@ int oracle_run_transient(const StrutModelDesc* m, int steps, double* disp_hist,
 /* One element state determination + assembly at u_free (parity entry). */
 int oracle_state_determination(const StrutModelDesc* m, const double* u_free,
                                double* f_int_free, double* band_out, int* half_bw);
-/* Multi-instance run over nthreads host threads (CPU baseline leg). */
+/* Number of BandGeneral factorisations that fell back to dense partial-pivot LU. */
 long oracle_dense_fallbacks(void);
+/* Multi-instance run over nthreads host threads (CPU baseline leg).  record_status (optional,
+ * n entries) receives each record's status; the return value is the first failure seen. */
 int oracle_run_transient_batch(const StrutModelDesc* models, int n, int steps, int nthreads,
-                               int* total_iters);
+                               int* total_iters, int* record_status);
 
 #ifdef __cplusplus
 }

@@ -721,6 +721,7 @@ int oracle_state_determination(const StrutModelDesc* d, const double* u_free,
 typedef struct {
     const StrutModelDesc* models;
     int n, steps, next, total_iters, rc;
+    int* record_status;
     pthread_mutex_t lock;
 } BatchJob;
 
@@ -740,6 +741,7 @@ static void* batch_worker(void* arg) {
         free(iters);
         pthread_mutex_lock(&job->lock);
         job->total_iters += tot;
+        if (job->record_status) job->record_status[i] = rc;
         if (rc != STRUT_OK && job->rc == STRUT_OK) job->rc = rc;
         pthread_mutex_unlock(&job->lock);
     }
@@ -747,9 +749,10 @@ static void* batch_worker(void* arg) {
 }
 
 int oracle_run_transient_batch(const StrutModelDesc* models, int n, int steps, int nthreads,
-                               int* total_iters) {
+                               int* total_iters, int* record_status) {
     BatchJob job;
     memset(&job, 0, sizeof(job));
+    job.record_status = record_status;
     job.models = models;
     job.n = n;
     job.steps = steps;

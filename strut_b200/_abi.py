@@ -188,6 +188,7 @@ PROF_INSTANCE = 1
 PROF_COMMIT = 2
 PROF_PREDICTOR = 3
 PROF_POST = 4
+PROF_ELEMENT_CRITICAL = 5
 
 
 # Every function the header declares, with its ctypes signature.  Used by the binding and by

@@ -1,13 +1,17 @@
 // Fused element state determination for forceBeamColumn2d / dispBeamColumn2d on sm_100a.
 //
-// One CTA per element, one warp per integration point (section).  The element's committed
-// fiber history (all of its sections, all families) is staged into shared memory with
-// cp.async.bulk (the TMA unit's bulk copy) completing on an mbarrier; every section evaluation
-// of the element-level flexibility iteration then reads shared memory only.  Each lane walks
-// the fibers of its warp's section, computes trial stress/tangent in registers and the warp
-// reduces the section resultants and tangent (N, Mz, k11, k12, k22) with shuffles.  Thread 0
-// runs the element-level algebra (3x3 flexibility inverse, work-norm test, subdivision and
-// scheme fallbacks); decisions are broadcast through shared memory so control stays uniform.
+// One CTA per element, one team of 128 threads (64 when an element has more than 5 points) per
+// integration point.  The element's committed fiber history (all of its sections, all
+// families) is staged into shared memory with cp.async.bulk (the TMA unit's bulk copy)
+// completing on an mbarrier; every section evaluation of the element-level flexibility
+// iteration then reads shared memory only.  Each thread computes the trial stress/tangent of
+// one or two fibers of its team's section in registers; the team reduces the section
+// resultants and tangent (N, Mz, k11, k12, k22) with shuffles and a fixed-order block sum.
+// The team leaders turn their section's tangent into its flexibility in parallel; thread 0 runs
+// the remaining element algebra (3x3 flexibility inverse, work-norm test, subdivision and
+// scheme fallbacks) and decisions are broadcast through shared memory so control stays uniform.
+// The per-iteration latency of one element is what bounds a batch whose slowest record keeps
+// failing its local iteration, so the work between barriers is kept short.
 //
 // Algorithm (paths relative to the Strut project root):
 //   src/mojo/elements/force_beam_column2d.mojo:223-272 (3x3 inverse), 608-801 (exact elastic,
@@ -71,6 +75,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase)
 
 enum { ELEM_ERR_NONE = 0, ELEM_ERR_TMA_TIMEOUT = 1, ELEM_ERR_FAILED = 2 };
 
+// Section teams: each integration point of an element is evaluated by a team of TEAM threads
+// (64 or 128).  The team's section sums follow one canonical order whatever TEAM is: fiber j of a
+// family (family-local index) is accumulated by virtual lane j % 128 in increasing j, each block of
+// 32 virtual lanes is summed by a shuffle butterfly, and the four block sums are added in block
+// order.  A record's result therefore never depends on the launch shape of the batch it is in.
+constexpr int kVLanes = 128;
+constexpr int kVBlocks = kVLanes / 32;
+
 // element-level scratch in shared memory
 struct ElemScratch {
     double q[3], acc_q[3], acc_v[3], v[3], rem[3], att[3], tv[3], zero3[3];
@@ -78,6 +90,8 @@ struct ElemScratch {
     double vs_e[kMaxIp], vs_k[kMaxIp];    // element state section deformations
     double pt_e[kMaxIp], pt_k[kMaxIp];    // points to evaluate
     double resp[kMaxIp][5];
+    double part[kMaxIp][kVBlocks][6];     // per-block section partial sums
+    double n00[kMaxIp], n01[kMaxIp], n11[kMaxIp];  // flexibility of the last evaluation
     double sub_e[kMaxIp], sub_k[kMaxIp], ssr_n[kMaxIp], ssr_m[kMaxIp];
     double fs00[kMaxIp], fs01[kMaxIp], fs11[kMaxIp];
     double best[10];
@@ -88,12 +102,14 @@ struct ElemScratch {
     int best_ok;
     int c_valid;
     int flag;
+    int sing;  // some section of the last evaluation had a singular tangent
     int loop_ctrl;
     int local_iters;
     int section_evals;
 };
 
-// Family views of the element's committed history in shared memory.
+// Family views of the element's committed history (shared memory, or global memory with the
+// family length as field stride).
 struct StageView {
     const double* c2;  // 5 fields x c2_blk
     const double* s2;  // 10 fields x s2_blk
@@ -102,99 +118,141 @@ struct StageView {
     int c2_blk, s2_blk, s1_blk;
 };
 
-// Warp-level section evaluation of section `ip` of the element at (eps0, kappa).
-// Lanes stride over each family's fibers; results are reduced with shuffles and returned in
-// every lane.  hist == nullptr evaluates elastic-only sections.
-__device__ __forceinline__ void section_eval_warp(const Geo& g, const DevSection& sd,
+__device__ __forceinline__ void acc_fiber(double* a, double fs, double ks, double y) {
+    a[0] += fs;
+    a[1] += -fs * y;
+    a[2] += ks;
+    a[3] += -ks * y;
+    a[4] += ks * y * y;
+}
+
+// Team evaluation of section `ip` of an element at (eps0, kappa); r is the thread's rank in
+// the team.  Writes the team's per-block partial sums (N, Mz, k11, k12, k22, elastic k12) to
+// part[kVBlocks][6]; the caller adds them in block order after a barrier.
+template <int TEAM>
+__device__ __forceinline__ void section_eval_team(const Geo& g, const DevSection& sd,
                                                   const StageView& sv, int ip, double eps0,
-                                                  double kappa, int lane, double out[5]) {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a3el = 0.0;
+                                                  double kappa, int r, double (*part)[6]) {
+    constexpr int NS = kVLanes / TEAM;  // virtual lanes per thread
+    double acc[NS][6];
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc[s][c] = 0.0;
     int base = sd.geo_off;
-    for (int j = lane; j < sd.n_s2; j += 32) {
-        const int idx = ip * sd.n_s2 + j;
-        S2State c;
-        const int B = sv.s2_blk;
-        c.eps = sv.s2[0 * B + idx];
-        c.sig = sv.s2[1 * B + idx];
-        c.tan = sv.s2[2 * B + idx];
-        c.epsmin = sv.s2[3 * B + idx];
-        c.epsmax = sv.s2[4 * B + idx];
-        c.epspl = sv.s2[5 * B + idx];
-        c.epss0 = sv.s2[6 * B + idx];
-        c.sigs0 = sv.s2[7 * B + idx];
-        c.epsr = sv.s2[8 * B + idx];
-        c.sigr = sv.s2[9 * B + idx];
-        c.kon = sv.kon[idx];
-        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
-        S2State t;
-        steel02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
-        const double fs = t.sig * A, ks = t.tan * A;
-        a0 += fs;
-        a1 += -fs * y;
-        a2 += ks;
-        a3 += -ks * y;
-        a4 += ks * y * y;
+    for (int j0 = 0; j0 < sd.n_s2; j0 += kVLanes) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = j0 + s * TEAM + r;
+            if (j >= sd.n_s2) continue;
+            const int idx = ip * sd.n_s2 + j;
+            const int B = sv.s2_blk;
+            S2State c;
+            c.eps = sv.s2[0 * B + idx];
+            c.sig = sv.s2[1 * B + idx];
+            c.tan = sv.s2[2 * B + idx];
+            c.epsmin = sv.s2[3 * B + idx];
+            c.epsmax = sv.s2[4 * B + idx];
+            c.epspl = sv.s2[5 * B + idx];
+            c.epss0 = sv.s2[6 * B + idx];
+            c.sigs0 = sv.s2[7 * B + idx];
+            c.epsr = sv.s2[8 * B + idx];
+            c.sigr = sv.s2[9 * B + idx];
+            c.kon = sv.kon[idx];
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            S2State t;
+            steel02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            acc_fiber(acc[s], t.sig * A, t.tan * A, y);
+        }
     }
     base += sd.n_s2;
-    for (int j = lane; j < sd.n_c2; j += 32) {
-        const int idx = ip * sd.n_c2 + j;
-        const int B = sv.c2_blk;
-        C2State c;
-        c.eps = sv.c2[0 * B + idx];
-        c.sig = sv.c2[1 * B + idx];
-        c.tan = sv.c2[2 * B + idx];
-        c.ecmin = sv.c2[3 * B + idx];
-        c.dept = sv.c2[4 * B + idx];
-        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
-        C2State t;
-        concrete02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
-        const double fs = t.sig * A, ks = t.tan * A;
-        a0 += fs;
-        a1 += -fs * y;
-        a2 += ks;
-        a3 += -ks * y;
-        a4 += ks * y * y;
+    for (int j0 = 0; j0 < sd.n_c2; j0 += kVLanes) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = j0 + s * TEAM + r;
+            if (j >= sd.n_c2) continue;
+            const int idx = ip * sd.n_c2 + j;
+            const int B = sv.c2_blk;
+            C2State c;
+            c.eps = sv.c2[0 * B + idx];
+            c.sig = sv.c2[1 * B + idx];
+            c.tan = sv.c2[2 * B + idx];
+            c.ecmin = sv.c2[3 * B + idx];
+            c.dept = sv.c2[4 * B + idx];
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            C2State t;
+            concrete02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            acc_fiber(acc[s], t.sig * A, t.tan * A, y);
+        }
     }
     base += sd.n_c2;
-    for (int j = lane; j < sd.n_s1; j += 32) {
-        const int idx = ip * sd.n_s1 + j;
-        const int B = sv.s1_blk;
-        S1State c;
-        c.eps = sv.s1[0 * B + idx];
-        c.sig = sv.s1[1 * B + idx];
-        c.tan = sv.s1[2 * B + idx];
-        c.epsp = sv.s1[3 * B + idx];
-        c.alpha = sv.s1[4 * B + idx];
-        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
-        S1State t;
-        steel01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
-        const double fs = t.sig * A, ks = t.tan * A;
-        a0 += fs;
-        a1 += -fs * y;
-        a2 += ks;
-        a3 += -ks * y;
-        a4 += ks * y * y;
+    for (int j0 = 0; j0 < sd.n_s1; j0 += kVLanes) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = j0 + s * TEAM + r;
+            if (j >= sd.n_s1) continue;
+            const int idx = ip * sd.n_s1 + j;
+            const int B = sv.s1_blk;
+            S1State c;
+            c.eps = sv.s1[0 * B + idx];
+            c.sig = sv.s1[1 * B + idx];
+            c.tan = sv.s1[2 * B + idx];
+            c.epsp = sv.s1[3 * B + idx];
+            c.alpha = sv.s1[4 * B + idx];
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            S1State t;
+            steel01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            acc_fiber(acc[s], t.sig * A, t.tan * A, y);
+        }
     }
     base += sd.n_s1;
-    for (int j = lane; j < sd.n_el; j += 32) {
-        const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
-        const double E = g.mats[__ldg(g.m + base + j)].p[0];
-        const double ks = E * A;
-        const double fs = ks * (eps0 - y * kappa);
-        a0 += fs;
-        a1 += -fs * y;
-        a2 += ks;
-        a3el += -ks * y;
-        a4 += ks * y * y;
+    for (int j0 = 0; j0 < sd.n_el; j0 += kVLanes) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = j0 + s * TEAM + r;
+            if (j >= sd.n_el) continue;
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            const double E = g.mats[__ldg(g.m + base + j)].p[0];
+            const double ks = E * A;
+            const double fs = ks * (eps0 - y * kappa);
+            acc[s][0] += fs;
+            acc[s][1] += -fs * y;
+            acc[s][2] += ks;
+            acc[s][5] += -ks * y;
+            acc[s][4] += ks * y * y;
+        }
     }
-    out[0] = warp_sum(a0);
-    out[1] = warp_sum(a1);
-    out[2] = warp_sum(a2);
-    // fiber2d.mojo:3491-3499: a section whose elastic fibers share one modulus reports no
-    // elastic k12 contribution.
-    const double k12el = warp_sum(a3el);
-    out[3] = warp_sum(a3) + (sd.el_uniform ? 0.0 : k12el);
-    out[4] = warp_sum(a4);
+    const int lane = r & 31, w = r >> 5;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        double v[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[c] = warp_sum(acc[s][c]);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) part[s * (TEAM / 32) + w][c] = v[c];
+        }
+    }
+}
+
+// Section resultants and tangent from the block partial sums, in block order.
+// fiber2d.mojo:3491-3499: a section whose elastic fibers share one modulus reports no
+// elastic k12 contribution.
+__device__ __forceinline__ void section_finish(const DevSection& sd, const double (*part)[6],
+                                               double* out) {
+    double v[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        double t = part[0][c];
+#pragma unroll
+        for (int b = 1; b < kVBlocks; ++b) t += part[b][c];
+        v[c] = t;
+    }
+    out[0] = v[0];
+    out[1] = v[1];
+    out[2] = v[2];
+    out[3] = v[3] + (sd.el_uniform ? 0.0 : v[5]);
+    out[4] = v[4];
 }
 
 __device__ __forceinline__ bool invert3(const double* F, double* k) {
@@ -238,41 +296,61 @@ __device__ __forceinline__ void flex_accum(double* F, double wL, double bmi, dou
     F[8] += wL * bmj * f11 * bmj;
 }
 
-// All warps with warp < nip evaluate their section at S.pt; lane 0 stores S.resp.
+// Every team with team < nip evaluates its section at S.pt; the team leaders then finish the
+// sums into S.resp and, when flex is set, the section flexibility into S.n00/n01/n11
+// (fiber_section2d_batch_eval_same_def: singular if |det| <= 1e-40, reported in S.sing, which
+// the caller cleared before the preceding barrier).
+template <int TEAM>
 __device__ __forceinline__ void eval_points(const Geo& g, const DevSection& sd,
                                             const StageView& sv, const DevElem& E,
-                                            ElemScratch& S) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp < E.nip) {
-        double r[5];
-        section_eval_warp(g, sd, sv, warp, S.pt_e[warp], S.pt_k[warp], lane, r);
-        if (lane == 0) {
-#pragma unroll
-            for (int c = 0; c < 5; ++c) S.resp[warp][c] = r[c];
+                                            ElemScratch& S, bool flex) {
+    const int team = threadIdx.x / TEAM, r = threadIdx.x % TEAM;
+    if (team < E.nip)
+        section_eval_team<TEAM>(g, sd, sv, team, S.pt_e[team], S.pt_k[team], r, S.part[team]);
+    __syncthreads();
+    if (r == 0 && team < E.nip) {
+        double* out = S.resp[team];
+        section_finish(sd, S.part[team], out);
+        if (flex) {
+            const double k11 = out[2], k12 = out[3], k22 = out[4];
+            const double det = k11 * k22 - k12 * k12;
+            if (fabs(det) <= 1.0e-40) {
+                S.sing = 1;
+            } else {
+                const double inv_det = 1.0 / det;
+                S.n00[team] = k22 * inv_det;
+                S.n01[team] = -k12 * inv_det;
+                S.n11[team] = k11 * inv_det;
+            }
         }
     }
-    __syncthreads();
     if (threadIdx.x == 0) S.section_evals += E.nip;
+    __syncthreads();
 }
 
-// Section flexibility of every evaluated point in ip order, stopping at the first singular
-// one (fiber_section2d_batch_eval_same_def).  Thread 0 only.
-__device__ __forceinline__ bool flex_of_resp(const ElemScratch& S, int nip, double* f00,
-                                             double* f01, double* f11) {
-    for (int ip = 0; ip < nip; ++ip) {
-        const double k11 = S.resp[ip][2], k12 = S.resp[ip][3], k22 = S.resp[ip][4];
-        const double det = k11 * k22 - k12 * k12;
-        if (fabs(det) <= 1.0e-40) return false;
-        const double inv_det = 1.0 / det;
-        f00[ip] = k22 * inv_det;
-        f01[ip] = -k12 * inv_det;
-        f11[ip] = k11 * inv_det;
+// Next corrector points: s(q) - s_r mapped through the section flexibility (initial section
+// flexibility for scheme 1 and for the first iteration of scheme 2).  Thread 0 only.
+__device__ __forceinline__ void fbc_next_points(const DevSection& sd, const DevElem& E,
+                                                ElemScratch& S, bool use_init) {
+    for (int ip = 0; ip < E.nip; ++ip) {
+        const double xi = E.xi[ip];
+        const double bmi = xi - 1.0, bmj = xi;
+        const double ss0 = S.q[0] + 0.0;
+        const double ss1 = bmi * S.q[1] + bmj * S.q[2] + 0.0;
+        const double dss0 = ss0 - S.ssr_n[ip];
+        const double dss1 = ss1 - S.ssr_m[ip];
+        const double a00 = use_init ? sd.f00 : S.fs00[ip];
+        const double a01 = use_init ? sd.f01 : S.fs01[ip];
+        const double a11 = use_init ? sd.f11 : S.fs11[ip];
+        S.pt_e[ip] = S.sub_e[ip] + (a00 * dss0 + a01 * dss1);
+        S.pt_k[ip] = S.sub_k[ip] + (a01 * dss0 + a11 * dss1);
     }
-    return true;
+    S.sing = 0;
 }
 
 // _force_beam_column2d_try_increment, executed collectively.  Starting state: S.q, S.vs_*.
 // On success S.q / S.vs_* hold the converged state and S.best the result.
+template <int TEAM>
 __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const StageView& sv,
                                   const DevElem& E, ElemScratch& S, const double* base,
                                   const double* dv, int scheme) {
@@ -284,10 +362,12 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
             S.pt_e[ip] = S.vs_e[ip];
             S.pt_k[ip] = S.vs_k[ip];
         }
+        S.sing = 0;
     }
     __syncthreads();
     const bool cached = S.c_valid != 0;
-    if (!cached) eval_points(g, sd, sv, E, S);
+    if (!cached) eval_points<TEAM>(g, sd, sv, E, S, true);
+    const int num_iters = scheme == 1 ? 100 : 10;
     if (tid == 0) {
         int ok;
         if (cached) {
@@ -300,7 +380,13 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
             }
             ok = 1;
         } else {
-            ok = flex_of_resp(S, nip, S.fs00, S.fs01, S.fs11) ? 1 : 0;
+            ok = S.sing ? 0 : 1;
+            if (ok)
+                for (int ip = 0; ip < nip; ++ip) {
+                    S.fs00[ip] = S.n00[ip];
+                    S.fs01[ip] = S.n01[ip];
+                    S.fs11[ip] = S.n11[ip];
+                }
         }
         if (ok) {
             double P[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -318,36 +404,19 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
                 S.q[1] += (pk[3] * dv[0] + pk[4] * dv[1] + pk[5] * dv[2]);
                 S.q[2] += (pk[6] * dv[0] + pk[7] * dv[1] + pk[8] * dv[2]);
             }
+            // points of the first corrector iteration
+            fbc_next_points(sd, E, S, scheme == 1 || scheme == 2);
         }
         S.flag = ok;
     }
     __syncthreads();
     if (!S.flag) return false;
-    const int num_iters = scheme == 1 ? 100 : 10;
     for (int it = 0; it < num_iters; ++it) {
+        eval_points<TEAM>(g, sd, sv, E, S, true);
         if (tid == 0) {
             S.local_iters++;
-            const bool use_init = scheme == 1 || (scheme == 2 && it == 0);
-            for (int ip = 0; ip < nip; ++ip) {
-                const double xi = E.xi[ip];
-                const double bmi = xi - 1.0, bmj = xi;
-                const double ss0 = S.q[0] + 0.0;
-                const double ss1 = bmi * S.q[1] + bmj * S.q[2] + 0.0;
-                const double dss0 = ss0 - S.ssr_n[ip];
-                const double dss1 = ss1 - S.ssr_m[ip];
-                const double a00 = use_init ? sd.f00 : S.fs00[ip];
-                const double a01 = use_init ? sd.f01 : S.fs01[ip];
-                const double a11 = use_init ? sd.f11 : S.fs11[ip];
-                S.pt_e[ip] = S.sub_e[ip] + (a00 * dss0 + a01 * dss1);
-                S.pt_k[ip] = S.sub_k[ip] + (a01 * dss0 + a11 * dss1);
-            }
-        }
-        __syncthreads();
-        eval_points(g, sd, sv, E, S);
-        if (tid == 0) {
-            double n00[kMaxIp], n01[kMaxIp], n11[kMaxIp];
             int res = 0;
-            if (flex_of_resp(S, nip, n00, n01, n11)) {
+            if (!S.sing) {
                 double F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
                 double vr0 = 0.0, vr1 = 0.0, vr2 = 0.0;
                 for (int ip = 0; ip < nip; ++ip) {
@@ -355,18 +424,19 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
                     const double bmi = xi - 1.0, bmj = xi;
                     const double ss0 = S.q[0] + 0.0;
                     const double ss1 = bmi * S.q[1] + bmj * S.q[2] + 0.0;
+                    const double n00 = S.n00[ip], n01 = S.n01[ip], n11 = S.n11[ip];
                     S.sub_e[ip] = S.pt_e[ip];
                     S.sub_k[ip] = S.pt_k[ip];
                     S.ssr_n[ip] = S.resp[ip][0];
                     S.ssr_m[ip] = S.resp[ip][1];
-                    S.fs00[ip] = n00[ip];
-                    S.fs01[ip] = n01[ip];
-                    S.fs11[ip] = n11[ip];
+                    S.fs00[ip] = n00;
+                    S.fs01[ip] = n01;
+                    S.fs11[ip] = n11;
                     const double dr0 = ss0 - S.ssr_n[ip];
                     const double dr1 = ss1 - S.ssr_m[ip];
-                    const double dvr0 = n00[ip] * dr0 + n01[ip] * dr1;
-                    const double dvr1 = n01[ip] * dr0 + n11[ip] * dr1;
-                    flex_accum(F, wL, bmi, bmj, n00[ip], n01[ip], n11[ip]);
+                    const double dvr0 = n00 * dr0 + n01 * dr1;
+                    const double dvr1 = n01 * dr0 + n11 * dr1;
+                    flex_accum(F, wL, bmi, bmj, n00, n01, n11);
                     vr0 += wL * (S.pt_e[ip] + dvr0);
                     vr1 += wL * bmi * (S.pt_k[ip] + dvr1);
                     vr2 += wL * bmj * (S.pt_k[ip] + dvr1);
@@ -406,6 +476,8 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
                         S.best[7] = k[4];
                         S.best[8] = k[5];
                         S.best[9] = k[8];
+                    } else if (it + 1 < num_iters) {
+                        fbc_next_points(sd, E, S, scheme == 1);
                     }
                 }
             }
@@ -498,11 +570,12 @@ __device__ __forceinline__ void copy_struct(T* dst, const T* src) {
     for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) d[i] = s[i];
 }
 
-// Stages the element's committed fiber history into shared memory.  Returns false (and sets
-// *err) if the bulk copy did not complete within the bounded wait.
+// Stages the element's committed fiber history into shared memory.  bar was initialised once
+// for the CTA; phase is the parity of its next completion (every thread tracks the same value).
+// Returns false (and sets *err) if the bulk copy did not complete within the bounded wait.
 __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState& fs,
-                                              double* sm, uint64_t* bar, StageView& sv,
-                                              int* err) {
+                                              double* sm, uint64_t* bar, uint32_t& phase,
+                                              StageView& sv, int* err) {
     double* c2 = sm;
     double* s2 = c2 + 5 * E.c2_blk;
     double* s1 = s2 + 10 * E.s2_blk;
@@ -518,11 +591,8 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
                                       4 * E.s2_blk);
     if (bytes == 0) return true;
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+        // the previous element's reads of this buffer (generic proxy) come before the copies
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive_expect_tx(bar, bytes);
         for (int f = 0; f < 5 && E.c2_blk; ++f)
             bulk_g2s(c2 + f * E.c2_blk, fs.c2 + f * fs.c2_n + E.c2_off, 8u * E.c2_blk, bar);
@@ -532,28 +602,49 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
         for (int f = 0; f < 5 && E.s1_blk; ++f)
             bulk_g2s(s1 + f * E.s1_blk, fs.s1 + f * fs.s1_n + E.s1_off, 8u * E.s1_blk, bar);
     }
-    if (!mbar_wait_bounded(bar, 0)) {
+    const uint32_t ph = phase;
+    phase ^= 1u;
+    const bool ok = mbar_wait_bounded(bar, ph);
+    // every thread takes the same branch
+    if (__syncthreads_or(ok ? 0 : 1)) {
         if (threadIdx.x == 0) *err = ELEM_ERR_TMA_TIMEOUT;
-        // let the copies land before the CTA exits (second bounded wait)
-        mbar_wait_bounded(bar, 0);
+        // let the copies land before the CTA stops (second bounded wait)
+        mbar_wait_bounded(bar, ph);
         return false;
     }
     return true;
 }
 
-// mode 0: state determination (writes k, f and the element state)
-__global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
+// State determination of every element of the active instances: k (6x6 global), f (6) and the
+// element state.  One CTA per element, one TEAM-thread team per integration point.
+//
+// Persistent: the grid is sized to the resident CTAs of the device and each CTA walks the list
+// of elements of the instances still iterating (all elements when all_elems is set), so a
+// Newton iteration of a few slow records launches no idle CTAs.
+template <int TEAM>
+__global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
     double* __restrict__ estate, double* __restrict__ ek, double* __restrict__ ef,
     const int* __restrict__ active, int* __restrict__ status, int* __restrict__ elem_err,
-    unsigned long long* __restrict__ counters) {
+    unsigned long long* __restrict__ counters, ElemList el, const DevCtl* __restrict__ ctl,
+    int all_elems, int n_elem) {
     extern __shared__ __align__(128) double smem_fib[];
     __shared__ DevElem E;
     __shared__ DevSection sd;
     __shared__ ElemScratch S;
     __shared__ __align__(8) uint64_t bar;
-    const int e = blockIdx.x;
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    const int cur = all_elems ? 0 : (ctl->iter & 1);
+    if (!all_elems && blockIdx.x == 0 && tid == 0) el.count[cur ^ 1] = 0;
+    const int total = all_elems ? n_elem : el.count[cur];
+    __syncthreads();
+    uint32_t phase = 0;
+    bool stop = false;
+    auto process = [&](const int e) -> void {
     copy_struct(&E, elems + e);
     __syncthreads();
     if (!active[E.inst]) return;
@@ -586,35 +677,37 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
     }
     StageView sv;
     int err = ELEM_ERR_NONE;
-    const bool staged = stage_element(E, fs, smem_fib, &bar, sv, &err);
+    const bool staged = stage_element(E, fs, smem_fib, &bar, phase, sv, &err);
     __syncthreads();
     if (!staged) {
         if (tid == 0) {
             elem_err[e] = err;
             status[E.inst] = 5;
         }
+        stop = true;
         return;
     }
     const int nip = E.nip;
     if (E.type == 3) {
         // ---------------- dispBeamColumn2d ----------------
-        const int warp = tid >> 5, lane = tid & 31;
+        const int team = tid / TEAM, r = tid % TEAM;
         const double L = E.L, inv_L = 1.0 / L, inv_L_sq = inv_L * inv_L;
-        if (warp < nip) {
-            const double xi = E.xi[warp];
+        double eps0 = 0.0, kappa = 0.0;
+        if (team < nip) {
+            const double xi = E.xi[team];
             const double b1 = curv_shape(1, inv_L, inv_L_sq, xi);
             const double b2 = curv_shape(2, inv_L, inv_L_sq, xi);
             const double b4 = curv_shape(4, inv_L, inv_L_sq, xi);
             const double b5 = curv_shape(5, inv_L, inv_L_sq, xi);
-            const double eps0 = (-inv_L) * S.ul[0] + inv_L * S.ul[3];
-            const double kappa = b1 * S.ul[1] + b2 * S.ul[2] + b4 * S.ul[4] + b5 * S.ul[5];
-            double r[5];
-            section_eval_warp(g, sd, sv, warp, eps0, kappa, lane, r);
-            if (lane == 0) {
-                for (int c = 0; c < 5; ++c) S.resp[warp][c] = r[c];
-                S.vs_e[warp] = eps0;
-                S.vs_k[warp] = kappa;
-            }
+            eps0 = (-inv_L) * S.ul[0] + inv_L * S.ul[3];
+            kappa = b1 * S.ul[1] + b2 * S.ul[2] + b4 * S.ul[4] + b5 * S.ul[5];
+            section_eval_team<TEAM>(g, sd, sv, team, eps0, kappa, r, S.part[team]);
+        }
+        __syncthreads();
+        if (team < nip && r == 0) {
+            section_finish(sd, S.part[team], S.resp[team]);
+            S.vs_e[team] = eps0;
+            S.vs_k[team] = kappa;
         }
         __syncthreads();
         if (tid < 36) {
@@ -758,7 +851,7 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
                     }
                 }
                 __syncthreads();
-                if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.zero3, scheme)) continue;
+                if (!fbc_try_increment<TEAM>(g, sd, sv, E, S, S.acc_v, S.zero3, scheme)) continue;
                 if (tid == 0) S.best_ok = 1;
                 converged = 1;
                 break;
@@ -781,7 +874,7 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
                         }
                     }
                     __syncthreads();
-                    if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme)) continue;
+                    if (!fbc_try_increment<TEAM>(g, sd, sv, E, S, S.acc_v, S.att, scheme)) continue;
                     if (tid == 0) {
                         for (int i = 0; i < 3; ++i) {
                             S.acc_v[i] = S.tv[i];
@@ -904,6 +997,7 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
         f_to_global(S.f, E.c, E.s);
         atomicAdd(&counters[3], (unsigned long long)E.io_bytes);
         atomicAdd(&counters[0], (unsigned long long)S.local_iters);
+        atomicMax(&counters[5], (unsigned long long)S.local_iters);
         atomicAdd(&counters[1], (unsigned long long)S.section_evals);
         atomicAdd(&counters[2], (unsigned long long)S.section_evals *
                                     (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
@@ -911,6 +1005,11 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
     __syncthreads();
     if (tid < 36) ek[(size_t)e * 36 + tid] = S.k[tid];
     else if (tid < 42) ef[(size_t)e * 6 + tid - 36] = S.f[tid - 36];
+    };
+    for (int li = blockIdx.x; li < total && !stop; li += gridDim.x) {
+        process(all_elems ? li : el.list[cur][li]);
+        __syncthreads();
+    }
 }
 
 // Commit: recompute each fiber's trial state at the section deformation stored in the element
@@ -919,16 +1018,18 @@ __global__ void __launch_bounds__(32 * kMaxIp) element_state_kernel(
 // (helpers.mojo:1832-1883) and, for recorded elements, the global end forces
 // (helpers.mojo:1500-1600 for forceBeamColumn2d; a section evaluation at the converged
 // displacements from the new committed state for dispBeamColumn2d).
-__global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
+template <int TEAM>
+__global__ void __launch_bounds__(kTeamThreads) commit_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
     double* __restrict__ estate, const int* __restrict__ status, double* __restrict__ rec_base,
     const int* __restrict__ rece_base, int rec_slots, const DevCtl* __restrict__ ctl) {
     __shared__ DevElem E;
     __shared__ DevSection sd;
     __shared__ double resp[kMaxIp][5];
+    __shared__ double part[kMaxIp][kVBlocks][6];
     __shared__ double ul[6];
     const int e = blockIdx.x;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, team = tid / TEAM, r = tid % TEAM;
     double* rec_out = rec_base ? rec_base + (size_t)ctl->step * rec_slots * 6 : nullptr;
     copy_struct(&E, elems + e);
     __syncthreads();
@@ -936,12 +1037,12 @@ __global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
     copy_struct(&sd, g.secs + E.sec);
     __syncthreads();
     const int nip = E.nip;
-    if (warp < nip) {
-        const double eps0 = estate[(size_t)e * kEStride + kEe + warp];
-        const double kappa = estate[(size_t)e * kEStride + kEk + warp];
+    if (team < nip) {
+        const double eps0 = estate[(size_t)e * kEStride + kEe + team];
+        const double kappa = estate[(size_t)e * kEStride + kEk + team];
         int base = sd.geo_off;
-        for (int j = lane; j < sd.n_s2; j += 32) {
-            const long long idx = E.s2_off + warp * sd.n_s2 + j;
+        for (int j = r; j < sd.n_s2; j += TEAM) {
+            const long long idx = E.s2_off + team * sd.n_s2 + j;
             double* F = fs.s2 + idx;
             const long long N = fs.s2_n;
             S2State c, t;
@@ -955,8 +1056,8 @@ __global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
             F[8 * N] = t.epsr; F[9 * N] = t.sigr; fs.s2_kon[idx] = t.kon;
         }
         base += sd.n_s2;
-        for (int j = lane; j < sd.n_c2; j += 32) {
-            const long long idx = E.c2_off + warp * sd.n_c2 + j;
+        for (int j = r; j < sd.n_c2; j += TEAM) {
+            const long long idx = E.c2_off + team * sd.n_c2 + j;
             double* F = fs.c2 + idx;
             const long long N = fs.c2_n;
             C2State c, t;
@@ -966,8 +1067,8 @@ __global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
             F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.ecmin; F[4 * N] = t.dept;
         }
         base += sd.n_c2;
-        for (int j = lane; j < sd.n_s1; j += 32) {
-            const long long idx = E.s1_off + warp * sd.n_s1 + j;
+        for (int j = r; j < sd.n_s1; j += TEAM) {
+            const long long idx = E.s1_off + team * sd.n_s1 + j;
             double* F = fs.s1 + idx;
             const long long N = fs.s1_n;
             S1State c, t;
@@ -1013,10 +1114,10 @@ __global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
     if (E.type != 3 || E.rec < 0 || !rec_out) return;
     __syncthreads();
     // dispBeamColumn2d recorder: section evaluation at the converged displacements from the
-    // just-committed state (each lane reads back exactly the fibers it wrote)
+    // just-committed state (each thread reads back exactly the fibers it wrote)
     const double L = E.L, inv_L = 1.0 / L, inv_L_sq = inv_L * inv_L;
-    if (warp < nip) {
-        const double xi = E.xi[warp];
+    if (team < nip) {
+        const double xi = E.xi[team];
         const double eps0 = (-inv_L) * ul[0] + inv_L * ul[3];
         const double kappa = curv_shape(1, inv_L, inv_L_sq, xi) * ul[1] +
                              curv_shape(2, inv_L, inv_L_sq, xi) * ul[2] +
@@ -1031,11 +1132,10 @@ __global__ void __launch_bounds__(32 * kMaxIp) commit_kernel(
         gv.c2_blk = (int)fs.c2_n;
         gv.s2_blk = (int)fs.s2_n;
         gv.s1_blk = (int)fs.s1_n;
-        double r[5];
-        section_eval_warp(g, sd, gv, warp, eps0, kappa, lane, r);
-        if (lane == 0)
-            for (int c = 0; c < 5; ++c) resp[warp][c] = r[c];
+        section_eval_team<TEAM>(g, sd, gv, team, eps0, kappa, r, part[team]);
     }
+    __syncthreads();
+    if (team < nip && r == 0) section_finish(sd, part[team], resp[team]);
     __syncthreads();
     if (tid == 0) {
         double f[6] = {0, 0, 0, 0, 0, 0};

@@ -26,6 +26,9 @@
 namespace strut {
 
 constexpr int kMaxIp = 10;
+// Threads of an element CTA: one team of 128 (up to 5 integration points) or 64 (up to 10)
+// threads per integration point.
+constexpr int kTeamThreads = 640;
 constexpr int kEStride = 80;  // doubles of element state
 constexpr int kEq = 0, kEe = 3, kEk = 13, kEv = 23;
 // Section responses at the stored deformations (N, Mz and the 2x2 flexibility), valid flag.
@@ -67,6 +70,19 @@ struct DevInst {
     double alpha_m, beta_k, beta_k_init, beta_k_comm;
     double io_bytes;  // algorithmic HBM bytes of one Newton iteration of this instance
     long long dense_off;  // offset of this instance's n x n fallback scratch
+    int elem_off, n_elem; // this instance's elements (contiguous)
+    int pad_e0, pad_e1;
+};
+
+// Elements of the instances still iterating, rebuilt every Newton iteration and double
+// buffered on the parity of DevCtl::iter: the predictor lists every element of the live
+// instances into buffer 0, the instance kernel of iteration i lists the elements of an
+// instance that has not converged into buffer (i + 1) & 1, and the element kernel of
+// iteration i reads buffer i & 1 and clears the other one's count.  The order inside a list
+// does not matter: elements are independent.
+struct ElemList {
+    int* list[2];
+    int* count;  // 2 entries
 };
 
 // Step / iteration control on the device (read by the kernels, advanced by step_end_kernel).

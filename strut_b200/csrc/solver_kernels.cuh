@@ -11,8 +11,8 @@
 //                             2302-2356
 //   effective matrix          linear_solver_backend.mojo:1877-1983 (K + a1 C + a0 M)
 //   BandGeneral factor/solve  linear_solver_backend.mojo:631-680, 735-770 (unpivoted Doolittle;
-//                             the dense partial-pivot fallback of 175-240 is reported as
-//                             STRUT_UNSUPPORTED for now)
+//                             when a row swap would be needed, the dense partial-pivot LU of
+//                             175-240 on the assembled values, in global scratch)
 //   BandSPD factor/solve      linear_solver_backend.mojo:689-726, 772-812
 //   Newmark                   transient_nonlinear.mojo:496-648, 1052-1055
 //   tests                     nonlinear_convergence.mojo:8-20, transient_nonlinear.mojo:2798-2811
@@ -49,6 +49,7 @@ struct InstArrays {
     double* dense;        // per instance n x n scratch for the partial-pivot fallback
     int* piv;             // per free dof
     int* fallbacks;       // per instance count of dense fallbacks
+    ElemList el;          // elements of the instances still iterating
 };
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -76,74 +77,72 @@ __device__ __forceinline__ double block_max(double v, double* red) {
     return s;
 }
 
-// Right-looking band LU without pivoting on the n x (2bw+1) band in shared memory.  Step k
-// updates the trailing bw x bw block with multipliers a_ik / a_kk computed in place and writes
-// the multipliers of column k-1 (no longer read).  Returns 0 ok, 2 singular, 6 pivoting needed.
-__device__ int band_lu_smem(double* B, int n, int bw, int rw, int* flag) {
+// Right-looking band LU without pivoting (Doolittle, unit-lower multipliers stored in place)
+// on the n x (2bw+1) band in shared memory.  Step k computes the multiplier a_ik / a_kk of each
+// row below the pivot once (fac, at least bw entries), checks the column for a row swap, then
+// updates the trailing block one warp per row.  Every entry receives the same single update
+// per step as in the reference's row loop.  Returns 0 ok, 2 singular, 6 a row swap would be
+// needed (the caller then factors the assembled matrix densely with partial pivoting).
+__device__ int band_lu_smem(double* B, int n, int bw, int rw, double* fac) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     for (int k = 0; k < n; ++k) {
         const int m = min(bw, n - 1 - k);
-        // pivot check (linear_solver_backend.mojo:637-657), every thread reads the column
         const double akk = B[k * rw + bw];
-        double cmax = fabs(akk);
-        bool swap = false;
-        for (int i = k + 1; i <= k + m; ++i) {
-            const double c = fabs(B[i * rw + (k - i + bw)]);
-            if (c > cmax) {
-                cmax = c;
-                swap = true;
-            }
+        const double aabs = fabs(akk);
+        int swap = 0, big = 0;
+        for (int t = tid; t < m; t += nt) {
+            const int i = k + 1 + t;
+            const double v = B[i * rw + (k - i + bw)];
+            const double c = fabs(v);
+            swap |= (c > aabs) ? 1 : 0;
+            big |= (c > 1.0e-14) ? 1 : 0;
+            fac[t] = v / akk;
         }
-        if (cmax <= 1.0e-14) return 2;
-        if (swap) return 6;
-        if (fabs(akk) <= 1.0e-14) return 2;
-        // multipliers of the previous column
-        if (k > 0) {
-            const int mp = min(bw, n - k);  // rows k .. k-1+bw below pivot k-1
-            const double apk = B[(k - 1) * rw + bw];
-            for (int t = tid; t < mp; t += nt) {
-                const int i = k + t;
-                const int sl = i * rw + (k - 1 - i + bw);
-                B[sl] = B[sl] / apk;
+        // pivot search of linear_solver_backend.mojo:640-657: an entry strictly larger than
+        // the diagonal selects another row; the largest candidate decides singularity
+        if (__syncthreads_or(swap)) return __syncthreads_or(big) ? 6 : 2;
+        if (aabs <= 1.0e-14) return 2;
+        for (int r = warp; r < m; r += nw) {
+            const int i = k + 1 + r;
+            const double f = fac[r];
+            if (lane == 0) B[i * rw + (k - i + bw)] = f;
+            if (f == 0.0) continue;
+            const double* rowk = B + k * rw + (bw - k);
+            double* rowi = B + i * rw + (bw - i);
+            for (int c = lane; c < m; c += 32) {
+                const int j = k + 1 + c;
+                rowi[j] -= f * rowk[j];
             }
-        }
-        // trailing update (reads column k, row k, writes the block; multiplier slots of
-        // column k are rewritten only at step k+1)
-        for (int t = tid; t < m * m; t += nt) {
-            const int i = k + 1 + t / m;
-            const int j = k + 1 + t % m;
-            const double factor = B[i * rw + (k - i + bw)] / akk;
-            if (factor != 0.0) B[i * rw + (j - i + bw)] -= factor * B[k * rw + (j - k + bw)];
         }
         __syncthreads();
     }
-    (void)flag;
     return 0;
 }
 
-// Row-oriented band Cholesky (L L^T) on the lower band stored in general layout: right-looking
-// variant with the same arithmetic per entry as the row-oriented reference up to summation
-// order.  Returns 0 ok, 2 not positive definite.
-__device__ int band_chol_smem(double* B, int n, int bw, int rw) {
+// Right-looking band Cholesky (L L^T) on the lower band stored in general layout: column k of
+// L is computed once per step (fac), then the trailing lower block is updated one warp per row.
+// Same arithmetic per entry as the row-oriented reference up to summation order.  Returns 0
+// ok, 2 not positive definite.
+__device__ int band_chol_smem(double* B, int n, int bw, int rw, double* fac) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     for (int k = 0; k < n; ++k) {
         const int m = min(bw, n - 1 - k);
         const double dkk = B[k * rw + bw];
         if (!(dkk > 0.0)) return 2;
         const double lkk = sqrt(dkk);
-        // column k of L (rows k+1..k+m) and the trailing lower update
-        for (int t = tid; t < m * m; t += nt) {
-            const int i = k + 1 + t / m;
-            const int j = k + 1 + t % m;
-            if (j > i) continue;
-            const double lik = B[i * rw + (k - i + bw)] / lkk;
-            const double ljk = B[j * rw + (k - j + bw)] / lkk;
-            B[i * rw + (j - i + bw)] -= lik * ljk;
-        }
-        __syncthreads();
         for (int t = tid; t < m; t += nt) {
             const int i = k + 1 + t;
-            B[i * rw + (k - i + bw)] = B[i * rw + (k - i + bw)] / lkk;
+            fac[t] = B[i * rw + (k - i + bw)] / lkk;
+        }
+        __syncthreads();
+        for (int r = warp; r < m; r += nw) {
+            const int i = k + 1 + r;
+            const double li = fac[r];
+            if (lane == 0) B[i * rw + (k - i + bw)] = li;
+            double* rowi = B + i * rw + (bw - i);
+            for (int c = lane; c <= r; c += 32) rowi[k + 1 + c] -= li * fac[c];
         }
         if (tid == 0) B[k * rw + bw] = lkk;
         __syncthreads();
@@ -151,47 +150,64 @@ __device__ int band_chol_smem(double* B, int n, int bw, int rw) {
     return 0;
 }
 
-// Forward/back substitution with one warp (rows are sequential; each row's band dot product
-// is split over the lanes).
+// BandGeneral forward/back substitution with one warp (_solve_band_general,
+// linear_solver_backend.mojo:735-770).  Forward: column-oriented, so row i receives
+// rhs_i - L_i,j0 w_j0 - L_i,j0+1 w_j0+1 - ... in increasing j, the order of the reference's row
+// loop.  Back: lane 0 runs each row's sum in the reference's order.  w may not alias rhs.
 __device__ void band_solve_lu_warp(const double* B, int n, int bw, int rw, const double* rhs,
                                    double* w, double* x) {
     const int lane = threadIdx.x & 31;
-    for (int i = 0; i < n; ++i) {
-        double s = 0.0;
-        const int j0 = max(0, i - bw);
-        for (int j = j0 + lane; j < i; j += 32) s += B[i * rw + (j - i + bw)] * w[j];
-        s = warp_sum(s);
-        if (lane == 0) w[i] = rhs[i] - s;
+    for (int i = lane; i < n; i += 32) w[i] = rhs[i];
+    __syncwarp();
+    for (int j = 0; j < n; ++j) {
+        const double wj = w[j];
+        const int m = min(bw, n - 1 - j);
+        for (int t = lane; t < m; t += 32) {
+            const int i = j + 1 + t;
+            w[i] -= B[i * rw + (j - i + bw)] * wj;
+        }
         __syncwarp();
     }
-    for (int i = n - 1; i >= 0; --i) {
-        double s = 0.0;
-        const int j1 = min(n - 1, i + bw);
-        for (int j = i + 1 + lane; j <= j1; j += 32) s += B[i * rw + (j - i + bw)] * x[j];
-        s = warp_sum(s);
-        if (lane == 0) x[i] = (w[i] - s) / B[i * rw + bw];
-        __syncwarp();
+    if (lane == 0) {
+        for (int i = n - 1; i >= 0; --i) {
+            const double* rowi = B + i * rw + (bw - i);
+            double s = w[i];
+            const int j1 = min(n - 1, i + bw);
+            for (int j = i + 1; j <= j1; ++j) s -= rowi[j] * x[j];
+            x[i] = s / rowi[i];
+        }
     }
+    __syncwarp();
 }
 
+// BandSPD substitution with one warp (_solve_band_spd, linear_solver_backend.mojo:772-812):
+// both sweeps are column-oriented, which is the reference's own order for each entry.
 __device__ void band_solve_chol_warp(const double* B, int n, int bw, int rw, const double* rhs,
                                      double* w, double* x) {
     const int lane = threadIdx.x & 31;
-    for (int i = 0; i < n; ++i) {
-        double s = 0.0;
-        const int j0 = max(0, i - bw);
-        for (int j = j0 + lane; j < i; j += 32) s += B[i * rw + (j - i + bw)] * w[j];
-        s = warp_sum(s);
-        if (lane == 0) w[i] = (rhs[i] - s) / B[i * rw + bw];
+    for (int i = lane; i < n; i += 32) w[i] = rhs[i];
+    __syncwarp();
+    for (int j = 0; j < n; ++j) {
+        // w_j = (rhs_j - sum_{k<j} L_jk w_k) / L_jj, then push w_j into the rows below
+        if (lane == 0) w[j] = w[j] / B[j * rw + bw];
+        __syncwarp();
+        const double wj = w[j];
+        const int m = min(bw, n - 1 - j);
+        for (int t = lane; t < m; t += 32) {
+            const int i = j + 1 + t;
+            w[i] -= B[i * rw + (j - i + bw)] * wj;
+        }
         __syncwarp();
     }
-    // L^T x = w : x_i = (w_i - sum_{j>i} L_ji x_j) / L_ii
-    for (int i = n - 1; i >= 0; --i) {
-        double s = 0.0;
-        const int j1 = min(n - 1, i + bw);
-        for (int j = i + 1 + lane; j <= j1; j += 32) s += B[j * rw + (i - j + bw)] * x[j];
-        s = warp_sum(s);
-        if (lane == 0) x[i] = (w[i] - s) / B[i * rw + bw];
+    for (int i = lane; i < n; i += 32) x[i] = w[i];
+    __syncwarp();
+    // L^T x = w: x_row /= L_row,row, then x_col -= L_row,col x_row for the columns of that row
+    for (int row = n - 1; row >= 0; --row) {
+        if (lane == 0) x[row] = x[row] / B[row * rw + bw];
+        __syncwarp();
+        const double xr = x[row];
+        const int first = max(0, row - bw);
+        for (int col = first + lane; col < row; col += 32) x[col] -= B[row * rw + (col - row + bw)] * xr;
         __syncwarp();
     }
 }
@@ -323,7 +339,6 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     __shared__ DevInst I;
     __shared__ double red[32];
     __shared__ int red_r[32];
-    __shared__ int ctrl;
     const int inst = blockIdx.x;
     const int tid = threadIdx.x, nt = blockDim.x;
     {
@@ -361,39 +376,67 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             w[i] = an;
         }
         __syncthreads();
-        // rows: gather K (element order), C, effective band; residual
+        // K: every band slot gathers its element contributions in element order (one lane
+        // per slot, so the dependent index loads of many slots are in flight at once)
         const long long sp0 = I.slot_ptr_off;
         const double* Kinit = A.Kinit + I.band_off;
+        const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+        for (int i = warp; i < n; i += nw)
+            for (int o = lane; o < rw; o += 32) {
+                const int j = i + o - bw;
+                const int slot = i * rw + o;
+                Kb[slot] = (j < 0 || j >= n) ? 0.0 : gather_slot(A, sp0, slot);
+            }
+        __syncthreads();
         int bad_sym = 0;
+        if (I.spd) {
+            // BandSPD takes the lower triangle after checking symmetry to 1e-10
+            // (linear_solver_backend.mojo:266-271, 1936-1948)
+            for (int i = warp; i < n; i += nw)
+                for (int o = lane; o < bw; o += 32) {
+                    const int j = i + o - bw;
+                    if (j < 0) continue;
+                    const int slot = i * rw + o, mslot = j * rw + (i - j + bw);
+                    const double K = Kb[slot], Kt = Kb[mslot];
+                    if (fabs(K - Kt) > 1.0e-10) bad_sym = 1;
+                    if (I.has_damping && I.a1 != 0.0) {
+                        double C = I.alpha_m * 0.0, Ct = 0.0;
+                        if (I.beta_k != 0.0) {
+                            C += I.beta_k * K;
+                            Ct += I.beta_k * Kt;
+                        }
+                        if (I.beta_k_init != 0.0) {
+                            C += I.beta_k_init * Kinit[slot];
+                            Ct += I.beta_k_init * Kinit[mslot];
+                        }
+                        if (fabs(C - Ct) > 1.0e-10) bad_sym = 1;
+                    }
+                }
+        }
+        if (__syncthreads_or(bad_sym)) {
+            if (tid == 0) {
+                A.status[inst] = 4;
+                if (mode == INST_MODE_NEWTON && A.active[inst]) {
+                    A.active[inst] = 0;
+                    atomicSub(A.nactive, 1);
+                }
+            }
+            return;
+        }
+        // rows: C, effective band entries in place, C v in column order, residual
         for (int i = tid; i < n; i += nt) {
             double cv = 0.0;
             for (int o = 0; o < rw; ++o) {
                 const int j = i + o - bw;
+                if (j < 0 || j >= n) continue;
                 const int slot = i * rw + o;
-                if (j < 0 || j >= n) {
-                    Kb[slot] = 0.0;
-                    continue;
-                }
-                const double K = gather_slot(A, sp0, slot);
+                const double K = Kb[slot];
                 double C = 0.0;
                 if (I.has_damping) {
                     C = I.alpha_m * (i == j ? A.Mrff[f0 + i] : 0.0);
                     if (I.beta_k != 0.0) C += I.beta_k * K;
                     if (I.beta_k_init != 0.0) C += I.beta_k_init * Kinit[slot];
                     cv += C * vt[j];
-                }
-                if (I.spd && j < i) {
-                    // BandSPD takes the lower triangle after checking symmetry to 1e-10
-                    // (linear_solver_backend.mojo:266-271, 1936-1948)
-                    const int mslot = j * rw + (i - j + bw);
-                    const double Kt = gather_slot(A, sp0, mslot);
-                    if (fabs(K - Kt) > 1.0e-10) bad_sym = 1;
-                    if (I.has_damping && I.a1 != 0.0) {
-                        double Ct = 0.0;
-                        if (I.beta_k != 0.0) Ct += I.beta_k * Kt;
-                        if (I.beta_k_init != 0.0) Ct += I.beta_k_init * Kinit[mslot];
-                        if (fabs(C - Ct) > 1.0e-10) bad_sym = 1;
-                    }
                 }
                 double keff = K;
                 if (I.has_damping && I.a1 != 0.0) keff += I.a1 * C;
@@ -408,20 +451,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             A.R[f0 + i] = R[i];
             if (mode == INST_MODE_EXPORT) A.export_f[f0 + i] = F;
         }
-        if (tid == 0) ctrl = 0;
         __syncthreads();
-        if (bad_sym) ctrl = 1;
-        __syncthreads();
-        if (ctrl) {
-            if (tid == 0) {
-                A.status[inst] = 4;
-                if (mode == INST_MODE_NEWTON && A.active[inst]) {
-                    A.active[inst] = 0;
-                    atomicSub(A.nactive, 1);
-                }
-            }
-            return;
-        }
         if (mode == INST_MODE_EXPORT) {
             for (int t = tid; t < n * rw; t += nt) A.export_band[I.band_off + t] = Kb[t];
             return;
@@ -441,9 +471,9 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
         }
     }
     if (I.spd)
-        rc = band_chol_smem(Kb, n, bw, rw);
+        rc = band_chol_smem(Kb, n, bw, rw, fac);
     else
-        rc = band_lu_smem(Kb, n, bw, rw, nullptr);
+        rc = band_lu_smem(Kb, n, bw, rw, fac);
     bool dense = false;
     double* D = A.dense + I.dense_off;
     int* piv = A.piv + f0;
@@ -520,6 +550,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             A.status[inst] = 3;
             conv = true;
         }
+        int base = -1;
         if (conv) {
             A.active[inst] = 0;
             atomicSub(A.nactive, 1);
@@ -529,7 +560,17 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             A.active[inst] = 0;
             atomicSub(A.nactive, 1);
             if (hrow) hrow[inst] = A.iters[inst];
+        } else if (A.ctl) {
+            base = atomicAdd(&A.el.count[(A.ctl->iter + 1) & 1], I.n_elem);
         }
+        red_r[0] = base;
+    }
+    __syncthreads();
+    // still iterating: list this instance's elements for the next element kernel
+    const int base = red_r[0];
+    if (base >= 0) {
+        int* list = A.el.list[(A.ctl->iter + 1) & 1];
+        for (int k = tid; k < I.n_elem; k += nt) list[base + k] = I.elem_off + k;
     }
 }
 
@@ -551,7 +592,12 @@ __global__ void predictor_kernel(const DevInst* __restrict__ insts, InstArrays A
         const bool ok = A.status[gi] == 0;
         A.active[gi] = ok ? 1 : 0;
         A.iters[gi] = 0;
-        if (ok) atomicAdd(A.nactive, 1);
+        if (ok) {
+            atomicAdd(A.nactive, 1);
+            const DevInst& I = insts[gi];
+            const int base = atomicAdd(&A.el.count[0], I.n_elem);
+            for (int k = 0; k < I.n_elem; ++k) A.el.list[0][base + k] = I.elem_off + k;
+        }
     }
     if (gi >= n_free_total) return;
     const int inst = free_inst[gi];
@@ -614,7 +660,7 @@ __global__ void newton_check_kernel(DevCtl* ctl, const int* __restrict__ nactive
 // failing step).
 __global__ void step_end_kernel(DevCtl* ctl, const int* __restrict__ status,
                                 int* __restrict__ fail_step, int n_inst, int* nactive,
-                                cudaGraphConditionalHandle outer, int use_cond) {
+                                ElemList el, cudaGraphConditionalHandle outer, int use_cond) {
     const int step = ctl->step;
     for (int i = threadIdx.x; i < n_inst; i += blockDim.x)
         if (status[i] != 0 && fail_step[i] < 0) fail_step[i] = step;
@@ -622,6 +668,8 @@ __global__ void step_end_kernel(DevCtl* ctl, const int* __restrict__ status,
     if (threadIdx.x == 0) {
         ctl->step = step + 1;
         *nactive = 0;
+        el.count[0] = 0;
+        el.count[1] = 0;
         const bool stop = ctl->single && status[0] != 0;
         if (use_cond) cudaGraphSetConditional(outer, (step + 1 < ctl->n_end && !stop) ? 1 : 0);
     }

@@ -250,6 +250,7 @@ struct StrutHandle {
     int* d_rec_dof = nullptr;
     int* d_rece_base = nullptr;
     int* d_elem_err = nullptr;
+    int elem_grid = 1;  // resident element CTAs (persistent element kernel)
     unsigned long long* d_counters = nullptr;
     double* d_ag = nullptr;
     int ag_cap = 0;
@@ -303,13 +304,34 @@ static int prof_end(StrutHandle* h, int k) {
     return STRUT_OK;
 }
 
-static int launch_elements(StrutHandle* h) {
+// Element kernels: one team of 128 threads per integration point up to 5 points, else 64.
+using ElemKernel = decltype(&element_state_kernel<128>);
+using CommitKernel = decltype(&commit_kernel<128>);
+static ElemKernel elem_kernel_of(const StrutHandle* h) {
+    return h->max_nip <= 5 ? element_state_kernel<128> : element_state_kernel<64>;
+}
+static CommitKernel commit_kernel_of(const StrutHandle* h) {
+    return h->max_nip <= 5 ? commit_kernel<128> : commit_kernel<64>;
+}
+static dim3 elem_block(const StrutHandle* h) { return dim3((h->max_nip <= 5 ? 128 : 64) * h->max_nip); }
+
+// all_elems: every element (set-up and single-iteration entries); otherwise the list of
+// elements of the instances still iterating.
+static int launch_elements(StrutHandle* h, int all_elems = 0) {
+    if (h->prof) CK(cudaMemsetAsync(h->d_counters + 5, 0, sizeof(unsigned long long), h->stream));
     TRY(prof_begin(h));
-    element_state_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), h->elem_smem, h->stream>>>(
+    elem_kernel_of(h)<<<all_elems ? h->n_elem : h->elem_grid, elem_block(h), h->elem_smem, h->stream>>>(
         h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->d_ek, h->d_ef, h->A.active,
-        h->A.status, h->d_elem_err, h->d_counters);
+        h->A.status, h->d_elem_err, h->d_counters, h->A.el, (const DevCtl*)h->d_ctl, all_elems, h->n_elem);
     CK(cudaGetLastError());
     TRY(prof_end(h, 0));
+    if (h->prof) {
+        unsigned long long mx = 0;
+        CK(cudaMemcpy(&mx, h->d_counters + 5, sizeof(mx), cudaMemcpyDeviceToHost));
+        h->P.launches[5] += 1;
+        h->P.bytes[5] += (double)mx;
+        h->P.ms[5] = h->P.ms[0];
+    }
     return STRUT_OK;
 }
 
@@ -427,16 +449,17 @@ static int build_graph(StrutHandle* h) {
     cudaGraph_t ibody;
     TRY(add_while_node(&n_inner, body, &n_pred, 1, inner, &ibody));
     cudaGraphNode_t n_el, n_in, n_chk;
-    TRY(add_kernel_node(&n_el, ibody, nullptr, 0, element_state_kernel, dim3(h->n_elem),
-                        dim3(32 * std::max(h->max_nip, 2)), h->elem_smem, (const DevElem*)h->d_elems, h->geo,
+    TRY(add_kernel_node(&n_el, ibody, nullptr, 0, elem_kernel_of(h), dim3(h->elem_grid),
+                        elem_block(h), h->elem_smem, (const DevElem*)h->d_elems, h->geo,
                         h->fs, (const double*)h->A.u_full, h->d_estate, h->d_ek, h->d_ef,
-                        (const int*)h->A.active, h->A.status, h->d_elem_err, h->d_counters));
+                        (const int*)h->A.active, h->A.status, h->d_elem_err, h->d_counters, h->A.el,
+                        (const DevCtl*)h->d_ctl, 0, h->n_elem));
     TRY(add_kernel_node(&n_in, ibody, &n_el, 1, instance_newton_kernel, dim3(h->n_inst), dim3(256),
                         h->inst_smem, (const DevInst*)h->d_insts, A, (int)INST_MODE_NEWTON, 0));
     TRY(add_kernel_node(&n_chk, ibody, &n_in, 1, newton_check_kernel, dim3(1), dim3(32), 0, h->d_ctl,
                         (const int*)h->A.nactive, inner, 1));
-    TRY(add_kernel_node(&n_commit, body, &n_inner, 1, commit_kernel, dim3(h->n_elem),
-                        dim3(32 * std::max(h->max_nip, 2)), 0, (const DevElem*)h->d_elems, h->geo, h->fs,
+    TRY(add_kernel_node(&n_commit, body, &n_inner, 1, commit_kernel_of(h), dim3(h->n_elem),
+                        elem_block(h), 0, (const DevElem*)h->d_elems, h->geo, h->fs,
                         (const double*)h->A.u_full, h->d_estate, (const int*)h->A.status, h->d_hist_ef,
                         (const int*)h->d_rece_base, std::max(h->n_rece_slots, 1), (const DevCtl*)h->d_ctl));
     TRY(add_kernel_node(&n_post, body, &n_commit, 1, post_step_kernel, dim3((nF + tb - 1) / tb), dim3(tb), 0,
@@ -449,7 +472,7 @@ static int build_graph(StrutHandle* h) {
         last = n_rec;
     }
     TRY(add_kernel_node(&n_end, body, &last, 1, step_end_kernel, dim3(1), dim3(256), 0, h->d_ctl,
-                        (const int*)h->A.status, h->d_fail_step, h->n_inst, h->A.nactive, outer, 1));
+                        (const int*)h->A.status, h->d_fail_step, h->n_inst, h->A.nactive, h->A.el, outer, 1));
     CK(cudaGraphInstantiate(&h->gexec, g, 0));
     h->graph_keys[0] = h->d_hist_disp;
     h->graph_keys[1] = h->d_hist_ef;
@@ -677,6 +700,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         I.slot_ptr_off = band_off;
         I.dense_off = dense_off;
         dense_off += (long long)nf * nf;
+        I.elem_off = e0;
+        I.n_elem = d.num_elements;
         I.fint_ptr_off = f_off;
         I.max_iters = d.max_iters;
         I.test_type = d.test_type;
@@ -751,7 +776,15 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     if (h->elem_smem > 200 * 1024) return bail(fail(STRUT_UNSUPPORTED, "element fiber history exceeds shared memory"));
     h->elem_smem = std::max<size_t>(h->elem_smem, 16);
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    CK(cudaFuncSetAttribute(element_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->elem_smem));
+    CK(cudaFuncSetAttribute(elem_kernel_of(h), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->elem_smem));
+    {
+        int per_sm = 0, n_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, elem_kernel_of(h), (int)elem_block(h).x,
+                                                         h->elem_smem));
+        CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->device));
+        if (per_sm < 1) return bail(fail(STRUT_UNSUPPORTED, "element kernel does not fit on an SM"));
+        h->elem_grid = std::max(1, std::min(h->n_elem, per_sm * n_sm));
+    }
     CK(cudaFuncSetAttribute(instance_newton_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::max<size_t>(h->inst_smem, 16)));
     auto& al = h->allocs;
@@ -828,7 +861,9 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         (rc = dzeros(&A.export_f, nF, al)) || (rc = dzeros(&h->d_rhs, nF, al)) ||
         (rc = dzeros(&h->d_elem_err, (size_t)h->n_elem, al)) ||
         (rc = dzeros(&h->d_counters, 8, al)) || (rc = dzeros(&A.dense, (size_t)h->dense_total, al)) ||
-        (rc = dzeros(&A.piv, nF, al)) || (rc = dzeros(&A.fallbacks, (size_t)h->n_inst, al)))
+        (rc = dzeros(&A.piv, nF, al)) || (rc = dzeros(&A.fallbacks, (size_t)h->n_inst, al)) ||
+        (rc = dzeros(&A.el.list[0], (size_t)h->n_elem, al)) || (rc = dzeros(&A.el.list[1], (size_t)h->n_elem, al)) ||
+        (rc = dzeros(&A.el.count, 2, al)))
         return bail(rc);
     double* d_Mff;
     double* d_Mrff;
@@ -873,7 +908,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     {
         std::vector<int> ones(h->n_inst, 1);
         CK(cudaMemcpy(A.active, ones.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice));
-        if ((rc = launch_elements(h)) != STRUT_OK) return bail(rc);
+        if ((rc = launch_elements(h, 1)) != STRUT_OK) return bail(rc);
         // Kinit = K gathered in element order; the export path of the instance kernel with
         // a0 = a1 = 0 and no damping would equal K, but a dedicated gather keeps it exact.
         std::vector<DevInst> tmp = h->insts;
@@ -955,6 +990,7 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
         c.single = h->n_inst == 1;
         CK(cudaMemcpyAsync(h->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemsetAsync(h->A.nactive, 0, 4 * sizeof(int), h->stream));
+        CK(cudaMemsetAsync(h->A.el.count, 0, 2 * sizeof(int), h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
     if (n_steps > 0 && !h->prof) {
@@ -974,12 +1010,14 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             for (int it = 0; it < h->max_iters_global; ++it) {
                 TRY(launch_elements(h));
                 TRY(launch_instances(h, INST_MODE_NEWTON, step));
+                newton_check_kernel<<<1, 32, 0, h->stream>>>(h->d_ctl, h->A.nactive, none, 0);
+                CK(cudaGetLastError());
                 CK(cudaMemcpyAsync(h->h_ctrl, h->A.nactive, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
                 CK(cudaStreamSynchronize(h->stream));
                 if (h->h_ctrl[0] <= 0) break;
             }
             TRY(prof_begin(h));
-            commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
+            commit_kernel_of(h)<<<h->n_elem, elem_block(h), 0, h->stream>>>(
                 h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, h->d_hist_ef, h->d_rece_base,
                 std::max(h->n_rece_slots, 1), h->d_ctl);
             CK(cudaGetLastError());
@@ -995,7 +1033,7 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
                 CK(cudaGetLastError());
             }
             step_end_kernel<<<1, 256, 0, h->stream>>>(h->d_ctl, h->A.status, h->d_fail_step, h->n_inst,
-                                                      h->A.nactive, none, 0);
+                                                      h->A.nactive, h->A.el, none, 0);
             CK(cudaGetLastError());
             if (h->n_inst == 1) {
                 int s0 = 0;
@@ -1177,7 +1215,7 @@ int strut_gpu_state_determination(StrutHandle* h, const double* u_free, double* 
     std::vector<int> ones(h->n_inst, 1), zeros(h->n_inst, 0);
     CK(cudaMemcpyAsync(h->A.active, ones.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->A.status, zeros.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));
-    TRY(launch_elements(h));
+    TRY(launch_elements(h, 1));
     TRY(launch_instances(h, INST_MODE_EXPORT, -1));
     CK(cudaStreamSynchronize(h->stream));
     std::vector<int> st(h->n_inst);
@@ -1229,7 +1267,7 @@ int strut_gpu_factor_solve(StrutHandle* h, const double* rhs, double* du) {
 
 int strut_gpu_commit(StrutHandle* h) {
     if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
-    commit_kernel<<<h->n_elem, 32 * std::max(h->max_nip, 2), 0, h->stream>>>(
+    commit_kernel_of(h)<<<h->n_elem, elem_block(h), 0, h->stream>>>(
         h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, nullptr, h->d_rece_base, 1, h->d_ctl);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
