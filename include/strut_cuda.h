@@ -302,6 +302,48 @@ int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_
 int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double* out,
                                   int32_t* n_fibers);
 
+/* ---- learned Newton predictor: the per-node network ---------------------------------------
+ * No counterpart in the reference (Strut has no learned predictor).  A per-node MLP with
+ * n_in <= 32 features, two hidden layers of 128 GELU (tanh form) units and n_out <= 16
+ * outputs, run on the tensor cores (tcgen05, bf16 operands, fp32 accumulation) with fp32
+ * master parameters packed as W1 (n_in x 128, W[k][j] maps input k to output j), b1 (128),
+ * W2 (128 x 128), b2 (128), W3 (128 x n_out), b3 (n_out). */
+typedef struct StrutMlp StrutMlp;
+int strut_gpu_mlp_create(int32_t n_in, int32_t n_out, StrutMlp** out);
+int strut_gpu_mlp_destroy(StrutMlp* m);
+int32_t strut_gpu_mlp_param_count(const StrutMlp* m);
+int strut_gpu_mlp_set_params(StrutMlp* m, const float* params);
+int strut_gpu_mlp_get_params(const StrutMlp* m, float* params);
+/* y (n x n_out) = network(x (n x n_in)); host buffers. */
+int strut_gpu_mlp_forward(StrutMlp* m, const float* x, int32_t n, float* y);
+/* Mean squared error of the network on (x, t) and its gradient with respect to the packed
+ * parameters (the tensor-core backward pass; one batch of all n rows). */
+int strut_gpu_mlp_loss_grad(StrutMlp* m, const float* x, const float* t, int32_t n, float* loss,
+                            float* grads);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) on minibatches of `batch` rows, `epochs` passes over the n
+ * rows in a seeded random order; *loss_out = mean squared error over the last pass. */
+int strut_gpu_mlp_train(StrutMlp* m, const float* x, const float* t, int32_t n, int32_t epochs,
+                        int32_t batch, float lr, uint64_t seed, float* loss_out);
+
+/* ---- learned Newton predictor on an analysis ----------------------------------------------
+ * No counterpart in the reference.  Attaches a trained network (not owned; it must outlive the
+ * attachment) to every instance of the handle: each step, per node with a free dof, the features
+ * (converged increments of the node's dofs at the 4 previous steps, ground acceleration at this
+ * and the 15 previous steps, node height over frame height; x_norm = (x - x_mean) * x_scale,
+ * 4 ndf + 17 of them) give a correction to the step's Newmark predictor (network output *
+ * y_scale per dof), the learned guess being predictor + correction.  The first
+ * Newton iteration evaluates both that guess and the Newmark predictor and keeps the one with
+ * the smaller residual norm; the iterations then run to the same convergence test.  m = NULL
+ * detaches (the plain method). */
+int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, const float* x_scale,
+                            const float* y_scale);
+/* Number of predicted nodes (all instances), i.e. rows of strut_gpu_predictor_features. */
+int32_t strut_gpu_predictor_nodes(const StrutHandle* h);
+/* First iterations offered a learned guess, and how many kept it. */
+int strut_gpu_predictor_stats(const StrutHandle* h, int64_t* offered, int64_t* chosen);
+/* The normalised features of the next step, nodes x (4 ndf + 17) (tests). */
+int strut_gpu_predictor_features(StrutHandle* h, float* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,7 @@ TEST_NORM_UNBALANCE = 2
 TEST_ENERGY_INCR = 3
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 _ip = C.POINTER(C.c_int32)
 
 
@@ -233,4 +234,18 @@ EXPORTS = {
         C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
     ),
     "strut_gpu_section_batch_state": (C.c_int, [C.c_void_p, C.c_int32, _dp, _ip]),
+    "strut_gpu_mlp_create": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "strut_gpu_mlp_destroy": (C.c_int, [C.c_void_p]),
+    "strut_gpu_mlp_param_count": (C.c_int32, [C.c_void_p]),
+    "strut_gpu_mlp_set_params": (C.c_int, [C.c_void_p, _fp]),
+    "strut_gpu_mlp_get_params": (C.c_int, [C.c_void_p, _fp]),
+    "strut_gpu_mlp_forward": (C.c_int, [C.c_void_p, _fp, C.c_int32, _fp]),
+    "strut_gpu_mlp_loss_grad": (C.c_int, [C.c_void_p, _fp, _fp, C.c_int32, _fp, _fp]),
+    "strut_gpu_set_predictor": (C.c_int, [C.c_void_p, C.c_void_p, _fp, _fp, _fp]),
+    "strut_gpu_predictor_nodes": (C.c_int32, [C.c_void_p]),
+    "strut_gpu_predictor_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "strut_gpu_predictor_features": (C.c_int, [C.c_void_p, _fp]),
+    "strut_gpu_mlp_train": (
+        C.c_int, [C.c_void_p, _fp, _fp, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _fp]
+    ),
 }

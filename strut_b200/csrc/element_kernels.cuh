@@ -1,17 +1,16 @@
 // Fused element state determination for forceBeamColumn2d / dispBeamColumn2d on sm_100a.
 //
-// One CTA per element, one team of 128 threads (64 when an element has more than 5 points) per
-// integration point.  The element's committed fiber history (all of its sections, all
-// families) is staged into shared memory with cp.async.bulk (the TMA unit's bulk copy)
-// completing on an mbarrier; every section evaluation of the element-level flexibility
-// iteration then reads shared memory only.  Each thread computes the trial stress/tangent of
-// one or two fibers of its team's section in registers; the team reduces the section
-// resultants and tangent (N, Mz, k11, k12, k22) with shuffles and a fixed-order block sum.
-// The team leaders turn their section's tangent into its flexibility in parallel; thread 0 runs
-// the remaining element algebra (3x3 flexibility inverse, work-norm test, subdivision and
-// scheme fallbacks) and decisions are broadcast through shared memory so control stays uniform.
-// The per-iteration latency of one element is what bounds a batch whose slowest record keeps
-// failing its local iteration, so the work between barriers is kept short.
+// One CTA per element (a persistent grid claiming elements from a list).  The element's
+// committed fiber history (all of its sections, all families) is staged into shared memory with
+// cp.async.bulk (the TMA unit's bulk copy) completing on an mbarrier, and the constants each
+// fiber's trial rule derives from its committed state are computed once per launch.  Every
+// section evaluation of the element-level flexibility iteration then reads shared memory only,
+// in two phases: the trial stress and tangent of every fiber of every integration point (one
+// fiber per thread, Steel02 fibers on one warp per SM sub-partition), then the section sums in a
+// fixed chunked order.  Warp 0 runs the element algebra with one lane per integration point
+// (section flexibilities, 3x3 inverse, work-norm test); thread 0 runs the subdivision and scheme
+// fallbacks.  The per-iteration latency of one element is what bounds a batch whose slowest
+// record keeps failing its local iteration, so the work between barriers is kept short.
 //
 // Algorithm (paths relative to the Strut project root):
 //   src/mojo/elements/force_beam_column2d.mojo:223-272 (3x3 inverse), 608-801 (exact elastic,
@@ -90,8 +89,8 @@ struct ElemScratch {
     double vs_e[kMaxIp], vs_k[kMaxIp];    // element state section deformations
     double pt_e[kMaxIp], pt_k[kMaxIp];    // points to evaluate
     double resp[kMaxIp][5];
-    double part[kMaxIp][kVBlocks][6];     // per-block section partial sums
-    double n00[kMaxIp], n01[kMaxIp], n11[kMaxIp];  // flexibility of the last evaluation
+    double raw[kMaxIp][6];                // section sums of the last evaluation
+    double scr[32][12];                   // per-point terms of the element algebra (warp 0)
     double sub_e[kMaxIp], sub_k[kMaxIp], ssr_n[kMaxIp], ssr_m[kMaxIp];
     double fs00[kMaxIp], fs01[kMaxIp], fs11[kMaxIp];
     double best[10];
@@ -111,12 +110,75 @@ struct ElemScratch {
 // Family views of the element's committed history (shared memory, or global memory with the
 // family length as field stride).
 struct StageView {
-    const double* c2;  // 5 fields x c2_blk
-    const double* s2;  // 10 fields x s2_blk
-    const int* kon;    // s2_blk
-    const double* s1;  // 5 fields x s1_blk
+    const double* c2;   // 5 fields x c2_blk
+    const double* s2;   // 10 fields x s2_blk
+    const int* kon;     // s2_blk
+    const double* s1;   // 5 fields x s1_blk
+    const double* c2d;  // C2Derived, 5 fields x c2_blk (shared-memory views only)
+    const double* s2d;  // S2Derived, 12 fields x s2_blk (shared-memory views only)
     int c2_blk, s2_blk, s1_blk;
 };
+
+__device__ __forceinline__ void load_c2(const StageView& sv, int idx, C2State& c) {
+    const int B = sv.c2_blk;
+    c.eps = sv.c2[0 * B + idx];
+    c.sig = sv.c2[1 * B + idx];
+    c.tan = sv.c2[2 * B + idx];
+    c.ecmin = sv.c2[3 * B + idx];
+    c.dept = sv.c2[4 * B + idx];
+}
+
+__device__ __forceinline__ void load_s2(const StageView& sv, int idx, S2State& c) {
+    const int B = sv.s2_blk;
+    c.eps = sv.s2[0 * B + idx];
+    c.sig = sv.s2[1 * B + idx];
+    c.tan = sv.s2[2 * B + idx];
+    c.epsmin = sv.s2[3 * B + idx];
+    c.epsmax = sv.s2[4 * B + idx];
+    c.epspl = sv.s2[5 * B + idx];
+    c.epss0 = sv.s2[6 * B + idx];
+    c.sigs0 = sv.s2[7 * B + idx];
+    c.epsr = sv.s2[8 * B + idx];
+    c.sigr = sv.s2[9 * B + idx];
+    c.kon = sv.kon[idx];
+}
+
+// Derived constants of every Concrete02 / Steel02 fiber of the staged element, computed once
+// per launch by the whole CTA (the committed state does not change inside a launch).
+__device__ __forceinline__ void derive_element(const Geo& g, const DevSection& sd, const DevElem& E,
+                                               const StageView& sv, double* c2d, double* s2d) {
+    const int nc = E.nip * sd.n_c2, ns = E.nip * sd.n_s2;
+    for (int idx = threadIdx.x; idx < nc; idx += blockDim.x) {
+        C2State c;
+        load_c2(sv, idx, c);
+        const int j = idx % sd.n_c2;
+        C2Derived d;
+        concrete02_derive(g.mats[__ldg(g.m + sd.geo_off + sd.n_s2 + j)], c, d);
+        const int B = sv.c2_blk;
+        c2d[0 * B + idx] = d.sigmm;
+        c2d[1 * B + idx] = d.er;
+        c2d[2 * B + idx] = d.ept;
+        c2d[3 * B + idx] = d.epn;
+        c2d[4 * B + idx] = d.etn;
+    }
+    for (int idx = threadIdx.x; idx < ns; idx += blockDim.x) {
+        S2State c;
+        load_s2(sv, idx, c);
+        const int j = idx % sd.n_s2;
+        S2Derived d;
+        steel02_derive(g.mats[__ldg(g.m + sd.geo_off + j)], c, d);
+        const int B = sv.s2_blk;
+        const S2Curve* cv[2] = {&d.up, &d.dn};
+        for (int k = 0; k < 2; ++k) {
+            s2d[(6 * k + 0) * B + idx] = cv[k]->epsr;
+            s2d[(6 * k + 1) * B + idx] = cv[k]->sigr;
+            s2d[(6 * k + 2) * B + idx] = cv[k]->denom;
+            s2d[(6 * k + 3) * B + idx] = cv[k]->dsig;
+            s2d[(6 * k + 4) * B + idx] = cv[k]->R;
+            s2d[(6 * k + 5) * B + idx] = cv[k]->invR;
+        }
+    }
+}
 
 __device__ __forceinline__ void acc_fiber(double* a, double fs, double ks, double y) {
     a[0] += fs;
@@ -296,192 +358,396 @@ __device__ __forceinline__ void flex_accum(double* F, double wL, double bmi, dou
     F[8] += wL * bmj * f11 * bmj;
 }
 
-// Every team with team < nip evaluates its section at S.pt; the team leaders then finish the
-// sums into S.resp and, when flex is set, the section flexibility into S.n00/n01/n11
-// (fiber_section2d_batch_eval_same_def: singular if |det| <= 1e-40, reported in S.sing, which
-// the caller cleared before the preceding barrier).
-template <int TEAM>
-__device__ __forceinline__ void eval_points(const Geo& g, const DevSection& sd,
+// ---- two-phase evaluation of all integration points of an element ----------------------
+//
+// Phase 1 computes the trial stress and tangent (times area) of every fiber of every point at
+// S.pt into fo[(ip * n_tot + g) * 2 + {0, 1}] (g: the fiber's index in the section, families in
+// order Steel02 | Concrete02 | Steel01 | Elastic).  Steel02 fibers (two pow calls each) go to
+// the first warps (32 consecutive fibers per warp), the other families to the remaining warps,
+// again 32 consecutive fibers per warp so that the staged arrays are read without bank
+// conflicts and no warp mixes the two code paths.
+//
+// Phase 2 forms the section sums in a fixed order: every value of point ip is summed over eight
+// contiguous chunks of the section's fibers, each chunk sequentially by one thread (which
+// carries all six sums of its chunk), and the eight chunk sums are added by a fixed pairwise tree.  The order does not depend on the launch shape, so a
+// record's result never depends on the batch it runs in.  Raw sums: N, Mz, k11, k12 of the
+// non-elastic fibers, k22, k12 of the elastic fibers (fiber2d.mojo:1338-1351, 3459-3501).
+
+__device__ __forceinline__ int steel_warps(int n_items, int n_warps) {
+    if (n_items <= 0) return 0;
+    int ws = (n_items + 31) / 32;
+    if (ws > n_warps / 2) ws = n_warps / 2;
+    return ws < 1 ? 1 : ws;
+}
+
+__device__ __forceinline__ void fiber_phase(const Geo& g, const DevSection& sd,
                                             const StageView& sv, const DevElem& E,
-                                            ElemScratch& S, bool flex) {
-    const int team = threadIdx.x / TEAM, r = threadIdx.x % TEAM;
-    if (team < E.nip)
-        section_eval_team<TEAM>(g, sd, sv, team, S.pt_e[team], S.pt_k[team], r, S.part[team]);
-    __syncthreads();
-    if (r == 0 && team < E.nip) {
-        double* out = S.resp[team];
-        section_finish(sd, S.part[team], out);
-        if (flex) {
-            const double k11 = out[2], k12 = out[3], k22 = out[4];
-            const double det = k11 * k22 - k12 * k12;
-            if (fabs(det) <= 1.0e-40) {
-                S.sing = 1;
+                                            const double* pe, const double* pk, double* fo) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int nip = E.nip;
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_s = nip * sd.n_s2;
+    const int ws = steel_warps(n_s, nw);
+    if (w < ws) {
+        for (int i = w * 32 + lane; i < n_s; i += ws * 32) {
+            const int ip = i / sd.n_s2, j = i - ip * sd.n_s2;
+            const int idx = ip * sd.n_s2 + j;
+            S2State c;
+            load_s2(sv, idx, c);
+            const double y = __ldg(g.y + sd.geo_off + j), A = __ldg(g.a + sd.geo_off + j);
+            const DevMat& mat = g.mats[__ldg(g.m + sd.geo_off + j)];
+            const double eps = steel02_strain(mat, pe[ip] - y * pk[ip]);
+            const double deps = eps - c.eps;
+            double sig, tan;
+            if (steel02_no_change(c, deps)) {
+                tan = mat.p[1];
+                sig = mat.p[10];
             } else {
-                const double inv_det = 1.0 / det;
-                S.n00[team] = k22 * inv_det;
-                S.n01[team] = -k12 * inv_det;
-                S.n11[team] = k11 * inv_det;
+                const int B = sv.s2_blk, k = steel02_up(c, deps) ? 0 : 6;
+                S2Curve cv;
+                cv.epsr = sv.s2d[(k + 0) * B + idx];
+                cv.sigr = sv.s2d[(k + 1) * B + idx];
+                cv.denom = sv.s2d[(k + 2) * B + idx];
+                cv.dsig = sv.s2d[(k + 3) * B + idx];
+                cv.R = sv.s2d[(k + 4) * B + idx];
+                cv.invR = sv.s2d[(k + 5) * B + idx];
+                steel02_curve_eval(mat, cv, eps, sig, tan);
             }
+            double* o = fo + 2 * (ip * n_tot + j);
+            o[0] = sig * A;
+            o[1] = tan * A;
+        }
+        return;
+    }
+    const int n_o_sec = sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_o = nip * n_o_sec;
+    const int nwo = nw - ws;
+    for (int k = (w - ws) * 32 + lane; k < n_o; k += nwo * 32) {
+        const int ip = k / n_o_sec, jj = k - ip * n_o_sec;
+        const double e0 = pe[ip], ka = pk[ip];
+        const int gi = sd.n_s2 + jj;  // index in the section
+        const double y = __ldg(g.y + sd.geo_off + gi), A = __ldg(g.a + sd.geo_off + gi);
+        const DevMat& mat = g.mats[__ldg(g.m + sd.geo_off + gi)];
+        double* o = fo + 2 * (ip * n_tot + gi);
+        if (jj < sd.n_c2) {
+            const int idx = ip * sd.n_c2 + jj;
+            C2State c;
+            load_c2(sv, idx, c);
+            const int B = sv.c2_blk;
+            C2Derived d;
+            d.sigmm = sv.c2d[0 * B + idx];
+            d.er = sv.c2d[1 * B + idx];
+            d.ept = sv.c2d[2 * B + idx];
+            d.epn = sv.c2d[3 * B + idx];
+            d.etn = sv.c2d[4 * B + idx];
+            double sig, tan;
+            concrete02_sig_tan(mat, c, d, e0 - y * ka, sig, tan);
+            o[0] = sig * A;
+            o[1] = tan * A;
+        } else if (jj < sd.n_c2 + sd.n_s1) {
+            const int idx = ip * sd.n_s1 + (jj - sd.n_c2);
+            const int B = sv.s1_blk;
+            S1State c;
+            c.eps = sv.s1[0 * B + idx];
+            c.sig = sv.s1[1 * B + idx];
+            c.tan = sv.s1[2 * B + idx];
+            c.epsp = sv.s1[3 * B + idx];
+            c.alpha = sv.s1[4 * B + idx];
+            S1State t;
+            steel01_trial(mat, c, e0 - y * ka, t);
+            o[0] = t.sig * A;
+            o[1] = t.tan * A;
+        } else {
+            // elastic: ks = E A, fs = ks (eps0 - y kappa)
+            const double ks = mat.p[0] * A;
+            o[0] = ks * (e0 - y * ka);
+            o[1] = ks;
         }
     }
+}
+
+// Phase 2: thread t < nip * 8 sums chunk t % 8 of point t / 8 (the elastic fibers, last in the
+// section, in a loop of their own); the eight chunk threads of a point are consecutive lanes and
+// combine their sums by a fixed pairwise tree ((c0 + c1) + (c2 + c3)) + ((c4 + c5) + (c6 + c7)).
+__device__ __forceinline__ void sum_phase(const DevSection& sd, int nip, const double* ys,
+                                          const double* fo, double (*raw)[6]) {
+    const int t = threadIdx.x;
+    const int n_sum = nip * 8;
+    if ((t & ~31) >= n_sum) return;  // whole warp outside
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_nl = n_tot - sd.n_el;
+    const bool act = t < n_sum;
+    const int ip = t >> 3, b = t & 7;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
+    if (act) {
+        const int cs = (n_tot + 7) >> 3;
+        const int g0 = b * cs, g1 = min(g0 + cs, n_tot);
+        const double* f = fo + 2 * ip * n_tot;
+        const int gm = min(g1, n_nl);
+#pragma unroll 4
+        for (int gg = g0; gg < gm; ++gg) {
+            const double fs = f[2 * gg], ks = f[2 * gg + 1], y = ys[gg];
+            a0 += fs;
+            a1 += -fs * y;
+            a2 += ks;
+            a3 += -ks * y;
+            a4 += ks * y * y;
+        }
+        for (int gg = max(g0, n_nl); gg < g1; ++gg) {
+            const double fs = f[2 * gg], ks = f[2 * gg + 1], y = ys[gg];
+            a0 += fs;
+            a1 += -fs * y;
+            a2 += ks;
+            a5 += -ks * y;
+            a4 += ks * y * y;
+        }
+    }
+    double a[6] = {a0, a1, a2, a3, a4, a5};
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        double p = a[c];
+        p += __shfl_down_sync(0xffffffffu, p, 1);  // (c0+c1), (c2+c3), ...
+        p += __shfl_down_sync(0xffffffffu, p, 2);  // ((c0+c1)+(c2+c3)), ...
+        p += __shfl_down_sync(0xffffffffu, p, 4);
+        if (act && b == 0) raw[ip][c] = p;
+    }
+}
+
+// Both phases for every point of the element at S.pt; S.raw holds the sums afterwards.
+__device__ __forceinline__ void eval_sections(const Geo& g, const DevSection& sd, const StageView& sv,
+                                              const DevElem& E, ElemScratch& S, const double* ys,
+                                              double* fo) {
+    fiber_phase(g, sd, sv, E, S.pt_e, S.pt_k, fo);
+    __syncthreads();
+    sum_phase(sd, E.nip, ys, fo, S.raw);
     if (threadIdx.x == 0) S.section_evals += E.nip;
     __syncthreads();
 }
 
-// Next corrector points: s(q) - s_r mapped through the section flexibility (initial section
-// flexibility for scheme 1 and for the first iteration of scheme 2).  Thread 0 only.
-__device__ __forceinline__ void fbc_next_points(const DevSection& sd, const DevElem& E,
-                                                ElemScratch& S, bool use_init) {
-    for (int ip = 0; ip < E.nip; ++ip) {
-        const double xi = E.xi[ip];
-        const double bmi = xi - 1.0, bmj = xi;
-        const double ss0 = S.q[0] + 0.0;
-        const double ss1 = bmi * S.q[1] + bmj * S.q[2] + 0.0;
-        const double dss0 = ss0 - S.ssr_n[ip];
-        const double dss1 = ss1 - S.ssr_m[ip];
-        const double a00 = use_init ? sd.f00 : S.fs00[ip];
-        const double a01 = use_init ? sd.f01 : S.fs01[ip];
-        const double a11 = use_init ? sd.f11 : S.fs11[ip];
-        S.pt_e[ip] = S.sub_e[ip] + (a00 * dss0 + a01 * dss1);
-        S.pt_k[ip] = S.sub_k[ip] + (a01 * dss0 + a11 * dss1);
-    }
-    S.sing = 0;
+// Resultants and tangent of a point from its raw sums (uniform-modulus elastic k12 quirk of
+// fiber2d.mojo:3491-3499).
+__device__ __forceinline__ void raw_resp(const DevSection& sd, const double* raw, double& N,
+                                         double& M, double& k11, double& k12, double& k22) {
+    N = raw[0];
+    M = raw[1];
+    k11 = raw[2];
+    k12 = raw[3] + (sd.el_uniform ? 0.0 : raw[5]);
+    k22 = raw[4];
 }
 
-// _force_beam_column2d_try_increment, executed collectively.  Starting state: S.q, S.vs_*.
-// On success S.q / S.vs_* hold the converged state and S.best the result.
-template <int TEAM>
+// Section flexibility (fiber_section2d_batch_eval_same_def): false if |det| <= 1e-40.
+__device__ __forceinline__ bool sec_flex(double k11, double k12, double k22, double& f00,
+                                         double& f01, double& f11) {
+    const double det = k11 * k22 - k12 * k12;
+    if (fabs(det) <= 1.0e-40) return false;
+    const double inv_det = 1.0 / det;
+    f00 = k22 * inv_det;
+    f01 = -k12 * inv_det;
+    f11 = k11 * inv_det;
+    return true;
+}
+
+// Sums, over the lanes 0..nip-1 of warp 0 in lane order, the NV values each lane put in
+// scr[lane][0..NV-1]; every lane gets the same sums.  Warp 0 only.
+template <int NV>
+__device__ __forceinline__ void lane_ordered_sums(double (*scr)[12], int nip, double* out) {
+    __syncwarp();
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = 0.0;
+    for (int ip = 0; ip < nip; ++ip) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v] += scr[ip][v];
+    }
+    __syncwarp();
+}
+
+// Flexibility integration terms of one point (flex_accum's nine products); lane = point.
+__device__ __forceinline__ void flex_terms(double* o, double wL, double bmi, double bmj, double f00,
+                                           double f01, double f11) {
+    const double f10 = f01;
+    o[0] = wL * f00;
+    o[1] = wL * f01 * bmi;
+    o[2] = wL * f01 * bmj;
+    o[3] = wL * bmi * f10;
+    o[4] = wL * bmi * f11 * bmi;
+    o[5] = wL * bmi * f11 * bmj;
+    o[6] = wL * bmj * f10;
+    o[7] = wL * bmj * f11 * bmi;
+    o[8] = wL * bmj * f11 * bmj;
+}
+
+// _force_beam_column2d_try_increment (force_beam_column2d.mojo:804-1189), executed
+// collectively: every thread evaluates fibers, warp 0 runs the element algebra with one lane per
+// integration point.  Starting state: S.q, S.vs_*; on success S.q / S.vs_* hold the converged
+// state, S.best the result, and the section-response cache is refreshed.
 __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const StageView& sv,
                                   const DevElem& E, ElemScratch& S, const double* base,
-                                  const double* dv, int scheme) {
-    const int tid = threadIdx.x;
+                                  const double* dv, int scheme, const double* ys, double* fo) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    const bool w0 = tid < 32;
     const int nip = E.nip;
+    const bool act = w0 && lane < nip;
     if (!sd.init_valid) return false;
-    if (tid == 0) {
-        for (int ip = 0; ip < nip; ++ip) {
-            S.pt_e[ip] = S.vs_e[ip];
-            S.pt_k[ip] = S.vs_k[ip];
-        }
-        S.sing = 0;
-    }
-    __syncthreads();
-    const bool cached = S.c_valid != 0;
-    if (!cached) eval_points<TEAM>(g, sd, sv, E, S, true);
+    const double xi = act ? E.xi[lane] : 0.0, wL = act ? E.w[lane] * E.L : 0.0;
+    const double bmi = xi - 1.0, bmj = xi;
+    // per-point state, held by lane ip of warp 0
+    double sub_e = 0.0, sub_k = 0.0, ssr_n = 0.0, ssr_m = 0.0, f00 = 0.0, f01 = 0.0, f11 = 0.0;
+    double pe = 0.0, pk = 0.0;
+    double q0 = 0.0, q1 = 0.0, q2 = 0.0;
     const int num_iters = scheme == 1 ? 100 : 10;
-    if (tid == 0) {
-        int ok;
-        if (cached) {
-            for (int ip = 0; ip < nip; ++ip) {
-                S.resp[ip][0] = S.c_n[ip];
-                S.resp[ip][1] = S.c_m[ip];
-                S.fs00[ip] = S.c_f00[ip];
-                S.fs01[ip] = S.c_f01[ip];
-                S.fs11[ip] = S.c_f11[ip];
+    const bool cached = S.c_valid != 0;
+    if (w0) {
+        q0 = S.q[0];
+        q1 = S.q[1];
+        q2 = S.q[2];
+        if (act) {
+            sub_e = S.vs_e[lane];
+            sub_k = S.vs_k[lane];
+            if (!cached) {
+                S.pt_e[lane] = sub_e;
+                S.pt_k[lane] = sub_k;
             }
-            ok = 1;
+        }
+    }
+    if (!cached) {
+        __syncthreads();
+        eval_sections(g, sd, sv, E, S, ys, fo);
+    }
+    // the next points: s(q) - s_r through the section flexibility (initial flexibility for
+    // scheme 1 and for the first iteration of scheme 2)
+    auto next_points = [&](bool use_init) {
+        const double ss0 = q0 + 0.0;
+        const double ss1 = bmi * q1 + bmj * q2 + 0.0;
+        const double dss0 = ss0 - ssr_n;
+        const double dss1 = ss1 - ssr_m;
+        const double a00 = use_init ? sd.f00 : f00;
+        const double a01 = use_init ? sd.f01 : f01;
+        const double a11 = use_init ? sd.f11 : f11;
+        pe = sub_e + (a00 * dss0 + a01 * dss1);
+        pk = sub_k + (a01 * dss0 + a11 * dss1);
+        if (act) {
+            S.pt_e[lane] = pe;
+            S.pt_k[lane] = pk;
+        }
+    };
+    if (w0) {
+        int ok = 1;
+        if (cached) {
+            if (act) {
+                ssr_n = S.c_n[lane];
+                ssr_m = S.c_m[lane];
+                f00 = S.c_f00[lane];
+                f01 = S.c_f01[lane];
+                f11 = S.c_f11[lane];
+            }
         } else {
-            ok = S.sing ? 0 : 1;
-            if (ok)
-                for (int ip = 0; ip < nip; ++ip) {
-                    S.fs00[ip] = S.n00[ip];
-                    S.fs01[ip] = S.n01[ip];
-                    S.fs11[ip] = S.n11[ip];
-                }
+            bool good = true;
+            if (act) {
+                double k11, k12, k22;
+                raw_resp(sd, S.raw[lane], ssr_n, ssr_m, k11, k12, k22);
+                good = sec_flex(k11, k12, k22, f00, f01, f11);
+            }
+            ok = __all_sync(0xffffffffu, good) ? 1 : 0;
         }
         if (ok) {
-            double P[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            for (int ip = 0; ip < nip; ++ip) {
-                S.ssr_n[ip] = S.resp[ip][0];
-                S.ssr_m[ip] = S.resp[ip][1];
-                S.sub_e[ip] = S.vs_e[ip];
-                S.sub_k[ip] = S.vs_k[ip];
-                const double xi = E.xi[ip], wL = E.w[ip] * E.L;
-                flex_accum(P, wL, xi - 1.0, xi, S.fs00[ip], S.fs01[ip], S.fs11[ip]);
+            if (act) flex_terms(S.scr[lane], wL, bmi, bmj, f00, f01, f11);
+            double P[9], pk9[9];
+            lane_ordered_sums<9>(S.scr, nip, P);
+            if (invert3(P, pk9)) {
+                q0 += (pk9[0] * dv[0] + pk9[1] * dv[1] + pk9[2] * dv[2]);
+                q1 += (pk9[3] * dv[0] + pk9[4] * dv[1] + pk9[5] * dv[2]);
+                q2 += (pk9[6] * dv[0] + pk9[7] * dv[1] + pk9[8] * dv[2]);
             }
-            double pk[9];
-            if (invert3(P, pk)) {
-                S.q[0] += (pk[0] * dv[0] + pk[1] * dv[1] + pk[2] * dv[2]);
-                S.q[1] += (pk[3] * dv[0] + pk[4] * dv[1] + pk[5] * dv[2]);
-                S.q[2] += (pk[6] * dv[0] + pk[7] * dv[1] + pk[8] * dv[2]);
-            }
-            // points of the first corrector iteration
-            fbc_next_points(sd, E, S, scheme == 1 || scheme == 2);
+            next_points(scheme == 1 || scheme == 2);
         }
-        S.flag = ok;
+        if (lane == 0) S.flag = ok;
     }
     __syncthreads();
     if (!S.flag) return false;
+    const double t0 = base[0] + dv[0], t1 = base[1] + dv[1], t2 = base[2] + dv[2];
     for (int it = 0; it < num_iters; ++it) {
-        eval_points<TEAM>(g, sd, sv, E, S, true);
-        if (tid == 0) {
-            S.local_iters++;
+        eval_sections(g, sd, sv, E, S, ys, fo);
+        if (w0) {
+            bool good = true;
+            double N = 0.0, M = 0.0, n00 = 0.0, n01 = 0.0, n11 = 0.0;
+            if (act) {
+                double k11, k12, k22;
+                raw_resp(sd, S.raw[lane], N, M, k11, k12, k22);
+                good = sec_flex(k11, k12, k22, n00, n01, n11);
+            }
             int res = 0;
-            if (!S.sing) {
-                double F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-                double vr0 = 0.0, vr1 = 0.0, vr2 = 0.0;
-                for (int ip = 0; ip < nip; ++ip) {
-                    const double xi = E.xi[ip], wL = E.w[ip] * E.L;
-                    const double bmi = xi - 1.0, bmj = xi;
-                    const double ss0 = S.q[0] + 0.0;
-                    const double ss1 = bmi * S.q[1] + bmj * S.q[2] + 0.0;
-                    const double n00 = S.n00[ip], n01 = S.n01[ip], n11 = S.n11[ip];
-                    S.sub_e[ip] = S.pt_e[ip];
-                    S.sub_k[ip] = S.pt_k[ip];
-                    S.ssr_n[ip] = S.resp[ip][0];
-                    S.ssr_m[ip] = S.resp[ip][1];
-                    S.fs00[ip] = n00;
-                    S.fs01[ip] = n01;
-                    S.fs11[ip] = n11;
-                    const double dr0 = ss0 - S.ssr_n[ip];
-                    const double dr1 = ss1 - S.ssr_m[ip];
-                    const double dvr0 = n00 * dr0 + n01 * dr1;
-                    const double dvr1 = n01 * dr0 + n11 * dr1;
-                    flex_accum(F, wL, bmi, bmj, n00, n01, n11);
-                    vr0 += wL * (S.pt_e[ip] + dvr0);
-                    vr1 += wL * bmi * (S.pt_k[ip] + dvr1);
-                    vr2 += wL * bmj * (S.pt_k[ip] + dvr1);
+            if (__all_sync(0xffffffffu, good)) {
+                const double ss0 = q0 + 0.0;
+                const double ss1 = bmi * q1 + bmj * q2 + 0.0;
+                sub_e = pe;
+                sub_k = pk;
+                ssr_n = N;
+                ssr_m = M;
+                f00 = n00;
+                f01 = n01;
+                f11 = n11;
+                const double dr0 = ss0 - ssr_n;
+                const double dr1 = ss1 - ssr_m;
+                const double dvr0 = n00 * dr0 + n01 * dr1;
+                const double dvr1 = n01 * dr0 + n11 * dr1;
+                if (act) {
+                    flex_terms(S.scr[lane], wL, bmi, bmj, n00, n01, n11);
+                    S.scr[lane][9] = wL * (pe + dvr0);
+                    S.scr[lane][10] = wL * bmi * (pk + dvr1);
+                    S.scr[lane][11] = wL * bmj * (pk + dvr1);
                 }
-                double k[9];
+                double F[12], k[9];
+                lane_ordered_sums<12>(S.scr, nip, F);
                 if (invert3(F, k)) {
-                    const double r0 = (base[0] + dv[0]) - vr0;
-                    const double r1 = (base[1] + dv[1]) - vr1;
-                    const double r2 = (base[2] + dv[2]) - vr2;
+                    const double r0 = t0 - F[9];
+                    const double r1 = t1 - F[10];
+                    const double r2 = t2 - F[11];
                     const double dq0 = k[0] * r0 + k[1] * r1 + k[2] * r2;
                     const double dq1 = k[3] * r0 + k[4] * r1 + k[5] * r2;
                     const double dq2 = k[6] * r0 + k[7] * r1 + k[8] * r2;
                     const double work = fabs(r0 * dq0 + r1 * dq1 + r2 * dq2);
-                    S.q[0] += dq0;
-                    S.q[1] += dq1;
-                    S.q[2] += dq2;
+                    q0 += dq0;
+                    q1 += dq1;
+                    q2 += dq2;
                     res = 1;
                     if (work < 1.0e-12) {
                         res = 2;
-                        for (int ip = 0; ip < nip; ++ip) {
-                            S.vs_e[ip] = S.sub_e[ip];
-                            S.vs_k[ip] = S.sub_k[ip];
-                            S.c_n[ip] = S.ssr_n[ip];
-                            S.c_m[ip] = S.ssr_m[ip];
-                            S.c_f00[ip] = S.fs00[ip];
-                            S.c_f01[ip] = S.fs01[ip];
-                            S.c_f11[ip] = S.fs11[ip];
+                        if (act) {
+                            S.vs_e[lane] = sub_e;
+                            S.vs_k[lane] = sub_k;
+                            S.c_n[lane] = ssr_n;
+                            S.c_m[lane] = ssr_m;
+                            S.c_f00[lane] = f00;
+                            S.c_f01[lane] = f01;
+                            S.c_f11[lane] = f11;
                         }
-                        S.c_valid = 1;
-                        S.best[0] = S.q[0];
-                        S.best[1] = S.q[1];
-                        S.best[2] = S.q[2];
-                        S.best[3] = k[0];
-                        S.best[4] = k[1];
-                        S.best[5] = k[2];
-                        S.best[6] = k[3];
-                        S.best[7] = k[4];
-                        S.best[8] = k[5];
-                        S.best[9] = k[8];
+                        if (lane == 0) {
+                            S.c_valid = 1;
+                            S.best[0] = q0;
+                            S.best[1] = q1;
+                            S.best[2] = q2;
+                            S.best[3] = k[0];
+                            S.best[4] = k[1];
+                            S.best[5] = k[2];
+                            S.best[6] = k[3];
+                            S.best[7] = k[4];
+                            S.best[8] = k[5];
+                            S.best[9] = k[8];
+                        }
                     } else if (it + 1 < num_iters) {
-                        fbc_next_points(sd, E, S, scheme == 1);
+                        next_points(scheme == 1);
                     }
                 }
             }
-            S.flag = res;
+            if (lane == 0) {
+                S.local_iters++;
+                S.flag = res;
+                if (res) {
+                    S.q[0] = q0;
+                    S.q[1] = q1;
+                    S.q[2] = q2;
+                }
+            }
         }
         __syncthreads();
         const int f = S.flag;
@@ -584,6 +850,9 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
     sv.s2 = s2;
     sv.s1 = s1;
     sv.kon = kon;
+    // derived constants follow the staged history (kon occupies s2_blk ints, s2_blk % 4 == 0)
+    sv.c2d = reinterpret_cast<const double*>(kon + E.s2_blk);
+    sv.s2d = sv.c2d + 5 * E.c2_blk;
     sv.c2_blk = E.c2_blk;
     sv.s2_blk = E.s2_blk;
     sv.s1_blk = E.s1_blk;
@@ -616,12 +885,12 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
 }
 
 // State determination of every element of the active instances: k (6x6 global), f (6) and the
-// element state.  One CTA per element, one TEAM-thread team per integration point.
+// element state.  One CTA of kTeamThreads threads per element at a time.
 //
-// Persistent: the grid is sized to the resident CTAs of the device and each CTA walks the list
-// of elements of the instances still iterating (all elements when all_elems is set), so a
-// Newton iteration of a few slow records launches no idle CTAs.
-template <int TEAM>
+// Persistent: the grid is sized to the resident CTAs of the device and each CTA claims elements
+// from the list of the instances still iterating (all elements when all_elems is set), so a
+// Newton iteration of a few slow records launches no idle CTAs and a slow element does not hold
+// up elements queued behind it on the same CTA.
 __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
     double* __restrict__ estate, double* __restrict__ ek, double* __restrict__ ef,
@@ -638,8 +907,12 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         mbar_init(&bar, 1);
         mbar_fence_init();
     }
+    __shared__ int s_next;
     const int cur = all_elems ? 0 : (ctl->iter & 1);
-    if (!all_elems && blockIdx.x == 0 && tid == 0) el.count[cur ^ 1] = 0;
+    if (!all_elems && blockIdx.x == 0 && tid == 0) {
+        el.count[cur ^ 1] = 0;
+        el.next[cur ^ 1] = 0;
+    }
     const int total = all_elems ? n_elem : el.count[cur];
     __syncthreads();
     uint32_t phase = 0;
@@ -687,27 +960,35 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         stop = true;
         return;
     }
+    derive_element(g, sd, E, sv, const_cast<double*>(sv.c2d), const_cast<double*>(sv.s2d));
+    // the section's fiber y (phase-2 sums) and the per-fiber results of phase 1 follow
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    double* ys = const_cast<double*>(sv.s2d) + 12 * E.s2_blk;
+    double* fo = ys + ((n_tot + 1) & ~1);
+    for (int gg = tid; gg < n_tot; gg += blockDim.x) ys[gg] = __ldg(g.y + sd.geo_off + gg);
+    __syncthreads();
     const int nip = E.nip;
     if (E.type == 3) {
         // ---------------- dispBeamColumn2d ----------------
-        const int team = tid / TEAM, r = tid % TEAM;
         const double L = E.L, inv_L = 1.0 / L, inv_L_sq = inv_L * inv_L;
-        double eps0 = 0.0, kappa = 0.0;
-        if (team < nip) {
-            const double xi = E.xi[team];
+        if (tid < nip) {
+            const double xi = E.xi[tid];
             const double b1 = curv_shape(1, inv_L, inv_L_sq, xi);
             const double b2 = curv_shape(2, inv_L, inv_L_sq, xi);
             const double b4 = curv_shape(4, inv_L, inv_L_sq, xi);
             const double b5 = curv_shape(5, inv_L, inv_L_sq, xi);
-            eps0 = (-inv_L) * S.ul[0] + inv_L * S.ul[3];
-            kappa = b1 * S.ul[1] + b2 * S.ul[2] + b4 * S.ul[4] + b5 * S.ul[5];
-            section_eval_team<TEAM>(g, sd, sv, team, eps0, kappa, r, S.part[team]);
+            const double eps0 = (-inv_L) * S.ul[0] + inv_L * S.ul[3];
+            const double kappa = b1 * S.ul[1] + b2 * S.ul[2] + b4 * S.ul[4] + b5 * S.ul[5];
+            S.pt_e[tid] = eps0;
+            S.pt_k[tid] = kappa;
+            S.vs_e[tid] = eps0;
+            S.vs_k[tid] = kappa;
         }
         __syncthreads();
-        if (team < nip && r == 0) {
-            section_finish(sd, S.part[team], S.resp[team]);
-            S.vs_e[team] = eps0;
-            S.vs_k[team] = kappa;
+        eval_sections(g, sd, sv, E, S, ys, fo);
+        if (tid < nip) {
+            double* r = S.resp[tid];
+            raw_resp(sd, S.raw[tid], r[0], r[1], r[2], r[3], r[4]);
         }
         __syncthreads();
         if (tid < 36) {
@@ -851,7 +1132,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
                     }
                 }
                 __syncthreads();
-                if (!fbc_try_increment<TEAM>(g, sd, sv, E, S, S.acc_v, S.zero3, scheme)) continue;
+                if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.zero3, scheme, ys, fo)) continue;
                 if (tid == 0) S.best_ok = 1;
                 converged = 1;
                 break;
@@ -874,7 +1155,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
                         }
                     }
                     __syncthreads();
-                    if (!fbc_try_increment<TEAM>(g, sd, sv, E, S, S.acc_v, S.att, scheme)) continue;
+                    if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme, ys, fo)) continue;
                     if (tid == 0) {
                         for (int i = 0; i < 3; ++i) {
                             S.acc_v[i] = S.tv[i];
@@ -1006,8 +1287,16 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     if (tid < 36) ek[(size_t)e * 36 + tid] = S.k[tid];
     else if (tid < 42) ef[(size_t)e * 6 + tid - 36] = S.f[tid - 36];
     };
-    for (int li = blockIdx.x; li < total && !stop; li += gridDim.x) {
+    // first element by block index, then dynamically: thread 0 claims the next list entry while
+    // the CTA works on the current one (the claim's latency hides behind the element)
+    int li = blockIdx.x;
+    while (li < total && !stop) {
+        int claimed = li + gridDim.x;
+        if (!all_elems && tid == 0) claimed = atomicAdd(&el.next[cur], 1) + gridDim.x;
         process(all_elems ? li : el.list[cur][li]);
+        if (tid == 0) s_next = claimed;
+        __syncthreads();
+        li = s_next;
         __syncthreads();
     }
 }

@@ -89,10 +89,60 @@ __device__ __forceinline__ void c2_tens_envlp(const DevMat& m, double strain, do
     }
 }
 
+// Constants of a Concrete02 fiber that depend on its committed state only: every trial from
+// that state evaluates them with these same expressions (fiber2d.mojo:1190-1244), so an
+// element evaluating many trial strains against one committed state computes them once.
+struct C2Derived {
+    double sigmm;  // compression envelope stress at ecmin
+    double er;     // unloading modulus
+    double ept;    // strain at zero stress on the unloading branch
+    double epn;    // ept + dept: end of the tension reloading branch
+    double etn;    // tension reloading modulus
+};
+
+__device__ __forceinline__ void concrete02_derive(const DevMat& m, const C2State& c, C2Derived& d) {
+    double tmm;
+    c2_compr_envlp(m, c.ecmin, d.sigmm, tmm);
+    d.er = (d.sigmm - m.k[C2K_SIGMR]) / (c.ecmin - m.k[C2K_EPSR]);
+    d.ept = c.ecmin - d.sigmm / d.er;
+    d.epn = d.ept + c.dept;
+    double sicn, tcn;
+    c2_tens_envlp(m, c.dept, sicn, tcn);
+    d.etn = m.k[C2K_EC0];
+    if (c.dept != 0.0) d.etn = sicn / c.dept;
+}
+
+// Stress and tangent for strain >= ecmin (unloading / reloading / tension branches).
+__device__ __forceinline__ void concrete02_unload(const DevMat& m, const C2State& c,
+                                                  const C2Derived& d, double strain, double deps,
+                                                  double& sig, double& tan) {
+    const double Ec0 = m.k[C2K_EC0];
+    if (strain <= d.ept) {
+        const double sigmin = d.sigmm + d.er * (strain - c.ecmin);
+        const double sigmax = 0.5 * d.er * (strain - d.ept);
+        double s = c.sig + Ec0 * deps;
+        double e = Ec0;
+        if (s <= sigmin) {
+            s = sigmin;
+            e = d.er;
+        }
+        if (s >= sigmax) {
+            s = sigmax;
+            e = 0.5 * d.er;
+        }
+        sig = s;
+        tan = e;
+    } else if (strain <= d.epn) {
+        tan = d.etn;
+        sig = d.etn * (strain - d.ept);
+    } else {
+        c2_tens_envlp(m, strain - d.ept, sig, tan);
+    }
+}
+
 // Concrete02 trial from committed c at strain -> t.
 __device__ __forceinline__ void concrete02_trial(const DevMat& m, const C2State& c,
                                                  double strain, C2State& t) {
-    const double Ec0 = m.k[C2K_EC0];
     t.ecmin = c.ecmin;
     t.dept = c.dept;
     t.eps = strain;
@@ -107,71 +157,56 @@ __device__ __forceinline__ void concrete02_trial(const DevMat& m, const C2State&
         t.ecmin = strain;
         return;
     }
-    double sigmm, tmm;
-    c2_compr_envlp(m, c.ecmin, sigmm, tmm);
-    const double er = (sigmm - m.k[C2K_SIGMR]) / (c.ecmin - m.k[C2K_EPSR]);
-    const double ept = c.ecmin - sigmm / er;
-    if (strain <= ept) {
-        const double sigmin = sigmm + er * (strain - c.ecmin);
-        const double sigmax = 0.5 * er * (strain - ept);
-        double s = c.sig + Ec0 * deps;
-        double e = Ec0;
-        if (s <= sigmin) {
-            s = sigmin;
-            e = er;
-        }
-        if (s >= sigmax) {
-            s = sigmax;
-            e = 0.5 * er;
-        }
-        t.sig = s;
-        t.tan = e;
-        return;
-    }
-    const double epn = ept + c.dept;
-    if (strain <= epn) {
-        double sicn, tcn;
-        c2_tens_envlp(m, c.dept, sicn, tcn);
-        double e = Ec0;
-        if (c.dept != 0.0) e = sicn / c.dept;
-        t.tan = e;
-        t.sig = e * (strain - ept);
-    } else {
-        c2_tens_envlp(m, strain - ept, t.sig, t.tan);
-        t.dept = strain - ept;
-    }
+    C2Derived d;
+    concrete02_derive(m, c, d);
+    concrete02_unload(m, c, d, strain, deps, t.sig, t.tan);
+    if (strain > d.epn) t.dept = strain - d.ept;
 }
 
-// Steel02 (Giuffre-Menegotto-Pinto with isotropic shift) trial from committed c.
-__device__ __forceinline__ void steel02_trial(const DevMat& m, const S2State& c,
-                                              double trial_eps, S2State& t) {
-    const double Fy = m.p[0], E0 = m.p[1], b = m.p[2], R0 = m.p[3], cR1 = m.p[4];
-    const double cR2 = m.p[5], a1 = m.p[6], a3 = m.p[8], sigini = m.p[10];
+// Stress and tangent of concrete02_trial, given the committed state's derived constants.
+__device__ __forceinline__ void concrete02_sig_tan(const DevMat& m, const C2State& c,
+                                                   const C2Derived& d, double strain,
+                                                   double& sig, double& tan) {
+    const double deps = strain - c.eps;
+    if (fabs(deps) < 2.220446049250313e-16) {
+        sig = c.sig;
+        tan = c.tan;
+        return;
+    }
+    if (strain < c.ecmin) {
+        c2_compr_envlp(m, strain, sig, tan);
+        return;
+    }
+    concrete02_unload(m, c, d, strain, deps, sig, tan);
+}
+
+// Steel02: given the committed state, the loading branch a trial follows depends only on the
+// sign of the strain increment (first loading from kon 0/3, continued loading, or a reversal
+// with the isotropic shift), so both possible branches can be formed once per committed state.
+struct S2Curve {
+    double epsr, sigr;
+    double denom;  // epss0 - epsr
+    double dsig;   // sigs0 - sigr
+    double R, invR;
+};
+struct S2Derived {
+    S2Curve up, dn;  // strain increasing / decreasing
+};
+
+// Branch state after an increment in direction `up` (fiber2d.mojo:1103-1187): everything of
+// the trial state except eps, sig and tan.  Call only when the no-change test failed.
+__device__ __forceinline__ void steel02_branch(const DevMat& m, const S2State& c, bool up,
+                                               S2State& t) {
+    const double Fy = m.p[0], E0 = m.p[1];
+    const double a1 = m.p[6], a3 = m.p[8];
     const double Esh = m.k[S2K_ESH], epsy = m.k[S2K_EPSY];
-    double eps = trial_eps;
-    if (sigini != 0.0) eps += m.k[S2K_SIGINI_E0];
-    t.eps = eps;
-    const double deps = eps - c.eps;
     double epsmax = c.epsmax, epsmin = c.epsmin, epspl = c.epspl, epss0 = c.epss0;
     double sigs0 = c.sigs0, epsr = c.epsr, sigr = c.sigr;
     int kon = c.kon;
     if (kon == 0 || kon == 3) {
-        if (fabs(deps) < 2.220446049250313e-15) {
-            t.tan = E0;
-            t.sig = sigini;
-            t.kon = 3;
-            t.epsmin = epsmin;
-            t.epsmax = epsmax;
-            t.epspl = epspl;
-            t.epss0 = epss0;
-            t.sigs0 = sigs0;
-            t.epsr = epsr;
-            t.sigr = sigr;
-            return;
-        }
         epsmax = epsy;
         epsmin = -epsy;
-        if (deps < 0.0) {
+        if (!up) {
             kon = 2;
             epss0 = epsmin;
             sigs0 = -Fy;
@@ -183,7 +218,7 @@ __device__ __forceinline__ void steel02_trial(const DevMat& m, const S2State& c,
             epspl = epsmax;
         }
     }
-    if (kon == 2 && deps > 0.0) {
+    if (kon == 2 && up) {
         kon = 1;
         epsr = c.eps;
         sigr = c.sig;
@@ -193,7 +228,7 @@ __device__ __forceinline__ void steel02_trial(const DevMat& m, const S2State& c,
         epss0 = (Fy * shft - m.k[S2K_ESHEPSY] * shft - sigr + E0 * epsr) / m.k[S2K_E0MESH];
         sigs0 = Fy * shft + Esh * (epss0 - epsy * shft);
         epspl = epsmax;
-    } else if (kon == 1 && deps < 0.0) {
+    } else if (kon == 1 && !up) {
         kon = 2;
         epsr = c.eps;
         sigr = c.sig;
@@ -204,17 +239,6 @@ __device__ __forceinline__ void steel02_trial(const DevMat& m, const S2State& c,
         sigs0 = -Fy * shft + Esh * (epss0 + epsy * shft);
         epspl = epsmin;
     }
-    const double xi = fabs((epspl - epss0) / epsy);
-    const double R = R0 * (1.0 - (cR1 * xi) / (cR2 + xi));
-    const double epsrat = (eps - epsr) / (epss0 - epsr);
-    const double dum1 = 1.0 + pow(fabs(epsrat), R);
-    const double dum2 = pow(dum1, 1.0 / R);
-    double sig = b * epsrat + (1.0 - b) * epsrat / dum2;
-    sig = sig * (sigs0 - sigr) + sigr;
-    double e = b + (1.0 - b) / (dum1 * dum2);
-    e = e * (sigs0 - sigr) / (epss0 - epsr);
-    t.sig = sig;
-    t.tan = e;
     t.epsmin = epsmin;
     t.epsmax = epsmax;
     t.epspl = epspl;
@@ -223,6 +247,97 @@ __device__ __forceinline__ void steel02_trial(const DevMat& m, const S2State& c,
     t.epsr = epsr;
     t.sigr = sigr;
     t.kon = kon;
+}
+
+__device__ __forceinline__ void steel02_curve_of(const DevMat& m, const S2State& t, S2Curve& cv) {
+    const double R0 = m.p[3], cR1 = m.p[4], cR2 = m.p[5];
+    const double epsy = m.k[S2K_EPSY];
+    const double xi = fabs((t.epspl - t.epss0) / epsy);
+    const double R = R0 * (1.0 - (cR1 * xi) / (cR2 + xi));
+    cv.epsr = t.epsr;
+    cv.sigr = t.sigr;
+    cv.denom = t.epss0 - t.epsr;
+    cv.dsig = t.sigs0 - t.sigr;
+    cv.R = R;
+    cv.invR = 1.0 / R;
+}
+
+// Menegotto-Pinto curve: stress and tangent at eps on the branch cv.
+__device__ __forceinline__ void steel02_curve_eval(const DevMat& m, const S2Curve& cv, double eps,
+                                                   double& sig, double& tan) {
+    const double b = m.p[2];
+    const double epsrat = (eps - cv.epsr) / cv.denom;
+    const double dum1 = 1.0 + pow(fabs(epsrat), cv.R);
+    const double dum2 = pow(dum1, cv.invR);
+    double s = b * epsrat + (1.0 - b) * epsrat / dum2;
+    s = s * cv.dsig + cv.sigr;
+    double e = b + (1.0 - b) / (dum1 * dum2);
+    e = e * cv.dsig / cv.denom;
+    sig = s;
+    tan = e;
+}
+
+__device__ __forceinline__ double steel02_strain(const DevMat& m, double trial_eps) {
+    double eps = trial_eps;
+    if (m.p[10] != 0.0) eps += m.k[S2K_SIGINI_E0];
+    return eps;
+}
+
+// True when the trial leaves the fiber at its initial state (kon 0 / 3 and no strain change).
+__device__ __forceinline__ bool steel02_no_change(const S2State& c, double deps) {
+    return (c.kon == 0 || c.kon == 3) && fabs(deps) < 2.220446049250313e-15;
+}
+
+// Direction of the branch: increasing strain, or no change on an increasing branch.
+__device__ __forceinline__ bool steel02_up(const S2State& c, double deps) {
+    return deps > 0.0 || (deps == 0.0 && c.kon == 1);
+}
+
+// Steel02 (Giuffre-Menegotto-Pinto with isotropic shift) trial from committed c.
+__device__ __forceinline__ void steel02_trial(const DevMat& m, const S2State& c,
+                                              double trial_eps, S2State& t) {
+    const double eps = steel02_strain(m, trial_eps);
+    t.eps = eps;
+    const double deps = eps - c.eps;
+    if (steel02_no_change(c, deps)) {
+        t.tan = m.p[1];
+        t.sig = m.p[10];
+        t.kon = 3;
+        t.epsmin = c.epsmin;
+        t.epsmax = c.epsmax;
+        t.epspl = c.epspl;
+        t.epss0 = c.epss0;
+        t.sigs0 = c.sigs0;
+        t.epsr = c.epsr;
+        t.sigr = c.sigr;
+        return;
+    }
+    steel02_branch(m, c, steel02_up(c, deps), t);
+    S2Curve cv;
+    steel02_curve_of(m, t, cv);
+    steel02_curve_eval(m, cv, eps, t.sig, t.tan);
+}
+
+__device__ __forceinline__ void steel02_derive(const DevMat& m, const S2State& c, S2Derived& d) {
+    S2State t;
+    steel02_branch(m, c, true, t);
+    steel02_curve_of(m, t, d.up);
+    steel02_branch(m, c, false, t);
+    steel02_curve_of(m, t, d.dn);
+}
+
+// Stress and tangent of steel02_trial, given the committed state's derived branches.
+__device__ __forceinline__ void steel02_sig_tan(const DevMat& m, const S2State& c,
+                                                const S2Derived& d, double trial_eps,
+                                                double& sig, double& tan) {
+    const double eps = steel02_strain(m, trial_eps);
+    const double deps = eps - c.eps;
+    if (steel02_no_change(c, deps)) {
+        tan = m.p[1];
+        sig = m.p[10];
+        return;
+    }
+    steel02_curve_eval(m, steel02_up(c, deps) ? d.up : d.dn, eps, sig, tan);
 }
 
 // Steel01 bilinear kinematic return map.

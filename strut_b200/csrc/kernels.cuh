@@ -26,8 +26,8 @@
 namespace strut {
 
 constexpr int kMaxIp = 10;
-// Threads of an element CTA: one team of 128 (up to 5 integration points) or 64 (up to 10)
-// threads per integration point.
+// Threads of an element CTA (element state determination; the commit kernel uses one team of
+// 128 (up to 5 integration points) or 64 (up to 10) threads per integration point).
 constexpr int kTeamThreads = 640;
 constexpr int kEStride = 80;  // doubles of element state
 constexpr int kEq = 0, kEe = 3, kEk = 13, kEv = 23;
@@ -83,6 +83,7 @@ struct DevInst {
 struct ElemList {
     int* list[2];
     int* count;  // 2 entries
+    int* next;   // 2 entries: work counter of the persistent element kernel
 };
 
 // Step / iteration control on the device (read by the kernels, advanced by step_end_kernel).

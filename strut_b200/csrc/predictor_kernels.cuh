@@ -1,0 +1,82 @@
+// Learned Newton predictor: per-node features, the network's increments back to a displacement
+// guess, and the copy of the element state the learned guess is evaluated from.
+//
+// Features of node p at step s (the step being computed, t = (s + 1) dt), n_in = 4 ndf + 17:
+//   the converged increments of its ndf dofs at steps s-1, s-2, s-3, s-4 (0 for a constrained dof
+//   or a step before the first), ground acceleration at steps s, s-1, ..., s-15 (0 before the
+//   record), the node height over the instance's height; each normalised (x - mean) * scale.
+// The network predicts, per dof and in units of y_scale, the correction the converged increment
+// of step s needs over the Newmark predictor's (the plain predictor stays the reference point).  Strut has no
+// learned predictor; the feature set is the one of the north-star configuration (2D: one ground
+// component; 41 features for a 3D node).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace strut {
+
+struct PredDev {
+    int n_nodes, ndf, n_in, n_free, n_inst, ag_len;
+    const int* node_free;   // n_nodes x ndf: global free index or -1
+    const int* node_inst;
+    const float* node_h;
+    const float* x_mean;    // n_in
+    const float* x_scale;   // n_in
+    const float* y_scale;   // ndf
+    const double* hist_du;  // 4 x n_free (slot = step % 4)
+    const double* ag_full;  // n_inst x ag_len: ground acceleration of step s
+};
+
+// Also clears the work counter the element evaluation of the learned guess claims from.
+__global__ void pred_features_kernel(PredDev P, const DevCtl* __restrict__ ctl, const int* __restrict__ status,
+                                     float* __restrict__ x, int* __restrict__ next_alt) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) {
+        next_alt[0] = 0;
+        next_alt[1] = 0;
+    }
+    if (p >= P.n_nodes) return;
+    const int s = ctl->step;
+    const int inst = P.node_inst[p];
+    float* xr = x + (size_t)p * P.n_in;
+    int k = 0;
+    for (int j = 0; j < 4; ++j) {
+        const int sj = s - 1 - j;
+        for (int d = 0; d < P.ndf; ++d, ++k) {
+            const int fi = P.node_free[p * P.ndf + d];
+            double v = 0.0;
+            if (fi >= 0 && sj >= 0) v = P.hist_du[(size_t)(sj & 3) * P.n_free + fi];
+            xr[k] = ((float)v - P.x_mean[k]) * P.x_scale[k];
+        }
+    }
+    for (int j = 0; j < 16; ++j, ++k) {
+        const int sj = s - j;
+        const double v = (sj >= 0 && sj < P.ag_len) ? P.ag_full[(size_t)inst * P.ag_len + sj] : 0.0;
+        xr[k] = ((float)v - P.x_mean[k]) * P.x_scale[k];
+    }
+    xr[k] = (P.node_h[p] - P.x_mean[k]) * P.x_scale[k];
+    (void)status;
+}
+
+// u_alt = u_pred + y * y_scale on the free dofs of every predicted node, u_pred being the Newmark
+// predictor the step starts from (the network predicts the correction to it); u_alt_full already
+// holds a copy of u_full, so constrained dofs keep their values.
+__global__ void pred_scatter_kernel(PredDev P, const float* __restrict__ y, const double* __restrict__ u_pred,
+                                    const int* __restrict__ free_dof, double* __restrict__ u_alt_f,
+                                    double* __restrict__ u_alt_full) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n_nodes * P.ndf) return;
+    const int p = q / P.ndf, d = q % P.ndf;
+    const int fi = P.node_free[p * P.ndf + d];
+    if (fi < 0) return;
+    const double u = u_pred[fi] + (double)y[(size_t)p * P.ndf + d] * (double)P.y_scale[d];
+    u_alt_f[fi] = u;
+    u_alt_full[free_dof[fi]] = u;
+}
+
+__global__ void copy_doubles_kernel(const double* __restrict__ src, double* __restrict__ dst, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+}  // namespace strut

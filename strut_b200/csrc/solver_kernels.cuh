@@ -50,6 +50,16 @@ struct InstArrays {
     int* piv;             // per free dof
     int* fallbacks;       // per instance count of dense fallbacks
     ElemList el;          // elements of the instances still iterating
+    // learned predictor (dual first iteration): the learned guess and its element results
+    int dual;
+    const double* u_alt_f;
+    const double* ek_alt;
+    const double* ef_alt;
+    double* estate;
+    const double* estate_alt;
+    long long* pred_stats;  // per instance: first iterations offered, learned guess chosen
+    double* hist_du;        // 4 x n_free ring of converged increments (slot = step % 4)
+    int n_free_total;
 };
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -219,6 +229,52 @@ __device__ __forceinline__ double gather_slot(const InstArrays& A, long long sp0
     return K;
 }
 
+// ||R||_2 of the Newmark residual R = P - F_int - C v - M a at the free displacements uf with
+// element results ek / ef (the residual of the first Newton iteration,
+// transient_nonlinear.mojo:2302-2356).  Collective; vs, as: n-entry shared scratch.
+__device__ double residual_norm(const DevInst& I, const InstArrays& A, const double* uf, const double* ek,
+                               const double* ef, double* vs, double* as, double* red) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = I.n, bw = I.bw, rw = I.rw, f0 = I.f_off;
+    for (int i = tid; i < n; i += nt) {
+        const int gi = f0 + i;
+        const double an = I.a0 * (uf[gi] - A.u_n[gi]) - I.a2 * A.v_n[gi] - I.a3 * A.a_n[gi];
+        vs[i] = A.v_n[gi] + I.dt * ((1.0 - I.gamma) * A.a_n[gi] + I.gamma * an);
+        as[i] = an;
+    }
+    __syncthreads();
+    const long long sp0 = I.slot_ptr_off;
+    const double* Kinit = A.Kinit + I.band_off;
+    double ss = 0.0;
+    for (int i = tid; i < n; i += nt) {
+        double cv = 0.0;
+        if (I.has_damping) {
+            for (int o = 0; o < rw; ++o) {
+                const int j = i + o - bw;
+                if (j < 0 || j >= n) continue;
+                const int slot = i * rw + o;
+                double C = I.alpha_m * (i == j ? A.Mrff[f0 + i] : 0.0);
+                if (I.beta_k != 0.0) {
+                    const long long c0 = A.slot_ptr[sp0 + slot], c1 = A.slot_ptr[sp0 + slot + 1];
+                    double K = 0.0;
+                    for (long long c = c0; c < c1; ++c) K += ek[A.slot_contrib[c]];
+                    C += I.beta_k * K;
+                }
+                if (I.beta_k_init != 0.0) C += I.beta_k_init * Kinit[slot];
+                cv += C * vs[j];
+            }
+        }
+        const int q0 = A.fint_ptr[I.fint_ptr_off + i], q1 = A.fint_ptr[I.fint_ptr_off + i + 1];
+        double F = 0.0;
+        for (int q = q0; q < q1; ++q) F += ef[A.fint_contrib[q]];
+        const double r = A.P_f[f0 + i] - F - 0.0 - cv - A.Mff[f0 + i] * as[i];
+        ss += r * r;
+    }
+    const double tot = block_sum(ss, red);
+    __syncthreads();
+    return sqrt(tot);
+}
+
 // Effective-matrix entry of band slot (i, j) exactly as the row assembly computes it
 // (load K, add a1 C, add a0 M).
 __device__ __forceinline__ double keff_slot(const DevInst& I, const InstArrays& A, long long sp0,
@@ -334,7 +390,8 @@ __device__ void dense_solve_warp(const double* D, const int* piv, int n, const d
 }
 
 __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __restrict__ insts,
-                                                              InstArrays A, int mode, int step) {
+                                                              InstArrays A0, int mode, int step) {
+    InstArrays A = A0;
     extern __shared__ __align__(16) double smem_inst[];
     __shared__ DevInst I;
     __shared__ double red[32];
@@ -348,6 +405,32 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     }
     __syncthreads();
     if (mode == INST_MODE_NEWTON && !A.active[inst]) return;
+    if (mode == INST_MODE_NEWTON && A.dual && A.ctl && A.ctl->iter == 0) {
+        // first iteration with a learned guess: both guesses were evaluated; keep the learned
+        // one only when its residual is the smaller (the plain predictor is the fallback)
+        double* vs = smem_inst;
+        double* as = smem_inst + I.n;
+        const double r_plain = residual_norm(I, A, A.u_f, A.ek, A.ef, vs, as, red);
+        const double r_learn = residual_norm(I, A, A.u_alt_f, A.ek_alt, A.ef_alt, vs, as, red);
+        const bool learn = isfinite(r_learn) && r_learn < r_plain;
+        if (learn) {
+            for (int i = tid; i < I.n; i += nt) {
+                const int gi = I.f_off + i;
+                const double u = A.u_alt_f[gi];
+                A.u_f[gi] = u;
+                A.u_full[A.free_dof[gi]] = u;
+            }
+            const size_t e0 = (size_t)I.elem_off * kEStride;
+            for (int t = tid; t < I.n_elem * kEStride; t += nt) A.estate[e0 + t] = A.estate_alt[e0 + t];
+            A.ek = A.ek_alt;
+            A.ef = A.ef_alt;
+        }
+        if (tid == 0 && A.pred_stats) {
+            A.pred_stats[2 * inst] += 1;
+            if (learn) A.pred_stats[2 * inst + 1] += 1;
+        }
+        __syncthreads();
+    }
     int* hrow = (A.hist_iters && A.ctl) ? A.hist_iters + (size_t)A.ctl->step * gridDim.x : nullptr;
     const int n = I.n, bw = I.bw, rw = I.rw;
     double* Kb = smem_inst;        // n * rw
@@ -637,6 +720,8 @@ __global__ void post_step_kernel(const DevInst* __restrict__ insts, InstArrays A
     const double vn = A.v_n[gi] + I.dt * ((1.0 - I.gamma) * A.a_n[gi] + I.gamma * an);
     A.a_f[gi] = an;
     A.v_f[gi] = vn;
+    // converged increment of this step for the learned predictor's features
+    if (A.hist_du && A.ctl) A.hist_du[(size_t)(A.ctl->step & 3) * A.n_free_total + gi] = A.u_f[gi] - A.u_n[gi];
 }
 
 __global__ void record_disp_kernel(const double* __restrict__ u_full,
@@ -670,6 +755,8 @@ __global__ void step_end_kernel(DevCtl* ctl, const int* __restrict__ status,
         *nactive = 0;
         el.count[0] = 0;
         el.count[1] = 0;
+        el.next[0] = 0;
+        el.next[1] = 0;
         const bool stop = ctl->single && status[0] != 0;
         if (use_cond) cudaGraphSetConditional(outer, (step + 1 < ctl->n_end && !stop) ? 1 : 0);
     }

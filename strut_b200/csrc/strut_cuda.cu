@@ -26,6 +26,7 @@
 #include "element_kernels.cuh"
 #include "kat_kernels.cuh"
 #include "solver_kernels.cuh"
+#include "predictor_kernels.cuh"
 
 using namespace strut;
 
@@ -268,12 +269,19 @@ struct StrutHandle {
     int* d_fail_step = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    const void* graph_keys[4] = {nullptr, nullptr, nullptr, nullptr};
+    const void* graph_keys[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* d_rhs = nullptr;
     std::vector<long long> elem_fibers;  // fibers per element (all families)
+    // node table of the learned predictor: nodes with a free dof, instance order then node order
+    std::vector<int> pn_free;   // per node ndf global free indices (-1: not free)
+    std::vector<int> pn_inst;
+    std::vector<float> pn_h;    // height / instance height
+    int pn_ndf = 3;
+    struct PredState* pred = nullptr;
     double commit_bytes_total = 0.0;
     long long dense_total = 0;
-    ~StrutHandle() {
+    ~StrutHandle();
+    void release() {
         for (void* p : allocs) cudaFree(p);
         if (d_hist_disp) cudaFree(d_hist_disp);
         if (d_hist_ef) cudaFree(d_hist_ef);
@@ -287,6 +295,16 @@ struct StrutHandle {
         if (stream) cudaStreamDestroy(stream);
     }
 };
+
+struct PredState;
+static void pred_free(PredState* p);
+StrutHandle::~StrutHandle() {
+    if (pred) pred_free(pred);
+    release();
+}
+// learned predictor steps of a Newton step (defined with the predictor's host code)
+static int pred_launch(StrutHandle* h);
+static int pred_add_nodes(StrutHandle* h, cudaGraph_t body, cudaGraphNode_t dep, cudaGraphNode_t* last);
 
 static int prof_begin(StrutHandle* h) {
     if (h->prof) CK(cudaEventRecord(h->ev0, h->stream));
@@ -304,16 +322,15 @@ static int prof_end(StrutHandle* h, int k) {
     return STRUT_OK;
 }
 
-// Element kernels: one team of 128 threads per integration point up to 5 points, else 64.
-using ElemKernel = decltype(&element_state_kernel<128>);
+// Element state kernel: kTeamThreads threads per element CTA.  Commit kernel: one team of 128
+// threads per integration point up to 5 points, else 64.
 using CommitKernel = decltype(&commit_kernel<128>);
-static ElemKernel elem_kernel_of(const StrutHandle* h) {
-    return h->max_nip <= 5 ? element_state_kernel<128> : element_state_kernel<64>;
-}
+static decltype(&element_state_kernel) elem_kernel_of(const StrutHandle*) { return element_state_kernel; }
+static dim3 elem_block(const StrutHandle*) { return dim3(kTeamThreads); }
 static CommitKernel commit_kernel_of(const StrutHandle* h) {
     return h->max_nip <= 5 ? commit_kernel<128> : commit_kernel<64>;
 }
-static dim3 elem_block(const StrutHandle* h) { return dim3((h->max_nip <= 5 ? 128 : 64) * h->max_nip); }
+static dim3 commit_block(const StrutHandle* h) { return dim3((h->max_nip <= 5 ? 128 : 64) * h->max_nip); }
 
 // all_elems: every element (set-up and single-iteration entries); otherwise the list of
 // elements of the instances still iterating.
@@ -447,7 +464,9 @@ static int build_graph(StrutHandle* h) {
                         (const DevInst*)h->d_insts, A, (const int*)h->d_free_inst, (const int*)h->d_free_dir,
                         (const double*)h->d_ag, nF, h->n_inst, h->d_ctl, inner, 1));
     cudaGraph_t ibody;
-    TRY(add_while_node(&n_inner, body, &n_pred, 1, inner, &ibody));
+    cudaGraphNode_t n_before_inner = n_pred;
+    if (h->pred) TRY(pred_add_nodes(h, body, n_pred, &n_before_inner));
+    TRY(add_while_node(&n_inner, body, &n_before_inner, 1, inner, &ibody));
     cudaGraphNode_t n_el, n_in, n_chk;
     TRY(add_kernel_node(&n_el, ibody, nullptr, 0, elem_kernel_of(h), dim3(h->elem_grid),
                         elem_block(h), h->elem_smem, (const DevElem*)h->d_elems, h->geo,
@@ -459,7 +478,7 @@ static int build_graph(StrutHandle* h) {
     TRY(add_kernel_node(&n_chk, ibody, &n_in, 1, newton_check_kernel, dim3(1), dim3(32), 0, h->d_ctl,
                         (const int*)h->A.nactive, inner, 1));
     TRY(add_kernel_node(&n_commit, body, &n_inner, 1, commit_kernel_of(h), dim3(h->n_elem),
-                        elem_block(h), 0, (const DevElem*)h->d_elems, h->geo, h->fs,
+                        commit_block(h), 0, (const DevElem*)h->d_elems, h->geo, h->fs,
                         (const double*)h->A.u_full, h->d_estate, (const int*)h->A.status, h->d_hist_ef,
                         (const int*)h->d_rece_base, std::max(h->n_rece_slots, 1), (const DevCtl*)h->d_ctl));
     TRY(add_kernel_node(&n_post, body, &n_commit, 1, post_step_kernel, dim3((nF + tb - 1) / tb), dim3(tb), 0,
@@ -478,12 +497,13 @@ static int build_graph(StrutHandle* h) {
     h->graph_keys[1] = h->d_hist_ef;
     h->graph_keys[2] = h->d_hist_iters;
     h->graph_keys[3] = h->d_ag;
+    h->graph_keys[4] = h->pred;
     return STRUT_OK;
 }
 
 static int ensure_graph(StrutHandle* h) {
     if (h->gexec && h->graph_keys[0] == h->d_hist_disp && h->graph_keys[1] == h->d_hist_ef &&
-        h->graph_keys[2] == h->d_hist_iters && h->graph_keys[3] == h->d_ag)
+        h->graph_keys[2] == h->d_hist_iters && h->graph_keys[3] == h->d_ag && h->graph_keys[4] == h->pred)
         return STRUT_OK;
     return build_graph(h);
 }
@@ -566,6 +586,23 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             if (d.f_const) fcf[fi] = d.f_const[dof];
         }
         if (!has_mass) return bail(fail(STRUT_BAD_ARG, "transient_nonlinear requires masses on free dofs"));
+        {
+            double hmax = 0.0;
+            for (int nd = 0; nd < d.num_nodes; ++nd) hmax = std::max(hmax, d.node_coords[d.ndm * nd + d.ndm - 1]);
+            for (int nd = 0; nd < d.num_nodes; ++nd) {
+                bool any = false;
+                for (int k = 0; k < d.ndf; ++k) any = any || d.free_index[nd * d.ndf + k] >= 0;
+                if (!any) continue;
+                for (int k = 0; k < d.ndf; ++k) {
+                    const int fi = d.free_index[nd * d.ndf + k];
+                    h->pn_free.push_back(fi >= 0 ? f_off + fi : -1);
+                }
+                h->pn_inst.push_back(inst);
+                const double y = d.node_coords[d.ndm * nd + d.ndm - 1];
+                h->pn_h.push_back(hmax > 0.0 ? (float)(y / hmax) : 0.0f);
+            }
+            h->pn_ndf = d.ndf;
+        }
         for (int fi = 0; fi < nf; ++fi) {
             if (fdof[fi] < 0) return bail(fail(STRUT_BAD_ARG, "free numbering has holes"));
             Mff.push_back(mff[fi]);
@@ -641,7 +678,12 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             E.s1_blk = round4(E.nip * sd.n_s1);
             s1_total += E.s1_blk;
             h->max_nip = std::max(h->max_nip, E.nip);
-            const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) + 4 * (size_t)E.s2_blk;
+            // staged history + derived constants (Concrete02 5, Steel02 12 doubles per fiber) +
+            // the section's fiber y + per-fiber stress and tangent of every point
+            const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+            const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) + 4 * (size_t)E.s2_blk +
+                                8 * (size_t)(5 * E.c2_blk + 12 * E.s2_blk) +
+                                8 * (size_t)(((n_tot + 1) & ~1) + 2 * E.nip * n_tot);
             h->elem_smem = std::max(h->elem_smem, smem);
             h->elem_fibers.push_back((long long)E.nip * (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
             {
@@ -863,7 +905,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         (rc = dzeros(&h->d_counters, 8, al)) || (rc = dzeros(&A.dense, (size_t)h->dense_total, al)) ||
         (rc = dzeros(&A.piv, nF, al)) || (rc = dzeros(&A.fallbacks, (size_t)h->n_inst, al)) ||
         (rc = dzeros(&A.el.list[0], (size_t)h->n_elem, al)) || (rc = dzeros(&A.el.list[1], (size_t)h->n_elem, al)) ||
-        (rc = dzeros(&A.el.count, 2, al)))
+        (rc = dzeros(&A.el.count, 2, al)) || (rc = dzeros(&A.el.next, 2, al)))
         return bail(rc);
     double* d_Mff;
     double* d_Mrff;
@@ -899,6 +941,9 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         if ((rc = upload(&h->d_fail_step, neg, al))) return bail(rc);
     }
     A.ctl = h->d_ctl;
+    A.estate = h->d_estate;
+    A.n_free_total = h->n_free_total;
+    A.dual = 0;
     CK(cudaMallocHost((void**)&h->h_ctrl, 4 * sizeof(int)));
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
@@ -991,6 +1036,7 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
         CK(cudaMemcpyAsync(h->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemsetAsync(h->A.nactive, 0, 4 * sizeof(int), h->stream));
         CK(cudaMemsetAsync(h->A.el.count, 0, 2 * sizeof(int), h->stream));
+        CK(cudaMemsetAsync(h->A.el.next, 0, 2 * sizeof(int), h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
     if (n_steps > 0 && !h->prof) {
@@ -1007,6 +1053,11 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
                 h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag, nF, h->n_inst, h->d_ctl, none, 0);
             CK(cudaGetLastError());
             TRY(prof_end(h, 3));
+            if (h->pred) {
+                TRY(prof_begin(h));
+                TRY(pred_launch(h));
+                TRY(prof_end(h, 6));
+            }
             for (int it = 0; it < h->max_iters_global; ++it) {
                 TRY(launch_elements(h));
                 TRY(launch_instances(h, INST_MODE_NEWTON, step));
@@ -1017,7 +1068,7 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
                 if (h->h_ctrl[0] <= 0) break;
             }
             TRY(prof_begin(h));
-            commit_kernel_of(h)<<<h->n_elem, elem_block(h), 0, h->stream>>>(
+            commit_kernel_of(h)<<<h->n_elem, commit_block(h), 0, h->stream>>>(
                 h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, h->d_hist_ef, h->d_rece_base,
                 std::max(h->n_rece_slots, 1), h->d_ctl);
             CK(cudaGetLastError());
@@ -1267,7 +1318,7 @@ int strut_gpu_factor_solve(StrutHandle* h, const double* rhs, double* du) {
 
 int strut_gpu_commit(StrutHandle* h) {
     if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
-    commit_kernel_of(h)<<<h->n_elem, elem_block(h), 0, h->stream>>>(
+    commit_kernel_of(h)<<<h->n_elem, commit_block(h), 0, h->stream>>>(
         h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, nullptr, h->d_rece_base, 1, h->d_ctl);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
@@ -1452,3 +1503,5 @@ int strut_gpu_section_path(const StrutUniMaterial* materials, int32_t num_materi
 }
 
 }  // extern "C"
+#include "mlp_host.cuh"
+#include "predictor_host.cuh"

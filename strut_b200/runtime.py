@@ -217,3 +217,82 @@ class SectionBatch:
             self.close()
         except Exception:
             pass
+
+
+_fp = C.POINTER(C.c_float)
+
+
+class Mlp:
+    """The learned predictor's per-node network on the GPU (strut_gpu_mlp_*)."""
+
+    H = 128
+
+    def __init__(self, n_in: int, n_out: int):
+        m = C.c_void_p()
+        _check(lib().strut_gpu_mlp_create(n_in, n_out, C.byref(m)), "strut_gpu_mlp_create")
+        self.m = m
+        self.n_in, self.n_out = n_in, n_out
+
+    def n_params(self) -> int:
+        return int(lib().strut_gpu_mlp_param_count(self.m))
+
+    @staticmethod
+    def pack(p: dict) -> np.ndarray:
+        return np.concatenate([np.asarray(p[k], dtype=np.float32).reshape(-1)
+                               for k in ("W1", "b1", "W2", "b2", "W3", "b3")])
+
+    def unpack(self, flat: np.ndarray) -> dict:
+        shapes = (("W1", (self.n_in, self.H)), ("b1", (self.H,)), ("W2", (self.H, self.H)), ("b2", (self.H,)),
+                  ("W3", (self.H, self.n_out)), ("b3", (self.n_out,)))
+        out, o = {}, 0
+        for k, sh in shapes:
+            n = int(np.prod(sh))
+            out[k] = flat[o:o + n].reshape(sh).copy()
+            o += n
+        return out
+
+    def set_params(self, p: dict):
+        flat = np.ascontiguousarray(self.pack(p))
+        assert flat.size == self.n_params()
+        _check(lib().strut_gpu_mlp_set_params(self.m, flat.ctypes.data_as(_fp)), "strut_gpu_mlp_set_params")
+
+    def get_params(self) -> dict:
+        flat = np.zeros(self.n_params(), dtype=np.float32)
+        _check(lib().strut_gpu_mlp_get_params(self.m, flat.ctypes.data_as(_fp)), "strut_gpu_mlp_get_params")
+        return self.unpack(flat)
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], self.n_out), dtype=np.float32)
+        _check(lib().strut_gpu_mlp_forward(self.m, x.ctypes.data_as(_fp), x.shape[0], y.ctypes.data_as(_fp)),
+               "strut_gpu_mlp_forward")
+        return y
+
+    def loss_grad(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = C.c_float()
+        g = np.zeros(self.n_params(), dtype=np.float32)
+        _check(lib().strut_gpu_mlp_loss_grad(self.m, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0],
+                                             C.byref(loss), g.ctypes.data_as(_fp)), "strut_gpu_mlp_loss_grad")
+        return float(loss.value), self.unpack(g)
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int, batch: int = 4096, lr: float = 1e-3,
+              seed: int = 0) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = C.c_float()
+        _check(lib().strut_gpu_mlp_train(self.m, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), x.shape[0], epochs,
+                                          batch, lr, seed, C.byref(loss)), "strut_gpu_mlp_train")
+        return float(loss.value)
+
+    def close(self):
+        if getattr(self, "m", None):
+            lib().strut_gpu_mlp_destroy(self.m)
+            self.m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

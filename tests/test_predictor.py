@@ -1,0 +1,101 @@
+"""Learned Newton predictor on the batched transient path: device features against the host
+restatement, the answer kept within tolerance of the plain method, and the fallback."""
+import numpy as np
+import pytest
+
+from strut_b200 import model as M
+from strut_b200 import predictor as PR
+from strut_b200 import workloads as W
+from helpers import rel_err_of_peak
+
+
+def _case(seed, steps, stories=3, bays=2, pga=0.3):
+    return W.rc_frame_case(stories=stories, bays=bays, steps=steps, seed=seed, pga_g=pga)
+
+
+def test_host_features_layout():
+    m = M.Model(_case(3, 30))
+    rng = np.random.default_rng(0)
+    u = np.cumsum(rng.standard_normal((30, m.num_free)) * 1e-4, axis=0)
+    X, T = PR.raw_features(m, u)
+    frees, hs = PR.node_table(m)
+    nn = frees.shape[0]
+    assert X.shape == (30 * nn, PR.n_features(m.ndf)) and T.shape == (30 * nn, m.ndf)
+    s, p = 7, 2
+    row = X[s * nn + p]
+    du = np.diff(np.vstack([np.zeros((1, m.num_free)), u]), axis=0)
+    for j in range(4):
+        for d in range(m.ndf):
+            fi = frees[p, d]
+            assert row[j * m.ndf + d] == np.float32(du[s - 1 - j, fi] if fi >= 0 else 0.0)
+    ag = PR.ground_series(m, 30)
+    assert row[4 * m.ndf] == np.float32(ag[s]) and row[4 * m.ndf + 7] == np.float32(ag[0])
+    assert row[4 * m.ndf + 8] == 0.0 and row[-1] == hs[p]
+
+
+@pytest.mark.gpu
+def test_device_features_match_host(gpu_lib):
+    m = PR.record_all_dofs(M.Model(_case(5, 60)))
+    pred = PR.LearnedPredictor(m.ndf, seed=1)
+    rng = np.random.default_rng(2)
+    pred.x_mean = rng.standard_normal(pred.n_in).astype(np.float32) * 1e-3
+    pred.x_scale = (1.0 + rng.random(pred.n_in)).astype(np.float32)
+    with gpu_lib.Analysis([m]) as an:
+        pred.attach(an)
+        an.run(40)
+        u = PR.free_history(an, 0)
+        dev = PR.device_features(an)
+    # host features of step 40 from the converged history of steps 0..39 (plus a dummy row)
+    X, _ = PR.raw_features(m, np.vstack([u, u[-1:]]))
+    nn = dev.shape[0]
+    host = (X[40 * nn:41 * nn] - pred.x_mean) * pred.x_scale
+    assert np.allclose(dev, host, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_learned_predictor_keeps_the_answer(gpu_lib):
+    """Train on plain histories of three records, run a fourth with and without the predictor:
+    the learned guess has the smaller residual on most steps, the displacements stay within 1e-7
+    of peak of the plain method's, and the Newton iteration count stays within 2% of it (the
+    gain itself is printed: a better first guess saves an iteration only where the plain
+    predictor's second correction was just above the tolerance)."""
+    steps = 400
+    train = [PR.record_all_dofs(M.Model(_case(s, steps))) for s in (41, 42, 43)]
+    with gpu_lib.Analysis(train) as an:
+        an.run(steps)
+        hists = [PR.free_history(an, i) for i in range(3)]
+    Xs, Ts = zip(*[PR.raw_features(m, h) for m, h in zip(train, hists)])
+    X, T = np.concatenate(Xs), np.concatenate(Ts)
+    pred = PR.LearnedPredictor(train[0].ndf, seed=3)
+    pred.fit(X, T, epochs=30, batch=4096, lr=2e-3, seed=4)
+    test = M.Model(_case(44, steps))
+    with gpu_lib.Analysis([test]) as plain:
+        plain.run(steps)
+        d0, e0, i0 = plain.history(0)
+    with gpu_lib.Analysis([M.Model(_case(44, steps))]) as learned:
+        pred.attach(learned)
+        learned.run(steps)
+        d1, e1, i1 = learned.history(0)
+        offered, chosen = PR.stats(learned)
+    assert offered == steps
+    assert chosen >= steps // 2
+    for j in range(d0.shape[1]):
+        assert rel_err_of_peak(d1[:, j], d0[:, j]) <= 1e-7
+    print(f"\nlearned guess kept on {chosen}/{offered} steps; Newton iterations {int(i1.sum())} "
+          f"with the predictor, {int(i0.sum())} without")
+    assert i1.sum() <= 1.02 * i0.sum()
+
+
+@pytest.mark.gpu
+def test_detached_predictor_is_the_plain_method(gpu_lib):
+    steps = 50
+    with gpu_lib.Analysis([M.Model(_case(7, steps))]) as a:
+        a.run(steps)
+        d0, _e, i0 = a.history(0)
+    pred = PR.LearnedPredictor(3, seed=5)
+    with gpu_lib.Analysis([M.Model(_case(7, steps))]) as b:
+        pred.attach(b)
+        PR.detach(b)
+        b.run(steps)
+        d1, _e, i1 = b.history(0)
+    assert np.array_equal(d0, d1) and np.array_equal(i0, i1)
