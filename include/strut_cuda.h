@@ -344,6 +344,26 @@ int strut_gpu_predictor_stats(const StrutHandle* h, int64_t* offered, int64_t* c
 /* The normalised features of the next step, nodes x (4 ndf + 17) (tests). */
 int strut_gpu_predictor_features(StrutHandle* h, float* out);
 
+/* ---- band factor-solve that allocates nothing -------------------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library allocate device
+ * memory: a host that reserves the device's memory for itself up front, or one that must not
+ * trigger the device-wide synchronisation a cudaMalloc / cudaFree can cause between Newton
+ * iterations.  Factors and solves one BandGeneral (band_dev: n x (2*half_bw+1), slot
+ * row*(2bw+1) + (col-row+bw)) or BandSPD (band_dev: n x (half_bw+1), slot row*(bw+1) +
+ * (row-col)) system held in device memory, with the kernels of strut_gpu_factor_solve, on
+ * `stream`; writes x_dev and *status_dev (0 ok, 2 singular or not positive definite).  The
+ * BandGeneral dense partial-pivot fallback works in a static device buffer compiled into the
+ * library (2 MiB, held by every GPU that loads the library until the process exits), so n is
+ * limited to 512: a larger n returns STRUT_BAD_ARG, a band too wide for shared memory
+ * STRUT_UNSUPPORTED.  Nothing in that buffer has to be cleared: each call writes what it reads.
+ * Every call on a device shares the buffer, so calls whose kernels may overlap on the GPU
+ * (unordered streams) race and must be serialised by the caller.  The first call on a device
+ * looks up the buffer's address and sets the kernel's shared-memory limit; make it before any
+ * stream capture.  Returns after the launch (asynchronous). */
+int strut_gpu_band_solve_noalloc(const double* band_dev, int32_t n, int32_t half_bw,
+                                 int32_t system, const double* rhs_dev, double* x_dev,
+                                 int32_t* status_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -245,6 +245,9 @@ EXPORTS = {
     "strut_gpu_predictor_nodes": (C.c_int32, [C.c_void_p]),
     "strut_gpu_predictor_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "strut_gpu_predictor_features": (C.c_int, [C.c_void_p, _fp]),
+    "strut_gpu_band_solve_noalloc": (
+        C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    ),
     "strut_gpu_mlp_train": (
         C.c_int, [C.c_void_p, _fp, _fp, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _fp]
     ),

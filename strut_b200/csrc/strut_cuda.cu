@@ -1505,3 +1505,4 @@ int strut_gpu_section_path(const StrutUniMaterial* materials, int32_t num_materi
 }  // extern "C"
 #include "mlp_host.cuh"
 #include "predictor_host.cuh"
+#include "noalloc.cuh"
