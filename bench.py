@@ -18,6 +18,10 @@ updates/s, simulated seconds per wall second.
 Multi-GPU: one process per GPU, each with its own 256 frames (records seeded per rank): weak
 scaling, no collective on the data path; the timing is the max over ranks.
 
+Learned arm (``learned`` in the line, off with --no-learned): a per-node network trained on the
+tensor cores on plain histories of 64 other frames proposes each step's first Newton guess; the
+first iteration keeps it only where its residual beats the Newmark predictor's.
+
 ``--impl reference`` times the reference algorithm's CPU implementation (the CPU oracle, a
 plain C restatement of Strut's path; Strut itself is Mojo and cannot be built here) on all host
 cores over a bounded sample of the same workload.
@@ -53,6 +57,9 @@ def parse():
     ap.add_argument("--frames", type=int, default=N_FRAMES)
     ap.add_argument("--record-steps", type=int, default=STEPS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor arm")
+    ap.add_argument("--train-frames", type=int, default=64)
+    ap.add_argument("--train-epochs", type=int, default=8)
     ap.add_argument("--profile-only", action="store_true",
                     help="one short analysis (for a profiler launch list); prints no bench line")
     return ap.parse_args()
@@ -161,6 +168,68 @@ def cpu_baseline(models, cases, nthreads=None, target_s=15.0):
     return rph, nthreads, sample
 
 
+def learned_arm(args, models, device, runtime, A, torch, world):
+    """The learned+batched arm: train the per-node network (tensor-core kernels) on histories the
+    plain method computes for separate training frames and records (seeds 5000+), then run the
+    same batch as the plain arm with the network proposing each step's first guess.  Untimed:
+    data generation and training; timed (device events): the analysis."""
+    from strut_b200 import model as Mo, predictor as PR, workloads as W
+
+    t0 = time.perf_counter()
+    tcases = W.batched_frames(args.train_frames, steps=args.record_steps, dt=DT, base_seed=5000)
+    tmodels = [PR.record_all_dofs(Mo.Model(c)) for c in tcases]
+    with runtime.Analysis(tmodels, device=device) as an:
+        an.run(args.record_steps, check=False)
+        status = an.instance_status()
+        Xs, Ts = [], []
+        for i, m in enumerate(tmodels):
+            if status[i] != 0:
+                continue
+            X, T = PR.raw_features(m, PR.free_history(an, i))
+            nn = X.shape[0] // args.record_steps
+            keep = (np.arange(X.shape[0]) // nn) % 4 == 0  # every 4th step
+            Xs.append(X[keep])
+            Ts.append(T[keep])
+    X, T = np.concatenate(Xs), np.concatenate(Ts)
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    pred = PR.LearnedPredictor(tmodels[0].ndf, seed=7)
+    loss = pred.fit(X, T, epochs=args.train_epochs, batch=8192, lr=1e-3, seed=11)
+    t_train = time.perf_counter() - t0
+
+    an = runtime.Analysis(models, device=device)
+    pred.attach(an)
+    stream = torch.cuda.ExternalStream(runtime.lib().strut_gpu_stream(an.h))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    st = an.run(args.record_steps, check=False)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    completed = int((an.instance_status() == 0).sum())
+    offered, chosen = PR.stats(an)
+    an.close()
+    if world > 1:
+        t = torch.tensor([ms, completed], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t)
+        ms, completed = float(mx[0].item()), int(t[1].item())
+    return {
+        "value": completed / (ms / 1000.0) * 3600.0, "unit": "records/hour", "ms": ms,
+        "newton_its_per_step": st.global_newton_iterations / float(args.frames * args.record_steps),
+        "records_completed": completed,
+        "learned_guess_kept_frac": chosen / max(offered, 1),
+        "train": {"frames": args.train_frames, "samples": int(X.shape[0]), "epochs": args.train_epochs,
+                  "final_mse_normalised": loss, "data_s": round(t_data, 1), "train_s": round(t_train, 1),
+                  "network": f"{PR.n_features(tmodels[0].ndf)}-128-128-{tmodels[0].ndf} bf16 tcgen05, GELU"},
+    }
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -219,7 +288,10 @@ def main():
     n_fibers = sum(m.num_fibers_total for m in models)
 
     if args.profile_only:
+        # host-driven loop (profiling mode): plain launches a profiler can attribute (kernel
+        # nodes of a graph with conditional nodes cannot be profiled one by one)
         with runtime.Analysis(models, device=device) as an:
+            runtime.lib().strut_gpu_set_profiling(an.h, 1)
             an.run(min(50, args.record_steps), check=False)
         return 0
 
@@ -321,6 +393,10 @@ def main():
         except Exception:
             traffic = None
 
+    learned = None
+    if not args.no_learned:
+        learned = learned_arm(args, models, device, runtime, A, torch, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rph, cores, sample = cpu_baseline(models, cases)
@@ -362,6 +438,9 @@ def main():
             "gpu_launches": int(args.steps * (sum(P.launches[i] for i in range(5)) + st.steps_done)),
             "clocks": clk.summary(),
         }
+        if learned:
+            learned["vs_plain"] = learned["value"] / value if value else None
+            line["learned"] = learned
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
