@@ -68,8 +68,10 @@ enum { STRUT_MAT_ELASTIC = 0, STRUT_MAT_STEEL01 = 1, STRUT_MAT_CONCRETE01 = 2,
 enum { STRUT_ELEM_FORCE_BEAM_COLUMN_2D = 2, STRUT_ELEM_DISP_BEAM_COLUMN_2D = 3,
        STRUT_ELEM_FORCE_BEAM_COLUMN_3D = 11, STRUT_ELEM_DISP_BEAM_COLUMN_3D = 12 };
 
-/* geomTransf. */
-enum { STRUT_GEOM_LINEAR = 0, STRUT_GEOM_PDELTA = 1 };
+/* geomTransf.  Corotational applies to the 3D beam-columns only: their local axes follow the
+ * displaced end positions and they add the PDelta axial term (force_beam_column3d.mojo:
+ * 510-547, beam_column3d_nonlinear.mojo:200-238). */
+enum { STRUT_GEOM_LINEAR = 0, STRUT_GEOM_PDELTA = 1, STRUT_GEOM_COROTATIONAL = 2 };
 
 /* AnalysisSystemTag (tag_types.mojo:43-51). */
 enum { STRUT_SYSTEM_BAND_GENERAL = 1, STRUT_SYSTEM_BAND_SPD = 2 };

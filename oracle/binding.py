@@ -45,6 +45,9 @@ def lib():
         L.oracle_section_batch_path.argtypes = [C.POINTER(A.StrutUniMaterial), C.c_int,
                                                 C.POINTER(A.StrutFiber), C.c_int, C.c_int, _dp,
                                                 C.c_int, _dp]
+        L.oracle_section3d_path.argtypes = [C.POINTER(A.StrutUniMaterial), C.c_int,
+                                            C.POINTER(A.StrutFiber), C.c_int, _dp, C.c_int, _dp]
+        L.oracle_element_state.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _dp]
         L.oracle_run_transient.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _ip, _ip]
         L.oracle_state_determination.argtypes = [C.POINTER(A.StrutModelDesc), _dp, _dp, _dp, _ip]
         L.oracle_run_transient_batch.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, C.c_int,
@@ -77,6 +80,17 @@ def section_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
     return out
 
 
+def section3d_path(mats, nmat, fibs, nfib, path) -> np.ndarray:
+    """path: (npts, 3) of (eps0, kappa_y, kappa_z) -> (npts, 9) of N, My, Mz, k11, k12, k13,
+    k22, k23, k33."""
+    p = np.ascontiguousarray(path, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((len(p), 9))
+    rc = lib().oracle_section3d_path(mats, nmat, fibs, nfib, _d(p), len(p), _d(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_section3d_path failed: {A.STATUS_NAMES.get(rc, rc)}")
+    return out
+
+
 def section_batch_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
     """eps0_kappa: (npts, n_inst, 2) -> (npts, n_inst, 5)"""
     ek = np.ascontiguousarray(eps0_kappa, dtype=np.float64)
@@ -89,12 +103,12 @@ def section_batch_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
 
 
 def run_transient(model, steps: int):
-    """(disp (steps, nrec), eforce (steps, nrece, 6), iters (steps,), rc, failed_step)"""
+    """(disp (steps, nrec), eforce (steps, nrece, 2*ndf), iters (steps,), rc, failed_step)"""
     d = model.desc()
     nrec = d.num_record_dofs
     nrece = d.num_record_elements
     disp = np.zeros((steps, max(nrec, 1)))
-    ef = np.zeros((steps, max(nrece, 1), 6))
+    ef = np.zeros((steps, max(nrece, 1), 2 * model.ndf))
     iters = np.zeros(steps, dtype=np.int32)
     failed = C.c_int(-1)
     rc = lib().oracle_run_transient(C.byref(d), steps, _d(disp), _d(ef),
@@ -115,6 +129,19 @@ def state_determination(model, u_free):
     band = np.zeros((model.num_free, rw))
     rc = lib().oracle_state_determination(C.byref(d), _d(u), _d(f), _d(band), C.byref(bw))
     return f, band, bw.value
+
+
+def element_state(model, elem: int, u_elem):
+    """(k (nd, nd), f (nd,)) of one element at element displacements u_elem."""
+    nd = 2 * model.ndf
+    d = model.desc()
+    u = np.ascontiguousarray(u_elem, dtype=np.float64)
+    k = np.zeros((nd, nd))
+    f = np.zeros(nd)
+    rc = lib().oracle_element_state(C.byref(d), int(elem), _d(u), _d(k), _d(f))
+    if rc != 0:
+        raise RuntimeError(f"oracle_element_state failed: {A.STATUS_NAMES.get(rc, rc)}")
+    return k, f
 
 
 def run_batch(models, steps: int, nthreads: int):

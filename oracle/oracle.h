@@ -48,12 +48,21 @@ int oracle_section_path(const StrutUniMaterial* mats, int nmat, const StrutFiber
 int oracle_section_batch_path(const StrutUniMaterial* mats, int nmat, const StrutFiber* fibers,
                               int nfib, int n_inst, const double* eps0_kappa, int npts,
                               double* out);
-/* Single-instance transient run (the reference's plain CPU path). */
+/* One FiberSection3d along npts (eps0, kappa_y, kappa_z) points (path: npts x 3), committing
+ * after each; out: npts x 9 = N, My, Mz, k11, k12, k13, k22, k23, k33. */
+int oracle_section3d_path(const StrutUniMaterial* mats, int nmat, const StrutFiber* fibers,
+                          int nfib, const double* path, int npts, double* out);
+/* Single-instance transient run (the reference's plain CPU path).  eforce_hist holds
+ * 2*ndf values per recorded element and step. */
 int oracle_run_transient(const StrutModelDesc* m, int steps, double* disp_hist,
                          double* eforce_hist, int* iters_hist, int* failed_step);
 /* One element state determination + assembly at u_free (parity entry). */
 int oracle_state_determination(const StrutModelDesc* m, const double* u_free,
                                double* f_int_free, double* band_out, int* half_bw);
+/* One element's global tangent (nd x nd) and resisting force (nd) at element displacements
+ * u_elem (nd = 2 * ndf), from the element's initial state. */
+int oracle_element_state(const StrutModelDesc* m, int elem, const double* u_elem, double* k,
+                         double* f);
 /* Number of BandGeneral factorisations that fell back to dense partial-pivot LU. */
 long oracle_dense_fallbacks(void);
 /* Multi-instance run over nthreads host threads (CPU baseline leg).  record_status (optional,

@@ -32,9 +32,11 @@ typedef struct OModel {
     const StrutModelDesc* d;
     int n, bw, rw; /* free count, half band width, general row width 2bw+1 */
     int spd;
+    int nd; /* element dofs: 6 (2D) or 12 (3D) */
     OSection* secs;
+    OSection3d* secs3;
     OElement* elems;
-    int* efree; /* num_elements x 6 free equation numbers */
+    int* efree; /* num_elements x nd free equation numbers */
     double *K, *Kinit, *Kcomm, *C, *Keff, *Kspd;
     double *Mff, *Mrff;
     double *dense;
@@ -83,6 +85,10 @@ static void model_free(OModel* m) {
         for (int s = 0; s < m->d->num_sections; ++s) oracle_section_free(&m->secs[s]);
         free(m->secs);
     }
+    if (m->secs3) {
+        for (int s = 0; s < m->d->num_sections; ++s) oracle_section3d_free(&m->secs3[s]);
+        free(m->secs3);
+    }
     free(m->efree);
     free(m->K); free(m->Kinit); free(m->Kcomm); free(m->C); free(m->Keff); free(m->Kspd);
     free(m->Mff); free(m->Mrff); free(m->dense); free(m->piv);
@@ -95,34 +101,70 @@ static void model_free(OModel* m) {
 static int model_build(OModel* m, const StrutModelDesc* d) {
     memset(m, 0, sizeof(*m));
     m->d = d;
-    if (d->ndm != 2 || d->ndf != 3) return STRUT_UNSUPPORTED;
+    int three_d = d->ndm == 3 && d->ndf == 6;
+    if (!three_d && (d->ndm != 2 || d->ndf != 3)) return STRUT_UNSUPPORTED;
+    int ned = 2 * d->ndf;
+    m->nd = ned;
     if (d->num_free <= 0 || d->num_elements <= 0) return STRUT_BAD_ARG;
     if (d->system != STRUT_SYSTEM_BAND_GENERAL && d->system != STRUT_SYSTEM_BAND_SPD)
         return STRUT_UNSUPPORTED;
     m->spd = d->system == STRUT_SYSTEM_BAND_SPD;
     m->n = d->num_free;
-    m->secs = (OSection*)calloc(d->num_sections, sizeof(OSection));
-    for (int s = 0; s < d->num_sections; ++s) {
-        int rc = oracle_section_build(&m->secs[s], d->materials, d->num_materials, d->fibers,
-                                      d->sections[s].fiber_offset, d->sections[s].fiber_count);
-        if (rc != STRUT_OK) return rc;
+    if (three_d) {
+        m->secs3 = (OSection3d*)calloc(d->num_sections, sizeof(OSection3d));
+        for (int s = 0; s < d->num_sections; ++s) {
+            int rc = oracle_section3d_build(&m->secs3[s], d->materials, d->num_materials,
+                                            d->fibers, d->sections[s].fiber_offset,
+                                            d->sections[s].fiber_count);
+            if (rc != STRUT_OK) return rc;
+        }
+    } else {
+        m->secs = (OSection*)calloc(d->num_sections, sizeof(OSection));
+        for (int s = 0; s < d->num_sections; ++s) {
+            int rc = oracle_section_build(&m->secs[s], d->materials, d->num_materials, d->fibers,
+                                          d->sections[s].fiber_offset, d->sections[s].fiber_count);
+            if (rc != STRUT_OK) return rc;
+        }
     }
     m->elems = (OElement*)calloc(d->num_elements, sizeof(OElement));
-    m->efree = (int*)malloc(sizeof(int) * 6 * d->num_elements);
+    m->efree = (int*)malloc(sizeof(int) * ned * d->num_elements);
     int bw = 0;
     for (int e = 0; e < d->num_elements; ++e) {
         const StrutFrameElement* ed = &d->elements[e];
         OElement* el = &m->elems[e];
-        if (ed->type != STRUT_ELEM_FORCE_BEAM_COLUMN_2D && ed->type != STRUT_ELEM_DISP_BEAM_COLUMN_2D)
-            return STRUT_UNSUPPORTED;
+        int is3 = ed->type == STRUT_ELEM_FORCE_BEAM_COLUMN_3D ||
+                  ed->type == STRUT_ELEM_DISP_BEAM_COLUMN_3D;
+        int is2 = ed->type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D ||
+                  ed->type == STRUT_ELEM_DISP_BEAM_COLUMN_2D;
+        if (three_d ? !is3 : !is2) return STRUT_UNSUPPORTED;
+        if (!three_d && ed->geom == STRUT_GEOM_COROTATIONAL) return STRUT_UNSUPPORTED;
         el->desc = ed;
-        el->sec = &m->secs[ed->section];
         const StrutBeamIntegration* r = &d->integrations[ed->integration];
         el->nip = r->num_int_pts;
         for (int ip = 0; ip < el->nip; ++ip) {
             el->xi[ip] = r->xi[ip];
             el->w[ip] = r->w[ip];
         }
+        if (three_d) {
+            el->sec3 = &m->secs3[ed->section];
+            for (int c = 0; c < 3; ++c) {
+                el->x1[c] = d->node_coords[3 * ed->node_i + c];
+                el->x2[c] = d->node_coords[3 * ed->node_j + c];
+            }
+            double dx = el->x2[0] - el->x1[0], dy = el->x2[1] - el->x1[1];
+            double dz = el->x2[2] - el->x1[2];
+            el->L = sqrt(dx * dx + dy * dy + dz * dz);
+            if (el->L == 0.0) return STRUT_BAD_ARG;
+            el->inv_L3 = 1.0 / el->L;
+            int rrc = oracle_rotation3d(el->x1, el->x2, ed->has_vecxz, ed->vecxz, el->R);
+            if (rrc != STRUT_OK) return rrc;
+            el->G = d->sections[ed->section].G;
+            el->J = d->sections[ed->section].J;
+            el->sst = (OSecState*)calloc(el->nip, sizeof(OSecState));
+            for (int ip = 0; ip < el->nip; ++ip)
+                oracle_section3d_state_alloc(el->sec3, &el->sst[ip]);
+        } else {
+        el->sec = &m->secs[ed->section];
         double x1 = d->node_coords[2 * ed->node_i], y1 = d->node_coords[2 * ed->node_i + 1];
         double x2 = d->node_coords[2 * ed->node_j], y2 = d->node_coords[2 * ed->node_j + 1];
         double dx = x2 - x1, dy = y2 - y1;
@@ -138,15 +180,16 @@ static int model_build(OModel* m, const StrutModelDesc* d) {
         el->s_sync = dy / el->L_sync;
         el->sst = (OSecState*)calloc(el->nip, sizeof(OSecState));
         for (int ip = 0; ip < el->nip; ++ip) oracle_section_state_alloc(el->sec, &el->sst[ip]);
-        for (int a = 0; a < 6; ++a) {
-            int dof = ed->dof[a];
-            m->efree[6 * e + a] = (dof >= 0 && dof < d->num_dofs) ? d->free_index[dof] : -1;
         }
-        for (int a = 0; a < 6; ++a) {
-            int ia = m->efree[6 * e + a];
+        for (int a = 0; a < ned; ++a) {
+            int dof = ed->dof[a];
+            m->efree[ned * e + a] = (dof >= 0 && dof < d->num_dofs) ? d->free_index[dof] : -1;
+        }
+        for (int a = 0; a < ned; ++a) {
+            int ia = m->efree[ned * e + a];
             if (ia < 0) continue;
-            for (int b = a + 1; b < 6; ++b) {
-                int ib = m->efree[6 * e + b];
+            for (int b = a + 1; b < ned; ++b) {
+                int ib = m->efree[ned * e + b];
                 if (ib < 0) continue;
                 int diff = ia > ib ? ia - ib : ib - ia;
                 if (diff > bw) bw = diff;
@@ -205,27 +248,37 @@ static int model_build(OModel* m, const StrutModelDesc* d) {
 }
 
 /* assemble_global_stiffness_and_internal_soa: zero K and F_int, then every element in order */
+/* one element's global tangent and resisting force (nd x nd, nd) */
+static int element_state(OElement* el, const double* ug, double* k, double* f) {
+    switch (el->desc->type) {
+        case STRUT_ELEM_FORCE_BEAM_COLUMN_2D: return oracle_fbc2d(el, ug, k, f);
+        case STRUT_ELEM_DISP_BEAM_COLUMN_2D: return oracle_dbc2d(el, ug, k, f);
+        case STRUT_ELEM_FORCE_BEAM_COLUMN_3D: return oracle_fbc3d(el, ug, k, f);
+        default: return oracle_dbc3d(el, ug, k, f);
+    }
+}
+
 static int assemble(OModel* m, double* ek_out, double* ef_out) {
     const StrutModelDesc* d = m->d;
+    int nd = m->nd;
     memset(m->K, 0, sizeof(double) * (size_t)m->n * m->rw);
     memset(m->Fint, 0, sizeof(double) * d->num_dofs);
     for (int e = 0; e < d->num_elements; ++e) {
         OElement* el = &m->elems[e];
-        double ug[6], k[36], f[6];
-        for (int a = 0; a < 6; ++a) ug[a] = m->u[el->desc->dof[a]];
-        int rc = el->desc->type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D ? oracle_fbc2d(el, ug, k, f)
-                                                                   : oracle_dbc2d(el, ug, k, f);
+        double ug[12], k[144], f[12];
+        for (int a = 0; a < nd; ++a) ug[a] = m->u[el->desc->dof[a]];
+        int rc = element_state(el, ug, k, f);
         if (rc != STRUT_OK) return rc;
-        if (ek_out) memcpy(ek_out + 36 * e, k, sizeof(k));
-        if (ef_out) memcpy(ef_out + 6 * e, f, sizeof(f));
-        for (int a = 0; a < 6; ++a) {
-            int ia = m->efree[6 * e + a];
+        if (ek_out) memcpy(ek_out + (size_t)nd * nd * e, k, sizeof(double) * nd * nd);
+        if (ef_out) memcpy(ef_out + (size_t)nd * e, f, sizeof(double) * nd);
+        for (int a = 0; a < nd; ++a) {
+            int ia = m->efree[nd * e + a];
             if (ia >= 0) {
-                for (int b = 0; b < 6; ++b) {
-                    int ib = m->efree[6 * e + b];
+                for (int b = 0; b < nd; ++b) {
+                    int ib = m->efree[nd * e + b];
                     if (ib < 0) continue;
                     int sl = gslot(m, ia, ib);
-                    if (sl >= 0) m->K[sl] += k[a * 6 + b];
+                    if (sl >= 0) m->K[sl] += k[a * nd + b];
                 }
             }
             m->Fint[el->desc->dof[a]] += f[a];
@@ -525,23 +578,43 @@ static int initial_assembly(OModel* m) {
 
 static double simd_sumsq(const double* x, int n) { return oracle_simd_dot(x, x, n); }
 
-static void record_step(OModel* m, int step, double* disp_hist, double* eforce_hist) {
+/* Recorders after the step's commit (transient_nonlinear.mojo:3225-3300): node displacements,
+ * and element forces computed once per element and step.  A 3D beam-column's force comes from
+ * a full element state determination at the converged displacements
+ * (helpers.mojo:544-775), which for forceBeamColumn3d also updates its trial basic forces and
+ * section deformations, so recording an element is part of the trajectory. */
+static int record_step(OModel* m, int step, double* disp_hist, double* eforce_hist) {
     const StrutModelDesc* d = m->d;
+    int nd = m->nd;
     if (disp_hist)
         for (int j = 0; j < d->num_record_dofs; ++j)
             disp_hist[(size_t)step * d->num_record_dofs + j] = m->u[d->record_dofs[j]];
-    if (eforce_hist) {
-        for (int j = 0; j < d->num_record_elements; ++j) {
-            OElement* el = &m->elems[d->record_elements[j]];
-            double ug[6], f[6], k[36];
-            for (int a = 0; a < 6; ++a) ug[a] = m->u[el->desc->dof[a]];
-            if (el->desc->type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D)
-                oracle_fbc2d_force_from_basic(el, ug, f);
-            else
-                oracle_dbc2d(el, ug, k, f);
-            memcpy(eforce_hist + ((size_t)step * d->num_record_elements + j) * 6, f, sizeof(f));
+    for (int j = 0; j < d->num_record_elements; ++j) {
+        int eidx = d->record_elements[j];
+        int first = j;
+        for (int i = 0; i < j; ++i)
+            if (d->record_elements[i] == eidx) {
+                first = i;
+                break;
+            }
+        double* out = eforce_hist ? eforce_hist + ((size_t)step * d->num_record_elements + j) * nd : 0;
+        if (first != j) {
+            if (out) memcpy(out, eforce_hist + ((size_t)step * d->num_record_elements + first) * nd,
+                            sizeof(double) * nd);
+            continue;
         }
+        OElement* el = &m->elems[eidx];
+        double ug[12], f[12], k[144];
+        for (int a = 0; a < nd; ++a) ug[a] = m->u[el->desc->dof[a]];
+        if (el->desc->type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D) {
+            oracle_fbc2d_force_from_basic(el, ug, f);
+        } else {
+            int rc = element_state(el, ug, k, f);
+            if (rc != STRUT_OK) return rc;
+        }
+        if (out) memcpy(out, f, sizeof(double) * nd);
     }
+    return STRUT_OK;
 }
 
 static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_hist,
@@ -676,7 +749,11 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
             m->a_f[i] = an;
             m->v_f[i] = vn;
         }
-        record_step(m, step, disp_hist, eforce_hist);
+        int rrc = record_step(m, step, disp_hist, eforce_hist);
+        if (rrc != STRUT_OK) {
+            if (failed_step) *failed_step = step;
+            return rrc;
+        }
     }
     return STRUT_OK;
 }
@@ -714,6 +791,16 @@ int oracle_state_determination(const StrutModelDesc* d, const double* u_free,
                 memcpy(band_out, m.Keff, sizeof(double) * (size_t)m.n * m.rw);
         }
     }
+    model_free(&m);
+    return rc;
+}
+
+int oracle_element_state(const StrutModelDesc* d, int elem, const double* u_elem, double* k,
+                         double* f) {
+    OModel m;
+    int rc = model_build(&m, d);
+    if (rc == STRUT_OK && (elem < 0 || elem >= d->num_elements)) rc = STRUT_BAD_ARG;
+    if (rc == STRUT_OK) rc = element_state(&m.elems[elem], u_elem, k, f);
     model_free(&m);
     return rc;
 }

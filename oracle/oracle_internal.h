@@ -45,6 +45,28 @@ void oracle_section_revert(OSecState* st);
 void oracle_section_response(const OSection* sd, OSecState* st, double eps0, double kappa,
                              double out[5]);
 
+/* FiberSection3d definition (fiber3d.mojo:156-188): elastic fibers and nonlinear fibers, each
+ * in fiber order, coordinates relative to the area centroid. */
+typedef struct OSection3d {
+    const StrutUniMaterial* mats;
+    int W;
+    int nfib;
+    double y_bar, z_bar;
+    int n_el;
+    double *el_y, *el_z, *el_a, *el_e;
+    int n_nl;
+    double *nl_y, *nl_z, *nl_a;
+    int* nl_mat;
+} OSection3d;
+
+int oracle_section3d_build(OSection3d* sd, const StrutUniMaterial* mats, int nmat,
+                           const StrutFiber* fibers, int off, int nfib);
+void oracle_section3d_free(OSection3d* sd);
+void oracle_section3d_state_alloc(const OSection3d* sd, OSecState* st);
+/* out = {N, My, Mz, k11, k12, k13, k22, k23, k33} */
+void oracle_section3d_response(const OSection3d* sd, OSecState* st, double eps0, double ky,
+                               double kz, double out[9]);
+
 /* One frame element's persistent data. */
 typedef struct OElement {
     const StrutFrameElement* desc;
@@ -61,6 +83,16 @@ typedef struct OElement {
     double eps0[STRUT_MAX_INT_PTS], kappa[STRUT_MAX_INT_PTS];
     double v[3];
     OSecState* sst; /* nip section states */
+    /* 3D elements (12 dofs) */
+    const OSection3d* sec3;
+    double R[9];            /* rows: local x, y, z axes (undeformed geometry)        */
+    double x1[3], x2[3];    /* end coordinates (Corotational rotation)              */
+    double inv_L3;          /* 1/L cached by forceBeamColumn3d                      */
+    double G, J;
+    /* forceBeamColumn3d force_basic_q block: q0..q4, eps0[nip], ky[nip], kz[nip]
+     * (loader.mojo:1836-1840) */
+    double q5[5];
+    double ky[STRUT_MAX_INT_PTS], kz[STRUT_MAX_INT_PTS];
     /* counters */
     long local_iters;
     long section_evals;
@@ -69,5 +101,9 @@ typedef struct OElement {
 int oracle_fbc2d(OElement* e, const double u_global[6], double k[36], double f[6]);
 int oracle_dbc2d(OElement* e, const double u_global[6], double k[36], double f[6]);
 void oracle_fbc2d_force_from_basic(const OElement* e, const double u_global[6], double f[6]);
+int oracle_rotation3d(const double x1[3], const double x2[3], int has_vecxz, const double* vecxz,
+                      double R[9]);
+int oracle_fbc3d(OElement* e, const double u_global[12], double k[144], double f[12]);
+int oracle_dbc3d(OElement* e, const double u_global[12], double k[144], double f[12]);
 
 #endif

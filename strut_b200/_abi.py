@@ -44,6 +44,7 @@ ELEM_DISP_BEAM_COLUMN_3D = 12
 
 GEOM_LINEAR = 0
 GEOM_PDELTA = 1
+GEOM_COROTATIONAL = 2
 
 SYSTEM_BAND_GENERAL = 1
 SYSTEM_BAND_SPD = 2

@@ -344,6 +344,10 @@ class Model:
                 g = A.GEOM_LINEAR
             elif geom == "PDelta":
                 g = A.GEOM_PDELTA
+            elif geom == "Corotational" and self.ndm == 3:
+                g = A.GEOM_COROTATIONAL
+            elif self.ndm == 3:
+                raise ModelError(f"{et} supports geomTransf Linear, PDelta, or Corotational")
             else:
                 raise ModelError(f"{et} supports geomTransf Linear | PDelta")
             integ = e.get("integration", "Lobatto")

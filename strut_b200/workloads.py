@@ -9,6 +9,10 @@
   envelope (rise, hold, decay) and scaling to a target peak ground acceleration.
 * ``batched_frames``: the 256-frame batch (stories U{3..12}, bays U{2..5}, wg U(8, 25) rad/s,
   PGA U(0.2, 0.6) g, record i seeded with 1000 + i).
+* ``rc_frame3d_case``: a 3D RC moment frame (z vertical) of forceBeamColumn3d or
+  dispBeamColumn3d elements with FiberSection3d sections (same fiber layout as the 2D
+  sections, plus G and J for torsion), masses on the three translations of every floor node,
+  one or two horizontal records.
 
 Builder choices that the workload description leaves open (recorded here): cover 0.04 m; the
 cover concrete is fpc -30 MPa, epsc0 -0.002, fpcu 0, epscu -0.004 with the core's rat, ft and
@@ -34,9 +38,20 @@ BAR_AREA = 500.0e-6
 COVER_T = 0.04
 
 
-def rc_section(sec_id: int, width: float, depth: float, core_mat=1, cover_mat=2, steel_mat=3):
-    """10x10 confined core, two 20-fiber cover layers, 2 x 4 bars: 148 fibers."""
+def rc_section(sec_id: int, width: float, depth: float, core_mat=1, cover_mat=2, steel_mat=3,
+               three_d: bool = False, G: float = 12.5e9):
+    """10x10 confined core, two 20-fiber cover layers, 2 x 4 bars: 148 fibers.  With three_d
+    the section is a FiberSection3d whose torsional constant is the rectangle's
+    J = beta * b^3 * h (beta from b/h) with shear modulus G."""
     h2, b2, c = 0.5 * depth, 0.5 * width, COVER_T
+    if three_d:
+        sec = rc_section(sec_id, width, depth, core_mat, cover_mat, steel_mat)
+        sec["type"] = "FiberSection3d"
+        b, h = min(width, depth), max(width, depth)
+        beta = 1.0 / 3.0 - 0.21 * (b / h) * (1.0 - (b / h) ** 4 / 12.0)
+        sec["params"]["G"] = G
+        sec["params"]["J"] = beta * b ** 3 * h
+        return sec
     return {
         "id": sec_id,
         "type": "FiberSection2d",
@@ -237,6 +252,201 @@ def rc_frame_case(stories: int = 3, bays: int = 3, story_h: float = 3.6, bay_w: 
     }
     alpha, beta, _w = rayleigh_from_modes(case, zeta=zeta)
     case["rayleigh"] = {"alphaM": alpha, "betaKInit": beta}
+    return case
+
+
+def _section3d_initial_flex(sec: dict, mats: dict) -> np.ndarray:
+    """3x3 initial flexibility (N, My, Mz) of a FiberSection3d from the fibers' initial
+    tangents, about the area centroid (fiber3d.mojo:191-256 sums with E0)."""
+    from .model import discretize_section
+
+    cells = discretize_section(sec["params"])
+    area = sum(c[2] for c in cells)
+    ybar = sum(c[2] * c[0] for c in cells) / area
+    zbar = sum(c[2] * c[1] for c in cells) / area
+    ks = np.zeros((3, 3))
+    for (y, z, a, m) in cells:
+        mat = mats[m]
+        if mat["type"] == "Concrete02":
+            E = 2.0 * mat["params"]["fpc"] / mat["params"]["epsc0"]
+        elif mat["type"] in ("Steel02", "Steel01"):
+            E = mat["params"]["E0"]
+        else:
+            E = mat["params"]["E"]
+        yr, zr = y - ybar, z - zbar
+        ea = E * a
+        ks += ea * np.array([[1.0, zr, -yr], [zr, zr * zr, -zr * yr], [-yr, -zr * yr, yr * yr]])
+    return np.linalg.inv(ks)
+
+
+def _rotation3d(p1, p2, vecxz=None) -> np.ndarray:
+    """Local axes rows (x, y, z) as in elements/utils.mojo:77-140."""
+    d = np.asarray(p2, float) - np.asarray(p1, float)
+    lx = d / np.linalg.norm(d)
+    if vecxz is None:
+        v = np.array([1.0, 0.0, 0.0])
+        if abs(lx @ v) >= 0.9:
+            v = np.array([0.0, 1.0, 0.0])
+            if abs(lx @ v) >= 0.9:
+                v = np.array([0.0, 0.0, 1.0])
+    else:
+        v = np.asarray(vecxz, float)
+    ly = np.cross(v, lx)
+    ly /= np.linalg.norm(ly)
+    lz = np.cross(lx, ly)
+    return np.array([lx, ly, lz])
+
+
+def initial_stiffness_3d(case: dict) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Dense initial K_ff, lumped M_ff diagonal and free map of a 3D frame case (numpy): the
+    force-based element flexibility from the sections' initial tangents, GJ/L torsion."""
+    nodes = case["nodes"]
+    idx = {n["id"]: i for i, n in enumerate(nodes)}
+    ndof = 6 * len(nodes)
+    fixed = np.zeros(ndof, dtype=bool)
+    for i, n in enumerate(nodes):
+        for d in n.get("constraints", []) or []:
+            fixed[6 * i + d - 1] = True
+    free = np.where(~fixed)[0]
+    mats = {m["id"]: m for m in case["materials"]}
+    flex = {s["id"]: _section3d_initial_flex(s, mats) for s in case["sections"]}
+    gj = {s["id"]: s["params"]["G"] * s["params"]["J"] for s in case["sections"]}
+    K = np.zeros((ndof, ndof))
+    for e in case["elements"]:
+        ni, nj = idx[e["nodes"][0]], idx[e["nodes"][1]]
+        p1 = [nodes[ni][k] for k in ("x", "y", "z")]
+        p2 = [nodes[nj][k] for k in ("x", "y", "z")]
+        L = float(np.linalg.norm(np.subtract(p2, p1)))
+        fs = flex[e["section"]]
+        xis, ws = beam_integration_rule(e.get("integration", "Lobatto"), e.get("num_int_pts", 3))
+        F = np.zeros((5, 5))
+        for xi, w in zip(xis, ws):
+            b = np.array([[1.0, 0.0, 0.0, 0.0, 0.0],
+                          [0.0, 0.0, 0.0, xi - 1.0, xi],
+                          [0.0, xi - 1.0, xi, 0.0, 0.0]])
+            F += w * L * b.T @ fs @ b
+        kb = np.linalg.inv(F)
+        a = np.zeros((6, 12))
+        a[0, 0], a[0, 6] = -1.0, 1.0
+        a[1, 1], a[1, 5], a[1, 7] = 1.0 / L, 1.0, -1.0 / L
+        a[2, 1], a[2, 7], a[2, 11] = 1.0 / L, -1.0 / L, 1.0
+        a[3, 2], a[3, 4], a[3, 8] = -1.0 / L, 1.0, 1.0 / L
+        a[4, 2], a[4, 8], a[4, 10] = -1.0 / L, 1.0 / L, 1.0
+        a[5, 3], a[5, 9] = -1.0, 1.0
+        kb6 = np.zeros((6, 6))
+        kb6[:5, :5] = kb
+        kb6[5, 5] = gj[e["section"]] / L
+        kl = a.T @ kb6 @ a
+        R = _rotation3d(p1, p2, e.get("vecxz"))
+        T = np.kron(np.eye(4), R)
+        kg = T.T @ kl @ T
+        dofs = [6 * ni + k for k in range(6)] + [6 * nj + k for k in range(6)]
+        K[np.ix_(dofs, dofs)] += kg
+    M = np.zeros(ndof)
+    for m in case.get("masses", []):
+        M[6 * idx[m["node"]] + m["dof"] - 1] += m["value"]
+    return K[np.ix_(free, free)], M[free], free
+
+
+def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h: float = 3.6,
+                    bay_w: float = 6.0, nip: int = 5, floor_mass: float = 60.0e3,
+                    dt: float = 0.01, steps: int = 2000, seed: int = 1000, wg: float = 15.0,
+                    zg: float = 0.6, pga_g: float = 0.35, tol: float = 1.0e-8,
+                    max_iters: int = 20, element: str = "forceBeamColumn3d",
+                    system: str = "BandGeneral", zeta: float = 0.05, geom: str = "Linear",
+                    bidirectional: bool = False, record_elements=(1,)) -> dict:
+    """3D RC frame: columns along z, beams along x and y, base fixed in all six dofs."""
+    nodes = []
+    grid = {}
+    nid = 1
+    for k in range(stories + 1):
+        for j in range(bays_y + 1):
+            for i in range(bays_x + 1):
+                n = {"id": nid, "x": i * bay_w, "y": j * bay_w, "z": k * story_h}
+                if k == 0:
+                    n["constraints"] = [1, 2, 3, 4, 5, 6]
+                nodes.append(n)
+                grid[(k, j, i)] = nid
+                nid += 1
+    elements = []
+    eid = 1
+
+    def add(n1, n2, sec):
+        nonlocal eid
+        elements.append({"id": eid, "type": element, "nodes": [n1, n2], "section": sec,
+                         "geomTransf": geom, "integration": "Lobatto", "num_int_pts": nip})
+        eid += 1
+
+    for k in range(stories):
+        for j in range(bays_y + 1):
+            for i in range(bays_x + 1):
+                add(grid[(k, j, i)], grid[(k + 1, j, i)], 1)
+    for k in range(1, stories + 1):
+        for j in range(bays_y + 1):
+            for i in range(bays_x):
+                add(grid[(k, j, i)], grid[(k, j, i + 1)], 2)
+        for j in range(bays_y):
+            for i in range(bays_x + 1):
+                add(grid[(k, j, i)], grid[(k, j + 1, i)], 2)
+    masses = []
+    for k in range(1, stories + 1):
+        for j in range(bays_y + 1):
+            for i in range(bays_x + 1):
+                for d in (1, 2, 3):
+                    masses.append({"node": grid[(k, j, i)], "dof": d, "value": floor_mass})
+    n_samples = steps + 1
+    series = [{"type": "Path", "tag": 1, "dt": dt,
+               "values": [float(v) for v in kanai_tajimi_record(seed, n_samples, dt, wg=wg,
+                                                               zg=zg, pga_g=pga_g)]}]
+    pattern = {"type": "UniformExcitation", "tag": 1, "direction": 1, "accel": 1}
+    if bidirectional:
+        series.append({"type": "Path", "tag": 2, "dt": dt,
+                       "values": [float(v) for v in kanai_tajimi_record(
+                           seed + 500000, n_samples, dt, wg=wg, zg=zg, pga_g=pga_g)]})
+        pattern = [pattern, {"type": "UniformExcitation", "tag": 2, "direction": 2, "accel": 2}]
+    top = grid[(stories, bays_y, bays_x)]
+    case = {
+        "schema_version": "1.0",
+        "metadata": {"name": f"rc_frame3d_{stories}s{bays_x}x{bays_y}b_seed{seed}",
+                     "units": "SI"},
+        "model": {"ndm": 3, "ndf": 6},
+        "nodes": nodes,
+        "materials": [
+            {"id": 1, "type": "Concrete02", "params": dict(CORE)},
+            {"id": 2, "type": "Concrete02", "params": dict(COVER)},
+            {"id": 3, "type": "Steel02", "params": dict(STEEL)},
+        ],
+        "sections": [rc_section(1, 0.5, 0.5, three_d=True), rc_section(2, 0.4, 0.6, three_d=True)],
+        "elements": elements,
+        "masses": masses,
+        "time_series": series,
+        "pattern": pattern,
+        "analysis": {"type": "transient_nonlinear", "steps": steps, "dt": dt,
+                     "integrator": {"type": "Newmark", "gamma": 0.5, "beta": 0.25},
+                     "algorithm": "Newton", "test_type": "NormDispIncr", "tol": tol,
+                     "max_iters": max_iters, "system": system, "numberer": "RCM"},
+        "recorders": [
+            {"type": "node_displacement", "nodes": [top], "dofs": [1, 2, 3, 4, 5, 6],
+             "output": "roof"},
+        ],
+    }
+    if record_elements:
+        case["recorders"].append({"type": "element_force", "elements": list(record_elements),
+                                  "output": "elements"})
+    K, M, _free = initial_stiffness_3d(case)
+    m_idx = np.where(M > 0.0)[0]
+    z_idx = np.where(M == 0.0)[0]
+    Kmm = K[np.ix_(m_idx, m_idx)]
+    Kmz = K[np.ix_(m_idx, z_idx)]
+    Kzz = K[np.ix_(z_idx, z_idx)]
+    Kc = Kmm - Kmz @ np.linalg.solve(Kzz, Kmz.T)
+    from scipy import linalg
+
+    lam = linalg.eigh(Kc, np.diag(M[m_idx]), eigvals_only=True)
+    w = np.sqrt(np.sort(lam))
+    wi, wj = w[0], w[2]
+    case["rayleigh"] = {"alphaM": float(2.0 * zeta * wi * wj / (wi + wj)),
+                        "betaKInit": float(2.0 * zeta / (wi + wj))}
     return case
 
 

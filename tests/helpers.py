@@ -72,3 +72,62 @@ def rel_err_of_peak(a, b):
     if peak == 0.0:
         return float(np.max(np.abs(a - b)))
     return float(np.max(np.abs(a - b)) / peak)
+
+
+def planar_frame_3d(case2: dict) -> dict:
+    """The same plane frame as a 3D model: the 2D plane becomes the global x-z plane, the
+    out-of-plane dofs (y translation, rotations about x and z) are restrained, and each
+    member's vecxz makes its local y the 2D local y, so the 3D beam-columns bend about local z
+    exactly as the 2D ones do.  Displacement records map (ux, uy, rz) -> (ux, uz, -ry)."""
+    import copy
+
+    c = copy.deepcopy(case2)
+    c["model"] = {"ndm": 3, "ndf": 6}
+    for n in c["nodes"]:
+        x, y = n["x"], n["y"]
+        n["x"], n["y"], n["z"] = x, 0.0, y
+        base = bool(n.get("constraints"))
+        n["constraints"] = [1, 2, 3, 4, 5, 6] if base else [2, 4, 6]
+    nodes = {n["id"]: n for n in c["nodes"]}
+    for e in c["elements"]:
+        e["type"] = e["type"].replace("2d", "3d")
+        a, b = nodes[e["nodes"][0]], nodes[e["nodes"][1]]
+        vertical = abs(b["z"] - a["z"]) > 0.0
+        e["vecxz"] = [0.0, 1.0, 0.0] if vertical else [0.0, -1.0, 0.0]
+    for s in c["sections"]:
+        s["type"] = "FiberSection3d"
+        s["params"]["G"] = 12.5e9
+        s["params"]["J"] = 0.01
+    for m in c["masses"]:
+        m["dof"] = {1: 1, 2: 3}[m["dof"]]
+    for r in c["recorders"]:
+        if r["type"] == "node_displacement":
+            r["dofs"] = [1, 3, 5]
+    return c
+
+
+def single_element_3d(etype: str, geom: str = "Linear", end=(3.0, 1.0, 2.0), vecxz=None,
+                      nonlinear: bool = True) -> dict:
+    """One free-free 3D beam-column (node 1 at the origin, node 2 at ``end``) with the RC
+    FiberSection3d of the synthetic frames, or an all-elastic copy of its fiber layout."""
+    from strut_b200 import workloads as W
+
+    if nonlinear:
+        mats = [{"id": 1, "type": "Concrete02", "params": dict(W.CORE)},
+                {"id": 2, "type": "Concrete02", "params": dict(W.COVER)},
+                {"id": 3, "type": "Steel02", "params": dict(W.STEEL)}]
+        sec = W.rc_section(1, 0.4, 0.6, three_d=True)
+    else:
+        mats = [{"id": 1, "type": "Elastic", "params": {"E": 3.0e10}}]
+        sec = W.rc_section(1, 0.4, 0.6, core_mat=1, cover_mat=1, steel_mat=1, three_d=True)
+    el = {"id": 1, "type": etype, "nodes": [1, 2], "section": 1, "geomTransf": geom,
+          "integration": "Lobatto", "num_int_pts": 5}
+    if vecxz is not None:
+        el["vecxz"] = list(vecxz)
+    return {"model": {"ndm": 3, "ndf": 6},
+            "nodes": [{"id": 1, "x": 0.0, "y": 0.0, "z": 0.0},
+                      {"id": 2, "x": end[0], "y": end[1], "z": end[2]}],
+            "materials": mats, "sections": [sec], "elements": [el],
+            "masses": [{"node": 2, "dof": 1, "value": 1.0}],
+            "analysis": {"type": "transient_nonlinear", "dt": 0.01, "steps": 1,
+                         "test_type": "NormDispIncr", "tol": 1e-8}}
