@@ -293,6 +293,14 @@ def main():
         with runtime.Analysis(models, device=device) as an:
             runtime.lib().strut_gpu_set_profiling(an.h, 1)
             an.run(min(50, args.record_steps), check=False)
+            P = A.StrutKernelProfile()
+            runtime.lib().strut_gpu_get_profile(an.h, __import__("ctypes").byref(P))
+        if rank == 0:
+            names = ("element", "instance", "commit", "predictor", "post")
+            print(json.dumps({"profile": {n: {"launches": int(P.launches[i]), "ms": P.ms[i],
+                                              "algorithmic_bytes": P.bytes[i]}
+                                          for i, n in enumerate(names)},
+                              "frames": len(models), "steps": min(50, args.record_steps)}))
         return 0
 
     def one_analysis(prof=False):
@@ -385,13 +393,15 @@ def main():
     achieved = (el_bytes / el_launch) / ((el_ms / el_launch) / 1000.0) / 1e9
     kernel_share = {k: P.ms[i] for k, i in (("element", 0), ("instance", 1), ("commit", 2),
                                               ("predictor", 3), ("post", 4))}
+    # DRAM bytes per launch: the measured traffic / algorithmic-bytes ratio of this kernel (one
+    # ncu capture of a smaller batch of the same frames, traffic growing with the elements
+    # processed) times this run's algorithmic bytes per launch
     traffic = None
-    tp = ROOT / "profiles" / "element_state_kernel_traffic.json"
+    tp = ROOT / "profiles" / "element_state_kernel_dram_traffic_rc_frames96.md"
     if tp.exists():
-        try:
-            traffic = json.loads(tp.read_text()).get("bytes_per_launch_full_batch")
-        except Exception:
-            traffic = None
+        for line in tp.read_text().splitlines():
+            if line.startswith("traffic_to_algorithmic_ratio:"):
+                traffic = float(line.split(":", 1)[1]) * (el_bytes / el_launch)
 
     learned = None
     if not args.no_learned:

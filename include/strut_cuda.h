@@ -236,8 +236,9 @@ int strut_gpu_num_instances(const StrutHandle* h);
  * step, status) is returned.  A single-instance handle stops at its failing step. */
 int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats);
 /* Copies recorder histories of one instance for steps [0, steps_done):
- * disp: steps x num_record_dofs, eforce: steps x num_record_elements x 6,
- * iters: Newton iterations per step.  Any pointer may be NULL. */
+ * disp: steps x num_record_dofs, eforce: steps x num_record_elements x (2 ndf) global end
+ * forces, iters: Newton iterations per step.  Any pointer may be NULL.  A handle holds either
+ * 2D (ndf 3) or 3D (ndf 6) instances. */
 int strut_gpu_get_history(StrutHandle* h, int32_t instance, double* disp, double* eforce,
                           int32_t* iters);
 /* Same for all instances at once, instance-major, each block sized as for one instance

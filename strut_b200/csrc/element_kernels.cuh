@@ -884,23 +884,52 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
     return true;
 }
 
-// State determination of every element of the active instances: k (6x6 global), f (6) and the
-// element state.  One CTA of kTeamThreads threads per element at a time.
+}  // namespace strut
+
+#include "element3d_kernels.cuh"
+
+namespace strut {
+
+// Elements processed by one launch of the element kernel.
+enum { ELEM_MODE_LIST = 0, ELEM_MODE_ALL = 1, ELEM_MODE_RECORD = 2 };
+
+// Record pass after a step's commit: the recorded 3D beam-columns of the live instances, whose
+// recorded force is a full state determination at the converged displacements
+// (helpers.mojo:544-775; for forceBeamColumn3d this also moves its trial basic forces and section
+// deformations, as in Strut).
+struct RecPass {
+    const int* list;      // element indices
+    int n;
+    double* hist_ef;      // step-major: [step][slot][ef_w]
+    const int* rece_base; // first record slot of each instance
+    int slots, ef_w;
+};
+
+// State determination of every element of the active instances: k (nd x nd global), f (nd)
+// and the element state.  One CTA of kTeamThreads threads per element at a time.
 //
 // Persistent: the grid is sized to the resident CTAs of the device and each CTA claims elements
 // from the list of the instances still iterating (all elements when all_elems is set), so a
 // Newton iteration of a few slow records launches no idle CTAs and a slow element does not hold
 // up elements queued behind it on the same CTA.
+//
+// DIM 2 instantiates the 2D elements' code only, DIM 3 the 3D elements' (a batch holds one kind).
+template <int DIM>
 __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
     double* __restrict__ estate, double* __restrict__ ek, double* __restrict__ ef,
     const int* __restrict__ active, int* __restrict__ status, int* __restrict__ elem_err,
     unsigned long long* __restrict__ counters, ElemList el, const DevCtl* __restrict__ ctl,
-    int all_elems, int n_elem) {
+    int mode, int n_elem, RecPass rp) {
     extern __shared__ __align__(128) double smem_fib[];
     __shared__ DevElem E;
     __shared__ DevSection sd;
-    __shared__ ElemScratch S;
+    __shared__ union ScratchU {
+        ElemScratch s2;
+        ElemScratch3 s3;
+    } SU;
+    ElemScratch& S = SU.s2;
+    const int all_elems = mode != ELEM_MODE_LIST;
     __shared__ __align__(8) uint64_t bar;
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -913,15 +942,25 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         el.count[cur ^ 1] = 0;
         el.next[cur ^ 1] = 0;
     }
-    const int total = all_elems ? n_elem : el.count[cur];
+    const int total = mode == ELEM_MODE_ALL ? n_elem
+                    : mode == ELEM_MODE_RECORD ? rp.n : el.count[cur];
     __syncthreads();
     uint32_t phase = 0;
     bool stop = false;
     auto process = [&](const int e) -> void {
     copy_struct(&E, elems + e);
     __syncthreads();
-    if (!active[E.inst]) return;
+    if (mode == ELEM_MODE_RECORD ? status[E.inst] != 0 : !active[E.inst]) return;
     copy_struct(&sd, g.secs + E.sec);
+    if constexpr (DIM == 3) {
+        __syncthreads();
+        double* rec_out = nullptr;
+        if (mode == ELEM_MODE_RECORD)
+            rec_out = rp.hist_ef + ((size_t)ctl->step * rp.slots + rp.rece_base[E.inst] + E.rec) * rp.ef_w;
+        element3d_process(g, sd, E, e, fs, u_full, estate, ek, ef, status, elem_err, counters, SU.s3,
+                          smem_fib, &bar, phase, stop, rec_out);
+        return;
+    }
     if (tid == 0) {
         S.local_iters = 0;
         S.section_evals = 0;
@@ -1035,8 +1074,8 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
             }
         }
         __syncthreads();
-        if (tid < 36) ek[(size_t)e * 36 + tid] = S.k[tid];
-        else if (tid < 42) ef[(size_t)e * 6 + tid - 36] = S.f[tid - 36];
+        if (tid < 36) ek[E.ek_off + tid] = S.k[tid];
+        else if (tid < 42) ef[E.ef_off + tid - 36] = S.f[tid - 36];
         if (tid == 0) {
             atomicAdd(&counters[3], (unsigned long long)E.io_bytes);
             atomicAdd(&counters[1], (unsigned long long)nip);
@@ -1284,8 +1323,8 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
                                     (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
     }
     __syncthreads();
-    if (tid < 36) ek[(size_t)e * 36 + tid] = S.k[tid];
-    else if (tid < 42) ef[(size_t)e * 6 + tid - 36] = S.f[tid - 36];
+    if (tid < 36) ek[E.ek_off + tid] = S.k[tid];
+    else if (tid < 42) ef[E.ef_off + tid - 36] = S.f[tid - 36];
     };
     // first element by block index, then dynamically: thread 0 claims the next list entry while
     // the CTA works on the current one (the claim's latency hides behind the element)
@@ -1293,7 +1332,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     while (li < total && !stop) {
         int claimed = li + gridDim.x;
         if (!all_elems && tid == 0) claimed = atomicAdd(&el.next[cur], 1) + gridDim.x;
-        process(all_elems ? li : el.list[cur][li]);
+        process(mode == ELEM_MODE_ALL ? li : mode == ELEM_MODE_RECORD ? rp.list[li] : el.list[cur][li]);
         if (tid == 0) s_next = claimed;
         __syncthreads();
         li = s_next;
@@ -1311,7 +1350,7 @@ template <int TEAM>
 __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
     double* __restrict__ estate, const int* __restrict__ status, double* __restrict__ rec_base,
-    const int* __restrict__ rece_base, int rec_slots, const DevCtl* __restrict__ ctl) {
+    const int* __restrict__ rece_base, int rec_slots, int ef_w, const DevCtl* __restrict__ ctl) {
     __shared__ DevElem E;
     __shared__ DevSection sd;
     __shared__ double resp[kMaxIp][5];
@@ -1319,16 +1358,25 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
     __shared__ double ul[6];
     const int e = blockIdx.x;
     const int tid = threadIdx.x, team = tid / TEAM, r = tid % TEAM;
-    double* rec_out = rec_base ? rec_base + (size_t)ctl->step * rec_slots * 6 : nullptr;
+    double* rec_out = rec_base ? rec_base + (size_t)ctl->step * rec_slots * ef_w : nullptr;
     copy_struct(&E, elems + e);
     __syncthreads();
     if (status[E.inst] != 0) return;
     copy_struct(&sd, g.secs + E.sec);
     __syncthreads();
     const int nip = E.nip;
+    const bool three_d = E.nd == 12;
     if (team < nip) {
-        const double eps0 = estate[(size_t)e * kEStride + kEe + team];
-        const double kappa = estate[(size_t)e * kEStride + kEk + team];
+        // strain of a fiber: eps0 - y kappa (2D); eps0 + z kappa_y - y kappa_z (3D)
+        const double* es = estate + (size_t)e * kEStride;
+        const double eps0 = three_d ? es[kE3e + team] : es[kEe + team];
+        const double kappa = three_d ? es[kE3z + team] : es[kEk + team];
+        const double kappa_y = three_d ? es[kE3y + team] : 0.0;
+        const double* gz = three_d ? g.z : nullptr;
+        auto strain = [&](int gi) {
+            const double y = __ldg(g.y + gi);
+            return three_d ? eps0 + __ldg(gz + gi) * kappa_y - y * kappa : eps0 - y * kappa;
+        };
         int base = sd.geo_off;
         for (int j = r; j < sd.n_s2; j += TEAM) {
             const long long idx = E.s2_off + team * sd.n_s2 + j;
@@ -1338,8 +1386,7 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
             c.eps = F[0 * N]; c.sig = F[1 * N]; c.tan = F[2 * N]; c.epsmin = F[3 * N];
             c.epsmax = F[4 * N]; c.epspl = F[5 * N]; c.epss0 = F[6 * N]; c.sigs0 = F[7 * N];
             c.epsr = F[8 * N]; c.sigr = F[9 * N]; c.kon = fs.s2_kon[idx];
-            const double y = __ldg(g.y + base + j);
-            steel02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            steel02_trial(g.mats[__ldg(g.m + base + j)], c, strain(base + j), t);
             F[0 * N] = t.eps; F[1 * N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.epsmin;
             F[4 * N] = t.epsmax; F[5 * N] = t.epspl; F[6 * N] = t.epss0; F[7 * N] = t.sigs0;
             F[8 * N] = t.epsr; F[9 * N] = t.sigr; fs.s2_kon[idx] = t.kon;
@@ -1351,8 +1398,7 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
             const long long N = fs.c2_n;
             C2State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.ecmin = F[3 * N]; c.dept = F[4 * N];
-            const double y = __ldg(g.y + base + j);
-            concrete02_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            concrete02_trial(g.mats[__ldg(g.m + base + j)], c, strain(base + j), t);
             F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.ecmin; F[4 * N] = t.dept;
         }
         base += sd.n_c2;
@@ -1362,10 +1408,14 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
             const long long N = fs.s1_n;
             S1State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.epsp = F[3 * N]; c.alpha = F[4 * N];
-            const double y = __ldg(g.y + base + j);
-            steel01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            steel01_trial(g.mats[__ldg(g.m + base + j)], c, strain(base + j), t);
             F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.epsp; F[4 * N] = t.alpha;
         }
+    }
+    if (three_d) {
+        // 3D recorders run as a separate pass (element state determination after commit)
+        if (tid == 0 && sd.n_s1 > 0) estate[(size_t)e * kEStride + kE3cv] = 0.0;
+        return;
     }
     if (tid == 0) {
         double ug[6];
@@ -1393,7 +1443,7 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
                     f[4] -= ps;
                 }
                 f_to_global(f, E.c_sync, E.s_sync);
-                double* out = rec_out + ((size_t)rece_base[E.inst] + E.rec) * 6;
+                double* out = rec_out + ((size_t)rece_base[E.inst] + E.rec) * ef_w;
                 for (int i = 0; i < 6; ++i) out[i] = f[i];
             }
         } else {
@@ -1442,7 +1492,7 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
             f[4] -= ps;
         }
         f_to_global(f, E.c_div, E.s_div);
-        double* out = rec_out + ((size_t)rece_base[E.inst] + E.rec) * 6;
+        double* out = rec_out + ((size_t)rece_base[E.inst] + E.rec) * ef_w;
         for (int i = 0; i < 6; ++i) out[i] = f[i];
     }
 }

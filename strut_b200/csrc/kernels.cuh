@@ -7,11 +7,15 @@
 //                    one block per family: [ip0 fibers | ip1 fibers | ...] padded to 4 entries,
 //                    so every field block is a 32-byte aligned contiguous run that one
 //                    cp.async.bulk moves into shared memory.
-//   element state    80 doubles per element: q0..q2 | eps0[10] | kappa[10] | v0..v2 (the
-//                    forceBeamColumn "force_basic_q" block of loader.mojo:1757-1771; for
-//                    dispBeamColumn the section deformations of the last state determination),
-//                    then the cached section responses at those deformations
-//   element output   k (6x6 global) and f (6) per element
+//   element state    128 doubles per element.  2D: q0..q2 | eps0[10] | kappa[10] | v0..v2 (the
+//                    forceBeamColumn2d "force_basic_q" block of loader.mojo:1757-1771; for
+//                    dispBeamColumn2d the section deformations of the last state
+//                    determination), then the cached section responses at those
+//                    deformations.  3D: q0..q4 | eps0[10] | kappa_y[10] | kappa_z[10]
+//                    (forceBeamColumn3d's block, loader.mojo:1836-1840), then the cached
+//                    responses (N, My, Mz and the six flexibility terms per point)
+//   element output   k (nd x nd global) and f (nd) per element, nd = 6 (2D) or 12 (3D), at
+//                    the element's own offsets
 //   instance arrays  free-dof vectors, band Kinit, gather lists for band slots and F_int
 //
 // Trial fiber state is never written to HBM: a fiber's trial state is a pure function of its
@@ -29,13 +33,17 @@ constexpr int kMaxIp = 10;
 // Threads of an element CTA (element state determination; the commit kernel uses one team of
 // 128 (up to 5 integration points) or 64 (up to 10) threads per integration point).
 constexpr int kTeamThreads = 640;
-constexpr int kEStride = 80;  // doubles of element state
+constexpr int kEStride = 128;  // doubles of element state
 constexpr int kEq = 0, kEe = 3, kEk = 13, kEv = 23;
 // Section responses at the stored deformations (N, Mz and the 2x2 flexibility), valid flag.
 // A forceBeamColumn state determination starts by re-evaluating every section at the stored
 // deformations (force_beam_column2d.mojo:877-925); when nothing changed since the evaluation
 // that produced them, those responses are these, bit for bit.
 constexpr int kEcv = 26, kEcN = 27, kEcM = 37, kEc00 = 47, kEc01 = 57, kEc11 = 67;
+// 3D element state: basic forces, section deformations, cache flag, cached resultants
+// (N, My, Mz) and flexibilities (f11, f12, f13, f22, f23, f33) per point.
+constexpr int kE3q = 0, kE3e = 5, kE3y = 15, kE3z = 25, kE3cv = 35, kE3cs = 36, kE3cf = 66;
+static_assert(kE3cf + 6 * kMaxIp <= kEStride, "3D element state fits the stride");
 
 struct DevSection {
     int n_s2, n_c2, n_s1, n_el;
@@ -43,17 +51,23 @@ struct DevSection {
     int el_uniform;
     int init_valid;
     int all_elastic;
+    int dim, pad;
     double f00, f01, f11;
 };
 
 struct DevElem {
     int type, geom, nip, sec;
     int inst, rec;              // rec: recorder slot of this element in its instance or -1
-    int dof[6];                 // absolute indices into the concatenated full u vector
+    int nd, has_vecxz;          // element dofs (6 or 12); vecxz given (3D)
+    int dof[12];                // absolute indices into the concatenated full u vector
     int s2_off, c2_off, s1_off; // block offsets into family arrays
     int s2_blk, c2_blk, s1_blk; // block lengths (multiples of 4)
+    long long ek_off, ef_off;   // offsets of this element's k (nd x nd) and f (nd)
     double L, inv_L, c, s, c_div, s_div, L_sync, c_sync, s_sync;
     double xi[kMaxIp], w[kMaxIp];
+    // 3D: local axes (rows x, y, z) of the undeformed element, end coordinates and vecxz for
+    // the Corotational axes, torsional G and J of the section
+    double R[9], X1[3], X2[3], vxz[3], G, J;
     double io_bytes;            // algorithmic HBM bytes of one state determination
     double commit_bytes;        // algorithmic HBM bytes of one commit
 };
@@ -110,6 +124,7 @@ struct FiberState {
 
 struct Geo {
     const double* y;
+    const double* z;  // 3D sections (0 for 2D sections)
     const double* a;
     const int* m;
     const DevMat* mats;

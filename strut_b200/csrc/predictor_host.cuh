@@ -62,7 +62,8 @@ static int pred_launch(StrutHandle* h) {
                                                                  ps->d_u_alt_f, ps->d_u_alt_full);
     elem_kernel_of(h)<<<h->elem_grid, elem_block(h), h->elem_smem, h->stream>>>(
         h->d_elems, h->geo, h->fs, ps->d_u_alt_full, ps->d_estate_alt, ps->d_ek_alt, ps->d_ef_alt, h->A.active,
-        h->A.status, h->d_elem_err, h->d_counters, alt_list(h), (const DevCtl*)h->d_ctl, 0, h->n_elem);
+        h->A.status, h->d_elem_err, h->d_counters, alt_list(h), (const DevCtl*)h->d_ctl,
+        (int)ELEM_MODE_LIST, h->n_elem, rec_pass_of(h));
     CK(cudaGetLastError());
     return STRUT_OK;
 }
@@ -91,7 +92,8 @@ static int pred_add_nodes(StrutHandle* h, cudaGraph_t body, cudaGraphNode_t dep,
     TRY(add_kernel_node(&g, body, &f, 1, elem_kernel_of(h), dim3(h->elem_grid), elem_block(h), h->elem_smem,
                         (const DevElem*)h->d_elems, h->geo, h->fs, (const double*)ps->d_u_alt_full, ps->d_estate_alt,
                         ps->d_ek_alt, ps->d_ef_alt, (const int*)h->A.active, h->A.status, h->d_elem_err,
-                        h->d_counters, alt_list(h), (const DevCtl*)h->d_ctl, 0, h->n_elem));
+                        h->d_counters, alt_list(h), (const DevCtl*)h->d_ctl, (int)ELEM_MODE_LIST, h->n_elem,
+                        rec_pass_of(h)));
     *last = g;
     return STRUT_OK;
 }
@@ -109,6 +111,7 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     h->A.hist_du = nullptr;
     h->A.pred_stats = nullptr;
     if (!m) return STRUT_OK;  // detached: the plain method
+    if (h->ndf_all < 0) return fail(STRUT_UNSUPPORTED, "the learned predictor needs instances of one ndf");
     const int ndf = h->pn_ndf, n_in = 4 * ndf + 17;
     if (m->n_in != n_in || m->n_out != ndf)
         return fail(STRUT_BAD_ARG, "network must take " + std::to_string(n_in) + " features and give " +
@@ -147,8 +150,8 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
         (rc = pred_alloc(ps, &ps->d_y, (size_t)nn * ndf)) || (rc = pred_alloc(ps, &ps->d_u_alt_f, (size_t)h->n_free_total)) ||
         (rc = pred_alloc(ps, &ps->d_u_alt_full, (size_t)h->n_dofs_total)) ||
         (rc = pred_alloc(ps, &ps->d_estate_alt, (size_t)h->n_elem * kEStride)) ||
-        (rc = pred_alloc(ps, &ps->d_ek_alt, (size_t)h->n_elem * 36)) ||
-        (rc = pred_alloc(ps, &ps->d_ef_alt, (size_t)h->n_elem * 6)) ||
+        (rc = pred_alloc(ps, &ps->d_ek_alt, (size_t)h->ek_total)) ||
+        (rc = pred_alloc(ps, &ps->d_ef_alt, (size_t)h->ef_total)) ||
         (rc = pred_alloc(ps, &ps->d_stats, (size_t)2 * h->n_inst)) || (rc = pred_alloc(ps, &ps->d_next_alt, 2)))
         return bail(rc);
     auto up = [&](void* dst, const void* src, size_t bytes) -> int {

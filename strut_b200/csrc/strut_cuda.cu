@@ -97,16 +97,19 @@ double initial_tangent(const StrutUniMaterial& m) {
 // Host image of the fiber geometry and section definitions.
 struct SectionPack {
     std::vector<DevSection> secs;
-    std::vector<double> y, a;
+    std::vector<double> y, z, a;
     std::vector<int> m;
 };
 
-// Builds one FiberSection2d definition (fiber2d.mojo:3323-3455): area centroid, families,
-// initial flexibility.  mat_base offsets material indices into the global table.
+// Builds one FiberSection2d definition (fiber2d.mojo:3323-3455: area centroid, families,
+// initial flexibility) or, with dim 3, one FiberSection3d (fiber3d.mojo:633-720: centroid
+// (y_bar, z_bar) = (sum A y, sum A z) / sum A, coordinates relative to it).  Families are
+// stored in the order Steel02 | Concrete02 | Steel01 | Elastic.  mat_base offsets material
+// indices into the global table.
 int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fibers, int off,
-                 int count, int mat_base, SectionPack& sp) {
+                 int count, int mat_base, int dim, SectionPack& sp) {
     if (count <= 0) return fail(STRUT_BAD_ARG, "section without fibers");
-    double area_sum = 0.0, qz_sum = 0.0;
+    double area_sum = 0.0, qz_sum = 0.0, qy_sum = 0.0;
     for (int i = 0; i < count; ++i) {
         const StrutFiber& f = fibers[off + i];
         if (f.material < 0 || f.material >= nmat) return fail(STRUT_BAD_ARG, "fiber material out of range");
@@ -115,10 +118,12 @@ int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fiber
             t != STRUT_MAT_CONCRETE02)
             return fail(STRUT_UNSUPPORTED, "fiber material type not implemented on this path");
         area_sum += f.area;
+        qy_sum += f.area * f.z;
         qz_sum += f.area * f.y;
     }
     if (!(area_sum > 0.0)) return fail(STRUT_BAD_ARG, "section total area must be > 0");
     const double y_bar = qz_sum / area_sum;
+    const double z_bar = dim == 3 ? qy_sum / area_sum : 0.0;
     DevSection sd;
     std::memset(&sd, 0, sizeof(sd));
     sd.geo_off = (int)sp.y.size();
@@ -139,6 +144,7 @@ int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fiber
             const StrutFiber& f = fibers[off + i];
             if (mats[f.material].type != order[fam]) continue;
             sp.y.push_back(f.y - y_bar);
+            sp.z.push_back(dim == 3 ? f.z - z_bar : 0.0);
             sp.a.push_back(f.area);
             sp.m.push_back(mat_base + f.material);
             counts[fam]++;
@@ -161,8 +167,9 @@ int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fiber
             else if (E != E0) sd.el_uniform = 0;
         }
     }
+    sd.dim = dim;
     const double det = ik11 * ik22 - ik12 * ik12;
-    if (std::fabs(det) > 1.0e-40) {
+    if (dim == 2 && std::fabs(det) > 1.0e-40) {
         const double inv_det = 1.0 / det;
         sd.init_valid = 1;
         sd.f00 = ik22 * inv_det;
@@ -171,6 +178,45 @@ int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fiber
     }
     sp.secs.push_back(sd);
     return STRUT_OK;
+}
+
+// Local axes of a 3D beam-column (rows x, y, z) from its end coordinates and vecxz
+// (elements/utils.mojo:59-140; force_beam_column3d.mojo:172-222).
+bool rotation3d_host(const double* x1, const double* x2, int has_vecxz, const double* vxz,
+                     double* R) {
+    const double dx = x2[0] - x1[0], dy = x2[1] - x1[1], dz = x2[2] - x1[2];
+    const double n = std::sqrt(dx * dx + dy * dy + dz * dz);
+    if (n == 0.0) return false;
+    const double lx = dx / n, ly = dy / n, lz = dz / n;
+    double vx = 1.0, vy = 0.0, vz = 0.0;
+    if (has_vecxz) {
+        vx = vxz[0];
+        vy = vxz[1];
+        vz = vxz[2];
+    } else if (std::fabs(lx) >= 0.9) {
+        vx = 0.0;
+        vy = 1.0;
+        if (std::fabs(ly) >= 0.9) {
+            vy = 0.0;
+            vz = 1.0;
+        }
+    }
+    double yx = vy * lz - vz * ly, yy = vz * lx - vx * lz, yz = vx * ly - vy * lx;
+    const double yn = std::sqrt(yx * yx + yy * yy + yz * yz);
+    if (yn == 0.0) return false;
+    yx /= yn;
+    yy /= yn;
+    yz /= yn;
+    R[0] = lx;
+    R[1] = ly;
+    R[2] = lz;
+    R[3] = yx;
+    R[4] = yy;
+    R[5] = yz;
+    R[6] = ly * yz - lz * yy;
+    R[7] = lz * yx - lx * yz;
+    R[8] = lx * yy - ly * yx;
+    return true;
 }
 
 double path_eval(const StrutExcitation& x, double t) {
@@ -231,6 +277,12 @@ struct StrutHandle {
     std::vector<int> rec_off, n_rec, rece_off, n_rece;
     std::vector<std::vector<int>> rece_map;  // record entry -> unique element record slot
     int n_rec_total = 0, n_rece_slots = 0;
+    int ef_w = 6;                    // doubles per element record slot: 6, or 12 with 3D
+    std::vector<int> inst_nd;        // element dofs (2 ndf) of each instance
+    int ndf_all = 3;                 // ndf shared by every instance, -1 when mixed
+    int* d_rec3 = nullptr;           // recorded 3D elements (record pass after commit)
+    int n_rec3 = 0;
+    long long ek_total = 0, ef_total = 0;
     int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
     long long band_total = 0;
     int max_nip = 1;
@@ -325,7 +377,10 @@ static int prof_end(StrutHandle* h, int k) {
 // Element state kernel: kTeamThreads threads per element CTA.  Commit kernel: one team of 128
 // threads per integration point up to 5 points, else 64.
 using CommitKernel = decltype(&commit_kernel<128>);
-static decltype(&element_state_kernel) elem_kernel_of(const StrutHandle*) { return element_state_kernel; }
+using ElemKernel = decltype(&element_state_kernel<2>);
+static ElemKernel elem_kernel_of(const StrutHandle* h) {
+    return h->ndf_all == 6 ? element_state_kernel<3> : element_state_kernel<2>;
+}
 static dim3 elem_block(const StrutHandle*) { return dim3(kTeamThreads); }
 static CommitKernel commit_kernel_of(const StrutHandle* h) {
     return h->max_nip <= 5 ? commit_kernel<128> : commit_kernel<64>;
@@ -334,12 +389,35 @@ static dim3 commit_block(const StrutHandle* h) { return dim3((h->max_nip <= 5 ? 
 
 // all_elems: every element (set-up and single-iteration entries); otherwise the list of
 // elements of the instances still iterating.
+static RecPass rec_pass_of(const StrutHandle* h) {
+    RecPass rp;
+    rp.list = h->d_rec3;
+    rp.n = h->n_rec3;
+    rp.hist_ef = h->d_hist_ef;
+    rp.rece_base = h->d_rece_base;
+    rp.slots = std::max(h->n_rece_slots, 1);
+    rp.ef_w = h->ef_w;
+    return rp;
+}
+
+// Record pass of the recorded 3D beam-columns after a step's commit.
+static int launch_record_pass(StrutHandle* h) {
+    if (h->n_rec3 == 0) return STRUT_OK;
+    elem_kernel_of(h)<<<std::min(h->n_rec3, h->elem_grid), elem_block(h), h->elem_smem, h->stream>>>(
+        h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->d_ek, h->d_ef, h->A.active,
+        h->A.status, h->d_elem_err, h->d_counters, h->A.el, (const DevCtl*)h->d_ctl,
+        (int)ELEM_MODE_RECORD, h->n_elem, rec_pass_of(h));
+    CK(cudaGetLastError());
+    return STRUT_OK;
+}
+
 static int launch_elements(StrutHandle* h, int all_elems = 0) {
     if (h->prof) CK(cudaMemsetAsync(h->d_counters + 5, 0, sizeof(unsigned long long), h->stream));
     TRY(prof_begin(h));
     elem_kernel_of(h)<<<all_elems ? h->n_elem : h->elem_grid, elem_block(h), h->elem_smem, h->stream>>>(
         h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->d_ek, h->d_ef, h->A.active,
-        h->A.status, h->d_elem_err, h->d_counters, h->A.el, (const DevCtl*)h->d_ctl, all_elems, h->n_elem);
+        h->A.status, h->d_elem_err, h->d_counters, h->A.el, (const DevCtl*)h->d_ctl,
+        all_elems ? (int)ELEM_MODE_ALL : (int)ELEM_MODE_LIST, h->n_elem, rec_pass_of(h));
     CK(cudaGetLastError());
     TRY(prof_end(h, 0));
     if (h->prof) {
@@ -370,13 +448,13 @@ static int ensure_history(StrutHandle* h, int need) {
     double* ne = nullptr;
     int* ni = nullptr;
     CK(cudaMalloc((void**)&nd, (size_t)cap * std::max(h->n_rec_total, 1) * sizeof(double)));
-    CK(cudaMalloc((void**)&ne, (size_t)cap * std::max(h->n_rece_slots, 1) * 6 * sizeof(double)));
+    CK(cudaMalloc((void**)&ne, (size_t)cap * std::max(h->n_rece_slots, 1) * h->ef_w * sizeof(double)));
     CK(cudaMalloc((void**)&ni, (size_t)cap * h->n_inst * sizeof(int)));
     CK(cudaMemset(ni, 0, (size_t)cap * h->n_inst * sizeof(int)));
     if (h->hist_cap > 0 && h->steps_done > 0) {
         CK(cudaMemcpy(nd, h->d_hist_disp, (size_t)h->steps_done * std::max(h->n_rec_total, 1) * sizeof(double),
                       cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy(ne, h->d_hist_ef, (size_t)h->steps_done * std::max(h->n_rece_slots, 1) * 6 * sizeof(double),
+        CK(cudaMemcpy(ne, h->d_hist_ef, (size_t)h->steps_done * std::max(h->n_rece_slots, 1) * h->ef_w * sizeof(double),
                       cudaMemcpyDeviceToDevice));
         CK(cudaMemcpy(ni, h->d_hist_iters, (size_t)h->steps_done * h->n_inst * sizeof(int),
                       cudaMemcpyDeviceToDevice));
@@ -472,7 +550,7 @@ static int build_graph(StrutHandle* h) {
                         elem_block(h), h->elem_smem, (const DevElem*)h->d_elems, h->geo,
                         h->fs, (const double*)h->A.u_full, h->d_estate, h->d_ek, h->d_ef,
                         (const int*)h->A.active, h->A.status, h->d_elem_err, h->d_counters, h->A.el,
-                        (const DevCtl*)h->d_ctl, 0, h->n_elem));
+                        (const DevCtl*)h->d_ctl, (int)ELEM_MODE_LIST, h->n_elem, rec_pass_of(h)));
     TRY(add_kernel_node(&n_in, ibody, &n_el, 1, instance_newton_kernel, dim3(h->n_inst), dim3(256),
                         h->inst_smem, (const DevInst*)h->d_insts, A, (int)INST_MODE_NEWTON, 0));
     TRY(add_kernel_node(&n_chk, ibody, &n_in, 1, newton_check_kernel, dim3(1), dim3(32), 0, h->d_ctl,
@@ -480,8 +558,18 @@ static int build_graph(StrutHandle* h) {
     TRY(add_kernel_node(&n_commit, body, &n_inner, 1, commit_kernel_of(h), dim3(h->n_elem),
                         commit_block(h), 0, (const DevElem*)h->d_elems, h->geo, h->fs,
                         (const double*)h->A.u_full, h->d_estate, (const int*)h->A.status, h->d_hist_ef,
-                        (const int*)h->d_rece_base, std::max(h->n_rece_slots, 1), (const DevCtl*)h->d_ctl));
-    TRY(add_kernel_node(&n_post, body, &n_commit, 1, post_step_kernel, dim3((nF + tb - 1) / tb), dim3(tb), 0,
+                        (const int*)h->d_rece_base, std::max(h->n_rece_slots, 1), h->ef_w, (const DevCtl*)h->d_ctl));
+    cudaGraphNode_t n_after_commit = n_commit;
+    if (h->n_rec3 > 0) {
+        cudaGraphNode_t n_rp;
+        TRY(add_kernel_node(&n_rp, body, &n_commit, 1, elem_kernel_of(h), dim3(std::min(h->n_rec3, h->elem_grid)),
+                            elem_block(h), h->elem_smem, (const DevElem*)h->d_elems, h->geo, h->fs,
+                            (const double*)h->A.u_full, h->d_estate, h->d_ek, h->d_ef, (const int*)h->A.active,
+                            h->A.status, h->d_elem_err, h->d_counters, h->A.el, (const DevCtl*)h->d_ctl,
+                            (int)ELEM_MODE_RECORD, h->n_elem, rec_pass_of(h)));
+        n_after_commit = n_rp;
+    }
+    TRY(add_kernel_node(&n_post, body, &n_after_commit, 1, post_step_kernel, dim3((nF + tb - 1) / tb), dim3(tb), 0,
                         (const DevInst*)h->d_insts, A, (const int*)h->d_free_inst, nF));
     cudaGraphNode_t last = n_post;
     if (h->n_rec_total > 0) {
@@ -549,7 +637,15 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     h->rece_map.resize(num_instances);
     for (int inst = 0; inst < num_instances; ++inst) {
         const StrutModelDesc& d = models[inst];
-        if (d.ndm != 2 || d.ndf != 3) return bail(fail(STRUT_UNSUPPORTED, "only 2D frames (ndm 2, ndf 3)"));
+        const bool three_d = d.ndm == 3 && d.ndf == 6;
+        if (!three_d && (d.ndm != 2 || d.ndf != 3))
+            return bail(fail(STRUT_UNSUPPORTED, "frames with ndm 2, ndf 3 or ndm 3, ndf 6"));
+        const int nd = 2 * d.ndf;
+        h->inst_nd.push_back(nd);
+        if (inst == 0) h->ndf_all = d.ndf;
+        else if (h->ndf_all != d.ndf)
+            return bail(fail(STRUT_UNSUPPORTED, "a batch holds either 2D (ndf 3) or 3D (ndf 6) frames"));
+        if (three_d) h->ef_w = 12;
         if (d.num_free <= 0 || d.num_elements <= 0 || d.num_dofs != d.num_nodes * d.ndf)
             return bail(fail(STRUT_BAD_ARG, "inconsistent model sizes"));
         if (d.system != STRUT_SYSTEM_BAND_GENERAL && d.system != STRUT_SYSTEM_BAND_SPD)
@@ -563,7 +659,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         sec_base[inst] = (int)sp.secs.size();
         for (int s = 0; s < d.num_sections; ++s) {
             rc = pack_section(d.materials, d.num_materials, d.fibers, d.sections[s].fiber_offset,
-                              d.sections[s].fiber_count, mat_base, sp);
+                              d.sections[s].fiber_count, mat_base, three_d ? 3 : 2, sp);
             if (rc != STRUT_OK) return bail(rc);
         }
         // free numbering / masses
@@ -615,7 +711,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         // elements
         const int e0 = (int)elems.size();
         int bw = 0;
-        std::vector<int> efree(6 * d.num_elements);
+        std::vector<int> efree((size_t)nd * d.num_elements);
         std::vector<int> rec_slot(d.num_elements, -1);
         std::vector<int>& rmap = h->rece_map[inst];
         int nslots = 0;
@@ -627,10 +723,14 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         }
         for (int e = 0; e < d.num_elements; ++e) {
             const StrutFrameElement& ed = d.elements[e];
-            if (ed.type != STRUT_ELEM_FORCE_BEAM_COLUMN_2D && ed.type != STRUT_ELEM_DISP_BEAM_COLUMN_2D)
+            const bool el3 = ed.type == STRUT_ELEM_FORCE_BEAM_COLUMN_3D || ed.type == STRUT_ELEM_DISP_BEAM_COLUMN_3D;
+            const bool el2 = ed.type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D || ed.type == STRUT_ELEM_DISP_BEAM_COLUMN_2D;
+            if (three_d ? !el3 : !el2)
                 return bail(fail(STRUT_UNSUPPORTED, "element type not implemented on this path"));
-            if (ed.geom != STRUT_GEOM_LINEAR && ed.geom != STRUT_GEOM_PDELTA)
-                return bail(fail(STRUT_UNSUPPORTED, "geomTransf must be Linear or PDelta"));
+            if (ed.geom != STRUT_GEOM_LINEAR && ed.geom != STRUT_GEOM_PDELTA &&
+                !(three_d && ed.geom == STRUT_GEOM_COROTATIONAL))
+                return bail(fail(STRUT_UNSUPPORTED, three_d ? "geomTransf must be Linear, PDelta or Corotational"
+                                                            : "geomTransf must be Linear or PDelta"));
             if (ed.section < 0 || ed.section >= d.num_sections || ed.integration < 0 ||
                 ed.integration >= d.num_integrations)
                 return bail(fail(STRUT_BAD_ARG, "element section / integration out of range"));
@@ -645,24 +745,48 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             E.sec = sec_base[inst] + ed.section;
             E.inst = inst;
             E.rec = rec_slot[e];
-            for (int a = 0; a < 6; ++a) {
+            E.nd = nd;
+            for (int a = 0; a < nd; ++a) {
                 if (ed.dof[a] < 0 || ed.dof[a] >= d.num_dofs) return bail(fail(STRUT_BAD_ARG, "element dof out of range"));
                 E.dof[a] = u_off + ed.dof[a];
-                efree[6 * e + a] = free_of_dof[ed.dof[a]];
+                efree[(size_t)nd * e + a] = free_of_dof[ed.dof[a]];
             }
-            const double x1 = d.node_coords[2 * ed.node_i], y1 = d.node_coords[2 * ed.node_i + 1];
-            const double x2 = d.node_coords[2 * ed.node_j], y2 = d.node_coords[2 * ed.node_j + 1];
-            const double dx = x2 - x1, dy = y2 - y1;
-            E.L = std::hypot(dx, dy);
-            if (E.L == 0.0) return bail(fail(STRUT_BAD_ARG, "zero-length element"));
-            E.inv_L = 1.0 / E.L;
-            E.c = dx * E.inv_L;
-            E.s = dy * E.inv_L;
-            E.c_div = dx / E.L;
-            E.s_div = dy / E.L;
-            E.L_sync = std::sqrt(dx * dx + dy * dy);
-            E.c_sync = dx / E.L_sync;
-            E.s_sync = dy / E.L_sync;
+            if (ed.node_i < 0 || ed.node_i >= d.num_nodes || ed.node_j < 0 || ed.node_j >= d.num_nodes)
+                return bail(fail(STRUT_BAD_ARG, "element node out of range"));
+            if (three_d) {
+                for (int c = 0; c < 3; ++c) {
+                    E.X1[c] = d.node_coords[3 * ed.node_i + c];
+                    E.X2[c] = d.node_coords[3 * ed.node_j + c];
+                    E.vxz[c] = ed.vecxz[c];
+                }
+                E.has_vecxz = ed.has_vecxz ? 1 : 0;
+                const double dx = E.X2[0] - E.X1[0], dy = E.X2[1] - E.X1[1], dz = E.X2[2] - E.X1[2];
+                E.L = std::sqrt(dx * dx + dy * dy + dz * dz);
+                if (E.L == 0.0) return bail(fail(STRUT_BAD_ARG, "zero-length element"));
+                E.inv_L = 1.0 / E.L;
+                if (!rotation3d_host(E.X1, E.X2, E.has_vecxz, E.vxz, E.R))
+                    return bail(fail(STRUT_BAD_ARG, "invalid beam3d vecxz orientation"));
+                E.G = d.sections[ed.section].G;
+                E.J = d.sections[ed.section].J;
+            } else {
+                const double x1 = d.node_coords[2 * ed.node_i], y1 = d.node_coords[2 * ed.node_i + 1];
+                const double x2 = d.node_coords[2 * ed.node_j], y2 = d.node_coords[2 * ed.node_j + 1];
+                const double dx = x2 - x1, dy = y2 - y1;
+                E.L = std::hypot(dx, dy);
+                if (E.L == 0.0) return bail(fail(STRUT_BAD_ARG, "zero-length element"));
+                E.inv_L = 1.0 / E.L;
+                E.c = dx * E.inv_L;
+                E.s = dy * E.inv_L;
+                E.c_div = dx / E.L;
+                E.s_div = dy / E.L;
+                E.L_sync = std::sqrt(dx * dx + dy * dy);
+                E.c_sync = dx / E.L_sync;
+                E.s_sync = dy / E.L_sync;
+            }
+            E.ek_off = h->ek_total;
+            E.ef_off = h->ef_total;
+            h->ek_total += (long long)nd * nd;
+            h->ef_total += nd;
             for (int ip = 0; ip < E.nip; ++ip) {
                 E.xi[ip] = r.xi[ip];
                 E.w[ip] = r.w[ip];
@@ -683,7 +807,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
             const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) + 4 * (size_t)E.s2_blk +
                                 8 * (size_t)(5 * E.c2_blk + 12 * E.s2_blk) +
-                                8 * (size_t)(((n_tot + 1) & ~1) + 2 * E.nip * n_tot);
+                                8 * (size_t)((three_d ? 2 : 1) * ((n_tot + 1) & ~1) + 2 * E.nip * n_tot);
             h->elem_smem = std::max(h->elem_smem, smem);
             h->elem_fibers.push_back((long long)E.nip * (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
             {
@@ -691,16 +815,16 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
                 // doubles + kon), element state read + written, k and f written, 6 dofs read,
                 // the element record itself
                 const double fib = (double)E.nip * (40.0 * sd.n_c2 + 84.0 * sd.n_s2 + 40.0 * sd.n_s1);
-                const double est = 8.0 * (6 + 2 * E.nip);
-                E.io_bytes = fib + 2.0 * est + 8.0 * 42 + 8.0 * 6 + (double)sizeof(DevElem);
-                E.commit_bytes = 2.0 * fib + est + 8.0 * 6 + (double)sizeof(DevElem);
+                const double est = three_d ? 8.0 * (5 + 3 * E.nip) : 8.0 * (6 + 2 * E.nip);
+                E.io_bytes = fib + 2.0 * est + 8.0 * (nd * nd + nd) + 8.0 * nd + (double)sizeof(DevElem);
+                E.commit_bytes = 2.0 * fib + est + 8.0 * nd + (double)sizeof(DevElem);
             }
             elems.push_back(E);
-            for (int a = 0; a < 6; ++a) {
-                const int ia = efree[6 * e + a];
+            for (int a = 0; a < nd; ++a) {
+                const int ia = efree[(size_t)nd * e + a];
                 if (ia < 0) continue;
-                for (int b = a + 1; b < 6; ++b) {
-                    const int ib = efree[6 * e + b];
+                for (int b = a + 1; b < nd; ++b) {
+                    const int ib = efree[(size_t)nd * e + b];
                     if (ib < 0) continue;
                     bw = std::max(bw, std::abs(ia - ib));
                 }
@@ -711,15 +835,16 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         std::vector<std::vector<int>> slots((size_t)nf * rw);
         std::vector<std::vector<int>> fcontr(nf);
         for (int e = 0; e < d.num_elements; ++e) {
-            for (int a = 0; a < 6; ++a) {
-                const int ia = efree[6 * e + a];
+            const DevElem& E = elems[e0 + e];
+            for (int a = 0; a < nd; ++a) {
+                const int ia = efree[(size_t)nd * e + a];
                 if (ia < 0) continue;
-                for (int b = 0; b < 6; ++b) {
-                    const int ib = efree[6 * e + b];
+                for (int b = 0; b < nd; ++b) {
+                    const int ib = efree[(size_t)nd * e + b];
                     if (ib < 0) continue;
-                    slots[(size_t)ia * rw + (ib - ia + bw)].push_back((e0 + e) * 36 + a * 6 + b);
+                    slots[(size_t)ia * rw + (ib - ia + bw)].push_back((int)(E.ek_off + a * nd + b));
                 }
-                fcontr[ia].push_back((e0 + e) * 6 + a);
+                fcontr[ia].push_back((int)(E.ef_off + a));
             }
         }
         for (auto& v : slots) {
@@ -833,13 +958,24 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     // geometry and definitions
     DevMat* d_mats;
     DevSection* d_secs;
-    double *d_y, *d_a;
+    double *d_y, *d_z, *d_a;
     int* d_m;
     if ((rc = upload(&d_mats, mats, al)) || (rc = upload(&d_secs, sp.secs, al)) ||
-        (rc = upload(&d_y, sp.y, al)) || (rc = upload(&d_a, sp.a, al)) || (rc = upload(&d_m, sp.m, al)) ||
-        (rc = upload(&h->d_elems, elems, al)) || (rc = upload(&h->d_insts, h->insts, al)))
+        (rc = upload(&d_y, sp.y, al)) || (rc = upload(&d_z, sp.z, al)) || (rc = upload(&d_a, sp.a, al)) ||
+        (rc = upload(&d_m, sp.m, al)) || (rc = upload(&h->d_elems, elems, al)) ||
+        (rc = upload(&h->d_insts, h->insts, al)))
         return bail(rc);
+    {
+        // recorded 3D beam-columns: their recorded force comes from a state determination after
+        // the step's commit
+        std::vector<int> rec3;
+        for (int e = 0; e < (int)elems.size(); ++e)
+            if (elems[e].nd == 12 && elems[e].rec >= 0) rec3.push_back(e);
+        h->n_rec3 = (int)rec3.size();
+        if ((rc = upload(&h->d_rec3, rec3, al))) return bail(rc);
+    }
     h->geo.y = d_y;
+    h->geo.z = d_z;
     h->geo.a = d_a;
     h->geo.m = d_m;
     h->geo.mats = d_mats;
@@ -889,8 +1025,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     std::memset(&A, 0, sizeof(A));
     const size_t nF = h->n_free_total;
     if ((rc = dzeros(&h->d_estate, (size_t)h->n_elem * kEStride, al)) ||
-        (rc = dzeros(&h->d_ek, (size_t)h->n_elem * 36, al)) ||
-        (rc = dzeros(&h->d_ef, (size_t)h->n_elem * 6, al)) || (rc = dzeros(&A.u_f, nF, al)) ||
+        (rc = dzeros(&h->d_ek, (size_t)h->ek_total, al)) ||
+        (rc = dzeros(&h->d_ef, (size_t)h->ef_total, al)) || (rc = dzeros(&A.u_f, nF, al)) ||
         (rc = dzeros(&A.v_f, nF, al)) || (rc = dzeros(&A.a_f, nF, al)) ||
         (rc = dzeros(&A.u_n, nF, al)) || (rc = dzeros(&A.v_n, nF, al)) ||
         (rc = dzeros(&A.a_n, nF, al)) || (rc = dzeros(&A.P_f, nF, al)) ||
@@ -1070,8 +1206,9 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             TRY(prof_begin(h));
             commit_kernel_of(h)<<<h->n_elem, commit_block(h), 0, h->stream>>>(
                 h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, h->d_hist_ef, h->d_rece_base,
-                std::max(h->n_rece_slots, 1), h->d_ctl);
+                std::max(h->n_rece_slots, 1), h->ef_w, h->d_ctl);
             CK(cudaGetLastError());
+            TRY(launch_record_pass(h));
             TRY(prof_end(h, 2));
             TRY(prof_begin(h));
             post_step_kernel<<<(nF + tb - 1) / tb, tb, 0, h->stream>>>(h->d_insts, h->A, h->d_free_inst, nF);
@@ -1162,15 +1299,15 @@ int strut_gpu_get_history(StrutHandle* h, int32_t instance, double* disp, double
                 disp[(size_t)s * h->n_rec[instance] + j] = all[(size_t)s * h->n_rec_total + h->rec_off[instance] + j];
     }
     if (eforce && !h->rece_map[instance].empty()) {
-        const int slots = std::max(h->n_rece_slots, 1);
-        std::vector<double> all((size_t)S * slots * 6);
+        const int slots = std::max(h->n_rece_slots, 1), W = h->ef_w, nd = h->inst_nd[instance];
+        std::vector<double> all((size_t)S * slots * W);
         CK(cudaMemcpy(all.data(), h->d_hist_ef, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
         const auto& mp = h->rece_map[instance];
         for (int s = 0; s < S; ++s)
             for (size_t j = 0; j < mp.size(); ++j)
-                for (int c = 0; c < 6; ++c)
-                    eforce[((size_t)s * mp.size() + j) * 6 + c] =
-                        all[((size_t)s * slots + h->rece_off[instance] + mp[j]) * 6 + c];
+                for (int c = 0; c < nd; ++c)
+                    eforce[((size_t)s * mp.size() + j) * nd + c] =
+                        all[((size_t)s * slots + h->rece_off[instance] + mp[j]) * W + c];
     }
     if (iters) {
         std::vector<int> all((size_t)S * h->n_inst);
@@ -1193,16 +1330,17 @@ int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int3
                 for (int j = 0; j < h->n_rec[i]; ++j) disp[o++] = all[(size_t)s * h->n_rec_total + h->rec_off[i] + j];
     }
     if (eforce) {
-        const int slots = std::max(h->n_rece_slots, 1);
-        std::vector<double> all((size_t)S * slots * 6);
+        const int slots = std::max(h->n_rece_slots, 1), W = h->ef_w;
+        std::vector<double> all((size_t)S * slots * W);
         CK(cudaMemcpy(all.data(), h->d_hist_ef, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
         size_t o = 0;
         for (int i = 0; i < h->n_inst; ++i) {
             const auto& mp = h->rece_map[i];
+            const int nd = h->inst_nd[i];
             for (int s = 0; s < S; ++s)
                 for (size_t j = 0; j < mp.size(); ++j)
-                    for (int c = 0; c < 6; ++c)
-                        eforce[o++] = all[((size_t)s * slots + h->rece_off[i] + mp[j]) * 6 + c];
+                    for (int c = 0; c < nd; ++c)
+                        eforce[o++] = all[((size_t)s * slots + h->rece_off[i] + mp[j]) * W + c];
         }
     }
     if (iters) {
@@ -1319,7 +1457,8 @@ int strut_gpu_factor_solve(StrutHandle* h, const double* rhs, double* du) {
 int strut_gpu_commit(StrutHandle* h) {
     if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
     commit_kernel_of(h)<<<h->n_elem, commit_block(h), 0, h->stream>>>(
-        h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, nullptr, h->d_rece_base, 1, h->d_ctl);
+        h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->A.status, nullptr, h->d_rece_base, 1,
+        h->ef_w, h->d_ctl);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
     return STRUT_OK;
@@ -1375,7 +1514,7 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
     if (!materials || !fibers || num_fibers <= 0 || n_inst <= 0 || !out) return fail(STRUT_BAD_ARG, "bad arguments");
     *out = nullptr;
     SectionPack sp;
-    int rc = pack_section(materials, num_materials, fibers, 0, num_fibers, 0, sp);
+    int rc = pack_section(materials, num_materials, fibers, 0, num_fibers, 0, 2, sp);
     if (rc != STRUT_OK) return rc;
     std::vector<DevMat> mats;
     for (int i = 0; i < num_materials; ++i) mats.push_back(make_devmat(materials[i]));

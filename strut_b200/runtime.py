@@ -98,7 +98,7 @@ class Analysis:
         m = self.models[instance]
         S = self.steps_done
         disp = np.zeros((S, max(len(m.record_dofs), 1)))
-        ef = np.zeros((S, max(len(m.record_elements), 1), 6))
+        ef = np.zeros((S, max(len(m.record_elements), 1), 2 * m.ndf))
         it = np.zeros(S, dtype=np.int32)
         _check(
             lib().strut_gpu_get_history(self.h, instance, _d(disp), _d(ef), it.ctypes.data_as(_ip)),
@@ -109,9 +109,9 @@ class Analysis:
     def history_all(self):
         S = self.steps_done
         nd = sum(len(m.record_dofs) for m in self.models)
-        ne = sum(len(m.record_elements) for m in self.models)
+        ne = sum(len(m.record_elements) * 2 * m.ndf for m in self.models)
         disp = np.zeros(max(S * nd, 1))
-        ef = np.zeros(max(S * ne * 6, 1))
+        ef = np.zeros(max(S * ne, 1))
         it = np.zeros(max(S * len(self.models), 1), dtype=np.int32)
         _check(
             lib().strut_gpu_get_history_all(self.h, _d(disp), _d(ef), it.ctypes.data_as(_ip)),
