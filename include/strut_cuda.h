@@ -280,6 +280,12 @@ int strut_gpu_revert(StrutHandle* h);
 int strut_gpu_section_path(const StrutUniMaterial* materials, int32_t num_materials,
                            const StrutFiber* fibers, int32_t num_fibers,
                            const double* eps0_kappa, int32_t n_points, double* out);
+/* section_path for one FiberSection3d (section_path.mojo:463-556): a path of (eps0, kappa_y,
+ * kappa_z) triples, committed after each point.  out: n_points x 9 = N, My, Mz, k11, k12, k13,
+ * k22, k23, k33 (fiber3d.mojo:769-836). */
+int strut_gpu_section3d_path(const StrutUniMaterial* materials, int32_t num_materials,
+                             const StrutFiber* fibers, int32_t num_fibers, const double* path,
+                             int32_t n_points, double* out);
 /* material_path: one uniaxial material, a strain history, commit after each strain (the
  * scalar uniaxial path of materials/uniaxial/ops.mojo:117-174). out: n x 2 stress, tangent. */
 int strut_gpu_material_path(const StrutUniMaterial* material, const double* strains,

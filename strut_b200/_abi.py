@@ -222,6 +222,11 @@ EXPORTS = {
         [C.POINTER(StrutUniMaterial), C.c_int32, C.POINTER(StrutFiber), C.c_int32, _dp,
          C.c_int32, _dp],
     ),
+    "strut_gpu_section3d_path": (
+        C.c_int,
+        [C.POINTER(StrutUniMaterial), C.c_int32, C.POINTER(StrutFiber), C.c_int32, _dp,
+         C.c_int32, _dp],
+    ),
     "strut_gpu_material_path": (
         C.c_int, [C.POINTER(StrutUniMaterial), _dp, C.c_int32, _dp]
     ),

@@ -1508,6 +1508,41 @@ int strut_gpu_material_path(const StrutUniMaterial* material, const double* stra
     return STRUT_OK;
 }
 
+}  // extern "C"
+
+// Initial committed state (UniMaterialState(mat_def), core.mojo:203-263) of n_inst copies of
+// the section sp.secs[0], laid out as section_batch_kernel reads it.
+static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>& mats, long long n_inst,
+                                std::vector<double>& s2, std::vector<double>& c2, std::vector<double>& s1,
+                                std::vector<int>& kon) {
+    const DevSection& sd = sp.secs[0];
+    const long long n2 = n_inst * sd.n_s2, n3 = n_inst * sd.n_c2, n1 = n_inst * sd.n_s1;
+    s2.assign(10 * std::max<long long>(n2, 1), 0.0);
+    c2.assign(5 * std::max<long long>(n3, 1), 0.0);
+    s1.assign(5 * std::max<long long>(n1, 1), 0.0);
+    kon.assign(std::max<long long>(n2, 1), 0);
+    for (long long i = 0; i < n_inst; ++i) {
+        int base = sd.geo_off;
+        for (int j = 0; j < sd.n_s2; ++j) {
+            const DevMat& m = mats[sp.m[base + j]];
+            const long long idx = i * sd.n_s2 + j;
+            s2[2 * n2 + idx] = m.p[1];
+            s2[4 * n2 + idx] = m.k[S2K_EPSY];
+            s2[3 * n2 + idx] = -m.k[S2K_EPSY];
+            if (m.p[10] != 0.0) {
+                s2[idx] = m.k[S2K_SIGINI_E0];
+                s2[n2 + idx] = m.p[10];
+            }
+        }
+        base += sd.n_s2;
+        for (int j = 0; j < sd.n_c2; ++j) c2[2 * n3 + i * sd.n_c2 + j] = mats[sp.m[base + j]].k[C2K_EC0];
+        base += sd.n_c2;
+        for (int j = 0; j < sd.n_s1; ++j) s1[2 * n1 + i * sd.n_s1 + j] = mats[sp.m[base + j]].p[1];
+    }
+}
+
+extern "C" {
+
 int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t num_materials,
                                    const StrutFiber* fibers, int32_t num_fibers, int32_t n_inst,
                                    StrutSectionBatch** out) {
@@ -1536,29 +1571,9 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
     b->geo.m = d_m;
     b->geo.mats = d_mats;
     b->geo.secs = d_secs;
-    const DevSection& sd = b->sd;
-    const long long n2 = (long long)n_inst * sd.n_s2, n3 = (long long)n_inst * sd.n_c2, n1 = (long long)n_inst * sd.n_s1;
-    std::vector<double> s2(10 * std::max<long long>(n2, 1), 0.0), c2(5 * std::max<long long>(n3, 1), 0.0),
-        s1(5 * std::max<long long>(n1, 1), 0.0);
-    std::vector<int> kon(std::max<long long>(n2, 1), 0);
-    for (long long i = 0; i < n_inst; ++i) {
-        int base = sd.geo_off;
-        for (int j = 0; j < sd.n_s2; ++j) {
-            const DevMat& m = mats[sp.m[base + j]];
-            const long long idx = i * sd.n_s2 + j;
-            s2[2 * n2 + idx] = m.p[1];
-            s2[4 * n2 + idx] = m.k[S2K_EPSY];
-            s2[3 * n2 + idx] = -m.k[S2K_EPSY];
-            if (m.p[10] != 0.0) {
-                s2[idx] = m.k[S2K_SIGINI_E0];
-                s2[n2 + idx] = m.p[10];
-            }
-        }
-        base += sd.n_s2;
-        for (int j = 0; j < sd.n_c2; ++j) c2[2 * n3 + i * sd.n_c2 + j] = mats[sp.m[base + j]].k[C2K_EC0];
-        base += sd.n_c2;
-        for (int j = 0; j < sd.n_s1; ++j) s1[2 * n1 + i * sd.n_s1 + j] = mats[sp.m[base + j]].p[1];
-    }
+    std::vector<double> s2, c2, s1;
+    std::vector<int> kon;
+    batch_initial_state(sp, mats, n_inst, s2, c2, s1, kon);
     if ((rc = upload(&b->bs.s2, s2, al)) || (rc = upload(&b->bs.c2, c2, al)) || (rc = upload(&b->bs.s1, s1, al)) ||
         (rc = upload(&b->bs.kon, kon, al))) {
         delete b;
@@ -1639,6 +1654,53 @@ int strut_gpu_section_path(const StrutUniMaterial* materials, int32_t num_materi
     strut_gpu_section_batch_destroy(b);
     if (e != cudaSuccess) return fail(STRUT_CUDA_ERROR, cudaGetErrorString(e));
     return rc;
+}
+
+int strut_gpu_section3d_path(const StrutUniMaterial* materials, int32_t num_materials,
+                             const StrutFiber* fibers, int32_t num_fibers, const double* path,
+                             int32_t n_points, double* out) {
+    if (!materials || !fibers || num_fibers <= 0 || n_points < 0 || (n_points > 0 && (!path || !out)))
+        return fail(STRUT_BAD_ARG, "bad arguments");
+    SectionPack sp;
+    int rc = pack_section(materials, num_materials, fibers, 0, num_fibers, 0, 3, sp);
+    if (rc != STRUT_OK) return rc;
+    if (n_points == 0) return STRUT_OK;
+    std::vector<DevMat> mats;
+    for (int i = 0; i < num_materials; ++i) mats.push_back(make_devmat(materials[i]));
+    std::vector<double> s2, c2, s1;
+    std::vector<int> kon;
+    batch_initial_state(sp, mats, 1, s2, c2, s1, kon);
+    std::vector<void*> al;
+    auto cleanup = [&]() {
+        for (void* p : al) cudaFree(p);
+    };
+    DevMat* d_mats = nullptr;
+    double *d_y = nullptr, *d_z = nullptr, *d_a = nullptr, *d_path = nullptr, *d_out = nullptr;
+    int* d_m = nullptr;
+    BatchState bs;
+    std::memset(&bs, 0, sizeof(bs));
+    std::vector<double> pv(path, path + 3 * (size_t)n_points);
+    if ((rc = upload(&d_mats, mats, al)) || (rc = upload(&d_y, sp.y, al)) || (rc = upload(&d_z, sp.z, al)) ||
+        (rc = upload(&d_a, sp.a, al)) || (rc = upload(&d_m, sp.m, al)) || (rc = upload(&bs.s2, s2, al)) ||
+        (rc = upload(&bs.c2, c2, al)) || (rc = upload(&bs.s1, s1, al)) || (rc = upload(&bs.kon, kon, al)) ||
+        (rc = upload(&d_path, pv, al)) || (rc = dzeros(&d_out, 9 * (size_t)n_points, al))) {
+        cleanup();
+        return rc;
+    }
+    bs.n_inst = 1;
+    Geo g;
+    std::memset(&g, 0, sizeof(g));
+    g.y = d_y;
+    g.z = d_z;
+    g.a = d_a;
+    g.m = d_m;
+    g.mats = d_mats;
+    section3d_path_kernel<<<1, 32>>>(g, sp.secs[0], bs, d_path, n_points, d_out);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out, d_out, 9 * (size_t)n_points * sizeof(double), cudaMemcpyDeviceToHost);
+    cleanup();
+    if (e != cudaSuccess) return fail(STRUT_CUDA_ERROR, cudaGetErrorString(e));
+    return STRUT_OK;
 }
 
 }  // extern "C"

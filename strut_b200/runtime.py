@@ -184,6 +184,15 @@ def section_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
     return out
 
 
+def section3d_path(mats, nmat, fibs, nfib, path) -> np.ndarray:
+    """FiberSection3d along (eps0, kappa_y, kappa_z) points -> (n, 9) responses."""
+    p = np.ascontiguousarray(path, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((len(p), 9))
+    _check(lib().strut_gpu_section3d_path(mats, nmat, fibs, nfib, _d(p), len(p), _d(out)),
+           "strut_gpu_section3d_path")
+    return out
+
+
 class SectionBatch:
     """n_inst independent histories of one FiberSection2d (device-resident)."""
 

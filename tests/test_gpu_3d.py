@@ -103,3 +103,24 @@ def test_mixed_2d_3d_batch_is_rejected(gpu_lib):
     m3 = M.Model(W.rc_frame3d_case(stories=1, bays_x=1, bays_y=1, steps=5))
     with pytest.raises(RuntimeError):
         gpu_lib.Analysis([m2, m3])
+
+
+def test_section3d_path_rc_cyclic(gpu_lib, oracle):
+    """The RC FiberSection3d along a biaxial cyclic path with commits (KAT driver form)."""
+    from tests.helpers import lcg_strains
+
+    mats = [{"id": 1, "type": "Concrete02", "params": dict(W.CORE)},
+            {"id": 2, "type": "Concrete02", "params": dict(W.COVER)},
+            {"id": 3, "type": "Steel02", "params": dict(W.STEEL)},
+            {"id": 4, "type": "Elastic", "params": {"E": 30.0e9}}]
+    sec = W.rc_section(1, 0.4, 0.6, three_d=True)
+    sec["params"]["fibers"] = [{"y": 0.05, "z": 0.02, "area": 1e-3, "material": 4}]
+    m, nm, f, nf = M.section_fibers(sec, mats)
+    n = 400
+    path = np.stack([lcg_strains(1, n, 2.0e-4, "walk") - 3.0e-4,
+                     lcg_strains(2, n, 3.0e-3, "cyclic") * 0.01,
+                     lcg_strains(3, n, 4.0e-3, "cyclic") * 0.01], 1)
+    ref = oracle.section3d_path(m, nm, f, nf, path)
+    got = gpu_lib.section3d_path(m, nm, f, nf, path)
+    scale = np.maximum(np.abs(ref).max(0), 1e-30)
+    assert np.all(np.abs(got - ref).max(0) <= 1e-9 * scale)
