@@ -85,7 +85,8 @@ struct DevInst {
     double io_bytes;  // algorithmic HBM bytes of one Newton iteration of this instance
     long long dense_off;  // offset of this instance's n x n fallback scratch
     int elem_off, n_elem; // this instance's elements (contiguous)
-    int pad_e0, pad_e1;
+    int large, large_idx; // band in global memory (too large for shared memory), its index
+    long long lband_off;  // offset of its band in the global band buffer
 };
 
 // Elements of the instances still iterating, rebuilt every Newton iteration and double

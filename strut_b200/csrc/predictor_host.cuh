@@ -112,6 +112,8 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     h->A.pred_stats = nullptr;
     if (!m) return STRUT_OK;  // detached: the plain method
     if (h->ndf_all < 0) return fail(STRUT_UNSUPPORTED, "the learned predictor needs instances of one ndf");
+    if (h->n_large > 0)
+        return fail(STRUT_UNSUPPORTED, "the learned predictor runs on instances whose band fits in shared memory");
     const int ndf = h->pn_ndf, n_in = 4 * ndf + 17;
     if (m->n_in != n_in || m->n_out != ndf)
         return fail(STRUT_BAD_ARG, "network must take " + std::to_string(n_in) + " features and give " +

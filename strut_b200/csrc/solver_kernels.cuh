@@ -60,6 +60,11 @@ struct InstArrays {
     long long* pred_stats;  // per instance: first iterations offered, learned guess chosen
     double* hist_du;        // 4 x n_free ring of converged increments (slot = step % 4)
     int n_free_total;
+    int n_inst;
+    // instances whose band lives in global memory
+    double* lband;          // effective band (factored in place), at DevInst::lband_off
+    int* lstatus;           // per large instance: 0 factored, 2 singular, 6 dense fallback,
+                            // 7 converged before the solve (NormUnbalance), -1 not active
 };
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -389,6 +394,9 @@ __device__ void dense_solve_warp(const double* D, const int* piv, int n, const d
     }
 }
 
+__device__ void newton_tail(const DevInst& I, InstArrays& A, int inst, const double* du,
+                            const double* R, int* hrow, double* red, int* red_r);
+
 __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __restrict__ insts,
                                                               InstArrays A0, int mode, int step) {
     InstArrays A = A0;
@@ -404,6 +412,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
         for (int i = tid; i < (int)(sizeof(DevInst) / 4); i += nt) d[i] = s[i];
     }
     __syncthreads();
+    if (I.large) return;  // global-memory band path (largeband_kernels.cuh)
     if (mode == INST_MODE_NEWTON && !A.active[inst]) return;
     if (mode == INST_MODE_NEWTON && A.dual && A.ctl && A.ctl->iter == 0) {
         // first iteration with a learned guess: both guesses were evaluated; keep the learned
@@ -609,6 +618,16 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
         for (int i = tid; i < n; i += nt) A.du[f0 + i] = du[i];
         return;
     }
+    newton_tail(I, A, inst, du, R, hrow, red, red_r);
+}
+
+// Displacement update, convergence test (NormDispIncr after the update,
+// transient_nonlinear.mojo:2539, 2798-2811; EnergyIncr, MaxDispIncr) and, for an instance that
+// keeps iterating, its elements appended to the next element list.  Collective over the CTA.
+__device__ void newton_tail(const DevInst& I, InstArrays& A, int inst, const double* du,
+                            const double* R, int* hrow, double* red, int* red_r) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = I.n, f0 = I.f_off;
     double ss = 0.0, en = 0.0, mx = 0.0;
     for (int i = tid; i < n; i += nt) {
         const int gi = f0 + i;

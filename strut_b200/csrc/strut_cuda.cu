@@ -26,6 +26,7 @@
 #include "element_kernels.cuh"
 #include "kat_kernels.cuh"
 #include "solver_kernels.cuh"
+#include "largeband_kernels.cuh"
 #include "predictor_kernels.cuh"
 
 using namespace strut;
@@ -283,6 +284,17 @@ struct StrutHandle {
     int* d_rec3 = nullptr;           // recorded 3D elements (record pass after commit)
     int n_rec3 = 0;
     long long ek_total = 0, ef_total = 0;
+    // instances whose band is factored in global memory
+    int n_large = 0, large_rows = 0, max_large_n = 0, lfactor_grid = 1;
+    long long lband_total = 0;
+    size_t lfactor_smem = 16, ldense_smem = 16;
+    std::vector<int> large_list_h;
+    int* d_large_list = nullptr;
+    int* d_large_rowbase = nullptr;
+    GridBarrier* d_gb = nullptr;
+    double* d_wbuf = nullptr;
+    double* d_ldense = nullptr;
+    int* d_lpiv = nullptr;
     int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
     long long band_total = 0;
     int max_nip = 1;
@@ -430,6 +442,41 @@ static int launch_elements(StrutHandle* h, int all_elems = 0) {
     return STRUT_OK;
 }
 
+// Instances with a global-memory band: assembly (or the exported band), cooperative blocked LU,
+// substitution + update + test, dense fallback.  mode as the instance kernel; EXPORT stops after
+// the assembly.
+static int launch_large(StrutHandle* h, int mode, const DevInst* insts = nullptr, InstArrays* Aover = nullptr) {
+    if (h->n_large == 0) return STRUT_OK;
+    InstArrays A = Aover ? *Aover : h->A;
+    if (!Aover) A.bytes_counter = h->d_counters + 4;
+    if (!insts) insts = h->d_insts;
+    if (mode == INST_MODE_SOLVE_EXPORTED) {
+        large_load_exported_kernel<<<dim3(64, h->n_large), 256, 0, h->stream>>>(insts, A, h->d_large_list,
+                                                                                h->n_large, h->d_gb);
+    } else {
+        const int blocks = (h->large_rows * 32 + 255) / 256;
+        large_assemble_kernel<<<blocks, 256, 0, h->stream>>>(insts, A, h->d_large_list, h->d_large_rowbase,
+                                                            h->n_large, h->large_rows, mode, h->d_gb);
+    }
+    CK(cudaGetLastError());
+    if (mode == INST_MODE_EXPORT) return STRUT_OK;
+    {
+        int n_large = h->n_large;
+        GridBarrier* gb = h->d_gb;
+        const int* ll = h->d_large_list;
+        void* args[] = {(void*)&insts, (void*)&A, (void*)&ll, (void*)&n_large, (void*)&mode, (void*)&gb};
+        CK(cudaLaunchCooperativeKernel((const void*)large_factor_kernel, dim3(h->lfactor_grid),
+                                       dim3(kLargeThreads), args, h->lfactor_smem, h->stream));
+    }
+    large_solve_kernel<<<h->n_large, kSolveThreads, 0, h->stream>>>(insts, A, h->d_large_list, h->n_large, mode,
+                                                                    h->d_wbuf, h->d_gb);
+    CK(cudaGetLastError());
+    large_dense_kernel<<<1, 256, h->ldense_smem, h->stream>>>(insts, A, h->d_large_list, h->n_large, mode,
+                                                               h->d_ldense, h->d_lpiv, h->d_wbuf);
+    CK(cudaGetLastError());
+    return STRUT_OK;
+}
+
 static int launch_instances(StrutHandle* h, int mode, int step) {
     InstArrays A = h->A;
     A.hist_iters = (mode == INST_MODE_NEWTON && step >= 0) ? h->d_hist_iters : nullptr;
@@ -437,6 +484,7 @@ static int launch_instances(StrutHandle* h, int mode, int step) {
     TRY(prof_begin(h));
     instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(h->d_insts, A, mode, step);
     CK(cudaGetLastError());
+    TRY(launch_large(h, mode));
     TRY(prof_end(h, 1));
     return STRUT_OK;
 }
@@ -553,7 +601,8 @@ static int build_graph(StrutHandle* h) {
                         (const DevCtl*)h->d_ctl, (int)ELEM_MODE_LIST, h->n_elem, rec_pass_of(h)));
     TRY(add_kernel_node(&n_in, ibody, &n_el, 1, instance_newton_kernel, dim3(h->n_inst), dim3(256),
                         h->inst_smem, (const DevInst*)h->d_insts, A, (int)INST_MODE_NEWTON, 0));
-    TRY(add_kernel_node(&n_chk, ibody, &n_in, 1, newton_check_kernel, dim3(1), dim3(32), 0, h->d_ctl,
+    cudaGraphNode_t n_before_chk = n_in;
+    TRY(add_kernel_node(&n_chk, ibody, &n_before_chk, 1, newton_check_kernel, dim3(1), dim3(32), 0, h->d_ctl,
                         (const int*)h->A.nactive, inner, 1));
     TRY(add_kernel_node(&n_commit, body, &n_inner, 1, commit_kernel_of(h), dim3(h->n_elem),
                         commit_block(h), 0, (const DevElem*)h->d_elems, h->geo, h->fs,
@@ -866,7 +915,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         I.band_off = band_off;
         I.slot_ptr_off = band_off;
         I.dense_off = dense_off;
-        dense_off += (long long)nf * nf;
+        if ((size_t)nf * rw * sizeof(double) + 6 * sizeof(double) * (size_t)nf <= 220 * 1024)
+            dense_off += (long long)nf * nf;
         I.elem_off = e0;
         I.n_elem = d.num_elements;
         I.fint_ptr_off = f_off;
@@ -912,9 +962,27 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         h->n_rec_total += d.num_record_dofs;
         h->n_rece_slots += nslots;
         const size_t ismem = ((size_t)nf * rw + 6 * (size_t)nf) * sizeof(double);
-        if (ismem > 220 * 1024)
-            return bail(fail(STRUT_UNSUPPORTED, "instance band does not fit in shared memory (n x (2bw+1) too large)"));
-        h->inst_smem = std::max(h->inst_smem, ismem);
+        if (ismem > 220 * 1024) {
+            // band too large for shared memory: blocked factorisation in global memory
+            if (I.spd)
+                return bail(fail(STRUT_UNSUPPORTED, "BandSPD bands beyond shared memory are not implemented"));
+            const int P = std::min(kPanel, std::max(bw, 1));
+            const size_t fsm = sizeof(double) * std::max((size_t)(P + bw) * P, (size_t)64 * kPanel);
+            if (fsm > 220 * 1024)
+                return bail(fail(STRUT_UNSUPPORTED, "band width too large for the blocked factorisation"));
+            I.large = 1;
+            I.large_idx = h->n_large++;
+            I.lband_off = h->lband_total;
+            h->lband_total += (long long)nf * rw;
+            h->large_list_h.push_back(inst);
+            h->max_large_n = std::max(h->max_large_n, nf);
+            h->lfactor_smem = std::max(h->lfactor_smem, fsm);
+            h->ldense_smem = std::max(h->ldense_smem, sizeof(double) * (size_t)nf);
+            if (h->ldense_smem > 220 * 1024)
+                return bail(fail(STRUT_UNSUPPORTED, "instance too large for the dense fallback scratch"));
+        } else {
+            h->inst_smem = std::max(h->inst_smem, ismem);
+        }
         h->max_iters_global = std::max(h->max_iters_global, d.max_iters);
         h->insts[inst] = I;
         // excitations
@@ -1079,7 +1147,30 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     A.ctl = h->d_ctl;
     A.estate = h->d_estate;
     A.n_free_total = h->n_free_total;
+    A.n_inst = h->n_inst;
     A.dual = 0;
+    if (h->n_large > 0) {
+        std::vector<int> rowbase(h->n_large + 1, 0);
+        for (int li = 0; li < h->n_large; ++li) rowbase[li + 1] = rowbase[li] + h->insts[h->large_list_h[li]].n;
+        h->large_rows = rowbase[h->n_large];
+        std::vector<int> lstat(h->n_large, -1);
+        if ((rc = upload(&h->d_large_list, h->large_list_h, al)) || (rc = upload(&h->d_large_rowbase, rowbase, al)) ||
+            (rc = dzeros(&A.lband, (size_t)h->lband_total, al)) || (rc = upload(&A.lstatus, lstat, al)) ||
+            (rc = dzeros(&h->d_gb, 1, al)) || (rc = dzeros(&h->d_wbuf, nF, al)) ||
+            (rc = dzeros(&h->d_ldense, (size_t)h->max_large_n * h->max_large_n, al)) ||
+            (rc = dzeros(&h->d_lpiv, (size_t)h->max_large_n, al)))
+            return bail(rc);
+        CK(cudaFuncSetAttribute(large_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)h->lfactor_smem));
+        CK(cudaFuncSetAttribute(large_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)h->ldense_smem));
+        int per_sm = 0, n_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, large_factor_kernel, kLargeThreads,
+                                                         h->lfactor_smem));
+        CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->device));
+        if (per_sm < 1) return bail(fail(STRUT_UNSUPPORTED, "band factorisation kernel does not fit on an SM"));
+        h->lfactor_grid = n_sm;  // one CTA per SM, all co-resident (cooperative launch)
+    }
     CK(cudaMallocHost((void**)&h->h_ctrl, 4 * sizeof(int)));
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
@@ -1105,6 +1196,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         B.export_band = d_Kinit;
         instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(d_tmp, B, INST_MODE_EXPORT, -1);
         CK(cudaGetLastError());
+        if ((rc = launch_large(h, INST_MODE_EXPORT, d_tmp, &B)) != STRUT_OK) return bail(rc);
         CK(cudaStreamSynchronize(h->stream));
         std::vector<int> st(h->n_inst);
         CK(cudaMemcpy(st.data(), A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));
@@ -1175,7 +1267,9 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
         CK(cudaMemsetAsync(h->A.el.next, 0, 2 * sizeof(int), h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
-    if (n_steps > 0 && !h->prof) {
+    if (n_steps > 0 && !h->prof && h->n_large == 0) {
+        // (instances with a global-memory band run the host-driven loop: their cooperative
+        // factorisation is launched with cudaLaunchCooperativeKernel)
         TRY(ensure_graph(h));
         CK(cudaGraphLaunch(h->gexec, h->stream));
     } else {
@@ -1445,6 +1539,7 @@ int strut_gpu_factor_solve(StrutHandle* h, const double* rhs, double* du) {
     CK(cudaMemcpyAsync(h->A.status, zeros.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));
     instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(h->d_insts, A, INST_MODE_SOLVE_EXPORTED, -1);
     CK(cudaGetLastError());
+    TRY(launch_large(h, INST_MODE_SOLVE_EXPORTED, nullptr, &A));
     CK(cudaStreamSynchronize(h->stream));
     std::vector<int> st(h->n_inst);
     CK(cudaMemcpy(st.data(), h->A.status, sizeof(int) * h->n_inst, cudaMemcpyDeviceToHost));

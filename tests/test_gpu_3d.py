@@ -124,3 +124,52 @@ def test_section3d_path_rc_cyclic(gpu_lib, oracle):
     got = gpu_lib.section3d_path(m, nm, f, nf, path)
     scale = np.maximum(np.abs(ref).max(0), 1e-30)
     assert np.all(np.abs(got - ref).max(0) <= 1e-9 * scale)
+
+
+# ---- bands beyond shared memory (blocked LU in global memory) ---------------------------------
+
+def _large_case(steps, seed=41, element="forceBeamColumn3d", bays_x=3, bays_y=2, stories=3):
+    # 12 nodes per floor: n = 216, half band ~77 -> a 268 KB band, factored in global memory
+    return W.rc_frame3d_case(stories=stories, bays_x=bays_x, bays_y=bays_y, steps=steps,
+                             element=element, seed=seed, pga_g=0.4, record_elements=(1,))
+
+
+def test_large_band_factor_solve(gpu_lib):
+    m = M.Model(_large_case(10))
+    u = _random_u(m, 5, 0.003)
+    with gpu_lib.Analysis([m]) as an:
+        bw, rw = an.band_info(0)
+        assert m.num_free * rw * 8 > 220 * 1024
+        (_f, band), = an.state_determination([u])
+        n = m.num_free
+        K = np.zeros((n, n))
+        for i in range(n):
+            for o in range(rw):
+                j = i + o - bw
+                if 0 <= j < n:
+                    K[i, j] = band[i, o]
+        rhs = np.random.default_rng(7).normal(size=n)
+        du, = an.factor_solve([rhs])
+    ref = np.linalg.solve(K, rhs)
+    np.testing.assert_allclose(du, ref, rtol=1e-8, atol=1e-12 * np.abs(ref).max())
+
+
+def test_large_band_state_determination(gpu_lib, oracle):
+    m = M.Model(_large_case(10, element="dispBeamColumn3d"))
+    u = _random_u(m, 6, 0.003)
+    f_ref, band_ref, bw = oracle.state_determination(m, u)
+    with gpu_lib.Analysis([m]) as an:
+        (f_got, band_got), = an.state_determination([u])
+    assert np.max(np.abs(f_got - f_ref)) <= 1e-9 * np.max(np.abs(f_ref))
+    assert np.max(np.abs(band_got - band_ref)) <= 1e-9 * np.max(np.abs(band_ref))
+
+
+def test_large_band_transient(gpu_lib, oracle):
+    _parity_3d(gpu_lib, oracle, [_large_case(80)], 80)
+
+
+def test_large_and_small_bands_in_one_batch(gpu_lib, oracle):
+    cases = [_large_case(60, seed=51),
+             W.rc_frame3d_case(stories=1, bays_x=1, bays_y=1, steps=60, seed=52, pga_g=0.4),
+             _large_case(60, seed=53, element="dispBeamColumn3d", bays_x=2, bays_y=3)]
+    _parity_3d(gpu_lib, oracle, cases, 60)
