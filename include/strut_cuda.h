@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define STRUT_ABI_VERSION 2
+#define STRUT_ABI_VERSION 3
 #define STRUT_MAX_INT_PTS 10
 
 /* Status codes.  No entry point aborts the process. */
@@ -188,6 +188,19 @@ typedef struct StrutModelDesc {
     int32_t num_record_elements;
     const int32_t* record_dofs;
     const int32_t* record_elements;
+    /* multi-point constraints, Transformation handler (loader.mojo:2239-2380): slave dof s
+     * follows its retained dofs, u_s = sum_k coef_k u_{master_k} (equalDOF: one term with
+     * coefficient 1; rigidDiaphragm: the constraint matrix row).  Slave dofs are neither free
+     * nor fixed; K, F_int and loads are collapsed onto the retained dofs, and the band keeps
+     * the half width detected from the elements' free dofs (slaves excluded), dropping coupled
+     * entries outside it as Strut does (linear_solver_backend.mojo:413-427, 1481-1507).  A slave
+     * dof may carry no mass.  num_slaves 0: none. */
+    int32_t num_slaves;
+    int32_t reserved_mpc;
+    const int32_t* slave_dof;      /* num_slaves full dof indices                          */
+    const int32_t* slave_ptr;      /* num_slaves + 1 offsets into the term arrays          */
+    const int32_t* slave_master;   /* retained full dof of each term                       */
+    const double* slave_coef;      /* coefficient of each term                             */
 } StrutModelDesc;
 
 /* Per-run statistics (RuntimeProfileMetrics counters, solver/profile.mojo:37-74). */

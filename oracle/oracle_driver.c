@@ -47,6 +47,18 @@ typedef struct OModel {
     double a0, a1, a2, a3;
     int has_damping;
     long newton_iters, factorizations;
+    /* multi-point constraints: full K in a CSR pattern (rows = full dofs, sorted columns),
+     * per element the position of each of its nd x nd entries, the collapse rows of every
+     * dof and the collapsed F_int (full size) */
+    int has_mpc;
+    int* mrow_ptr;     /* num_dofs + 1: collapse terms of each dof (none for a fixed dof) */
+    int* mrow_dof;
+    double* mrow_coef;
+    int* kptr;         /* num_dofs + 1 */
+    int* kcol;
+    double* kval;
+    int* epos;         /* num_elements x nd x nd */
+    double* Fred;
 } OModel;
 
 static double path_eval(const StrutExcitation* x, double t) {
@@ -95,7 +107,138 @@ static void model_free(OModel* m) {
     free(m->u); free(m->u_f); free(m->v_f); free(m->a_f); free(m->u_n); free(m->v_n);
     free(m->a_n); free(m->Fint); free(m->Fext); free(m->P_f); free(m->R_f); free(m->du);
     free(m->at); free(m->vt); free(m->work);
+    free(m->mrow_ptr); free(m->mrow_dof); free(m->mrow_coef); free(m->kptr); free(m->kcol);
+    free(m->kval); free(m->epos); free(m->Fred);
     memset(m, 0, sizeof(*m));
+}
+
+static int cmp_int(const void* a, const void* b) {
+    int x = *(const int*)a, y = *(const int*)b;
+    return (x > y) - (x < y);
+}
+
+/* Collapse rows (loader.mojo:2239-2380): a free dof maps to itself with coefficient 1, a slave
+ * to its retained dofs, a fixed dof to nothing.  Full K pattern from the elements' dof pairs.
+ * A slave dof may carry no mass (the collapsed mass would not be diagonal). */
+static int mpc_build(OModel* m) {
+    const StrutModelDesc* d = m->d;
+    int nd = d->num_dofs, ned = m->nd;
+    int* slave_of = (int*)malloc(sizeof(int) * nd);
+    for (int i = 0; i < nd; ++i) slave_of[i] = -1;
+    for (int s = 0; s < d->num_slaves; ++s) {
+        int dof = d->slave_dof[s];
+        if (dof < 0 || dof >= nd) {
+            free(slave_of);
+            return STRUT_BAD_ARG;
+        }
+        slave_of[dof] = s;
+        if (d->mass[dof] != 0.0 || (d->mass_rayleigh && d->mass_rayleigh[dof] != 0.0)) {
+            free(slave_of);
+            return STRUT_UNSUPPORTED;
+        }
+    }
+    m->mrow_ptr = (int*)calloc(nd + 1, sizeof(int));
+    int total = 0;
+    for (int i = 0; i < nd; ++i) {
+        m->mrow_ptr[i] = total;
+        if (slave_of[i] >= 0) total += d->slave_ptr[slave_of[i] + 1] - d->slave_ptr[slave_of[i]];
+        else if (d->free_index[i] >= 0) total += 1;
+    }
+    m->mrow_ptr[nd] = total;
+    m->mrow_dof = (int*)malloc(sizeof(int) * (total + 1));
+    m->mrow_coef = (double*)malloc(sizeof(double) * (total + 1));
+    for (int i = 0; i < nd; ++i) {
+        int o = m->mrow_ptr[i];
+        if (slave_of[i] >= 0) {
+            int s = slave_of[i];
+            for (int t = d->slave_ptr[s]; t < d->slave_ptr[s + 1]; ++t) {
+                m->mrow_dof[o] = d->slave_master[t];
+                m->mrow_coef[o] = d->slave_coef[t];
+                ++o;
+            }
+        } else if (d->free_index[i] >= 0) {
+            m->mrow_dof[o] = i;
+            m->mrow_coef[o] = 1.0;
+        }
+    }
+    free(slave_of);
+    /* full K pattern */
+    int* cnt = (int*)calloc(nd, sizeof(int));
+    for (int e = 0; e < d->num_elements; ++e)
+        for (int a = 0; a < ned; ++a) cnt[d->elements[e].dof[a]] += ned;
+    m->kptr = (int*)calloc(nd + 1, sizeof(int));
+    for (int i = 0; i < nd; ++i) m->kptr[i + 1] = m->kptr[i] + cnt[i];
+    int* tmp = (int*)malloc(sizeof(int) * (m->kptr[nd] + 1));
+    for (int i = 0; i < nd; ++i) cnt[i] = 0;
+    for (int e = 0; e < d->num_elements; ++e)
+        for (int a = 0; a < ned; ++a) {
+            int r = d->elements[e].dof[a];
+            for (int b = 0; b < ned; ++b) tmp[m->kptr[r] + cnt[r]++] = d->elements[e].dof[b];
+        }
+    /* sort and unique each row */
+    int nnz = 0;
+    int* nptr = (int*)calloc(nd + 1, sizeof(int));
+    for (int i = 0; i < nd; ++i) {
+        int* row = tmp + m->kptr[i];
+        int len = m->kptr[i + 1] - m->kptr[i];
+        qsort(row, len, sizeof(int), cmp_int);
+        int u = 0;
+        for (int k = 0; k < len; ++k)
+            if (u == 0 || row[u - 1] != row[k]) row[u++] = row[k];
+        nptr[i] = nnz;
+        nnz += u;
+        cnt[i] = u;
+    }
+    nptr[nd] = nnz;
+    m->kcol = (int*)malloc(sizeof(int) * (nnz + 1));
+    for (int i = 0; i < nd; ++i) memcpy(m->kcol + nptr[i], tmp + m->kptr[i], sizeof(int) * cnt[i]);
+    free(m->kptr);
+    m->kptr = nptr;
+    free(tmp);
+    free(cnt);
+    m->kval = (double*)calloc(nnz + 1, sizeof(double));
+    m->epos = (int*)malloc(sizeof(int) * (size_t)d->num_elements * ned * ned);
+    for (int e = 0; e < d->num_elements; ++e)
+        for (int a = 0; a < ned; ++a) {
+            int r = d->elements[e].dof[a];
+            for (int b = 0; b < ned; ++b) {
+                int c = d->elements[e].dof[b];
+                int lo = m->kptr[r], hi = m->kptr[r + 1] - 1, pos = -1;
+                while (lo <= hi) {
+                    int mid = (lo + hi) / 2;
+                    if (m->kcol[mid] == c) {
+                        pos = mid;
+                        break;
+                    }
+                    if (m->kcol[mid] < c) lo = mid + 1;
+                    else hi = mid - 1;
+                }
+                m->epos[((size_t)e * ned + a) * ned + b] = pos;
+            }
+        }
+    m->Fred = (double*)calloc(nd, sizeof(double));
+    m->has_mpc = 1;
+    return STRUT_OK;
+}
+
+/* _collapse_vector_by_mpc (helpers.mojo:3288-3301): out[r] += c * v[i], i ascending */
+static void mpc_collapse_vector(const OModel* m, const double* v, double* out) {
+    int nd = m->d->num_dofs;
+    for (int i = 0; i < nd; ++i) out[i] = 0.0;
+    for (int i = 0; i < nd; ++i)
+        for (int t = m->mrow_ptr[i]; t < m->mrow_ptr[i + 1]; ++t)
+            out[m->mrow_dof[t]] += m->mrow_coef[t] * v[i];
+}
+
+/* _enforce_mpc_values (helpers.mojo:3380-3400) on the full displacement vector */
+static void mpc_enforce(const OModel* m, double* u) {
+    const StrutModelDesc* d = m->d;
+    for (int s = 0; s < d->num_slaves; ++s) {
+        double value = 0.0;
+        for (int t = d->slave_ptr[s]; t < d->slave_ptr[s + 1]; ++t)
+            value += d->slave_coef[t] * u[d->slave_master[t]];
+        u[d->slave_dof[s]] = value;
+    }
 }
 
 static int model_build(OModel* m, const StrutModelDesc* d) {
@@ -244,6 +387,10 @@ static int model_build(OModel* m, const StrutModelDesc* d) {
     m->a3 = 1.0 / (2.0 * beta) - 1.0;
     m->has_damping = d->alpha_m != 0.0 || d->beta_k != 0.0 || d->beta_k_init != 0.0 ||
                      d->beta_k_comm != 0.0;
+    if (d->num_slaves > 0) {
+        int rc = mpc_build(m);
+        if (rc != STRUT_OK) return rc;
+    }
     return STRUT_OK;
 }
 
@@ -258,11 +405,65 @@ static int element_state(OElement* el, const double* ug, double* k, double* f) {
     }
 }
 
+/* assemble_global_stiffness_and_internal_soa into the full K, then _collapse_matrix_by_mpc
+ * (helpers.mojo:3345-3377: out[r_i][r_j] += c_i K[i][j] c_j over i, j ascending, zero entries
+ * skipped) straight into the band, where an entry outside the detected half width is dropped
+ * as _update_banded_general_values_from_dense drops it (linear_solver_backend.mojo:413-427);
+ * F_int collapsed by _collapse_vector_by_mpc. */
+static void mpc_collapse_K(OModel* m) {
+    const StrutModelDesc* d = m->d;
+    int nd = d->num_dofs;
+    memset(m->K, 0, sizeof(double) * (size_t)m->n * m->rw);
+    for (int i = 0; i < nd; ++i) {
+        int ti0 = m->mrow_ptr[i], ti1 = m->mrow_ptr[i + 1];
+        if (ti0 == ti1) continue;
+        for (int k = m->kptr[i]; k < m->kptr[i + 1]; ++k) {
+            double value = m->kval[k];
+            if (value == 0.0) continue;
+            int j = m->kcol[k];
+            int tj0 = m->mrow_ptr[j], tj1 = m->mrow_ptr[j + 1];
+            if (tj0 == tj1) continue;
+            for (int ti = ti0; ti < ti1; ++ti) {
+                int fi = d->free_index[m->mrow_dof[ti]];
+                double ci = m->mrow_coef[ti];
+                for (int tj = tj0; tj < tj1; ++tj) {
+                    int fj = d->free_index[m->mrow_dof[tj]];
+                    double contrib = ci * value * m->mrow_coef[tj];
+                    if (fi < 0 || fj < 0) continue;
+                    int sl = gslot(m, fi, fj);
+                    if (sl >= 0) m->K[sl] += contrib;
+                }
+            }
+        }
+    }
+    mpc_collapse_vector(m, m->Fint, m->Fred);
+}
+
 static int assemble(OModel* m, double* ek_out, double* ef_out) {
     const StrutModelDesc* d = m->d;
     int nd = m->nd;
     memset(m->K, 0, sizeof(double) * (size_t)m->n * m->rw);
     memset(m->Fint, 0, sizeof(double) * d->num_dofs);
+    if (m->has_mpc) {
+        int nnz = m->kptr[d->num_dofs];
+        memset(m->kval, 0, sizeof(double) * (nnz + 1));
+        for (int e = 0; e < d->num_elements; ++e) {
+            OElement* el = &m->elems[e];
+            double ug[12], k[144], f[12];
+            for (int a = 0; a < nd; ++a) ug[a] = m->u[el->desc->dof[a]];
+            int rc = element_state(el, ug, k, f);
+            if (rc != STRUT_OK) return rc;
+            if (ek_out) memcpy(ek_out + (size_t)nd * nd * e, k, sizeof(double) * nd * nd);
+            if (ef_out) memcpy(ef_out + (size_t)nd * e, f, sizeof(double) * nd);
+            const int* pos = m->epos + (size_t)e * nd * nd;
+            for (int a = 0; a < nd; ++a) {
+                for (int b = 0; b < nd; ++b) m->kval[pos[a * nd + b]] += k[a * nd + b];
+                m->Fint[el->desc->dof[a]] += f[a];
+            }
+        }
+        mpc_collapse_K(m);
+        return STRUT_OK;
+    }
     for (int e = 0; e < d->num_elements; ++e) {
         OElement* el = &m->elems[e];
         double ug[12], k[144], f[12];
@@ -563,6 +764,7 @@ static void scatter_u(OModel* m) {
         int fi = d->free_index[dof];
         if (fi >= 0) m->u[dof] = m->u_f[fi];
     }
+    if (m->has_mpc) mpc_enforce(m, m->u);
 }
 
 static int initial_assembly(OModel* m) {
@@ -644,9 +846,38 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
                 }
             }
         }
-        for (int dof = 0; dof < d->num_dofs; ++dof) {
-            int fi = d->free_index[dof];
-            if (fi >= 0) m->P_f[fi] = m->Fext[dof];
+        if (m->has_mpc) {
+            /* F_const is collapsed once at load, the inertia load of each excitation every
+             * step (loader.mojo:2344, transient_nonlinear.mojo:1836-1848) */
+            int nd = d->num_dofs;
+            double* acc = (double*)calloc((size_t)nd, sizeof(double));
+            double* inert = (double*)calloc((size_t)nd, sizeof(double));
+            double* red = (double*)calloc((size_t)nd, sizeof(double));
+            for (int dof = 0; dof < nd; ++dof) inert[dof] = d->f_const ? d->f_const[dof] : 0.0;
+            mpc_collapse_vector(m, inert, acc);
+            for (int x = 0; x < d->num_excitations; ++x) {
+                const StrutExcitation* ex = &d->excitation[x];
+                if (ex->direction < 1) continue;
+                double ag = path_eval(ex, t);
+                for (int dof = 0; dof < nd; ++dof) {
+                    inert[dof] = 0.0;
+                    if ((dof % d->ndf) + 1 == ex->direction) inert[dof] += -d->mass[dof] * ag;
+                }
+                mpc_collapse_vector(m, inert, red);
+                for (int dof = 0; dof < nd; ++dof) acc[dof] += red[dof];
+            }
+            for (int dof = 0; dof < nd; ++dof) {
+                int fi = d->free_index[dof];
+                if (fi >= 0) m->P_f[fi] = acc[dof];
+            }
+            free(acc);
+            free(inert);
+            free(red);
+        } else {
+            for (int dof = 0; dof < d->num_dofs; ++dof) {
+                int fi = d->free_index[dof];
+                if (fi >= 0) m->P_f[fi] = m->Fext[dof];
+            }
         }
         int converged = 0;
         int it;
@@ -675,7 +906,8 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
                 double damping = 0.0;
                 if (m->has_damping) damping = band_row_dot(m, m->C, i, m->vt);
                 double inertia = diag_dot(m, m->Mff, i, m->at);
-                m->R_f[i] = m->P_f[i] - m->Fint[dof] - 0.0 - damping - inertia;
+                const double fint = m->has_mpc ? m->Fred[dof] : m->Fint[dof];
+                m->R_f[i] = m->P_f[i] - fint - 0.0 - damping - inertia;
             }
             if (d->test_type == STRUT_TEST_NORM_UNBALANCE) {
                 if (sqrt(simd_sumsq(m->R_f, n)) <= d->tol) {
@@ -783,7 +1015,8 @@ int oracle_state_determination(const StrutModelDesc* d, const double* u_free,
         if (half_bw) *half_bw = m.bw;
         if (f_int_free)
             for (int dof = 0; dof < d->num_dofs; ++dof)
-                if (d->free_index[dof] >= 0) f_int_free[d->free_index[dof]] = m.Fint[dof];
+                if (d->free_index[dof] >= 0)
+                    f_int_free[d->free_index[dof]] = m.has_mpc ? m.Fred[dof] : m.Fint[dof];
         if (band_out) {
             if (m.spd)
                 memcpy(band_out, m.Kspd, sizeof(double) * (size_t)m.n * (m.bw + 1));

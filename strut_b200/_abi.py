@@ -160,6 +160,12 @@ class StrutModelDesc(C.Structure):
         ("num_record_elements", C.c_int32),
         ("record_dofs", _ip),
         ("record_elements", _ip),
+        ("num_slaves", C.c_int32),
+        ("reserved_mpc", C.c_int32),
+        ("slave_dof", _ip),
+        ("slave_ptr", _ip),
+        ("slave_master", _ip),
+        ("slave_coef", _dp),
     ]
 
 

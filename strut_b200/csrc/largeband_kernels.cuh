@@ -137,8 +137,7 @@ __global__ void __launch_bounds__(256) large_assemble_kernel(const DevInst* __re
         const int gi = f0 + i;
         const double an = I.a0 * (A.u_f[gi] - A.u_n[gi]) - I.a2 * A.v_n[gi] - I.a3 * A.a_n[gi];
         const int q0 = A.fint_ptr[I.fint_ptr_off + i], q1 = A.fint_ptr[I.fint_ptr_off + i + 1];
-        double F = 0.0;
-        for (int q = q0; q < q1; ++q) F += A.ef[A.fint_contrib[q]];
+        const double F = gather_fint(A, A.ef, q0, q1);
         const double ma = A.Mff[gi] * an;
         A.R[gi] = A.P_f[gi] - F - 0.0 - cv - ma;
         if (mode == INST_MODE_EXPORT) A.export_f[gi] = F;

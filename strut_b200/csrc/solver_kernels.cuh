@@ -61,6 +61,14 @@ struct InstArrays {
     double* hist_du;        // 4 x n_free ring of converged increments (slot = step % 4)
     int n_free_total;
     int n_inst;
+    // multi-point constraints: per-contribution coefficients of the gathers (null without
+    // constraints) and the slave dofs u_s = sum_k coef_k u_{master_k} (absolute u_full indices)
+    const double* slot_coef;
+    const double* fint_coef;
+    const int* sl_dof;
+    const int* sl_ptr;
+    const int* sl_master;
+    const double* sl_coef;
     // instances whose band lives in global memory
     double* lband;          // effective band (factored in place), at DevInst::lband_off
     int* lstatus;           // per large instance: 0 factored, 2 singular, 6 dense fallback,
@@ -230,8 +238,36 @@ __device__ void band_solve_chol_warp(const double* B, int n, int bw, int rw, con
 __device__ __forceinline__ double gather_slot(const InstArrays& A, long long sp0, int slot) {
     const long long c0 = A.slot_ptr[sp0 + slot], c1 = A.slot_ptr[sp0 + slot + 1];
     double K = 0.0;
-    for (long long c = c0; c < c1; ++c) K += A.ek[A.slot_contrib[c]];
+    if (A.slot_coef) {
+        // collapsed through multi-point constraints: c_i k c_j
+        for (long long c = c0; c < c1; ++c) K += A.slot_coef[c] * A.ek[A.slot_contrib[c]];
+    } else {
+        for (long long c = c0; c < c1; ++c) K += A.ek[A.slot_contrib[c]];
+    }
     return K;
+}
+
+// F_int of free dof i of an instance: its element end forces in element order (times the
+// collapse coefficient under multi-point constraints).
+__device__ __forceinline__ double gather_fint(const InstArrays& A, const double* ef, int q0, int q1) {
+    double F = 0.0;
+    if (A.fint_coef) {
+        for (int q = q0; q < q1; ++q) F += A.fint_coef[q] * ef[A.fint_contrib[q]];
+    } else {
+        for (int q = q0; q < q1; ++q) F += ef[A.fint_contrib[q]];
+    }
+    return F;
+}
+
+// Slave dofs of an instance from their retained dofs (_enforce_mpc_values,
+// helpers.mojo:3380-3400), collectively over the CTA.
+__device__ __forceinline__ void enforce_slaves(const DevInst& I, const InstArrays& A) {
+    for (int s = threadIdx.x; s < I.n_sl; s += blockDim.x) {
+        const int k = I.sl_off + s;
+        double value = 0.0;
+        for (int t = A.sl_ptr[k]; t < A.sl_ptr[k + 1]; ++t) value += A.sl_coef[t] * A.u_full[A.sl_master[t]];
+        A.u_full[A.sl_dof[k]] = value;
+    }
 }
 
 // ||R||_2 of the Newmark residual R = P - F_int - C v - M a at the free displacements uf with
@@ -262,7 +298,8 @@ __device__ double residual_norm(const DevInst& I, const InstArrays& A, const dou
                 if (I.beta_k != 0.0) {
                     const long long c0 = A.slot_ptr[sp0 + slot], c1 = A.slot_ptr[sp0 + slot + 1];
                     double K = 0.0;
-                    for (long long c = c0; c < c1; ++c) K += ek[A.slot_contrib[c]];
+                    for (long long c = c0; c < c1; ++c)
+                        K += (A.slot_coef ? A.slot_coef[c] : 1.0) * ek[A.slot_contrib[c]];
                     C += I.beta_k * K;
                 }
                 if (I.beta_k_init != 0.0) C += I.beta_k_init * Kinit[slot];
@@ -270,8 +307,7 @@ __device__ double residual_norm(const DevInst& I, const InstArrays& A, const dou
             }
         }
         const int q0 = A.fint_ptr[I.fint_ptr_off + i], q1 = A.fint_ptr[I.fint_ptr_off + i + 1];
-        double F = 0.0;
-        for (int q = q0; q < q1; ++q) F += ef[A.fint_contrib[q]];
+        const double F = gather_fint(A, ef, q0, q1);
         const double r = A.P_f[f0 + i] - F - 0.0 - cv - A.Mff[f0 + i] * as[i];
         ss += r * r;
     }
@@ -536,8 +572,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
                 Kb[slot] = keff;
             }
             const int q0 = A.fint_ptr[I.fint_ptr_off + i], q1 = A.fint_ptr[I.fint_ptr_off + i + 1];
-            double F = 0.0;
-            for (int q = q0; q < q1; ++q) F += A.ef[A.fint_contrib[q]];
+            const double F = gather_fint(A, A.ef, q0, q1);
             const double ma = A.Mff[f0 + i] * w[i];
             R[i] = A.P_f[f0 + i] - F - 0.0 - cv - ma;
             A.R[f0 + i] = R[i];
@@ -639,6 +674,10 @@ __device__ void newton_tail(const DevInst& I, InstArrays& A, int inst, const dou
         const double un = A.u_f[gi] + d;
         A.u_f[gi] = un;
         A.u_full[A.free_dof[gi]] = un;
+    }
+    if (I.n_sl > 0) {
+        __syncthreads();
+        enforce_slaves(I, A);
     }
     const double norm = sqrt(block_sum(ss, red));
     const double energy = fabs(block_sum(en, red));
@@ -785,6 +824,16 @@ __global__ void scatter_free_kernel(const double* __restrict__ u_f, const int* _
                                     double* __restrict__ u_full, int n) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) u_full[free_dof[t]] = u_f[t];
+}
+
+// Every slave dof of every instance from its retained dofs (after the Newmark predictor or a
+// host-side displacement write; transient_nonlinear.mojo:1768-1790).
+__global__ void slave_enforce_kernel(InstArrays A, int n_slaves) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_slaves) return;
+    double value = 0.0;
+    for (int t = A.sl_ptr[k]; t < A.sl_ptr[k + 1]; ++t) value += A.sl_coef[t] * A.u_full[A.sl_master[t]];
+    A.u_full[A.sl_dof[k]] = value;
 }
 
 }  // namespace strut

@@ -295,6 +295,7 @@ struct StrutHandle {
     double* d_wbuf = nullptr;
     double* d_ldense = nullptr;
     int* d_lpiv = nullptr;
+    int n_slaves_total = 0;          // slave dofs of every instance (multi-point constraints)
     int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
     long long band_total = 0;
     int max_nip = 1;
@@ -484,7 +485,7 @@ static int launch_instances(StrutHandle* h, int mode, int step) {
     TRY(prof_begin(h));
     instance_newton_kernel<<<h->n_inst, 256, h->inst_smem, h->stream>>>(h->d_insts, A, mode, step);
     CK(cudaGetLastError());
-    TRY(launch_large(h, mode));
+    TRY(launch_large(h, mode, nullptr, &A));
     TRY(prof_end(h, 1));
     return STRUT_OK;
 }
@@ -591,7 +592,13 @@ static int build_graph(StrutHandle* h) {
                         (const double*)h->d_ag, nF, h->n_inst, h->d_ctl, inner, 1));
     cudaGraph_t ibody;
     cudaGraphNode_t n_before_inner = n_pred;
-    if (h->pred) TRY(pred_add_nodes(h, body, n_pred, &n_before_inner));
+    if (h->n_slaves_total > 0) {
+        cudaGraphNode_t n_sl;
+        TRY(add_kernel_node(&n_sl, body, &n_pred, 1, slave_enforce_kernel, dim3((h->n_slaves_total + tb - 1) / tb),
+                            dim3(tb), 0, A, h->n_slaves_total));
+        n_before_inner = n_sl;
+    }
+    if (h->pred) TRY(pred_add_nodes(h, body, n_before_inner, &n_before_inner));
     TRY(add_while_node(&n_inner, body, &n_before_inner, 1, inner, &ibody));
     cudaGraphNode_t n_el, n_in, n_chk;
     TRY(add_kernel_node(&n_el, ibody, nullptr, 0, elem_kernel_of(h), dim3(h->elem_grid),
@@ -672,6 +679,11 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     std::vector<long long> slot_ptr(1, 0);
     std::vector<int> slot_contrib;
     std::vector<int> fint_ptr(1, 0), fint_contrib;
+    std::vector<double> slot_coef, fint_coef;        // filled when some instance has constraints
+    std::vector<int> sl_dof, sl_ptr(1, 0), sl_master;
+    std::vector<double> sl_coef;
+    bool any_mpc = false;
+    for (int inst = 0; inst < num_instances; ++inst) any_mpc = any_mpc || models[inst].num_slaves > 0;
     long long c2_total = 0, s2_total = 0, s1_total = 0;
     std::vector<int> sec_base(num_instances);
     int u_off = 0, f_off = 0;
@@ -731,6 +743,58 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             if (d.f_const) fcf[fi] = d.f_const[dof];
         }
         if (!has_mass) return bail(fail(STRUT_BAD_ARG, "transient_nonlinear requires masses on free dofs"));
+        // collapse rows of every dof (loader.mojo:2239-2380): a free dof maps to itself, a
+        // slave to its retained dofs, a fixed dof to nothing
+        std::vector<int> slave_of(d.num_dofs, -1);
+        const int sl0 = (int)sl_dof.size();
+        if (d.num_slaves < 0 || (d.num_slaves > 0 && (!d.slave_dof || !d.slave_ptr || !d.slave_master || !d.slave_coef)))
+            return bail(fail(STRUT_BAD_ARG, "slave arrays missing"));
+        for (int k = 0; k < d.num_slaves; ++k) {
+            const int sd = d.slave_dof[k];
+            if (sd < 0 || sd >= d.num_dofs || d.free_index[sd] >= 0 || slave_of[sd] >= 0)
+                return bail(fail(STRUT_BAD_ARG, "slave dof out of range, free, or repeated"));
+            if (d.mass[sd] != 0.0 || (d.mass_rayleigh && d.mass_rayleigh[sd] != 0.0))
+                return bail(fail(STRUT_UNSUPPORTED, "mass on a constrained (slave) dof"));
+            slave_of[sd] = k;
+            if (d.slave_ptr[k + 1] < d.slave_ptr[k]) return bail(fail(STRUT_BAD_ARG, "slave_ptr not increasing"));
+            sl_dof.push_back(u_off + sd);
+            for (int t = d.slave_ptr[k]; t < d.slave_ptr[k + 1]; ++t) {
+                const int md = d.slave_master[t];
+                if (md < 0 || md >= d.num_dofs) return bail(fail(STRUT_BAD_ARG, "retained dof out of range"));
+                sl_master.push_back(u_off + md);
+                sl_coef.push_back(d.slave_coef[t]);
+            }
+            sl_ptr.push_back((int)sl_master.size());
+        }
+        for (int k = 0; k < d.num_slaves; ++k)
+            for (int t = d.slave_ptr[k]; t < d.slave_ptr[k + 1]; ++t)
+                if (slave_of[d.slave_master[t]] >= 0)
+                    return bail(fail(STRUT_BAD_ARG, "a retained dof cannot itself be constrained"));
+        auto rows_of = [&](int dof, std::vector<std::pair<int, double>>& out) {
+            out.clear();
+            if (slave_of[dof] >= 0) {
+                const int k = slave_of[dof];
+                for (int t = d.slave_ptr[k]; t < d.slave_ptr[k + 1]; ++t)
+                    out.emplace_back(d.free_index[d.slave_master[t]], d.slave_coef[t]);
+            } else if (d.free_index[dof] >= 0) {
+                out.emplace_back(d.free_index[dof], 1.0);
+            }
+        };
+        if (d.num_slaves > 0 && d.f_const) {
+            // F_const collapsed onto the retained dofs (loader.mojo:2344)
+            std::vector<double> red(d.num_dofs, 0.0);
+            for (int dof = 0; dof < d.num_dofs; ++dof) {
+                if (slave_of[dof] >= 0) {
+                    const int k = slave_of[dof];
+                    for (int t = d.slave_ptr[k]; t < d.slave_ptr[k + 1]; ++t)
+                        red[d.slave_master[t]] += d.slave_coef[t] * d.f_const[dof];
+                } else if (d.free_index[dof] >= 0) {
+                    red[dof] += 1.0 * d.f_const[dof];
+                }
+            }
+            for (int dof = 0; dof < d.num_dofs; ++dof)
+                if (d.free_index[dof] >= 0) fcf[d.free_index[dof]] = red[dof];
+        }
         {
             double hmax = 0.0;
             for (int nd = 0; nd < d.num_nodes; ++nd) hmax = std::max(hmax, d.node_coords[d.ndm * nd + d.ndm - 1]);
@@ -883,29 +947,70 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         // band slot contributions, element order (stiffness_internal_frame2d.mojo:594-619)
         std::vector<std::vector<int>> slots((size_t)nf * rw);
         std::vector<std::vector<int>> fcontr(nf);
-        for (int e = 0; e < d.num_elements; ++e) {
-            const DevElem& E = elems[e0 + e];
-            for (int a = 0; a < nd; ++a) {
-                const int ia = efree[(size_t)nd * e + a];
-                if (ia < 0) continue;
-                for (int b = 0; b < nd; ++b) {
-                    const int ib = efree[(size_t)nd * e + b];
-                    if (ib < 0) continue;
-                    slots[(size_t)ia * rw + (ib - ia + bw)].push_back((int)(E.ek_off + a * nd + b));
+        std::vector<std::vector<double>> slotc, fc;
+        if (any_mpc) {
+            slotc.resize((size_t)nf * rw);
+            fc.resize(nf);
+        }
+        if (d.num_slaves == 0) {
+            for (int e = 0; e < d.num_elements; ++e) {
+                const DevElem& E = elems[e0 + e];
+                for (int a = 0; a < nd; ++a) {
+                    const int ia = efree[(size_t)nd * e + a];
+                    if (ia < 0) continue;
+                    for (int b = 0; b < nd; ++b) {
+                        const int ib = efree[(size_t)nd * e + b];
+                        if (ib < 0) continue;
+                        const size_t sl = (size_t)ia * rw + (ib - ia + bw);
+                        slots[sl].push_back((int)(E.ek_off + a * nd + b));
+                        if (any_mpc) slotc[sl].push_back(1.0);
+                    }
+                    fcontr[ia].push_back((int)(E.ef_off + a));
+                    if (any_mpc) fc[ia].push_back(1.0);
                 }
-                fcontr[ia].push_back((int)(E.ef_off + a));
+            }
+        } else {
+            // collapse c_i k c_j onto the retained free dofs; entries outside the half width
+            // detected from the elements' free dofs are dropped, as Strut's band load drops
+            // them (linear_solver_backend.mojo:413-427)
+            std::vector<std::pair<int, double>> ra, rb;
+            for (int e = 0; e < d.num_elements; ++e) {
+                const DevElem& E = elems[e0 + e];
+                for (int a = 0; a < nd; ++a) {
+                    rows_of(d.elements[e].dof[a], ra);
+                    for (int b = 0; b < nd; ++b) {
+                        rows_of(d.elements[e].dof[b], rb);
+                        for (auto& ta : ra)
+                            for (auto& tb : rb) {
+                                if (ta.first < 0 || tb.first < 0 || std::abs(ta.first - tb.first) > bw) continue;
+                                if (ta.second == 0.0 || tb.second == 0.0) continue;
+                                const size_t sl = (size_t)ta.first * rw + (tb.first - ta.first + bw);
+                                slots[sl].push_back((int)(E.ek_off + a * nd + b));
+                                slotc[sl].push_back(ta.second * tb.second);
+                            }
+                    }
+                    for (auto& ta : ra) {
+                        if (ta.first < 0 || ta.second == 0.0) continue;
+                        fcontr[ta.first].push_back((int)(E.ef_off + a));
+                        fc[ta.first].push_back(ta.second);
+                    }
+                }
             }
         }
-        for (auto& v : slots) {
-            slot_contrib.insert(slot_contrib.end(), v.begin(), v.end());
+        for (size_t k = 0; k < slots.size(); ++k) {
+            slot_contrib.insert(slot_contrib.end(), slots[k].begin(), slots[k].end());
+            if (any_mpc) slot_coef.insert(slot_coef.end(), slotc[k].begin(), slotc[k].end());
             slot_ptr.push_back((long long)slot_contrib.size());
         }
-        for (auto& v : fcontr) {
-            fint_contrib.insert(fint_contrib.end(), v.begin(), v.end());
+        for (int k = 0; k < nf; ++k) {
+            fint_contrib.insert(fint_contrib.end(), fcontr[k].begin(), fcontr[k].end());
+            if (any_mpc) fint_coef.insert(fint_coef.end(), fc[k].begin(), fc[k].end());
             fint_ptr.push_back((int)fint_contrib.size());
         }
         DevInst I;
         std::memset(&I, 0, sizeof(I));
+        I.sl_off = sl0;
+        I.n_sl = d.num_slaves;
         I.n = nf;
         I.bw = bw;
         I.rw = rw;
@@ -1139,6 +1244,21 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     A.ek = h->d_ek;
     A.ef = h->d_ef;
     A.Kinit = d_Kinit;
+    if (any_mpc) {
+        double *d_sc, *d_fc, *d_slc;
+        int *d_sld, *d_slp, *d_slm;
+        if ((rc = upload(&d_sc, slot_coef, al)) || (rc = upload(&d_fc, fint_coef, al)) ||
+            (rc = upload(&d_sld, sl_dof, al)) || (rc = upload(&d_slp, sl_ptr, al)) ||
+            (rc = upload(&d_slm, sl_master, al)) || (rc = upload(&d_slc, sl_coef, al)))
+            return bail(rc);
+        A.slot_coef = d_sc;
+        A.fint_coef = d_fc;
+        A.sl_dof = d_sld;
+        A.sl_ptr = d_slp;
+        A.sl_master = d_slm;
+        A.sl_coef = d_slc;
+        h->n_slaves_total = (int)sl_dof.size();
+    }
     if ((rc = dzeros(&h->d_ctl, 1, al))) return bail(rc);
     {
         std::vector<int> neg(h->n_inst, -1);
@@ -1282,6 +1402,10 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             predictor_kernel<<<(npred + tb - 1) / tb, tb, 0, h->stream>>>(
                 h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag, nF, h->n_inst, h->d_ctl, none, 0);
             CK(cudaGetLastError());
+            if (h->n_slaves_total > 0) {
+                slave_enforce_kernel<<<(h->n_slaves_total + tb - 1) / tb, tb, 0, h->stream>>>(h->A, h->n_slaves_total);
+                CK(cudaGetLastError());
+            }
             TRY(prof_end(h, 3));
             if (h->pred) {
                 TRY(prof_begin(h));
@@ -1495,6 +1619,10 @@ int strut_gpu_state_determination(StrutHandle* h, const double* u_free, double* 
     CK(cudaMemcpyAsync(h->A.u_f, u_free, nF * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     scatter_free_kernel<<<(nF + 255) / 256, 256, 0, h->stream>>>(h->A.u_f, h->A.free_dof, h->A.u_full, nF);
     CK(cudaGetLastError());
+    if (h->n_slaves_total > 0) {
+        slave_enforce_kernel<<<(h->n_slaves_total + 255) / 256, 256, 0, h->stream>>>(h->A, h->n_slaves_total);
+        CK(cudaGetLastError());
+    }
     std::vector<int> ones(h->n_inst, 1), zeros(h->n_inst, 0);
     CK(cudaMemcpyAsync(h->A.active, ones.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->A.status, zeros.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice, h->stream));

@@ -283,8 +283,7 @@ class Model:
                 if d < 1 or d > self.ndf:
                     raise ModelError("constraint dof out of range")
                 constrained[i * self.ndf + d - 1] = True
-        if case.get("mp_constraints"):
-            raise ModelError("multi-point constraints are not implemented on this path")
+        mpcs = case.get("mp_constraints") or []
 
         # materials
         mats = case.get("materials", [])
@@ -386,11 +385,14 @@ class Model:
         self.integrations = rule_structs
         self.elem_index = {eid: i for i, eid in enumerate(self.elem_ids)}
 
-        # natural-order free numbering (loader.mojo:2439-2446)
+        # multi-point constraints, Transformation handler (loader.mojo:2239-2340)
+        self.slaves = self._mp_constraints(mpcs, case, constrained)
+        slave_set = set(self.slaves)
+        # natural-order free numbering, slaves and fixed dofs skipped (loader.mojo:2439-2446)
         self.free_index = np.full(self.num_dofs, -1, dtype=np.int32)
         nf = 0
         for dof in range(self.num_dofs):
-            if not constrained[dof]:
+            if not constrained[dof] and dof not in slave_set:
                 self.free_index[dof] = nf
                 nf += 1
         if nf == 0:
@@ -496,6 +498,80 @@ class Model:
         self.record_dofs = np.asarray(rec_dofs, dtype=np.int32)
         self.record_elements = np.asarray(rec_elems, dtype=np.int32)
 
+    def _mp_constraints(self, mpcs, case, constrained):
+        """{slave dof: [(retained dof, coefficient), ...]} in constraint order."""
+        if not mpcs:
+            return {}
+        an = case.get("analysis", {})
+        handler = an.get("constraints", "Plain")
+        if handler not in ("Transformation", "Lagrange"):
+            raise ModelError("mp_constraints require analysis.constraints=Transformation or Lagrange")
+        ndf = self.ndf
+        slaves = {}
+        mpc_constrained_nodes = set()
+        for m in mpcs:
+            cn = int(m["constrained_node"])
+            if cn in self.node_index:
+                mpc_constrained_nodes.add(self.node_index[cn])
+        for m in mpcs:
+            t = m.get("type")
+            if t not in ("equalDOF", "rigidDiaphragm"):
+                raise ModelError(f"unsupported mp constraint type: {t}")
+            rn, cn = int(m["retained_node"]), int(m["constrained_node"])
+            if rn not in self.node_index:
+                raise ModelError(f"{t} retained_node not found")
+            if cn not in self.node_index:
+                raise ModelError(f"{t} constrained_node not found")
+            ri, ci = self.node_index[rn], self.node_index[cn]
+            if ri in mpc_constrained_nodes:
+                raise ModelError(f"{t} retained_node cannot also be constrained")
+            if t == "equalDOF":
+                dofs = [int(d) for d in m.get("dofs", [])]
+                if not dofs:
+                    raise ModelError("equalDOF requires non-empty dofs")
+                for d in dofs:
+                    if d < 1 or d > ndf:
+                        raise ModelError("equalDOF dof out of range")
+                    sd = ci * ndf + d - 1
+                    if sd in slaves:
+                        raise ModelError("equalDOF constrained dof already controlled")
+                    slaves[sd] = [(ri * ndf + d - 1, 1.0)]
+            else:
+                if not ((self.ndm == 3 and ndf == 6) or (self.ndm == 2 and ndf == 3)):
+                    raise ModelError("rigidDiaphragm requires a 3D/6DOF or 2D/3DOF model")
+                perp = int(m.get("perp_dirn", 0))
+                if perp < 1 or perp > 3:
+                    raise ModelError("rigidDiaphragm perp_dirn must be in 1..3")
+                cdofs = [int(d) for d in m.get("constrained_dofs", [])]
+                rdofs = [int(d) for d in m.get("retained_dofs", [])]
+                mat = m.get("matrix", [])
+                if not cdofs or not rdofs:
+                    raise ModelError("rigidDiaphragm requires constrained_dofs and retained_dofs")
+                if len(cdofs) > 3 or len(rdofs) > 3:
+                    raise ModelError("rigidDiaphragm holds at most 3 constrained and 3 retained dofs")
+                if len(mat) != len(cdofs):
+                    raise ModelError("rigidDiaphragm matrix rows must match constrained_dofs")
+                for row, cd in enumerate(cdofs):
+                    if len(mat[row]) != len(rdofs):
+                        raise ModelError("rigidDiaphragm matrix columns must match retained_dofs")
+                    if cd < 1 or cd > ndf:
+                        raise ModelError("rigidDiaphragm dof out of range")
+                    sd = ci * ndf + cd - 1
+                    if sd in slaves:
+                        raise ModelError("rigidDiaphragm constrained dof already controlled")
+                    terms = []
+                    for col, rd in enumerate(rdofs):
+                        if rd < 1 or rd > ndf:
+                            raise ModelError("rigidDiaphragm dof out of range")
+                        terms.append((ri * ndf + rd - 1, float(mat[row][col])))
+                    slaves[sd] = terms
+                    constrained[sd] = True
+        for sd, terms in slaves.items():
+            for md, _c in terms:
+                if md in slaves:
+                    raise ModelError("a retained dof cannot itself be constrained")
+        return slaves
+
     # -----------------------------------------------------------------------------------
     def desc(self) -> A.StrutModelDesc:
         """The C struct; the Model keeps every buffer it points to alive."""
@@ -548,6 +624,18 @@ class Model:
         d.record_dofs = iptr(self.record_dofs)
         d.num_record_elements = len(self.record_elements)
         d.record_elements = iptr(self.record_elements)
+        sl = sorted(self.slaves)
+        d.num_slaves = len(sl)
+        ptr, mdof, coef = [0], [], []
+        for sd in sl:
+            for md, c in self.slaves[sd]:
+                mdof.append(md)
+                coef.append(c)
+            ptr.append(len(mdof))
+        d.slave_dof = iptr(np.asarray(sl, dtype=np.int32))
+        d.slave_ptr = iptr(np.asarray(ptr, dtype=np.int32))
+        d.slave_master = iptr(np.asarray(mdof, dtype=np.int32))
+        d.slave_coef = dptr(np.asarray(coef, dtype=np.float64))
         self._keep = keep
         return d
 

@@ -345,6 +345,26 @@ def initial_stiffness_3d(case: dict) -> tuple[np.ndarray, np.ndarray, np.ndarray
     M = np.zeros(ndof)
     for m in case.get("masses", []):
         M[6 * idx[m["node"]] + m["dof"] - 1] += m["value"]
+    mpcs = case.get("mp_constraints") or []
+    if mpcs:
+        # Transformation: u = T u_r, the slaves following their retained dofs
+        slave = {}
+        for c in mpcs:
+            ri, ci = idx[c["retained_node"]], idx[c["constrained_node"]]
+            for row, cd in enumerate(c["constrained_dofs"]):
+                slave[6 * ci + cd - 1] = [(6 * ri + rd - 1, c["matrix"][row][col])
+                                          for col, rd in enumerate(c["retained_dofs"])]
+        keep = [d for d in range(ndof) if not fixed[d] and d not in slave]
+        col = {d: k for k, d in enumerate(keep)}
+        T = np.zeros((ndof, len(keep)))
+        for d in keep:
+            T[d, col[d]] = 1.0
+        for d, terms in slave.items():
+            for md, c in terms:
+                T[d, col[md]] += c
+        Kr = T.T @ K @ T
+        Mr = np.diag(T.T @ np.diag(M) @ T)
+        return Kr, Mr, np.asarray(keep)
     return K[np.ix_(free, free)], M[free], free
 
 
@@ -354,8 +374,12 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
                     zg: float = 0.6, pga_g: float = 0.35, tol: float = 1.0e-8,
                     max_iters: int = 20, element: str = "forceBeamColumn3d",
                     system: str = "BandGeneral", zeta: float = 0.05, geom: str = "Linear",
-                    bidirectional: bool = False, record_elements=(1,)) -> dict:
-    """3D RC frame: columns along z, beams along x and y, base fixed in all six dofs."""
+                    bidirectional: bool = False, record_elements=(1,), diaphragm: bool = False,
+                    beam_element: str | None = None, dt_record=None) -> dict:
+    """3D RC frame: columns along z, beams along x and y, base fixed in all six dofs.  With
+    ``diaphragm`` every floor is a rigid diaphragm (perp_dirn 3) retained by its central node,
+    which carries the floor's horizontal masses and rotational inertia; the other nodes keep
+    their vertical mass only.  ``beam_element`` (default: ``element``) sets the beams' type."""
     nodes = []
     grid = {}
     nid = 1
@@ -371,9 +395,9 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
     elements = []
     eid = 1
 
-    def add(n1, n2, sec):
+    def add(n1, n2, sec, etype=element):
         nonlocal eid
-        elements.append({"id": eid, "type": element, "nodes": [n1, n2], "section": sec,
+        elements.append({"id": eid, "type": etype, "nodes": [n1, n2], "section": sec,
                          "geomTransf": geom, "integration": "Lobatto", "num_int_pts": nip})
         eid += 1
 
@@ -381,19 +405,44 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
         for j in range(bays_y + 1):
             for i in range(bays_x + 1):
                 add(grid[(k, j, i)], grid[(k + 1, j, i)], 1)
+    bt = beam_element or element
     for k in range(1, stories + 1):
         for j in range(bays_y + 1):
             for i in range(bays_x):
-                add(grid[(k, j, i)], grid[(k, j, i + 1)], 2)
+                add(grid[(k, j, i)], grid[(k, j, i + 1)], 2, bt)
         for j in range(bays_y):
             for i in range(bays_x + 1):
-                add(grid[(k, j, i)], grid[(k, j + 1, i)], 2)
+                add(grid[(k, j, i)], grid[(k, j + 1, i)], 2, bt)
     masses = []
+    mpcs = []
+    jm, im = bays_y // 2, bays_x // 2
     for k in range(1, stories + 1):
+        if not diaphragm:
+            for j in range(bays_y + 1):
+                for i in range(bays_x + 1):
+                    for d in (1, 2, 3):
+                        masses.append({"node": grid[(k, j, i)], "dof": d, "value": floor_mass})
+            continue
+        master = grid[(k, jm, im)]
+        xm, ym = im * bay_w, jm * bay_w
+        total, inertia = 0.0, 0.0
         for j in range(bays_y + 1):
             for i in range(bays_x + 1):
-                for d in (1, 2, 3):
-                    masses.append({"node": grid[(k, j, i)], "dof": d, "value": floor_mass})
+                node = grid[(k, j, i)]
+                masses.append({"node": node, "dof": 3, "value": floor_mass})
+                dx, dy = i * bay_w - xm, j * bay_w - ym
+                total += floor_mass
+                inertia += floor_mass * (dx * dx + dy * dy)
+                if node == master:
+                    continue
+                mpcs.append({"type": "rigidDiaphragm", "retained_node": master,
+                             "constrained_node": node, "perp_dirn": 3,
+                             "constrained_dofs": [1, 2, 6], "retained_dofs": [1, 2, 6],
+                             "matrix": [[1.0, 0.0, -dy], [0.0, 1.0, dx], [0.0, 0.0, 1.0]],
+                             "dx": dx, "dy": dy, "dz": 0.0})
+        masses += [{"node": master, "dof": 1, "value": total},
+                   {"node": master, "dof": 2, "value": total},
+                   {"node": master, "dof": 6, "value": inertia}]
     n_samples = steps + 1
     series = [{"type": "Path", "tag": 1, "dt": dt,
                "values": [float(v) for v in kanai_tajimi_record(seed, n_samples, dt, wg=wg,
@@ -430,6 +479,9 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
              "output": "roof"},
         ],
     }
+    if mpcs:
+        case["mp_constraints"] = mpcs
+        case["analysis"]["constraints"] = "Transformation"
     if record_elements:
         case["recorders"].append({"type": "element_force", "elements": list(record_elements),
                                   "output": "elements"})

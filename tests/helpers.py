@@ -131,3 +131,69 @@ def single_element_3d(etype: str, geom: str = "Linear", end=(3.0, 1.0, 2.0), vec
             "masses": [{"node": 2, "dof": 1, "value": 1.0}],
             "analysis": {"type": "transient_nonlinear", "dt": 0.01, "steps": 1,
                          "test_type": "NormDispIncr", "tol": 1e-8}}
+
+
+def equal_dof_floors_2d(case2: dict) -> dict:
+    """The 2D frame with every floor's horizontal displacement tied to its first node by
+    equalDOF (Transformation handler); the tied nodes' horizontal masses move to that node."""
+    import copy
+
+    c = copy.deepcopy(case2)
+    by_y = {}
+    for n in c["nodes"]:
+        if n.get("constraints"):
+            continue
+        by_y.setdefault(n["y"], []).append(n["id"])
+    mpcs = []
+    moved = {}
+    for y, ids in by_y.items():
+        master = ids[0]
+        for nid in ids[1:]:
+            mpcs.append({"type": "equalDOF", "retained_node": master, "constrained_node": nid,
+                         "dofs": [1]})
+            moved[nid] = master
+    masses = []
+    extra = {}
+    for m in c["masses"]:
+        if m["dof"] == 1 and m["node"] in moved:
+            extra[moved[m["node"]]] = extra.get(moved[m["node"]], 0.0) + m["value"]
+        else:
+            masses.append(m)
+    for m in masses:
+        if m["dof"] == 1 and m["node"] in extra:
+            m["value"] += extra[m["node"]]
+    c["masses"] = masses
+    c["mp_constraints"] = mpcs
+    c["analysis"]["constraints"] = "Transformation"
+    return c
+
+
+def transformation_matrix(m_red, m_full):
+    """T with u_free(m_full) = T u_free(m_red) for a model and its copy without constraints."""
+    import numpy as np
+
+    T = np.zeros((m_full.num_free, m_red.num_free))
+    for dof in range(m_red.num_dofs):
+        f2 = m_full.free_index[dof]
+        if f2 < 0:
+            continue
+        f = m_red.free_index[dof]
+        if f >= 0:
+            T[f2, f] = 1.0
+        elif dof in m_red.slaves:
+            for md, c in m_red.slaves[dof]:
+                if m_red.free_index[md] >= 0:
+                    T[f2, m_red.free_index[md]] += c
+    return T
+
+
+def band_to_dense(band, n, bw):
+    import numpy as np
+
+    K = np.zeros((n, n))
+    for i in range(n):
+        for o in range(band.shape[1]):
+            j = i + o - bw
+            if 0 <= j < n:
+                K[i, j] = band[i, o]
+    return K

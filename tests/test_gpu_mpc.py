@@ -1,0 +1,66 @@
+"""GPU parity with multi-point constraints (rigidDiaphragm, equalDOF; Transformation handler)
+against the CPU oracle: one state determination within 1e-9 of the largest entry, transient
+histories within 1e-7 of peak with Newton iteration counts equal on >= 99% of steps."""
+import numpy as np
+import pytest
+
+from strut_b200 import model as M
+from strut_b200 import workloads as W
+from tests.helpers import equal_dof_floors_2d, rel_err_of_peak
+
+pytestmark = pytest.mark.gpu
+
+
+def _parity(gpu_lib, oracle, cases, steps):
+    models = [M.Model(c) for c in cases]
+    with gpu_lib.Analysis(models) as an:
+        an.run(steps)
+        got = [an.history(i) for i in range(len(models))]
+    for m, (gd, ge, gi) in zip(models, got):
+        rd, re, ri, rc, failed = oracle.run_transient(m, steps)
+        assert rc == 0, f"oracle failed at step {failed}"
+        for j in range(rd.shape[1]):
+            if np.max(np.abs(rd[:, j])) > 1e-9:
+                assert rel_err_of_peak(gd[:, j], rd[:, j]) <= 1e-7, f"disp {j}"
+        for j in range(re.shape[1]):
+            peak = np.max(np.abs(re[:, j, :]))
+            assert np.max(np.abs(ge[:, j, :] - re[:, j, :])) <= 1e-7 * peak, f"eforce {j}"
+        assert np.mean(gi == ri) >= 0.99
+
+
+@pytest.mark.parametrize("beam", ["forceBeamColumn3d", "dispBeamColumn3d"])
+def test_diaphragm_state_determination(gpu_lib, oracle, beam):
+    case = W.rc_frame3d_case(stories=2, bays_x=2, bays_y=1, steps=10, element="forceBeamColumn3d",
+                             beam_element=beam, diaphragm=True, seed=4)
+    m = M.Model(case)
+    u = np.random.default_rng(2).normal(0.0, 2e-3, m.num_free)
+    f_ref, band_ref, bw = oracle.state_determination(m, u)
+    with gpu_lib.Analysis([m]) as an:
+        (f_got, band_got), = an.state_determination([u])
+        assert an.band_info(0)[0] == bw
+    assert np.max(np.abs(f_got - f_ref)) <= 1e-9 * np.max(np.abs(f_ref))
+    assert np.max(np.abs(band_got - band_ref)) <= 1e-9 * np.max(np.abs(band_ref))
+
+
+def test_diaphragm_transient_bidirectional(gpu_lib, oracle):
+    case = W.rc_frame3d_case(stories=2, bays_x=2, bays_y=2, steps=100, element="forceBeamColumn3d",
+                             beam_element="dispBeamColumn3d", diaphragm=True, seed=12, pga_g=0.4,
+                             bidirectional=True, record_elements=(1, 20))
+    _parity(gpu_lib, oracle, [case], 100)
+
+
+def test_diaphragm_large_band(gpu_lib, oracle):
+    """A diaphragm frame whose band exceeds shared memory (global-memory LU path)."""
+    case = W.rc_frame3d_case(stories=5, bays_x=3, bays_y=3, steps=40, element="forceBeamColumn3d",
+                             beam_element="dispBeamColumn3d", diaphragm=True, seed=13, pga_g=0.35)
+    m = M.Model(case)
+    with gpu_lib.Analysis([m]) as an:
+        _bw, rw = an.band_info(0)
+    assert m.num_free * rw * 8 > 220 * 1024
+    _parity(gpu_lib, oracle, [case], 40)
+
+
+def test_equal_dof_2d_batch(gpu_lib, oracle):
+    cases = [equal_dof_floors_2d(W.rc_frame_case(stories=s, bays=2, steps=120, seed=20 + s, pga_g=0.4))
+             for s in (2, 3)]
+    _parity(gpu_lib, oracle, cases, 120)
