@@ -15,6 +15,7 @@ extern "C" {
 enum { S2_EPSMIN = 0, S2_EPSMAX, S2_EPSPL, S2_EPSS0, S2_SIGS0, S2_EPSR, S2_SIGR };
 enum { C2_ECMIN = 0, C2_DEPT = 1 };
 enum { S1_EPSP = 0, S1_ALPHA = 1 };
+enum { C1_MIN = 0, C1_END = 1, C1_SLOPE = 2 };
 
 typedef struct OFiberState {
     double eps, sig, tan;
@@ -30,6 +31,8 @@ void oracle_concrete02_trial(const StrutUniMaterial* m, const OFiberState* c, OF
                              double eps);
 void oracle_steel01_trial(const StrutUniMaterial* m, const OFiberState* c, OFiberState* t,
                           double eps);
+void oracle_concrete01_trial(const StrutUniMaterial* m, const OFiberState* c, OFiberState* t,
+                             double eps);
 void oracle_elastic_trial(const StrutUniMaterial* m, const OFiberState* c, OFiberState* t,
                           double eps);
 void oracle_fiber_trial(const StrutUniMaterial* m, const OFiberState* c, OFiberState* t,

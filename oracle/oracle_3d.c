@@ -44,7 +44,7 @@ int oracle_section3d_build(OSection3d* sd, const StrutUniMaterial* mats, int nma
         if (f->material < 0 || f->material >= nmat) return STRUT_BAD_ARG;
         int t = mats[f->material].type;
         if (t != STRUT_MAT_ELASTIC && t != STRUT_MAT_STEEL01 && t != STRUT_MAT_STEEL02 &&
-            t != STRUT_MAT_CONCRETE02)
+            t != STRUT_MAT_CONCRETE02 && t != STRUT_MAT_CONCRETE01)
             return STRUT_UNSUPPORTED;
         area_sum += f->area;
         qy_sum += f->area * f->z;

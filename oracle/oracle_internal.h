@@ -23,10 +23,13 @@ typedef struct OSection {
     int n_s1;
     double *s1_y, *s1_a;
     int* s1_mat;
+    int n_c1;
+    double *c1_y, *c1_a;
+    int* c1_mat;
 } OSection;
 
 /* Committed and trial states of one section instance: Steel02 slots, then Concrete02, then
- * Steel01 (each family in its padded runtime order). */
+ * Steel01, then Concrete01 (each family in its padded runtime order). */
 typedef struct OSecState {
     int n;
     OFiberState* c;

@@ -51,6 +51,103 @@ void oracle_fiber_init(const StrutUniMaterial* m, OFiberState* s) {
             s->sig = sigini;
         }
     }
+    if (m->type == STRUT_MAT_CONCRETE01) s->h[C1_SLOPE] = tangent;
+}
+
+/* Concrete01 (Kent-Scott-Park, no tension): materials/uniaxial/concrete01.mojo:3-70, the trial
+ * rule of ops.mojo:56-115 / fiber2d.mojo:1049-1101. */
+static void c1_envelope(double fpc, double epsc0, double fpcu, double epscu, double strain,
+                        double* sig, double* tan) {
+    if (strain > epsc0) {
+        double eta = strain / epsc0;
+        *sig = fpc * (2.0 * eta - eta * eta);
+        double Ec0 = (2.0 * fpc) / epsc0;
+        *tan = Ec0 * (1.0 - eta);
+    } else if (strain > epscu) {
+        *tan = (fpc - fpcu) / (epsc0 - epscu);
+        *sig = fpc + *tan * (strain - epsc0);
+    } else {
+        *sig = fpcu;
+        *tan = 0.0;
+    }
+}
+
+static void c1_unload(double fpc, double epsc0, double epscu, double min_strain, double stress,
+                      double* end_strain, double* slope) {
+    double temp_strain = min_strain;
+    if (temp_strain < epscu) temp_strain = epscu;
+    double eta = temp_strain / epsc0;
+    double ratio = 0.707 * (eta - 2.0) + 0.834;
+    if (eta < 2.0) ratio = 0.145 * eta * eta + 0.13 * eta;
+    double es = ratio * epsc0;
+    double temp1 = min_strain - es;
+    double Ec0 = (2.0 * fpc) / epsc0;
+    double temp2 = stress / Ec0;
+    if (temp1 > -1.0e-14) {
+        *end_strain = es;
+        *slope = Ec0;
+    } else if (temp1 <= temp2) {
+        *end_strain = min_strain - temp1;
+        *slope = stress / temp1;
+    } else {
+        *end_strain = min_strain - temp2;
+        *slope = Ec0;
+    }
+}
+
+void oracle_concrete01_trial(const StrutUniMaterial* m, const OFiberState* c, OFiberState* t,
+                             double eps) {
+    double fpc = m->p[0], epsc0 = m->p[1], fpcu = m->p[2], epscu = m->p[3];
+    double d_strain = eps - c->eps;
+    t->eps = eps;
+    if (fabs(d_strain) < 1.0e-14) {
+        t->sig = c->sig;
+        t->tan = c->tan;
+        t->h[C1_MIN] = c->h[C1_MIN];
+        t->h[C1_END] = c->h[C1_END];
+        t->h[C1_SLOPE] = c->h[C1_SLOPE];
+        return;
+    }
+    double min_strain = c->h[C1_MIN], end_strain = c->h[C1_END], slope = c->h[C1_SLOPE];
+    t->h[C1_MIN] = min_strain;
+    t->h[C1_END] = end_strain;
+    t->h[C1_SLOPE] = slope;
+    if (eps > 0.0) {
+        t->sig = 0.0;
+        t->tan = 0.0;
+        return;
+    }
+    double temp_stress = c->sig + slope * eps - slope * c->eps;
+    if (eps <= c->eps) {
+        /* _concrete01_reload: may move min_strain, end_strain and the unloading slope */
+        double rs, rt;
+        if (eps <= min_strain) {
+            min_strain = eps;
+            c1_envelope(fpc, epsc0, fpcu, epscu, eps, &rs, &rt);
+            c1_unload(fpc, epsc0, epscu, min_strain, rs, &end_strain, &slope);
+        } else if (eps <= end_strain) {
+            rt = slope;
+            rs = rt * (eps - end_strain);
+        } else {
+            rs = 0.0;
+            rt = 0.0;
+        }
+        t->h[C1_MIN] = min_strain;
+        t->h[C1_END] = end_strain;
+        t->h[C1_SLOPE] = slope;
+        t->sig = rs;
+        t->tan = rt;
+        if (temp_stress > t->sig) {
+            t->sig = temp_stress;
+            t->tan = slope;
+        }
+    } else if (temp_stress <= 0.0) {
+        t->sig = temp_stress;
+        t->tan = slope;
+    } else {
+        t->sig = 0.0;
+        t->tan = 0.0;
+    }
 }
 
 /* Concrete02 envelopes, concrete02.mojo:3-31. */
@@ -271,6 +368,7 @@ void oracle_fiber_trial(const StrutUniMaterial* m, const OFiberState* c, OFiberS
         case STRUT_MAT_STEEL02: oracle_steel02_trial(m, c, t, eps); break;
         case STRUT_MAT_CONCRETE02: oracle_concrete02_trial(m, c, t, eps); break;
         case STRUT_MAT_STEEL01: oracle_steel01_trial(m, c, t, eps); break;
+        case STRUT_MAT_CONCRETE01: oracle_concrete01_trial(m, c, t, eps); break;
         default: oracle_elastic_trial(m, c, t, eps); break;
     }
 }
@@ -285,18 +383,10 @@ void oracle_material_path(const StrutUniMaterial* m, const double* strains, int 
     t = c;
     for (int i = 0; i < n; ++i) {
         double eps = strains[i];
-        int skip = (m->type != STRUT_MAT_CONCRETE01) && (eps == t.eps);
+        int skip = eps == t.eps;
         if (!skip) {
             OFiberState next = t;
-            if (m->type == STRUT_MAT_STEEL02) {
-                oracle_steel02_trial(m, &c, &next, eps);
-            } else if (m->type == STRUT_MAT_CONCRETE02) {
-                oracle_concrete02_trial(m, &c, &next, eps);
-            } else if (m->type == STRUT_MAT_STEEL01) {
-                oracle_steel01_trial(m, &c, &next, eps);
-            } else {
-                oracle_elastic_trial(m, &c, &next, eps);
-            }
+            oracle_fiber_trial(m, &c, &next, eps);
             t = next;
         }
         out[2 * i + 0] = t.sig;

@@ -124,8 +124,6 @@ int oracle_section_build(OSection* sd, const StrutUniMaterial* mats, int nmat,
     for (int i = 0; i < nfib; ++i) {
         const StrutFiber* f = &fibers[off + i];
         if (f->material < 0 || f->material >= nmat) return STRUT_BAD_ARG;
-        int t = mats[f->material].type;
-        if (t == STRUT_MAT_CONCRETE01) return STRUT_UNSUPPORTED;
         area_sum += f->area;
         qz_sum += f->area * f->y;
     }
@@ -134,7 +132,7 @@ int oracle_section_build(OSection* sd, const StrutUniMaterial* mats, int nmat,
     sd->y_bar = qz_sum / area_sum;
     sd->mats = mats;
     double ik11 = 0.0, ik12 = 0.0, ik22 = 0.0;
-    int n_el = 0, n_s1 = 0;
+    int n_el = 0, n_s1 = 0, n_c1 = 0;
     for (int i = 0; i < nfib; ++i) {
         const StrutFiber* f = &fibers[off + i];
         double y_rel = f->y - sd->y_bar;
@@ -144,6 +142,7 @@ int oracle_section_build(OSection* sd, const StrutUniMaterial* mats, int nmat,
         ik22 += ks * y_rel * y_rel;
         if (mats[f->material].type == STRUT_MAT_ELASTIC) ++n_el;
         if (mats[f->material].type == STRUT_MAT_STEEL01) ++n_s1;
+        if (mats[f->material].type == STRUT_MAT_CONCRETE01) ++n_c1;
     }
     sd->n_el = n_el;
     sd->el_y = (double*)calloc(n_el + 1, sizeof(double));
@@ -153,7 +152,11 @@ int oracle_section_build(OSection* sd, const StrutUniMaterial* mats, int nmat,
     sd->s1_y = (double*)calloc(n_s1 + 1, sizeof(double));
     sd->s1_a = (double*)calloc(n_s1 + 1, sizeof(double));
     sd->s1_mat = (int*)calloc(n_s1 + 1, sizeof(int));
-    int ie = 0, i1 = 0;
+    sd->n_c1 = n_c1;
+    sd->c1_y = (double*)calloc(n_c1 + 1, sizeof(double));
+    sd->c1_a = (double*)calloc(n_c1 + 1, sizeof(double));
+    sd->c1_mat = (int*)calloc(n_c1 + 1, sizeof(int));
+    int ie = 0, i1 = 0, ic1 = 0;
     for (int i = 0; i < nfib; ++i) {
         const StrutFiber* f = &fibers[off + i];
         double y_rel = f->y - sd->y_bar;
@@ -167,6 +170,11 @@ int oracle_section_build(OSection* sd, const StrutUniMaterial* mats, int nmat,
             sd->s1_a[i1] = f->area;
             sd->s1_mat[i1] = f->material;
             ++i1;
+        } else if (mats[f->material].type == STRUT_MAT_CONCRETE01) {
+            sd->c1_y[ic1] = y_rel;
+            sd->c1_a[ic1] = f->area;
+            sd->c1_mat[ic1] = f->material;
+            ++ic1;
         }
     }
     sd->nonlinear_count = nfib - n_el;
@@ -191,13 +199,14 @@ int oracle_section_build(OSection* sd, const StrutUniMaterial* mats, int nmat,
 void oracle_section_free(OSection* sd) {
     free(sd->el_y); free(sd->el_a); free(sd->el_e);
     free(sd->s1_y); free(sd->s1_a); free(sd->s1_mat);
+    free(sd->c1_y); free(sd->c1_a); free(sd->c1_mat);
     free(sd->s2_y); free(sd->s2_a); free(sd->s2_mat); free(sd->s2_goff); free(sd->s2_gpad);
     free(sd->c2_y); free(sd->c2_a); free(sd->c2_mat); free(sd->c2_goff); free(sd->c2_gpad);
     memset(sd, 0, sizeof(*sd));
 }
 
 void oracle_section_state_alloc(const OSection* sd, OSecState* st) {
-    int n = sd->n_s2 + sd->n_c2 + sd->n_s1;
+    int n = sd->n_s2 + sd->n_c2 + sd->n_s1 + sd->n_c1;
     st->n = n;
     st->c = (OFiberState*)calloc(n + 1, sizeof(OFiberState));
     st->t = (OFiberState*)calloc(n + 1, sizeof(OFiberState));
@@ -210,6 +219,8 @@ void oracle_section_state_alloc(const OSection* sd, OSecState* st) {
             oracle_fiber_init(&sd->mats[sd->c2_mat[k]], &st->c[sd->n_s2 + k]);
     for (int k = 0; k < sd->n_s1; ++k)
         oracle_fiber_init(&sd->mats[sd->s1_mat[k]], &st->c[sd->n_s2 + sd->n_c2 + k]);
+    for (int k = 0; k < sd->n_c1; ++k)
+        oracle_fiber_init(&sd->mats[sd->c1_mat[k]], &st->c[sd->n_s2 + sd->n_c2 + sd->n_s1 + k]);
     memcpy(st->t, st->c, sizeof(OFiberState) * (n + 1));
 }
 
@@ -311,6 +322,20 @@ void oracle_section_response(const OSection* sd, OSecState* st, double eps0, dou
                              eps0 - y * kappa);
         double fs = st->t[slot].sig * sd->s1_a[k];
         double ks = st->t[slot].tan * sd->s1_a[k];
+        acc[0] += fs;
+        acc[1] += -fs * y;
+        acc[2] += ks;
+        acc[3] += -ks * y;
+        acc[4] += ks * y * y;
+    }
+    /* Concrete01 fibers one by one after Steel01 (fiber2d.mojo:1388-1420) */
+    for (int k = 0; k < sd->n_c1; ++k) {
+        int slot = sd->n_s2 + sd->n_c2 + sd->n_s1 + k;
+        double y = sd->c1_y[k];
+        oracle_concrete01_trial(&sd->mats[sd->c1_mat[k]], &st->c[slot], &st->t[slot],
+                                eps0 - y * kappa);
+        double fs = st->t[slot].sig * sd->c1_a[k];
+        double ks = st->t[slot].tan * sd->c1_a[k];
         acc[0] += fs;
         acc[1] += -fs * y;
         acc[2] += ks;

@@ -64,7 +64,7 @@ __device__ __forceinline__ void fiber_phase3(const Geo& g, const DevSection& sd,
                                              const double (*pt)[3], double* fo) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int nip = E.nip;
-    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     const int n_s = nip * sd.n_s2;
     const int ws = steel_warps(n_s, nw);
     if (w < ws) {
@@ -98,7 +98,7 @@ __device__ __forceinline__ void fiber_phase3(const Geo& g, const DevSection& sd,
         }
         return;
     }
-    const int n_o_sec = sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_o_sec = sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     const int n_o = nip * n_o_sec;
     const int nwo = nw - ws;
     for (int k = (w - ws) * 32 + lane; k < n_o; k += nwo * 32) {
@@ -137,6 +137,12 @@ __device__ __forceinline__ void fiber_phase3(const Geo& g, const DevSection& sd,
             steel01_trial(mat, c, strain, t);
             o[0] = t.sig * A;
             o[1] = t.tan * A;
+        } else if (jj < sd.n_c2 + sd.n_s1 + sd.n_c1) {
+            C1State c, t;
+            load_c1(sv, ip * sd.n_c1 + (jj - sd.n_c2 - sd.n_s1), c);
+            concrete01_trial(mat, c, strain, t);
+            o[0] = t.sig * A;
+            o[1] = t.tan * A;
         } else {
             const double ks = mat.p[0] * A;
             o[0] = ks * strain;
@@ -154,7 +160,7 @@ __device__ __forceinline__ void sum_phase3(const DevSection& sd, int nip, const 
     const int t = threadIdx.x;
     const int n_sum = nip * 8;
     if ((t & ~31) >= n_sum) return;
-    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     const int n_nl = n_tot - sd.n_el;
     const bool act = t < n_sum;
     const int ip = t >> 3, b = t & 7;
@@ -623,7 +629,7 @@ __device__ void element3d_process(const Geo& g, const DevSection& sd, const DevE
         return;
     }
     derive_element(g, sd, E, sv, const_cast<double*>(sv.c2d), const_cast<double*>(sv.s2d));
-    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     double* ys = const_cast<double*>(sv.s2d) + 12 * E.s2_blk;
     double* zs = ys + ((n_tot + 1) & ~1);
     double* fo = zs + ((n_tot + 1) & ~1);

@@ -114,10 +114,21 @@ struct StageView {
     const double* s2;   // 10 fields x s2_blk
     const int* kon;     // s2_blk
     const double* s1;   // 5 fields x s1_blk
+    const double* c1;   // 6 fields x c1_blk
     const double* c2d;  // C2Derived, 5 fields x c2_blk (shared-memory views only)
     const double* s2d;  // S2Derived, 12 fields x s2_blk (shared-memory views only)
-    int c2_blk, s2_blk, s1_blk;
+    int c2_blk, s2_blk, s1_blk, c1_blk;
 };
+
+__device__ __forceinline__ void load_c1(const StageView& sv, int idx, C1State& c) {
+    const int B = sv.c1_blk;
+    c.eps = sv.c1[0 * B + idx];
+    c.sig = sv.c1[1 * B + idx];
+    c.tan = sv.c1[2 * B + idx];
+    c.emin = sv.c1[3 * B + idx];
+    c.eend = sv.c1[4 * B + idx];
+    c.slope = sv.c1[5 * B + idx];
+}
 
 __device__ __forceinline__ void load_c2(const StageView& sv, int idx, C2State& c) {
     const int B = sv.c2_blk;
@@ -268,6 +279,19 @@ __device__ __forceinline__ void section_eval_team(const Geo& g, const DevSection
         }
     }
     base += sd.n_s1;
+    for (int j0 = 0; j0 < sd.n_c1; j0 += kVLanes) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = j0 + s * TEAM + r;
+            if (j >= sd.n_c1) continue;
+            C1State c, t;
+            load_c1(sv, ip * sd.n_c1 + j, c);
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            concrete01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            acc_fiber(acc[s], t.sig * A, t.tan * A, y);
+        }
+    }
+    base += sd.n_c1;
     for (int j0 = 0; j0 < sd.n_el; j0 += kVLanes) {
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -385,7 +409,7 @@ __device__ __forceinline__ void fiber_phase(const Geo& g, const DevSection& sd,
                                             const double* pe, const double* pk, double* fo) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int nip = E.nip;
-    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     const int n_s = nip * sd.n_s2;
     const int ws = steel_warps(n_s, nw);
     if (w < ws) {
@@ -419,7 +443,7 @@ __device__ __forceinline__ void fiber_phase(const Geo& g, const DevSection& sd,
         }
         return;
     }
-    const int n_o_sec = sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_o_sec = sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     const int n_o = nip * n_o_sec;
     const int nwo = nw - ws;
     for (int k = (w - ws) * 32 + lane; k < n_o; k += nwo * 32) {
@@ -457,6 +481,12 @@ __device__ __forceinline__ void fiber_phase(const Geo& g, const DevSection& sd,
             steel01_trial(mat, c, e0 - y * ka, t);
             o[0] = t.sig * A;
             o[1] = t.tan * A;
+        } else if (jj < sd.n_c2 + sd.n_s1 + sd.n_c1) {
+            C1State c, t;
+            load_c1(sv, ip * sd.n_c1 + (jj - sd.n_c2 - sd.n_s1), c);
+            concrete01_trial(mat, c, e0 - y * ka, t);
+            o[0] = t.sig * A;
+            o[1] = t.tan * A;
         } else {
             // elastic: ks = E A, fs = ks (eps0 - y kappa)
             const double ks = mat.p[0] * A;
@@ -474,7 +504,7 @@ __device__ __forceinline__ void sum_phase(const DevSection& sd, int nip, const d
     const int t = threadIdx.x;
     const int n_sum = nip * 8;
     if ((t & ~31) >= n_sum) return;  // whole warp outside
-    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     const int n_nl = n_tot - sd.n_el;
     const bool act = t < n_sum;
     const int ip = t >> 3, b = t & 7;
@@ -845,10 +875,12 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
     double* c2 = sm;
     double* s2 = c2 + 5 * E.c2_blk;
     double* s1 = s2 + 10 * E.s2_blk;
-    int* kon = reinterpret_cast<int*>(s1 + 5 * E.s1_blk);
+    double* c1 = s1 + 5 * E.s1_blk;
+    int* kon = reinterpret_cast<int*>(c1 + 6 * E.c1_blk);
     sv.c2 = c2;
     sv.s2 = s2;
     sv.s1 = s1;
+    sv.c1 = c1;
     sv.kon = kon;
     // derived constants follow the staged history (kon occupies s2_blk ints, s2_blk % 4 == 0)
     sv.c2d = reinterpret_cast<const double*>(kon + E.s2_blk);
@@ -856,7 +888,8 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
     sv.c2_blk = E.c2_blk;
     sv.s2_blk = E.s2_blk;
     sv.s1_blk = E.s1_blk;
-    const uint32_t bytes = (uint32_t)(8 * (5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) +
+    sv.c1_blk = E.c1_blk;
+    const uint32_t bytes = (uint32_t)(8 * (5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
                                       4 * E.s2_blk);
     if (bytes == 0) return true;
     if (threadIdx.x == 0) {
@@ -870,6 +903,8 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
         if (E.s2_blk) bulk_g2s(kon, fs.s2_kon + E.s2_off, 4u * E.s2_blk, bar);
         for (int f = 0; f < 5 && E.s1_blk; ++f)
             bulk_g2s(s1 + f * E.s1_blk, fs.s1 + f * fs.s1_n + E.s1_off, 8u * E.s1_blk, bar);
+        for (int f = 0; f < 6 && E.c1_blk; ++f)
+            bulk_g2s(c1 + f * E.c1_blk, fs.c1 + f * fs.c1_n + E.c1_off, 8u * E.c1_blk, bar);
     }
     const uint32_t ph = phase;
     phase ^= 1u;
@@ -1001,7 +1036,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     }
     derive_element(g, sd, E, sv, const_cast<double*>(sv.c2d), const_cast<double*>(sv.s2d));
     // the section's fiber y (phase-2 sums) and the per-fiber results of phase 1 follow
-    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     double* ys = const_cast<double*>(sv.s2d) + 12 * E.s2_blk;
     double* fo = ys + ((n_tot + 1) & ~1);
     for (int gg = tid; gg < n_tot; gg += blockDim.x) ys[gg] = __ldg(g.y + sd.geo_off + gg);
@@ -1080,7 +1115,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
             atomicAdd(&counters[3], (unsigned long long)E.io_bytes);
             atomicAdd(&counters[1], (unsigned long long)nip);
             atomicAdd(&counters[2], (unsigned long long)nip *
-                                        (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
+                                        (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el));
         }
         return;
     }
@@ -1320,7 +1355,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         atomicMax(&counters[5], (unsigned long long)S.local_iters);
         atomicAdd(&counters[1], (unsigned long long)S.section_evals);
         atomicAdd(&counters[2], (unsigned long long)S.section_evals *
-                                    (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
+                                    (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el));
     }
     __syncthreads();
     if (tid < 36) ek[E.ek_off + tid] = S.k[tid];
@@ -1411,6 +1446,18 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
             steel01_trial(g.mats[__ldg(g.m + base + j)], c, strain(base + j), t);
             F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.epsp; F[4 * N] = t.alpha;
         }
+        base += sd.n_s1;
+        for (int j = r; j < sd.n_c1; j += TEAM) {
+            const long long idx = E.c1_off + team * sd.n_c1 + j;
+            double* F = fs.c1 + idx;
+            const long long N = fs.c1_n;
+            C1State c, t;
+            c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.emin = F[3 * N]; c.eend = F[4 * N];
+            c.slope = F[5 * N];
+            concrete01_trial(g.mats[__ldg(g.m + base + j)], c, strain(base + j), t);
+            F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.emin; F[4 * N] = t.eend;
+            F[5 * N] = t.slope;
+        }
     }
     if (three_d) {
         // 3D recorders run as a separate pass (element state determination after commit)
@@ -1468,9 +1515,11 @@ __global__ void __launch_bounds__(kTeamThreads) commit_kernel(
         gv.s2 = fs.s2 + E.s2_off;
         gv.kon = fs.s2_kon + E.s2_off;
         gv.s1 = fs.s1 + E.s1_off;
+        gv.c1 = fs.c1 + E.c1_off;
         gv.c2_blk = (int)fs.c2_n;
         gv.s2_blk = (int)fs.s2_n;
         gv.s1_blk = (int)fs.s1_n;
+        gv.c1_blk = (int)fs.c1_n;
         section_eval_team<TEAM>(g, sd, gv, team, eps0, kappa, r, part[team]);
     }
     __syncthreads();

@@ -5,6 +5,8 @@
 //   Concrete02  src/mojo/sections/fiber2d.mojo:1190-1244 (SIMD form 1785-1972), envelopes
 //               src/mojo/materials/uniaxial/concrete02.mojo:3-31
 //   Steel01     src/mojo/sections/fiber2d.mojo:1021-1045
+//   Concrete01  src/mojo/sections/fiber2d.mojo:1049-1101, envelope / unloading / reloading
+//               src/mojo/materials/uniaxial/concrete01.mojo:3-70
 //   Elastic     src/mojo/materials/uniaxial/ops.mojo:10-21
 // Every trial state is a pure function of the committed state and the strain; nothing is kept
 // between calls.  That is what lets the element kernels keep trial fiber state out of HBM.
@@ -42,7 +44,9 @@ enum {
     // Steel01
     S1K_H = 0,         // (b E0) / (1 - b)
     S1K_EH = 1,        // (E0 H) / (E0 + H)
-    S1K_E0PH = 2       // E0 + H
+    S1K_E0PH = 2,      // E0 + H
+    // Concrete01
+    C1K_EC0 = 0        // (2 fpc) / epsc0
 };
 
 // Committed history of one fiber, by family (structure-of-arrays in HBM, these are the
@@ -57,6 +61,92 @@ struct S2State {
 struct S1State {
     double eps, sig, tan, epsp, alpha;
 };
+struct C1State {
+    double eps, sig, tan, emin, eend, slope;  // min strain, end strain, unloading slope
+};
+
+// Concrete01 (Kent-Scott-Park without tension) trial from committed c.
+__device__ __forceinline__ void concrete01_trial(const DevMat& m, const C1State& c, double eps,
+                                                 C1State& t) {
+    const double fpc = m.p[0], epsc0 = m.p[1], fpcu = m.p[2], epscu = m.p[3];
+    const double Ec0 = m.k[C1K_EC0];
+    t.eps = eps;
+    const double d_strain = eps - c.eps;
+    if (fabs(d_strain) < 1.0e-14) {
+        t.sig = c.sig;
+        t.tan = c.tan;
+        t.emin = c.emin;
+        t.eend = c.eend;
+        t.slope = c.slope;
+        return;
+    }
+    double emin = c.emin, eend = c.eend, slope = c.slope;
+    if (eps > 0.0) {
+        t.sig = 0.0;
+        t.tan = 0.0;
+        t.emin = emin;
+        t.eend = eend;
+        t.slope = slope;
+        return;
+    }
+    const double temp_stress = c.sig + slope * eps - slope * c.eps;
+    if (eps <= c.eps) {
+        double rs, rt;
+        if (eps <= emin) {
+            // envelope, then the new unloading point (_concrete01_reload / _unload)
+            emin = eps;
+            if (eps > epsc0) {
+                const double eta = eps / epsc0;
+                rs = fpc * (2.0 * eta - eta * eta);
+                rt = Ec0 * (1.0 - eta);
+            } else if (eps > epscu) {
+                rt = (fpc - fpcu) / (epsc0 - epscu);
+                rs = fpc + rt * (eps - epsc0);
+            } else {
+                rs = fpcu;
+                rt = 0.0;
+            }
+            double ts = emin < epscu ? epscu : emin;
+            const double eta = ts / epsc0;
+            double ratio = 0.707 * (eta - 2.0) + 0.834;
+            if (eta < 2.0) ratio = 0.145 * eta * eta + 0.13 * eta;
+            const double es = ratio * epsc0;
+            const double temp1 = emin - es;
+            const double temp2 = rs / Ec0;
+            if (temp1 > -1.0e-14) {
+                eend = es;
+                slope = Ec0;
+            } else if (temp1 <= temp2) {
+                eend = emin - temp1;
+                slope = rs / temp1;
+            } else {
+                eend = emin - temp2;
+                slope = Ec0;
+            }
+        } else if (eps <= eend) {
+            rt = slope;
+            rs = rt * (eps - eend);
+        } else {
+            rs = 0.0;
+            rt = 0.0;
+        }
+        t.sig = rs;
+        t.tan = rt;
+        if (temp_stress > t.sig) {
+            t.sig = temp_stress;
+            t.tan = slope;
+        }
+    } else if (temp_stress <= 0.0) {
+        t.sig = temp_stress;
+        t.tan = slope;
+    } else {
+        t.sig = 0.0;
+        t.tan = 0.0;
+    }
+    t.emin = emin;
+    t.eend = eend;
+    t.slope = slope;
+}
 
 __device__ __forceinline__ void c2_compr_envlp(const DevMat& m, double strain, double& sig,
                                                double& tan) {

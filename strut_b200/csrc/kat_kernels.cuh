@@ -46,6 +46,16 @@ __global__ void material_path_kernel(DevMat m, const double* __restrict__ strain
             out[2 * i + 1] = t.tan;
             c = t;
         }
+    } else if (m.type == 2) {
+        C1State c{0.0, 0.0, m.k[C1K_EC0], 0.0, 0.0, m.k[C1K_EC0]};
+        C1State t = c;
+        for (int i = 0; i < n; ++i) {
+            const double eps = strains[i];
+            if (eps != t.eps) concrete01_trial(m, c, eps, t);
+            out[2 * i] = t.sig;
+            out[2 * i + 1] = t.tan;
+            c = t;
+        }
     } else if (m.type == 1) {
         S1State c{0.0, 0.0, m.p[1], 0.0, 0.0};
         S1State t = c;
@@ -78,6 +88,7 @@ struct BatchState {
     double* s2;
     int* kon;
     double* s1;
+    double* c1;
     long long n_inst;
 };
 
@@ -147,6 +158,24 @@ __global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd
         }
     }
     base += sd.n_s1;
+    {
+        const long long N = bs.n_inst * sd.n_c1;
+        for (int j = lane; j < sd.n_c1; j += 32) {
+            double* F = bs.c1 + i * sd.n_c1 + j;
+            C1State c, t;
+            c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.emin = F[3 * N]; c.eend = F[4 * N];
+            c.slope = F[5 * N];
+            const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
+            concrete01_trial(g.mats[__ldg(g.m + base + j)], c, eps0 - y * kappa, t);
+            if (commit) {
+                F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.emin;
+                F[4 * N] = t.eend; F[5 * N] = t.slope;
+            }
+            const double fs = t.sig * A, ks = t.tan * A;
+            a0 += fs; a1 += -fs * y; a2 += ks; a3 += -ks * y; a4 += ks * y * y;
+        }
+    }
+    base += sd.n_c1;
     for (int j = lane; j < sd.n_el; j += 32) {
         const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
         const double ks = g.mats[__ldg(g.m + base + j)].p[0] * A;
@@ -227,6 +256,19 @@ __global__ void section3d_path_kernel(Geo g, DevSection sd, BatchState bs,
             acc(t.sig * A, t.tan * A, y, z, false);
         }
         base += sd.n_s1;
+        for (int j = lane; j < sd.n_c1; j += 32) {
+            const long long N = sd.n_c1;
+            double* F = bs.c1 + j;
+            C1State c, t;
+            c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.emin = F[3 * N]; c.eend = F[4 * N];
+            c.slope = F[5 * N];
+            const double y = g.y[base + j], z = g.z[base + j], A = g.a[base + j];
+            concrete01_trial(g.mats[g.m[base + j]], c, e0 + z * ky - y * kz, t);
+            F[0] = t.eps; F[N] = t.sig; F[2 * N] = t.tan; F[3 * N] = t.emin; F[4 * N] = t.eend;
+            F[5 * N] = t.slope;
+            acc(t.sig * A, t.tan * A, y, z, false);
+        }
+        base += sd.n_c1;
         for (int j = lane; j < sd.n_el; j += 32) {
             const double y = g.y[base + j], z = g.z[base + j], A = g.a[base + j];
             const double ks = g.mats[g.m[base + j]].p[0] * A;

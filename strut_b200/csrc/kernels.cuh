@@ -2,7 +2,8 @@
 //
 // HBM layout (all instances concatenated, instance-major):
 //   fiber geometry   per section definition, families contiguous: Steel02 | Concrete02 |
-//                    Steel01 | Elastic; y relative to the area centroid, area, material index
+//                    Steel01 | Concrete01 | Elastic; y (and z) relative to the area centroid,
+//                    area, material index
 //   fiber history    structure-of-arrays per family, committed state only.  Element e owns
 //                    one block per family: [ip0 fibers | ip1 fibers | ...] padded to 4 entries,
 //                    so every field block is a 32-byte aligned contiguous run that one
@@ -51,7 +52,7 @@ struct DevSection {
     int el_uniform;
     int init_valid;
     int all_elastic;
-    int dim, pad;
+    int dim, n_c1;
     double f00, f01, f11;
 };
 
@@ -62,6 +63,7 @@ struct DevElem {
     int dof[12];                // absolute indices into the concatenated full u vector
     int s2_off, c2_off, s1_off; // block offsets into family arrays
     int s2_blk, c2_blk, s1_blk; // block lengths (multiples of 4)
+    int c1_off, c1_blk;         // Concrete01 block
     long long ek_off, ef_off;   // offsets of this element's k (nd x nd) and f (nd)
     double L, inv_L, c, s, c_div, s_div, L_sync, c_sync, s_sync;
     double xi[kMaxIp], w[kMaxIp];
@@ -122,6 +124,8 @@ struct FiberState {
     long long s2_n;
     double* s1;
     long long s1_n;
+    double* c1;  // Concrete01: eps, sig, tan, min strain, end strain, unloading slope
+    long long c1_n;
 };
 
 struct Geo {

@@ -74,6 +74,8 @@ DevMat make_devmat(const StrutUniMaterial& m) {
         d.k[S2K_DNEG] = 2.0 * (a2 * epsy);
         d.k[S2K_E0MESH] = E0 - Esh;
         d.k[S2K_ESHEPSY] = Esh * epsy;
+    } else if (m.type == STRUT_MAT_CONCRETE01) {
+        d.k[C1K_EC0] = (2.0 * p[0]) / p[1];
     } else if (m.type == STRUT_MAT_STEEL01) {
         const double E0 = p[1], b = p[2];
         const double H = (b * E0) / (1.0 - b);
@@ -105,7 +107,7 @@ struct SectionPack {
 // Builds one FiberSection2d definition (fiber2d.mojo:3323-3455: area centroid, families,
 // initial flexibility) or, with dim 3, one FiberSection3d (fiber3d.mojo:633-720: centroid
 // (y_bar, z_bar) = (sum A y, sum A z) / sum A, coordinates relative to it).  Families are
-// stored in the order Steel02 | Concrete02 | Steel01 | Elastic.  mat_base offsets material
+// stored in the order Steel02 | Concrete02 | Steel01 | Concrete01 | Elastic.  mat_base offsets material
 // indices into the global table.
 int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fibers, int off,
                  int count, int mat_base, int dim, SectionPack& sp) {
@@ -116,7 +118,7 @@ int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fiber
         if (f.material < 0 || f.material >= nmat) return fail(STRUT_BAD_ARG, "fiber material out of range");
         const int t = mats[f.material].type;
         if (t != STRUT_MAT_ELASTIC && t != STRUT_MAT_STEEL01 && t != STRUT_MAT_STEEL02 &&
-            t != STRUT_MAT_CONCRETE02)
+            t != STRUT_MAT_CONCRETE02 && t != STRUT_MAT_CONCRETE01)
             return fail(STRUT_UNSUPPORTED, "fiber material type not implemented on this path");
         area_sum += f.area;
         qy_sum += f.area * f.z;
@@ -137,10 +139,10 @@ int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fiber
         ik12 += -ks * y_rel;
         ik22 += ks * y_rel * y_rel;
     }
-    const int order[4] = {STRUT_MAT_STEEL02, STRUT_MAT_CONCRETE02, STRUT_MAT_STEEL01,
-                          STRUT_MAT_ELASTIC};
-    int counts[4] = {0, 0, 0, 0};
-    for (int fam = 0; fam < 4; ++fam) {
+    const int order[5] = {STRUT_MAT_STEEL02, STRUT_MAT_CONCRETE02, STRUT_MAT_STEEL01,
+                          STRUT_MAT_CONCRETE01, STRUT_MAT_ELASTIC};
+    int counts[5] = {0, 0, 0, 0, 0};
+    for (int fam = 0; fam < 5; ++fam) {
         for (int i = 0; i < count; ++i) {
             const StrutFiber& f = fibers[off + i];
             if (mats[f.material].type != order[fam]) continue;
@@ -154,8 +156,9 @@ int pack_section(const StrutUniMaterial* mats, int nmat, const StrutFiber* fiber
     sd.n_s2 = counts[0];
     sd.n_c2 = counts[1];
     sd.n_s1 = counts[2];
-    sd.n_el = counts[3];
-    sd.all_elastic = (sd.n_s2 + sd.n_c2 + sd.n_s1) == 0;
+    sd.n_c1 = counts[3];
+    sd.n_el = counts[4];
+    sd.all_elastic = (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1) == 0;
     sd.el_uniform = 0;
     if (sd.n_el > 0) {
         sd.el_uniform = 1;
@@ -684,7 +687,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     std::vector<double> sl_coef;
     bool any_mpc = false;
     for (int inst = 0; inst < num_instances; ++inst) any_mpc = any_mpc || models[inst].num_slaves > 0;
-    long long c2_total = 0, s2_total = 0, s1_total = 0;
+    long long c2_total = 0, s2_total = 0, s1_total = 0, c1_total = 0;
     std::vector<int> sec_base(num_instances);
     int u_off = 0, f_off = 0;
     long long band_off = 0;
@@ -914,20 +917,25 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             E.s1_off = (int)s1_total;
             E.s1_blk = round4(E.nip * sd.n_s1);
             s1_total += E.s1_blk;
+            E.c1_off = (int)c1_total;
+            E.c1_blk = round4(E.nip * sd.n_c1);
+            c1_total += E.c1_blk;
             h->max_nip = std::max(h->max_nip, E.nip);
             // staged history + derived constants (Concrete02 5, Steel02 12 doubles per fiber) +
             // the section's fiber y + per-fiber stress and tangent of every point
-            const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el;
-            const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk) + 4 * (size_t)E.s2_blk +
+            const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
+            const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
+                                4 * (size_t)E.s2_blk +
                                 8 * (size_t)(5 * E.c2_blk + 12 * E.s2_blk) +
                                 8 * (size_t)((three_d ? 2 : 1) * ((n_tot + 1) & ~1) + 2 * E.nip * n_tot);
             h->elem_smem = std::max(h->elem_smem, smem);
-            h->elem_fibers.push_back((long long)E.nip * (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_el));
+            h->elem_fibers.push_back((long long)E.nip * (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el));
             {
-                // committed history read once (Concrete02 / Steel01 5 doubles, Steel02 10
-                // doubles + kon), element state read + written, k and f written, 6 dofs read,
-                // the element record itself
-                const double fib = (double)E.nip * (40.0 * sd.n_c2 + 84.0 * sd.n_s2 + 40.0 * sd.n_s1);
+                // committed history read once (Concrete02 / Steel01 5 doubles, Concrete01 6,
+                // Steel02 10 doubles + kon), element state read + written, k and f written,
+                // the element's dofs read, the element record itself
+                const double fib = (double)E.nip * (40.0 * sd.n_c2 + 84.0 * sd.n_s2 + 40.0 * sd.n_s1 +
+                                                    48.0 * sd.n_c1);
                 const double est = three_d ? 8.0 * (5 + 3 * E.nip) : 8.0 * (6 + 2 * E.nip);
                 E.io_bytes = fib + 2.0 * est + 8.0 * (nd * nd + nd) + 8.0 * nd + (double)sizeof(DevElem);
                 E.commit_bytes = 2.0 * fib + est + 8.0 * nd + (double)sizeof(DevElem);
@@ -1158,7 +1166,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         const long long c2n = round4((int)std::max<long long>(c2_total, 4));
         const long long s2n = round4((int)std::max<long long>(s2_total, 4));
         const long long s1n = round4((int)std::max<long long>(s1_total, 4));
-        std::vector<double> c2(5 * c2n, 0.0), s2(10 * s2n, 0.0), s1(5 * s1n, 0.0);
+        const long long c1n = round4((int)std::max<long long>(c1_total, 4));
+        std::vector<double> c2(5 * c2n, 0.0), s2(10 * s2n, 0.0), s1(5 * s1n, 0.0), c1(6 * c1n, 0.0);
         std::vector<int> kon(s2n, 0);
         for (const DevElem& E : elems) {
             const DevSection& sd = sp.secs[E.sec];
@@ -1185,14 +1194,22 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
                     const DevMat& m = mats[sp.m[base + j]];
                     s1[2 * s1n + E.s1_off + ip * sd.n_s1 + j] = m.p[1];
                 }
+                base += sd.n_s1;
+                for (int j = 0; j < sd.n_c1; ++j) {
+                    const DevMat& m = mats[sp.m[base + j]];
+                    c1[2 * c1n + E.c1_off + ip * sd.n_c1 + j] = m.k[C1K_EC0];
+                    c1[5 * c1n + E.c1_off + ip * sd.n_c1 + j] = m.k[C1K_EC0];
+                }
             }
         }
         if ((rc = upload(&h->fs.c2, c2, al)) || (rc = upload(&h->fs.s2, s2, al)) ||
-            (rc = upload(&h->fs.s2_kon, kon, al)) || (rc = upload(&h->fs.s1, s1, al)))
+            (rc = upload(&h->fs.s2_kon, kon, al)) || (rc = upload(&h->fs.s1, s1, al)) ||
+            (rc = upload(&h->fs.c1, c1, al)))
             return bail(rc);
         h->fs.c2_n = c2n;
         h->fs.s2_n = s2n;
         h->fs.s1_n = s1n;
+        h->fs.c1_n = c1n;
     }
     InstArrays& A = h->A;
     std::memset(&A, 0, sizeof(A));
@@ -1717,7 +1734,6 @@ int strut_gpu_material_path(const StrutUniMaterial* material, const double* stra
     if (!material || (n > 0 && (!strains || !out)) || n < 0) return fail(STRUT_BAD_ARG, "bad arguments");
     if (n == 0) return STRUT_OK;
     DevMat m = make_devmat(*material);
-    if (m.type == STRUT_MAT_CONCRETE01) return fail(STRUT_UNSUPPORTED, "Concrete01 not implemented on this path");
     double *d_s = nullptr, *d_o = nullptr;
     CK(cudaMalloc((void**)&d_s, n * sizeof(double)));
     CK(cudaMalloc((void**)&d_o, 2 * n * sizeof(double)));
@@ -1737,12 +1753,14 @@ int strut_gpu_material_path(const StrutUniMaterial* material, const double* stra
 // the section sp.secs[0], laid out as section_batch_kernel reads it.
 static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>& mats, long long n_inst,
                                 std::vector<double>& s2, std::vector<double>& c2, std::vector<double>& s1,
-                                std::vector<int>& kon) {
+                                std::vector<double>& c1, std::vector<int>& kon) {
     const DevSection& sd = sp.secs[0];
-    const long long n2 = n_inst * sd.n_s2, n3 = n_inst * sd.n_c2, n1 = n_inst * sd.n_s1;
+    const long long n2 = n_inst * sd.n_s2, n3 = n_inst * sd.n_c2, n1 = n_inst * sd.n_s1,
+                    n4 = n_inst * sd.n_c1;
     s2.assign(10 * std::max<long long>(n2, 1), 0.0);
     c2.assign(5 * std::max<long long>(n3, 1), 0.0);
     s1.assign(5 * std::max<long long>(n1, 1), 0.0);
+    c1.assign(6 * std::max<long long>(n4, 1), 0.0);
     kon.assign(std::max<long long>(n2, 1), 0);
     for (long long i = 0; i < n_inst; ++i) {
         int base = sd.geo_off;
@@ -1761,6 +1779,11 @@ static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>
         for (int j = 0; j < sd.n_c2; ++j) c2[2 * n3 + i * sd.n_c2 + j] = mats[sp.m[base + j]].k[C2K_EC0];
         base += sd.n_c2;
         for (int j = 0; j < sd.n_s1; ++j) s1[2 * n1 + i * sd.n_s1 + j] = mats[sp.m[base + j]].p[1];
+        base += sd.n_s1;
+        for (int j = 0; j < sd.n_c1; ++j) {
+            c1[2 * n4 + i * sd.n_c1 + j] = mats[sp.m[base + j]].k[C1K_EC0];
+            c1[5 * n4 + i * sd.n_c1 + j] = mats[sp.m[base + j]].k[C1K_EC0];
+        }
     }
 }
 
@@ -1794,11 +1817,11 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
     b->geo.m = d_m;
     b->geo.mats = d_mats;
     b->geo.secs = d_secs;
-    std::vector<double> s2, c2, s1;
+    std::vector<double> s2, c2, s1, c1;
     std::vector<int> kon;
-    batch_initial_state(sp, mats, n_inst, s2, c2, s1, kon);
+    batch_initial_state(sp, mats, n_inst, s2, c2, s1, c1, kon);
     if ((rc = upload(&b->bs.s2, s2, al)) || (rc = upload(&b->bs.c2, c2, al)) || (rc = upload(&b->bs.s1, s1, al)) ||
-        (rc = upload(&b->bs.kon, kon, al))) {
+        (rc = upload(&b->bs.c1, c1, al)) || (rc = upload(&b->bs.kon, kon, al))) {
         delete b;
         return rc;
     }
@@ -1828,14 +1851,14 @@ int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_
 int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double* out, int32_t* n_fibers) {
     if (!b || instance < 0 || instance >= b->n_inst) return fail(STRUT_BAD_ARG, "bad arguments");
     const DevSection& sd = b->sd;
-    const int nf = sd.n_s2 + sd.n_c2 + sd.n_s1;
+    const int nf = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1;
     if (n_fibers) *n_fibers = nf;
     if (!out) return STRUT_OK;
     CK(cudaDeviceSynchronize());
     // 16 doubles per fiber: the family's committed fields in declaration order, kon in slot 15
     std::vector<double> o((size_t)nf * 16, 0.0);
     const long long n2 = (long long)b->n_inst * sd.n_s2, n3 = (long long)b->n_inst * sd.n_c2,
-                    n1 = (long long)b->n_inst * sd.n_s1;
+                    n1 = (long long)b->n_inst * sd.n_s1, n4 = (long long)b->n_inst * sd.n_c1;
     for (int j = 0; j < sd.n_s2; ++j) {
         for (int f = 0; f < 10; ++f)
             CK(cudaMemcpy(&o[(size_t)j * 16 + f], b->bs.s2 + f * n2 + (long long)instance * sd.n_s2 + j, sizeof(double),
@@ -1852,6 +1875,10 @@ int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double
         for (int f = 0; f < 5; ++f)
             CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + sd.n_c2 + j) * 16 + f],
                           b->bs.s1 + f * n1 + (long long)instance * sd.n_s1 + j, sizeof(double), cudaMemcpyDeviceToHost));
+    for (int j = 0; j < sd.n_c1; ++j)
+        for (int f = 0; f < 6; ++f)
+            CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + sd.n_c2 + sd.n_s1 + j) * 16 + f],
+                          b->bs.c1 + f * n4 + (long long)instance * sd.n_c1 + j, sizeof(double), cudaMemcpyDeviceToHost));
     std::memcpy(out, o.data(), o.size() * sizeof(double));
     return STRUT_OK;
 }
@@ -1890,9 +1917,9 @@ int strut_gpu_section3d_path(const StrutUniMaterial* materials, int32_t num_mate
     if (n_points == 0) return STRUT_OK;
     std::vector<DevMat> mats;
     for (int i = 0; i < num_materials; ++i) mats.push_back(make_devmat(materials[i]));
-    std::vector<double> s2, c2, s1;
+    std::vector<double> s2, c2, s1, c1;
     std::vector<int> kon;
-    batch_initial_state(sp, mats, 1, s2, c2, s1, kon);
+    batch_initial_state(sp, mats, 1, s2, c2, s1, c1, kon);
     std::vector<void*> al;
     auto cleanup = [&]() {
         for (void* p : al) cudaFree(p);
@@ -1905,7 +1932,8 @@ int strut_gpu_section3d_path(const StrutUniMaterial* materials, int32_t num_mate
     std::vector<double> pv(path, path + 3 * (size_t)n_points);
     if ((rc = upload(&d_mats, mats, al)) || (rc = upload(&d_y, sp.y, al)) || (rc = upload(&d_z, sp.z, al)) ||
         (rc = upload(&d_a, sp.a, al)) || (rc = upload(&d_m, sp.m, al)) || (rc = upload(&bs.s2, s2, al)) ||
-        (rc = upload(&bs.c2, c2, al)) || (rc = upload(&bs.s1, s1, al)) || (rc = upload(&bs.kon, kon, al)) ||
+        (rc = upload(&bs.c2, c2, al)) || (rc = upload(&bs.s1, s1, al)) || (rc = upload(&bs.c1, c1, al)) ||
+        (rc = upload(&bs.kon, kon, al)) ||
         (rc = upload(&d_path, pv, al)) || (rc = dzeros(&d_out, 9 * (size_t)n_points, al))) {
         cleanup();
         return rc;

@@ -88,6 +88,29 @@ def uniaxial_material(mat: dict) -> A.StrutUniMaterial:
         sig_init = float(p["sigInit"]) if has_sig else 0.0
         m.type = A.MAT_STEEL02
         vals = [Fy, E0, b, R0, cR1, cR2, a1, a2, a3, a4, sig_init]
+    elif t == "Concrete01":
+        fpc, epsc0 = float(p["fpc"]), float(p["epsc0"])
+        fpcu, epscu = float(p["fpcu"]), float(p["epscu"])
+        if fpc > 0.0:
+            fpc = -fpc
+        if epsc0 > 0.0:
+            epsc0 = -epsc0
+        if fpcu > 0.0:
+            fpcu = -fpcu
+        if epscu > 0.0:
+            epscu = -epscu
+        if fpc >= 0.0:
+            raise ModelError("Concrete01 fpc must be < 0")
+        if epsc0 >= 0.0:
+            raise ModelError("Concrete01 epsc0 must be < 0")
+        if epscu >= 0.0:
+            raise ModelError("Concrete01 epscu must be < 0")
+        if epscu >= epsc0:
+            raise ModelError("Concrete01 epscu must be < epsc0")
+        if fpcu > 0.0 or fpcu < fpc:
+            raise ModelError("Concrete01 fpcu must be between fpc and 0")
+        m.type = A.MAT_CONCRETE01
+        vals[0:4] = [fpc, epsc0, fpcu, epscu]
     elif t == "Concrete02":
         fpc, epsc0 = float(p["fpc"]), float(p["epsc0"])
         fpcu, epscu = float(p["fpcu"]), float(p["epscu"])

@@ -38,6 +38,41 @@ BAR_AREA = 500.0e-6
 COVER_T = 0.04
 
 
+def rc_section_208(sec_id: int, width: float, depth: float, core_mat=1, cover_mat=2,
+                   steel_mat=3, G: float = 12.5e9) -> dict:
+    """FiberSection3d with ~200 fibers: a 12x12 confined core, 20-fiber top and bottom cover
+    layers, 8-fiber side covers, 2 x 4 bars (208 fibers)."""
+    h2, b2, c = 0.5 * depth, 0.5 * width, COVER_T
+    b, h = min(width, depth), max(width, depth)
+    beta = 1.0 / 3.0 - 0.21 * (b / h) * (1.0 - (b / h) ** 4 / 12.0)
+    return {
+        "id": sec_id,
+        "type": "FiberSection3d",
+        "params": {
+            "patches": [
+                {"type": "rect", "material": core_mat, "num_subdiv_y": 12, "num_subdiv_z": 12,
+                 "y_i": -(h2 - c), "z_i": -(b2 - c), "y_j": h2 - c, "z_j": b2 - c},
+                {"type": "rect", "material": cover_mat, "num_subdiv_y": 1, "num_subdiv_z": 20,
+                 "y_i": h2 - c, "z_i": -b2, "y_j": h2, "z_j": b2},
+                {"type": "rect", "material": cover_mat, "num_subdiv_y": 1, "num_subdiv_z": 20,
+                 "y_i": -h2, "z_i": -b2, "y_j": -(h2 - c), "z_j": b2},
+                {"type": "rect", "material": cover_mat, "num_subdiv_y": 8, "num_subdiv_z": 1,
+                 "y_i": -(h2 - c), "z_i": b2 - c, "y_j": h2 - c, "z_j": b2},
+                {"type": "rect", "material": cover_mat, "num_subdiv_y": 8, "num_subdiv_z": 1,
+                 "y_i": -(h2 - c), "z_i": -b2, "y_j": h2 - c, "z_j": -(b2 - c)},
+            ],
+            "layers": [
+                {"type": "straight", "material": steel_mat, "num_bars": 4, "bar_area": BAR_AREA,
+                 "y_start": h2 - c, "z_start": -(b2 - c), "y_end": h2 - c, "z_end": b2 - c},
+                {"type": "straight", "material": steel_mat, "num_bars": 4, "bar_area": BAR_AREA,
+                 "y_start": -(h2 - c), "z_start": -(b2 - c), "y_end": -(h2 - c), "z_end": b2 - c},
+            ],
+            "G": G,
+            "J": beta * b ** 3 * h,
+        },
+    }
+
+
 def rc_section(sec_id: int, width: float, depth: float, core_mat=1, cover_mat=2, steel_mat=3,
                three_d: bool = False, G: float = 12.5e9):
     """10x10 confined core, two 20-fiber cover layers, 2 x 4 bars: 148 fibers.  With three_d
@@ -375,11 +410,14 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
                     max_iters: int = 20, element: str = "forceBeamColumn3d",
                     system: str = "BandGeneral", zeta: float = 0.05, geom: str = "Linear",
                     bidirectional: bool = False, record_elements=(1,), diaphragm: bool = False,
-                    beam_element: str | None = None, dt_record=None) -> dict:
+                    beam_element: str | None = None, sections=None,
+                    diaphragm_mass: float | None = None) -> dict:
     """3D RC frame: columns along z, beams along x and y, base fixed in all six dofs.  With
     ``diaphragm`` every floor is a rigid diaphragm (perp_dirn 3) retained by its central node,
     which carries the floor's horizontal masses and rotational inertia; the other nodes keep
-    their vertical mass only.  ``beam_element`` (default: ``element``) sets the beams' type."""
+    their vertical mass only.  ``beam_element`` (default: ``element``) sets the beams' type;
+    ``sections`` replaces the (column, beam) sections; ``diaphragm_mass`` is the floor's total
+    horizontal mass (default: floor_mass per node)."""
     nodes = []
     grid = {}
     nid = 1
@@ -426,13 +464,15 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
         master = grid[(k, jm, im)]
         xm, ym = im * bay_w, jm * bay_w
         total, inertia = 0.0, 0.0
+        n_floor = (bays_x + 1) * (bays_y + 1)
+        m_node = floor_mass if diaphragm_mass is None else diaphragm_mass / n_floor
         for j in range(bays_y + 1):
             for i in range(bays_x + 1):
                 node = grid[(k, j, i)]
-                masses.append({"node": node, "dof": 3, "value": floor_mass})
+                masses.append({"node": node, "dof": 3, "value": m_node})
                 dx, dy = i * bay_w - xm, j * bay_w - ym
-                total += floor_mass
-                inertia += floor_mass * (dx * dx + dy * dy)
+                total += m_node
+                inertia += m_node * (dx * dx + dy * dy)
                 if node == master:
                     continue
                 mpcs.append({"type": "rigidDiaphragm", "retained_node": master,
@@ -465,7 +505,8 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
             {"id": 2, "type": "Concrete02", "params": dict(COVER)},
             {"id": 3, "type": "Steel02", "params": dict(STEEL)},
         ],
-        "sections": [rc_section(1, 0.5, 0.5, three_d=True), rc_section(2, 0.4, 0.6, three_d=True)],
+        "sections": list(sections) if sections else [rc_section(1, 0.5, 0.5, three_d=True),
+                                                      rc_section(2, 0.4, 0.6, three_d=True)],
         "elements": elements,
         "masses": masses,
         "time_series": series,
@@ -500,6 +541,22 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
     case["rayleigh"] = {"alphaM": float(2.0 * zeta * wi * wj / (wi + wj)),
                         "betaKInit": float(2.0 * zeta / (wi + wj))}
     return case
+
+
+def tall_frame3d_case(stories: int = 20, bays: int = 6, steps: int = 4000, dt: float = 0.005,
+                      seed: int = 7000, pga_g: float = 0.4, record_elements=(1,)) -> dict:
+    """The large single-instance 3D RC frame: 20 stories x 6x6 bays of 7 m, story height
+    3.5 m (1029 nodes, 980 forceBeamColumn3d columns, 1680 dispBeamColumn3d beams), 5 Lobatto
+    points and 208-fiber sections, a rigid diaphragm per floor carrying 400 t, two horizontal
+    seeded Kanai-Tajimi records at PGA 0.4 g, dt 0.005 s.  Builder choices: columns
+    0.7 x 0.7 m, beams 0.5 x 0.7 m; the diaphragm's rotational inertia is that of the floor's
+    nodes with the floor mass spread evenly over them, which also carry it vertically."""
+    return rc_frame3d_case(stories=stories, bays_x=bays, bays_y=bays, story_h=3.5, bay_w=7.0,
+                           nip=5, dt=dt, steps=steps, seed=seed, pga_g=pga_g,
+                           element="forceBeamColumn3d", beam_element="dispBeamColumn3d",
+                           diaphragm=True, diaphragm_mass=400.0e3, bidirectional=True,
+                           sections=[rc_section_208(1, 0.7, 0.7), rc_section_208(2, 0.5, 0.7)],
+                           record_elements=record_elements)
 
 
 def batched_frame_params(n: int = 256, base_seed: int = 1000):

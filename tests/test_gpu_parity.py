@@ -25,6 +25,8 @@ MATS = [
     {"id": 3, "type": "Concrete02", "params": dict(W.COVER)},
     {"id": 4, "type": "Steel01", "params": {"Fy": 350.0e6, "E0": 200.0e9, "b": 0.01}},
     {"id": 5, "type": "Elastic", "params": {"E": 30.0e9}},
+    {"id": 6, "type": "Concrete01", "params": {"fpc": -30.0e6, "epsc0": -0.002, "fpcu": -6.0e6,
+                                                "epscu": -0.006}},
 ]
 
 
@@ -261,3 +263,19 @@ def test_graph_loop_equals_host_loop(gpu_lib):
             out.append([an.history(i) for i in range(2)])
     for (d0, e0, i0), (d1, e1, i1) in zip(out[0], out[1]):
         assert np.array_equal(d0, d1) and np.array_equal(e0, e1) and np.array_equal(i0, i1)
+
+
+def _concrete01_frame(element, steps, seed):
+    """The RC frame with its cover concrete as Concrete01 (fpc -30 MPa, epsc0 -0.002, fpcu 0,
+    epscu -0.004)."""
+    case = W.rc_frame_case(stories=2, bays=2, steps=steps, element=element, seed=seed, pga_g=0.4)
+    for m in case["materials"]:
+        if m["id"] == 2:
+            m["type"] = "Concrete01"
+            m["params"] = {"fpc": -30.0e6, "epsc0": -0.002, "fpcu": 0.0, "epscu": -0.004}
+    return case
+
+
+@pytest.mark.parametrize("element", ["forceBeamColumn2d", "dispBeamColumn2d"])
+def test_transient_concrete01_cover(gpu_lib, oracle, element):
+    _transient_parity(gpu_lib, oracle, [_concrete01_frame(element, 150, 31)], 150)

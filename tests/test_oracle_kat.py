@@ -119,6 +119,8 @@ MATS = [
     {"id": 6, "type": "Steel02", "params": {"Fy": 420.0, "E0": 200000.0, "b": 0.012, "R0": 18.0,
                                              "cR1": 0.925, "cR2": 0.15, "a1": 0.01, "a2": 1.0,
                                              "a3": 0.01, "a4": 1.0, "sigInit": 50.0}},
+    {"id": 7, "type": "Concrete01", "params": {"fpc": -30.0e6, "epsc0": -0.002, "fpcu": -6.0e6,
+                                                "epscu": -0.006}},
 ]
 
 
@@ -242,3 +244,25 @@ def test_nonconvergence_is_reported_not_aborted(oracle):
     assert rc == A.STRUT_NONCONVERGED
     assert failed == 0
     assert it[0] == 2
+
+
+def test_concrete01_known_points(oracle):
+    """Kent-Scott-Park envelope (concrete01.mojo:3-20): parabola to fpc at epsc0 (zero tangent),
+    linear to fpcu at epscu, constant beyond; no tension; unloading towards the end strain."""
+    m = M.uniaxial_material({"id": 1, "type": "Concrete01",
+                             "params": {"fpc": -30.0e6, "epsc0": -0.002, "fpcu": -6.0e6,
+                                        "epscu": -0.006}})
+    out = oracle.material_path(m, [-0.001])
+    assert math.isclose(out[0, 0], -30.0e6 * (2 * 0.5 - 0.25), rel_tol=1e-12)
+    out = oracle.material_path(m, [-0.002, -0.004, -0.008])
+    # at epsc0 itself the softening branch applies (strain > epsc0 is false)
+    assert math.isclose(out[0, 0], -30.0e6, rel_tol=1e-12)
+    assert math.isclose(out[0, 1], -24.0e6 / 0.004, rel_tol=1e-12)
+    assert math.isclose(out[1, 0], -30.0e6 + (-24.0e6 / 0.004) * (-0.004 + 0.002), rel_tol=1e-12)
+    assert out[2, 0] == -6.0e6 and out[2, 1] == 0.0
+    out = oracle.material_path(m, [0.001])
+    assert out[0, 0] == 0.0 and out[0, 1] == 0.0
+    # unloading from -0.003 is linear with the unloading slope and stays non-positive
+    out = oracle.material_path(m, [-0.003, -0.0025, 0.0])
+    assert out[1, 0] > out[0, 0] and out[1, 0] <= 0.0 and out[1, 1] > 0.0
+    assert out[2, 0] == 0.0
