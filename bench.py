@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor arm")
     ap.add_argument("--train-frames", type=int, default=64)
     ap.add_argument("--train-epochs", type=int, default=8)
+    ap.add_argument("--no-tall", action="store_true",
+                    help="skip the large single-instance 3D frame (20 stories, 6x6 bays)")
+    ap.add_argument("--tall-steps", type=int, default=60,
+                    help="timed steps of the 4000-step large 3D frame record")
     ap.add_argument("--profile-only", action="store_true",
                     help="one short analysis (for a profiler launch list); prints no bench line")
     return ap.parse_args()
@@ -166,6 +170,51 @@ def cpu_baseline(models, cases, nthreads=None, target_s=15.0):
     sample = (f"{nfr} frames of the batch x {steps} of {STEPS} steps on {nthreads} threads, "
               f"{n_ok} completed, {el:.1f} s, {tot_iters / (nfr * steps):.2f} Newton its/step")
     return rph, nthreads, sample
+
+
+def tall_arm(args, device, runtime, A, torch):
+    """The large single instance: the 20-story 6x6-bay 3D RC frame with rigid diaphragms
+    (1029 nodes, 2660 elements, 2.77 M fibers, 3000 free dofs, band in global memory), two
+    horizontal records, dt 0.005 s.  Device time of --tall-steps steps after 3 warm-up steps
+    (its fiber history, 2.77 M fibers x ~10 doubles, exceeds L2); records/hour is one 4000-step
+    record at that rate.  Beside it, the CPU oracle on 2 steps of the same record."""
+    from strut_b200 import model as M
+    from strut_b200 import workloads as W
+
+    case = W.tall_frame3d_case(steps=args.tall_steps + 3)
+    m = M.Model(case)
+    an = runtime.Analysis([m], device=device)
+    an.run(3, check=False)
+    stream = torch.cuda.ExternalStream(runtime.lib().strut_gpu_stream(an.h))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    an.run(args.tall_steps, check=False)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    _d, _e, it = an.history(0)
+    status = int(an.instance_status()[0])
+    an.close()
+    ms_step = ms / args.tall_steps
+    out = {"workload": "tall_3d_rc_frame_20s_6x6b_diaphragm", "nodes": m.num_nodes,
+           "elements": len(m.elements), "free_dofs": m.num_free, "fibers": m.num_fibers_total,
+           "record_steps": 4000, "dt": 0.005, "steps_timed": args.tall_steps, "warmup_steps": 3,
+           "ms_per_step": ms_step, "records_per_hour": 3600.0 / (ms_step * 4000 / 1000.0),
+           "newton_its_per_step": float(np.mean(it[3:])) if len(it) > 3 else None,
+           "status": status}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT))
+        from oracle import binding as O
+
+        O.build()
+        t0 = time.perf_counter()
+        rc = O.run_transient(m, 2)[3]
+        t = (time.perf_counter() - t0) / 2.0
+        out["cpu_baseline"] = {"value": 3600.0 / (t * 4000), "unit": "records/hour", "cores": 1,
+                               "kind": "port", "status": int(rc),
+                               "sample": f"first 2 of 4000 steps on 1 thread, {t:.2f} s/step"}
+    return out
 
 
 def learned_arm(args, models, device, runtime, A, torch, world):
@@ -407,6 +456,10 @@ def main():
     if not args.no_learned:
         learned = learned_arm(args, models, device, runtime, A, torch, world)
 
+    tall = None
+    if rank == 0 and world == 1 and not args.no_tall:
+        tall = tall_arm(args, device, runtime, A, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rph, cores, sample = cpu_baseline(models, cases)
@@ -453,6 +506,8 @@ def main():
             line["learned"] = learned
         if cpu:
             line["cpu_baseline"] = cpu
+        if tall:
+            line["tall_frame3d"] = tall
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()

@@ -89,6 +89,7 @@ struct DevInst {
     int elem_off, n_elem; // this instance's elements (contiguous)
     int large, large_idx; // band in global memory (too large for shared memory), its index
     long long lband_off;  // offset of its band in the global band buffer
+    int lrw, pad_l;       // slots per row of that band (3 bw + 1)
     int sl_off, n_sl;     // this instance's slave dofs (multi-point constraints)
 };
 

@@ -5,21 +5,28 @@
 //                          effective entries K + a1 C + a0 M written to the global band, the row's
 //                          residual P - F_int - C v - M a (transient_nonlinear.mojo:2302-2356,
 //                          linear_solver_backend.mojo:1877-1983)
-//   large_factor_kernel    cooperative (all CTAs co-resident): blocked right-looking band LU
-//                          without pivoting, panel width kPanel.  CTA 0 factors the panel
-//                          (rows k0 .. k0+kb-1+bw) in shared memory with Strut's pivot test
-//                          (a sub-diagonal entry larger than the pivot -> dense partial-pivot
-//                          fallback, linear_solver_backend.mojo:631-680) and forms U12 =
-//                          L11^-1 A12; every CTA then updates tiles of the trailing block
-//                          A22 -= L21 U12.  Two bounded grid barriers per panel.
-//   large_solve_kernel     one CTA per instance: blocked forward / back substitution
-//                          (_solve_band_general, 735-770), then the displacement update and
-//                          the convergence test shared with the shared-memory path.
-//   large_dense_kernel     the dense partial-pivot fallback (175-240) of the instances whose
-//                          band factorisation asked for it, one at a time in one n x n scratch.
+//   large_factor_kernel    cooperative (all CTAs co-resident): blocked right-looking band LU with
+//                          partial pivoting, panel width kPanel, the right-hand side carried as
+//                          one more column.  CTA 0 factors the panel in shared memory; every CTA
+//                          then takes column tiles of the trailing block (the panel's row
+//                          interchanges, then the eliminations in column order).  Two bounded
+//                          grid barriers per panel.
+//   large_solve_kernel     one CTA per instance: blocked back substitution through U, then the
+//                          displacement update and the convergence test shared with the
+//                          shared-memory path.
 //
-// The entries are the reference's; only the order of the sums in the trailing updates and the
-// substitutions differs (blocked), so the GPU agrees with the oracle to rounding.
+// Strut's BandGeneral factorises without pivoting and, at the first column whose pivot test
+// fails (a sub-diagonal entry larger than the pivot, linear_solver_backend.mojo:631-680),
+// restarts from the original matrix with a dense partial-pivot LU (175-240).  The columns
+// before that one choose no interchange under partial pivoting either (the same strict test,
+// the first largest entry wins), so one partial-pivot factorisation performs the reference's
+// interchanges and eliminations on every entry; it needs only the band, because below the
+// band the dense matrix's columns are zero (rows never come from further than bw below) and
+// the pivot rows' fill stays within 2 bw of the diagonal (storage: columns i - bw .. i + 2 bw
+// of row i, 3 bw + 1 slots).  A factorisation that interchanged rows counts as a dense
+// fallback in the statistics.  The order of the subtractions on an entry is the reference's
+// (column by column); the substitution through U is blocked, so the GPU agrees with the
+// oracle to rounding.
 #pragma once
 
 #include "solver_kernels.cuh"
@@ -30,7 +37,8 @@ constexpr int kPanel = 32;         // panel width of the blocked band LU
 constexpr int kLargeThreads = 256; // threads of a factorisation CTA
 constexpr int kSolveThreads = 1024;
 
-enum { LSTAT_OK = 0, LSTAT_SINGULAR = 2, LSTAT_DENSE = 6, LSTAT_CONVERGED = 7, LSTAT_IDLE = -1 };
+constexpr int kColTile = 16;       // trailing-update columns per tile
+enum { LSTAT_OK = 0, LSTAT_SINGULAR = 2, LSTAT_CONVERGED = 7, LSTAT_IDLE = -1 };
 
 struct GridBarrier {
     unsigned int count;
@@ -70,20 +78,22 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, unsigned int& gen)
     return __syncthreads_and(ok) != 0;
 }
 
-__device__ __forceinline__ long long lslot(int rw, int bw, int i, int j) {
-    return (long long)i * rw + (j - i + bw);
+// Slot of (i, j) in the factorisation band: row i holds columns i - bw .. i + 2 bw.
+__device__ __forceinline__ long long lslot(int lrw, int bw, int i, int j) {
+    return (long long)i * lrw + (j - i + bw);
 }
 
 // ---- assembly and residual ---------------------------------------------------------------
 
 // grid.x: warps over the rows of all large instances (row r of the concatenation over
 // large_list).  mode INST_MODE_NEWTON skips inactive instances; INST_MODE_EXPORT also writes the
-// band and F_int to the export buffers.
+// band and F_int to the export buffers.  The residual is also written to wbuf, the column the
+// factorisation carries along.
 __global__ void __launch_bounds__(256) large_assemble_kernel(const DevInst* __restrict__ insts,
                                                              InstArrays A, const int* __restrict__ large_list,
                                                              const int* __restrict__ row_base,
                                                              int n_large, int total_rows, int mode,
-                                                             GridBarrier* gb) {
+                                                             GridBarrier* gb, double* __restrict__ wbuf) {
     const int warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -105,13 +115,14 @@ __global__ void __launch_bounds__(256) large_assemble_kernel(const DevInst* __re
     }
     const long long sp0 = I.slot_ptr_off;
     const double* Kinit = A.Kinit + I.band_off;
-    double* B = A.lband + I.lband_off;
+    double* B = A.lband + I.lband_off + (long long)i * I.lrw;
+    for (int o = rw + lane; o < I.lrw; o += 32) B[o] = 0.0;  // fill slots
     double cv = 0.0;
     for (int o = lane; o < rw; o += 32) {
         const int j = i + o - bw;
         const long long slot = (long long)i * rw + o;
         if (j < 0 || j >= n) {
-            B[slot] = 0.0;
+            B[o] = 0.0;
             if (mode == INST_MODE_EXPORT) A.export_band[I.band_off + slot] = 0.0;
             continue;
         }
@@ -129,7 +140,7 @@ __global__ void __launch_bounds__(256) large_assemble_kernel(const DevInst* __re
         double keff = K;
         if (I.has_damping && I.a1 != 0.0) keff += I.a1 * C;
         if (i == j) keff += I.a0 * A.Mff[f0 + i];
-        B[slot] = keff;
+        B[o] = keff;
         if (mode == INST_MODE_EXPORT) A.export_band[I.band_off + slot] = keff;
     }
     cv = warp_sum(cv);
@@ -140,17 +151,19 @@ __global__ void __launch_bounds__(256) large_assemble_kernel(const DevInst* __re
         const double F = gather_fint(A, A.ef, q0, q1);
         const double ma = A.Mff[gi] * an;
         A.R[gi] = A.P_f[gi] - F - 0.0 - cv - ma;
+        wbuf[gi] = A.R[gi];
         if (mode == INST_MODE_EXPORT) A.export_f[gi] = F;
     }
 }
 
-// ---- blocked band LU ------------------------------------------------------------------------
+// ---- blocked band LU with partial pivoting -------------------------------------------------
 
-// Copies the exported band of every large instance into its factorisation buffer
-// (strut_gpu_factor_solve on a band from strut_gpu_state_determination).
+// Copies the exported band of every large instance into its factorisation band (fill slots
+// zero) and the right-hand side into wbuf (strut_gpu_factor_solve on a band from
+// strut_gpu_state_determination).
 __global__ void large_load_exported_kernel(const DevInst* __restrict__ insts, InstArrays A,
                                            const int* __restrict__ large_list, int n_large,
-                                           GridBarrier* gb) {
+                                           GridBarrier* gb, double* __restrict__ wbuf) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
         gb->count = 0u;
         gb->err = 0;
@@ -158,20 +171,37 @@ __global__ void large_load_exported_kernel(const DevInst* __restrict__ insts, In
     const int li = blockIdx.y;
     if (li >= n_large) return;
     const DevInst& I = insts[large_list[li]];
-    const long long total = (long long)I.n * I.rw;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x)
-        A.lband[I.lband_off + t] = A.export_band[I.band_off + t];
+    const long long total = (long long)I.n * I.lrw;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (long long t = first; t < total; t += stride) {
+        const long long i = t / I.lrw;
+        const int o = (int)(t - i * I.lrw);
+        A.lband[I.lband_off + t] = o < I.rw ? A.export_band[I.band_off + i * I.rw + o] : 0.0;
+    }
+    for (long long i = first; i < I.n; i += stride) wbuf[I.f_off + i] = A.rhs_in[I.f_off + i];
 }
 
-// Cooperative.  Dynamic shared memory: panel (kPanel + bw) x kPanel, then two 32 x kPanel tiles.
+// Shared memory of large_factor_kernel for a band of half-width bw: CTA 0's panel
+// (kPanel + bw) x (kPanel + 1), or a tile's panel copy of that size plus its column slab
+// (kPanel + bw) x kColTile.
+__host__ __device__ inline size_t large_factor_smem(int bw) {
+    return sizeof(double) * (size_t)(kPanel + bw) * (kPanel + 1 + kColTile);
+}
+
+// Cooperative.  wbuf holds the right-hand side on entry and L^-1 P b on exit; the band holds U
+// on exit (its strictly lower part is left stale: the substitution reads U only).  lpan / lpiv:
+// the factored panel and its interchanges, passed from CTA 0 to the others.
 __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
     const DevInst* __restrict__ insts, InstArrays A, const int* __restrict__ large_list,
-    int n_large, int mode, GridBarrier* gb) {
+    int n_large, int mode, GridBarrier* gb, double* wbuf, double* lpan, int* lpiv) {
     extern __shared__ __align__(16) double smem_lf[];
     __shared__ int s_flag[2];
+    __shared__ int s_piv[kPanel];
     __shared__ double red[32];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    __shared__ int red_r[32];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5;
+    const int nwarps = nt >> 5;
     unsigned int gen = 0;
     if (tid == 0) gen = atomicAdd(&gb->gen, 0u);
     for (int li = 0; li < n_large; ++li) {
@@ -181,8 +211,9 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
             if (blockIdx.x == 0 && tid == 0) A.lstatus[li] = LSTAT_IDLE;
             continue;
         }
-        const int n = I.n, bw = I.bw, rw = I.rw;
+        const int n = I.n, bw = I.bw, lrw = I.lrw;
         double* B = A.lband + I.lband_off;
+        double* w = wbuf + I.f_off;
         if (mode == INST_MODE_NEWTON && I.test_type == 2) {
             // NormUnbalance is tested on the residual before the solve; every CTA reaches the
             // same decision from the same sums
@@ -196,45 +227,78 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
         }
         const int P = min(kPanel, max(bw, 1));
         int result = LSTAT_OK;
+        int pivoted = 0;
         for (int k0 = 0; k0 < n && result == LSTAT_OK; k0 += P) {
             const int kb = min(P, n - k0);
-            const int r1 = min(n - 1, k0 + kb - 1 + bw);  // last row touched by the panel
+            const int r1 = min(n - 1, k0 + kb - 1 + bw);      // last row with a nonzero in the panel
             const int pr = r1 - k0 + 1;
-            const int c1 = min(n - 1, k0 + kb - 1 + bw);  // last column of U12
+            const int c1 = min(n - 1, k0 + kb - 1 + 2 * bw);  // last column the panel's rows reach
+            const int ps = kb + 1;                            // padded row stride of the panel
             if (blockIdx.x == 0) {
-                // ---- panel: rows k0..r1, columns k0..k0+kb-1 (row-major, stride kb)
+                // ---- panel: rows k0..r1, columns k0..k0+kb-1; one thread per row in the updates
                 double* Pm = smem_lf;
                 for (int t = tid; t < pr * kb; t += nt) {
                     const int r = t / kb, c = t % kb;
-                    const int i = k0 + r, j = k0 + c;
-                    Pm[t] = (i - j <= bw && j - i <= bw) ? B[lslot(rw, bw, i, j)] : 0.0;
+                    const int d = c - r;
+                    Pm[r * ps + c] = (d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, k0 + r, k0 + c)] : 0.0;
                 }
                 if (tid == 0) s_flag[0] = LSTAT_OK;
                 __syncthreads();
                 for (int c = 0; c < kb; ++c) {
-                    const int k = k0 + c;
-                    const int last = min(pr - 1, c + bw);  // rows of column k inside the band
-                    const double akk = Pm[c * kb + c];
-                    const double aabs = fabs(akk);
-                    int swap = 0, big = 0;
-                    for (int r = c + 1 + tid; r <= last; r += nt) {
-                        const double v = fabs(Pm[r * kb + c]);
-                        swap |= v > aabs ? 1 : 0;
-                        big |= v > 1.0e-14 ? 1 : 0;
+                    const int last = min(pr - 1, c + bw);  // rows of column k0+c inside the band
+                    // the first largest |entry| of the column (the reference's strict '>' scan)
+                    double bv = -1.0;
+                    int br = c;
+                    for (int r = c + tid; r <= last; r += nt) {
+                        const double v = fabs(Pm[r * ps + c]);
+                        if (v > bv) {
+                            bv = v;
+                            br = r;
+                        }
                     }
-                    const int any_swap = __syncthreads_or(swap);
-                    const int any_big = __syncthreads_or(big);
-                    if (any_swap || aabs <= 1.0e-14) {
-                        if (tid == 0) s_flag[0] = (any_swap && any_big) ? LSTAT_DENSE : LSTAT_SINGULAR;
+                    for (int off = 16; off > 0; off >>= 1) {
+                        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                        const int orr = __shfl_xor_sync(0xffffffffu, br, off);
+                        if (ov > bv || (ov == bv && orr < br)) {
+                            bv = ov;
+                            br = orr;
+                        }
+                    }
+                    if (lane == 0) {
+                        red[wid] = bv;
+                        red_r[wid] = br;
+                    }
+                    __syncthreads();
+                    double pv = red[0];
+                    int p = red_r[0];
+                    for (int q = 1; q < nwarps; ++q) {
+                        if (red[q] > pv || (red[q] == pv && red_r[q] < p)) {
+                            pv = red[q];
+                            p = red_r[q];
+                        }
+                    }
+                    if (pv <= 1.0e-14) {
+                        if (tid == 0) s_flag[0] = LSTAT_SINGULAR;
                         break;
                     }
-                    (void)k;
-                    for (int r = c + 1 + tid; r <= last; r += nt) Pm[r * kb + c] = Pm[r * kb + c] / akk;
-                    __syncthreads();
-                    const int rows = last - c, cols = kb - 1 - c;
-                    for (int t = tid; t < rows * cols; t += nt) {
-                        const int r = c + 1 + t / cols, cc = c + 1 + t % cols;
-                        Pm[r * kb + cc] -= Pm[r * kb + c] * Pm[c * kb + cc];
+                    if (tid == 0) s_piv[c] = p;
+                    if (p != c) {
+                        // whole panel rows, multipliers included, so that the trailing columns
+                        // can take all interchanges first and the eliminations after
+                        pivoted = 1;
+                        for (int cc = tid; cc < kb; cc += nt) {
+                            const double t0 = Pm[c * ps + cc];
+                            Pm[c * ps + cc] = Pm[p * ps + cc];
+                            Pm[p * ps + cc] = t0;
+                        }
+                        __syncthreads();
+                    }
+                    const double diag = Pm[c * ps + c];
+                    for (int r = c + 1 + tid; r <= last; r += nt) {
+                        const double f = Pm[r * ps + c] / diag;
+                        Pm[r * ps + c] = f;
+                        if (f == 0.0) continue;
+                        for (int cc = c + 1; cc < kb; ++cc) Pm[r * ps + cc] -= f * Pm[c * ps + cc];
                     }
                     __syncthreads();
                 }
@@ -242,70 +306,96 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                 if (s_flag[0] == LSTAT_OK) {
                     for (int t = tid; t < pr * kb; t += nt) {
                         const int r = t / kb, c = t % kb;
-                        const int i = k0 + r, j = k0 + c;
-                        if (i - j <= bw && j - i <= bw) B[lslot(rw, bw, i, j)] = Pm[t];
+                        const double v = Pm[r * ps + c];
+                        lpan[r * ps + c] = v;
+                        if (r <= c) B[lslot(lrw, bw, k0 + r, k0 + c)] = v;
                     }
-                    // U12 = L11^-1 A12: one thread per column j of k0+kb..c1, rows in order
-                    for (int j = k0 + kb + tid; j <= c1; j += nt) {
-                        double u[kPanel];
-                        for (int r = 0; r < kb; ++r) {
-                            const int i = k0 + r;
-                            double v = (j - i <= bw) ? B[lslot(rw, bw, i, j)] : 0.0;
-                            for (int s = 0; s < r; ++s) v -= Pm[r * kb + s] * u[s];
-                            u[r] = v;
-                            if (j - i <= bw) B[lslot(rw, bw, i, j)] = v;
-                        }
-                    }
+                    for (int c = tid; c < kb; c += nt) lpiv[c] = s_piv[c];
                 }
-                if (tid == 0) s_flag[1] = s_flag[0];
-                __syncthreads();
-                if (tid == 0) A.lstatus[li] = s_flag[0];
-                // publish the panel result to the other CTAs through gb->pad
-                if (tid == 0) atomicExch(&gb->pad, s_flag[0]);
+                if (tid == 0) {
+                    A.lstatus[li] = s_flag[0];
+                    // publish the panel result to the other CTAs through gb->pad
+                    atomicExch(&gb->pad, s_flag[0]);
+                }
             }
             if (!grid_barrier(gb, gen)) return;
             if (tid == 0) s_flag[1] = atomicAdd(&gb->pad, 0);
             __syncthreads();
             result = s_flag[1];
             if (result != LSTAT_OK) break;
-            // ---- trailing update A22 -= L21 U12 over rows / columns k0+kb .. r1
-            const int m = r1 - (k0 + kb) + 1;
-            if (m > 0) {
-                const int nbt = (m + 31) / 32;
-                double* Lt = smem_lf;                 // 32 x kb
-                double* Ut = smem_lf + 32 * kPanel;   // kb x 32
-                for (int tile = blockIdx.x; tile < nbt * nbt; tile += gridDim.x) {
-                    const int ti = tile / nbt, tj = tile % nbt;
-                    const int i0 = k0 + kb + 32 * ti, j0 = k0 + kb + 32 * tj;
-                    __syncthreads();
-                    for (int t = tid; t < 32 * kb; t += nt) {
-                        const int r = t / kb, s = t % kb;
-                        const int i = i0 + r, kk = k0 + s;
-                        Lt[t] = (i <= r1 && i - kk <= bw) ? B[lslot(rw, bw, i, kk)] : 0.0;
-                        const int s2 = t / 32, cc = t % 32;
-                        const int j = j0 + cc, k2 = k0 + s2;
-                        Ut[t] = (j <= r1 && j - k2 <= bw) ? B[lslot(rw, bw, k2, j)] : 0.0;
+            // ---- trailing columns k0+kb .. c1 in tiles of kColTile, and the right-hand side
+            const int j_first = k0 + kb;
+            const int ncols = c1 - j_first + 1;
+            const int ntiles = (ncols > 0 ? (ncols + kColTile - 1) / kColTile : 0) + 1;
+            double* Ls = smem_lf;                                         // pr x ps
+            double* S = smem_lf + (size_t)(kPanel + bw) * (kPanel + 1);   // pr x kColTile
+            bool loaded = false;
+            for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+                __syncthreads();
+                if (!loaded) {
+                    for (int t = tid; t < pr * ps; t += nt) Ls[t] = lpan[t];
+                    for (int c = tid; c < kb; c += nt) s_piv[c] = lpiv[c];
+                    loaded = true;
+                }
+                const bool rhs = tile == ntiles - 1;
+                const int j0 = j_first + tile * kColTile;
+                const int ct = rhs ? 1 : min(kColTile, c1 - j0 + 1);
+                for (int t = tid; t < pr * ct; t += nt) {
+                    const int r = t / ct, q = t % ct;
+                    const int i = k0 + r;
+                    double v;
+                    if (rhs) {
+                        v = w[i];
+                    } else {
+                        const int d = j0 + q - i;
+                        v = (d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, i, j0 + q)] : 0.0;
+                    }
+                    S[r * kColTile + q] = v;
+                }
+                __syncthreads();
+                for (int q = tid; q < ct; q += nt) {
+                    for (int c = 0; c < kb; ++c) {
+                        const int p = s_piv[c];
+                        if (p != c) {
+                            const double t0 = S[c * kColTile + q];
+                            S[c * kColTile + q] = S[p * kColTile + q];
+                            S[p * kColTile + q] = t0;
+                        }
+                    }
+                }
+                __syncthreads();
+                for (int sc = 0; sc < kb; ++sc) {
+                    // the panel's interchanges carried multipliers of column sc down to any
+                    // panel row, not only the bw rows below it
+                    const int rows = pr - 1 - sc;
+                    for (int t = tid; t < rows * ct; t += nt) {
+                        const int r = sc + 1 + t / ct, q = t % ct;
+                        const double f = Ls[r * ps + sc];
+                        if (f != 0.0) S[r * kColTile + q] -= f * S[sc * kColTile + q];
                     }
                     __syncthreads();
-                    for (int t = tid; t < 32 * 32; t += nt) {
-                        const int r = t / 32, cc = t % 32;
-                        const int i = i0 + r, j = j0 + cc;
-                        if (i > r1 || j > r1) continue;
-                        double acc = 0.0;
-                        for (int s = 0; s < kb; ++s) acc += Lt[r * kb + s] * Ut[s * 32 + cc];
-                        B[lslot(rw, bw, i, j)] -= acc;
+                }
+                for (int t = tid; t < pr * ct; t += nt) {
+                    const int r = t / ct, q = t % ct;
+                    const int i = k0 + r;
+                    if (rhs) {
+                        w[i] = S[r * kColTile + q];
+                    } else {
+                        const int d = j0 + q - i;
+                        if (d >= -bw && d <= 2 * bw) B[lslot(lrw, bw, i, j0 + q)] = S[r * kColTile + q];
                     }
                 }
             }
             if (!grid_barrier(gb, gen)) return;
         }
+        if (blockIdx.x == 0 && tid == 0 && pivoted && result == LSTAT_OK && A.fallbacks) A.fallbacks[inst] += 1;
     }
 }
 
 // ---- substitution, update and test ---------------------------------------------------------
 
-// One CTA per large instance.  Forward: L (unit lower) in blocks of 32 rows, each block solved
-// by warp 0 then pushed into the next bw rows; back: U in blocks of 32 rows from the end.
+// One CTA per large instance: U x = L^-1 P b (left in wbuf by the factorisation) in blocks of 32
+// rows from the end, each block solved by warp 0 then pushed into the 2 bw rows above.
 __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
     const DevInst* __restrict__ insts, InstArrays A, const int* __restrict__ large_list, int n_large,
     int mode, double* __restrict__ wbuf, const GridBarrier* __restrict__ gb) {
@@ -329,9 +419,9 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
         }
         return;
     }
-    if (st == LSTAT_DENSE) return;  // large_dense_kernel
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int n = I.n, bw = I.bw, rw = I.rw, f0 = I.f_off;
+    const int n = I.n, bw = I.bw, lrw = I.lrw, f0 = I.f_off;
+    const int ub = 2 * bw;  // reach of U
     int* hrow = (mode == INST_MODE_NEWTON && A.hist_iters && A.ctl)
                     ? A.hist_iters + (size_t)A.ctl->step * A.n_inst : nullptr;
     if (st == LSTAT_CONVERGED) {
@@ -353,44 +443,16 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
         return;
     }
     const double* B = A.lband + I.lband_off;
-    double* w = wbuf + f0;             // forward result, then x
-    const double* rhs = (mode == INST_MODE_SOLVE_EXPORTED) ? A.rhs_in + f0 : A.R + f0;
-    for (int i = tid; i < n; i += nt) w[i] = rhs[i];
-    __syncthreads();
+    double* w = wbuf + f0;  // L^-1 P b, then x
     const int lane = tid & 31;
-    for (int r0 = 0; r0 < n; r0 += 32) {
-        const int rb = min(32, n - r0);
-        if (tid < 32) {
-            double v = lane < rb ? w[r0 + lane] : 0.0;
-            for (int s = 0; s < rb; ++s) {
-                const double ws = __shfl_sync(0xffffffffu, v, s);
-                if (lane > s && lane < rb && (lane - s) <= bw) v -= B[lslot(rw, bw, r0 + lane, r0 + s)] * ws;
-            }
-            if (lane < rb) {
-                w[r0 + lane] = v;
-                xb[lane] = v;
-            }
-        }
-        __syncthreads();
-        const int i_last = min(n - 1, r0 + rb - 1 + bw);
-        for (int i = r0 + rb + tid; i <= i_last; i += nt) {
-            double acc = 0.0;
-            for (int s = 0; s < rb; ++s) {
-                const int j = r0 + s;
-                if (i - j <= bw) acc += B[lslot(rw, bw, i, j)] * xb[s];
-            }
-            w[i] -= acc;
-        }
-        __syncthreads();
-    }
     for (int r1 = n; r1 > 0; r1 -= 32) {
         const int r0 = max(0, r1 - 32), rb = r1 - r0;
         if (tid < 32) {
             double v = lane < rb ? w[r0 + lane] : 0.0;
             for (int s = rb - 1; s >= 0; --s) {
-                if (lane == s) v = v / B[lslot(rw, bw, r0 + s, r0 + s)];
+                if (lane == s) v = v / B[lslot(lrw, bw, r0 + s, r0 + s)];
                 const double xs = __shfl_sync(0xffffffffu, v, s);
-                if (lane < s && (s - lane) <= bw) v -= B[lslot(rw, bw, r0 + lane, r0 + s)] * xs;
+                if (lane < s && (s - lane) <= ub) v -= B[lslot(lrw, bw, r0 + lane, r0 + s)] * xs;
             }
             if (lane < rb) {
                 w[r0 + lane] = v;
@@ -398,12 +460,12 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
             }
         }
         __syncthreads();
-        const int i_first = max(0, r0 - bw);
+        const int i_first = max(0, r0 - ub);
         for (int i = i_first + tid; i < r0; i += nt) {
             double acc = 0.0;
             for (int s = 0; s < rb; ++s) {
                 const int j = r0 + s;
-                if (j - i <= bw) acc += B[lslot(rw, bw, i, j)] * xb[s];
+                if (j - i <= ub) acc += B[lslot(lrw, bw, i, j)] * xb[s];
             }
             w[i] -= acc;
         }
@@ -415,62 +477,6 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
     }
     InstArrays Ar = A;
     newton_tail(I, Ar, inst, w, A.R + f0, hrow, red, red_r);
-}
-
-// Dense partial-pivot fallback of the large instances that asked for it, one at a time (one
-// CTA, one n x n scratch): D from the assembled effective entries, LU, solve, update, test.
-__global__ void __launch_bounds__(256) large_dense_kernel(const DevInst* __restrict__ insts,
-                                                          InstArrays A, const int* __restrict__ large_list,
-                                                          int n_large, int mode, double* __restrict__ D,
-                                                          int* __restrict__ piv, double* __restrict__ wbuf) {
-    extern __shared__ __align__(16) double smem_ld[];  // fac (max n)
-    __shared__ double red[32];
-    __shared__ int red_r[32];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int li = 0; li < n_large; ++li) {
-        if (A.lstatus[li] != LSTAT_DENSE) continue;
-        const int inst = large_list[li];
-        const DevInst& I = insts[inst];
-        if (mode == INST_MODE_NEWTON && !A.active[inst]) continue;
-        const int n = I.n, bw = I.bw, rw = I.rw, f0 = I.f_off;
-        for (long long t = tid; t < (long long)n * n; t += nt) D[t] = 0.0;
-        __syncthreads();
-        const double* Kinit = A.Kinit + I.band_off;
-        for (long long t = tid; t < (long long)n * rw; t += nt) {
-            const int i = (int)(t / rw), j = i + (int)(t % rw) - bw;
-            if (j < 0 || j >= n) continue;
-            D[(size_t)i * n + j] = (mode == INST_MODE_SOLVE_EXPORTED)
-                                       ? A.export_band[I.band_off + t]
-                                       : keff_slot(I, A, I.slot_ptr_off, Kinit, i, j, (int)t);
-        }
-        __syncthreads();
-        const int rc = dense_lu_global(D, piv, n, smem_ld, red, red_r);
-        if (tid == 0 && A.fallbacks) A.fallbacks[inst] += 1;
-        if (rc != 0) {
-            if (tid == 0) {
-                A.status[inst] = rc;
-                if (mode == INST_MODE_NEWTON && A.active[inst]) {
-                    A.active[inst] = 0;
-                    atomicSub(A.nactive, 1);
-                }
-            }
-            __syncthreads();
-            continue;
-        }
-        __syncthreads();
-        double* w = wbuf + f0;
-        double* x = A.du + f0;
-        const double* rhs = (mode == INST_MODE_SOLVE_EXPORTED) ? A.rhs_in + f0 : A.R + f0;
-        if (tid < 32) dense_solve_warp(D, piv, n, rhs, w, x);
-        __syncthreads();
-        if (mode == INST_MODE_SOLVE_EXPORTED) continue;
-        int* hrow = (A.hist_iters && A.ctl) ? A.hist_iters + (size_t)A.ctl->step * A.n_inst : nullptr;
-        for (int i = tid; i < n; i += nt) w[i] = x[i];
-        __syncthreads();
-        InstArrays Ar = A;
-        newton_tail(I, Ar, inst, w, A.R + f0, hrow, red, red_r);
-        __syncthreads();
-    }
 }
 
 }  // namespace strut

@@ -290,14 +290,15 @@ struct StrutHandle {
     // instances whose band is factored in global memory
     int n_large = 0, large_rows = 0, max_large_n = 0, lfactor_grid = 1;
     long long lband_total = 0;
-    size_t lfactor_smem = 16, ldense_smem = 16;
+    size_t lfactor_smem = 16;
+    int max_large_bw = 0;
     std::vector<int> large_list_h;
     int* d_large_list = nullptr;
     int* d_large_rowbase = nullptr;
     GridBarrier* d_gb = nullptr;
     double* d_wbuf = nullptr;
-    double* d_ldense = nullptr;
-    int* d_lpiv = nullptr;
+    double* d_lpan = nullptr;  // factored panel, CTA 0 -> the other CTAs
+    int* d_lpiv = nullptr;     // its interchanges
     int n_slaves_total = 0;          // slave dofs of every instance (multi-point constraints)
     int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
     long long band_total = 0;
@@ -446,8 +447,8 @@ static int launch_elements(StrutHandle* h, int all_elems = 0) {
     return STRUT_OK;
 }
 
-// Instances with a global-memory band: assembly (or the exported band), cooperative blocked LU,
-// substitution + update + test, dense fallback.  mode as the instance kernel; EXPORT stops after
+// Instances with a global-memory band: assembly (or the exported band), cooperative blocked LU
+// with partial pivoting, back substitution + update + test.  mode as the instance kernel; EXPORT stops after
 // the assembly.
 static int launch_large(StrutHandle* h, int mode, const DevInst* insts = nullptr, InstArrays* Aover = nullptr) {
     if (h->n_large == 0) return STRUT_OK;
@@ -456,11 +457,12 @@ static int launch_large(StrutHandle* h, int mode, const DevInst* insts = nullptr
     if (!insts) insts = h->d_insts;
     if (mode == INST_MODE_SOLVE_EXPORTED) {
         large_load_exported_kernel<<<dim3(64, h->n_large), 256, 0, h->stream>>>(insts, A, h->d_large_list,
-                                                                                h->n_large, h->d_gb);
+                                                                                h->n_large, h->d_gb, h->d_wbuf);
     } else {
         const int blocks = (h->large_rows * 32 + 255) / 256;
         large_assemble_kernel<<<blocks, 256, 0, h->stream>>>(insts, A, h->d_large_list, h->d_large_rowbase,
-                                                            h->n_large, h->large_rows, mode, h->d_gb);
+                                                            h->n_large, h->large_rows, mode, h->d_gb,
+                                                            h->d_wbuf);
     }
     CK(cudaGetLastError());
     if (mode == INST_MODE_EXPORT) return STRUT_OK;
@@ -468,15 +470,16 @@ static int launch_large(StrutHandle* h, int mode, const DevInst* insts = nullptr
         int n_large = h->n_large;
         GridBarrier* gb = h->d_gb;
         const int* ll = h->d_large_list;
-        void* args[] = {(void*)&insts, (void*)&A, (void*)&ll, (void*)&n_large, (void*)&mode, (void*)&gb};
+        double* wb = h->d_wbuf;
+        double* lpan = h->d_lpan;
+        int* lpiv = h->d_lpiv;
+        void* args[] = {(void*)&insts, (void*)&A,  (void*)&ll,   (void*)&n_large, (void*)&mode,
+                        (void*)&gb,    (void*)&wb, (void*)&lpan, (void*)&lpiv};
         CK(cudaLaunchCooperativeKernel((const void*)large_factor_kernel, dim3(h->lfactor_grid),
                                        dim3(kLargeThreads), args, h->lfactor_smem, h->stream));
     }
     large_solve_kernel<<<h->n_large, kSolveThreads, 0, h->stream>>>(insts, A, h->d_large_list, h->n_large, mode,
                                                                     h->d_wbuf, h->d_gb);
-    CK(cudaGetLastError());
-    large_dense_kernel<<<1, 256, h->ldense_smem, h->stream>>>(insts, A, h->d_large_list, h->n_large, mode,
-                                                               h->d_ldense, h->d_lpiv, h->d_wbuf);
     CK(cudaGetLastError());
     return STRUT_OK;
 }
@@ -1079,20 +1082,18 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             // band too large for shared memory: blocked factorisation in global memory
             if (I.spd)
                 return bail(fail(STRUT_UNSUPPORTED, "BandSPD bands beyond shared memory are not implemented"));
-            const int P = std::min(kPanel, std::max(bw, 1));
-            const size_t fsm = sizeof(double) * std::max((size_t)(P + bw) * P, (size_t)64 * kPanel);
+            const size_t fsm = large_factor_smem(bw);
             if (fsm > 220 * 1024)
                 return bail(fail(STRUT_UNSUPPORTED, "band width too large for the blocked factorisation"));
             I.large = 1;
             I.large_idx = h->n_large++;
+            I.lrw = 3 * bw + 1;  // columns i - bw .. i + 2 bw: room for the pivot rows' fill
             I.lband_off = h->lband_total;
-            h->lband_total += (long long)nf * rw;
+            h->lband_total += (long long)nf * I.lrw;
             h->large_list_h.push_back(inst);
             h->max_large_n = std::max(h->max_large_n, nf);
+            h->max_large_bw = std::max(h->max_large_bw, bw);
             h->lfactor_smem = std::max(h->lfactor_smem, fsm);
-            h->ldense_smem = std::max(h->ldense_smem, sizeof(double) * (size_t)nf);
-            if (h->ldense_smem > 220 * 1024)
-                return bail(fail(STRUT_UNSUPPORTED, "instance too large for the dense fallback scratch"));
         } else {
             h->inst_smem = std::max(h->inst_smem, ismem);
         }
@@ -1294,13 +1295,11 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         if ((rc = upload(&h->d_large_list, h->large_list_h, al)) || (rc = upload(&h->d_large_rowbase, rowbase, al)) ||
             (rc = dzeros(&A.lband, (size_t)h->lband_total, al)) || (rc = upload(&A.lstatus, lstat, al)) ||
             (rc = dzeros(&h->d_gb, 1, al)) || (rc = dzeros(&h->d_wbuf, nF, al)) ||
-            (rc = dzeros(&h->d_ldense, (size_t)h->max_large_n * h->max_large_n, al)) ||
-            (rc = dzeros(&h->d_lpiv, (size_t)h->max_large_n, al)))
+            (rc = dzeros(&h->d_lpan, (size_t)(kPanel + h->max_large_bw) * (kPanel + 1), al)) ||
+            (rc = dzeros(&h->d_lpiv, (size_t)kPanel, al)))
             return bail(rc);
         CK(cudaFuncSetAttribute(large_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)h->lfactor_smem));
-        CK(cudaFuncSetAttribute(large_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)h->ldense_smem));
         int per_sm = 0, n_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, large_factor_kernel, kLargeThreads,
                                                          h->lfactor_smem));

@@ -33,7 +33,12 @@ def test_diaphragm_state_determination(gpu_lib, oracle, beam):
     case = W.rc_frame3d_case(stories=2, bays_x=2, bays_y=1, steps=10, element="forceBeamColumn3d",
                              beam_element=beam, diaphragm=True, seed=4)
     m = M.Model(case)
-    u = np.random.default_rng(2).normal(0.0, 2e-3, m.num_free)
+    # Random master rotations are multiplied by the diaphragm's lever arms (up to ~10 m) on the
+    # slave translations, so 2e-4 here drives the columns about as hard as 2e-3 drives an
+    # unconstrained frame.  At 2e-3 one forceBeamColumn3d lands where the oracle's own tangent
+    # moves by up to 3e-7 of the largest entry when u is perturbed by 1e-15 relative: no
+    # rounding-level comparison is possible there.
+    u = np.random.default_rng(2).normal(0.0, 2e-4, m.num_free)
     f_ref, band_ref, bw = oracle.state_determination(m, u)
     with gpu_lib.Analysis([m]) as an:
         (f_got, band_got), = an.state_determination([u])
@@ -58,6 +63,32 @@ def test_diaphragm_large_band(gpu_lib, oracle):
         _bw, rw = an.band_info(0)
     assert m.num_free * rw * 8 > 220 * 1024
     _parity(gpu_lib, oracle, [case], 40)
+
+
+def test_large_band_pivoting_factor_solve(gpu_lib, oracle):
+    """The collapsed diaphragm band fails Strut's band pivot test (the oracle restarts with its
+    dense partial-pivot LU); the global-memory path's partial-pivot band LU solves the same
+    system."""
+    case = W.rc_frame3d_case(stories=5, bays_x=3, bays_y=3, steps=5, element="forceBeamColumn3d",
+                             beam_element="dispBeamColumn3d", diaphragm=True, seed=13, pga_g=0.35)
+    m = M.Model(case)
+    u = np.random.default_rng(3).normal(0.0, 2e-4, m.num_free)
+    with gpu_lib.Analysis([m]) as an:
+        bw, rw = an.band_info(0)
+        assert m.num_free * rw * 8 > 220 * 1024
+        (_f, band), = an.state_determination([u])
+        n = m.num_free
+        K = np.zeros((n, n))
+        for i in range(n):
+            for o in range(rw):
+                j = i + o - bw
+                if 0 <= j < n:
+                    K[i, j] = band[i, o]
+        # without interchanges column 25's pivot test fails on this band
+        rhs = np.random.default_rng(8).normal(size=n)
+        du, = an.factor_solve([rhs])
+    ref = np.linalg.solve(K, rhs)
+    assert np.max(np.abs(du - ref)) <= 1e-9 * np.max(np.abs(ref))
 
 
 def test_equal_dof_2d_batch(gpu_lib, oracle):
