@@ -34,7 +34,7 @@
 namespace strut {
 
 constexpr int kPanel = 32;         // panel width of the blocked band LU
-constexpr int kLargeThreads = 256; // threads of a factorisation CTA
+constexpr int kLargeThreads = 384; // threads of a factorisation CTA (one per panel row)
 constexpr int kSolveThreads = 1024;
 
 constexpr int kColTile = 16;       // trailing-update columns per tile
@@ -182,26 +182,71 @@ __global__ void large_load_exported_kernel(const DevInst* __restrict__ insts, In
     for (long long i = first; i < I.n; i += stride) wbuf[I.f_off + i] = A.rhs_in[I.f_off + i];
 }
 
-// Shared memory of large_factor_kernel for a band of half-width bw: CTA 0's panel
-// (kPanel + bw) x (kPanel + 1), or a tile's panel copy of that size plus its column slab
-// (kPanel + bw) x kColTile.
+// Shared memory of large_factor_kernel: the panel's unit lower triangle L11
+// (kPanel x (kPanel + 1)); CTA 0's panel rows (kLargeThreads x (kPanel + 1)), whose space the
+// column slab of the trailing phase ((kPanel + bw) x (kColTile + 1)) reuses; the row at the
+// diagonal (two, by column parity) and the row that replaces it; the panel's row permutation.
 __host__ __device__ inline size_t large_factor_smem(int bw) {
-    return sizeof(double) * (size_t)(kPanel + bw) * (kPanel + 1 + kColTile);
+    (void)bw;
+    return sizeof(double) * ((size_t)kPanel * (kPanel + 1) + (size_t)kLargeThreads * (kPanel + 1) + 3 * kPanel) +
+           sizeof(int) * (size_t)kLargeThreads;
+}
+
+// Column tiles of the trailing update of one panel (+1: the right-hand side): the CTAs a
+// factorisation can keep busy.
+__host__ __device__ inline int large_factor_tiles(int bw) {
+    return (2 * bw + kColTile - 1) / kColTile + 1;
+}
+
+// Largest half-band the factorisation takes: one thread per panel row.
+constexpr int kLargeMaxBw = kLargeThreads - kPanel;
+
+// Argmax over a warp, the first (smallest index) of equal values winning.
+__device__ __forceinline__ void warp_argmax_first(double& v, int& idx) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
+        if (ov > v || (ov == v && oi < idx)) {
+            v = ov;
+            idx = oi;
+        }
+    }
 }
 
 // Cooperative.  wbuf holds the right-hand side on entry and L^-1 P b on exit; the band holds U
-// on exit (its strictly lower part is left stale: the substitution reads U only).  lpan / lpiv:
-// the factored panel and its interchanges, passed from CTA 0 to the others.
+// on exit (its strictly lower part is left stale: the substitution reads U only).  lpan
+// (column-major, leading dimension kLargeThreads) / lperm: the factored panel and the row
+// permutation of its interchanges, from CTA 0 to the others.
+//
+// Per panel: CTA 0 factors the panel columns with one thread per panel row, the row in
+// registers, four columns per rolled step (the finished columns go to shared memory and the
+// row shifts left).  Per column the row at the diagonal publishes itself as the pivot row and
+// one block vote asks whether any row below beats it strictly; only then the full search for the
+// first largest entry runs and the two rows are exchanged whole (multipliers included).  Grid
+// barrier; every CTA takes column tiles of the trailing block: loads them with the panel's row
+// permutation applied, solves the panel rows against the unit lower L11 on the warps (lane =
+// row), subtracts L21 U12 from the rows below entry by entry in column order (one thread per
+// row, the row's multipliers in registers); grid barrier.
 __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
     const DevInst* __restrict__ insts, InstArrays A, const int* __restrict__ large_list,
-    int n_large, int mode, GridBarrier* gb, double* wbuf, double* lpan, int* lpiv) {
+    int n_large, int mode, GridBarrier* gb, double* wbuf, double* lpan, int* lperm) {
     extern __shared__ __align__(16) double smem_lf[];
     __shared__ int s_flag[2];
     __shared__ int s_piv[kPanel];
     __shared__ double red[32];
     __shared__ int red_r[32];
+    constexpr int kPs = kPanel + 1;     // row stride of the panel rows and L11
+    constexpr int kSs = kColTile + 1;   // row stride of the slab
+    constexpr int kLd = kLargeThreads;  // leading dimension of lpan
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5;
     const int nwarps = nt >> 5;
+    double* L11 = smem_lf;                              // kPanel x kPs
+    double* Pout = L11 + kPanel * kPs;                  // panel rows (CTA 0), kLargeThreads x kPs
+    double* S = Pout;                                   // slab of the trailing phase, pr x kSs
+    double* prow2 = Pout + (size_t)kLargeThreads * kPs; // row at the diagonal, by column parity
+    double* crow = prow2 + 2 * kPanel;                  // the row that replaces it
+    int* s_perm = (int*)(crow + kPanel);                // panel row -> original row
     unsigned int gen = 0;
     if (tid == 0) gen = atomicAdd(&gb->gen, 0u);
     for (int li = 0; li < n_large; ++li) {
@@ -233,84 +278,118 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
             const int r1 = min(n - 1, k0 + kb - 1 + bw);      // last row with a nonzero in the panel
             const int pr = r1 - k0 + 1;
             const int c1 = min(n - 1, k0 + kb - 1 + 2 * bw);  // last column the panel's rows reach
-            const int ps = kb + 1;                            // padded row stride of the panel
+            const int r = tid;                                // the panel row of this thread
+            const bool own = r < pr;
             if (blockIdx.x == 0) {
-                // ---- panel: rows k0..r1, columns k0..k0+kb-1; one thread per row in the updates
-                double* Pm = smem_lf;
-                for (int t = tid; t < pr * kb; t += nt) {
-                    const int r = t / kb, c = t % kb;
-                    const int d = c - r;
-                    Pm[r * ps + c] = (d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, k0 + r, k0 + c)] : 0.0;
+                // ---- panel: rows k0..r1, columns k0..k0+kb-1 (rows loaded coalesced, lane = column)
+                for (int rr = wid; rr < pr; rr += nwarps) {
+                    const int d = lane - rr;
+                    Pout[rr * kPs + lane] =
+                        (lane < kb && d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, k0 + rr, k0 + lane)] : 0.0;
                 }
+                if (own) s_perm[r] = r;
                 if (tid == 0) s_flag[0] = LSTAT_OK;
                 __syncthreads();
-                for (int c = 0; c < kb; ++c) {
-                    const int last = min(pr - 1, c + bw);  // rows of column k0+c inside the band
-                    // the first largest |entry| of the column (the reference's strict '>' scan)
-                    double bv = -1.0;
-                    int br = c;
-                    for (int r = c + tid; r <= last; r += nt) {
-                        const double v = fabs(Pm[r * ps + c]);
-                        if (v > bv) {
-                            bv = v;
-                            br = r;
+                double a[kPanel];  // a[q] = column c0 + q of this thread's row
+#pragma unroll
+                for (int q = 0; q < kPanel; ++q) a[q] = own ? Pout[r * kPs + q] : 0.0;
+                bool failed = false;
+                for (int c0 = 0; c0 < kb; c0 += 4) {
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const int c = c0 + cc;
+                        if (c < kb && !failed) {
+                            const int last = min(pr - 1, c + bw);  // rows of column k0+c in the band
+                            const bool act = own && r > c && r <= last;
+                            // double buffered: a slow thread may still read the previous one
+                            double* prow = prow2 + (c & 1) * kPanel;
+                            if (r == c) {
+#pragma unroll
+                                for (int q = 0; q < kPanel; ++q) prow[q] = a[q];
+                            }
+                            __syncthreads();
+                            // the reference's strict '>' scan keeps the diagonal unless a row
+                            // below beats it
+                            const double dabs = fabs(prow[cc]);
+                            const int any = __syncthreads_or(act && fabs(a[cc]) > dabs);
+                            const double* pivrow = prow;
+                            int p = c;
+                            if (any || dabs <= 1.0e-14) {
+                                double bv = (own && r >= c && r <= last) ? fabs(a[cc]) : -1.0;
+                                int br = r;
+                                warp_argmax_first(bv, br);
+                                if (lane == 0) {
+                                    red[wid] = bv;
+                                    red_r[wid] = br;
+                                }
+                                __syncthreads();
+                                double pv = lane < nwarps ? red[lane] : -2.0;
+                                p = lane < nwarps ? red_r[lane] : 0x7fffffff;
+                                warp_argmax_first(pv, p);
+                                if (pv <= 1.0e-14) {
+                                    failed = true;
+                                    if (tid == 0) s_flag[0] = LSTAT_SINGULAR;
+                                } else if (p != c) {
+                                    // whole rows, multipliers included, so that the trailing
+                                    // columns can take all interchanges first and the
+                                    // eliminations after
+                                    pivoted = 1;
+                                    if (r == p) {
+#pragma unroll
+                                        for (int q = 0; q < kPanel; ++q) crow[q] = a[q];
+                                    }
+                                    if (tid == 0) {
+                                        const int o = s_perm[c];
+                                        s_perm[c] = s_perm[p];
+                                        s_perm[p] = o;
+                                    }
+                                    if (wid == 0 && lane < c0) {
+                                        // finished columns of earlier steps
+                                        const double t0 = Pout[c * kPs + lane];
+                                        Pout[c * kPs + lane] = Pout[p * kPs + lane];
+                                        Pout[p * kPs + lane] = t0;
+                                    }
+                                    __syncthreads();
+                                    if (r == c) {
+#pragma unroll
+                                        for (int q = 0; q < kPanel; ++q) a[q] = crow[q];
+                                    } else if (r == p) {
+#pragma unroll
+                                        for (int q = 0; q < kPanel; ++q) a[q] = prow[q];
+                                    }
+                                    pivrow = crow;
+                                }
+                            }
+                            if (!failed) {
+                                if (act) {
+                                    const double f = a[cc] / pivrow[cc];
+                                    a[cc] = f;
+#pragma unroll
+                                    for (int q = cc + 1; q < kPanel; ++q)
+                                        if (c0 + q < kb) a[q] = fma(-f, pivrow[q], a[q]);
+                                }
+                                if (tid == 0) s_piv[c] = p;
+                            }
                         }
                     }
-                    for (int off = 16; off > 0; off >>= 1) {
-                        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                        const int orr = __shfl_xor_sync(0xffffffffu, br, off);
-                        if (ov > bv || (ov == bv && orr < br)) {
-                            bv = ov;
-                            br = orr;
-                        }
+                    // columns c0 .. c0+3 are final: keep them, shift the row left by four
+                    if (own) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            if (c0 + q < kPanel) Pout[r * kPs + c0 + q] = a[q];
                     }
-                    if (lane == 0) {
-                        red[wid] = bv;
-                        red_r[wid] = br;
-                    }
-                    __syncthreads();
-                    double pv = red[0];
-                    int p = red_r[0];
-                    for (int q = 1; q < nwarps; ++q) {
-                        if (red[q] > pv || (red[q] == pv && red_r[q] < p)) {
-                            pv = red[q];
-                            p = red_r[q];
-                        }
-                    }
-                    if (pv <= 1.0e-14) {
-                        if (tid == 0) s_flag[0] = LSTAT_SINGULAR;
-                        break;
-                    }
-                    if (tid == 0) s_piv[c] = p;
-                    if (p != c) {
-                        // whole panel rows, multipliers included, so that the trailing columns
-                        // can take all interchanges first and the eliminations after
-                        pivoted = 1;
-                        for (int cc = tid; cc < kb; cc += nt) {
-                            const double t0 = Pm[c * ps + cc];
-                            Pm[c * ps + cc] = Pm[p * ps + cc];
-                            Pm[p * ps + cc] = t0;
-                        }
-                        __syncthreads();
-                    }
-                    const double diag = Pm[c * ps + c];
-                    for (int r = c + 1 + tid; r <= last; r += nt) {
-                        const double f = Pm[r * ps + c] / diag;
-                        Pm[r * ps + c] = f;
-                        if (f == 0.0) continue;
-                        for (int cc = c + 1; cc < kb; ++cc) Pm[r * ps + cc] -= f * Pm[c * ps + cc];
-                    }
-                    __syncthreads();
+#pragma unroll
+                    for (int q = 0; q < kPanel; ++q) a[q] = q + 4 < kPanel ? a[q + 4] : 0.0;
                 }
                 __syncthreads();
                 if (s_flag[0] == LSTAT_OK) {
-                    for (int t = tid; t < pr * kb; t += nt) {
-                        const int r = t / kb, c = t % kb;
-                        const double v = Pm[r * ps + c];
-                        lpan[r * ps + c] = v;
-                        if (r <= c) B[lslot(lrw, bw, k0 + r, k0 + c)] = v;
+                    for (int t = tid; t < kb * pr; t += nt) {
+                        const int q = t / pr, rr = t - q * pr;
+                        lpan[q * kLd + rr] = Pout[rr * kPs + q];
                     }
-                    for (int c = tid; c < kb; c += nt) lpiv[c] = s_piv[c];
+                    for (int rr = wid; rr < kb; rr += nwarps)
+                        if (lane >= rr && lane < kb) B[lslot(lrw, bw, k0 + rr, k0 + lane)] = Pout[rr * kPs + lane];
+                    if (own) lperm[r] = s_perm[r];
                 }
                 if (tid == 0) {
                     A.lstatus[li] = s_flag[0];
@@ -327,62 +406,77 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
             const int j_first = k0 + kb;
             const int ncols = c1 - j_first + 1;
             const int ntiles = (ncols > 0 ? (ncols + kColTile - 1) / kColTile : 0) + 1;
-            double* Ls = smem_lf;                                         // pr x ps
-            double* S = smem_lf + (size_t)(kPanel + bw) * (kPanel + 1);   // pr x kColTile
-            bool loaded = false;
-            for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-                __syncthreads();
-                if (!loaded) {
-                    for (int t = tid; t < pr * ps; t += nt) Ls[t] = lpan[t];
-                    for (int c = tid; c < kb; c += nt) s_piv[c] = lpiv[c];
-                    loaded = true;
+            if (blockIdx.x >= ntiles) {
+                if (!grid_barrier(gb, gen)) return;
+                continue;
+            }
+            // this thread's panel row: its multipliers (L21, or L11 for the first kb rows)
+            double lrow[kPanel];
+#pragma unroll
+            for (int q = 0; q < kPanel; ++q) lrow[q] = (own && q < kb) ? lpan[q * kLd + r] : 0.0;
+            if (own) {
+                s_perm[r] = lperm[r];
+                if (r < kb) {
+#pragma unroll
+                    for (int q = 0; q < kPanel; ++q) L11[r * kPs + q] = lrow[q];
                 }
+            }
+            for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
                 const bool rhs = tile == ntiles - 1;
                 const int j0 = j_first + tile * kColTile;
                 const int ct = rhs ? 1 : min(kColTile, c1 - j0 + 1);
+                __syncthreads();
                 for (int t = tid; t < pr * ct; t += nt) {
-                    const int r = t / ct, q = t % ct;
-                    const int i = k0 + r;
+                    const int rr = t / ct, q = t - rr * ct;
+                    const int src = k0 + s_perm[rr];
                     double v;
                     if (rhs) {
-                        v = w[i];
+                        v = w[src];
                     } else {
-                        const int d = j0 + q - i;
-                        v = (d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, i, j0 + q)] : 0.0;
+                        const int d = j0 + q - src;
+                        v = (d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, src, j0 + q)] : 0.0;
                     }
-                    S[r * kColTile + q] = v;
+                    S[rr * kSs + q] = v;
                 }
                 __syncthreads();
-                for (int q = tid; q < ct; q += nt) {
-                    for (int c = 0; c < kb; ++c) {
-                        const int p = s_piv[c];
-                        if (p != c) {
-                            const double t0 = S[c * kColTile + q];
-                            S[c * kColTile + q] = S[p * kColTile + q];
-                            S[p * kColTile + q] = t0;
+                // U12 = L11^-1 (P A12): one warp per column, lane = panel row
+                for (int q = wid; q < ct; q += nwarps) {
+                    double v = lane < kb ? S[lane * kSs + q] : 0.0;
+                    for (int sc = 0; sc + 1 < kb; ++sc) {
+                        const double u = __shfl_sync(0xffffffffu, v, sc);
+                        if (lane > sc && lane < kb) v = fma(-L11[lane * kPs + sc], u, v);
+                    }
+                    if (lane < kb) S[lane * kSs + q] = v;
+                }
+                __syncthreads();
+                // A22 -= L21 U12 entry by entry, column order; one thread per row
+                double v[kColTile];
+                if (own && r >= kb) {
+#pragma unroll
+                    for (int q = 0; q < kColTile; ++q) v[q] = S[r * kSs + q];
+#pragma unroll
+                    for (int sc = 0; sc < kPanel; ++sc) {
+                        if (sc < kb) {
+                            const double f = lrow[sc];
+#pragma unroll
+                            for (int q = 0; q < kColTile; ++q) v[q] = fma(-f, S[sc * kSs + q], v[q]);
                         }
                     }
                 }
                 __syncthreads();
-                for (int sc = 0; sc < kb; ++sc) {
-                    // the panel's interchanges carried multipliers of column sc down to any
-                    // panel row, not only the bw rows below it
-                    const int rows = pr - 1 - sc;
-                    for (int t = tid; t < rows * ct; t += nt) {
-                        const int r = sc + 1 + t / ct, q = t % ct;
-                        const double f = Ls[r * ps + sc];
-                        if (f != 0.0) S[r * kColTile + q] -= f * S[sc * kColTile + q];
-                    }
-                    __syncthreads();
+                if (own && r >= kb) {
+#pragma unroll
+                    for (int q = 0; q < kColTile; ++q) S[r * kSs + q] = v[q];
                 }
+                __syncthreads();
                 for (int t = tid; t < pr * ct; t += nt) {
-                    const int r = t / ct, q = t % ct;
-                    const int i = k0 + r;
+                    const int rr = t / ct, q = t - rr * ct;
+                    const int i = k0 + rr;
                     if (rhs) {
-                        w[i] = S[r * kColTile + q];
+                        w[i] = S[rr * kSs];
                     } else {
                         const int d = j0 + q - i;
-                        if (d >= -bw && d <= 2 * bw) B[lslot(lrw, bw, i, j0 + q)] = S[r * kColTile + q];
+                        if (d >= -bw && d <= 2 * bw) B[lslot(lrw, bw, i, j0 + q)] = S[rr * kSs + q];
                     }
                 }
             }
@@ -394,14 +488,22 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
 
 // ---- substitution, update and test ---------------------------------------------------------
 
-// One CTA per large instance: U x = L^-1 P b (left in wbuf by the factorisation) in blocks of 32
-// rows from the end, each block solved by warp 0 then pushed into the 2 bw rows above.
+// Dynamic shared memory of large_solve_kernel: x (n) and one 32 x 33 diagonal block of U.
+__host__ __device__ inline size_t large_solve_smem(int n) {
+    return sizeof(double) * ((size_t)n + 32 * 33);
+}
+
+// One CTA per large instance (32 warps): U x = L^-1 P b (left in wbuf by the factorisation) in
+// blocks of 32 rows from the end.  Warp r of a block forms row r's sum over the columns below
+// the block (the row's U entries are contiguous in the band), then warp 0 solves the block's
+// triangle with shuffles.  x stays in shared memory.
 __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
     const DevInst* __restrict__ insts, InstArrays A, const int* __restrict__ large_list, int n_large,
     int mode, double* __restrict__ wbuf, const GridBarrier* __restrict__ gb) {
+    extern __shared__ __align__(16) double smem_ls[];
     __shared__ double red[32];
     __shared__ int red_r[32];
-    __shared__ double xb[32];
+    __shared__ double tb[32];
     const int li = blockIdx.x;
     if (li >= n_large) return;
     const int inst = large_list[li];
@@ -419,7 +521,7 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
         }
         return;
     }
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5;
     const int n = I.n, bw = I.bw, lrw = I.lrw, f0 = I.f_off;
     const int ub = 2 * bw;  // reach of U
     int* hrow = (mode == INST_MODE_NEWTON && A.hist_iters && A.ctl)
@@ -444,33 +546,37 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
     }
     const double* B = A.lband + I.lband_off;
     double* w = wbuf + f0;  // L^-1 P b, then x
-    const int lane = tid & 31;
+    double* xs = smem_ls;         // n
+    double* Ud = smem_ls + n;     // 32 x 33
+    const int nwarps = nt >> 5;
     for (int r1 = n; r1 > 0; r1 -= 32) {
         const int r0 = max(0, r1 - 32), rb = r1 - r0;
-        if (tid < 32) {
-            double v = lane < rb ? w[r0 + lane] : 0.0;
-            for (int s = rb - 1; s >= 0; --s) {
-                if (lane == s) v = v / B[lslot(lrw, bw, r0 + s, r0 + s)];
-                const double xs = __shfl_sync(0xffffffffu, v, s);
-                if (lane < s && (s - lane) <= ub) v -= B[lslot(lrw, bw, r0 + lane, r0 + s)] * xs;
-            }
-            if (lane < rb) {
-                w[r0 + lane] = v;
-                xb[lane] = v;
-            }
+        for (int r = wid; r < rb; r += nwarps) {
+            const int i = r0 + r;
+            const double* urow = B + (long long)i * lrw + bw;  // U(i, i + o), o = 0 .. 2 bw
+            double acc = 0.0;
+            const int jmax = min(n - 1, i + ub);
+#pragma unroll 8
+            for (int j = r1 + lane; j <= jmax; j += 32) acc = fma(urow[j - i], xs[j], acc);
+            acc = warp_sum(acc);
+            const int o = r0 + lane - i;
+            if (lane < rb) Ud[r * 33 + lane] = (o >= 0 && o <= ub) ? urow[o] : 0.0;
+            if (lane == 0) tb[r] = w[i] - acc;
         }
         __syncthreads();
-        const int i_first = max(0, r0 - ub);
-        for (int i = i_first + tid; i < r0; i += nt) {
-            double acc = 0.0;
-            for (int s = 0; s < rb; ++s) {
-                const int j = r0 + s;
-                if (j - i <= ub) acc += B[lslot(lrw, bw, i, j)] * xb[s];
+        if (wid == 0) {
+            double v = lane < rb ? tb[lane] : 0.0;
+            for (int s = rb - 1; s >= 0; --s) {
+                if (lane == s) v = v / Ud[s * 33 + s];
+                const double x = __shfl_sync(0xffffffffu, v, s);
+                if (lane < s) v = fma(-Ud[lane * 33 + s], x, v);
             }
-            w[i] -= acc;
+            if (lane < rb) xs[r0 + lane] = v;
         }
         __syncthreads();
     }
+    for (int i = tid; i < n; i += nt) w[i] = xs[i];
+    __syncthreads();
     if (mode == INST_MODE_SOLVE_EXPORTED) {
         for (int i = tid; i < n; i += nt) A.du[f0 + i] = w[i];
         return;

@@ -298,7 +298,7 @@ struct StrutHandle {
     GridBarrier* d_gb = nullptr;
     double* d_wbuf = nullptr;
     double* d_lpan = nullptr;  // factored panel, CTA 0 -> the other CTAs
-    int* d_lpiv = nullptr;     // its interchanges
+    int* d_lpiv = nullptr;     // its row permutation
     int n_slaves_total = 0;          // slave dofs of every instance (multi-point constraints)
     int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
     long long band_total = 0;
@@ -478,7 +478,7 @@ static int launch_large(StrutHandle* h, int mode, const DevInst* insts = nullptr
         CK(cudaLaunchCooperativeKernel((const void*)large_factor_kernel, dim3(h->lfactor_grid),
                                        dim3(kLargeThreads), args, h->lfactor_smem, h->stream));
     }
-    large_solve_kernel<<<h->n_large, kSolveThreads, 0, h->stream>>>(insts, A, h->d_large_list, h->n_large, mode,
+    large_solve_kernel<<<h->n_large, kSolveThreads, large_solve_smem(h->max_large_n), h->stream>>>(insts, A, h->d_large_list, h->n_large, mode,
                                                                     h->d_wbuf, h->d_gb);
     CK(cudaGetLastError());
     return STRUT_OK;
@@ -1083,8 +1083,10 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             if (I.spd)
                 return bail(fail(STRUT_UNSUPPORTED, "BandSPD bands beyond shared memory are not implemented"));
             const size_t fsm = large_factor_smem(bw);
-            if (fsm > 220 * 1024)
+            if (fsm > 220 * 1024 || bw > kLargeMaxBw)
                 return bail(fail(STRUT_UNSUPPORTED, "band width too large for the blocked factorisation"));
+            if (large_solve_smem(nf) > 220 * 1024)
+                return bail(fail(STRUT_UNSUPPORTED, "system too large for the band substitution"));
             I.large = 1;
             I.large_idx = h->n_large++;
             I.lrw = 3 * bw + 1;  // columns i - bw .. i + 2 bw: room for the pivot rows' fill
@@ -1295,8 +1297,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         if ((rc = upload(&h->d_large_list, h->large_list_h, al)) || (rc = upload(&h->d_large_rowbase, rowbase, al)) ||
             (rc = dzeros(&A.lband, (size_t)h->lband_total, al)) || (rc = upload(&A.lstatus, lstat, al)) ||
             (rc = dzeros(&h->d_gb, 1, al)) || (rc = dzeros(&h->d_wbuf, nF, al)) ||
-            (rc = dzeros(&h->d_lpan, (size_t)(kPanel + h->max_large_bw) * (kPanel + 1), al)) ||
-            (rc = dzeros(&h->d_lpiv, (size_t)kPanel, al)))
+            (rc = dzeros(&h->d_lpan, (size_t)kPanel * kLargeThreads, al)) ||
+            (rc = dzeros(&h->d_lpiv, (size_t)kLargeThreads, al)))
             return bail(rc);
         CK(cudaFuncSetAttribute(large_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)h->lfactor_smem));
@@ -1305,7 +1307,11 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
                                                          h->lfactor_smem));
         CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->device));
         if (per_sm < 1) return bail(fail(STRUT_UNSUPPORTED, "band factorisation kernel does not fit on an SM"));
-        h->lfactor_grid = n_sm;  // one CTA per SM, all co-resident (cooperative launch)
+        // one CTA per SM at most, all co-resident (cooperative launch), and no more than one
+        // panel's trailing tiles can use
+        h->lfactor_grid = std::max(1, std::min(n_sm, large_factor_tiles(h->max_large_bw)));
+        CK(cudaFuncSetAttribute(large_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)large_solve_smem(h->max_large_n)));
     }
     CK(cudaMallocHost((void**)&h->h_ctrl, 4 * sizeof(int)));
     CK(cudaEventCreate(&h->ev0));
