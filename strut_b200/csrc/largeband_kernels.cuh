@@ -184,7 +184,7 @@ __global__ void large_load_exported_kernel(const DevInst* __restrict__ insts, In
 
 // Shared memory of large_factor_kernel: the panel's unit lower triangle L11
 // (kPanel x (kPanel + 1)); CTA 0's panel rows (kLargeThreads x (kPanel + 1)), whose space the
-// column slab of the trailing phase ((kPanel + bw) x (kColTile + 1)) reuses; the row at the
+// column slab of the trailing phase ((kPanel + bw) x (kColTile + 2)) reuses; the row at the
 // diagonal (two, by column parity) and the row that replaces it; the panel's row permutation.
 __host__ __device__ inline size_t large_factor_smem(int bw) {
     (void)bw;
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
     __shared__ double red[32];
     __shared__ int red_r[32];
     constexpr int kPs = kPanel + 1;     // row stride of the panel rows and L11
-    constexpr int kSs = kColTile + 1;   // row stride of the slab
+    constexpr int kSs = kColTile + 2;   // row stride of the slab (even: 16-byte rows)
     constexpr int kLd = kLargeThreads;  // leading dimension of lpan
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5;
     const int nwarps = nt >> 5;
@@ -282,10 +282,18 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
             const bool own = r < pr;
             if (blockIdx.x == 0) {
                 // ---- panel: rows k0..r1, columns k0..k0+kb-1 (rows loaded coalesced, lane = column)
-                for (int rr = wid; rr < pr; rr += nwarps) {
-                    const int d = lane - rr;
-                    Pout[rr * kPs + lane] =
-                        (lane < kb && d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, k0 + rr, k0 + lane)] : 0.0;
+                for (int rb = wid; rb < pr; rb += 4 * nwarps) {
+                    double v[4];  // four rows in flight per warp
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int rr = rb + m * nwarps;
+                        const int d = lane - rr;
+                        v[m] = (rr < pr && lane < kb && d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, k0 + rr, k0 + lane)]
+                                                                                 : 0.0;
+                    }
+#pragma unroll
+                    for (int m = 0; m < 4; ++m)
+                        if (rb + m * nwarps < pr) Pout[(rb + m * nwarps) * kPs + lane] = v[m];
                 }
                 if (own) s_perm[r] = r;
                 if (tid == 0) s_flag[0] = LSTAT_OK;
@@ -426,17 +434,28 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                 const int j0 = j_first + tile * kColTile;
                 const int ct = rhs ? 1 : min(kColTile, c1 - j0 + 1);
                 __syncthreads();
-                for (int t = tid; t < pr * ct; t += nt) {
-                    const int rr = t / ct, q = t - rr * ct;
-                    const int src = k0 + s_perm[rr];
-                    double v;
-                    if (rhs) {
-                        v = w[src];
-                    } else {
-                        const int d = j0 + q - src;
-                        v = (d >= -bw && d <= 2 * bw) ? B[lslot(lrw, bw, src, j0 + q)] : 0.0;
+                for (int t0 = tid; t0 < pr * ct; t0 += 4 * nt) {
+                    double v[4];  // four loads in flight per thread
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int t = t0 + m * nt;
+                        v[m] = 0.0;
+                        if (t < pr * ct) {
+                            const int rr = t / ct, q = t - rr * ct;
+                            const int src = k0 + s_perm[rr];
+                            const int d = j0 + q - src;
+                            if (rhs) v[m] = w[src];
+                            else if (d >= -bw && d <= 2 * bw) v[m] = B[lslot(lrw, bw, src, j0 + q)];
+                        }
                     }
-                    S[rr * kSs + q] = v;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int t = t0 + m * nt;
+                        if (t < pr * ct) {
+                            const int rr = t / ct;
+                            S[rr * kSs + (t - rr * ct)] = v[m];
+                        }
+                    }
                 }
                 __syncthreads();
                 // U12 = L11^-1 (P A12): one warp per column, lane = panel row
@@ -459,7 +478,11 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                         if (sc < kb) {
                             const double f = lrow[sc];
 #pragma unroll
-                            for (int q = 0; q < kColTile; ++q) v[q] = fma(-f, S[sc * kSs + q], v[q]);
+                            for (int q2 = 0; q2 < kColTile / 2; ++q2) {
+                                const double2 u = reinterpret_cast<const double2*>(S + sc * kSs)[q2];
+                                v[2 * q2] = fma(-f, u.x, v[2 * q2]);
+                                v[2 * q2 + 1] = fma(-f, u.y, v[2 * q2 + 1]);
+                            }
                         }
                     }
                 }
