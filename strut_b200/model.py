@@ -507,17 +507,64 @@ class Model:
                 )
             )
 
-        # recorders
-        rec_dofs = []
-        rec_elems = []
+        # recorders (transient_nonlinear.mojo:1550-1700): each needs displacement columns (full
+        # dof indices) and element-force columns of the device history, shared between recorders
+        rec_dofs, rec_elems = [], []
+        dof_col, elem_col = {}, {}
+
+        def dcol(dof):
+            if dof not in dof_col:
+                dof_col[dof] = len(rec_dofs)
+                rec_dofs.append(dof)
+            return dof_col[dof]
+
+        def ecol(e):
+            if e not in elem_col:
+                elem_col[e] = len(rec_elems)
+                rec_elems.append(e)
+            return elem_col[e]
+
+        def node_of(nid, what):
+            if int(nid) not in self.node_index:
+                raise ModelError(f"{what}: node {nid} not found")
+            return self.node_index[int(nid)]
+
+        def dof_of(d, what):
+            d = int(d)
+            if d < 1 or d > self.ndf:
+                raise ModelError(f"{what}: dof {d} out of range 1..{self.ndf}")
+            return d - 1
+
+        self.recorder_plan = []
         for r in case.get("recorders", []) or []:
-            if r["type"] == "node_displacement":
+            t = r["type"]
+            out = str(r.get("output", t))
+            if t in ("node_displacement", "envelope_node_displacement"):
                 for nid in r["nodes"]:
-                    for d in r["dofs"]:
-                        rec_dofs.append(self.node_index[int(nid)] * self.ndf + int(d) - 1)
-            elif r["type"] == "element_force":
+                    ni = node_of(nid, t)
+                    cols = [dcol(ni * self.ndf + dof_of(d, t)) for d in r["dofs"]]
+                    self.recorder_plan.append({"type": t, "file": f"{out}_node{int(nid)}.out", "disp_cols": cols})
+            elif t in ("element_force", "envelope_element_force"):
                 for eid in r["elements"]:
-                    rec_elems.append(self.elem_index[int(eid)])
+                    if int(eid) not in self.elem_index:
+                        raise ModelError(f"{t}: element {eid} not found")
+                    c = ecol(self.elem_index[int(eid)])
+                    self.recorder_plan.append({"type": t, "file": f"{out}_ele{int(eid)}.out", "elem_col": c})
+            elif t == "drift":
+                i_node, j_node = int(r["i_node"]), int(r["j_node"])
+                ii, jj = node_of(i_node, t), node_of(j_node, t)
+                d = dof_of(r["dof"], t)
+                perp = int(r["perp_dirn"])
+                if perp < 1 or perp > 3 or (perp == 3 and self.ndm < 3):
+                    raise ModelError("drift perp_dirn must be in 1..ndm")
+                dx = self.coords[self.ndm * jj + perp - 1] - self.coords[self.ndm * ii + perp - 1]
+                if dx == 0.0:
+                    raise ModelError("drift denominator is zero")
+                self.recorder_plan.append({"type": t, "file": f"{out}_i{i_node}_j{j_node}.out",
+                                           "i_col": dcol(ii * self.ndf + d), "j_col": dcol(jj * self.ndf + d),
+                                           "dx": float(dx)})
+            else:
+                raise ModelError(f"recorder type {t!r} is not on this path")
         self.record_dofs = np.asarray(rec_dofs, dtype=np.int32)
         self.record_elements = np.asarray(rec_elems, dtype=np.int32)
 
