@@ -77,6 +77,13 @@ enum { STRUT_GEOM_LINEAR = 0, STRUT_GEOM_PDELTA = 1, STRUT_GEOM_COROTATIONAL = 2
 enum { STRUT_SYSTEM_BAND_GENERAL = 1, STRUT_SYSTEM_BAND_SPD = 2 };
 
 /* Transient test modes (transient_nonlinear.mojo:671-684). */
+/* Newton variants (transient_nonlinear.mojo:650-668, 2072-2085, 2236-2268, 2421-2440): Newton
+ * refreshes the tangent every iteration; ModifiedNewton takes the first iteration's tangent (and
+ * the Rayleigh C built from it) for the whole step and factors once per step; ModifiedNewtonInitial
+ * does the same with the initial tangent. */
+enum { STRUT_ALGORITHM_NEWTON = 0, STRUT_ALGORITHM_MODIFIED_NEWTON = 1,
+       STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL = 2 };
+
 enum { STRUT_TEST_MAX_DISP_INCR = 0, STRUT_TEST_NORM_DISP_INCR = 1,
        STRUT_TEST_NORM_UNBALANCE = 2, STRUT_TEST_ENERGY_INCR = 3 };
 
@@ -196,7 +203,7 @@ typedef struct StrutModelDesc {
      * entries outside it as Strut does (linear_solver_backend.mojo:413-427, 1481-1507).  A slave
      * dof may carry no mass.  num_slaves 0: none. */
     int32_t num_slaves;
-    int32_t reserved_mpc;
+    int32_t algorithm;             /* STRUT_ALGORITHM_* (0, Newton, when left zero)        */
     const int32_t* slave_dof;      /* num_slaves full dof indices                          */
     const int32_t* slave_ptr;      /* num_slaves + 1 offsets into the term arrays          */
     const int32_t* slave_master;   /* retained full dof of each term                       */

@@ -771,7 +771,8 @@ static int initial_assembly(OModel* m) {
     int rc = assemble(m, 0, 0);
     if (rc != STRUT_OK) return rc;
     size_t bsz = (size_t)m->n * m->rw;
-    if (m->d->beta_k_init != 0.0) memcpy(m->Kinit, m->K, sizeof(double) * bsz);
+    if (m->d->beta_k_init != 0.0 || m->d->algorithm == STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL)
+        memcpy(m->Kinit, m->K, sizeof(double) * bsz);
     if (m->d->beta_k_comm != 0.0) memcpy(m->Kcomm, m->K, sizeof(double) * bsz);
     for (int e = 0; e < m->d->num_elements; ++e)
         for (int ip = 0; ip < m->elems[e].nip; ++ip) oracle_section_revert(&m->elems[e].sst[ip]);
@@ -850,9 +851,9 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
             /* F_const is collapsed once at load, the inertia load of each excitation every
              * step (loader.mojo:2344, transient_nonlinear.mojo:1836-1848) */
             int nd = d->num_dofs;
-            double* acc = (double*)calloc((size_t)nd, sizeof(double));
-            double* inert = (double*)calloc((size_t)nd, sizeof(double));
-            double* red = (double*)calloc((size_t)nd, sizeof(double));
+            double* acc = (double*)calloc((size_t)(nd > 0 ? nd : 1), sizeof(double));
+            double* inert = (double*)calloc((size_t)(nd > 0 ? nd : 1), sizeof(double));
+            double* red = (double*)calloc((size_t)(nd > 0 ? nd : 1), sizeof(double));
             for (int dof = 0; dof < nd; ++dof) inert[dof] = d->f_const ? d->f_const[dof] : 0.0;
             mpc_collapse_vector(m, inert, acc);
             for (int x = 0; x < d->num_excitations; ++x) {
@@ -888,10 +889,18 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
                 if (failed_step) *failed_step = step;
                 return rc;
             }
-            rc = build_keff(m);
-            if (rc != STRUT_OK) {
-                if (failed_step) *failed_step = step;
-                return rc;
+            /* Newton refreshes K_ff, C_ff and the factors every iteration; ModifiedNewton keeps
+             * the first iteration's for the step, ModifiedNewtonInitial takes K_init_ff
+             * (transient_nonlinear.mojo:2072-2085, 2236-2268, 2302-2335, 2421-2440) */
+            const int refresh = d->algorithm == STRUT_ALGORITHM_NEWTON || it == 0;
+            if (refresh) {
+                if (d->algorithm == STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL)
+                    memcpy(m->K, m->Kinit, sizeof(double) * (size_t)n * m->rw);
+                rc = build_keff(m);
+                if (rc != STRUT_OK) {
+                    if (failed_step) *failed_step = step;
+                    return rc;
+                }
             }
             for (int i = 0; i < n; ++i) {
                 double an = m->a0 * (m->u_f[i] - m->u_n[i]) - m->a2 * m->v_n[i] - m->a3 * m->a_n[i];
@@ -915,12 +924,14 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
                     break;
                 }
             }
-            rc = m->spd ? band_spd_factor(m) : band_general_factor(m);
-            if (rc != STRUT_OK) {
-                if (failed_step) *failed_step = step;
-                return rc;
+            if (refresh) {
+                rc = m->spd ? band_spd_factor(m) : band_general_factor(m);
+                if (rc != STRUT_OK) {
+                    if (failed_step) *failed_step = step;
+                    return rc;
+                }
+                m->factorizations++;
             }
-            m->factorizations++;
             rc = m->spd ? band_spd_solve(m, m->R_f, m->du) : band_general_solve(m, m->R_f, m->du);
             if (rc != STRUT_OK) {
                 if (failed_step) *failed_step = step;

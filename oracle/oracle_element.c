@@ -94,7 +94,7 @@ static int fbc_try_increment(OElement* e, const double base[3], const double dv[
     double q0 = e->q[0], q1 = e->q[1], q2 = e->q[2];
     double t0 = base[0] + dv[0], t1 = base[1] + dv[1], t2 = base[2] + dv[2];
     if (!sd->init_valid) return 0;
-    double vs_e[STRUT_MAX_INT_PTS], vs_k[STRUT_MAX_INT_PTS];
+    double vs_e[STRUT_MAX_INT_PTS] = {0}, vs_k[STRUT_MAX_INT_PTS] = {0};
     double sub_e[STRUT_MAX_INT_PTS], sub_k[STRUT_MAX_INT_PTS];
     double ssr_n[STRUT_MAX_INT_PTS], ssr_m[STRUT_MAX_INT_PTS];
     double fs00[STRUT_MAX_INT_PTS], fs01[STRUT_MAX_INT_PTS], fs11[STRUT_MAX_INT_PTS];

@@ -53,6 +53,7 @@ TEST_MAX_DISP_INCR = 0
 TEST_NORM_DISP_INCR = 1
 TEST_NORM_UNBALANCE = 2
 TEST_ENERGY_INCR = 3
+ALGORITHM_NEWTON, ALGORITHM_MODIFIED_NEWTON, ALGORITHM_MODIFIED_NEWTON_INITIAL = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -161,7 +162,7 @@ class StrutModelDesc(C.Structure):
         ("record_dofs", _ip),
         ("record_elements", _ip),
         ("num_slaves", C.c_int32),
-        ("reserved_mpc", C.c_int32),
+        ("algorithm", C.c_int32),
         ("slave_dof", _ip),
         ("slave_ptr", _ip),
         ("slave_master", _ip),

@@ -90,6 +90,7 @@ struct DevInst {
     int large, large_idx; // band in global memory (too large for shared memory), its index
     long long lband_off;  // offset of its band in the global band buffer
     int lrw, pad_l;       // slots per row of that band (3 bw + 1)
+    int algorithm, pad_al; // STRUT_ALGORITHM_* (Newton, ModifiedNewton, ModifiedNewtonInitial)
     int sl_off, n_sl;     // this instance's slave dofs (multi-point constraints)
 };
 

@@ -116,6 +116,9 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
         return fail(STRUT_UNSUPPORTED, "the learned predictor runs on instances whose band fits in shared memory");
     if (h->n_slaves_total > 0)
         return fail(STRUT_UNSUPPORTED, "the learned predictor does not run with multi-point constraints");
+    for (const DevInst& I : h->insts)
+        if (I.algorithm != STRUT_ALGORITHM_NEWTON)
+            return fail(STRUT_UNSUPPORTED, "the learned predictor runs with the Newton algorithm");
     const int ndf = h->pn_ndf, n_in = 4 * ndf + 17;
     if (m->n_in != n_in || m->n_out != ndf)
         return fail(STRUT_BAD_ARG, "network must take " + std::to_string(n_in) + " features and give " +

@@ -70,6 +70,11 @@ struct InstArrays {
     const int* sl_master;
     const double* sl_coef;
     // instances whose band lives in global memory
+    // ModifiedNewton / ModifiedNewtonInitial: the step's tangent (band_off layout), its factored
+    // effective band, and whether the factors are the dense fallback's (A.dense, A.piv)
+    double* kfrz;
+    double* lufrz;
+    int* lu_dense;
     double* lband;          // effective band (factored in place), at DevInst::lband_off
     int* lstatus;           // per large instance: 0 factored, 2 singular, 6 dense fallback,
                             // 7 converged before the solve (NormUnbalance), -1 not active
@@ -318,6 +323,20 @@ __device__ double residual_norm(const DevInst& I, const InstArrays& A, const dou
 
 // Effective-matrix entry of band slot (i, j) exactly as the row assembly computes it
 // (load K, add a1 C, add a0 M).
+__device__ __forceinline__ double keff_of(const DevInst& I, const InstArrays& A, const double* Kinit, int i,
+                                          int j, int slot, double K) {
+    double C = 0.0;
+    if (I.has_damping) {
+        C = I.alpha_m * (i == j ? A.Mrff[I.f_off + i] : 0.0);
+        if (I.beta_k != 0.0) C += I.beta_k * K;
+        if (I.beta_k_init != 0.0) C += I.beta_k_init * Kinit[slot];
+    }
+    double keff = K;
+    if (I.has_damping && I.a1 != 0.0) keff += I.a1 * C;
+    if (i == j) keff += I.a0 * A.Mff[I.f_off + i];
+    return keff;
+}
+
 __device__ __forceinline__ double keff_slot(const DevInst& I, const InstArrays& A, long long sp0,
                                             const double* Kinit, int i, int j, int slot) {
     const double K = gather_slot(A, sp0, slot);
@@ -440,12 +459,14 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     __shared__ DevInst I;
     __shared__ double red[32];
     __shared__ int red_r[32];
+    __shared__ int s_it;  // this instance's Newton iterations of the step so far
     const int inst = blockIdx.x;
     const int tid = threadIdx.x, nt = blockDim.x;
     {
         const uint32_t* s = reinterpret_cast<const uint32_t*>(insts + inst);
         uint32_t* d = reinterpret_cast<uint32_t*>(&I);
         for (int i = tid; i < (int)(sizeof(DevInst) / 4); i += nt) d[i] = s[i];
+        if (tid == 0) s_it = mode == INST_MODE_NEWTON ? A.iters[inst] : 0;
     }
     __syncthreads();
     if (I.large) return;  // global-memory band path (largeband_kernels.cuh)
@@ -486,6 +507,12 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     double* fac = du + n;
     const int f0 = I.f_off;
     int rc = 0;
+    // ModifiedNewton(Initial): the first iteration of the step freezes the tangent (the current
+    // one, or K_init) and factors; later iterations reuse both (transient_nonlinear.mojo:
+    // 2072-2085, 2236-2268, 2302-2335, 2421-2440)
+    const bool modified = mode == INST_MODE_NEWTON && I.algorithm != 0;
+    const bool refresh = !modified || s_it == 0;
+    double* Kfz = modified ? A.kfrz + I.band_off : nullptr;
     if (mode == INST_MODE_SOLVE_EXPORTED) {
         for (int t = tid; t < n * rw; t += nt) Kb[t] = A.export_band[I.band_off + t];
         for (int i = tid; i < n; i += nt) R[i] = A.rhs_in[f0 + i];
@@ -513,7 +540,18 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             for (int o = lane; o < rw; o += 32) {
                 const int j = i + o - bw;
                 const int slot = i * rw + o;
-                Kb[slot] = (j < 0 || j >= n) ? 0.0 : gather_slot(A, sp0, slot);
+                double K = 0.0;
+                if (j >= 0 && j < n) {
+                    if (!modified) {
+                        K = gather_slot(A, sp0, slot);
+                    } else if (refresh) {
+                        K = I.algorithm == 2 ? Kinit[slot] : gather_slot(A, sp0, slot);
+                        Kfz[slot] = K;
+                    } else {
+                        K = Kfz[slot];
+                    }
+                }
+                Kb[slot] = K;
             }
         __syncthreads();
         int bad_sym = 0;
@@ -597,14 +635,23 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             }
         }
     }
-    if (I.spd)
-        rc = band_chol_smem(Kb, n, bw, rw, fac);
-    else
-        rc = band_lu_smem(Kb, n, bw, rw, fac);
     bool dense = false;
     double* D = A.dense + I.dense_off;
     int* piv = A.piv + f0;
-    if (rc == 6) {
+    if (!refresh) {
+        // the step's factors
+        dense = A.lu_dense[inst] != 0;
+        if (!dense) {
+            const double* LU = A.lufrz + I.band_off;
+            for (int t = tid; t < n * rw; t += nt) Kb[t] = LU[t];
+        }
+        __syncthreads();
+    } else if (I.spd) {
+        rc = band_chol_smem(Kb, n, bw, rw, fac);
+    } else {
+        rc = band_lu_smem(Kb, n, bw, rw, fac);
+    }
+    if (refresh && rc == 6) {
         // BandGeneral: a row swap would be needed, so the whole effective matrix is factored
         // densely with partial pivoting (linear_solver_backend.mojo:650-657, 612-629), starting
         // again from the assembled values.
@@ -620,13 +667,23 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             const double* Kinit = A.Kinit + I.band_off;
             for (int t = tid; t < n * rw; t += nt) {
                 const int i = t / rw, j = i + t % rw - bw;
-                if (j >= 0 && j < n) D[(size_t)i * n + j] = keff_slot(I, A, I.slot_ptr_off, Kinit, i, j, t);
+                if (j >= 0 && j < n)
+                    D[(size_t)i * n + j] = modified ? keff_of(I, A, Kinit, i, j, t, Kfz[t])
+                                                    : keff_slot(I, A, I.slot_ptr_off, Kinit, i, j, t);
             }
         }
         __syncthreads();
         rc = dense_lu_global(D, piv, n, fac, red, red_r);
         dense = true;
         if (tid == 0 && A.fallbacks) A.fallbacks[inst] += 1;
+    }
+    if (modified && refresh && rc == 0) {
+        __syncthreads();
+        if (!dense) {
+            double* LU = A.lufrz + I.band_off;
+            for (int t = tid; t < n * rw; t += nt) LU[t] = Kb[t];
+        }
+        if (tid == 0) A.lu_dense[inst] = dense ? 1 : 0;
     }
     if (rc != 0) {
         if (tid == 0) {

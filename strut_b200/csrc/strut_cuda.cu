@@ -302,6 +302,7 @@ struct StrutHandle {
     int n_slaves_total = 0;          // slave dofs of every instance (multi-point constraints)
     int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
     long long band_total = 0;
+    int any_modified = 0;  // an instance runs ModifiedNewton(Initial)
     int max_nip = 1;
     size_t elem_smem = 0, inst_smem = 0;
     int max_iters_global = 1;
@@ -1038,6 +1039,10 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         I.fint_ptr_off = f_off;
         I.max_iters = d.max_iters;
         I.test_type = d.test_type;
+        if (d.algorithm < STRUT_ALGORITHM_NEWTON || d.algorithm > STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL)
+            return bail(fail(STRUT_BAD_ARG, "unknown algorithm"));
+        I.algorithm = d.algorithm;
+        if (I.algorithm != STRUT_ALGORITHM_NEWTON) h->any_modified = 1;
         I.spd = d.system == STRUT_SYSTEM_BAND_SPD;
         I.has_damping = d.alpha_m != 0.0 || d.beta_k != 0.0 || d.beta_k_init != 0.0 || d.beta_k_comm != 0.0;
         I.dt = d.dt;
@@ -1082,6 +1087,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             // band too large for shared memory: blocked factorisation in global memory
             if (I.spd)
                 return bail(fail(STRUT_UNSUPPORTED, "BandSPD bands beyond shared memory are not implemented"));
+            if (I.algorithm != STRUT_ALGORITHM_NEWTON)
+                return bail(fail(STRUT_UNSUPPORTED, "ModifiedNewton on bands beyond shared memory is not implemented"));
             const size_t fsm = large_factor_smem(bw);
             if (fsm > 220 * 1024 || bw > kLargeMaxBw)
                 return bail(fail(STRUT_UNSUPPORTED, "band width too large for the blocked factorisation"));
@@ -1235,6 +1242,10 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         (rc = dzeros(&A.piv, nF, al)) || (rc = dzeros(&A.fallbacks, (size_t)h->n_inst, al)) ||
         (rc = dzeros(&A.el.list[0], (size_t)h->n_elem, al)) || (rc = dzeros(&A.el.list[1], (size_t)h->n_elem, al)) ||
         (rc = dzeros(&A.el.count, 2, al)) || (rc = dzeros(&A.el.next, 2, al)))
+        return bail(rc);
+    if (h->any_modified &&
+        ((rc = dzeros(&A.kfrz, (size_t)h->band_total, al)) || (rc = dzeros(&A.lufrz, (size_t)h->band_total, al)) ||
+         (rc = dzeros(&A.lu_dense, (size_t)h->n_inst, al))))
         return bail(rc);
     double* d_Mff;
     double* d_Mrff;
@@ -1507,10 +1518,14 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             std::vector<int> it((size_t)st.steps_done * h->n_inst);
             CK(cudaMemcpy(it.data(), h->d_hist_iters + (size_t)first * h->n_inst, it.size() * sizeof(int),
                           cudaMemcpyDeviceToHost));
-            long long tot = 0;
-            for (int v : it) tot += v;
+            long long tot = 0, fac = 0;
+            for (size_t k = 0; k < it.size(); ++k) {
+                tot += it[k];
+                // ModifiedNewton factors once per step
+                fac += h->insts[k % h->n_inst].algorithm == STRUT_ALGORITHM_NEWTON ? it[k] : (it[k] > 0 ? 1 : 0);
+            }
             st.global_newton_iterations = tot;
-            st.factorizations = tot;
+            st.factorizations = fac;
         }
     }
     // fiber updates: per section evaluation, the section's fiber count

@@ -455,8 +455,12 @@ class Model:
         self.beta = float(integ.get("beta", 0.25))
         if self.beta <= 0.0:
             raise ModelError("Newmark beta must be > 0")
-        if an.get("algorithm", "Newton") != "Newton":
-            raise ModelError("this path implements the Newton algorithm")
+        amap = {"Newton": A.ALGORITHM_NEWTON, "ModifiedNewton": A.ALGORITHM_MODIFIED_NEWTON,
+                "ModifiedNewtonInitial": A.ALGORITHM_MODIFIED_NEWTON_INITIAL}
+        alg = an.get("algorithm", "Newton")
+        if alg not in amap:
+            raise ModelError(f"this path implements Newton, ModifiedNewton and ModifiedNewtonInitial, not {alg}")
+        self.algorithm = amap[alg]
         tmap = {
             "MaxDispIncr": A.TEST_MAX_DISP_INCR,
             "NormDispIncr": A.TEST_NORM_DISP_INCR,
@@ -682,6 +686,7 @@ class Model:
         d.dt, d.gamma, d.beta = self.dt, self.gamma, self.beta
         d.tol, d.max_iters = self.tol, self.max_iters
         d.test_type, d.system = self.test_type, self.system
+        d.algorithm = self.algorithm
         d.num_excitations = len(self.excitations)
         for i, x in enumerate(self.excitations):
             ex = d.excitation[i]
