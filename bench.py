@@ -66,6 +66,8 @@ def parse():
                     help="timed steps of the 4000-step large 3D frame record")
     ap.add_argument("--profile-only", action="store_true",
                     help="one short analysis (for a profiler launch list); prints no bench line")
+    ap.add_argument("--profile-tall", action="store_true",
+                    help="with --profile-only: --tall-steps steps of the 20-story 3D frame instead")
     return ap.parse_args()
 
 
@@ -332,6 +334,23 @@ def main():
         B.build()
     if world > 1:
         torch.distributed.barrier()
+
+    if args.profile_only and args.profile_tall:
+        from strut_b200 import model as Mo
+        from strut_b200 import workloads as W
+
+        m = Mo.Model(W.tall_frame3d_case(steps=args.tall_steps))
+        with runtime.Analysis([m], device=device) as an:
+            runtime.lib().strut_gpu_set_profiling(an.h, 1)
+            an.run(args.tall_steps, check=False)
+            P = A.StrutKernelProfile()
+            runtime.lib().strut_gpu_get_profile(an.h, __import__("ctypes").byref(P))
+        if rank == 0:
+            names = ("element", "instance", "commit", "predictor", "post")
+            print(json.dumps({"profile": {n: {"launches": int(P.launches[i]), "ms": P.ms[i]}
+                                          for i, n in enumerate(names)},
+                              "workload": "tall_3d_rc_frame_20s_6x6b_diaphragm", "steps": args.tall_steps}))
+        return 0
 
     models, cases = build_models(args.frames, args.record_steps, 1000 + rank * args.frames)
     n_fibers = sum(m.num_fibers_total for m in models)
