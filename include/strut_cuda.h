@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define STRUT_ABI_VERSION 3
+#define STRUT_ABI_VERSION 4
 #define STRUT_MAX_INT_PTS 10
 
 /* Status codes.  No entry point aborts the process. */
@@ -160,6 +160,17 @@ typedef struct StrutExcitation {
     int32_t reserved;
 } StrutExcitation;
 
+/* ShellMITC4 on an ElasticMembranePlateSection (elements/shell4.mojo:10-363): a linear
+ * four-node shell whose 24 x 24 global stiffness is computed once from the node coordinates,
+ * E, nu and the thickness h; its internal force is that stiffness times the element
+ * displacements.  Requires ndm 3, ndf 6.  Its section's rho enters the lumped translational
+ * masses through StrutModelDesc.mass (loader.mojo:2060-2100), not here. */
+typedef struct StrutShellElement {
+    int32_t nodes[4];      /* node indices, counter-clockwise                         */
+    int32_t dof[24];       /* global dof indices node*6 + (d-1), nodes in order       */
+    double E, nu, h;
+} StrutShellElement;
+
 /* One analysis instance (one frame + one record). */
 typedef struct StrutModelDesc {
     int32_t ndm;                 /* 2 (ndf 3) or 3 (ndf 6)                               */
@@ -208,6 +219,11 @@ typedef struct StrutModelDesc {
     const int32_t* slave_ptr;      /* num_slaves + 1 offsets into the term arrays          */
     const int32_t* slave_master;   /* retained full dof of each term                       */
     const double* slave_coef;      /* coefficient of each term                             */
+    /* linear shells, assembled after the frame elements as Strut's assembly groups them
+     * (stiffness_internal.mojo: frames, then surfaces) */
+    int32_t num_shells;
+    int32_t reserved_shell;
+    const StrutShellElement* shells;
 } StrutModelDesc;
 
 /* Per-run statistics (RuntimeProfileMetrics counters, solver/profile.mojo:37-74). */

@@ -80,6 +80,22 @@ def section_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
     return out
 
 
+def shell4_stiffness(E: float, nu: float, h: float, xyz) -> np.ndarray:
+    """24 x 24 global stiffness of a ShellMITC4 on an ElasticMembranePlateSection; xyz (4, 3)."""
+    L = lib()
+    P = np.ascontiguousarray(xyz, dtype=np.float64).reshape(4, 3)
+    x, y, z = (np.ascontiguousarray(P[:, k]) for k in range(3))
+    K = np.zeros(576)
+    dp = C.POINTER(C.c_double)
+    fn = L.oracle_shell4_stiffness
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp, dp, dp]
+    rc = fn(E, nu, h, x.ctypes.data_as(dp), y.ctypes.data_as(dp), z.ctypes.data_as(dp), K.ctypes.data_as(dp))
+    if rc != 0:
+        raise RuntimeError("oracle_shell4_stiffness failed")
+    return K.reshape(24, 24)
+
+
 def section3d_path(mats, nmat, fibs, nfib, path) -> np.ndarray:
     """path: (npts, 3) of (eps0, kappa_y, kappa_z) -> (npts, 9) of N, My, Mz, k11, k12, k13,
     k22, k23, k33."""

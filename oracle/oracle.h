@@ -53,6 +53,8 @@ int oracle_section_batch_path(const StrutUniMaterial* mats, int nmat, const Stru
                               double* out);
 /* One FiberSection3d along npts (eps0, kappa_y, kappa_z) points (path: npts x 3), committing
  * after each; out: npts x 9 = N, My, Mz, k11, k12, k13, k22, k23, k33. */
+int oracle_shell4_stiffness(double E, double nu, double h, const double* x, const double* y, const double* z,
+                            double* K);
 int oracle_section3d_path(const StrutUniMaterial* mats, int nmat, const StrutFiber* fibers,
                           int nfib, const double* path, int npts, double* out);
 /* Single-instance transient run (the reference's plain CPU path).  eforce_hist holds

@@ -58,6 +58,9 @@ typedef struct OModel {
     int* kcol;
     double* kval;
     int* epos;         /* num_elements x nd x nd */
+    int* epos_sh;      /* num_shells x 24 x 24 */
+    double* shell_k;   /* num_shells x 576, constant */
+    int* efree_sh;     /* num_shells x 24 */
     double* Fred;
 } OModel;
 
@@ -109,6 +112,7 @@ static void model_free(OModel* m) {
     free(m->at); free(m->vt); free(m->work);
     free(m->mrow_ptr); free(m->mrow_dof); free(m->mrow_coef); free(m->kptr); free(m->kcol);
     free(m->kval); free(m->epos); free(m->Fred);
+    free(m->epos_sh); free(m->shell_k); free(m->efree_sh);
     memset(m, 0, sizeof(*m));
 }
 
@@ -166,6 +170,8 @@ static int mpc_build(OModel* m) {
     int* cnt = (int*)calloc(nd, sizeof(int));
     for (int e = 0; e < d->num_elements; ++e)
         for (int a = 0; a < ned; ++a) cnt[d->elements[e].dof[a]] += ned;
+    for (int s = 0; s < d->num_shells; ++s)
+        for (int a = 0; a < 24; ++a) cnt[d->shells[s].dof[a]] += 24;
     m->kptr = (int*)calloc(nd + 1, sizeof(int));
     for (int i = 0; i < nd; ++i) m->kptr[i + 1] = m->kptr[i] + cnt[i];
     int* tmp = (int*)malloc(sizeof(int) * (m->kptr[nd] + 1));
@@ -174,6 +180,11 @@ static int mpc_build(OModel* m) {
         for (int a = 0; a < ned; ++a) {
             int r = d->elements[e].dof[a];
             for (int b = 0; b < ned; ++b) tmp[m->kptr[r] + cnt[r]++] = d->elements[e].dof[b];
+        }
+    for (int s = 0; s < d->num_shells; ++s)
+        for (int a = 0; a < 24; ++a) {
+            int r = d->shells[s].dof[a];
+            for (int b = 0; b < 24; ++b) tmp[m->kptr[r] + cnt[r]++] = d->shells[s].dof[b];
         }
     /* sort and unique each row */
     int nnz = 0;
@@ -214,6 +225,25 @@ static int mpc_build(OModel* m) {
                     else hi = mid - 1;
                 }
                 m->epos[((size_t)e * ned + a) * ned + b] = pos;
+            }
+        }
+    m->epos_sh = (int*)malloc(sizeof(int) * ((size_t)d->num_shells * 576 + 1));
+    for (int s = 0; s < d->num_shells; ++s)
+        for (int a = 0; a < 24; ++a) {
+            int r = d->shells[s].dof[a];
+            for (int b = 0; b < 24; ++b) {
+                int c = d->shells[s].dof[b];
+                int lo = m->kptr[r], hi = m->kptr[r + 1] - 1, pos = -1;
+                while (lo <= hi) {
+                    int mid = (lo + hi) / 2;
+                    if (m->kcol[mid] == c) {
+                        pos = mid;
+                        break;
+                    }
+                    if (m->kcol[mid] < c) lo = mid + 1;
+                    else hi = mid - 1;
+                }
+                m->epos_sh[((size_t)s * 24 + a) * 24 + b] = pos;
             }
         }
     m->Fred = (double*)calloc(nd, sizeof(double));
@@ -333,6 +363,37 @@ static int model_build(OModel* m, const StrutModelDesc* d) {
             if (ia < 0) continue;
             for (int b = a + 1; b < ned; ++b) {
                 int ib = m->efree[ned * e + b];
+                if (ib < 0) continue;
+                int diff = ia > ib ? ia - ib : ib - ia;
+                if (diff > bw) bw = diff;
+            }
+        }
+    }
+    /* linear shells (shell4.mojo:10-363): constant stiffness, their free-dof pairs in the band */
+    if (d->num_shells > 0 && (d->ndm != 3 || d->ndf != 6 || !d->shells)) return STRUT_BAD_ARG;
+    m->shell_k = (double*)malloc(sizeof(double) * ((size_t)d->num_shells * 576 + 1));
+    m->efree_sh = (int*)malloc(sizeof(int) * ((size_t)d->num_shells * 24 + 1));
+    for (int s = 0; s < d->num_shells; ++s) {
+        const StrutShellElement* sh = &d->shells[s];
+        double xs[4], ys[4], zs[4];
+        for (int k = 0; k < 4; ++k) {
+            if (sh->nodes[k] < 0 || sh->nodes[k] >= d->num_nodes) return STRUT_BAD_ARG;
+            xs[k] = d->node_coords[3 * sh->nodes[k]];
+            ys[k] = d->node_coords[3 * sh->nodes[k] + 1];
+            zs[k] = d->node_coords[3 * sh->nodes[k] + 2];
+        }
+        if (oracle_shell4_stiffness(sh->E, sh->nu, sh->h, xs, ys, zs, m->shell_k + (size_t)576 * s) != STRUT_OK)
+            return STRUT_BAD_ARG;
+        for (int a = 0; a < 24; ++a) {
+            int dof = sh->dof[a];
+            if (dof < 0 || dof >= d->num_dofs) return STRUT_BAD_ARG;
+            m->efree_sh[24 * s + a] = d->free_index[dof];
+        }
+        for (int a = 0; a < 24; ++a) {
+            int ia = m->efree_sh[24 * s + a];
+            if (ia < 0) continue;
+            for (int b = a + 1; b < 24; ++b) {
+                int ib = m->efree_sh[24 * s + b];
                 if (ib < 0) continue;
                 int diff = ia > ib ? ia - ib : ib - ia;
                 if (diff > bw) bw = diff;
@@ -461,6 +522,16 @@ static int assemble(OModel* m, double* ek_out, double* ef_out) {
                 m->Fint[el->desc->dof[a]] += f[a];
             }
         }
+        for (int s = 0; s < d->num_shells; ++s) {
+            const double* k = m->shell_k + (size_t)576 * s;
+            double ue[24];
+            for (int b = 0; b < 24; ++b) ue[b] = m->u[d->shells[s].dof[b]];
+            const int* pos = m->epos_sh + (size_t)s * 576;
+            for (int a = 0; a < 24; ++a) {
+                for (int b = 0; b < 24; ++b) m->kval[pos[a * 24 + b]] += k[a * 24 + b];
+                m->Fint[d->shells[s].dof[a]] += oracle_simd_dot(k + 24 * a, ue, 24);
+            }
+        }
         mpc_collapse_K(m);
         return STRUT_OK;
     }
@@ -483,6 +554,25 @@ static int assemble(OModel* m, double* ek_out, double* ef_out) {
                 }
             }
             m->Fint[el->desc->dof[a]] += f[a];
+        }
+    }
+    /* shells after the frames (stiffness_internal_surface.mojo:240-280): K rows scattered,
+     * F_int the row dot the element displacements */
+    for (int s = 0; s < d->num_shells; ++s) {
+        const double* k = m->shell_k + (size_t)576 * s;
+        double ue[24];
+        for (int b = 0; b < 24; ++b) ue[b] = m->u[d->shells[s].dof[b]];
+        for (int a = 0; a < 24; ++a) {
+            int ia = m->efree_sh[24 * s + a];
+            if (ia >= 0) {
+                for (int b = 0; b < 24; ++b) {
+                    int ib = m->efree_sh[24 * s + b];
+                    if (ib < 0) continue;
+                    int sl = gslot(m, ia, ib);
+                    if (sl >= 0) m->K[sl] += k[a * 24 + b];
+                }
+            }
+            m->Fint[d->shells[s].dof[a]] += oracle_simd_dot(k + 24 * a, ue, 24);
         }
     }
     return STRUT_OK;

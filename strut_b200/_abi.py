@@ -109,6 +109,16 @@ class StrutFrameElement(C.Structure):
     ]
 
 
+class StrutShellElement(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_int32 * 4),
+        ("dof", C.c_int32 * 24),
+        ("E", C.c_double),
+        ("nu", C.c_double),
+        ("h", C.c_double),
+    ]
+
+
 class StrutExcitation(C.Structure):
     _fields_ = [
         ("direction", C.c_int32),
@@ -167,6 +177,9 @@ class StrutModelDesc(C.Structure):
         ("slave_ptr", _ip),
         ("slave_master", _ip),
         ("slave_coef", _dp),
+        ("num_shells", C.c_int32),
+        ("reserved_shell", C.c_int32),
+        ("shells", C.POINTER(StrutShellElement)),
     ]
 
 

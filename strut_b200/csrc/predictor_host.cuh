@@ -116,6 +116,7 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
         return fail(STRUT_UNSUPPORTED, "the learned predictor runs on instances whose band fits in shared memory");
     if (h->n_slaves_total > 0)
         return fail(STRUT_UNSUPPORTED, "the learned predictor does not run with multi-point constraints");
+    if (h->n_shells > 0) return fail(STRUT_UNSUPPORTED, "the learned predictor does not run with shells");
     for (const DevInst& I : h->insts)
         if (I.algorithm != STRUT_ALGORITHM_NEWTON)
             return fail(STRUT_UNSUPPORTED, "the learned predictor runs with the Newton algorithm");

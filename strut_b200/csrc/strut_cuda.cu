@@ -27,6 +27,7 @@
 #include "kat_kernels.cuh"
 #include "solver_kernels.cuh"
 #include "largeband_kernels.cuh"
+#include "shell_kernels.cuh"
 #include "predictor_kernels.cuh"
 
 using namespace strut;
@@ -287,6 +288,9 @@ struct StrutHandle {
     int* d_rec3 = nullptr;           // recorded 3D elements (record pass after commit)
     int n_rec3 = 0;
     long long ek_total = 0, ef_total = 0;
+    std::vector<DevShell> shells_h;  // linear shells of all instances
+    DevShell* d_shells = nullptr;
+    int n_shells = 0;
     // instances whose band is factored in global memory
     int n_large = 0, large_rows = 0, max_large_n = 0, lfactor_grid = 1;
     long long lband_total = 0;
@@ -437,6 +441,11 @@ static int launch_elements(StrutHandle* h, int all_elems = 0) {
         h->A.status, h->d_elem_err, h->d_counters, h->A.el, (const DevCtl*)h->d_ctl,
         all_elems ? (int)ELEM_MODE_ALL : (int)ELEM_MODE_LIST, h->n_elem, rec_pass_of(h));
     CK(cudaGetLastError());
+    if (h->n_shells > 0) {
+        shell_force_kernel<<<(h->n_shells * 32 + 255) / 256, 256, 0, h->stream>>>(h->d_shells, h->n_shells, h->d_ek,
+                                                                                h->d_ef, h->A.u_full);
+        CK(cudaGetLastError());
+    }
     TRY(prof_end(h, 0));
     if (h->prof) {
         unsigned long long mx = 0;
@@ -613,7 +622,15 @@ static int build_graph(StrutHandle* h) {
                         h->fs, (const double*)h->A.u_full, h->d_estate, h->d_ek, h->d_ef,
                         (const int*)h->A.active, h->A.status, h->d_elem_err, h->d_counters, h->A.el,
                         (const DevCtl*)h->d_ctl, (int)ELEM_MODE_LIST, h->n_elem, rec_pass_of(h)));
-    TRY(add_kernel_node(&n_in, ibody, &n_el, 1, instance_newton_kernel, dim3(h->n_inst), dim3(256),
+    cudaGraphNode_t n_after_el = n_el;
+    if (h->n_shells > 0) {
+        cudaGraphNode_t n_sh;
+        TRY(add_kernel_node(&n_sh, ibody, &n_el, 1, shell_force_kernel, dim3((h->n_shells * 32 + 255) / 256),
+                            dim3(256), 0, (const DevShell*)h->d_shells, h->n_shells, (const double*)h->d_ek, h->d_ef,
+                            (const double*)h->A.u_full));
+        n_after_el = n_sh;
+    }
+    TRY(add_kernel_node(&n_in, ibody, &n_after_el, 1, instance_newton_kernel, dim3(h->n_inst), dim3(256),
                         h->inst_smem, (const DevInst*)h->d_insts, A, (int)INST_MODE_NEWTON, 0));
     cudaGraphNode_t n_before_chk = n_in;
     TRY(add_kernel_node(&n_chk, ibody, &n_before_chk, 1, newton_check_kernel, dim3(1), dim3(32), 0, h->d_ctl,
@@ -955,6 +972,47 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
                 }
             }
         }
+        // linear shells (elements/shell4.mojo:10-363): constant 24 x 24 stiffness after the frame
+        // elements' entries, their free-dof pairs in the band
+        const int sh0 = (int)h->shells_h.size();
+        std::vector<int> sfree((size_t)24 * d.num_shells);
+        if (d.num_shells > 0 && (d.ndm != 3 || d.ndf != 6 || !d.shells))
+            return bail(fail(STRUT_BAD_ARG, "shells need ndm 3, ndf 6 and a shell array"));
+        for (int s = 0; s < d.num_shells; ++s) {
+            const StrutShellElement& se = d.shells[s];
+            DevShell S;
+            std::memset(&S, 0, sizeof(S));
+            for (int k = 0; k < 4; ++k) {
+                if (se.nodes[k] < 0 || se.nodes[k] >= d.num_nodes) return bail(fail(STRUT_BAD_ARG, "shell node out of range"));
+                S.x[k] = d.node_coords[3 * se.nodes[k]];
+                S.y[k] = d.node_coords[3 * se.nodes[k] + 1];
+                S.z[k] = d.node_coords[3 * se.nodes[k] + 2];
+            }
+            if (!(se.E > 0.0 && se.h > 0.0 && se.nu > -1.0 && se.nu < 0.5))
+                return bail(fail(STRUT_BAD_ARG, "shell section needs E > 0, h > 0, -1 < nu < 0.5"));
+            S.E = se.E;
+            S.nu = se.nu;
+            S.h = se.h;
+            for (int a = 0; a < 24; ++a) {
+                const int dof = se.dof[a];
+                if (dof < 0 || dof >= d.num_dofs) return bail(fail(STRUT_BAD_ARG, "shell dof out of range"));
+                S.dof[a] = u_off + dof;
+                sfree[(size_t)24 * s + a] = d.free_index[dof];
+            }
+            S.ek_off = h->ek_total;
+            S.ef_off = h->ef_total;
+            h->ek_total += 576;
+            h->ef_total += 24;
+            h->shells_h.push_back(S);
+            for (int a = 0; a < 24; ++a) {
+                const int ia = sfree[(size_t)24 * s + a];
+                if (ia < 0) continue;
+                for (int b = a + 1; b < 24; ++b) {
+                    const int ib = sfree[(size_t)24 * s + b];
+                    if (ib >= 0) bw = std::max(bw, std::abs(ia - ib));
+                }
+            }
+        }
         const int rw = 2 * bw + 1;
         // band slot contributions, element order (stiffness_internal_frame2d.mojo:594-619)
         std::vector<std::vector<int>> slots((size_t)nf * rw);
@@ -981,6 +1039,22 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
                     if (any_mpc) fc[ia].push_back(1.0);
                 }
             }
+            for (int s = 0; s < d.num_shells; ++s) {
+                const DevShell& S = h->shells_h[sh0 + s];
+                for (int a = 0; a < 24; ++a) {
+                    const int ia = sfree[(size_t)24 * s + a];
+                    if (ia < 0) continue;
+                    for (int b = 0; b < 24; ++b) {
+                        const int ib = sfree[(size_t)24 * s + b];
+                        if (ib < 0) continue;
+                        const size_t sl = (size_t)ia * rw + (ib - ia + bw);
+                        slots[sl].push_back((int)(S.ek_off + a * 24 + b));
+                        if (any_mpc) slotc[sl].push_back(1.0);
+                    }
+                    fcontr[ia].push_back((int)(S.ef_off + a));
+                    if (any_mpc) fc[ia].push_back(1.0);
+                }
+            }
         } else {
             // collapse c_i k c_j onto the retained free dofs; entries outside the half width
             // detected from the elements' free dofs are dropped, as Strut's band load drops
@@ -1004,6 +1078,28 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
                     for (auto& ta : ra) {
                         if (ta.first < 0 || ta.second == 0.0) continue;
                         fcontr[ta.first].push_back((int)(E.ef_off + a));
+                        fc[ta.first].push_back(ta.second);
+                    }
+                }
+            }
+            for (int s = 0; s < d.num_shells; ++s) {
+                const DevShell& S = h->shells_h[sh0 + s];
+                for (int a = 0; a < 24; ++a) {
+                    rows_of(d.shells[s].dof[a], ra);
+                    for (int b = 0; b < 24; ++b) {
+                        rows_of(d.shells[s].dof[b], rb);
+                        for (auto& ta : ra)
+                            for (auto& tb : rb) {
+                                if (ta.first < 0 || tb.first < 0 || std::abs(ta.first - tb.first) > bw) continue;
+                                if (ta.second == 0.0 || tb.second == 0.0) continue;
+                                const size_t sl = (size_t)ta.first * rw + (tb.first - ta.first + bw);
+                                slots[sl].push_back((int)(S.ek_off + a * 24 + b));
+                                slotc[sl].push_back(ta.second * tb.second);
+                            }
+                    }
+                    for (auto& ta : ra) {
+                        if (ta.first < 0 || ta.second == 0.0) continue;
+                        fcontr[ta.first].push_back((int)(S.ef_off + a));
                         fc[ta.first].push_back(ta.second);
                     }
                 }
@@ -1333,6 +1429,18 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     {
         std::vector<int> ones(h->n_inst, 1);
         CK(cudaMemcpy(A.active, ones.data(), sizeof(int) * h->n_inst, cudaMemcpyHostToDevice));
+        if (!h->shells_h.empty()) {
+            h->n_shells = (int)h->shells_h.size();
+            int* d_err = nullptr;
+            if ((rc = upload(&h->d_shells, h->shells_h, al)) || (rc = dzeros(&d_err, 1, al))) return bail(rc);
+            shell_stiffness_kernel<<<(h->n_shells + 63) / 64, 64, 0, h->stream>>>(h->d_shells, h->n_shells, h->d_ek,
+                                                                                d_err);
+            CK(cudaGetLastError());
+            int herr = 0;
+            CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            if (herr) return bail(fail(STRUT_BAD_ARG, "shell with a singular Jacobian"));
+        }
         if ((rc = launch_elements(h, 1)) != STRUT_OK) return bail(rc);
         // Kinit = K gathered in element order; the export path of the instance kernel with
         // a0 = a1 = 0 and no damping would equal K, but a dedicated gather keeps it exact.

@@ -322,7 +322,15 @@ class Model:
         fibers = []
         sections = []
         want = "FiberSection2d" if self.ndm == 2 else "FiberSection3d"
+        self.plate_sections = {}
         for s in case.get("sections", []):
+            if s["type"] == "ElasticMembranePlateSection" and self.ndm == 3:
+                prm = s.get("params", {})
+                E, nu, h = float(prm.get("E", 0.0)), float(prm.get("nu", 0.0)), float(prm.get("h", 0.0))
+                if not (E > 0.0 and h > 0.0 and -1.0 < nu < 0.5):
+                    raise ModelError("ElasticMembranePlateSection needs E > 0, h > 0, -1 < nu < 0.5")
+                self.plate_sections[int(s["id"])] = (E, nu, h, float(prm.get("rho", 0.0)))
+                continue
             if s["type"] != want:
                 raise ModelError(f"unsupported section type for this path: {s['type']}")
             cells = discretize_section(s.get("params", {}))
@@ -352,8 +360,27 @@ class Model:
         rule_structs = []
         elems = []
         self.elem_ids = []
+        shells = []
+        self.shell_ids = []
         for e in case.get("elements", []):
             et = e["type"]
+            if et == "shell" and self.ndm == 3:
+                # ShellMITC4 on an ElasticMembranePlateSection (elements/shell4.mojo:10-363)
+                sid = int(e["section"])
+                if sid not in self.plate_sections:
+                    raise ModelError("shell requires an ElasticMembranePlateSection")
+                nodes4 = [self.node_index[int(x)] for x in e["nodes"]]
+                if len(nodes4) != 4:
+                    raise ModelError("shell requires 4 nodes")
+                sh = A.StrutShellElement()
+                for k, ni in enumerate(nodes4):
+                    sh.nodes[k] = ni
+                    for a in range(6):
+                        sh.dof[6 * k + a] = ni * 6 + a
+                sh.E, sh.nu, sh.h = self.plate_sections[sid][:3]
+                shells.append(sh)
+                self.shell_ids.append(int(e["id"]))
+                continue
             tags = {"forceBeamColumn2d": (A.ELEM_FORCE_BEAM_COLUMN_2D, 2),
                     "dispBeamColumn2d": (A.ELEM_DISP_BEAM_COLUMN_2D, 2),
                     "forceBeamColumn3d": (A.ELEM_FORCE_BEAM_COLUMN_3D, 3),
@@ -405,6 +432,8 @@ class Model:
             self.elem_ids.append(int(e["id"]))
             elems.append(el)
         self.elements = elems
+        self.shells = shells
+        self._shell_sections = [int(e["section"]) for e in case.get("elements", []) if e["type"] == "shell"]
         self.integrations = rule_structs
         self.elem_index = {eid: i for i, eid in enumerate(self.elem_ids)}
 
@@ -429,6 +458,22 @@ class Model:
             if d < 1 or d > self.ndf:
                 raise ModelError("mass dof out of range")
             self.mass[self.node_index[int(m["node"])] * self.ndf + d - 1] += float(m["value"])
+        # shell mass: rho h area / 4 on each node's translations (loader.mojo:2060-2100)
+        for sh, sid in zip(self.shells, self._shell_sections):
+            rho = self.plate_sections[sid][3]
+            if rho == 0.0:
+                continue
+            P = [self.coords[3 * sh.nodes[k]: 3 * sh.nodes[k] + 3] for k in range(4)]
+            a = (P[1] - P[0]) + (P[2] - P[3])
+            b = (P[3] - P[0]) + (P[2] - P[1])
+            cr = np.cross(a, b)
+            area = 0.25 * float(np.sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]))
+            if area <= 0.0:
+                raise ModelError("shell area must be > 0")
+            lumped = rho * self.plate_sections[sid][2] * area / 4.0
+            for d in range(3):
+                for k in range(4):
+                    self.mass[sh.nodes[k] * 6 + d] += lumped
         self.mass_rayleigh = self.mass.copy()
         self.f_const = np.zeros(self.num_dofs)
         for ld in case.get("loads", []) or []:
@@ -711,6 +756,11 @@ class Model:
         d.slave_ptr = iptr(np.asarray(ptr, dtype=np.int32))
         d.slave_master = iptr(np.asarray(mdof, dtype=np.int32))
         d.slave_coef = dptr(np.asarray(coef, dtype=np.float64))
+        d.num_shells = len(self.shells)
+        if self.shells:
+            sh = _struct_array(A.StrutShellElement, self.shells)
+            keep.append(sh)
+            d.shells = C.cast(sh, C.POINTER(A.StrutShellElement))
         self._keep = keep
         return d
 

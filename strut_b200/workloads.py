@@ -344,10 +344,14 @@ def initial_stiffness_3d(case: dict) -> tuple[np.ndarray, np.ndarray, np.ndarray
             fixed[6 * i + d - 1] = True
     free = np.where(~fixed)[0]
     mats = {m["id"]: m for m in case["materials"]}
-    flex = {s["id"]: _section3d_initial_flex(s, mats) for s in case["sections"]}
-    gj = {s["id"]: s["params"]["G"] * s["params"]["J"] for s in case["sections"]}
+    # the frame alone: slab shells (if any) do not enter the Rayleigh coefficients
+    fsecs = [s for s in case["sections"] if s["type"] == "FiberSection3d"]
+    flex = {s["id"]: _section3d_initial_flex(s, mats) for s in fsecs}
+    gj = {s["id"]: s["params"]["G"] * s["params"]["J"] for s in fsecs}
     K = np.zeros((ndof, ndof))
     for e in case["elements"]:
+        if e["type"] == "shell":
+            continue
         ni, nj = idx[e["nodes"][0]], idx[e["nodes"][1]]
         p1 = [nodes[ni][k] for k in ("x", "y", "z")]
         p2 = [nodes[nj][k] for k in ("x", "y", "z")]
@@ -411,7 +415,7 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
                     system: str = "BandGeneral", zeta: float = 0.05, geom: str = "Linear",
                     bidirectional: bool = False, record_elements=(1,), diaphragm: bool = False,
                     beam_element: str | None = None, sections=None,
-                    diaphragm_mass: float | None = None) -> dict:
+                    diaphragm_mass: float | None = None, slabs: dict | None = None) -> dict:
     """3D RC frame: columns along z, beams along x and y, base fixed in all six dofs.  With
     ``diaphragm`` every floor is a rigid diaphragm (perp_dirn 3) retained by its central node,
     which carries the floor's horizontal masses and rotational inertia; the other nodes keep
@@ -451,6 +455,16 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
         for j in range(bays_y):
             for i in range(bays_x + 1):
                 add(grid[(k, j, i)], grid[(k, j + 1, i)], 2, bt)
+    if slabs:
+        # one ShellMITC4 per bay and floor on the beam-column joints (counter-clockwise seen
+        # from +z), ElasticMembranePlateSection {E, nu, h, rho}
+        for k in range(1, stories + 1):
+            for j in range(bays_y):
+                for i in range(bays_x):
+                    elements.append({"id": eid, "type": "shell", "section": 3,
+                                     "nodes": [grid[(k, j, i)], grid[(k, j, i + 1)],
+                                               grid[(k, j + 1, i + 1)], grid[(k, j + 1, i)]]})
+                    eid += 1
     masses = []
     mpcs = []
     jm, im = bays_y // 2, bays_x // 2
@@ -506,7 +520,7 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
             {"id": 3, "type": "Steel02", "params": dict(STEEL)},
         ],
         "sections": list(sections) if sections else [rc_section(1, 0.5, 0.5, three_d=True),
-                                                      rc_section(2, 0.4, 0.6, three_d=True)],
+                                                      rc_section(2, 0.4, 0.6, three_d=True)] + ([{"id": 3, "type": "ElasticMembranePlateSection", "params": dict(slabs)}] if slabs else []),
         "elements": elements,
         "masses": masses,
         "time_series": series,

@@ -29,7 +29,7 @@ def test_library_exports_every_header_symbol(gpu_lib):
 
 def test_abi_version_and_error_text_without_gpu(gpu_lib):
     lib = gpu_lib.lib()
-    assert lib.strut_gpu_abi_version() == 3
+    assert lib.strut_gpu_abi_version() == 4
     assert isinstance(lib.strut_gpu_last_error(), bytes)
 
 
