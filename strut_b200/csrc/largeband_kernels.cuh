@@ -589,8 +589,10 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
         __syncthreads();
         if (wid == 0) {
             double v = lane < rb ? tb[lane] : 0.0;
+            // the block's reciprocal pivots at once, off the sequential chain
+            const double rdiag = lane < rb ? 1.0 / Ud[lane * 33 + lane] : 0.0;
             for (int s = rb - 1; s >= 0; --s) {
-                if (lane == s) v = v / Ud[s * 33 + s];
+                if (lane == s) v = v * rdiag;
                 const double x = __shfl_sync(0xffffffffu, v, s);
                 if (lane < s) v = fma(-Ud[lane * 33 + s], x, v);
             }
