@@ -66,3 +66,17 @@ def test_modified_newton_on_a_wide_band_is_unsupported(gpu_lib):
     with pytest.raises(gpu_lib.StrutError) as ei:
         gpu_lib.Analysis([M.Model(case)])
     assert ei.value.code == A.STRUT_UNSUPPORTED
+
+
+@pytest.mark.parametrize("algorithm", ["ModifiedNewton", "ModifiedNewtonInitial"])
+def test_variant_on_3d_diaphragm_frame_with_slabs(gpu_lib, oracle, algorithm):
+    """The variants through the 3D element kernel, the multi-point-constraint collapse and the
+    slab shells' constant stiffness at once."""
+    steps = 60
+    case = W.rc_frame3d_case(stories=2, bays_x=2, bays_y=2, steps=steps, element="forceBeamColumn3d",
+                             beam_element="dispBeamColumn3d", seed=71, pga_g=0.3, bidirectional=True,
+                             diaphragm=True, record_elements=(1,), max_iters=40,
+                             slabs={"E": 30.0e9, "nu": 0.2, "h": 0.2, "rho": 0.0})
+    case["analysis"]["algorithm"] = algorithm
+    st, _ = _parity(gpu_lib, oracle, [case], steps)
+    assert st.factorizations == steps
