@@ -38,6 +38,8 @@ def lib():
             build()
         L = C.CDLL(str(LIB_PATH))
         L.oracle_set_simd_width.argtypes = [C.c_int]
+        L.oracle_subdivisions.restype = C.c_long
+        L.oracle_dense_fallbacks.restype = C.c_long
         L.oracle_get_simd_width.restype = C.c_int
         L.oracle_material_path.argtypes = [C.POINTER(A.StrutUniMaterial), _dp, C.c_int, _dp]
         L.oracle_section_path.argtypes = [C.POINTER(A.StrutUniMaterial), C.c_int,
@@ -51,13 +53,18 @@ def lib():
         L.oracle_run_transient.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _ip, _ip]
         L.oracle_state_determination.argtypes = [C.POINTER(A.StrutModelDesc), _dp, _dp, _dp, _ip]
         L.oracle_run_transient_batch.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, C.c_int,
-                                                 C.c_int, _ip, _ip]
+                                                 C.c_int, _ip, _ip, _ip, _ip]
         _lib = L
     return _lib
 
 
 def _d(a):
     return a.ctypes.data_as(_dp)
+
+
+def subdivisions() -> int:
+    """forceBeamColumn2d subdivision passes in which every scheme failed, since load."""
+    return int(lib().oracle_subdivisions())
 
 
 def set_simd_width(w: int):
@@ -160,14 +167,20 @@ def element_state(model, elem: int, u_elem):
     return k, f
 
 
-def run_batch(models, steps: int, nthreads: int):
+def run_batch(models, steps: int, nthreads: int, detail: bool = False):
     """Runs every model for `steps` steps over `nthreads` host threads.  Returns
-    (first failure status or 0, total Newton iterations, per-record status array)."""
+    (first failure status or 0, total Newton iterations, per-record status array), plus, with
+    detail, the per-record failing step (-1: none) and Newton iteration arrays."""
     descs = (A.StrutModelDesc * len(models))()
     for i, m in enumerate(models):
         descs[i] = m.desc()
     tot = C.c_int(0)
     st = np.zeros(len(models), dtype=np.int32)
+    fs = np.zeros(len(models), dtype=np.int32)
+    it = np.zeros(len(models), dtype=np.int32)
     rc = lib().oracle_run_transient_batch(descs, len(models), steps, nthreads, C.byref(tot),
-                                          st.ctypes.data_as(_ip))
+                                          st.ctypes.data_as(_ip), fs.ctypes.data_as(_ip),
+                                          it.ctypes.data_as(_ip))
+    if detail:
+        return rc, tot.value, st, fs, it
     return rc, tot.value, st

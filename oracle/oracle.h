@@ -70,10 +70,14 @@ int oracle_element_state(const StrutModelDesc* m, int elem, const double* u_elem
                          double* f);
 /* Number of BandGeneral factorisations that fell back to dense partial-pivot LU. */
 long oracle_dense_fallbacks(void);
-/* Multi-instance run over nthreads host threads (CPU baseline leg).  record_status (optional,
- * n entries) receives each record's status; the return value is the first failure seen. */
+/* Number of forceBeamColumn2d subdivision passes in which every scheme failed. */
+long oracle_subdivisions(void);
+/* Multi-instance run over nthreads host threads (CPU baseline leg, batch parity).  Optional
+ * n-entry outputs: record_status (each record's status), record_failed_step (its failing step
+ * or -1) and record_iters (its Newton iterations); the return value is the first failure seen. */
 int oracle_run_transient_batch(const StrutModelDesc* models, int n, int steps, int nthreads,
-                               int* total_iters, int* record_status);
+                               int* total_iters, int* record_status, int* record_failed_step,
+                               int* record_iters);
 
 #ifdef __cplusplus
 }

@@ -1143,6 +1143,8 @@ typedef struct {
     const StrutModelDesc* models;
     int n, steps, next, total_iters, rc;
     int* record_status;
+    int* record_failed_step;   /* optional: failing step of each record, -1 if none */
+    int* record_iters;         /* optional: Newton iterations of each record          */
     pthread_mutex_t lock;
 } BatchJob;
 
@@ -1163,6 +1165,8 @@ static void* batch_worker(void* arg) {
         pthread_mutex_lock(&job->lock);
         job->total_iters += tot;
         if (job->record_status) job->record_status[i] = rc;
+        if (job->record_failed_step) job->record_failed_step[i] = failed;
+        if (job->record_iters) job->record_iters[i] = tot;
         if (rc != STRUT_OK && job->rc == STRUT_OK) job->rc = rc;
         pthread_mutex_unlock(&job->lock);
     }
@@ -1170,10 +1174,13 @@ static void* batch_worker(void* arg) {
 }
 
 int oracle_run_transient_batch(const StrutModelDesc* models, int n, int steps, int nthreads,
-                               int* total_iters, int* record_status) {
+                               int* total_iters, int* record_status, int* record_failed_step,
+                               int* record_iters) {
     BatchJob job;
     memset(&job, 0, sizeof(job));
     job.record_status = record_status;
+    job.record_failed_step = record_failed_step;
+    job.record_iters = record_iters;
     job.models = models;
     job.n = n;
     job.steps = steps;

@@ -18,6 +18,11 @@
 #include <math.h>
 #include <string.h>
 
+/* Passes of forceBeamColumn2d's subdivision loop in which every scheme failed (the increment
+ * was cut back), over all elements since the library was loaded. */
+static long g_subdivisions = 0;
+long oracle_subdivisions(void) { return g_subdivisions; }
+
 static int invert3(double a, double b, double c, double d, double e, double f, double g,
                    double h, double i, double k[9]) {
     double co00 = e * i - f * h;
@@ -408,6 +413,7 @@ int oracle_fbc2d(OElement* e, const double ug[6], double k[36], double f[6]) {
             att[1] /= 10.0;
             att[2] /= 10.0;
             num_subdivide += 1;
+            __atomic_add_fetch(&g_subdivisions, 1, __ATOMIC_RELAXED);
         }
     }
     if (!converged) {
