@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define STRUT_ABI_VERSION 4
+#define STRUT_ABI_VERSION 5
 #define STRUT_MAX_INT_PTS 10
 
 /* Status codes.  No entry point aborts the process. */
@@ -237,6 +237,8 @@ typedef struct StrutStepStats {
     int32_t failed_instance;           /* first instance with a non-OK status, or -1 */
     int32_t failed_step;
     int32_t status;
+    int64_t fanned_out;                /* forceBeamColumn2d determinations whose attempts ran
+                                          fanned out (StrutTuning.fan_out)               */
 } StrutStepStats;
 
 typedef struct StrutHandle StrutHandle;
@@ -245,7 +247,11 @@ typedef struct StrutHandle StrutHandle;
  * stream while profiling is enabled (no counterpart in the reference; used for rooflines).
  * Index: 0 element state, 1 instance Newton, 2 commit, 3 predictor, 4 post-step;
  * 5 the element critical path: bytes[5] sums, over element launches, the largest number of
- * forceBeamColumn local iterations one element ran in that launch (ms[5] = ms[0]). */
+ * forceBeamColumn local iterations one element ran in that launch (ms[5] = ms[0]).
+ * bytes[0] counts, per section evaluation, one fiber-state update of every fiber: its committed
+ * history read and its trial history written (Concrete02 80 B, Steel02 168 B, Steel01 56 B,
+ * Concrete01 96 B per fiber), whether or not those bytes reach HBM; bytes[2] the commit's
+ * reads and writes of the same histories. */
 #define STRUT_PROF_KERNELS 8
 typedef struct StrutKernelProfile {
     int64_t launches[STRUT_PROF_KERNELS];
@@ -291,6 +297,30 @@ int strut_gpu_set_profiling(StrutHandle* h, int32_t enabled);
 int strut_gpu_get_profile(const StrutHandle* h, StrutKernelProfile* out);
 /* The cudaStream_t every kernel of this handle is launched on (for callers' own events). */
 void* strut_gpu_stream(const StrutHandle* h);
+
+/* Launch-shape choices of a handle.  No counterpart in the reference (Strut runs one CPU
+ * thread); every choice gives the same results bit for bit and changes only the speed.
+ *   fan_out      1: a forceBeamColumn2d element whose last state determination needed a
+ *                subdivided increment runs the twelve attempts of its next first pass (three
+ *                schemes x four subdivision levels, force_beam_column2d.mojo:1669-1763, each
+ *                from the accepted state) on twelve CTAs at once, and the first success in
+ *                Strut's order is kept; 0: the attempts run one after another.  Default 1.
+ *   commit_team  threads per integration point in the commit kernel, 64 or 128 (default 128
+ *                for up to 5 points, else 64; 128 needs at most 5 points).
+ *   factor_ctas  CTAs of the cooperative wide-band factorisation (1 .. its resident limit;
+ *                0: the default, as many as one panel has trailing tiles).
+ *   element_threads  threads of an element CTA: 640 (default, one CTA per SM: the shortest
+ *                per-element iteration) or 320 (two CTAs per SM: twice the elements in flight).
+ * strut_gpu_set_tuning with t = NULL restores the defaults. */
+typedef struct StrutTuning {
+    int32_t fan_out;
+    int32_t commit_team;
+    int32_t factor_ctas;
+    int32_t element_threads;
+    int32_t reserved[4];
+} StrutTuning;
+int strut_gpu_set_tuning(StrutHandle* h, const StrutTuning* t);
+int strut_gpu_get_tuning(const StrutHandle* h, StrutTuning* out);
 
 /* ---- single-iteration entries (parity tests) --------------------------------------- */
 /* Sets the trial free displacements of every instance (concatenated in instance order),

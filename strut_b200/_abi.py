@@ -194,6 +194,17 @@ class StrutStepStats(C.Structure):
         ("failed_instance", C.c_int32),
         ("failed_step", C.c_int32),
         ("status", C.c_int32),
+        ("fanned_out", C.c_int64),
+    ]
+
+
+class StrutTuning(C.Structure):
+    _fields_ = [
+        ("fan_out", C.c_int32),
+        ("commit_team", C.c_int32),
+        ("factor_ctas", C.c_int32),
+        ("element_threads", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -232,6 +243,8 @@ EXPORTS = {
     "strut_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "strut_gpu_get_profile": (C.c_int, [C.c_void_p, C.POINTER(StrutKernelProfile)]),
     "strut_gpu_stream": (C.c_void_p, [C.c_void_p]),
+    "strut_gpu_set_tuning": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "strut_gpu_get_tuning": (C.c_int, [C.c_void_p, C.c_void_p]),
     "strut_gpu_state_determination": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "strut_gpu_band_info": (C.c_int, [C.c_void_p, C.c_int32, _ip, _ip]),
     "strut_gpu_factor_solve": (C.c_int, [C.c_void_p, _dp, _dp]),

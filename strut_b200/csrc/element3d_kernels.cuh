@@ -733,6 +733,7 @@ __device__ void element3d_process(const Geo& g, const DevSection& sd, const DevE
             atomicAdd(&counters[3], (unsigned long long)E.io_bytes);
             atomicAdd(&counters[1], (unsigned long long)nip);
             atomicAdd(&counters[2], (unsigned long long)nip * n_tot);
+            atomicAdd(&counters[7], (unsigned long long)nip * section_update_bytes(sd));
         }
         __syncthreads();
         to_global3(S);
@@ -792,7 +793,7 @@ __device__ void element3d_process(const Geo& g, const DevSection& sd, const DevE
     {
         int num_subdivide = 1;
         int guard = 0;
-        while (num_subdivide <= 4 && guard < 1000) {
+        while (num_subdivide <= 4 && guard < 10000) {
             ++guard;
             int scheme_success = 0;
             if (tid == 0)
@@ -855,6 +856,7 @@ __device__ void element3d_process(const Geo& g, const DevSection& sd, const DevE
         atomicMax(&counters[5], (unsigned long long)S.local_iters);
         atomicAdd(&counters[1], (unsigned long long)S.section_evals);
         atomicAdd(&counters[2], (unsigned long long)S.section_evals * n_tot);
+        atomicAdd(&counters[7], (unsigned long long)S.section_evals * section_update_bytes(sd));
     }
     __syncthreads();
     if (S.flag) {

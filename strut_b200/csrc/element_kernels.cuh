@@ -105,6 +105,7 @@ struct ElemScratch {
     int loop_ctrl;
     int local_iters;
     int section_evals;
+    int hard;  // this determination needed a subdivided increment (fan out next time)
 };
 
 // Family views of the element's committed history (shared memory, or global memory with the
@@ -857,6 +858,126 @@ __device__ __forceinline__ double axial_shape(int idx, double inv_L) {
     return 0.0;
 }
 
+// One attempt of an element's fan-out (level fa / 3, scheme fa % 3 of the first subdivision
+// pass, force_beam_column2d.mojo:1669-1763) from the accepted state in S, its outcome recorded in
+// the fan slot; the last attempt to finish resolves the pass.  Returns -2 for an attempt that is
+// not the last (the caller stops), else the first successful attempt in the reference's order
+// (-1: none), with S as the sequential algorithm leaves it after that acceptance: q, the section
+// deformations and the response cache of the chosen attempt, the accepted basic state advanced,
+// S.loop_ctrl 1 when nothing remains, else 0 with S.att the remainder; S.local_iters and
+// S.section_evals count the attempts the sequential algorithm would have run.  Not inlined: it
+// runs at most once per element determination and keeps the sequential path's registers free.
+__device__ __noinline__ int fan_attempt(const Geo& g, const DevSection& sd, const StageView& sv,
+                                        const DevElem& E, ElemScratch& S, const ElemList& el, int cur,
+                                        int fslot, int fa, const double* ys, double* fo) {
+    const int tid = threadIdx.x, nip = E.nip;
+    const int level = fa / 3, scheme = fa - 3 * (fa / 3);
+    if (tid == 0) {
+        for (int l = 0; l < level; ++l)
+            for (int i = 0; i < 3; ++i) S.att[i] /= 10.0;
+        for (int i = 0; i < 3; ++i) {
+            S.tv[i] = S.acc_v[i] + S.att[i];
+            S.q[i] = S.acc_q[i];
+        }
+        for (int ip = 0; ip < nip; ++ip) {
+            S.vs_e[ip] = S.svs_e[ip];
+            S.vs_k[ip] = S.svs_k[ip];
+        }
+    }
+    __syncthreads();
+    const bool ok = fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme, ys, fo);
+    double* const slot_rec = el.fan_rec + (size_t)(cur * kFanCap + fslot) * kFanAttempts * kFanRec;
+    double* rec = slot_rec + (size_t)fa * kFanRec;
+    if (tid == 0) {
+        rec[0] = ok ? 1.0 : 0.0;
+        rec[1] = (double)S.local_iters;
+        rec[2] = (double)S.section_evals;
+        for (int i = 0; i < 3; ++i) rec[3 + i] = S.q[i];
+        for (int i = 0; i < 10; ++i) rec[6 + i] = S.best[i];
+        rec[86] = (double)S.c_valid;
+    } else if (tid <= nip) {
+        const int ip = tid - 1;
+        rec[16 + ip] = S.vs_e[ip];
+        rec[26 + ip] = S.vs_k[ip];
+        rec[36 + ip] = S.c_n[ip];
+        rec[46 + ip] = S.c_m[ip];
+        rec[56 + ip] = S.c_f00[ip];
+        rec[66 + ip] = S.c_f01[ip];
+        rec[76 + ip] = S.c_f11[ip];
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        const int old = atomicAdd(&el.fan_done[cur * kFanCap + fslot], 1);
+        S.flag = (old % kFanAttempts) == kFanAttempts - 1;
+    }
+    __syncthreads();
+    if (!S.flag) return -2;
+    __threadfence();
+    if (tid == 0) {
+        int best_a = -1;
+        long long li = 0, se = 0;
+        for (int a = 0; a < kFanAttempts; ++a) {
+            const double* r = slot_rec + (size_t)a * kFanRec;
+            li += (long long)__ldcg(r + 1);
+            se += (long long)__ldcg(r + 2);
+            if (__ldcg(r) != 0.0) {
+                best_a = a;
+                break;
+            }
+        }
+        S.local_iters = (int)li;
+        S.section_evals = (int)se;
+        S.loop_ctrl = best_a;
+        if (best_a < 0 || best_a >= 3) S.hard = 1;
+    }
+    __syncthreads();
+    const int best_a = S.loop_ctrl;
+    if (best_a < 0) return -1;
+    const double* r = slot_rec + (size_t)best_a * kFanRec;
+    if (tid == 0) {
+        for (int i = 0; i < 3; ++i) S.q[i] = __ldcg(r + 3 + i);
+        for (int i = 0; i < 10; ++i) S.best[i] = __ldcg(r + 6 + i);
+        S.c_valid = (int)__ldcg(r + 86);
+        // S.att holds this CTA's own level: recompute the chosen one's
+        for (int i = 0; i < 3; ++i) S.att[i] = S.rem[i];
+        for (int l = 0; l < best_a / 3; ++l)
+            for (int i = 0; i < 3; ++i) S.att[i] /= 10.0;
+        for (int i = 0; i < 3; ++i) S.tv[i] = S.acc_v[i] + S.att[i];
+    } else if (tid <= nip) {
+        const int ip = tid - 1;
+        S.vs_e[ip] = __ldcg(r + 16 + ip);
+        S.vs_k[ip] = __ldcg(r + 26 + ip);
+        S.c_n[ip] = __ldcg(r + 36 + ip);
+        S.c_m[ip] = __ldcg(r + 46 + ip);
+        S.c_f00[ip] = __ldcg(r + 56 + ip);
+        S.c_f01[ip] = __ldcg(r + 66 + ip);
+        S.c_f11[ip] = __ldcg(r + 76 + ip);
+    }
+    __syncthreads();
+    // the acceptance of the sequential loop
+    if (tid == 0) {
+        for (int i = 0; i < 3; ++i) {
+            S.acc_v[i] = S.tv[i];
+            S.acc_q[i] = S.best[i];
+        }
+        for (int ip = 0; ip < nip; ++ip) {
+            S.svs_e[ip] = S.vs_e[ip];
+            S.svs_k[ip] = S.vs_k[ip];
+        }
+        S.best_ok = 1;
+        for (int i = 0; i < 3; ++i) S.rem[i] = S.v[i] - S.acc_v[i];
+        if (max_abs3(S.rem) <= 1.0e-12) {
+            S.loop_ctrl = 1;
+        } else {
+            for (int i = 0; i < 3; ++i) S.att[i] = S.rem[i];
+            S.loop_ctrl = 0;
+        }
+    }
+    __syncthreads();
+    return best_a;
+}
+
 // Copies a POD struct from global to shared memory with 4-byte words.
 template <typename T>
 __device__ __forceinline__ void copy_struct(T* dst, const T* src) {
@@ -941,7 +1062,8 @@ struct RecPass {
 };
 
 // State determination of every element of the active instances: k (nd x nd global), f (nd)
-// and the element state.  One CTA of kTeamThreads threads per element at a time.
+// and the element state.  One CTA of NT threads (kTeamThreads, or half as many with two CTAs per
+// SM) per element at a time.
 //
 // Persistent: the grid is sized to the resident CTAs of the device and each CTA claims elements
 // from the list of the instances still iterating (all elements when all_elems is set), so a
@@ -949,8 +1071,8 @@ struct RecPass {
 // up elements queued behind it on the same CTA.
 //
 // DIM 2 instantiates the 2D elements' code only, DIM 3 the 3D elements' (a batch holds one kind).
-template <int DIM>
-__global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
+template <int DIM, int NT>
+__global__ void __launch_bounds__(NT, kTeamThreads / NT) element_state_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
     double* __restrict__ estate, double* __restrict__ ek, double* __restrict__ ef,
     const int* __restrict__ active, int* __restrict__ status, int* __restrict__ elem_err,
@@ -972,17 +1094,22 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         mbar_fence_init();
     }
     __shared__ int s_next;
+    __shared__ int s_fan;  // a fan attempt has already counted itself in (fan_done)
     const int cur = all_elems ? 0 : (ctl->iter & 1);
+    // fanned-out elements of this list (their attempts come first in the work order)
+    const int n_fan = all_elems ? 0 : min(el.hard_count[cur], (int)kFanCap) * kFanAttempts;
     if (!all_elems && blockIdx.x == 0 && tid == 0) {
         el.count[cur ^ 1] = 0;
         el.next[cur ^ 1] = 0;
+        el.hard_count[cur ^ 1] = 0;
     }
     const int total = mode == ELEM_MODE_ALL ? n_elem
-                    : mode == ELEM_MODE_RECORD ? rp.n : el.count[cur];
+                    : mode == ELEM_MODE_RECORD ? rp.n : n_fan + el.count[cur];
     __syncthreads();
     uint32_t phase = 0;
     bool stop = false;
-    auto process = [&](const int e) -> void {
+    // fslot >= 0: attempt fa of the fan-out of element e in slot fslot of this list
+    auto process = [&](const int e, const int fslot, const int fa) -> void {
     copy_struct(&E, elems + e);
     __syncthreads();
     if (mode == ELEM_MODE_RECORD ? status[E.inst] != 0 : !active[E.inst]) return;
@@ -999,6 +1126,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     if (tid == 0) {
         S.local_iters = 0;
         S.section_evals = 0;
+        S.hard = 0;
         for (int i = 0; i < 3; ++i) {
             S.q[i] = estate[(size_t)e * kEStride + kEq + i];
             S.acc_v[i] = estate[(size_t)e * kEStride + kEv + i];
@@ -1116,6 +1244,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
             atomicAdd(&counters[1], (unsigned long long)nip);
             atomicAdd(&counters[2], (unsigned long long)nip *
                                         (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el));
+            atomicAdd(&counters[7], (unsigned long long)nip * section_update_bytes(sd));
         }
         return;
     }
@@ -1195,6 +1324,8 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         __syncthreads();
         converged = S.flag;
     }
+    // a fanned-out element with nothing to subdivide runs on its first attempt's CTA alone
+    if (fslot >= 0 && fa != 0 && (converged || max_abs3(S.rem) <= 1.0e-16)) return;
     if (!converged) {
         if (max_abs3(S.rem) <= 1.0e-16) {
             for (int scheme = 0; scheme < 3; ++scheme) {
@@ -1214,7 +1345,25 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         } else {
             int num_subdivide = 1;
             int guard = 0;
-            while (num_subdivide <= 4 && guard < 1000) {
+            bool run_loop = true;
+            if (fslot >= 0) {
+                const int best_a = fan_attempt(g, sd, sv, E, S, el, cur, fslot, fa, ys, fo);
+                if (best_a == -2) {
+                    s_fan = 1;
+                    return;  // not the last attempt: the last one finishes the element
+                }
+                if (tid == 0) s_fan = 1;
+                if (best_a < 0) {
+                    run_loop = false;  // every attempt failed: the initial-tangent fallback
+                } else {
+                    if (S.loop_ctrl == 1) {
+                        converged = 1;
+                        run_loop = false;
+                    }
+                    guard = best_a / 3 + 1;
+                }
+            }
+            while (run_loop && num_subdivide <= 4 && guard < 10000) {
                 ++guard;
                 int scheme_success = 0;
                 if (tid == 0)
@@ -1256,8 +1405,10 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
                 }
                 if (converged) break;
                 if (scheme_success) continue;
-                if (tid == 0)
+                if (tid == 0) {
                     for (int i = 0; i < 3; ++i) S.att[i] /= 10.0;
+                    S.hard = 1;
+                }
                 __syncthreads();
                 num_subdivide += 1;
             }
@@ -1307,6 +1458,8 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
             es[kEc11 + ip] = S.c_f11[ip];
         }
         es[kEcv] = S.c_valid ? 1.0 : 0.0;
+        if (el.hard_flag && mode == ELEM_MODE_LIST) el.hard_flag[e] = ctl->fan ? S.hard : 0;
+        if (fslot >= 0) atomicAdd(&counters[6], 1ull);
     }
     __syncthreads();
     if (S.flag) {
@@ -1356,6 +1509,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         atomicAdd(&counters[1], (unsigned long long)S.section_evals);
         atomicAdd(&counters[2], (unsigned long long)S.section_evals *
                                     (sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el));
+        atomicAdd(&counters[7], (unsigned long long)S.section_evals * section_update_bytes(sd));
     }
     __syncthreads();
     if (tid < 36) ek[E.ek_off + tid] = S.k[tid];
@@ -1367,7 +1521,28 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     while (li < total && !stop) {
         int claimed = li + gridDim.x;
         if (!all_elems && tid == 0) claimed = atomicAdd(&el.next[cur], 1) + gridDim.x;
-        process(mode == ELEM_MODE_ALL ? li : mode == ELEM_MODE_RECORD ? rp.list[li] : el.list[cur][li]);
+        int pe = -1;
+        const bool fan_item = mode == ELEM_MODE_LIST && li < n_fan;
+        if (mode == ELEM_MODE_ALL) {
+            pe = li;
+        } else if (mode == ELEM_MODE_RECORD) {
+            pe = rp.list[li];
+        } else if (fan_item) {
+            pe = el.hard[cur][li / kFanAttempts];
+        } else {
+            const int ent = el.list[cur][li - n_fan];
+            if (!(ent & kFanBit)) pe = ent;
+        }
+        if (tid == 0) s_fan = 0;
+        if (pe >= 0) process(pe, fan_item ? li / kFanAttempts : -1, li % kFanAttempts);
+        if (fan_item) {
+            __syncthreads();
+            // every attempt counts itself in exactly once, whatever path it took
+            if (tid == 0 && !s_fan) {
+                __threadfence();
+                atomicAdd(&el.fan_done[cur * kFanCap + li / kFanAttempts], 1);
+            }
+        }
         if (tid == 0) s_next = claimed;
         __syncthreads();
         li = s_next;

@@ -74,6 +74,14 @@ struct DevElem {
     double commit_bytes;        // algorithmic HBM bytes of one commit
 };
 
+// Algorithmic HBM bytes of one evaluation of a section's fibers: per fiber-state update its
+// committed history read and its trial history written (Concrete02 5 + 5 doubles, Steel02 10 + 10
+// doubles and kon, Steel01 eps_p and alpha read, five doubles written, Concrete01 6 + 6 doubles;
+// elastic fibers have no history).
+__host__ __device__ __forceinline__ unsigned long long section_update_bytes(const DevSection& sd) {
+    return 80ull * sd.n_c2 + 168ull * sd.n_s2 + 56ull * sd.n_s1 + 96ull * sd.n_c1;
+}
+
 struct DevInst {
     int n, bw, rw, num_dofs;
     int u_off, f_off;
@@ -100,11 +108,46 @@ struct DevInst {
 // instance that has not converged into buffer (i + 1) & 1, and the element kernel of
 // iteration i reads buffer i & 1 and clears the other one's count.  The order inside a list
 // does not matter: elements are independent.
+//
+// Attempt fan-out.  forceBeamColumn2d tries an increment with three schemes at up to four
+// subdivision levels, each attempt starting again from the element's accepted state
+// (force_beam_column2d.mojo:1669-1763), so the twelve attempts of one pass are independent.  An
+// element whose previous state determination needed more than the first level (hard_flag) is
+// listed once more in `hard`, and the element kernel runs its twelve attempts on twelve CTAs at
+// once: each writes its outcome to fan_rec, the last to finish takes the first success in the
+// reference's order (level by level, scheme 0, 1, 2) and carries on from there as the sequential
+// algorithm would, so the result is the sequential one bit for bit.  Its plain list entry carries
+// kFanBit and is skipped.  At most kFanCap elements are fanned out per list.
+constexpr int kFanAttempts = 12;  // 4 subdivision levels x 3 schemes
+constexpr int kFanCap = 512;
+constexpr int kFanRec = 88;       // doubles per attempt record
+constexpr int kFanBit = 0x40000000;
+
 struct ElemList {
     int* list[2];
     int* count;  // 2 entries
     int* next;   // 2 entries: work counter of the persistent element kernel
+    int* hard[2];       // elements fanned out in this list (kFanCap entries each)
+    int* hard_count;    // 2 entries (may exceed kFanCap; only the first kFanCap are fanned out)
+    int* hard_flag;     // per element: its last state determination needed a subdivision
+    int* fan_done;      // 2 x kFanCap: attempts finished per slot, zeroed when the slot is
+                        // handed out; every launch over the list adds kFanAttempts, so the
+                        // last attempt of a launch is the one that finds count % 12 == 11
+    double* fan_rec;    // 2 x kFanCap x kFanAttempts x kFanRec attempt records
 };
+
+// List entry of element e in list buffer `buf`: a flagged element also gets a fan slot.
+__device__ __forceinline__ int list_entry(const ElemList& el, int buf, int e) {
+    if (el.hard_flag && el.hard_flag[e]) {
+        const int slot = atomicAdd(&el.hard_count[buf], 1);
+        if (slot < kFanCap) {
+            el.hard[buf][slot] = e;
+            el.fan_done[buf * kFanCap + slot] = 0;
+            return e | kFanBit;
+        }
+    }
+    return e;
+}
 
 // Step / iteration control on the device (read by the kernels, advanced by step_end_kernel).
 struct DevCtl {
@@ -114,7 +157,8 @@ struct DevCtl {
     int iter;       // Newton iteration of the current step
     int max_iters;  // max over instances
     int single;     // single-instance handle: stop at the failing step
-    int pad0, pad1;
+    int fan;        // attempt fan-out enabled (StrutTuning.fan_out)
+    int pad1;
 };
 
 struct FiberState {

@@ -767,8 +767,9 @@ __device__ void newton_tail(const DevInst& I, InstArrays& A, int inst, const dou
     // still iterating: list this instance's elements for the next element kernel
     const int base = red_r[0];
     if (base >= 0) {
-        int* list = A.el.list[(A.ctl->iter + 1) & 1];
-        for (int k = tid; k < I.n_elem; k += nt) list[base + k] = I.elem_off + k;
+        const int buf = (A.ctl->iter + 1) & 1;
+        int* list = A.el.list[buf];
+        for (int k = tid; k < I.n_elem; k += nt) list[base + k] = list_entry(A.el, buf, I.elem_off + k);
     }
 }
 
@@ -794,7 +795,7 @@ __global__ void predictor_kernel(const DevInst* __restrict__ insts, InstArrays A
             atomicAdd(A.nactive, 1);
             const DevInst& I = insts[gi];
             const int base = atomicAdd(&A.el.count[0], I.n_elem);
-            for (int k = 0; k < I.n_elem; ++k) A.el.list[0][base + k] = I.elem_off + k;
+            for (int k = 0; k < I.n_elem; ++k) A.el.list[0][base + k] = list_entry(A.el, 0, I.elem_off + k);
         }
     }
     if (gi >= n_free_total) return;
@@ -872,6 +873,8 @@ __global__ void step_end_kernel(DevCtl* ctl, const int* __restrict__ status,
         el.count[1] = 0;
         el.next[0] = 0;
         el.next[1] = 0;
+        el.hard_count[0] = 0;
+        el.hard_count[1] = 0;
         const bool stop = ctl->single && status[0] != 0;
         if (use_cond) cudaGraphSetConditional(outer, (step + 1 < ctl->n_end && !stop) ? 1 : 0);
     }

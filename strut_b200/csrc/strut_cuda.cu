@@ -292,7 +292,7 @@ struct StrutHandle {
     DevShell* d_shells = nullptr;
     int n_shells = 0;
     // instances whose band is factored in global memory
-    int n_large = 0, large_rows = 0, max_large_n = 0, lfactor_grid = 1;
+    int n_large = 0, large_rows = 0, max_large_n = 0, lfactor_grid = 1, max_factor_grid = 1;
     long long lband_total = 0;
     size_t lfactor_smem = 16;
     int max_large_bw = 0;
@@ -354,6 +354,10 @@ struct StrutHandle {
     struct PredState* pred = nullptr;
     double commit_bytes_total = 0.0;
     long long dense_total = 0;
+    StrutTuning tune = {1, 0, 0, 0, {0, 0, 0, 0}};
+    int default_factor_grid = 1;
+    int tune_gen = 0;       // bumped by strut_gpu_set_tuning (the graph bakes launch shapes in)
+    int graph_tune_gen = -1;
     ~StrutHandle();
     void release() {
         for (void* p : allocs) cudaFree(p);
@@ -399,15 +403,35 @@ static int prof_end(StrutHandle* h, int k) {
 // Element state kernel: kTeamThreads threads per element CTA.  Commit kernel: one team of 128
 // threads per integration point up to 5 points, else 64.
 using CommitKernel = decltype(&commit_kernel<128>);
-using ElemKernel = decltype(&element_state_kernel<2>);
+using ElemKernel = decltype(&element_state_kernel<2, kTeamThreads>);
+static int elem_threads_of(const StrutHandle* h) {
+    return h->tune.element_threads == kTeamThreads / 2 ? kTeamThreads / 2 : kTeamThreads;
+}
 static ElemKernel elem_kernel_of(const StrutHandle* h) {
-    return h->ndf_all == 6 ? element_state_kernel<3> : element_state_kernel<2>;
+    if (elem_threads_of(h) == kTeamThreads)
+        return h->ndf_all == 6 ? element_state_kernel<3, kTeamThreads> : element_state_kernel<2, kTeamThreads>;
+    return h->ndf_all == 6 ? element_state_kernel<3, kTeamThreads / 2> : element_state_kernel<2, kTeamThreads / 2>;
 }
-static dim3 elem_block(const StrutHandle*) { return dim3(kTeamThreads); }
+static dim3 elem_block(const StrutHandle* h) { return dim3(elem_threads_of(h)); }
+// Resident CTAs of the element kernel the handle's tuning selects (its persistent grid).
+static int elem_grid_of(StrutHandle* h) {
+    int per_sm = 0, n_sm = 0;
+    CK(cudaFuncSetAttribute(elem_kernel_of(h), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->elem_smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, elem_kernel_of(h), (int)elem_block(h).x, h->elem_smem));
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->device));
+    if (per_sm < 1) return fail(STRUT_UNSUPPORTED, "element kernel does not fit on an SM");
+    h->elem_grid = std::max(1, std::min(h->n_elem, per_sm * n_sm));
+    return STRUT_OK;
+}
+static int commit_team_of(const StrutHandle* h) {
+    // the commit kernel is launched with at most kTeamThreads threads: team x points
+    if (h->tune.commit_team == 64 || (h->tune.commit_team == 128 && h->max_nip <= 5)) return h->tune.commit_team;
+    return h->max_nip <= 5 ? 128 : 64;
+}
 static CommitKernel commit_kernel_of(const StrutHandle* h) {
-    return h->max_nip <= 5 ? commit_kernel<128> : commit_kernel<64>;
+    return commit_team_of(h) == 128 ? commit_kernel<128> : commit_kernel<64>;
 }
-static dim3 commit_block(const StrutHandle* h) { return dim3((h->max_nip <= 5 ? 128 : 64) * h->max_nip); }
+static dim3 commit_block(const StrutHandle* h) { return dim3(commit_team_of(h) * h->max_nip); }
 
 // all_elems: every element (set-up and single-iteration entries); otherwise the list of
 // elements of the instances still iterating.
@@ -666,11 +690,12 @@ static int build_graph(StrutHandle* h) {
     h->graph_keys[2] = h->d_hist_iters;
     h->graph_keys[3] = h->d_ag;
     h->graph_keys[4] = h->pred;
+    h->graph_tune_gen = h->tune_gen;
     return STRUT_OK;
 }
 
 static int ensure_graph(StrutHandle* h) {
-    if (h->gexec && h->graph_keys[0] == h->d_hist_disp && h->graph_keys[1] == h->d_hist_ef &&
+    if (h->gexec && h->graph_tune_gen == h->tune_gen && h->graph_keys[0] == h->d_hist_disp && h->graph_keys[1] == h->d_hist_ef &&
         h->graph_keys[2] == h->d_hist_iters && h->graph_keys[3] == h->d_ag && h->graph_keys[4] == h->pred)
         return STRUT_OK;
     return build_graph(h);
@@ -1230,15 +1255,7 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     if (h->elem_smem > 200 * 1024) return bail(fail(STRUT_UNSUPPORTED, "element fiber history exceeds shared memory"));
     h->elem_smem = std::max<size_t>(h->elem_smem, 16);
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    CK(cudaFuncSetAttribute(elem_kernel_of(h), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->elem_smem));
-    {
-        int per_sm = 0, n_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, elem_kernel_of(h), (int)elem_block(h).x,
-                                                         h->elem_smem));
-        CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->device));
-        if (per_sm < 1) return bail(fail(STRUT_UNSUPPORTED, "element kernel does not fit on an SM"));
-        h->elem_grid = std::max(1, std::min(h->n_elem, per_sm * n_sm));
-    }
+    if ((rc = elem_grid_of(h)) != STRUT_OK) return bail(rc);
     CK(cudaFuncSetAttribute(instance_newton_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::max<size_t>(h->inst_smem, 16)));
     auto& al = h->allocs;
@@ -1337,8 +1354,24 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         (rc = dzeros(&h->d_counters, 8, al)) || (rc = dzeros(&A.dense, (size_t)h->dense_total, al)) ||
         (rc = dzeros(&A.piv, nF, al)) || (rc = dzeros(&A.fallbacks, (size_t)h->n_inst, al)) ||
         (rc = dzeros(&A.el.list[0], (size_t)h->n_elem, al)) || (rc = dzeros(&A.el.list[1], (size_t)h->n_elem, al)) ||
-        (rc = dzeros(&A.el.count, 2, al)) || (rc = dzeros(&A.el.next, 2, al)))
+        (rc = dzeros(&A.el.count, 2, al)) || (rc = dzeros(&A.el.next, 2, al)) ||
+        (rc = dzeros(&A.el.hard[0], (size_t)kFanCap, al)) || (rc = dzeros(&A.el.hard[1], (size_t)kFanCap, al)) ||
+        (rc = dzeros(&A.el.hard_count, 2, al)) || (rc = dzeros(&A.el.fan_done, (size_t)2 * kFanCap, al)))
         return bail(rc);
+    {
+        // attempt fan-out of forceBeamColumn2d elements (none in a 3D handle)
+        bool any_fbc2d = false;
+        for (int i = 0; i < num_instances && !any_fbc2d; ++i)
+            for (int k = 0; k < models[i].num_elements; ++k)
+                if (models[i].elements[k].type == STRUT_ELEM_FORCE_BEAM_COLUMN_2D) {
+                    any_fbc2d = true;
+                    break;
+                }
+        if (any_fbc2d &&
+            ((rc = dzeros(&A.el.hard_flag, (size_t)h->n_elem, al)) ||
+             (rc = dzeros(&A.el.fan_rec, (size_t)2 * kFanCap * kFanAttempts * kFanRec, al))))
+            return bail(rc);
+    }
     if (h->any_modified &&
         ((rc = dzeros(&A.kfrz, (size_t)h->band_total, al)) || (rc = dzeros(&A.lufrz, (size_t)h->band_total, al)) ||
          (rc = dzeros(&A.lu_dense, (size_t)h->n_inst, al))))
@@ -1417,6 +1450,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         // one CTA per SM at most, all co-resident (cooperative launch), and no more than one
         // panel's trailing tiles can use
         h->lfactor_grid = std::max(1, std::min(n_sm, large_factor_tiles(h->max_large_bw)));
+        h->default_factor_grid = h->lfactor_grid;
+        h->max_factor_grid = n_sm * per_sm;
         CK(cudaFuncSetAttribute(large_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)large_solve_smem(h->max_large_n)));
     }
@@ -1522,10 +1557,14 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
         c.n_end = step0 + n_steps;
         c.max_iters = h->max_iters_global;
         c.single = h->n_inst == 1;
+        c.fan = h->tune.fan_out ? 1 : 0;
+        if (!c.fan && h->A.el.hard_flag)
+            CK(cudaMemsetAsync(h->A.el.hard_flag, 0, sizeof(int) * (size_t)h->n_elem, h->stream));
         CK(cudaMemcpyAsync(h->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemsetAsync(h->A.nactive, 0, 4 * sizeof(int), h->stream));
         CK(cudaMemsetAsync(h->A.el.count, 0, 2 * sizeof(int), h->stream));
         CK(cudaMemsetAsync(h->A.el.next, 0, 2 * sizeof(int), h->stream));
+        CK(cudaMemsetAsync(h->A.el.hard_count, 0, 2 * sizeof(int), h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
     if (n_steps > 0 && !h->prof && h->n_large == 0) {
@@ -1613,12 +1652,14 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
     unsigned long long cnt[8];
     CK(cudaMemcpy(cnt, h->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
     if (h->prof) {
-        h->P.bytes[0] += (double)cnt[3];
+        // element kernel: the fiber-state update bytes of its section evaluations
+        h->P.bytes[0] += (double)cnt[7];
         h->P.bytes[1] += (double)cnt[4];
         h->P.bytes[3] += (double)st.steps_done * 8.0 * 12.0 * h->n_free_total;
         h->P.bytes[4] += (double)st.steps_done * 8.0 * 8.0 * h->n_free_total;
     }
     st.local_element_iterations = (int64_t)cnt[0];
+    st.fanned_out = (int64_t)cnt[6];
     st.section_evaluations = (int64_t)cnt[1];
     {
         const int first = h->steps_done - st.steps_done;
@@ -1738,6 +1779,37 @@ int strut_gpu_set_profiling(StrutHandle* h, int32_t enabled) {
     if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
     h->prof = enabled != 0;
     if (h->prof) std::memset(&h->P, 0, sizeof(h->P));
+    return STRUT_OK;
+}
+
+int strut_gpu_set_tuning(StrutHandle* h, const StrutTuning* t) {
+    if (!h) return fail(STRUT_BAD_ARG, "bad arguments");
+    StrutTuning d = {1, 0, 0, 0, {0, 0, 0, 0}};
+    if (t) {
+        if ((t->fan_out != 0 && t->fan_out != 1) || (t->commit_team != 0 && t->commit_team != 64 && t->commit_team != 128) ||
+            (t->commit_team == 128 && h->max_nip > 5) || t->factor_ctas < 0 ||
+            (t->element_threads != 0 && t->element_threads != kTeamThreads && t->element_threads != kTeamThreads / 2))
+            return fail(STRUT_BAD_ARG, "tuning value out of range");
+        d = *t;
+    }
+    const StrutTuning old = h->tune;
+    h->tune = d;
+    if (elem_grid_of(h) != STRUT_OK) {
+        h->tune = old;
+        elem_grid_of(h);
+        return fail(STRUT_UNSUPPORTED, "the element kernel with that many threads does not fit on an SM");
+    }
+    h->lfactor_grid = d.factor_ctas > 0 ? std::min(d.factor_ctas, h->max_factor_grid) : h->default_factor_grid;
+    h->tune_gen += 1;
+    return STRUT_OK;
+}
+
+int strut_gpu_get_tuning(const StrutHandle* h, StrutTuning* out) {
+    if (!h || !out) return fail(STRUT_BAD_ARG, "bad arguments");
+    *out = h->tune;
+    out->commit_team = commit_team_of(h);
+    out->element_threads = elem_threads_of(h);
+    out->factor_ctas = h->n_large ? h->lfactor_grid : 0;
     return STRUT_OK;
 }
 

@@ -94,6 +94,21 @@ class Analysis:
         self.last_status = rc
         return st
 
+    def set_tuning(self, fan_out=None, commit_team=None, factor_ctas=None, element_threads=None):
+        """Launch-shape choices (strut_gpu_set_tuning); None keeps the current value.  Every
+        choice gives the same results bit for bit."""
+        t = self.tuning()
+        for name, v in (("fan_out", fan_out), ("commit_team", commit_team), ("factor_ctas", factor_ctas),
+                        ("element_threads", element_threads)):
+            if v is not None:
+                setattr(t, name, int(v))
+        _check(lib().strut_gpu_set_tuning(self.h, C.byref(t)), "strut_gpu_set_tuning")
+
+    def tuning(self) -> A.StrutTuning:
+        t = A.StrutTuning()
+        _check(lib().strut_gpu_get_tuning(self.h, C.byref(t)), "strut_gpu_get_tuning")
+        return t
+
     def history(self, instance: int = 0):
         m = self.models[instance]
         S = self.steps_done
