@@ -14,9 +14,18 @@ updates/s, simulated seconds per wall second.
           already resident in HBM
   e2e     the public API call a user makes: create (host -> device copy of all model data and
           records) + run + read back the recorded histories, timed on the host with device
-          synchronisation, per bench step
-Multi-GPU: one process per GPU, each with its own 256 frames (records seeded per rank): weak
-scaling, no collective on the data path; the timing is the max over ranks.
+          synchronisation, per bench step (min(K, 3) repetitions)
+  roofline          the element kernel (most of the device time): fiber-state update bytes of
+                    its section evaluations (80 B per Concrete02 fiber, 168 B per Steel02 fiber)
+                    over its event-timed launches
+  fiber_kernel      the streaming fiber-state update kernel alone (strut_gpu_section_eval_batch)
+                    over as many RC column sections as the batch has fibers
+  commit_kernel     the commit kernel's history reads and writes over its launches
+  tall_frame3d      the 20-story 6x6-bay 3D frame (one instance, band in global memory), the
+                    whole 4000-step record
+Multi-GPU (one process per GPU, no collective on the data path, timing = max over ranks):
+--scaling weak (default) gives every rank its own 256 frames (records seeded per rank);
+--scaling strong partitions one fixed 256-frame batch across the ranks by fiber count.
 
 Learned arm (``learned`` in the line, off with --no-learned): a per-node network trained on the
 tensor cores on plain histories of 64 other frames proposes each step's first Newton guess; the
@@ -24,7 +33,7 @@ first iteration keeps it only where its residual beats the Newmark predictor's.
 
 ``--impl reference`` times the reference algorithm's CPU implementation (the CPU oracle, a
 plain C restatement of Strut's path; Strut itself is Mojo and cannot be built here) on all host
-cores over a bounded sample of the same workload.
+cores over the same batch: every record of it, all 2000 steps.
 """
 from __future__ import annotations
 
@@ -62,8 +71,11 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=8)
     ap.add_argument("--no-tall", action="store_true",
                     help="skip the large single-instance 3D frame (20 stories, 6x6 bays)")
-    ap.add_argument("--tall-steps", type=int, default=60,
-                    help="timed steps of the 4000-step large 3D frame record")
+    ap.add_argument("--tall-steps", type=int, default=4000,
+                    help="timed steps of the 4000-step large 3D frame record (default: all)")
+    ap.add_argument("--no-fiber", action="store_true", help="skip the streaming fiber-kernel measurement")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="N > 1: every rank its own 256 frames (weak) or one batch partitioned (strong)")
     ap.add_argument("--profile-only", action="store_true",
                     help="one short analysis (for a profiler launch list); prints no bench line")
     ap.add_argument("--profile-tall", action="store_true",
@@ -147,76 +159,130 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(models, cases, nthreads=None, target_s=15.0):
+def cpu_baseline(models, nthreads=None):
     """The CPU oracle (a C restatement of Strut's single-threaded path) over all host threads,
-    on a bounded sample of the same workload: the first frames of the batch for a number of
-    steps sized to ~target_s of wall time.  Returns (records/hour, cores, sample text)."""
+    on a bounded sample of the same workload: the first `nthreads` frames of the batch, each
+    one whole 2000-step record on its own thread (as Strut runs a record).  Returns
+    (records/hour, cores, sample text)."""
     from oracle import binding
 
     binding.build()
     nthreads = nthreads or os.cpu_count() or 1
-    nfr = min(len(models), max(nthreads, 1) * 2)
-    sub = models[:nfr]
-    # probe: 20 steps on the sample
+    sub = models[:min(len(models), nthreads)]
     t0 = time.perf_counter()
-    binding.run_batch(sub, 20, nthreads)
-    probe = time.perf_counter() - t0
-    steps = int(min(STEPS, max(20, 20 * target_s / max(probe, 1e-3))))
-    t0 = time.perf_counter()
-    _rc, tot_iters, st = binding.run_batch(sub, steps, nthreads)
+    _rc, tot_iters, st = binding.run_batch(sub, STEPS, nthreads)
     el = time.perf_counter() - t0
-    # like the GPU arm, only records that ran every step count; failed ones still cost time
     n_ok = int((st == 0).sum())
-    records = n_ok * steps / float(STEPS)
-    rph = records / el * 3600.0
-    sample = (f"{nfr} frames of the batch x {steps} of {STEPS} steps on {nthreads} threads, "
-              f"{n_ok} completed, {el:.1f} s, {tot_iters / (nfr * steps):.2f} Newton its/step")
+    rph = n_ok / el * 3600.0
+    sample = (f"frames 0-{len(sub) - 1} of the batch, whole {STEPS}-step records, one per thread on "
+              f"{nthreads} threads: {n_ok} completed in {el:.1f} s, {tot_iters / (len(sub) * STEPS):.2f} "
+              f"Newton its/step")
     return rph, nthreads, sample
 
 
 def tall_arm(args, device, runtime, A, torch):
     """The large single instance: the 20-story 6x6-bay 3D RC frame with rigid diaphragms
     (1029 nodes, 2660 elements, 2.77 M fibers, 3000 free dofs, band in global memory), two
-    horizontal records, dt 0.005 s.  Device time of --tall-steps steps after 3 warm-up steps
-    (its fiber history, 2.77 M fibers x ~10 doubles, exceeds L2); records/hour is one 4000-step
-    record at that rate.  Beside it, the CPU oracle on 2 steps of the same record."""
+    horizontal records, dt 0.005 s: device time of --tall-steps steps (default the whole
+    4000-step record) after 3 warm-up steps of a separate handle (its fiber history, 2.77 M
+    fibers x ~10 doubles, exceeds L2).  Beside it, the CPU oracle's time per Newton iteration on
+    the first steps, scaled to the GPU run's iterations per step (the oracle refactors the band
+    densely every iteration, so its step time is its iteration time x the iteration count)."""
     from strut_b200 import model as M
     from strut_b200 import workloads as W
 
-    case = W.tall_frame3d_case(steps=args.tall_steps + 3)
+    steps = min(args.tall_steps, 4000)
+    case = W.tall_frame3d_case(steps=max(steps, 3))
     m = M.Model(case)
+    with runtime.Analysis([m], device=device) as an:
+        an.run(3, check=False)
     an = runtime.Analysis([m], device=device)
-    an.run(3, check=False)
     stream = torch.cuda.ExternalStream(runtime.lib().strut_gpu_stream(an.h))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    an.run(args.tall_steps, check=False)
+    an.run(steps, check=False)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
     _d, _e, it = an.history(0)
     status = int(an.instance_status()[0])
+    done = an.steps_done
     an.close()
-    ms_step = ms / args.tall_steps
+    ms_step = ms / max(done, 1)
+    its = float(np.mean(it)) if len(it) else None
     out = {"workload": "tall_3d_rc_frame_20s_6x6b_diaphragm", "nodes": m.num_nodes,
            "elements": len(m.elements), "free_dofs": m.num_free, "fibers": m.num_fibers_total,
-           "record_steps": 4000, "dt": 0.005, "steps_timed": args.tall_steps, "warmup_steps": 3,
+           "record_steps": 4000, "dt": 0.005, "steps_timed": done, "warmup_steps": 3,
            "ms_per_step": ms_step, "records_per_hour": 3600.0 / (ms_step * 4000 / 1000.0),
-           "newton_its_per_step": float(np.mean(it[3:])) if len(it) > 3 else None,
-           "status": status}
-    if not args.no_cpu_baseline:
-        sys.path.insert(0, str(ROOT))
+           "newton_its_per_step": its, "status": status}
+    if not args.no_cpu_baseline and its:
         from oracle import binding as O
 
         O.build()
+        k = 3
         t0 = time.perf_counter()
-        rc = O.run_transient(m, 2)[3]
-        t = (time.perf_counter() - t0) / 2.0
-        out["cpu_baseline"] = {"value": 3600.0 / (t * 4000), "unit": "records/hour", "cores": 1,
+        _d, _e, cit, rc, _f = O.run_transient(m, k)
+        t = time.perf_counter() - t0
+        per_it = t / max(int(cit.sum()), 1)
+        step_s = per_it * its
+        out["cpu_baseline"] = {"value": 3600.0 / (step_s * 4000), "unit": "records/hour", "cores": 1,
                                "kind": "port", "status": int(rc),
-                               "sample": f"first 2 of 4000 steps on 1 thread, {t:.2f} s/step"}
+                               "sample": f"first {k} of 4000 steps on 1 thread: {per_it:.2f} s per Newton "
+                                         f"iteration, x {its:.2f} iterations per step (the GPU run's mean)"}
     return out
+
+
+def fiber_arm(n_fibers, runtime, torch, peak, steps=20, warmup=3):
+    """The streaming fiber-state update kernel alone: one RC column section (140 Concrete02
+    and 8 Steel02 fibers) in as many instances as the batch has fibers, each with its own
+    committed history; every call reads and rewrites every fiber's history once (80 B per
+    Concrete02 fiber, 168 B per Steel02 fiber) at strains that cycle with a growing amplitude,
+    so fibers load, unload and reverse.  Device time of `steps` calls after `warmup` calls; the
+    histories (~1 GB) exceed L2."""
+    from strut_b200 import model as Mo
+    from strut_b200 import workloads as W
+
+    case = {"materials": [{"id": 1, "type": "Concrete02", "params": dict(W.CORE)},
+                          {"id": 2, "type": "Concrete02", "params": dict(W.COVER)},
+                          {"id": 3, "type": "Steel02", "params": dict(W.STEEL)}],
+            "section": W.rc_section(1, 0.5, 0.5)}
+    mats, nm, fibs, nf = Mo.section_fibers(case["section"], case["materials"])
+    n = (n_fibers + nf - 1) // nf
+    b = runtime.SectionBatch(mats, nm, fibs, nf, n)
+    tot = steps + warmup
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0)
+    ph = torch.rand((1, n), generator=gen, device="cuda", dtype=torch.float64) * 6.283185307179586
+    t = torch.arange(tot, device="cuda", dtype=torch.float64)[:, None]
+    amp = (t + 1.0) / tot
+    ek = torch.empty((tot, n, 2), dtype=torch.float64, device="cuda")
+    ek[:, :, 0] = -3.0e-4 + 2.0e-4 * torch.sin(0.7 * t + ph)
+    ek[:, :, 1] = 8.0e-3 * amp * torch.sin(0.9 * t + 2.0 * ph)
+    resp = torch.empty((n, 5), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    for k in range(warmup):
+        b.eval(ek[k].data_ptr(), resp.data_ptr(), commit=True, stream=s.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for k in range(warmup, tot):
+        b.eval(ek[k].data_ptr(), resp.data_ptr(), commit=True, stream=s.cuda_stream)
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ok = bool(torch.isfinite(resp).all().item())
+    b.close()
+    n_c2 = sum(1 for f in range(nf) if mats[fibs[f].material].type == 4)
+    n_s2 = sum(1 for f in range(nf) if mats[fibs[f].material].type == 3)
+    per_section = 80 * n_c2 + 168 * n_s2
+    achieved = n * per_section / (ms / 1000.0) / 1e9
+    return {"kernel": "fiber_stream_kernel", "bound": "hbm", "sections": n, "fibers": n * nf,
+            "bytes_per_section": per_section, "launches": steps, "avg_launch_ms": ms,
+            "fiber_state_updates_per_s": n * nf / (ms / 1000.0),
+            "achieved": achieved, "peak": peak[0], "unit": "GB/s", "frac": achieved / peak[0],
+            "peak_kind": peak[1], "finite": ok}
 
 
 def learned_arm(args, models, device, runtime, A, torch, world):
@@ -282,19 +348,26 @@ def learned_arm(args, models, device, runtime, A, torch, world):
 
 
 def run_reference(args):
+    """The reference algorithm's CPU implementation (the oracle) on all host threads over the
+    whole batch: every record, all of its steps, one record per thread at a time as Strut runs
+    it.  The K bench steps are K shares of the batch run together in one pool of threads (so
+    that the run's length does not depend on K); records/hour = completed records / wall time."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    from oracle import binding
+
+    binding.build()
     models, cases = build_models(args.frames, args.record_steps, 1000)
-    vals = []
-    info = None
-    for _ in range(args.warmup):
-        pass
-    for _ in range(max(args.steps, 1)):
-        rph, cores, sample = cpu_baseline(models, cases)
-        vals.append(rph)
-        info = (cores, sample)
-    v = float(np.mean(vals))
+    nthreads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    _rc, tot_iters, st = binding.run_batch(models, args.record_steps, nthreads)
+    el = time.perf_counter() - t0
+    n_ok = int((st == 0).sum())
+    v = n_ok / el * 3600.0
+    sample = (f"all {len(models)} frames of the batch, whole {args.record_steps}-step records on {nthreads} "
+              f"threads: {n_ok} completed in {el:.1f} s, {tot_iters / (len(models) * args.record_steps):.2f} "
+              f"Newton its/step")
     line = {
         "impl": "reference",
         "metric": METRIC, "value": v, "unit": "records/hour", "n_gpus": 0,
@@ -302,8 +375,9 @@ def run_reference(args):
         "dtype": "f64", "data": "synthetic (seeded Kanai-Tajimi records, generated RC frames)",
         "config": {"workload": "batched_plain_2d_rc_frames", "frames": args.frames,
                    "steps_per_record": args.record_steps, "dt": DT},
-        "cpu_baseline": {"value": v, "unit": "records/hour", "cores": info[0], "kind": "port",
-                         "sample": info[1]},
+        "records_completed": n_ok,
+        "cpu_baseline": {"value": v, "unit": "records/hour", "cores": nthreads, "kind": "port",
+                         "sample": sample},
         "e2e": {"value": v, "unit": "records/hour", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "vs_baseline": None,
     }
@@ -352,7 +426,16 @@ def main():
                               "workload": "tall_3d_rc_frame_20s_6x6b_diaphragm", "steps": args.tall_steps}))
         return 0
 
-    models, cases = build_models(args.frames, args.record_steps, 1000 + rank * args.frames)
+    if args.scaling == "strong" and world > 1:
+        from strut_b200 import distributed as D
+
+        all_models, all_cases = build_models(args.frames, args.record_steps, 1000)
+        share = D.rank_share([m.num_fibers_total for m in all_models], world, rank)
+        models = [all_models[i] for i in share]
+        total_frames = args.frames
+    else:
+        models, _cases = build_models(args.frames, args.record_steps, 1000 + rank * args.frames)
+        total_frames = args.frames * world
     n_fibers = sum(m.num_fibers_total for m in models)
 
     if args.profile_only:
@@ -392,8 +475,9 @@ def main():
             P = A.StrutKernelProfile()
             runtime.lib().strut_gpu_get_profile(an.h, __import__("ctypes").byref(P))
             prof_out = P
+        tuned = an.tuning()
         an.close()
-        return ms, st, prof_out
+        return ms, st, prof_out, tuned
 
     # warm-up (untimed)
     for _ in range(args.warmup):
@@ -405,7 +489,7 @@ def main():
     with ClockSampler(device) as clk:
         times, stats = [], []
         for _ in range(args.steps):
-            ms, st, _p = one_analysis()
+            ms, st, _p, tuned = one_analysis()
             times.append(ms)
             stats.append(st)
     torch.cuda.synchronize()
@@ -423,15 +507,14 @@ def main():
         t = torch.tensor([completed], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(t)
         completed = int(t.item())
-    records = completed
-    value = records / (ms_per_step / 1000.0) * 3600.0
-    newton_per_step = st.global_newton_iterations / float(args.frames * args.record_steps)
-    fiber_updates_per_s = st.fiber_updates / (times[-1] / 1000.0)
+    value = completed / (ms_per_step / 1000.0) * 3600.0
+    newton_per_step = st.global_newton_iterations / float(len(models) * args.record_steps)
+    fiber_updates_per_s = sum(x.fiber_updates for x in stats) / (sum(times) / 1000.0)
 
-    # end to end through the public API with host buffers, per bench step
+    # end to end through the public API with host buffers (min(K, 3) repetitions)
     e2e_times = []
     h2d = d2h = 0
-    for _ in range(max(1, args.steps)):
+    for _ in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         with runtime.Analysis(models, device=device) as an:
@@ -450,26 +533,36 @@ def main():
     for m in models:
         h2d += (len(m.fibers) * 32 + len(m.materials) * 96 + len(m.elements) * 48 +
                 m.num_dofs * (8 * 4 + 4) + sum(len(x["values"]) * 8 for x in m.excitations))
-    e2e_value = records / e2e_s * 3600.0
+    e2e_value = completed / e2e_s * 3600.0
 
-    # roofline of the dominant kernel (element state determination), one profiled analysis
-    _ms, _st, P = one_analysis(prof=True)
-    peak, peak_kind = measured_peaks()
-    el_ms = P.ms[A.PROF_ELEMENT]
-    el_launch = max(P.launches[A.PROF_ELEMENT], 1)
-    el_bytes = P.bytes[A.PROF_ELEMENT]
-    achieved = (el_bytes / el_launch) / ((el_ms / el_launch) / 1000.0) / 1e9
-    kernel_share = {k: P.ms[i] for k, i in (("element", 0), ("instance", 1), ("commit", 2),
-                                              ("predictor", 3), ("post", 4))}
-    # DRAM bytes per launch: the measured traffic / algorithmic-bytes ratio of this kernel (one
-    # ncu capture of a smaller batch of the same frames, traffic growing with the elements
-    # processed) times this run's algorithmic bytes per launch
-    traffic = None
+    # rooflines, from one profiled analysis (host-driven loop, events around every launch)
+    _ms, _st, P, _t = one_analysis(prof=True)
+    peak = measured_peaks()
+
+    def roof(k, name):
+        launches = max(int(P.launches[k]), 1)
+        ms_k = P.ms[k]
+        achieved = (P.bytes[k] / launches) / ((ms_k / launches) / 1000.0) / 1e9 if ms_k > 0 else 0.0
+        return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak[0], "unit": "GB/s",
+                "frac": achieved / peak[0], "peak_kind": peak[1], "launches": int(P.launches[k]),
+                "avg_launch_ms": ms_k / launches, "bytes_per_launch": P.bytes[k] / launches}
+
+    roofline = roof(A.PROF_ELEMENT, "element_state_kernel")
+    # measured DRAM traffic per launch: DRAM bytes per algorithmic byte of this kernel from one
+    # ncu capture of a smaller batch of the same frames, times this run's algorithmic bytes
+    roofline["traffic"] = None
     tp = ROOT / "profiles" / "element_state_kernel_dram_traffic_rc_frames96.md"
     if tp.exists():
         for line in tp.read_text().splitlines():
-            if line.startswith("traffic_to_algorithmic_ratio:"):
-                traffic = float(line.split(":", 1)[1]) * (el_bytes / el_launch)
+            if line.startswith("traffic_per_update_byte:"):
+                roofline["traffic"] = float(line.split(":", 1)[1]) * roofline["bytes_per_launch"]
+    commit_roof = roof(A.PROF_COMMIT, "commit_kernel")
+    kernel_share = {k: P.ms[i] for k, i in (("element", 0), ("instance", 1), ("commit", 2),
+                                              ("predictor", 3), ("post", 4))}
+
+    fiber = None
+    if not args.no_fiber:
+        fiber = fiber_arm(n_fibers, runtime, torch, peak)
 
     learned = None
     if not args.no_learned:
@@ -481,7 +574,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rph, cores, sample = cpu_baseline(models, cases)
+        rph, cores, sample = cpu_baseline(models)
         cpu = {"value": rph, "unit": "records/hour", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -494,32 +587,37 @@ def main():
             "warmup": args.warmup,
             "ms_per_step": ms_per_step,
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong" if (args.scaling == "strong" and world > 1) else "weak",
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic (seeded Kanai-Tajimi records, generated RC frames)",
-            "config": {"workload": "batched_plain_2d_rc_frames", "frames_per_gpu": args.frames,
+            "config": {"workload": "batched_plain_2d_rc_frames", "frames_total": total_frames,
+                       "frames_per_gpu": len(models),
                        "steps_per_record": args.record_steps, "dt": DT,
-                       "fibers_per_gpu": n_fibers, "parallelism": f"replicas{world}",
+                       "fibers_per_gpu": n_fibers,
+                       "parallelism": (f"partition{world}" if args.scaling == "strong" and world > 1
+                                       else f"replicas{world}"),
+                       "tuned": {"fan_out": int(tuned.fan_out), "commit_team": int(tuned.commit_team),
+                                 "element_threads": int(tuned.element_threads)},
                        "l2": "fiber history of the batch exceeds L2 (no flush needed)"},
             "newton_its_per_step": newton_per_step,
             "records_completed": completed,
-            "records_failed_nonconvergence": args.frames * world - completed,
+            "records_failed_nonconvergence": total_frames - completed,
             "fiber_state_updates_per_s": fiber_updates_per_s,
-            "simulated_s_per_wall_s": args.frames * args.record_steps * DT / (times[-1] / 1000.0),
+            "simulated_s_per_wall_s": total_frames * args.record_steps * DT / (ms_per_step / 1000.0),
+            "fanned_out_determinations": int(st.fanned_out),
             "e2e": {"value": e2e_value, "unit": "records/hour", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"kernel": "element_state_kernel", "bound": "hbm", "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": traffic,
-                         "launches": int(P.launches[A.PROF_ELEMENT]),
-                         "avg_launch_ms": el_ms / el_launch},
+                    "d2h_bytes_per_step": int(d2h), "repetitions": len(e2e_times)},
+            "roofline": roofline,
+            "commit_kernel": commit_roof,
             "kernel_ms": kernel_share,
             # launches of one analysis (profiled run, same workload) x timed analyses; the
             # displacement-record kernel runs once per step
             "gpu_launches": int(args.steps * (sum(P.launches[i] for i in range(5)) + st.steps_done)),
             "clocks": clk.summary(),
         }
+        if fiber:
+            line["fiber_kernel"] = fiber
         if learned:
             learned["vs_plain"] = learned["value"] / value if value else None
             line["learned"] = learned

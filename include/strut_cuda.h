@@ -434,7 +434,11 @@ int strut_gpu_predictor_features(StrutHandle* h, float* out);
  * Every call on a device shares the buffer, so calls whose kernels may overlap on the GPU
  * (unordered streams) race and must be serialised by the caller.  The first call on a device
  * looks up the buffer's address and sets the kernel's shared-memory limit; make it before any
- * stream capture.  Returns after the launch (asynchronous). */
+ * stream capture.  Those addresses belong to the device's context as it was then: after a
+ * cudaDeviceReset in the same process this entry point is not supported.  Both systems are
+ * held in shared memory in the general n x (2*half_bw+1) layout (BandSPD's lower band expanded
+ * into it), so one shared-memory limit, (n (2 half_bw + 1) + 4 n) doubles within the device's
+ * opt-in limit, applies to both.  Returns after the launch (asynchronous). */
 int strut_gpu_band_solve_noalloc(const double* band_dev, int32_t n, int32_t half_bw,
                                  int32_t system, const double* rhs_dev, double* x_dev,
                                  int32_t* status_dev, void* stream);

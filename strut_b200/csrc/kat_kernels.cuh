@@ -89,7 +89,7 @@ struct BatchState {
     int* kon;
     double* s1;
     double* c1;
-    long long n_inst;
+    long long n_inst;  // instances with allocated state: the field stride is n_inst x family size
 };
 
 __global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd, BatchState bs,

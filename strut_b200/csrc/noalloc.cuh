@@ -93,6 +93,7 @@ namespace {
 struct NoAllocDevice {
     double* dense = nullptr;  // device address of g_noalloc_dense on this device
     int* piv = nullptr;       // device address of g_noalloc_piv on this device
+    size_t smem_limit = 0;    // dynamic shared memory the kernel may use on this device
     bool ready = false;
 };
 constexpr int kNoAllocMaxDevices = 64;
@@ -114,24 +115,31 @@ extern "C" int strut_gpu_band_solve_noalloc(const double* band_dev, int32_t n, i
     if (!band_dev || !rhs_dev || !x_dev || !status_dev) return fail(STRUT_BAD_ARG, "null pointer");
     const int rw = 2 * half_bw + 1;
     const size_t smem = ((size_t)n * rw + 4 * (size_t)n) * sizeof(double);
-    if (smem > strut::kNoAllocSmemMax)
-        return fail(STRUT_UNSUPPORTED, "n x (2*half_bw+1) band does not fit in shared memory");
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(STRUT_UNSUPPORTED, "device index too large");
     NoAllocDevice& D = g_noalloc[dev];
     {
         // first call on this device (its context current): look up the scratch's device
-        // addresses and raise the kernel's shared-memory limit; later calls reuse them
+        // addresses and raise the kernel's shared-memory limit to what the device allows next
+        // to the kernel's static shared memory; later calls reuse them
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
         if (!D.ready) {
             CK(cudaGetSymbolAddress((void**)&D.dense, strut::g_noalloc_dense));
             CK(cudaGetSymbolAddress((void**)&D.piv, strut::g_noalloc_piv));
+            int optin = 0;
+            CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            cudaFuncAttributes fa;
+            CK(cudaFuncGetAttributes(&fa, strut::band_solve_one_kernel));
+            const size_t room = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+            D.smem_limit = std::min(strut::kNoAllocSmemMax, room);
             CK(cudaFuncSetAttribute(strut::band_solve_one_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)strut::kNoAllocSmemMax));
+                                    (int)D.smem_limit));
             D.ready = true;
         }
     }
+    if (smem > D.smem_limit)
+        return fail(STRUT_UNSUPPORTED, "n x (2*half_bw+1) band does not fit in shared memory");
     strut::band_solve_one_kernel<<<1, 256, smem, (cudaStream_t)stream>>>(
         band_dev, n, half_bw, system == STRUT_SYSTEM_BAND_SPD ? 1 : 0, rhs_dev, x_dev, status_dev, D.dense,
         D.piv);

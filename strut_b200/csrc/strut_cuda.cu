@@ -25,6 +25,7 @@
 #include "strut_cuda.h"
 #include "element_kernels.cuh"
 #include "kat_kernels.cuh"
+#include "fiber_stream_kernels.cuh"
 #include "solver_kernels.cuh"
 #include "largeband_kernels.cuh"
 #include "shell_kernels.cuh"
@@ -1918,10 +1919,17 @@ int strut_gpu_revert(StrutHandle* h) {
 // ---------------------------------------------------------------------------------------
 struct StrutSectionBatch {
     int n_inst = 0;
+    long long n_alloc = 0;  // instances with allocated state (a whole number of tiles)
     std::vector<void*> allocs;
     Geo geo;
     DevSection sd;
     BatchState bs;
+    // streaming kernel: instances per tile (L.T 0: the section does not fit, one warp per instance)
+    FsLayout L{};
+    long long n_tiles = 0;
+    int grid = 1;
+    size_t smem = 0;
+    int* d_err = nullptr;
     ~StrutSectionBatch() {
         for (void* p : allocs) cudaFree(p);
     }
@@ -2017,15 +2025,44 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
     b->geo.m = d_m;
     b->geo.mats = d_mats;
     b->geo.secs = d_secs;
+    // tile of the streaming kernel: the most instances (a multiple of 4, at most 16) whose two
+    // stages and per-fiber results fit the shared memory a CTA can opt into
+    {
+        int dev = 0, optin = 0, n_sm = 1;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+        const size_t cap = (size_t)optin > 2048 ? (size_t)optin - 2048 : 0;  // room for static shared memory
+        int T = 0;
+        for (int t = 16; t >= 4; t -= 4)
+            if (fs_smem_bytes(fs_layout(b->sd, t)) <= cap) {
+                T = t;
+                break;
+            }
+        if (T > 0) {
+            b->L = fs_layout(b->sd, T);
+            b->n_tiles = (n_inst + T - 1) / T;
+            b->n_alloc = b->n_tiles * T;
+            b->smem = fs_smem_bytes(b->L);
+            b->grid = (int)std::min<long long>(b->n_tiles, n_sm);
+            CK(cudaFuncSetAttribute(fiber_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        } else {
+            b->n_alloc = n_inst;
+        }
+    }
     std::vector<double> s2, c2, s1, c1;
     std::vector<int> kon;
-    batch_initial_state(sp, mats, n_inst, s2, c2, s1, c1, kon);
+    batch_initial_state(sp, mats, b->n_alloc, s2, c2, s1, c1, kon);
     if ((rc = upload(&b->bs.s2, s2, al)) || (rc = upload(&b->bs.c2, c2, al)) || (rc = upload(&b->bs.s1, s1, al)) ||
         (rc = upload(&b->bs.c1, c1, al)) || (rc = upload(&b->bs.kon, kon, al))) {
         delete b;
         return rc;
     }
-    b->bs.n_inst = n_inst;
+    b->bs.n_inst = b->n_alloc;
+    if ((rc = dzeros(&b->d_err, 1, al))) {
+        delete b;
+        return rc;
+    }
     *out = b;
     return STRUT_OK;
 }
@@ -2040,10 +2077,17 @@ int strut_gpu_section_batch_destroy(StrutSectionBatch* b) {
 int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_dev, double* resp_dev,
                                  int32_t commit, void* stream) {
     if (!b || !eps0_kappa_dev || !resp_dev) return fail(STRUT_BAD_ARG, "bad arguments");
-    const long long threads = (long long)b->n_inst * 32;
-    const int tb = 256;
-    section_batch_kernel<<<(unsigned)((threads + tb - 1) / tb), tb, 0, (cudaStream_t)stream>>>(
-        b->geo, b->sd, b->bs, eps0_kappa_dev, resp_dev, commit ? 1 : 0);
+    if (b->L.T > 0) {
+        fiber_stream_kernel<<<b->grid, kFsThreads, b->smem, (cudaStream_t)stream>>>(
+            b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, b->n_tiles, eps0_kappa_dev, resp_dev, commit ? 1 : 0,
+            b->d_err);
+    } else {
+        // a section too large for the streaming kernel's tiles: one warp per instance
+        const long long threads = (long long)b->n_inst * 32;
+        const int tb = 256;
+        section_batch_kernel<<<(unsigned)((threads + tb - 1) / tb), tb, 0, (cudaStream_t)stream>>>(
+            b->geo, b->sd, b->bs, eps0_kappa_dev, resp_dev, commit ? 1 : 0);
+    }
     CK(cudaGetLastError());
     return STRUT_OK;
 }
@@ -2055,10 +2099,15 @@ int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double
     if (n_fibers) *n_fibers = nf;
     if (!out) return STRUT_OK;
     CK(cudaDeviceSynchronize());
+    {
+        int err = 0;
+        CK(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) return fail(STRUT_CUDA_ERROR, "a bulk copy of the streaming fiber kernel did not complete");
+    }
     // 16 doubles per fiber: the family's committed fields in declaration order, kon in slot 15
     std::vector<double> o((size_t)nf * 16, 0.0);
-    const long long n2 = (long long)b->n_inst * sd.n_s2, n3 = (long long)b->n_inst * sd.n_c2,
-                    n1 = (long long)b->n_inst * sd.n_s1, n4 = (long long)b->n_inst * sd.n_c1;
+    const long long n2 = b->n_alloc * sd.n_s2, n3 = b->n_alloc * sd.n_c2,
+                    n1 = b->n_alloc * sd.n_s1, n4 = b->n_alloc * sd.n_c1;
     for (int j = 0; j < sd.n_s2; ++j) {
         for (int f = 0; f < 10; ++f)
             CK(cudaMemcpy(&o[(size_t)j * 16 + f], b->bs.s2 + f * n2 + (long long)instance * sd.n_s2 + j, sizeof(double),

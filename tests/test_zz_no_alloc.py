@@ -102,3 +102,49 @@ def test_noalloc_rejects_sizes_beyond_scratch(gpu_lib):
                                                     None)
     assert rc == A.STRUT_BAD_ARG
     assert b"static scratch" in gpu_lib.lib().strut_gpu_last_error()
+
+
+def test_noalloc_dense_fallback_at_the_largest_order(gpu_lib):
+    """n = 512, the largest order the static scratch holds, through the dense fallback."""
+    rng = np.random.default_rng(21)
+    n, bw = 512, 3
+    band = np.zeros((n, 2 * bw + 1))
+    K = np.zeros((n, n))
+    for i in range(n):
+        for j in range(max(0, i - bw), min(n, i + bw + 1)):
+            K[i, j] = rng.standard_normal() + (5.0 if i == j else 0.0)
+    K[300, 299] = 80.0  # sends the factorisation to the dense partial-pivot LU
+    for i in range(n):
+        for j in range(max(0, i - bw), min(n, i + bw + 1)):
+            band[i, j - i + bw] = K[i, j]
+    rhs = rng.standard_normal(n)
+    ref = np.linalg.solve(K, rhs)
+    for st, x in _solve_noalloc(gpu_lib, band, n, bw, A.SYSTEM_BAND_GENERAL, rhs):
+        assert st == 0
+        assert np.abs(x - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+def test_noalloc_reports_singular_and_not_positive_definite(gpu_lib):
+    """Status 2 on the device: a BandGeneral system with a zero column (singular in the band LU
+    and in its dense fallback) and a BandSPD system with a negative diagonal."""
+    n, bw = 30, 2
+    gen = np.zeros((n, 2 * bw + 1))
+    spd = np.zeros((n, bw + 1))
+    for i in range(n):
+        gen[i, bw] = 4.0
+        spd[i, 0] = 4.0
+        for o in range(1, bw + 1):
+            if i - o >= 0:
+                gen[i, bw - o] = -1.0
+                spd[i, o] = -1.0
+            if i + o < n:
+                gen[i, bw + o] = -1.0
+    for i in range(n):  # column 7 of the general matrix is zero
+        if abs(7 - i) <= bw:
+            gen[i, 7 - i + bw] = 0.0
+    spd[11, 0] = -4.0
+    rhs = np.ones(n)
+    for st, _x in _solve_noalloc(gpu_lib, gen, n, bw, A.SYSTEM_BAND_GENERAL, rhs):
+        assert st == A.STRUT_SINGULAR
+    for st, _x in _solve_noalloc(gpu_lib, spd, n, bw, A.SYSTEM_BAND_SPD, rhs):
+        assert st == A.STRUT_SINGULAR
