@@ -321,6 +321,12 @@ typedef struct StrutTuning {
 } StrutTuning;
 int strut_gpu_set_tuning(StrutHandle* h, const StrutTuning* t);
 int strut_gpu_get_tuning(const StrutHandle* h, StrutTuning* out);
+/* How many times a CTA of the cooperative wide-band factorisation polls a grid barrier before it
+ * gives up (default 4194304); when one gives up, every CTA of the launch returns and the
+ * instance ends with STRUT_CUDA_ERROR instead of the GPU waiting for good.  No counterpart in the
+ * reference: failure-detection tests set it to 0 to make the wait run out on purpose.  A handle
+ * without a wide band ignores it. */
+int strut_gpu_set_wait_limit(StrutHandle* h, int32_t polls);
 
 /* ---- single-iteration entries (parity tests) --------------------------------------- */
 /* Sets the trial free displacements of every instance (concatenated in instance order),

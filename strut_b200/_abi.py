@@ -245,6 +245,7 @@ EXPORTS = {
     "strut_gpu_stream": (C.c_void_p, [C.c_void_p]),
     "strut_gpu_set_tuning": (C.c_int, [C.c_void_p, C.c_void_p]),
     "strut_gpu_get_tuning": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "strut_gpu_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int32]),
     "strut_gpu_state_determination": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "strut_gpu_band_info": (C.c_int, [C.c_void_p, C.c_int32, _ip, _ip]),
     "strut_gpu_factor_solve": (C.c_int, [C.c_void_p, _dp, _dp]),

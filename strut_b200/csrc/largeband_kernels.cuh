@@ -45,11 +45,16 @@ struct GridBarrier {
     unsigned int gen;
     int err;
     int pad;
+    int limit;  // polls a waiting CTA makes before it gives up (strut_gpu_set_wait_limit)
+    int pad2;
 };
+
+constexpr int kBarrierPolls = 1 << 22;
 
 // Grid-wide barrier of a cooperative launch.  Thread 0 of each CTA arrives; the last arrival
 // resets the count and advances the generation; the others wait for the generation to move,
-// for a bounded number of polls, after which the barrier records an error and every CTA stops.
+// for a bounded number of polls (gb->limit), after which the barrier records an error and every
+// CTA stops.
 __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, unsigned int& gen) {
     __syncthreads();
     int ok = 1;
@@ -63,8 +68,9 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, unsigned int& gen)
             atomicAdd(&gb->gen, 1u);
         } else {
             int polls = 0;
+            const int limit = *(volatile int*)&gb->limit;
             while (atomicAdd(&gb->gen, 0u) == g) {
-                if (++polls > (1 << 22) || atomicAdd(&gb->err, 0) != 0) {
+                if (++polls > limit || atomicAdd(&gb->err, 0) != 0) {
                     atomicExch(&gb->err, 1);
                     ok = 0;
                     break;

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1441,6 +1442,10 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             (rc = dzeros(&h->d_lpan, (size_t)kPanel * kLargeThreads, al)) ||
             (rc = dzeros(&h->d_lpiv, (size_t)kLargeThreads, al)))
             return bail(rc);
+        {
+            const int polls = kBarrierPolls;
+            CK(cudaMemcpy((char*)h->d_gb + offsetof(GridBarrier, limit), &polls, sizeof(int), cudaMemcpyHostToDevice));
+        }
         CK(cudaFuncSetAttribute(large_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)h->lfactor_smem));
         int per_sm = 0, n_sm = 0;
@@ -1802,6 +1807,14 @@ int strut_gpu_set_tuning(StrutHandle* h, const StrutTuning* t) {
     }
     h->lfactor_grid = d.factor_ctas > 0 ? std::min(d.factor_ctas, h->max_factor_grid) : h->default_factor_grid;
     h->tune_gen += 1;
+    return STRUT_OK;
+}
+
+int strut_gpu_set_wait_limit(StrutHandle* h, int32_t polls) {
+    if (!h || polls < 0) return fail(STRUT_BAD_ARG, "bad arguments");
+    if (!h->d_gb) return STRUT_OK;  // no cooperative factorisation in this handle
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy((char*)h->d_gb + offsetof(GridBarrier, limit), &polls, sizeof(int), cudaMemcpyHostToDevice));
     return STRUT_OK;
 }
 
