@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--tall-steps", type=int, default=4000,
                     help="timed steps of the 4000-step large 3D frame record (default: all)")
     ap.add_argument("--no-fiber", action="store_true", help="skip the streaming fiber-kernel measurement")
+    ap.add_argument("--autotune", action="store_true",
+                    help="search the launch shapes on the whole batch, record them in "
+                         "strut_b200/tuned_shapes.json, print the result and exit")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="N > 1: every rank its own 256 frames (weak) or one batch partitioned (strong)")
     ap.add_argument("--profile-only", action="store_true",
@@ -454,8 +457,17 @@ def main():
                               "frames": len(models), "steps": min(50, args.record_steps)}))
         return 0
 
+    from strut_b200 import autotune
+
+    if args.autotune:
+        key, best, times = autotune.tune(models, args.record_steps, device=device, save=rank == 0)
+        if rank == 0:
+            print(json.dumps({"autotune": {"class": key, "best": best, "ms": times}}), flush=True)
+        return 0
+
     def one_analysis(prof=False):
         an = runtime.Analysis(models, device=device)
+        autotune.apply(an)
         if prof:
             runtime.lib().strut_gpu_set_profiling(an.h, 1)
         stream = torch.cuda.ExternalStream(runtime.lib().strut_gpu_stream(an.h))
@@ -598,7 +610,9 @@ def main():
                        "parallelism": (f"partition{world}" if args.scaling == "strong" and world > 1
                                        else f"replicas{world}"),
                        "tuned": {"fan_out": int(tuned.fan_out), "commit_team": int(tuned.commit_team),
-                                 "element_threads": int(tuned.element_threads)},
+                                 "element_threads": int(tuned.element_threads),
+                                 "source": ("strut_b200/tuned_shapes.json" if autotune.lookup(models, False)
+                                            else "defaults")},
                        "l2": "fiber history of the batch exceeds L2 (no flush needed)"},
             "newton_its_per_step": newton_per_step,
             "records_completed": completed,
