@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define STRUT_ABI_VERSION 5
+#define STRUT_ABI_VERSION 6
 #define STRUT_MAX_INT_PTS 10
 
 /* Status codes.  No entry point aborts the process. */
@@ -171,6 +171,17 @@ typedef struct StrutShellElement {
     double E, nu, h;
 } StrutShellElement;
 
+/* One attempt of a step's solver chain (SolverAttemptInput, input_types.mojo; the retry loop of
+ * transient_nonlinear.mojo:1925-1942).  algorithm STRUT_ALGORITHM_*, test_type STRUT_TEST_*. */
+#define STRUT_MAX_ATTEMPTS 4
+typedef struct StrutSolverAttempt {
+    int32_t algorithm;
+    int32_t test_type;
+    int32_t max_iters;
+    int32_t reserved;
+    double tol;
+} StrutSolverAttempt;
+
 /* One analysis instance (one frame + one record). */
 typedef struct StrutModelDesc {
     int32_t ndm;                 /* 2 (ndf 3) or 3 (ndf 6)                               */
@@ -224,6 +235,15 @@ typedef struct StrutModelDesc {
     int32_t num_shells;
     int32_t reserved_shell;
     const StrutShellElement* shells;
+    /* solver chain (analysis.solver_chain; transient_nonlinear.mojo:758-830, 1925-1942): when a
+     * step does not converge with attempt k, u, the elements' basic state and the fibers' trial
+     * state go back to the step's start (its Newmark predictor) and attempt k + 1 runs; the step
+     * fails when the last attempt does.  num_attempts 0: the chain is the primary settings
+     * (algorithm, test_type, max_iters, tol) followed, when the algorithm is not Newton, by Newton
+     * with the same test, iterations and tolerance (Strut's automatic fallback, 804-829). */
+    int32_t num_attempts;          /* 0 .. STRUT_MAX_ATTEMPTS                              */
+    int32_t reserved_attempts;
+    StrutSolverAttempt attempts[STRUT_MAX_ATTEMPTS];
 } StrutModelDesc;
 
 /* Per-run statistics (RuntimeProfileMetrics counters, solver/profile.mojo:37-74). */

@@ -861,8 +861,10 @@ static int initial_assembly(OModel* m) {
     int rc = assemble(m, 0, 0);
     if (rc != STRUT_OK) return rc;
     size_t bsz = (size_t)m->n * m->rw;
-    if (m->d->beta_k_init != 0.0 || m->d->algorithm == STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL)
-        memcpy(m->Kinit, m->K, sizeof(double) * bsz);
+    int initial_tangent = m->d->algorithm == STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL;
+    for (int k = 0; k < m->d->num_attempts; ++k)
+        if (m->d->attempts[k].algorithm == STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL) initial_tangent = 1;
+    if (m->d->beta_k_init != 0.0 || initial_tangent) memcpy(m->Kinit, m->K, sizeof(double) * bsz);
     if (m->d->beta_k_comm != 0.0) memcpy(m->Kcomm, m->K, sizeof(double) * bsz);
     for (int e = 0; e < m->d->num_elements; ++e)
         for (int ip = 0; ip < m->elems[e].nip; ++ip) oracle_section_revert(&m->elems[e].sst[ip]);
@@ -910,8 +912,72 @@ static int record_step(OModel* m, int step, double* disp_hist, double* eforce_hi
     return STRUT_OK;
 }
 
+/* The step's solver chain (transient_nonlinear.mojo:758-830): the attempts as given, or the
+ * primary settings followed by Newton when the primary algorithm is not Newton. */
+static int resolve_chain(const StrutModelDesc* d, StrutSolverAttempt* at) {
+    if (d->num_attempts > 0) {
+        for (int k = 0; k < d->num_attempts; ++k) at[k] = d->attempts[k];
+        return d->num_attempts;
+    }
+    at[0].algorithm = d->algorithm;
+    at[0].test_type = d->test_type;
+    at[0].max_iters = d->max_iters;
+    at[0].tol = d->tol;
+    if (d->algorithm == STRUT_ALGORITHM_NEWTON) return 1;
+    at[1] = at[0];
+    at[1].algorithm = STRUT_ALGORITHM_NEWTON;
+    return 2;
+}
+
+/* The force_basic_q blocks of every element (2D: q, eps0, kappa, v; 3D: q5, eps0, ky, kz),
+ * saved at a step's start and put back before a retry (transient_nonlinear.mojo:1925-1942). */
+typedef struct {
+    double q[3], eps0[STRUT_MAX_INT_PTS], kappa[STRUT_MAX_INT_PTS], v[3];
+    double q5[5], ky[STRUT_MAX_INT_PTS], kz[STRUT_MAX_INT_PTS];
+} OBasicState;
+
+static void basic_save(const OElement* e, OBasicState* b) {
+    memcpy(b->q, e->q, sizeof(b->q));
+    memcpy(b->eps0, e->eps0, sizeof(b->eps0));
+    memcpy(b->kappa, e->kappa, sizeof(b->kappa));
+    memcpy(b->v, e->v, sizeof(b->v));
+    memcpy(b->q5, e->q5, sizeof(b->q5));
+    memcpy(b->ky, e->ky, sizeof(b->ky));
+    memcpy(b->kz, e->kz, sizeof(b->kz));
+}
+
+static void basic_restore(OElement* e, const OBasicState* b) {
+    memcpy(e->q, b->q, sizeof(b->q));
+    memcpy(e->eps0, b->eps0, sizeof(b->eps0));
+    memcpy(e->kappa, b->kappa, sizeof(b->kappa));
+    memcpy(e->v, b->v, sizeof(b->v));
+    memcpy(e->q5, b->q5, sizeof(b->q5));
+    memcpy(e->ky, b->ky, sizeof(b->ky));
+    memcpy(e->kz, b->kz, sizeof(b->kz));
+}
+
+static int run_steps_chain(OModel* m, int steps, double* disp_hist, double* eforce_hist,
+                           int* iters_hist, int* failed_step, const StrutSolverAttempt* chain,
+                           int n_att, OBasicState* base, double* u_base);
+
 static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_hist,
                      int* iters_hist, int* failed_step) {
+    const StrutModelDesc* d = m->d;
+    StrutSolverAttempt chain[STRUT_MAX_ATTEMPTS];
+    const int n_att = resolve_chain(d, chain);
+    OBasicState* base = n_att > 1 ? (OBasicState*)calloc((size_t)(d->num_elements > 0 ? d->num_elements : 1),
+                                                         sizeof(OBasicState)) : 0;
+    double* u_base = n_att > 1 ? (double*)calloc((size_t)(m->n > 0 ? m->n : 1), sizeof(double)) : 0;
+    int rc_out = run_steps_chain(m, steps, disp_hist, eforce_hist, iters_hist, failed_step, chain, n_att,
+                                 base, u_base);
+    free(base);
+    free(u_base);
+    return rc_out;
+}
+
+static int run_steps_chain(OModel* m, int steps, double* disp_hist, double* eforce_hist,
+                           int* iters_hist, int* failed_step, const StrutSolverAttempt* chain,
+                           int n_att, OBasicState* base, double* u_base) {
     const StrutModelDesc* d = m->d;
     int n = m->n;
     double dt = d->dt, beta = d->beta, gamma = d->gamma;
@@ -971,8 +1037,25 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
             }
         }
         int converged = 0;
-        int it;
-        for (it = 0; it < d->max_iters; ++it) {
+        int it = 0, step_iters = 0;
+        if (n_att > 1) {
+            for (int e = 0; e < d->num_elements; ++e) basic_save(&m->elems[e], &base[e]);
+            memcpy(u_base, m->u_f, sizeof(double) * n);
+        }
+        for (int att = 0; att < n_att && !converged; ++att) {
+        const int alg = chain[att].algorithm, test = chain[att].test_type, max_iters = chain[att].max_iters;
+        const double tol = chain[att].tol;
+        if (att > 0) {
+            /* back to the step's start: u at the predictor, basic states, fiber trial states */
+            memcpy(m->u_f, u_base, sizeof(double) * n);
+            scatter_u(m);
+            for (int e = 0; e < d->num_elements; ++e) {
+                OElement* el = &m->elems[e];
+                basic_restore(el, &base[e]);
+                for (int ip = 0; ip < el->nip; ++ip) oracle_section_revert(&el->sst[ip]);
+            }
+        }
+        for (it = 0; it < max_iters; ++it) {
             m->newton_iters++;
             int rc = assemble(m, 0, 0);
             if (rc != STRUT_OK) {
@@ -982,9 +1065,9 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
             /* Newton refreshes K_ff, C_ff and the factors every iteration; ModifiedNewton keeps
              * the first iteration's for the step, ModifiedNewtonInitial takes K_init_ff
              * (transient_nonlinear.mojo:2072-2085, 2236-2268, 2302-2335, 2421-2440) */
-            const int refresh = d->algorithm == STRUT_ALGORITHM_NEWTON || it == 0;
+            const int refresh = alg == STRUT_ALGORITHM_NEWTON || it == 0;
             if (refresh) {
-                if (d->algorithm == STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL)
+                if (alg == STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL)
                     memcpy(m->K, m->Kinit, sizeof(double) * (size_t)n * m->rw);
                 rc = build_keff(m);
                 if (rc != STRUT_OK) {
@@ -1008,8 +1091,8 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
                 const double fint = m->has_mpc ? m->Fred[dof] : m->Fint[dof];
                 m->R_f[i] = m->P_f[i] - fint - 0.0 - damping - inertia;
             }
-            if (d->test_type == STRUT_TEST_NORM_UNBALANCE) {
-                if (sqrt(simd_sumsq(m->R_f, n)) <= d->tol) {
+            if (test == STRUT_TEST_NORM_UNBALANCE) {
+                if (sqrt(simd_sumsq(m->R_f, n)) <= tol) {
                     converged = 1;
                     break;
                 }
@@ -1038,20 +1121,22 @@ static int run_steps(OModel* m, int steps, double* disp_hist, double* eforce_his
                 if (failed_step) *failed_step = step;
                 return STRUT_NAN;
             }
-            if (d->test_type == STRUT_TEST_NORM_DISP_INCR && norm <= d->tol) {
+            if (test == STRUT_TEST_NORM_DISP_INCR && norm <= tol) {
                 converged = 1;
                 break;
             }
-            if (d->test_type == STRUT_TEST_ENERGY_INCR && energy <= d->tol) {
+            if (test == STRUT_TEST_ENERGY_INCR && energy <= tol) {
                 converged = 1;
                 break;
             }
-            if (d->test_type == STRUT_TEST_MAX_DISP_INCR && max_diff <= d->tol) {
+            if (test == STRUT_TEST_MAX_DISP_INCR && max_diff <= tol) {
                 converged = 1;
                 break;
             }
         }
-        if (iters_hist) iters_hist[step] = converged ? it + 1 : d->max_iters;
+        step_iters += converged ? it + 1 : max_iters;
+        }
+        if (iters_hist) iters_hist[step] = step_iters;
         if (!converged) {
             if (failed_step) *failed_step = step;
             return STRUT_NONCONVERGED;

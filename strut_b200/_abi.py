@@ -132,6 +132,19 @@ class StrutExcitation(C.Structure):
     ]
 
 
+MAX_ATTEMPTS = 4
+
+
+class StrutSolverAttempt(C.Structure):
+    _fields_ = [
+        ("algorithm", C.c_int32),
+        ("test_type", C.c_int32),
+        ("max_iters", C.c_int32),
+        ("reserved", C.c_int32),
+        ("tol", C.c_double),
+    ]
+
+
 class StrutModelDesc(C.Structure):
     _fields_ = [
         ("ndm", C.c_int32),
@@ -180,6 +193,9 @@ class StrutModelDesc(C.Structure):
         ("num_shells", C.c_int32),
         ("reserved_shell", C.c_int32),
         ("shells", C.POINTER(StrutShellElement)),
+        ("num_attempts", C.c_int32),
+        ("reserved_attempts", C.c_int32),
+        ("attempts", StrutSolverAttempt * MAX_ATTEMPTS),
     ]
 
 

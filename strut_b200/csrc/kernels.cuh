@@ -100,6 +100,17 @@ struct DevInst {
     int lrw, pad_l;       // slots per row of that band (3 bw + 1)
     int algorithm, pad_al; // STRUT_ALGORITHM_* (Newton, ModifiedNewton, ModifiedNewtonInitial)
     int sl_off, n_sl;     // this instance's slave dofs (multi-point constraints)
+    // solver chain (transient_nonlinear.mojo:758-830, 1925-1942): attempt k's algorithm, test,
+    // iteration limit and tolerance; attempt 0 is (algorithm, test_type, max_iters, tol)
+    int n_att, pad_att;
+    int att_alg[4], att_test[4], att_maxit[4];
+    double att_tol[4];
+};
+
+// The solver settings of an instance's current attempt.
+struct Attempt {
+    int alg, test, max_iters;
+    double tol;
 };
 
 // Elements of the instances still iterating, rebuilt every Newton iteration and double

@@ -265,13 +265,14 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
         const int n = I.n, bw = I.bw, lrw = I.lrw;
         double* B = A.lband + I.lband_off;
         double* w = wbuf + I.f_off;
-        if (mode == INST_MODE_NEWTON && I.test_type == 2) {
+        const Attempt at = attempt_of(I, A, inst);
+        if (mode == INST_MODE_NEWTON && at.test == 2) {
             // NormUnbalance is tested on the residual before the solve; every CTA reaches the
             // same decision from the same sums
             double s = 0.0;
             for (int i = tid; i < n; i += nt) s += A.R[I.f_off + i] * A.R[I.f_off + i];
             s = block_sum(s, red);
-            if (sqrt(s) <= I.tol) {
+            if (sqrt(s) <= at.tol) {
                 if (blockIdx.x == 0 && tid == 0) A.lstatus[li] = LSTAT_CONVERGED;
                 continue;
             }
@@ -559,7 +560,7 @@ __global__ void __launch_bounds__(kSolveThreads) large_solve_kernel(
         if (tid == 0) {
             A.active[inst] = 0;
             atomicSub(A.nactive, 1);
-            if (hrow) hrow[inst] = A.iters[inst];
+            if (hrow) hrow[inst] = A.iters[inst] + (A.iters_prev ? A.iters_prev[inst] : 0);
         }
         return;
     }

@@ -118,8 +118,9 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
         return fail(STRUT_UNSUPPORTED, "the learned predictor does not run with multi-point constraints");
     if (h->n_shells > 0) return fail(STRUT_UNSUPPORTED, "the learned predictor does not run with shells");
     for (const DevInst& I : h->insts)
-        if (I.algorithm != STRUT_ALGORITHM_NEWTON)
-            return fail(STRUT_UNSUPPORTED, "the learned predictor runs with the Newton algorithm");
+        for (int k = 0; k < I.n_att; ++k)
+            if (I.att_alg[k] != STRUT_ALGORITHM_NEWTON)
+                return fail(STRUT_UNSUPPORTED, "the learned predictor runs with the Newton algorithm");
     const int ndf = h->pn_ndf, n_in = 4 * ndf + 17;
     if (m->n_in != n_in || m->n_out != ndf)
         return fail(STRUT_BAD_ARG, "network must take " + std::to_string(n_in) + " features and give " +

@@ -75,10 +75,26 @@ struct InstArrays {
     double* kfrz;
     double* lufrz;
     int* lu_dense;
+    // solver chain: current attempt and the iterations of earlier attempts of the step, per
+    // instance; the predictor's displacements and the element state at the step's start
+    int* attempt;
+    int* iters_prev;
+    double* u_base;
+    double* estate_base;
     double* lband;          // effective band (factored in place), at DevInst::lband_off
     int* lstatus;           // per large instance: 0 factored, 2 singular, 6 dense fallback,
                             // 7 converged before the solve (NormUnbalance), -1 not active
 };
+
+__device__ __forceinline__ Attempt attempt_of(const DevInst& I, const InstArrays& A, int inst) {
+    const int k = A.attempt ? A.attempt[inst] : 0;
+    Attempt a;
+    a.alg = I.att_alg[k];
+    a.test = I.att_test[k];
+    a.max_iters = I.att_maxit[k];
+    a.tol = I.att_tol[k];
+    return a;
+}
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
     v = warp_sum(v);
@@ -510,7 +526,8 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     // ModifiedNewton(Initial): the first iteration of the step freezes the tangent (the current
     // one, or K_init) and factors; later iterations reuse both (transient_nonlinear.mojo:
     // 2072-2085, 2236-2268, 2302-2335, 2421-2440)
-    const bool modified = mode == INST_MODE_NEWTON && I.algorithm != 0;
+    const Attempt at = attempt_of(I, A, inst);
+    const bool modified = mode == INST_MODE_NEWTON && at.alg != 0;
     const bool refresh = !modified || s_it == 0;
     double* Kfz = modified ? A.kfrz + I.band_off : nullptr;
     if (mode == INST_MODE_SOLVE_EXPORTED) {
@@ -545,7 +562,7 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
                     if (!modified) {
                         K = gather_slot(A, sp0, slot);
                     } else if (refresh) {
-                        K = I.algorithm == 2 ? Kinit[slot] : gather_slot(A, sp0, slot);
+                        K = at.alg == 2 ? Kinit[slot] : gather_slot(A, sp0, slot);
                         Kfz[slot] = K;
                     } else {
                         K = Kfz[slot];
@@ -621,15 +638,15 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
             for (int t = tid; t < n * rw; t += nt) A.export_band[I.band_off + t] = Kb[t];
             return;
         }
-        if (I.test_type == 2) {  // NormUnbalance before the solve
+        if (at.test == 2) {  // NormUnbalance before the solve
             double s = 0.0;
             for (int i = tid; i < n; i += nt) s += R[i] * R[i];
             s = block_sum(s, red);
-            if (sqrt(s) <= I.tol) {
+            if (sqrt(s) <= at.tol) {
                 if (tid == 0) {
                     A.active[inst] = 0;
                     atomicSub(A.nactive, 1);
-                    if (hrow) hrow[inst] = A.iters[inst];
+                    if (hrow) hrow[inst] = A.iters[inst] + (A.iters_prev ? A.iters_prev[inst] : 0);
                 }
                 return;
             }
@@ -739,31 +756,60 @@ __device__ void newton_tail(const DevInst& I, InstArrays& A, int inst, const dou
     const double norm = sqrt(block_sum(ss, red));
     const double energy = fabs(block_sum(en, red));
     const double maxd = block_max(mx, red);
+    const Attempt at = attempt_of(I, A, inst);
     if (tid == 0) {
         bool conv = false;
-        if (I.test_type == 1) conv = norm <= I.tol;
-        else if (I.test_type == 3) conv = energy <= I.tol;
-        else if (I.test_type == 0) conv = maxd <= I.tol;
+        if (at.test == 1) conv = norm <= at.tol;
+        else if (at.test == 3) conv = energy <= at.tol;
+        else if (at.test == 0) conv = maxd <= at.tol;
         if (!isfinite(norm)) {
             A.status[inst] = 3;
             conv = true;
         }
-        int base = -1;
+        const int prev = A.iters_prev ? A.iters_prev[inst] : 0;
+        int base = -1, retry = 0, failed = 0;
         if (conv) {
             A.active[inst] = 0;
             atomicSub(A.nactive, 1);
-            if (hrow) hrow[inst] = A.iters[inst];
-        } else if (A.iters[inst] >= I.max_iters) {
-            A.status[inst] = 1;
-            A.active[inst] = 0;
-            atomicSub(A.nactive, 1);
-            if (hrow) hrow[inst] = A.iters[inst];
-        } else if (A.ctl) {
-            base = atomicAdd(&A.el.count[(A.ctl->iter + 1) & 1], I.n_elem);
+            if (hrow) hrow[inst] = A.iters[inst] + prev;
+        } else if (A.iters[inst] >= at.max_iters) {
+            if (A.attempt && A.attempt[inst] + 1 < I.n_att) {
+                // the next attempt of the chain, from the step's start
+                A.attempt[inst] += 1;
+                A.iters_prev[inst] = prev + A.iters[inst];
+                A.iters[inst] = 0;
+                retry = 1;
+            } else {
+                A.status[inst] = 1;
+                A.active[inst] = 0;
+                atomicSub(A.nactive, 1);
+                if (hrow) hrow[inst] = A.iters[inst] + prev;
+                failed = 1;
+            }
         }
+        if (!conv && !failed && A.ctl)
+            base = atomicAdd(&A.el.count[(A.ctl->iter + 1) & 1], I.n_elem);
         red_r[0] = base;
+        red_r[1] = retry;
     }
     __syncthreads();
+    if (red_r[1]) {
+        // back to the step's start (transient_nonlinear.mojo:1925-1942): the predictor's
+        // displacements, the elements' basic state; fiber trial state is recomputed from the
+        // committed state and needs nothing
+        for (int i = tid; i < n; i += nt) {
+            const int gi = f0 + i;
+            const double u = A.u_base[gi];
+            A.u_f[gi] = u;
+            A.u_full[A.free_dof[gi]] = u;
+        }
+        const size_t e0 = (size_t)I.elem_off * kEStride;
+        for (size_t t = tid; t < (size_t)I.n_elem * kEStride; t += nt) A.estate[e0 + t] = A.estate_base[e0 + t];
+        if (I.n_sl > 0) {
+            __syncthreads();
+            enforce_slaves(I, A);
+        }
+    }
     // still iterating: list this instance's elements for the next element kernel
     const int base = red_r[0];
     if (base >= 0) {
@@ -791,6 +837,10 @@ __global__ void predictor_kernel(const DevInst* __restrict__ insts, InstArrays A
         const bool ok = A.status[gi] == 0;
         A.active[gi] = ok ? 1 : 0;
         A.iters[gi] = 0;
+        if (A.attempt) {
+            A.attempt[gi] = 0;
+            A.iters_prev[gi] = 0;
+        }
         if (ok) {
             atomicAdd(A.nactive, 1);
             const DevInst& I = insts[gi];
@@ -807,6 +857,7 @@ __global__ void predictor_kernel(const DevInst* __restrict__ insts, InstArrays A
     A.a_n[gi] = an;
     const double up = un + I.dt * vn + I.coeff * an;
     A.u_f[gi] = up;
+    if (A.u_base) A.u_base[gi] = up;
     A.u_full[A.free_dof[gi]] = up;
     double p = A.fconst[gi];
     // ag holds, per instance, the ground acceleration of each excitation direction at this

@@ -309,6 +309,7 @@ struct StrutHandle {
     int n_free_total = 0, n_dofs_total = 0, n_elem = 0;
     long long band_total = 0;
     int any_modified = 0;  // an instance runs ModifiedNewton(Initial)
+    int any_chain = 0;     // an instance's solver chain has more than one attempt
     int max_nip = 1;
     size_t elem_smem = 0, inst_smem = 0;
     int max_iters_global = 1;
@@ -634,9 +635,16 @@ static int build_graph(StrutHandle* h) {
                         (const double*)h->d_ag, nF, h->n_inst, h->d_ctl, inner, 1));
     cudaGraph_t ibody;
     cudaGraphNode_t n_before_inner = n_pred;
+    if (h->any_chain) {
+        // the element state at the step's start, for a retry of the solver chain
+        cudaGraphNode_t n_snap;
+        TRY(add_kernel_node(&n_snap, body, &n_pred, 1, copy_doubles_kernel, dim3(592), dim3(tb), 0,
+                            (const double*)h->d_estate, h->A.estate_base, (long long)h->n_elem * kEStride));
+        n_before_inner = n_snap;
+    }
     if (h->n_slaves_total > 0) {
         cudaGraphNode_t n_sl;
-        TRY(add_kernel_node(&n_sl, body, &n_pred, 1, slave_enforce_kernel, dim3((h->n_slaves_total + tb - 1) / tb),
+        TRY(add_kernel_node(&n_sl, body, &n_before_inner, 1, slave_enforce_kernel, dim3((h->n_slaves_total + tb - 1) / tb),
                             dim3(tb), 0, A, h->n_slaves_total));
         n_before_inner = n_sl;
     }
@@ -1165,7 +1173,44 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         if (d.algorithm < STRUT_ALGORITHM_NEWTON || d.algorithm > STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL)
             return bail(fail(STRUT_BAD_ARG, "unknown algorithm"));
         I.algorithm = d.algorithm;
-        if (I.algorithm != STRUT_ALGORITHM_NEWTON) h->any_modified = 1;
+        {
+            // the solver chain: as given, or the primary settings followed by Newton when the
+            // primary algorithm is not Newton (transient_nonlinear.mojo:758-830)
+            if (d.num_attempts < 0 || d.num_attempts > STRUT_MAX_ATTEMPTS)
+                return bail(fail(STRUT_BAD_ARG, "num_attempts must be 0.." + std::to_string(STRUT_MAX_ATTEMPTS)));
+            StrutSolverAttempt ch[STRUT_MAX_ATTEMPTS];
+            int na = d.num_attempts;
+            if (na > 0) {
+                for (int k = 0; k < na; ++k) ch[k] = d.attempts[k];
+            } else {
+                ch[0].algorithm = d.algorithm;
+                ch[0].test_type = d.test_type;
+                ch[0].max_iters = d.max_iters;
+                ch[0].tol = d.tol;
+                na = 1;
+                if (d.algorithm != STRUT_ALGORITHM_NEWTON) {
+                    ch[1] = ch[0];
+                    ch[1].algorithm = STRUT_ALGORITHM_NEWTON;
+                    na = 2;
+                }
+            }
+            I.n_att = na;
+            int total = 0;
+            for (int k = 0; k < na; ++k) {
+                if (ch[k].algorithm < STRUT_ALGORITHM_NEWTON || ch[k].algorithm > STRUT_ALGORITHM_MODIFIED_NEWTON_INITIAL ||
+                    ch[k].test_type < STRUT_TEST_MAX_DISP_INCR || ch[k].test_type > STRUT_TEST_ENERGY_INCR ||
+                    ch[k].max_iters < 1)
+                    return bail(fail(STRUT_BAD_ARG, "solver attempt out of range"));
+                I.att_alg[k] = ch[k].algorithm;
+                I.att_test[k] = ch[k].test_type;
+                I.att_maxit[k] = ch[k].max_iters;
+                I.att_tol[k] = ch[k].tol;
+                if (ch[k].algorithm != STRUT_ALGORITHM_NEWTON) h->any_modified = 1;
+                total += ch[k].max_iters;
+            }
+            if (na > 1) h->any_chain = 1;
+            h->max_iters_global = std::max(h->max_iters_global, total);
+        }
         I.spd = d.system == STRUT_SYSTEM_BAND_SPD;
         I.has_damping = d.alpha_m != 0.0 || d.beta_k != 0.0 || d.beta_k_init != 0.0 || d.beta_k_comm != 0.0;
         I.dt = d.dt;
@@ -1210,8 +1255,9 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             // band too large for shared memory: blocked factorisation in global memory
             if (I.spd)
                 return bail(fail(STRUT_UNSUPPORTED, "BandSPD bands beyond shared memory are not implemented"));
-            if (I.algorithm != STRUT_ALGORITHM_NEWTON)
-                return bail(fail(STRUT_UNSUPPORTED, "ModifiedNewton on bands beyond shared memory is not implemented"));
+            for (int k = 0; k < I.n_att; ++k)
+                if (I.att_alg[k] != STRUT_ALGORITHM_NEWTON)
+                    return bail(fail(STRUT_UNSUPPORTED, "ModifiedNewton on bands beyond shared memory is not implemented"));
             const size_t fsm = large_factor_smem(bw);
             if (fsm > 220 * 1024 || bw > kLargeMaxBw)
                 return bail(fail(STRUT_UNSUPPORTED, "band width too large for the blocked factorisation"));
@@ -1229,7 +1275,6 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         } else {
             h->inst_smem = std::max(h->inst_smem, ismem);
         }
-        h->max_iters_global = std::max(h->max_iters_global, d.max_iters);
         h->insts[inst] = I;
         // excitations
         ExcHost& ex = h->exc[inst];
@@ -1377,6 +1422,10 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
     if (h->any_modified &&
         ((rc = dzeros(&A.kfrz, (size_t)h->band_total, al)) || (rc = dzeros(&A.lufrz, (size_t)h->band_total, al)) ||
          (rc = dzeros(&A.lu_dense, (size_t)h->n_inst, al))))
+        return bail(rc);
+    if (h->any_chain &&
+        ((rc = dzeros(&A.attempt, (size_t)h->n_inst, al)) || (rc = dzeros(&A.iters_prev, (size_t)h->n_inst, al)) ||
+         (rc = dzeros(&A.u_base, nF, al)) || (rc = dzeros(&A.estate_base, (size_t)h->n_elem * kEStride, al))))
         return bail(rc);
     double* d_Mff;
     double* d_Mrff;
@@ -1588,6 +1637,11 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             predictor_kernel<<<(npred + tb - 1) / tb, tb, 0, h->stream>>>(
                 h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag, nF, h->n_inst, h->d_ctl, none, 0);
             CK(cudaGetLastError());
+            if (h->any_chain) {
+                copy_doubles_kernel<<<592, tb, 0, h->stream>>>(h->d_estate, h->A.estate_base,
+                                                               (long long)h->n_elem * kEStride);
+                CK(cudaGetLastError());
+            }
             if (h->n_slaves_total > 0) {
                 slave_enforce_kernel<<<(h->n_slaves_total + tb - 1) / tb, tb, 0, h->stream>>>(h->A, h->n_slaves_total);
                 CK(cudaGetLastError());

@@ -518,6 +518,21 @@ class Model:
         self.test_type = tmap[tt]
         self.tol = float(an.get("tol", 1.0e-10))
         self.max_iters = int(an.get("max_iters", 20))
+        # solver chain (transient_nonlinear.mojo:758-830): attempts tried in turn on a step that
+        # does not converge; an absent chain is resolved by the library (Strut's rule)
+        self.attempts = []
+        for at in an.get("solver_chain", []) or []:
+            a_alg = at.get("algorithm", "Newton")
+            if a_alg not in amap:
+                raise ModelError(f"solver_chain: this path implements Newton, ModifiedNewton and "
+                                 f"ModifiedNewtonInitial, not {a_alg}")
+            a_tt = at.get("test_type", tt)
+            if a_tt not in tmap:
+                raise ModelError(f"solver_chain: unsupported test_type {a_tt}")
+            self.attempts.append((amap[a_alg], tmap[a_tt], int(at.get("max_iters", self.max_iters)),
+                                  float(at.get("tol", self.tol))))
+        if len(self.attempts) > A.MAX_ATTEMPTS:
+            raise ModelError(f"solver_chain: at most {A.MAX_ATTEMPTS} attempts")
         system = an.get("system", an.get("solver", "")) or "BandGeneral"
         if system in ("BandGEN", "BandGen"):
             system = "BandGeneral"
@@ -732,6 +747,10 @@ class Model:
         d.tol, d.max_iters = self.tol, self.max_iters
         d.test_type, d.system = self.test_type, self.system
         d.algorithm = self.algorithm
+        d.num_attempts = len(self.attempts)
+        for k, (a_alg, a_tt, a_mi, a_tol) in enumerate(self.attempts):
+            d.attempts[k].algorithm, d.attempts[k].test_type = a_alg, a_tt
+            d.attempts[k].max_iters, d.attempts[k].tol = a_mi, a_tol
         d.num_excitations = len(self.excitations)
         for i, x in enumerate(self.excitations):
             ex = d.excitation[i]
