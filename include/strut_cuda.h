@@ -432,10 +432,14 @@ int strut_gpu_mlp_train(StrutMlp* m, const float* x, const float* t, int32_t n, 
  * (converged increments of the node's dofs at the 4 previous steps, ground acceleration at this
  * and the 15 previous steps, node height over frame height; x_norm = (x - x_mean) * x_scale,
  * 4 ndf + 17 of them) give a correction to the step's Newmark predictor (network output *
- * y_scale per dof), the learned guess being predictor + correction.  The first
- * Newton iteration evaluates both that guess and the Newmark predictor and keeps the one with
- * the smaller residual norm; the iterations then run to the same convergence test.  m = NULL
- * detaches (the plain method). */
+ * y_scale per dof), the learned guess being predictor + correction (slave dofs of multi-point
+ * constraints then follow their masters).  The step starts from that guess.  Its first Newton
+ * iteration assembles the residual R(u_l) and effective tangent K_eff at the guess u_l and
+ * compares |R(u_l)| with the Newmark predictor u_p's residual to first order,
+ * |R(u_l) + K_eff (u_l - u_p)|: when the learned one is the larger the step goes back to u_p
+ * (the plain predictor is the fallback) and that evaluation is not counted as an iteration.  The
+ * iterations then run to the same convergence test.  Instances must use Newton and have their
+ * band in shared memory.  m = NULL detaches (the plain method). */
 int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, const float* x_scale,
                             const float* y_scale);
 /* Number of predicted nodes (all instances), i.e. rows of strut_gpu_predictor_features. */

@@ -10,13 +10,9 @@ struct PredState {
     float* d_x = nullptr;
     __nv_bfloat16* d_xt = nullptr;
     float* d_y = nullptr;
-    double* d_u_alt_f = nullptr;
-    double* d_u_alt_full = nullptr;
-    double* d_estate_alt = nullptr;
-    double* d_ek_alt = nullptr;
-    double* d_ef_alt = nullptr;
     long long* d_stats = nullptr;
-    int* d_next_alt = nullptr;
+    int* d_rejected = nullptr;
+    bool owns_base = false;  // u_base / estate_base were allocated for the predictor
     ~PredState() {
         for (void* p : allocs) cudaFree(p);
     }
@@ -34,24 +30,15 @@ int pred_alloc(PredState* ps, T** p, size_t n) {
     return STRUT_OK;
 }
 
-ElemList alt_list(const StrutHandle* h) {
-    ElemList el = h->A.el;
-    el.next = h->pred->d_next_alt;
-    return el;
-}
 
 }  // namespace
 
-// Feature and network launches plus the element evaluation of the learned guess, after the
-// Newmark predictor kernel of a step.
+// Feature and network launches after the Newmark predictor kernel of a step: the learned guess
+// replaces the predictor's displacements (which u_base keeps) on every predicted free dof.
 static int pred_launch(StrutHandle* h) {
     PredState* ps = h->pred;
     const int tb = 256;
-    const long long ne = (long long)h->n_elem * kEStride;
-    copy_doubles_kernel<<<592, tb, 0, h->stream>>>(h->d_estate, ps->d_estate_alt, ne);
-    copy_doubles_kernel<<<148, tb, 0, h->stream>>>(h->A.u_full, ps->d_u_alt_full, h->n_dofs_total);
-    pred_features_kernel<<<(ps->P.n_nodes + tb - 1) / tb, tb, 0, h->stream>>>(ps->P, h->d_ctl, h->A.status,
-                                                                             ps->d_x, ps->d_next_alt);
+    pred_features_kernel<<<(ps->P.n_nodes + tb - 1) / tb, tb, 0, h->stream>>>(ps->P, h->d_ctl, ps->d_x);
     const long long tot = (long long)ps->n_tiles * kMlpTile * kMlpKin;
     mlp_pack_x_kernel<<<(unsigned)((tot + tb - 1) / tb), tb, 0, h->stream>>>(ps->d_x, ps->P.n_nodes, ps->P.n_in,
                                                                             ps->d_xt, ps->n_tiles);
@@ -59,26 +46,22 @@ static int pred_launch(StrutHandle* h) {
                                                                       ps->d_y, ps->P.ndf, ps->mlp->d_err);
     const int nq = ps->P.n_nodes * ps->P.ndf;
     pred_scatter_kernel<<<(nq + tb - 1) / tb, tb, 0, h->stream>>>(ps->P, ps->d_y, h->A.u_f, h->A.free_dof,
-                                                                 ps->d_u_alt_f, ps->d_u_alt_full);
-    elem_kernel_of(h)<<<h->elem_grid, elem_block(h), h->elem_smem, h->stream>>>(
-        h->d_elems, h->geo, h->fs, ps->d_u_alt_full, ps->d_estate_alt, ps->d_ek_alt, ps->d_ef_alt, h->A.active,
-        h->A.status, h->d_elem_err, h->d_counters, alt_list(h), (const DevCtl*)h->d_ctl,
-        (int)ELEM_MODE_LIST, h->n_elem, rec_pass_of(h));
+                                                                 h->A.u_full);
     CK(cudaGetLastError());
+    if (h->n_slaves_total > 0) {
+        // a learned value of a slave dof is overwritten by its constraint (helpers.mojo:3380-3400)
+        slave_enforce_kernel<<<(h->n_slaves_total + tb - 1) / tb, tb, 0, h->stream>>>(h->A, h->n_slaves_total);
+        CK(cudaGetLastError());
+    }
     return STRUT_OK;
 }
 
 static int pred_add_nodes(StrutHandle* h, cudaGraph_t body, cudaGraphNode_t dep, cudaGraphNode_t* last) {
     PredState* ps = h->pred;
     const int tb = 256;
-    const long long ne = (long long)h->n_elem * kEStride;
-    cudaGraphNode_t a, b, c, d, e, f, g;
-    TRY(add_kernel_node(&a, body, &dep, 1, copy_doubles_kernel, dim3(592), dim3(tb), 0, (const double*)h->d_estate,
-                        ps->d_estate_alt, ne));
-    TRY(add_kernel_node(&b, body, &a, 1, copy_doubles_kernel, dim3(148), dim3(tb), 0, (const double*)h->A.u_full,
-                        ps->d_u_alt_full, (long long)h->n_dofs_total));
-    TRY(add_kernel_node(&c, body, &b, 1, pred_features_kernel, dim3((ps->P.n_nodes + tb - 1) / tb), dim3(tb), 0,
-                        ps->P, (const DevCtl*)h->d_ctl, (const int*)h->A.status, ps->d_x, ps->d_next_alt));
+    cudaGraphNode_t c, d, e, f;
+    TRY(add_kernel_node(&c, body, &dep, 1, pred_features_kernel, dim3((ps->P.n_nodes + tb - 1) / tb), dim3(tb), 0,
+                        ps->P, (const DevCtl*)h->d_ctl, ps->d_x));
     const long long tot = (long long)ps->n_tiles * kMlpTile * kMlpKin;
     TRY(add_kernel_node(&d, body, &c, 1, mlp_pack_x_kernel, dim3((unsigned)((tot + tb - 1) / tb)), dim3(tb), 0,
                         (const float*)ps->d_x, ps->P.n_nodes, ps->P.n_in, ps->d_xt, ps->n_tiles));
@@ -87,14 +70,14 @@ static int pred_add_nodes(StrutHandle* h, cudaGraph_t body, cudaGraphNode_t dep,
                         ps->mlp->d_err));
     const int nq = ps->P.n_nodes * ps->P.ndf;
     TRY(add_kernel_node(&f, body, &e, 1, pred_scatter_kernel, dim3((nq + tb - 1) / tb), dim3(tb), 0, ps->P,
-                        (const float*)ps->d_y, (const double*)h->A.u_f, (const int*)h->A.free_dof, ps->d_u_alt_f,
-                        ps->d_u_alt_full));
-    TRY(add_kernel_node(&g, body, &f, 1, elem_kernel_of(h), dim3(h->elem_grid), elem_block(h), h->elem_smem,
-                        (const DevElem*)h->d_elems, h->geo, h->fs, (const double*)ps->d_u_alt_full, ps->d_estate_alt,
-                        ps->d_ek_alt, ps->d_ef_alt, (const int*)h->A.active, h->A.status, h->d_elem_err,
-                        h->d_counters, alt_list(h), (const DevCtl*)h->d_ctl, (int)ELEM_MODE_LIST, h->n_elem,
-                        rec_pass_of(h)));
-    *last = g;
+                        (const float*)ps->d_y, h->A.u_f, (const int*)h->A.free_dof, h->A.u_full));
+    *last = f;
+    if (h->n_slaves_total > 0) {
+        cudaGraphNode_t g;
+        TRY(add_kernel_node(&g, body, &f, 1, slave_enforce_kernel, dim3((h->n_slaves_total + tb - 1) / tb), dim3(tb),
+                            0, h->A, h->n_slaves_total));
+        *last = g;
+    }
     return STRUT_OK;
 }
 
@@ -110,13 +93,16 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     h->A.dual = 0;
     h->A.hist_du = nullptr;
     h->A.pred_stats = nullptr;
+    h->A.rejected = nullptr;
+    if (h->pred_owns_base) {
+        h->A.u_base = nullptr;
+        h->A.estate_base = nullptr;
+        h->pred_owns_base = false;
+    }
     if (!m) return STRUT_OK;  // detached: the plain method
     if (h->ndf_all < 0) return fail(STRUT_UNSUPPORTED, "the learned predictor needs instances of one ndf");
     if (h->n_large > 0)
         return fail(STRUT_UNSUPPORTED, "the learned predictor runs on instances whose band fits in shared memory");
-    if (h->n_slaves_total > 0)
-        return fail(STRUT_UNSUPPORTED, "the learned predictor does not run with multi-point constraints");
-    if (h->n_shells > 0) return fail(STRUT_UNSUPPORTED, "the learned predictor does not run with shells");
     for (const DevInst& I : h->insts)
         for (int k = 0; k < I.n_att; ++k)
             if (I.att_alg[k] != STRUT_ALGORITHM_NEWTON)
@@ -156,13 +142,20 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
         (rc = pred_alloc(ps, &d_hist, (size_t)4 * h->n_free_total)) || (rc = pred_alloc(ps, &d_ag, ag.size())) ||
         (rc = pred_alloc(ps, &ps->d_x, (size_t)nn * n_in)) ||
         (rc = pred_alloc(ps, &ps->d_xt, (size_t)ps->n_tiles * kMlpBytesX / 2)) ||
-        (rc = pred_alloc(ps, &ps->d_y, (size_t)nn * ndf)) || (rc = pred_alloc(ps, &ps->d_u_alt_f, (size_t)h->n_free_total)) ||
-        (rc = pred_alloc(ps, &ps->d_u_alt_full, (size_t)h->n_dofs_total)) ||
-        (rc = pred_alloc(ps, &ps->d_estate_alt, (size_t)h->n_elem * kEStride)) ||
-        (rc = pred_alloc(ps, &ps->d_ek_alt, (size_t)h->ek_total)) ||
-        (rc = pred_alloc(ps, &ps->d_ef_alt, (size_t)h->ef_total)) ||
-        (rc = pred_alloc(ps, &ps->d_stats, (size_t)2 * h->n_inst)) || (rc = pred_alloc(ps, &ps->d_next_alt, 2)))
+        (rc = pred_alloc(ps, &ps->d_y, (size_t)nn * ndf)) ||
+        (rc = pred_alloc(ps, &ps->d_stats, (size_t)2 * h->n_inst)) ||
+        (rc = pred_alloc(ps, &ps->d_rejected, (size_t)h->n_inst)))
         return bail(rc);
+    double* d_u_base = h->A.u_base;
+    double* d_estate_base = h->A.estate_base;
+    if (!d_u_base) {
+        // the predictor's displacements and the element state at the step's start, for the
+        // return to the plain predictor
+        if ((rc = pred_alloc(ps, &d_u_base, (size_t)h->n_free_total)) ||
+            (rc = pred_alloc(ps, &d_estate_base, (size_t)h->n_elem * kEStride)))
+            return bail(rc);
+        ps->owns_base = true;
+    }
     auto up = [&](void* dst, const void* src, size_t bytes) -> int {
         CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
         return STRUT_OK;
@@ -176,10 +169,10 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
                     d_hist, d_ag};
     h->pred = ps;
     h->A.dual = 1;
-    h->A.u_alt_f = ps->d_u_alt_f;
-    h->A.ek_alt = ps->d_ek_alt;
-    h->A.ef_alt = ps->d_ef_alt;
-    h->A.estate_alt = ps->d_estate_alt;
+    h->A.rejected = ps->d_rejected;
+    h->A.u_base = d_u_base;
+    h->A.estate_base = d_estate_base;
+    h->pred_owns_base = ps->owns_base;
     h->A.pred_stats = ps->d_stats;
     h->A.hist_du = d_hist;
     return STRUT_OK;
@@ -208,8 +201,7 @@ int strut_gpu_predictor_features(StrutHandle* h, float* out) {
     CK(cudaMemcpy(&c, h->d_ctl, sizeof(c), cudaMemcpyDeviceToHost));
     c.step = h->steps_done;  // features of the next step
     CK(cudaMemcpy(h->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
-    pred_features_kernel<<<(ps->P.n_nodes + 255) / 256, 256, 0, h->stream>>>(ps->P, h->d_ctl, h->A.status, ps->d_x,
-                                                                             ps->d_next_alt);
+    pred_features_kernel<<<(ps->P.n_nodes + 255) / 256, 256, 0, h->stream>>>(ps->P, h->d_ctl, ps->d_x);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
     CK(cudaMemcpy(out, ps->d_x, (size_t)ps->P.n_nodes * ps->P.n_in * 4, cudaMemcpyDeviceToHost));

@@ -1,5 +1,5 @@
-// Learned Newton predictor: per-node features, the network's increments back to a displacement
-// guess, and the copy of the element state the learned guess is evaluated from.
+// Learned Newton predictor: per-node features and the network's increments back to a displacement
+// guess.
 //
 // Features of node p at step s (the step being computed, t = (s + 1) dt), n_in = 4 ndf + 17:
 //   the converged increments of its ndf dofs at steps s-1, s-2, s-3, s-4 (0 for a constrained dof
@@ -27,14 +27,8 @@ struct PredDev {
     const double* ag_full;  // n_inst x ag_len: ground acceleration of step s
 };
 
-// Also clears the work counter the element evaluation of the learned guess claims from.
-__global__ void pred_features_kernel(PredDev P, const DevCtl* __restrict__ ctl, const int* __restrict__ status,
-                                     float* __restrict__ x, int* __restrict__ next_alt) {
+__global__ void pred_features_kernel(PredDev P, const DevCtl* __restrict__ ctl, float* __restrict__ x) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p == 0) {
-        next_alt[0] = 0;
-        next_alt[1] = 0;
-    }
     if (p >= P.n_nodes) return;
     const int s = ctl->step;
     const int inst = P.node_inst[p];
@@ -55,23 +49,21 @@ __global__ void pred_features_kernel(PredDev P, const DevCtl* __restrict__ ctl, 
         xr[k] = ((float)v - P.x_mean[k]) * P.x_scale[k];
     }
     xr[k] = (P.node_h[p] - P.x_mean[k]) * P.x_scale[k];
-    (void)status;
 }
 
-// u_alt = u_pred + y * y_scale on the free dofs of every predicted node, u_pred being the Newmark
-// predictor the step starts from (the network predicts the correction to it); u_alt_full already
-// holds a copy of u_full, so constrained dofs keep their values.
-__global__ void pred_scatter_kernel(PredDev P, const float* __restrict__ y, const double* __restrict__ u_pred,
-                                    const int* __restrict__ free_dof, double* __restrict__ u_alt_f,
-                                    double* __restrict__ u_alt_full) {
+// The learned guess: u += y * y_scale on the free dofs of every predicted node, u holding the
+// Newmark predictor the step starts from (the network predicts the correction to it).  Each free
+// dof belongs to one node, so every entry is updated by one thread.
+__global__ void pred_scatter_kernel(PredDev P, const float* __restrict__ y, double* __restrict__ u_f,
+                                    const int* __restrict__ free_dof, double* __restrict__ u_full) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n_nodes * P.ndf) return;
     const int p = q / P.ndf, d = q % P.ndf;
     const int fi = P.node_free[p * P.ndf + d];
     if (fi < 0) return;
-    const double u = u_pred[fi] + (double)y[(size_t)p * P.ndf + d] * (double)P.y_scale[d];
-    u_alt_f[fi] = u;
-    u_alt_full[free_dof[fi]] = u;
+    const double u = u_f[fi] + (double)y[(size_t)p * P.ndf + d] * (double)P.y_scale[d];
+    u_f[fi] = u;
+    u_full[free_dof[fi]] = u;
 }
 
 __global__ void copy_doubles_kernel(const double* __restrict__ src, double* __restrict__ dst, long long n) {

@@ -50,13 +50,12 @@ struct InstArrays {
     int* piv;             // per free dof
     int* fallbacks;       // per instance count of dense fallbacks
     ElemList el;          // elements of the instances still iterating
-    // learned predictor (dual first iteration): the learned guess and its element results
+    // learned predictor: the step starts from the learned guess (dual 1), whose first iteration
+    // checks it against the Newmark predictor's (u_base); rejected: per instance, the step went
+    // back to the predictor
     int dual;
-    const double* u_alt_f;
-    const double* ek_alt;
-    const double* ef_alt;
+    int* rejected;
     double* estate;
-    const double* estate_alt;
     long long* pred_stats;  // per instance: first iterations offered, learned guess chosen
     double* hist_du;        // 4 x n_free ring of converged increments (slot = step % 4)
     int n_free_total;
@@ -487,32 +486,6 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
     __syncthreads();
     if (I.large) return;  // global-memory band path (largeband_kernels.cuh)
     if (mode == INST_MODE_NEWTON && !A.active[inst]) return;
-    if (mode == INST_MODE_NEWTON && A.dual && A.ctl && A.ctl->iter == 0) {
-        // first iteration with a learned guess: both guesses were evaluated; keep the learned
-        // one only when its residual is the smaller (the plain predictor is the fallback)
-        double* vs = smem_inst;
-        double* as = smem_inst + I.n;
-        const double r_plain = residual_norm(I, A, A.u_f, A.ek, A.ef, vs, as, red);
-        const double r_learn = residual_norm(I, A, A.u_alt_f, A.ek_alt, A.ef_alt, vs, as, red);
-        const bool learn = isfinite(r_learn) && r_learn < r_plain;
-        if (learn) {
-            for (int i = tid; i < I.n; i += nt) {
-                const int gi = I.f_off + i;
-                const double u = A.u_alt_f[gi];
-                A.u_f[gi] = u;
-                A.u_full[A.free_dof[gi]] = u;
-            }
-            const size_t e0 = (size_t)I.elem_off * kEStride;
-            for (int t = tid; t < I.n_elem * kEStride; t += nt) A.estate[e0 + t] = A.estate_alt[e0 + t];
-            A.ek = A.ek_alt;
-            A.ef = A.ef_alt;
-        }
-        if (tid == 0 && A.pred_stats) {
-            A.pred_stats[2 * inst] += 1;
-            if (learn) A.pred_stats[2 * inst + 1] += 1;
-        }
-        __syncthreads();
-    }
     int* hrow = (A.hist_iters && A.ctl) ? A.hist_iters + (size_t)A.ctl->step * gridDim.x : nullptr;
     const int n = I.n, bw = I.bw, rw = I.rw;
     double* Kb = smem_inst;        // n * rw
@@ -650,6 +623,64 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
                 }
                 return;
             }
+        }
+        if (mode == INST_MODE_NEWTON && A.dual && A.rejected && s_it == 0 && !A.rejected[inst] &&
+            (!A.attempt || A.attempt[inst] == 0)) {
+            // The step started from the learned guess u_l.  The Newmark predictor's u_p would
+            // have the residual R(u_p) = R(u_l) + K_eff (u_l - u_p) to first order, K_eff being
+            // the effective tangent just assembled at u_l; keep u_l unless its residual is the
+            // larger, else go back to u_p (the plain predictor is the fallback).
+            for (int i = tid; i < n; i += nt) du[i] = A.u_f[f0 + i] - A.u_base[f0 + i];
+            __syncthreads();
+            double sl = 0.0, sp = 0.0;
+            for (int i = tid; i < n; i += nt) {
+                double kd = 0.0;
+                for (int o = 0; o < rw; ++o) {
+                    const int j = i + o - bw;
+                    if (j >= 0 && j < n) kd += Kb[i * rw + o] * du[j];
+                }
+                if (I.spd)  // BandSPD holds the lower band: the upper half from the rows below
+                    for (int j = i + 1; j <= min(n - 1, i + bw); ++j) kd += Kb[j * rw + (i - j + bw)] * du[j];
+                const double rp = R[i] + kd;
+                sl += R[i] * R[i];
+                sp += rp * rp;
+            }
+            sl = block_sum(sl, red);
+            sp = block_sum(sp, red);
+            const bool keep = isfinite(sl) && sl <= sp;
+            if (tid == 0 && A.pred_stats) {
+                A.pred_stats[2 * inst] += 1;
+                if (keep) A.pred_stats[2 * inst + 1] += 1;
+            }
+            if (!keep) {
+                for (int i = tid; i < n; i += nt) {
+                    const int gi = f0 + i;
+                    const double u = A.u_base[gi];
+                    A.u_f[gi] = u;
+                    A.u_full[A.free_dof[gi]] = u;
+                }
+                const size_t e0 = (size_t)I.elem_off * kEStride;
+                for (size_t t = tid; t < (size_t)I.n_elem * kEStride; t += nt) A.estate[e0 + t] = A.estate_base[e0 + t];
+                if (I.n_sl > 0) {
+                    __syncthreads();
+                    enforce_slaves(I, A);
+                }
+                if (tid == 0) {
+                    // the rejected evaluation is not a Newton iteration of the step
+                    A.iters[inst] -= 1;
+                    A.rejected[inst] = 1;
+                    red_r[0] = A.ctl ? atomicAdd(&A.el.count[(A.ctl->iter + 1) & 1], I.n_elem) : -1;
+                }
+                __syncthreads();
+                const int base = red_r[0];
+                if (base >= 0) {
+                    const int buf = (A.ctl->iter + 1) & 1;
+                    for (int k = tid; k < I.n_elem; k += nt)
+                        A.el.list[buf][base + k] = list_entry(A.el, buf, I.elem_off + k);
+                }
+                return;
+            }
+            __syncthreads();
         }
     }
     bool dense = false;
@@ -841,6 +872,7 @@ __global__ void predictor_kernel(const DevInst* __restrict__ insts, InstArrays A
             A.attempt[gi] = 0;
             A.iters_prev[gi] = 0;
         }
+        if (A.rejected) A.rejected[gi] = 0;
         if (ok) {
             atomicAdd(A.nactive, 1);
             const DevInst& I = insts[gi];

@@ -310,6 +310,7 @@ struct StrutHandle {
     long long band_total = 0;
     int any_modified = 0;  // an instance runs ModifiedNewton(Initial)
     int any_chain = 0;     // an instance's solver chain has more than one attempt
+    bool pred_owns_base = false;  // A.u_base / estate_base belong to the attached predictor
     int max_nip = 1;
     size_t elem_smem = 0, inst_smem = 0;
     int max_iters_global = 1;
@@ -635,8 +636,9 @@ static int build_graph(StrutHandle* h) {
                         (const double*)h->d_ag, nF, h->n_inst, h->d_ctl, inner, 1));
     cudaGraph_t ibody;
     cudaGraphNode_t n_before_inner = n_pred;
-    if (h->any_chain) {
-        // the element state at the step's start, for a retry of the solver chain
+    if (h->any_chain || h->pred) {
+        // the element state at the step's start, for a retry of the solver chain or the return
+        // from the learned guess to the predictor
         cudaGraphNode_t n_snap;
         TRY(add_kernel_node(&n_snap, body, &n_pred, 1, copy_doubles_kernel, dim3(592), dim3(tb), 0,
                             (const double*)h->d_estate, h->A.estate_base, (long long)h->n_elem * kEStride));
@@ -1637,7 +1639,7 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
             predictor_kernel<<<(npred + tb - 1) / tb, tb, 0, h->stream>>>(
                 h->d_insts, h->A, h->d_free_inst, h->d_free_dir, h->d_ag, nF, h->n_inst, h->d_ctl, none, 0);
             CK(cudaGetLastError());
-            if (h->any_chain) {
+            if (h->any_chain || h->pred) {
                 copy_doubles_kernel<<<592, tb, 0, h->stream>>>(h->d_estate, h->A.estate_base,
                                                                (long long)h->n_elem * kEStride);
                 CK(cudaGetLastError());

@@ -1,10 +1,11 @@
 """Learned Newton predictor: training data from the plain method's converged histories, feature
 normalisation, and attaching a trained network to an analysis.
 
-The predictor proposes each step's displacement increment node by node; the step's first Newton
-iteration evaluates both the learned guess and the plain Newmark predictor and keeps the one with
-the smaller residual, so Newton converges to the same NormDispIncr tolerance either way and the
-plain predictor is the fallback.  Strut has no learned predictor (this follows the north-star
+The predictor proposes each step's displacement increment node by node and the step starts from
+that guess; its first Newton iteration compares the guess's residual with the plain Newmark
+predictor's, estimated to first order from the tangent assembled at the guess, and goes back to
+the plain predictor when the learned residual is the larger.  Newton converges to the same
+NormDispIncr tolerance either way and the plain predictor is the fallback.  Strut has no learned predictor (this follows the north-star
 configuration's network and features); the analysis path it plugs into is Strut's
 transient_nonlinear Newton loop (src/mojo/solver/run_case/analysis/transient_nonlinear.mojo).
 
