@@ -116,30 +116,35 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     ps->mlp = m;
     const int nn = (int)h->pn_inst.size();
     ps->n_tiles = (nn + kMlpTile - 1) / kMlpTile;
-    // ground acceleration of every step of every instance (first excitation), as the step loop
-    // evaluates it: t = (s + 1) dt
+    // ground acceleration of every step of every instance, per excitation component, as the
+    // step loop evaluates it: t = (s + 1) dt
     int ag_len = 1;
     for (int i = 0; i < h->n_inst; ++i)
-        if (h->exc[i].num > 0) {
-            const StrutExcitation& x = h->exc[i].x[0];
+        for (int c = 0; c < h->exc[i].num; ++c) {
+            const StrutExcitation& x = h->exc[i].x[c];
             ag_len = std::max(ag_len, (int)std::ceil(x.count * x.dt / h->insts[i].dt) + 2);
         }
-    std::vector<double> ag((size_t)h->n_inst * ag_len, 0.0);
-    for (int i = 0; i < h->n_inst; ++i)
-        if (h->exc[i].num > 0)
-            for (int s = 0; s < ag_len; ++s) ag[(size_t)i * ag_len + s] = path_eval(h->exc[i].x[0], (s + 1) * h->insts[i].dt);
+    std::vector<double> ag((size_t)2 * h->n_inst * ag_len, 0.0);
+    std::vector<int> comp(h->n_inst, 1);
+    for (int i = 0; i < h->n_inst; ++i) {
+        comp[i] = h->exc[i].num == 2 ? 2 : 1;
+        for (int c = 0; c < h->exc[i].num; ++c)
+            for (int s = 0; s < ag_len; ++s)
+                ag[((size_t)c * h->n_inst + i) * ag_len + s] = path_eval(h->exc[i].x[c], (s + 1) * h->insts[i].dt);
+    }
     int rc = STRUT_OK;
     auto bail = [&](int code) {
         delete ps;
         return code;
     };
-    int *d_nf, *d_ni;
+    int *d_nf, *d_ni, *d_comp;
     float *d_nh, *d_xm, *d_xs, *d_ys;
     double *d_hist, *d_ag;
     if ((rc = pred_alloc(ps, &d_nf, h->pn_free.size())) || (rc = pred_alloc(ps, &d_ni, (size_t)nn)) ||
         (rc = pred_alloc(ps, &d_nh, (size_t)nn)) || (rc = pred_alloc(ps, &d_xm, (size_t)n_in)) ||
         (rc = pred_alloc(ps, &d_xs, (size_t)n_in)) || (rc = pred_alloc(ps, &d_ys, (size_t)ndf)) ||
         (rc = pred_alloc(ps, &d_hist, (size_t)4 * h->n_free_total)) || (rc = pred_alloc(ps, &d_ag, ag.size())) ||
+        (rc = pred_alloc(ps, &d_comp, comp.size())) ||
         (rc = pred_alloc(ps, &ps->d_x, (size_t)nn * n_in)) ||
         (rc = pred_alloc(ps, &ps->d_xt, (size_t)ps->n_tiles * kMlpBytesX / 2)) ||
         (rc = pred_alloc(ps, &ps->d_y, (size_t)nn * ndf)) ||
@@ -163,10 +168,10 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     if ((rc = up(d_nf, h->pn_free.data(), h->pn_free.size() * 4)) || (rc = up(d_ni, h->pn_inst.data(), (size_t)nn * 4)) ||
         (rc = up(d_nh, h->pn_h.data(), (size_t)nn * 4)) || (rc = up(d_xm, x_mean, (size_t)n_in * 4)) ||
         (rc = up(d_xs, x_scale, (size_t)n_in * 4)) || (rc = up(d_ys, y_scale, (size_t)ndf * 4)) ||
-        (rc = up(d_ag, ag.data(), ag.size() * 8)))
+        (rc = up(d_ag, ag.data(), ag.size() * 8)) || (rc = up(d_comp, comp.data(), comp.size() * 4)))
         return bail(rc);
     ps->P = PredDev{nn, ndf, n_in, h->n_free_total, h->n_inst, ag_len, d_nf, d_ni, d_nh, d_xm, d_xs, d_ys,
-                    d_hist, d_ag};
+                    d_hist, d_ag, d_comp};
     h->pred = ps;
     h->A.dual = 1;
     h->A.rejected = ps->d_rejected;

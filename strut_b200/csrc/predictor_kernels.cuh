@@ -3,8 +3,9 @@
 //
 // Features of node p at step s (the step being computed, t = (s + 1) dt), n_in = 4 ndf + 17:
 //   the converged increments of its ndf dofs at steps s-1, s-2, s-3, s-4 (0 for a constrained dof
-//   or a step before the first), ground acceleration at steps s, s-1, ..., s-15 (0 before the
-//   record), the node height over the instance's height; each normalised (x - mean) * scale.
+//   or a step before the first), ground acceleration at steps s, s-1, ..., s-15 (one excitation)
+//   or of each of the two components at steps s .. s-7 (0 before the record), the node height
+//   over the instance's height; each normalised (x - mean) * scale.
 // The network predicts, per dof and in units of y_scale, the correction the converged increment
 // of step s needs over the Newmark predictor's (the plain predictor stays the reference point).  Strut has no
 // learned predictor; the feature set is the one of the north-star configuration (2D: one ground
@@ -24,7 +25,8 @@ struct PredDev {
     const float* x_scale;   // n_in
     const float* y_scale;   // ndf
     const double* hist_du;  // 4 x n_free (slot = step % 4)
-    const double* ag_full;  // n_inst x ag_len: ground acceleration of step s
+    const double* ag_full;  // 2 x n_inst x ag_len: ground acceleration of step s, per component
+    const int* inst_comp;   // n_inst: excitation components of the instance (1 or 2)
 };
 
 __global__ void pred_features_kernel(PredDev P, const DevCtl* __restrict__ ctl, float* __restrict__ x) {
@@ -43,9 +45,11 @@ __global__ void pred_features_kernel(PredDev P, const DevCtl* __restrict__ ctl, 
             xr[k] = ((float)v - P.x_mean[k]) * P.x_scale[k];
         }
     }
+    // one component: its 16 latest samples; two: the 8 latest of each
+    const int two = P.inst_comp[inst] == 2;
     for (int j = 0; j < 16; ++j, ++k) {
-        const int sj = s - j;
-        const double v = (sj >= 0 && sj < P.ag_len) ? P.ag_full[(size_t)inst * P.ag_len + sj] : 0.0;
+        const int c = two ? j / 8 : 0, sj = s - (two ? j % 8 : j);
+        const double v = (sj >= 0 && sj < P.ag_len) ? P.ag_full[((size_t)c * P.n_inst + inst) * P.ag_len + sj] : 0.0;
         xr[k] = ((float)v - P.x_mean[k]) * P.x_scale[k];
     }
     xr[k] = (P.node_h[p] - P.x_mean[k]) * P.x_scale[k];

@@ -63,11 +63,12 @@ def path_eval(ex: dict, t: float) -> float:
     return ex["factor"] * (v1 + (v2 - v1) * (incr - i1))
 
 
-def ground_series(model, steps: int) -> np.ndarray:
-    """Ground acceleration of steps 0..steps-1 (first excitation), as the step loop evaluates it."""
-    if not model.excitations:
+def ground_series(model, steps: int, component: int = 0) -> np.ndarray:
+    """Ground acceleration of steps 0..steps-1 of one excitation component, as the step loop
+    evaluates it."""
+    if len(model.excitations) <= component:
         return np.zeros(steps)
-    ex = model.excitations[0]
+    ex = model.excitations[component]
     return np.array([path_eval(ex, (s + 1) * model.dt) for s in range(steps)])
 
 
@@ -84,15 +85,18 @@ def raw_features(model, u_free_hist: np.ndarray):
     du_pad = np.hstack([du, np.zeros((steps, 1))])    # column -1 -> 0 for constrained dofs
     col = np.where(frees >= 0, frees, du.shape[1])    # (nodes, ndf)
     node_du = du_pad[:, col]                          # (steps, nodes, ndf)
-    ag = ground_series(model, steps)
     nn = frees.shape[0]
     X = np.zeros((steps, nn, n_features(ndf)), dtype=np.float32)
     for j in range(N_HIST):
         sl = slice(j * ndf, (j + 1) * ndf)
         X[1 + j:, :, sl] = node_du[:steps - 1 - j].astype(np.float32)
-    agp = np.concatenate([np.zeros(N_AG - 1), ag]).astype(np.float32)  # agp[k + 15] = ag[k]
+    # one excitation: its 16 latest samples; two: the 8 latest of each component
+    two = len(model.excitations) == 2
     for j in range(N_AG):
-        X[:, :, N_HIST * ndf + j] = agp[N_AG - 1 - j:N_AG - 1 - j + steps][:, None]
+        c, lag = (j // 8, j % 8) if two else (0, j)
+        ag = ground_series(model, steps, c)
+        agp = np.concatenate([np.zeros(N_AG - 1), ag]).astype(np.float32)  # agp[k + 15] = ag[k]
+        X[:, :, N_HIST * ndf + j] = agp[N_AG - 1 - lag:N_AG - 1 - lag + steps][:, None]
     X[:, :, -1] = hs[None, :]
     # Newmark velocity / acceleration of the converged history (transient_nonlinear.mojo:594-647)
     dt, gam, bet = model.dt, model.gamma, model.beta

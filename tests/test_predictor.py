@@ -99,3 +99,60 @@ def test_detached_predictor_is_the_plain_method(gpu_lib):
         b.run(steps)
         d1, _e, i1 = b.history(0)
     assert np.array_equal(d0, d1) and np.array_equal(i0, i1)
+
+
+def _diaphragm_case(seed, steps):
+    return W.rc_frame3d_case(stories=4, bays_x=3, bays_y=3, steps=steps, dt=0.005, seed=seed,
+                             element="forceBeamColumn3d", beam_element="dispBeamColumn3d",
+                             diaphragm=True, bidirectional=True, pga_g=0.4)
+
+
+def test_host_features_two_components():
+    """Two horizontal records: the ground features are the 8 latest samples of each."""
+    m = M.Model(_diaphragm_case(3, 30))
+    assert len(m.excitations) == 2 and PR.n_features(m.ndf) == 41
+    u = np.zeros((30, m.num_free))
+    X, _T = PR.raw_features(m, u)
+    nn = X.shape[0] // 30
+    s = 12
+    row = X[s * nn]
+    a0, a1 = PR.ground_series(m, 30, 0), PR.ground_series(m, 30, 1)
+    for lag in range(8):
+        assert row[24 + lag] == np.float32(a0[s - lag])
+        assert row[32 + lag] == np.float32(a1[s - lag])
+
+
+@pytest.mark.gpu
+def test_learned_predictor_on_diaphragm_frames(gpu_lib):
+    """The 41-feature network on bidirectional 3D rigid-diaphragm frames (slave dofs follow their
+    masters after the learned guess): device features equal the host's, and runs with the
+    predictor stay within 1e-7 of peak of the plain runs on unseen records."""
+    steps = 300
+    train = [PR.record_all_dofs(M.Model(_diaphragm_case(s, steps))) for s in range(8)]
+    with gpu_lib.Analysis(train) as an:
+        an.run(steps)
+        hists = [PR.free_history(an, i) for i in range(len(train))]
+    Xs, Ts = zip(*[PR.raw_features(m, h) for m, h in zip(train, hists)])
+    pred = PR.LearnedPredictor(6, seed=3)
+    pred.fit(np.concatenate(Xs), np.concatenate(Ts), epochs=20, batch=4096, lr=2e-3, seed=4)
+    probe = PR.record_all_dofs(M.Model(_diaphragm_case(64, steps)))
+    test = [probe] + [M.Model(_diaphragm_case(s, steps)) for s in (65, 66)]
+    with gpu_lib.Analysis(test) as plain:
+        plain.run(steps)
+        ref = [plain.history(i) for i in range(len(test))]
+    with gpu_lib.Analysis(test) as learned:
+        pred.attach(learned)
+        learned.run(steps)
+        got = [learned.history(i) for i in range(len(test))]
+        offered, chosen = PR.stats(learned)
+        u = PR.free_history(learned, 0)
+        dev = PR.device_features(learned)
+    assert offered >= steps * len(test) and chosen > 0
+    for (d0, _e0, _i0), (d1, _e1, _i1) in zip(ref, got):
+        for j in range(d0.shape[1]):
+            if np.max(np.abs(d0[:, j])) > 0.0:
+                assert rel_err_of_peak(d1[:, j], d0[:, j]) <= 1e-7
+    X, _ = PR.raw_features(probe, np.vstack([u, u[-1:]]))
+    nn = X.shape[0] // (steps + 1)
+    host = (X[steps * nn:(steps + 1) * nn] - pred.x_mean) * pred.x_scale
+    assert np.allclose(dev[:nn], host, rtol=1e-5, atol=1e-5)
