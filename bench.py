@@ -68,7 +68,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor arm")
     ap.add_argument("--train-frames", type=int, default=64)
-    ap.add_argument("--train-epochs", type=int, default=8)
+    ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--learned3d-steps", type=int, default=4000,
+                    help="record steps of the 3D learned-predictor arm (config 3)")
+    ap.add_argument("--no-learned3d", action="store_true", help="skip the 3D learned-predictor arm")
     ap.add_argument("--no-tall", action="store_true",
                     help="skip the large single-instance 3D frame (20 stories, 6x6 bays)")
     ap.add_argument("--tall-steps", type=int, default=4000,
@@ -288,51 +291,75 @@ def fiber_arm(n_fibers, runtime, torch, peak, steps=20, warmup=3):
             "peak_kind": peak[1], "finite": ok}
 
 
-def learned_arm(args, models, device, runtime, A, torch, world):
-    """The learned+batched arm: train the per-node network (tensor-core kernels) on histories the
-    plain method computes for separate training frames and records (seeds 5000+), then run the
-    same batch as the plain arm with the network proposing each step's first guess.  Untimed:
-    data generation and training; timed (device events): the analysis."""
-    from strut_b200 import model as Mo, predictor as PR, workloads as W
+def train_predictor(models, steps, device, runtime, every, epochs, seed=7):
+    """Runs `models` (recording every dof) with the plain method, builds the learned predictor's
+    features and targets from the converged histories (every `every`-th step of each completed
+    record) and trains the network on the tensor cores.  Returns (predictor, info)."""
+    from strut_b200 import predictor as PR
 
     t0 = time.perf_counter()
-    tcases = W.batched_frames(args.train_frames, steps=args.record_steps, dt=DT, base_seed=5000)
-    tmodels = [PR.record_all_dofs(Mo.Model(c)) for c in tcases]
-    with runtime.Analysis(tmodels, device=device) as an:
-        an.run(args.record_steps, check=False)
+    rec = [PR.record_all_dofs(m) for m in models]
+    with runtime.Analysis(rec, device=device) as an:
+        an.run(steps, check=False)
         status = an.instance_status()
         Xs, Ts = [], []
-        for i, m in enumerate(tmodels):
+        for i, m in enumerate(rec):
             if status[i] != 0:
                 continue
             X, T = PR.raw_features(m, PR.free_history(an, i))
-            nn = X.shape[0] // args.record_steps
-            keep = (np.arange(X.shape[0]) // nn) % 4 == 0  # every 4th step
+            nn = X.shape[0] // steps
+            keep = (np.arange(X.shape[0]) // nn) % every == 0
             Xs.append(X[keep])
             Ts.append(T[keep])
     X, T = np.concatenate(Xs), np.concatenate(Ts)
     t_data = time.perf_counter() - t0
     t0 = time.perf_counter()
-    pred = PR.LearnedPredictor(tmodels[0].ndf, seed=7)
-    loss = pred.fit(X, T, epochs=args.train_epochs, batch=8192, lr=1e-3, seed=11)
-    t_train = time.perf_counter() - t0
+    pred = PR.LearnedPredictor(models[0].ndf, seed=seed)
+    loss = pred.fit(X, T, epochs=epochs, batch=8192, lr=1e-3, seed=11)
+    info = {"records": len(models), "samples": int(X.shape[0]), "epochs": epochs,
+            "final_mse_normalised": loss, "data_s": round(t_data, 1),
+            "train_s": round(time.perf_counter() - t0, 1),
+            "network": f"{PR.n_features(models[0].ndf)}-128-128-{models[0].ndf} bf16 tcgen05, GELU"}
+    return pred, info
+
+
+def timed_run(models, steps, device, runtime, torch, pred=None):
+    """One analysis of `models`, device time; returns (ms, stats, completed, histories, pred
+    stats)."""
+    from strut_b200 import predictor as PR
 
     an = runtime.Analysis(models, device=device)
-    pred.attach(an)
+    if pred is not None:
+        pred.attach(an)
     stream = torch.cuda.ExternalStream(runtime.lib().strut_gpu_stream(an.h))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        torch.distributed.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
-    st = an.run(args.record_steps, check=False)
+    st = an.run(steps, check=False)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
-    completed = int((an.instance_status() == 0).sum())
-    offered, chosen = PR.stats(an)
+    status = an.instance_status()
+    hist = an.history_all()
+    ps = PR.stats(an) if pred is not None else (0, 0)
     an.close()
+    return ms, st, int((status == 0).sum()), (hist, status), ps
+
+
+def learned_arm(args, models, device, runtime, A, torch, world):
+    """The learned+batched arm on the plain arm's batch: the per-node network (tensor-core
+    kernels) is trained on histories the plain method computes for 64 other frames and records
+    (seeds 5000+), then the same batch runs with the network proposing each step's first guess.
+    Untimed: data generation and training; timed (device events): the analysis."""
+    from strut_b200 import model as Mo, workloads as W
+
+    tmodels = [Mo.Model(c) for c in W.batched_frames(args.train_frames, steps=args.record_steps, dt=DT,
+                                                      base_seed=5000)]
+    pred, info = train_predictor(tmodels, args.record_steps, device, runtime, 4, args.train_epochs)
+    if world > 1:
+        torch.distributed.barrier()
+    ms, st, completed, _h, (offered, chosen) = timed_run(models, args.record_steps, device, runtime, torch, pred)
     if world > 1:
         t = torch.tensor([ms, completed], dtype=torch.float64, device="cuda")
         mx = t.clone()
@@ -341,13 +368,49 @@ def learned_arm(args, models, device, runtime, A, torch, world):
         ms, completed = float(mx[0].item()), int(t[1].item())
     return {
         "value": completed / (ms / 1000.0) * 3600.0, "unit": "records/hour", "ms": ms,
-        "newton_its_per_step": st.global_newton_iterations / float(args.frames * args.record_steps),
+        "newton_its_per_step": st.global_newton_iterations / float(len(models) * args.record_steps),
         "records_completed": completed,
         "learned_guess_kept_frac": chosen / max(offered, 1),
-        "train": {"frames": args.train_frames, "samples": int(X.shape[0]), "epochs": args.train_epochs,
-                  "final_mse_normalised": loss, "data_s": round(t_data, 1), "train_s": round(t_train, 1),
-                  "network": f"{PR.n_features(tmodels[0].ndf)}-128-128-{tmodels[0].ndf} bf16 tcgen05, GELU"},
+        "train": info,
     }
+
+
+def learned3d_arm(args, device, runtime, torch):
+    """Config 3's learned predictor on 3D RC frames with rigid diaphragms (4 stories, 3x3 bays of
+    6 m, forceBeamColumn3d columns, dispBeamColumn3d beams, 148-fiber sections, a diaphragm per
+    floor) under two horizontal seeded Kanai-Tajimi records at PGA 0.4 g, dt 0.005 s: the
+    41-feature network (6 dof x 4 increments, the 8 latest samples of each ground component, the
+    height) is trained on the plain histories of 64 records (seeds 0-63) and evaluated on 32
+    unseen records (seeds 64-95), plain and learned batches of those 32 timed on the device.  The
+    frame is the largest of this family whose band fits the instance kernel's shared memory."""
+    from strut_b200 import model as Mo, workloads as W
+
+    steps = args.learned3d_steps
+
+    def case(seed):
+        return W.rc_frame3d_case(stories=4, bays_x=3, bays_y=3, steps=steps, dt=0.005, seed=seed,
+                                 element="forceBeamColumn3d", beam_element="dispBeamColumn3d",
+                                 diaphragm=True, bidirectional=True, pga_g=0.4)
+
+    train = [Mo.Model(case(s)) for s in range(64)]
+    pred, info = train_predictor(train, steps, device, runtime, 8, args.train_epochs)
+    evals = [Mo.Model(case(s)) for s in range(64, 96)]
+    ms0, st0, c0, (h0, s0), _ = timed_run(evals, steps, device, runtime, torch)
+    ms1, st1, c1, (h1, s1), (offered, chosen) = timed_run(evals, steps, device, runtime, torch, pred)
+    d0, d1 = h0[0], h1[0]
+    ok = (s0 == 0) & (s1 == 0)
+    worst = float(np.max(np.abs(d1 - d0)) / max(np.max(np.abs(d0)), 1e-300)) if ok.all() else None
+    n = len(evals) * steps
+    plain_rph = c0 / (ms0 / 1000.0) * 3600.0
+    learned_rph = c1 / (ms1 / 1000.0) * 3600.0
+    return {"workload": "diaphragm_3d_rc_frames_4s_3x3b_bidirectional", "train_records": 64,
+            "eval_records": len(evals), "steps": steps, "dt": 0.005,
+            "plain": {"records_per_hour": plain_rph, "ms": ms0, "newton_its_per_step": st0.global_newton_iterations / n,
+                      "records_completed": c0},
+            "learned": {"records_per_hour": learned_rph, "ms": ms1, "newton_its_per_step": st1.global_newton_iterations / n,
+                        "records_completed": c1, "learned_guess_kept_frac": chosen / max(offered, 1)},
+            "vs_plain": learned_rph / plain_rph if plain_rph else None,
+            "max_disp_diff_of_peak_vs_plain": worst, "train": info}
 
 
 def run_reference(args):
@@ -580,6 +643,10 @@ def main():
     if not args.no_learned:
         learned = learned_arm(args, models, device, runtime, A, torch, world)
 
+    learned3d = None
+    if rank == 0 and world == 1 and not args.no_learned3d:
+        learned3d = learned3d_arm(args, device, runtime, torch)
+
     tall = None
     if rank == 0 and world == 1 and not args.no_tall:
         tall = tall_arm(args, device, runtime, A, torch)
@@ -635,6 +702,8 @@ def main():
         if learned:
             learned["vs_plain"] = learned["value"] / value if value else None
             line["learned"] = learned
+        if learned3d:
+            line["learned_3d"] = learned3d
         if cpu:
             line["cpu_baseline"] = cpu
         if tall:
