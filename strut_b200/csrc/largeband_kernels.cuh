@@ -162,6 +162,72 @@ __global__ void __launch_bounds__(256) large_assemble_kernel(const DevInst* __re
     }
 }
 
+// The learned guess's check on the global-memory band path, between the assembly and the
+// factorisation (the instance kernel's check, the same arithmetic): one CTA per large instance.
+// At the step's first iteration from a learned guess u_l, compare |R(u_l)| with the first-order
+// residual of the Newmark predictor u_p, |R(u_l) + K_eff (u_l - u_p)|, K_eff being the band just
+// assembled (row i: columns i - bw .. i + bw at slots 0 .. 2 bw); when the learned one is the
+// larger, go back to u_p, skip this iteration's factorisation and list the elements again.
+__global__ void __launch_bounds__(256) large_learned_check_kernel(const DevInst* __restrict__ insts, InstArrays A,
+                                                                  const int* __restrict__ large_list,
+                                                                  int n_large) {
+    __shared__ double red[32];
+    __shared__ int red_r[2];
+    const int li = blockIdx.x;
+    if (li >= n_large) return;
+    const int inst = large_list[li];
+    const DevInst& I = insts[inst];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) A.skip[inst] = 0;
+    if (!A.active[inst] || A.iters[inst] != 1 || A.rejected[inst] || (A.attempt && A.attempt[inst] != 0)) return;
+    const int n = I.n, bw = I.bw, f0 = I.f_off;
+    const double* B = A.lband + I.lband_off;
+    double sl = 0.0, sp = 0.0;
+    for (int i = tid; i < n; i += nt) {
+        double kd = 0.0;
+        for (int o = 0; o <= 2 * bw; ++o) {
+            const int j = i + o - bw;
+            if (j >= 0 && j < n) kd += B[(long long)i * I.lrw + o] * (A.u_f[f0 + j] - A.u_base[f0 + j]);
+        }
+        const double r = A.R[f0 + i];
+        const double rp = r + kd;
+        sl += r * r;
+        sp += rp * rp;
+    }
+    sl = block_sum(sl, red);
+    sp = block_sum(sp, red);
+    const bool keep = isfinite(sl) && sl <= sp;
+    if (tid == 0 && A.pred_stats) {
+        A.pred_stats[2 * inst] += 1;
+        if (keep) A.pred_stats[2 * inst + 1] += 1;
+    }
+    if (keep) return;
+    for (int i = tid; i < n; i += nt) {
+        const int gi = f0 + i;
+        const double u = A.u_base[gi];
+        A.u_f[gi] = u;
+        A.u_full[A.free_dof[gi]] = u;
+    }
+    const size_t e0 = (size_t)I.elem_off * kEStride;
+    for (size_t t = tid; t < (size_t)I.n_elem * kEStride; t += nt) A.estate[e0 + t] = A.estate_base[e0 + t];
+    if (I.n_sl > 0) {
+        __syncthreads();
+        enforce_slaves(I, A);
+    }
+    if (tid == 0) {
+        A.iters[inst] -= 1;  // the rejected evaluation is not a Newton iteration of the step
+        A.rejected[inst] = 1;
+        A.skip[inst] = 1;
+        red_r[0] = A.ctl ? atomicAdd(&A.el.count[(A.ctl->iter + 1) & 1], I.n_elem) : -1;
+    }
+    __syncthreads();
+    const int base = red_r[0];
+    if (base >= 0) {
+        const int buf = (A.ctl->iter + 1) & 1;
+        for (int k = tid; k < I.n_elem; k += nt) A.el.list[buf][base + k] = list_entry(A.el, buf, I.elem_off + k);
+    }
+}
+
 // ---- blocked band LU with partial pivoting -------------------------------------------------
 
 // Copies the exported band of every large instance into its factorisation band (fill slots
@@ -258,7 +324,7 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
     for (int li = 0; li < n_large; ++li) {
         const int inst = large_list[li];
         const DevInst& I = insts[inst];
-        if (mode == INST_MODE_NEWTON && !A.active[inst]) {
+        if (mode == INST_MODE_NEWTON && (!A.active[inst] || (A.skip && A.skip[inst]))) {
             if (blockIdx.x == 0 && tid == 0) A.lstatus[li] = LSTAT_IDLE;
             continue;
         }

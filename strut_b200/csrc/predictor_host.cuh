@@ -12,6 +12,7 @@ struct PredState {
     float* d_y = nullptr;
     long long* d_stats = nullptr;
     int* d_rejected = nullptr;
+    int* d_skip = nullptr;
     bool owns_base = false;  // u_base / estate_base were allocated for the predictor
     ~PredState() {
         for (void* p : allocs) cudaFree(p);
@@ -94,6 +95,7 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     h->A.hist_du = nullptr;
     h->A.pred_stats = nullptr;
     h->A.rejected = nullptr;
+    h->A.skip = nullptr;
     if (h->pred_owns_base) {
         h->A.u_base = nullptr;
         h->A.estate_base = nullptr;
@@ -101,8 +103,6 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     }
     if (!m) return STRUT_OK;  // detached: the plain method
     if (h->ndf_all < 0) return fail(STRUT_UNSUPPORTED, "the learned predictor needs instances of one ndf");
-    if (h->n_large > 0)
-        return fail(STRUT_UNSUPPORTED, "the learned predictor runs on instances whose band fits in shared memory");
     for (const DevInst& I : h->insts)
         for (int k = 0; k < I.n_att; ++k)
             if (I.att_alg[k] != STRUT_ALGORITHM_NEWTON)
@@ -149,7 +149,7 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
         (rc = pred_alloc(ps, &ps->d_xt, (size_t)ps->n_tiles * kMlpBytesX / 2)) ||
         (rc = pred_alloc(ps, &ps->d_y, (size_t)nn * ndf)) ||
         (rc = pred_alloc(ps, &ps->d_stats, (size_t)2 * h->n_inst)) ||
-        (rc = pred_alloc(ps, &ps->d_rejected, (size_t)h->n_inst)))
+        (rc = pred_alloc(ps, &ps->d_rejected, (size_t)h->n_inst)) || (rc = pred_alloc(ps, &ps->d_skip, (size_t)h->n_inst)))
         return bail(rc);
     double* d_u_base = h->A.u_base;
     double* d_estate_base = h->A.estate_base;
@@ -175,6 +175,7 @@ int strut_gpu_set_predictor(StrutHandle* h, StrutMlp* m, const float* x_mean, co
     h->pred = ps;
     h->A.dual = 1;
     h->A.rejected = ps->d_rejected;
+    h->A.skip = ps->d_skip;
     h->A.u_base = d_u_base;
     h->A.estate_base = d_estate_base;
     h->pred_owns_base = ps->owns_base;

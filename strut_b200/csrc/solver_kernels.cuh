@@ -55,6 +55,7 @@ struct InstArrays {
     // back to the predictor
     int dual;
     int* rejected;
+    int* skip;              // global-memory band path: skip the factorisation this iteration
     double* estate;
     long long* pred_stats;  // per instance: first iterations offered, learned guess chosen
     double* hist_du;        // 4 x n_free ring of converged increments (slot = step % 4)

@@ -504,6 +504,10 @@ static int launch_large(StrutHandle* h, int mode, const DevInst* insts = nullptr
     }
     CK(cudaGetLastError());
     if (mode == INST_MODE_EXPORT) return STRUT_OK;
+    if (mode == INST_MODE_NEWTON && A.dual && A.skip) {
+        large_learned_check_kernel<<<h->n_large, 256, 0, h->stream>>>(insts, A, h->d_large_list, h->n_large);
+        CK(cudaGetLastError());
+    }
     {
         int n_large = h->n_large;
         GridBarrier* gb = h->d_gb;
