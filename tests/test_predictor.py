@@ -156,3 +156,37 @@ def test_learned_predictor_on_diaphragm_frames(gpu_lib):
     nn = X.shape[0] // (steps + 1)
     host = (X[steps * nn:(steps + 1) * nn] - pred.x_mean) * pred.x_scale
     assert np.allclose(dev[:nn], host, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_learned_predictor_on_the_wide_band_path(gpu_lib):
+    """A 5-story 3x3-bay diaphragm frame, whose band is factored in global memory: a network
+    trained on the 4-story frames of the same family proposes the guesses; the check between
+    the wide-band assembly and factorisation keeps or rejects them, and the run stays within 1e-7
+    of peak of the plain run."""
+    steps = 120
+    train = [PR.record_all_dofs(M.Model(_diaphragm_case(s, steps))) for s in range(4)]
+    with gpu_lib.Analysis(train) as an:
+        an.run(steps)
+        hists = [PR.free_history(an, i) for i in range(len(train))]
+    Xs, Ts = zip(*[PR.raw_features(m, h) for m, h in zip(train, hists)])
+    pred = PR.LearnedPredictor(6, seed=5)
+    pred.fit(np.concatenate(Xs), np.concatenate(Ts), epochs=20, batch=4096, lr=2e-3, seed=6)
+    case = W.rc_frame3d_case(stories=5, bays_x=3, bays_y=3, steps=steps, dt=0.005, seed=70,
+                             element="forceBeamColumn3d", beam_element="dispBeamColumn3d",
+                             diaphragm=True, bidirectional=True, pga_g=0.4)
+    m = M.Model(case)
+    with gpu_lib.Analysis([m]) as plain:
+        _bw, rw = plain.band_info(0)
+        assert m.num_free * rw * 8 > 220 * 1024  # the global-memory band path
+        plain.run(steps)
+        d0, _e0, _i0 = plain.history(0)
+    with gpu_lib.Analysis([M.Model(case)]) as learned:
+        pred.attach(learned)
+        learned.run(steps)
+        d1, _e1, _i1 = learned.history(0)
+        offered, chosen = PR.stats(learned)
+    assert offered == steps
+    for j in range(d0.shape[1]):
+        if np.max(np.abs(d0[:, j])) > 0.0:
+            assert rel_err_of_peak(d1[:, j], d0[:, j]) <= 1e-7
