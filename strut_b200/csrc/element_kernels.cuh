@@ -610,10 +610,15 @@ __device__ __forceinline__ void flex_terms(double* o, double wL, double bmi, dou
 // _force_beam_column2d_try_increment (force_beam_column2d.mojo:804-1189), executed
 // collectively: every thread evaluates fibers, warp 0 runs the element algebra with one lane per
 // integration point.  Starting state: S.q, S.vs_*; on success S.q / S.vs_* hold the converged
-// state, S.best the result, and the section-response cache is refreshed.
-__device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const StageView& sv,
+// state, S.best the result, and the section-response cache is refreshed.  Compiled once (not
+// inlined): an attempt run by the sequential loop and the same attempt run by a fanned-out CTA
+// execute the same instructions, so their floating-point results are the same bit for bit.
+// stop / my: a fanned-out attempt (my = its index) gives up as soon as *stop, the earliest
+// successful attempt of its element, is below it; null in the sequential order.
+__device__ __noinline__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const StageView& sv,
                                   const DevElem& E, ElemScratch& S, const double* base,
-                                  const double* dv, int scheme, const double* ys, double* fo) {
+                                  const double* dv, int scheme, const double* ys, double* fo,
+                                  const int* stop, int my) {
     const int tid = threadIdx.x, lane = tid & 31;
     const bool w0 = tid < 32;
     const int nip = E.nip;
@@ -772,6 +777,8 @@ __device__ bool fbc_try_increment(const Geo& g, const DevSection& sd, const Stag
             }
             if (lane == 0) {
                 S.local_iters++;
+                // an earlier attempt of a fanned-out element has succeeded: this one is moot
+                if (stop && *(volatile const int*)stop < my) res = 0;
                 S.flag = res;
                 if (res) {
                     S.q[0] = q0;
@@ -885,7 +892,9 @@ __device__ __noinline__ int fan_attempt(const Geo& g, const DevSection& sd, cons
         }
     }
     __syncthreads();
-    const bool ok = fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme, ys, fo);
+    int* first = el.fan_first + cur * kFanCap + fslot;
+    const bool ok = fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme, ys, fo, first, fa);
+    if (ok && threadIdx.x == 0) atomicMin(first, fa);
     double* const slot_rec = el.fan_rec + (size_t)(cur * kFanCap + fslot) * kFanAttempts * kFanRec;
     double* rec = slot_rec + (size_t)fa * kFanRec;
     if (tid == 0) {
@@ -1062,8 +1071,8 @@ struct RecPass {
 };
 
 // State determination of every element of the active instances: k (nd x nd global), f (nd)
-// and the element state.  One CTA of NT threads (kTeamThreads, or half as many with two CTAs per
-// SM) per element at a time.
+// and the element state.  One CTA of kTeamThreads threads (or half as many, two CTAs per SM) per
+// element at a time; one compiled kernel serves both block sizes, so the arithmetic is the same.
 //
 // Persistent: the grid is sized to the resident CTAs of the device and each CTA claims elements
 // from the list of the instances still iterating (all elements when all_elems is set), so a
@@ -1071,8 +1080,8 @@ struct RecPass {
 // up elements queued behind it on the same CTA.
 //
 // DIM 2 instantiates the 2D elements' code only, DIM 3 the 3D elements' (a batch holds one kind).
-template <int DIM, int NT>
-__global__ void __launch_bounds__(NT, kTeamThreads / NT) element_state_kernel(
+template <int DIM>
+__global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     const DevElem* __restrict__ elems, Geo g, FiberState fs, const double* __restrict__ u_full,
     double* __restrict__ estate, double* __restrict__ ek, double* __restrict__ ef,
     const int* __restrict__ active, int* __restrict__ status, int* __restrict__ elem_err,
@@ -1337,7 +1346,7 @@ __global__ void __launch_bounds__(NT, kTeamThreads / NT) element_state_kernel(
                     }
                 }
                 __syncthreads();
-                if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.zero3, scheme, ys, fo)) continue;
+                if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.zero3, scheme, ys, fo, nullptr, 0)) continue;
                 if (tid == 0) S.best_ok = 1;
                 converged = 1;
                 break;
@@ -1378,7 +1387,7 @@ __global__ void __launch_bounds__(NT, kTeamThreads / NT) element_state_kernel(
                         }
                     }
                     __syncthreads();
-                    if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme, ys, fo)) continue;
+                    if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme, ys, fo, nullptr, 0)) continue;
                     if (tid == 0) {
                         for (int i = 0; i < 3; ++i) {
                             S.acc_v[i] = S.tv[i];

@@ -14,9 +14,10 @@
 //
 // Persistent CTAs, one per SM, walk the instance tiles with a two-stage pipeline: while the
 // threads update tile k in shared memory, the TMA unit (cp.async.bulk, mbarrier completion, no
-// multicast) brings tile k + 1 in; the updated tile goes back with a bulk store from shared memory.
-// Inside a tile every thread takes fibers of the flattened (family, instance, fiber) order, so a
-// warp's shared-memory accesses are consecutive; the per-fiber stress and tangent (times area) go
+// multicast) brings tile k + 1 in; each thread writes its fibers' new state straight back to HBM
+// (a warp's stores are consecutive, so they coalesce), so a stage is free again as soon as it has
+// been read.  Inside a tile every thread takes fibers of the flattened (family, instance, fiber)
+// order, so a warp's shared-memory accesses are consecutive; the per-fiber stress and tangent (times area) go
 // to shared memory and each instance's sums are formed in the element kernel's fixed order (eight
 // chunks of the section's fibers, each summed sequentially, then a pairwise tree), so results do
 // not depend on the launch shape.
@@ -28,17 +29,6 @@
 namespace strut {
 
 constexpr int kFsThreads = 512;
-
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit_group() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// The shared-memory sources of every committed bulk store have been read.
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// Every committed bulk store has completed.
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // Per-tile geometry of the stage buffers, identical for every tile.
 struct FsLayout {
@@ -97,22 +87,6 @@ __device__ __forceinline__ void fs_load_tile(const FsLayout& L, const BatchState
         bulk_g2s(st + L.off_c1 + f * T * L.n_c1, bs.c1 + f * N4 + tile * T * L.n_c1, L.bytes_c1, bar);
 }
 
-// The bulk stores of an updated stage back to tile `tile` (thread 0), as one bulk group.
-__device__ __forceinline__ void fs_store_tile(const FsLayout& L, const BatchState& bs, long long N2, long long N3,
-                                              long long N1, long long N4, long long tile, const double* st) {
-    const long long T = L.T;
-    for (int f = 0; f < 5 && L.bytes_c2; ++f)
-        bulk_s2g(bs.c2 + f * N3 + tile * T * L.n_c2, st + L.off_c2 + f * T * L.n_c2, L.bytes_c2);
-    for (int f = 0; f < 10 && L.bytes_s2; ++f)
-        bulk_s2g(bs.s2 + f * N2 + tile * T * L.n_s2, st + L.off_s2 + f * T * L.n_s2, L.bytes_s2);
-    if (L.bytes_kon) bulk_s2g(bs.kon + tile * T * L.n_s2, st + L.off_kon, L.bytes_kon);
-    for (int f = 0; f < 5 && L.bytes_s1; ++f)
-        bulk_s2g(bs.s1 + f * N1 + tile * T * L.n_s1, st + L.off_s1 + f * T * L.n_s1, L.bytes_s1);
-    for (int f = 0; f < 6 && L.bytes_c1; ++f)
-        bulk_s2g(bs.c1 + f * N4 + tile * T * L.n_c1, st + L.off_c1 + f * T * L.n_c1, L.bytes_c1);
-    bulk_commit_group();
-}
-
 // n_inst instances (state allocated for n_tiles * T); ek: n_inst x 2 (eps0, kappa); resp:
 // n_inst x 5 (N, Mz, k11, k12, k22).  *err is set when a bulk copy does not complete within the
 // bounded wait.
@@ -145,11 +119,8 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
         const int s = k & 1;
         double* st = fs_smem + s * L.stage_doubles;
         const long long next = tile + gridDim.x;
-        if (next < n_tiles && tid == 0) {
-            // the other stage's last bulk store must have read its shared memory first
-            bulk_wait_read_all();
+        if (next < n_tiles && tid == 0)
             fs_load_tile(L, bs, N2, N3, N1, N4, next, fs_smem + (s ^ 1) * L.stage_doubles, &bar[s ^ 1]);
-        }
         const long long i0 = tile * T;
         const int nvalid = (int)min((long long)T, n_inst - i0);
         for (int t = tid; t < 2 * T; t += nt) strain[t] = t < 2 * nvalid ? ek[2 * i0 + t] : 0.0;
@@ -162,20 +133,25 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
                 // let the copies in flight land before the CTA stops
                 mbar_wait_bounded(&bar[s], ph);
                 if (next < n_tiles) mbar_wait_bounded(&bar[s ^ 1], (phases >> (s ^ 1)) & 1u);
-                bulk_wait_all();
             }
             return;
         }
-        // phase 1: every fiber of the tile, flattened family by family
+        // phase 1: every fiber of the tile, flattened family by family; the new committed state
+        // goes to the same places in HBM (Xg: this tile's fibers of family X, field stride NX)
         const int n_s2t = T * L.n_s2, n_c2t = T * L.n_c2, n_s1t = T * L.n_s1, n_c1t = T * L.n_c1, n_elt = T * L.n_el;
+        double* const S2g = bs.s2 + tile * n_s2t;
+        int* const Kg = bs.kon + tile * n_s2t;
+        double* const C2g = bs.c2 + tile * n_c2t;
+        double* const S1g = bs.s1 + tile * n_s1t;
+        double* const C1g = bs.c1 + tile * n_c1t;
         const int n_items = n_s2t + n_c2t + n_s1t + n_c1t + n_elt;
         for (int it = tid; it < n_items; it += nt) {
             int r = it;
             if (r < n_s2t) {
                 const int si = r / L.n_s2, j = r - si * L.n_s2;
                 if (si < nvalid) {
-                    double* F = st + L.off_s2 + r;
-                    int* K = reinterpret_cast<int*>(st + L.off_kon) + r;
+                    const double* F = st + L.off_s2 + r;
+                    const int* K = reinterpret_cast<const int*>(st + L.off_kon) + r;
                     const int gi = geo_s2 + j;
                     const double y = __ldg(g.y + gi), A = __ldg(g.a + gi);
                     S2State c, t;
@@ -184,9 +160,10 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
                     c.sigs0 = F[7 * n_s2t]; c.epsr = F[8 * n_s2t]; c.sigr = F[9 * n_s2t]; c.kon = *K;
                     steel02_trial(g.mats[__ldg(g.m + gi)], c, strain[2 * si] - y * strain[2 * si + 1], t);
                     if (commit) {
-                        F[0 * n_s2t] = t.eps; F[1 * n_s2t] = t.sig; F[2 * n_s2t] = t.tan; F[3 * n_s2t] = t.epsmin;
-                        F[4 * n_s2t] = t.epsmax; F[5 * n_s2t] = t.epspl; F[6 * n_s2t] = t.epss0;
-                        F[7 * n_s2t] = t.sigs0; F[8 * n_s2t] = t.epsr; F[9 * n_s2t] = t.sigr; *K = t.kon;
+                        double* G = S2g + r;
+                        G[0 * N2] = t.eps; G[1 * N2] = t.sig; G[2 * N2] = t.tan; G[3 * N2] = t.epsmin;
+                        G[4 * N2] = t.epsmax; G[5 * N2] = t.epspl; G[6 * N2] = t.epss0;
+                        G[7 * N2] = t.sigs0; G[8 * N2] = t.epsr; G[9 * N2] = t.sigr; Kg[r] = t.kon;
                     }
                     double* o = fk + 2 * (si * L.n_tot + j);
                     o[0] = t.sig * A;
@@ -198,15 +175,15 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
             if (r < n_c2t) {
                 const int si = r / L.n_c2, j = r - si * L.n_c2;
                 if (si < nvalid) {
-                    double* F = st + L.off_c2 + r;
+                    const double* F = st + L.off_c2 + r;
                     const int gi = geo_c2 + j;
                     const double y = __ldg(g.y + gi), A = __ldg(g.a + gi);
                     C2State c, t;
                     c.eps = F[0]; c.sig = F[n_c2t]; c.tan = F[2 * n_c2t]; c.ecmin = F[3 * n_c2t]; c.dept = F[4 * n_c2t];
                     concrete02_trial(g.mats[__ldg(g.m + gi)], c, strain[2 * si] - y * strain[2 * si + 1], t);
                     if (commit) {
-                        F[0] = t.eps; F[n_c2t] = t.sig; F[2 * n_c2t] = t.tan; F[3 * n_c2t] = t.ecmin;
-                        F[4 * n_c2t] = t.dept;
+                        double* G = C2g + r;
+                        G[0] = t.eps; G[N3] = t.sig; G[2 * N3] = t.tan; G[3 * N3] = t.ecmin; G[4 * N3] = t.dept;
                     }
                     double* o = fk + 2 * (si * L.n_tot + L.n_s2 + j);
                     o[0] = t.sig * A;
@@ -218,15 +195,15 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
             if (r < n_s1t) {
                 const int si = r / L.n_s1, j = r - si * L.n_s1;
                 if (si < nvalid) {
-                    double* F = st + L.off_s1 + r;
+                    const double* F = st + L.off_s1 + r;
                     const int gi = geo_s1 + j;
                     const double y = __ldg(g.y + gi), A = __ldg(g.a + gi);
                     S1State c, t;
                     c.eps = F[0]; c.sig = F[n_s1t]; c.tan = F[2 * n_s1t]; c.epsp = F[3 * n_s1t]; c.alpha = F[4 * n_s1t];
                     steel01_trial(g.mats[__ldg(g.m + gi)], c, strain[2 * si] - y * strain[2 * si + 1], t);
                     if (commit) {
-                        F[0] = t.eps; F[n_s1t] = t.sig; F[2 * n_s1t] = t.tan; F[3 * n_s1t] = t.epsp;
-                        F[4 * n_s1t] = t.alpha;
+                        double* G = S1g + r;
+                        G[0] = t.eps; G[N1] = t.sig; G[2 * N1] = t.tan; G[3 * N1] = t.epsp; G[4 * N1] = t.alpha;
                     }
                     double* o = fk + 2 * (si * L.n_tot + L.n_s2 + L.n_c2 + j);
                     o[0] = t.sig * A;
@@ -238,7 +215,7 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
             if (r < n_c1t) {
                 const int si = r / L.n_c1, j = r - si * L.n_c1;
                 if (si < nvalid) {
-                    double* F = st + L.off_c1 + r;
+                    const double* F = st + L.off_c1 + r;
                     const int gi = geo_c1 + j;
                     const double y = __ldg(g.y + gi), A = __ldg(g.a + gi);
                     C1State c, t;
@@ -246,8 +223,9 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
                     c.eend = F[4 * n_c1t]; c.slope = F[5 * n_c1t];
                     concrete01_trial(g.mats[__ldg(g.m + gi)], c, strain[2 * si] - y * strain[2 * si + 1], t);
                     if (commit) {
-                        F[0] = t.eps; F[n_c1t] = t.sig; F[2 * n_c1t] = t.tan; F[3 * n_c1t] = t.emin;
-                        F[4 * n_c1t] = t.eend; F[5 * n_c1t] = t.slope;
+                        double* G = C1g + r;
+                        G[0] = t.eps; G[N4] = t.sig; G[2 * N4] = t.tan; G[3 * N4] = t.emin; G[4 * N4] = t.eend;
+                        G[5 * N4] = t.slope;
                     }
                     double* o = fk + 2 * (si * L.n_tot + L.n_s2 + L.n_c2 + L.n_s1 + j);
                     o[0] = t.sig * A;
@@ -266,10 +244,7 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
                 o[1] = ks;
             }
         }
-        // the updated stage goes back to HBM while the sums are formed
-        if (commit) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (commit && tid == 0) fs_store_tile(L, bs, N2, N3, N1, N4, tile, st);
         // phase 2: thread t < 8 T sums chunk t % 8 of instance t / 8 (the element kernel's order:
         // running sums over a chunk, the elastic fibers' k12 apart, then a pairwise tree)
         {
@@ -321,9 +296,8 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
                 }
             }
         }
-        __syncthreads();  // fk and strain are rewritten for the next tile
+        __syncthreads();  // fk, strain and this stage are rewritten for later tiles
     }
-    if (tid == 0) bulk_wait_all();
 }
 
 }  // namespace strut

@@ -145,6 +145,8 @@ struct ElemList {
                         // handed out; every launch over the list adds kFanAttempts, so the
                         // last attempt of a launch is the one that finds count % 12 == 11
     double* fan_rec;    // 2 x kFanCap x kFanAttempts x kFanRec attempt records
+    int* fan_first;     // 2 x kFanCap: the earliest attempt that has succeeded (kFanAttempts:
+                        // none yet); a later attempt stops as soon as it sees an earlier success
 };
 
 // List entry of element e in list buffer `buf`: a flagged element also gets a fan slot.
@@ -154,6 +156,7 @@ __device__ __forceinline__ int list_entry(const ElemList& el, int buf, int e) {
         if (slot < kFanCap) {
             el.hard[buf][slot] = e;
             el.fan_done[buf * kFanCap + slot] = 0;
+            el.fan_first[buf * kFanCap + slot] = kFanAttempts;
             return e | kFanBit;
         }
     }

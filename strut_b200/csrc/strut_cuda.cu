@@ -407,14 +407,12 @@ static int prof_end(StrutHandle* h, int k) {
 // Element state kernel: kTeamThreads threads per element CTA.  Commit kernel: one team of 128
 // threads per integration point up to 5 points, else 64.
 using CommitKernel = decltype(&commit_kernel<128>);
-using ElemKernel = decltype(&element_state_kernel<2, kTeamThreads>);
+using ElemKernel = decltype(&element_state_kernel<2>);
 static int elem_threads_of(const StrutHandle* h) {
     return h->tune.element_threads == kTeamThreads / 2 ? kTeamThreads / 2 : kTeamThreads;
 }
 static ElemKernel elem_kernel_of(const StrutHandle* h) {
-    if (elem_threads_of(h) == kTeamThreads)
-        return h->ndf_all == 6 ? element_state_kernel<3, kTeamThreads> : element_state_kernel<2, kTeamThreads>;
-    return h->ndf_all == 6 ? element_state_kernel<3, kTeamThreads / 2> : element_state_kernel<2, kTeamThreads / 2>;
+    return h->ndf_all == 6 ? element_state_kernel<3> : element_state_kernel<2>;
 }
 static dim3 elem_block(const StrutHandle* h) { return dim3(elem_threads_of(h)); }
 // Resident CTAs of the element kernel the handle's tuning selects (its persistent grid).
@@ -1409,7 +1407,8 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         (rc = dzeros(&A.el.list[0], (size_t)h->n_elem, al)) || (rc = dzeros(&A.el.list[1], (size_t)h->n_elem, al)) ||
         (rc = dzeros(&A.el.count, 2, al)) || (rc = dzeros(&A.el.next, 2, al)) ||
         (rc = dzeros(&A.el.hard[0], (size_t)kFanCap, al)) || (rc = dzeros(&A.el.hard[1], (size_t)kFanCap, al)) ||
-        (rc = dzeros(&A.el.hard_count, 2, al)) || (rc = dzeros(&A.el.fan_done, (size_t)2 * kFanCap, al)))
+        (rc = dzeros(&A.el.hard_count, 2, al)) || (rc = dzeros(&A.el.fan_done, (size_t)2 * kFanCap, al)) ||
+        (rc = dzeros(&A.el.fan_first, (size_t)2 * kFanCap, al)))
         return bail(rc);
     {
         // attempt fan-out of forceBeamColumn2d elements (none in a 3D handle)

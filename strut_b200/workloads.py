@@ -415,19 +415,32 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
                     system: str = "BandGeneral", zeta: float = 0.05, geom: str = "Linear",
                     bidirectional: bool = False, record_elements=(1,), diaphragm: bool = False,
                     beam_element: str | None = None, sections=None,
-                    diaphragm_mass: float | None = None, slabs: dict | None = None) -> dict:
+                    diaphragm_mass: float | None = None, slabs: dict | None = None,
+                    slab_mesh: int = 1) -> dict:
     """3D RC frame: columns along z, beams along x and y, base fixed in all six dofs.  With
     ``diaphragm`` every floor is a rigid diaphragm (perp_dirn 3) retained by its central node,
     which carries the floor's horizontal masses and rotational inertia; the other nodes keep
     their vertical mass only.  ``beam_element`` (default: ``element``) sets the beams' type;
     ``sections`` replaces the (column, beam) sections; ``diaphragm_mass`` is the floor's total
-    horizontal mass (default: floor_mass per node)."""
+    horizontal mass (default: floor_mass per node).  ``slab_mesh`` m > 1 meshes every bay's slab
+    with m x m shells: the floor grid gets nodes every bay_w / m, beams are split at them (one
+    element per segment), columns stay at the bay corners, and the Rayleigh coefficients are
+    those of the same frame with whole-bay beams and no slab."""
+    ms = max(1, int(slab_mesh))
+    if ms > 1:
+        coarse = rc_frame3d_case(stories, bays_x, bays_y, story_h, bay_w, nip, floor_mass, dt, steps,
+                                 seed, wg, zg, pga_g, tol, max_iters, element, system, zeta, geom,
+                                 bidirectional, record_elements, diaphragm, beam_element, sections,
+                                 diaphragm_mass, None, 1)
+    bays_x, bays_y, bay_w = bays_x * ms, bays_y * ms, bay_w / ms
     nodes = []
     grid = {}
     nid = 1
     for k in range(stories + 1):
         for j in range(bays_y + 1):
             for i in range(bays_x + 1):
+                if k == 0 and (i % ms or j % ms):
+                    continue  # no column below a slab-only node
                 n = {"id": nid, "x": i * bay_w, "y": j * bay_w, "z": k * story_h}
                 if k == 0:
                     n["constraints"] = [1, 2, 3, 4, 5, 6]
@@ -444,16 +457,16 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
         eid += 1
 
     for k in range(stories):
-        for j in range(bays_y + 1):
-            for i in range(bays_x + 1):
+        for j in range(0, bays_y + 1, ms):
+            for i in range(0, bays_x + 1, ms):
                 add(grid[(k, j, i)], grid[(k + 1, j, i)], 1)
     bt = beam_element or element
     for k in range(1, stories + 1):
-        for j in range(bays_y + 1):
+        for j in range(0, bays_y + 1, ms):
             for i in range(bays_x):
                 add(grid[(k, j, i)], grid[(k, j, i + 1)], 2, bt)
         for j in range(bays_y):
-            for i in range(bays_x + 1):
+            for i in range(0, bays_x + 1, ms):
                 add(grid[(k, j, i)], grid[(k, j + 1, i)], 2, bt)
     if slabs:
         # one ShellMITC4 per bay and floor on the beam-column joints (counter-clockwise seen
@@ -540,6 +553,9 @@ def rc_frame3d_case(stories: int = 2, bays_x: int = 2, bays_y: int = 2, story_h:
     if record_elements:
         case["recorders"].append({"type": "element_force", "elements": list(record_elements),
                                   "output": "elements"})
+    if ms > 1:
+        case["rayleigh"] = dict(coarse["rayleigh"])
+        return case
     K, M, _free = initial_stiffness_3d(case)
     m_idx = np.where(M > 0.0)[0]
     z_idx = np.where(M == 0.0)[0]
@@ -571,6 +587,37 @@ def tall_frame3d_case(stories: int = 20, bays: int = 6, steps: int = 4000, dt: f
                            diaphragm=True, diaphragm_mass=400.0e3, bidirectional=True,
                            sections=[rc_section_208(1, 0.7, 0.7), rc_section_208(2, 0.5, 0.7)],
                            record_elements=record_elements)
+
+
+SLAB = {"E": 30.0e9, "nu": 0.2, "h": 0.2, "rho": 0.0}
+
+
+def slab_frame3d_case(stories: int, bays: int, steps: int = 4000, dt: float = 0.005, seed: int = 8000,
+                      pga_g: float = 0.45, wg: float = 15.0, record_elements=(1,)) -> dict:
+    """A frame of the batched slab-frame set: a 3D RC frame of `stories` stories and bays x bays
+    bays of 7 m (story height 3.5 m), forceBeamColumn3d columns (0.7 x 0.7 m) and dispBeamColumn3d
+    beams (0.5 x 0.7 m) with 5 Lobatto points and 208-fiber sections, ShellMITC4 floor slabs on an
+    ElasticMembranePlateSection (E 30 GPa, nu 0.2, h 0.2 m, massless) meshed 2 x 2 per bay, a rigid
+    diaphragm per floor carrying 400 t, two horizontal seeded Kanai-Tajimi records at `pga_g`."""
+    sec = [rc_section_208(1, 0.7, 0.7), rc_section_208(2, 0.5, 0.7),
+           {"id": 3, "type": "ElasticMembranePlateSection", "params": dict(SLAB)}]
+    return rc_frame3d_case(stories=stories, bays_x=bays, bays_y=bays, story_h=3.5, bay_w=7.0, nip=5, dt=dt,
+                           steps=steps, seed=seed, pga_g=pga_g, wg=wg, element="forceBeamColumn3d",
+                           beam_element="dispBeamColumn3d", diaphragm=True, diaphragm_mass=400.0e3,
+                           bidirectional=True, sections=sec, slabs=dict(SLAB), slab_mesh=2,
+                           record_elements=record_elements)
+
+
+def slab_frame_params(n: int, base_seed: int = 8000, max_bays: int = 6):
+    """Sizes and records of the batched slab-frame set: stories U{10..30}, bays U{4..max_bays},
+    PGA U(0.3, 0.6) g, wg U(8, 25) rad/s, record i seeded with base_seed + i."""
+    out = []
+    for i in range(n):
+        rng = np.random.default_rng(base_seed + i)
+        out.append(dict(stories=int(rng.integers(10, 31)), bays=int(rng.integers(4, max_bays + 1)),
+                        pga_g=float(rng.uniform(0.3, 0.6)), wg=float(rng.uniform(8.0, 25.0)),
+                        seed=base_seed + i))
+    return out
 
 
 def batched_frame_params(n: int = 256, base_seed: int = 1000):

@@ -16,7 +16,6 @@ import pytest
 
 from strut_b200 import model as M
 from strut_b200 import workloads as W
-from tests.helpers import rel_err_of_peak
 
 pytestmark = pytest.mark.gpu
 
@@ -35,18 +34,22 @@ def record_everything(case: dict) -> dict:
 
 
 def compare_histories(gd, ge, gi, rd, re, ri):
-    """(worst displacement error of peak, worst element-force error of peak, steps whose
-    iteration counts differ)."""
-    worst_d = 0.0
-    for j in range(rd.shape[1]):
-        if np.max(np.abs(rd[:, j])) > 0.0:
-            worst_d = max(worst_d, rel_err_of_peak(gd[:, j], rd[:, j]))
-    worst_e = 0.0
-    for j in range(re.shape[1]):
-        for c in range(re.shape[2]):
-            if np.max(np.abs(re[:, j, c])) > 0.0:
-                worst_e = max(worst_e, rel_err_of_peak(ge[:, j, c], re[:, j, c]))
-    return worst_d, worst_e, int(np.sum(gi != ri))
+    """(worst displacement error, worst element-force error, steps whose iteration counts
+    differ).  Each history's error is taken relative to its peak, the peak floored at 1e-6 of the
+    largest history of the same recorder: a history that is zero in exact arithmetic (the axial
+    displacement of a transversely excited cantilever, say) holds only rounding noise, and its
+    own peak is no scale for it."""
+    def worst(g, r):
+        r2 = r.reshape(r.shape[0], -1)
+        g2 = g.reshape(g.shape[0], -1)
+        if r2.size == 0:
+            return 0.0
+        peaks = np.max(np.abs(r2), axis=0)
+        floor = 1e-6 * float(peaks.max())
+        if floor == 0.0:
+            return float(np.max(np.abs(g2)))
+        return float(np.max(np.max(np.abs(g2 - r2), axis=0) / np.maximum(peaks, floor)))
+    return worst(gd, rd), worst(ge, re), int(np.sum(gi != ri))
 
 
 def test_config0_full_record(gpu_lib, oracle):
