@@ -35,6 +35,11 @@ namespace strut {
 
 constexpr int kPanel = 32;         // panel width of the blocked band LU
 constexpr int kLargeThreads = 384; // threads of a factorisation CTA (one per panel row)
+// The variant for wider bands: 16-column panels and 640 threads (the panel rows' registers halve,
+// so more rows fit a CTA).  Every entry receives the same subtractions in the same column order
+// with either variant, so their results are the same bit for bit.
+constexpr int kPanelWide = 16;
+constexpr int kLargeThreadsWide = 640;
 constexpr int kSolveThreads = 1024;
 
 constexpr int kColTile = 16;       // trailing-update columns per tile
@@ -258,10 +263,13 @@ __global__ void large_load_exported_kernel(const DevInst* __restrict__ insts, In
 // (kPanel x (kPanel + 1)); CTA 0's panel rows (kLargeThreads x (kPanel + 1)), whose space the
 // column slab of the trailing phase ((kPanel + bw) x (kColTile + 2)) reuses; the row at the
 // diagonal (two, by column parity) and the row that replaces it; the panel's row permutation.
-__host__ __device__ inline size_t large_factor_smem(int bw) {
-    (void)bw;
-    return sizeof(double) * ((size_t)kPanel * (kPanel + 1) + (size_t)kLargeThreads * (kPanel + 1) + 3 * kPanel) +
-           sizeof(int) * (size_t)kLargeThreads;
+// Row stride of the panel-row buffer, which the slab (stride kColTile + 2) reuses.
+__host__ __device__ constexpr int large_row_stride(int panel) {
+    return panel + 1 > kColTile + 2 ? panel + 1 : kColTile + 2;
+}
+__host__ __device__ inline size_t large_factor_smem(int panel, int threads) {
+    return sizeof(double) * ((size_t)panel * (panel + 1) + (size_t)threads * large_row_stride(panel) + 3 * panel) +
+           sizeof(int) * (size_t)threads;
 }
 
 // Column tiles of the trailing update of one panel (+1: the right-hand side): the CTAs a
@@ -270,8 +278,9 @@ __host__ __device__ inline int large_factor_tiles(int bw) {
     return (2 * bw + kColTile - 1) / kColTile + 1;
 }
 
-// Largest half-band the factorisation takes: one thread per panel row.
+// Largest half-band each variant takes: one thread per panel row.
 constexpr int kLargeMaxBw = kLargeThreads - kPanel;
+constexpr int kLargeMaxBwWide = kLargeThreadsWide - kPanelWide;
 
 // Argmax over a warp, the first (smallest index) of equal values winning.
 __device__ __forceinline__ void warp_argmax_first(double& v, int& idx) {
@@ -300,25 +309,27 @@ __device__ __forceinline__ void warp_argmax_first(double& v, int& idx) {
 // permutation applied, solves the panel rows against the unit lower L11 on the warps (lane =
 // row), subtracts L21 U12 from the rows below entry by entry in column order (one thread per
 // row, the row's multipliers in registers); grid barrier.
-__global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
+template <int PANEL, int THREADS>
+__global__ void __launch_bounds__(THREADS) large_factor_kernel(
     const DevInst* __restrict__ insts, InstArrays A, const int* __restrict__ large_list,
     int n_large, int mode, GridBarrier* gb, double* wbuf, double* lpan, int* lperm) {
     extern __shared__ __align__(16) double smem_lf[];
     __shared__ int s_flag[2];
-    __shared__ int s_piv[kPanel];
+    __shared__ int s_piv[PANEL];
     __shared__ double red[32];
     __shared__ int red_r[32];
-    constexpr int kPs = kPanel + 1;     // row stride of the panel rows and L11
+    constexpr int kPs = PANEL + 1;     // row stride of L11
+    constexpr int kRs = large_row_stride(PANEL);  // row stride of the panel rows and the slab
     constexpr int kSs = kColTile + 2;   // row stride of the slab (even: 16-byte rows)
-    constexpr int kLd = kLargeThreads;  // leading dimension of lpan
+    constexpr int kLd = THREADS;  // leading dimension of lpan
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5;
     const int nwarps = nt >> 5;
-    double* L11 = smem_lf;                              // kPanel x kPs
-    double* Pout = L11 + kPanel * kPs;                  // panel rows (CTA 0), kLargeThreads x kPs
+    double* L11 = smem_lf;                              // PANEL x kPs
+    double* Pout = L11 + PANEL * kPs;                  // panel rows (CTA 0), THREADS x kRs
     double* S = Pout;                                   // slab of the trailing phase, pr x kSs
-    double* prow2 = Pout + (size_t)kLargeThreads * kPs; // row at the diagonal, by column parity
-    double* crow = prow2 + 2 * kPanel;                  // the row that replaces it
-    int* s_perm = (int*)(crow + kPanel);                // panel row -> original row
+    double* prow2 = Pout + (size_t)THREADS * kRs;       // row at the diagonal, by column parity
+    double* crow = prow2 + 2 * PANEL;                  // the row that replaces it
+    int* s_perm = (int*)(crow + PANEL);                // panel row -> original row
     unsigned int gen = 0;
     if (tid == 0) gen = atomicAdd(&gb->gen, 0u);
     for (int li = 0; li < n_large; ++li) {
@@ -343,7 +354,7 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                 continue;
             }
         }
-        const int P = min(kPanel, max(bw, 1));
+        const int P = min(PANEL, max(bw, 1));
         int result = LSTAT_OK;
         int pivoted = 0;
         for (int k0 = 0; k0 < n && result == LSTAT_OK; k0 += P) {
@@ -366,14 +377,14 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                     }
 #pragma unroll
                     for (int m = 0; m < 4; ++m)
-                        if (rb + m * nwarps < pr) Pout[(rb + m * nwarps) * kPs + lane] = v[m];
+                        if (rb + m * nwarps < pr && lane < PANEL) Pout[(rb + m * nwarps) * kRs + lane] = v[m];
                 }
                 if (own) s_perm[r] = r;
                 if (tid == 0) s_flag[0] = LSTAT_OK;
                 __syncthreads();
-                double a[kPanel];  // a[q] = column c0 + q of this thread's row
+                double a[PANEL];  // a[q] = column c0 + q of this thread's row
 #pragma unroll
-                for (int q = 0; q < kPanel; ++q) a[q] = own ? Pout[r * kPs + q] : 0.0;
+                for (int q = 0; q < PANEL; ++q) a[q] = own ? Pout[r * kRs + q] : 0.0;
                 bool failed = false;
                 for (int c0 = 0; c0 < kb; c0 += 4) {
 #pragma unroll
@@ -383,10 +394,10 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                             const int last = min(pr - 1, c + bw);  // rows of column k0+c in the band
                             const bool act = own && r > c && r <= last;
                             // double buffered: a slow thread may still read the previous one
-                            double* prow = prow2 + (c & 1) * kPanel;
+                            double* prow = prow2 + (c & 1) * PANEL;
                             if (r == c) {
 #pragma unroll
-                                for (int q = 0; q < kPanel; ++q) prow[q] = a[q];
+                                for (int q = 0; q < PANEL; ++q) prow[q] = a[q];
                             }
                             __syncthreads();
                             // the reference's strict '>' scan keeps the diagonal unless a row
@@ -417,7 +428,7 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                                     pivoted = 1;
                                     if (r == p) {
 #pragma unroll
-                                        for (int q = 0; q < kPanel; ++q) crow[q] = a[q];
+                                        for (int q = 0; q < PANEL; ++q) crow[q] = a[q];
                                     }
                                     if (tid == 0) {
                                         const int o = s_perm[c];
@@ -426,17 +437,17 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                                     }
                                     if (wid == 0 && lane < c0) {
                                         // finished columns of earlier steps
-                                        const double t0 = Pout[c * kPs + lane];
-                                        Pout[c * kPs + lane] = Pout[p * kPs + lane];
-                                        Pout[p * kPs + lane] = t0;
+                                        const double t0 = Pout[c * kRs + lane];
+                                        Pout[c * kRs + lane] = Pout[p * kRs + lane];
+                                        Pout[p * kRs + lane] = t0;
                                     }
                                     __syncthreads();
                                     if (r == c) {
 #pragma unroll
-                                        for (int q = 0; q < kPanel; ++q) a[q] = crow[q];
+                                        for (int q = 0; q < PANEL; ++q) a[q] = crow[q];
                                     } else if (r == p) {
 #pragma unroll
-                                        for (int q = 0; q < kPanel; ++q) a[q] = prow[q];
+                                        for (int q = 0; q < PANEL; ++q) a[q] = prow[q];
                                     }
                                     pivrow = crow;
                                 }
@@ -446,7 +457,7 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                                     const double f = a[cc] / pivrow[cc];
                                     a[cc] = f;
 #pragma unroll
-                                    for (int q = cc + 1; q < kPanel; ++q)
+                                    for (int q = cc + 1; q < PANEL; ++q)
                                         if (c0 + q < kb) a[q] = fma(-f, pivrow[q], a[q]);
                                 }
                                 if (tid == 0) s_piv[c] = p;
@@ -457,19 +468,19 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                     if (own) {
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
-                            if (c0 + q < kPanel) Pout[r * kPs + c0 + q] = a[q];
+                            if (c0 + q < PANEL) Pout[r * kRs + c0 + q] = a[q];
                     }
 #pragma unroll
-                    for (int q = 0; q < kPanel; ++q) a[q] = q + 4 < kPanel ? a[q + 4] : 0.0;
+                    for (int q = 0; q < PANEL; ++q) a[q] = q + 4 < PANEL ? a[q + 4] : 0.0;
                 }
                 __syncthreads();
                 if (s_flag[0] == LSTAT_OK) {
                     for (int t = tid; t < kb * pr; t += nt) {
                         const int q = t / pr, rr = t - q * pr;
-                        lpan[q * kLd + rr] = Pout[rr * kPs + q];
+                        lpan[q * kLd + rr] = Pout[rr * kRs + q];
                     }
                     for (int rr = wid; rr < kb; rr += nwarps)
-                        if (lane >= rr && lane < kb) B[lslot(lrw, bw, k0 + rr, k0 + lane)] = Pout[rr * kPs + lane];
+                        if (lane >= rr && lane < kb) B[lslot(lrw, bw, k0 + rr, k0 + lane)] = Pout[rr * kRs + lane];
                     if (own) lperm[r] = s_perm[r];
                 }
                 if (tid == 0) {
@@ -492,14 +503,14 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
                 continue;
             }
             // this thread's panel row: its multipliers (L21, or L11 for the first kb rows)
-            double lrow[kPanel];
+            double lrow[PANEL];
 #pragma unroll
-            for (int q = 0; q < kPanel; ++q) lrow[q] = (own && q < kb) ? lpan[q * kLd + r] : 0.0;
+            for (int q = 0; q < PANEL; ++q) lrow[q] = (own && q < kb) ? lpan[q * kLd + r] : 0.0;
             if (own) {
                 s_perm[r] = lperm[r];
                 if (r < kb) {
 #pragma unroll
-                    for (int q = 0; q < kPanel; ++q) L11[r * kPs + q] = lrow[q];
+                    for (int q = 0; q < PANEL; ++q) L11[r * kPs + q] = lrow[q];
                 }
             }
             for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -547,7 +558,7 @@ __global__ void __launch_bounds__(kLargeThreads) large_factor_kernel(
 #pragma unroll
                     for (int q = 0; q < kColTile; ++q) v[q] = S[r * kSs + q];
 #pragma unroll
-                    for (int sc = 0; sc < kPanel; ++sc) {
+                    for (int sc = 0; sc < PANEL; ++sc) {
                         if (sc < kb) {
                             const double f = lrow[sc];
 #pragma unroll

@@ -303,6 +303,7 @@ struct StrutHandle {
     int* d_large_rowbase = nullptr;
     GridBarrier* d_gb = nullptr;
     double* d_wbuf = nullptr;
+    int lfactor_wide = 0;      // the 16-column / 640-thread factorisation (half bands beyond 352)
     double* d_lpan = nullptr;  // factored panel, CTA 0 -> the other CTAs
     int* d_lpiv = nullptr;     // its row permutation
     int n_slaves_total = 0;          // slave dofs of every instance (multi-point constraints)
@@ -515,8 +516,14 @@ static int launch_large(StrutHandle* h, int mode, const DevInst* insts = nullptr
         int* lpiv = h->d_lpiv;
         void* args[] = {(void*)&insts, (void*)&A,  (void*)&ll,   (void*)&n_large, (void*)&mode,
                         (void*)&gb,    (void*)&wb, (void*)&lpan, (void*)&lpiv};
-        CK(cudaLaunchCooperativeKernel((const void*)large_factor_kernel, dim3(h->lfactor_grid),
-                                       dim3(kLargeThreads), args, h->lfactor_smem, h->stream));
+        if (h->lfactor_wide)
+            CK(cudaLaunchCooperativeKernel((const void*)large_factor_kernel<kPanelWide, kLargeThreadsWide>,
+                                           dim3(h->lfactor_grid), dim3(kLargeThreadsWide), args, h->lfactor_smem,
+                                           h->stream));
+        else
+            CK(cudaLaunchCooperativeKernel((const void*)large_factor_kernel<kPanel, kLargeThreads>,
+                                           dim3(h->lfactor_grid), dim3(kLargeThreads), args, h->lfactor_smem,
+                                           h->stream));
     }
     large_solve_kernel<<<h->n_large, kSolveThreads, large_solve_smem(h->max_large_n), h->stream>>>(insts, A, h->d_large_list, h->n_large, mode,
                                                                     h->d_wbuf, h->d_gb);
@@ -1262,8 +1269,9 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             for (int k = 0; k < I.n_att; ++k)
                 if (I.att_alg[k] != STRUT_ALGORITHM_NEWTON)
                     return bail(fail(STRUT_UNSUPPORTED, "ModifiedNewton on bands beyond shared memory is not implemented"));
-            const size_t fsm = large_factor_smem(bw);
-            if (fsm > 220 * 1024 || bw > kLargeMaxBw)
+            const size_t fsm = bw > kLargeMaxBw ? large_factor_smem(kPanelWide, kLargeThreadsWide)
+                                                : large_factor_smem(kPanel, kLargeThreads);
+            if (fsm > 220 * 1024 || bw > kLargeMaxBwWide)
                 return bail(fail(STRUT_UNSUPPORTED, "band width too large for the blocked factorisation"));
             if (large_solve_smem(nf) > 220 * 1024)
                 return bail(fail(STRUT_UNSUPPORTED, "system too large for the band substitution"));
@@ -1493,17 +1501,19 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         if ((rc = upload(&h->d_large_list, h->large_list_h, al)) || (rc = upload(&h->d_large_rowbase, rowbase, al)) ||
             (rc = dzeros(&A.lband, (size_t)h->lband_total, al)) || (rc = upload(&A.lstatus, lstat, al)) ||
             (rc = dzeros(&h->d_gb, 1, al)) || (rc = dzeros(&h->d_wbuf, nF, al)) ||
-            (rc = dzeros(&h->d_lpan, (size_t)kPanel * kLargeThreads, al)) ||
-            (rc = dzeros(&h->d_lpiv, (size_t)kLargeThreads, al)))
+            (rc = dzeros(&h->d_lpan, (size_t)std::max(kPanel * kLargeThreads, kPanelWide * kLargeThreadsWide), al)) ||
+            (rc = dzeros(&h->d_lpiv, (size_t)std::max(kLargeThreads, kLargeThreadsWide), al)))
             return bail(rc);
         {
             const int polls = kBarrierPolls;
             CK(cudaMemcpy((char*)h->d_gb + offsetof(GridBarrier, limit), &polls, sizeof(int), cudaMemcpyHostToDevice));
         }
-        CK(cudaFuncSetAttribute(large_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)h->lfactor_smem));
+        h->lfactor_wide = h->max_large_bw > kLargeMaxBw ? 1 : 0;
+        const void* fk = h->lfactor_wide ? (const void*)large_factor_kernel<kPanelWide, kLargeThreadsWide>
+                                         : (const void*)large_factor_kernel<kPanel, kLargeThreads>;
+        CK(cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->lfactor_smem));
         int per_sm = 0, n_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, large_factor_kernel, kLargeThreads,
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk, h->lfactor_wide ? kLargeThreadsWide : kLargeThreads,
                                                          h->lfactor_smem));
         CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->device));
         if (per_sm < 1) return bail(fail(STRUT_UNSUPPORTED, "band factorisation kernel does not fit on an SM"));
