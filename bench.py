@@ -72,6 +72,11 @@ def parse():
     ap.add_argument("--learned3d-steps", type=int, default=4000,
                     help="record steps of the 3D learned-predictor arm (config 3)")
     ap.add_argument("--no-learned3d", action="store_true", help="skip the 3D learned-predictor arm")
+    ap.add_argument("--no-slab", action="store_true", help="skip the batched slab-frame window (config 4)")
+    ap.add_argument("--slab-frames", type=int, default=8)
+    ap.add_argument("--slab-steps", type=int, default=10)
+    ap.add_argument("--slab-train-frames", type=int, default=8)
+    ap.add_argument("--slab-train-steps", type=int, default=40)
     ap.add_argument("--no-tall", action="store_true",
                     help="skip the large single-instance 3D frame (20 stories, 6x6 bays)")
     ap.add_argument("--tall-steps", type=int, default=4000,
@@ -413,6 +418,59 @@ def learned3d_arm(args, device, runtime, torch):
             "max_disp_diff_of_peak_vs_plain": worst, "train": info}
 
 
+def slab_arm(args, device, runtime, torch):
+    """Config 4 on a window: a batch of `args.slab_frames` frames of the batched slab-frame set
+    (stories U{10..30}, bays U{4..6} of 7 m, 2 x 2 ShellMITC4 slabs per bay, rigid diaphragms,
+    two horizontal Kanai-Tajimi records at PGA U(0.3, 0.6) g, dt 0.005 s) in one handle, uneven
+    sizes together; the device time of `args.slab_steps` steps after 3 warm-up steps, plain and
+    with the learned predictor, whose network is retrained on the plain histories of other frames
+    of the set (seeds 9000+) over the first `args.slab_train_steps` steps.  The whole set (256
+    frames x 4000 steps) is out of reach of one timed run; records/hour is the batch at this
+    window's rate over a 4000-step record."""
+    from strut_b200 import model as Mo, workloads as W
+
+    steps = 3 + args.slab_steps
+
+    def build(n, seed0, st):
+        return [Mo.Model(W.slab_frame3d_case(p["stories"], p["bays"], steps=st, seed=p["seed"], pga_g=p["pga_g"],
+                                             wg=p["wg"]))
+                for p in W.slab_frame_params(n, base_seed=seed0)]
+
+    train = build(args.slab_train_frames, 9000, args.slab_train_steps)
+    pred, info = train_predictor(train, args.slab_train_steps, device, runtime, 1, args.train_epochs)
+    models = build(args.slab_frames, 8000, steps)
+    out = {"workload": "slab_3d_rc_frames_10to30s_4to6b_bidirectional", "frames": len(models),
+           "fibers": int(sum(m.num_fibers_total for m in models)), "free_dofs": int(sum(m.num_free for m in models)),
+           "steps_timed": args.slab_steps, "warmup_steps": 3, "record_steps": 4000, "dt": 0.005, "train": info}
+    for arm, p in (("plain", None), ("learned", pred)):
+        an = runtime.Analysis(models, device=device)
+        if p is not None:
+            p.attach(an)
+        an.run(3, check=False)
+        stream = torch.cuda.ExternalStream(runtime.lib().strut_gpu_stream(an.h))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = an.run(args.slab_steps, check=False)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        ok = int((an.instance_status() == 0).sum())
+        from strut_b200 import predictor as PR
+
+        offered, chosen = PR.stats(an) if p is not None else (0, 0)
+        an.close()
+        ms_step = ms / args.slab_steps
+        out[arm] = {"ms_per_step": ms_step, "records_per_hour": ok * 3600.0 / (ms_step * 4000 / 1000.0),
+                    "records_running": ok,
+                    "newton_its_per_step": st.global_newton_iterations / float(len(models) * args.slab_steps)}
+        if p is not None:
+            out[arm]["learned_guess_kept_frac"] = chosen / max(offered, 1)
+    out["vs_plain"] = (out["learned"]["records_per_hour"] / out["plain"]["records_per_hour"]
+                       if out["plain"]["records_per_hour"] else None)
+    return out
+
+
 def run_reference(args):
     """The reference algorithm's CPU implementation (the oracle) on all host threads over the
     whole batch: every record, all of its steps, one record per thread at a time as Strut runs
@@ -647,6 +705,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_learned3d:
         learned3d = learned3d_arm(args, device, runtime, torch)
 
+    slab = None
+    if rank == 0 and world == 1 and not args.no_slab:
+        slab = slab_arm(args, device, runtime, torch)
+
     tall = None
     if rank == 0 and world == 1 and not args.no_tall:
         tall = tall_arm(args, device, runtime, A, torch)
@@ -704,6 +766,8 @@ def main():
             line["learned"] = learned
         if learned3d:
             line["learned_3d"] = learned3d
+        if slab:
+            line["slab_frames_window"] = slab
         if cpu:
             line["cpu_baseline"] = cpu
         if tall:
