@@ -16,27 +16,41 @@ from strut_b200 import _abi as A
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
+LIB_PATH_FMA = HERE / "liboracle_fma.so"  # the same oracle with contracted multiply-adds
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
-def build(force: bool = False) -> Path:
+def build(force: bool = False, fma: bool = False) -> Path:
+    path = LIB_PATH_FMA if fma else LIB_PATH
     srcs = list(HERE.glob("*.c")) + list(HERE.glob("*.h")) + [HERE.parent / "include" / "strut_cuda.h"]
-    if force or not LIB_PATH.exists() or any(p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in srcs):
-        subprocess.check_call(["make", "-s", "-C", str(HERE), "liboracle.so"])
-    return LIB_PATH
+    if force or not path.exists() or any(p.stat().st_mtime > path.stat().st_mtime for p in srcs):
+        subprocess.check_call(["make", "-s", "-C", str(HERE), path.name])
+    return path
 
 
 _lib = None
+_fma = False
+
+
+def use_fma(on: bool):
+    """Selects the oracle build for the following calls: separately rounded multiplies and adds
+    (the default) or contracted multiply-adds.  Together with the SIMD width this gives the
+    reference's algorithm under several roundings."""
+    global _lib, _fma
+    if bool(on) != _fma:
+        _fma = bool(on)
+        _lib = None
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
-            build()
-        L = C.CDLL(str(LIB_PATH))
+        path = LIB_PATH_FMA if _fma else LIB_PATH
+        if not path.exists():
+            build(fma=_fma)
+        L = C.CDLL(str(path))
         L.oracle_set_simd_width.argtypes = [C.c_int]
         L.oracle_subdivisions.restype = C.c_long
         L.oracle_dense_fallbacks.restype = C.c_long

@@ -12,11 +12,12 @@
 // N = n_alloc * n_fam, n_alloc a multiple of the tile, so the fibers of a tile of consecutive
 // instances are one contiguous 16-byte aligned run per field.
 //
-// Persistent CTAs, one per SM, walk the instance tiles with a two-stage pipeline: while the
-// threads update tile k in shared memory, the TMA unit (cp.async.bulk, mbarrier completion, no
-// multicast) brings tile k + 1 in; each thread writes its fibers' new state straight back to HBM
-// (a warp's stores are consecutive, so they coalesce), so a stage is free again as soon as it has
-// been read.  Inside a tile every thread takes fibers of the flattened (family, instance, fiber)
+// Persistent CTAs (one of 512 threads or two of 256 per SM) walk the instance tiles with a
+// two-stage pipeline: while the threads update tile k in shared memory, the TMA unit
+// (cp.async.bulk, mbarrier completion, no multicast) brings tile k + 1 in; each thread writes its
+// fibers' new state straight back to HBM (a warp's stores are consecutive, so they coalesce), so a
+// stage is free again as soon as it has been read.  With two CTAs per SM one CTA's section sums
+// and barriers overlap the other's fiber updates.  Inside a tile every thread takes fibers of the flattened (family, instance, fiber)
 // order, so a warp's shared-memory accesses are consecutive; the per-fiber stress and tangent (times area) go
 // to shared memory and each instance's sums are formed in the element kernel's fixed order (eight
 // chunks of the section's fibers, each summed sequentially, then a pairwise tree), so results do
@@ -28,7 +29,9 @@
 
 namespace strut {
 
-constexpr int kFsThreads = 512;
+constexpr int kFsThreads = 512;      // one CTA per SM
+constexpr int kFsThreadsPair = 256;  // two CTAs per SM
+constexpr int kFsTileQuantum = 48;   // instances are allocated in multiples of every tile size (4..16)
 
 // Per-tile geometry of the stage buffers, identical for every tile.
 struct FsLayout {
@@ -37,7 +40,16 @@ struct FsLayout {
     int off_c2, off_s2, off_s1, off_c1, off_kon;  // offsets in a stage, in doubles
     int stage_doubles;           // one stage, kon included, rounded to 16 bytes
     uint32_t bytes_c2, bytes_s2, bytes_s1, bytes_c1, bytes_kon;  // per field per tile
+    float inv_s2, inv_c2, inv_s1, inv_c1, inv_el;  // 1 / family length (0 for an empty family)
 };
+
+// q = r / n for 0 <= r < 2^22 and n >= 1, from a float estimate corrected to the exact quotient.
+__device__ __forceinline__ int fs_div(int r, int n, float inv) {
+    int q = __float2int_rz(__int2float_rz(r) * inv);
+    if (q * n > r) --q;
+    else if ((q + 1) * n <= r) ++q;
+    return q;
+}
 
 __host__ __device__ inline FsLayout fs_layout(const DevSection& sd, int T) {
     FsLayout L;
@@ -60,6 +72,11 @@ __host__ __device__ inline FsLayout fs_layout(const DevSection& sd, int T) {
     L.bytes_s1 = 8u * T * sd.n_s1;
     L.bytes_c1 = 8u * T * sd.n_c1;
     L.bytes_kon = 4u * T * sd.n_s2;
+    L.inv_s2 = sd.n_s2 ? 1.0f / sd.n_s2 : 0.0f;
+    L.inv_c2 = sd.n_c2 ? 1.0f / sd.n_c2 : 0.0f;
+    L.inv_s1 = sd.n_s1 ? 1.0f / sd.n_s1 : 0.0f;
+    L.inv_c1 = sd.n_c1 ? 1.0f / sd.n_c1 : 0.0f;
+    L.inv_el = sd.n_el ? 1.0f / sd.n_el : 0.0f;
     return L;
 }
 
@@ -87,21 +104,24 @@ __device__ __forceinline__ void fs_load_tile(const FsLayout& L, const BatchState
         bulk_g2s(st + L.off_c1 + f * T * L.n_c1, bs.c1 + f * N4 + tile * T * L.n_c1, L.bytes_c1, bar);
 }
 
-// n_inst instances (state allocated for n_tiles * T); ek: n_inst x 2 (eps0, kappa); resp:
-// n_inst x 5 (N, Mz, k11, k12, k22).  *err is set when a bulk copy does not complete within the
-// bounded wait.
-__global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSection sd, BatchState bs, FsLayout L,
+// n_inst instances (state allocated for bs.n_inst >= n_tiles * T); ek: n_inst x 2 (eps0,
+// kappa); resp: n_inst x 5 (N, Mz, k11, k12, k22).  *err is set when a bulk copy does not complete
+// within the bounded wait.  THREADS x MINB = 512 threads per SM: both shapes have the same
+// register budget (128 per thread).
+template <int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) fiber_stream_kernel(Geo g, DevSection sd, BatchState bs, FsLayout L,
                                                                   long long n_inst, long long n_tiles,
                                                                   const double* __restrict__ ek,
                                                                   double* __restrict__ resp, int commit,
                                                                   int* __restrict__ err) {
     extern __shared__ __align__(128) double fs_smem[];
     __shared__ __align__(8) uint64_t bar[2];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x;
+    constexpr int nt = THREADS;
     const int T = L.T;
     double* fk = fs_smem + 2 * L.stage_doubles;  // T x n_tot x {sig A, tan A}
     double* strain = fk + 2 * T * L.n_tot;       // T x {eps0, kappa}
-    const long long n_alloc = n_tiles * T;
+    const long long n_alloc = bs.n_inst;  // allocated instances: the field stride
     const long long N2 = n_alloc * L.n_s2, N3 = n_alloc * L.n_c2, N1 = n_alloc * L.n_s1, N4 = n_alloc * L.n_c1;
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -148,7 +168,7 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
         for (int it = tid; it < n_items; it += nt) {
             int r = it;
             if (r < n_s2t) {
-                const int si = r / L.n_s2, j = r - si * L.n_s2;
+                const int si = fs_div(r, L.n_s2, L.inv_s2), j = r - si * L.n_s2;
                 if (si < nvalid) {
                     const double* F = st + L.off_s2 + r;
                     const int* K = reinterpret_cast<const int*>(st + L.off_kon) + r;
@@ -173,7 +193,7 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
             }
             r -= n_s2t;
             if (r < n_c2t) {
-                const int si = r / L.n_c2, j = r - si * L.n_c2;
+                const int si = fs_div(r, L.n_c2, L.inv_c2), j = r - si * L.n_c2;
                 if (si < nvalid) {
                     const double* F = st + L.off_c2 + r;
                     const int gi = geo_c2 + j;
@@ -193,7 +213,7 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
             }
             r -= n_c2t;
             if (r < n_s1t) {
-                const int si = r / L.n_s1, j = r - si * L.n_s1;
+                const int si = fs_div(r, L.n_s1, L.inv_s1), j = r - si * L.n_s1;
                 if (si < nvalid) {
                     const double* F = st + L.off_s1 + r;
                     const int gi = geo_s1 + j;
@@ -213,7 +233,7 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
             }
             r -= n_s1t;
             if (r < n_c1t) {
-                const int si = r / L.n_c1, j = r - si * L.n_c1;
+                const int si = fs_div(r, L.n_c1, L.inv_c1), j = r - si * L.n_c1;
                 if (si < nvalid) {
                     const double* F = st + L.off_c1 + r;
                     const int gi = geo_c1 + j;
@@ -235,7 +255,8 @@ __global__ void __launch_bounds__(kFsThreads) fiber_stream_kernel(Geo g, DevSect
             }
             r -= n_c1t;
             {
-                const int si = r / L.n_el, j = r - si * L.n_el;
+                const int si = fs_div(r, L.n_el, L.inv_el), j = r - si * L.n_el;
+                if (si >= nvalid) continue;
                 const int gi = geo_el + j;
                 const double y = __ldg(g.y + gi), A = __ldg(g.a + gi);
                 const double ks = g.mats[__ldg(g.m + gi)].p[0] * A;

@@ -158,7 +158,7 @@ extern "C" {
 
 int strut_gpu_mlp_create(int32_t n_in, int32_t n_out, StrutMlp** out) {
     if (!out || n_in < 1 || n_in > strut::kMlpKin || n_out < 1 || n_out > strut::kMlpNout)
-        return fail(STRUT_BAD_ARG, "the predictor network takes 1..32 features and 1..16 outputs");
+        return fail(STRUT_BAD_ARG, "the predictor network takes 1..48 features and 1..16 outputs");
     *out = nullptr;
     StrutMlp* m = new StrutMlp();
     m->n_in = n_in;

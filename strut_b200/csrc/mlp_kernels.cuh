@@ -27,7 +27,7 @@
 namespace strut {
 
 constexpr int kMlpH = 128;     // hidden width
-constexpr int kMlpKin = 32;    // input features, padded (a multiple of 16)
+constexpr int kMlpKin = 48;    // input features, padded (a multiple of 16; 41 for a 3D node)
 constexpr int kMlpNout = 16;   // outputs, padded (N of the last MMA)
 constexpr int kMlpTile = 128;  // rows (nodes) per CTA = MMA M
 
@@ -174,8 +174,8 @@ struct MlpDev {
     const float* b3;           // kMlpNout
 };
 
-constexpr uint32_t kMlpBytesX = kMlpTile * kMlpKin * 2;   // 8 KiB
-constexpr uint32_t kMlpBytesW1 = kMlpH * kMlpKin * 2;     // 8 KiB
+constexpr uint32_t kMlpBytesX = kMlpTile * kMlpKin * 2;   // 12 KiB
+constexpr uint32_t kMlpBytesW1 = kMlpH * kMlpKin * 2;     // 12 KiB
 constexpr uint32_t kMlpBytesH = kMlpTile * kMlpH * 2;     // 32 KiB
 constexpr uint32_t kMlpBytesW2 = kMlpH * kMlpH * 2;       // 32 KiB
 constexpr uint32_t kMlpBytesW3 = kMlpNout * kMlpH * 2;    // 4 KiB
@@ -293,7 +293,7 @@ struct MlpTrainDev {
     const __nv_bfloat16* w3;   // chunk-major, kMlpH rows (inputs) x kMlpNout (outputs): dH2 = dY W3^T
 };
 
-constexpr uint32_t kMlpBytesXT = kMlpKin * kMlpTile * 2;   // X^T: kMlpKin rows x kMlpTile   8 KiB
+constexpr uint32_t kMlpBytesXT = kMlpKin * kMlpTile * 2;   // X^T: kMlpKin rows x kMlpTile   12 KiB
 constexpr uint32_t kMlpBytesDY = kMlpTile * kMlpNout * 2;  // dY: 128 rows x 16                4 KiB
 // region offsets (bytes) of the training kernel's shared memory
 constexpr uint32_t kTrX = 0;
@@ -309,7 +309,8 @@ constexpr uint32_t kTrR2 = kTrR1 + kMlpBytesH;             // W2t (layer-2 B), t
 constexpr uint32_t kTrR3 = kTrR2 + kMlpBytesH;             // H1 (layer-2 A), then dZ2^T (dW2's B)
 constexpr uint32_t kTrR4 = kTrR3 + kMlpBytesH;             // H2 (layer-3 A), then dZ1^T (dW1t's A)
 constexpr uint32_t kTrRed = kTrR4 + kMlpBytesH;            // 4 warps x 128 floats (column sums)
-constexpr uint32_t kMlpTrainSmem = kTrRed + 4 * kMlpH * 4 + 1024;
+constexpr uint32_t kMlpTrainSmem = kTrRed + 4 * kMlpH * 4 + 1024;  // 215 KiB
+static_assert(kMlpTrainSmem <= 227 * 1024, "training tile exceeds the opt-in shared memory");
 
 // Writes element (r, k) = v as bf16 into a chunk-major operand of R rows.
 __device__ __forceinline__ void store_bf16(char* base, int r, int k, int R, float v) {
@@ -536,7 +537,7 @@ __global__ void __launch_bounds__(128) mlp_train_tile_kernel(MlpTrainDev w, cons
     }
     mma_begin();
     if (ok) gb1[tid] = ((red[tid] + red[kMlpH + tid]) + red[2 * kMlpH + tid]) + red[3 * kMlpH + tid];
-    // ---- layer 1 backward: dW1t = dZ1^T X (rows: outputs, cols 128..159: inputs)
+    // ---- layer 1 backward: dW1t = dZ1^T X (rows: outputs, cols 128..175: inputs)
     if (tid == 0 && ok) {
         tc_fence_after();
         umma_gemm(tb + 128, R4, XT, kMlpTile, kMlpKin, false);

@@ -2010,6 +2010,7 @@ struct StrutSectionBatch {
     FsLayout L{};
     long long n_tiles = 0;
     int grid = 1;
+    int ctas_per_sm = 1;  // 1: 512-thread CTAs, 2: pairs of 256-thread CTAs
     size_t smem = 0;
     int* d_err = nullptr;
     ~StrutSectionBatch() {
@@ -2077,6 +2078,43 @@ static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>
     }
 }
 
+// Shape of the streaming kernel: ctas_per_sm CTAs of 512 / ctas_per_sm threads per SM, each with
+// the largest tile (a multiple of 4, at most 16 instances) whose two stages and per-fiber results
+// fit its share of the SM's shared memory, checked against the occupancy calculator.
+static int fs_configure(StrutSectionBatch* b, int ctas_per_sm) {
+    if (ctas_per_sm != 1 && ctas_per_sm != 2) return fail(STRUT_BAD_ARG, "ctas_per_sm must be 1 or 2");
+    int dev = 0, optin = 0, n_sm = 1, per_sm = 0, reserved = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    CK(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    const long long share = (long long)per_sm / ctas_per_sm - reserved - 256;  // 256: static shared memory
+    const size_t cap = (size_t)std::max(0LL, std::min<long long>(share, (long long)optin - 256));
+    int T = 0;
+    for (int t = 16; t >= 4; t -= 4)
+        if (fs_smem_bytes(fs_layout(b->sd, t)) <= cap) {
+            T = t;
+            break;
+        }
+    if (T == 0) return fail(STRUT_UNSUPPORTED, "the section's tiles do not fit this shape's shared memory");
+    const FsLayout L = fs_layout(b->sd, T);
+    const size_t smem = fs_smem_bytes(L);
+    const int threads = ctas_per_sm == 1 ? kFsThreads : kFsThreadsPair;
+    const void* fn = ctas_per_sm == 1 ? (const void*)fiber_stream_kernel<kFsThreads, 1>
+                                      : (const void*)fiber_stream_kernel<kFsThreadsPair, 2>;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int resident = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fn, threads, smem));
+    if (resident < ctas_per_sm) return fail(STRUT_UNSUPPORTED, "this shape's CTAs are not co-resident");
+    b->L = L;
+    b->ctas_per_sm = ctas_per_sm;
+    b->smem = smem;
+    b->n_tiles = (b->n_inst + T - 1) / T;
+    b->grid = (int)std::min<long long>(b->n_tiles, (long long)n_sm * ctas_per_sm);
+    return STRUT_OK;
+}
+
 extern "C" {
 
 int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t num_materials,
@@ -2107,33 +2145,11 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
     b->geo.m = d_m;
     b->geo.mats = d_mats;
     b->geo.secs = d_secs;
-    // tile of the streaming kernel: the most instances (a multiple of 4, at most 16) whose two
-    // stages and per-fiber results fit the shared memory a CTA can opt into
-    {
-        int dev = 0, optin = 0, n_sm = 1;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-        const size_t cap = (size_t)optin > 2048 ? (size_t)optin - 2048 : 0;  // room for static shared memory
-        int T = 0;
-        for (int t = 16; t >= 4; t -= 4)
-            if (fs_smem_bytes(fs_layout(b->sd, t)) <= cap) {
-                T = t;
-                break;
-            }
-        if (T > 0) {
-            b->L = fs_layout(b->sd, T);
-            b->n_tiles = (n_inst + T - 1) / T;
-            b->n_alloc = b->n_tiles * T;
-            b->smem = fs_smem_bytes(b->L);
-            b->grid = (int)std::min<long long>(b->n_tiles, n_sm);
-            CK(cudaFuncSetAttribute(fiber_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
-        } else {
-            b->n_alloc = n_inst;
-        }
-    }
     std::vector<double> s2, c2, s1, c1;
     std::vector<int> kon;
+    // state for a whole number of tiles of every tile size, so the shape can change later
+    b->n_alloc = (n_inst + kFsTileQuantum - 1) / kFsTileQuantum * kFsTileQuantum;
+    if (fs_configure(b, 1) != STRUT_OK) b->L.T = 0;  // the one-warp-per-instance kernel
     batch_initial_state(sp, mats, b->n_alloc, s2, c2, s1, c1, kon);
     if ((rc = upload(&b->bs.s2, s2, al)) || (rc = upload(&b->bs.c2, c2, al)) || (rc = upload(&b->bs.s1, s1, al)) ||
         (rc = upload(&b->bs.c1, c1, al)) || (rc = upload(&b->bs.kon, kon, al))) {
@@ -2156,13 +2172,25 @@ int strut_gpu_section_batch_destroy(StrutSectionBatch* b) {
     return STRUT_OK;
 }
 
+int strut_gpu_section_batch_set_shape(StrutSectionBatch* b, int32_t ctas_per_sm) {
+    if (!b) return fail(STRUT_BAD_ARG, "bad arguments");
+    if (b->L.T == 0) return fail(STRUT_UNSUPPORTED, "the section is evaluated one warp per instance");
+    CK(cudaDeviceSynchronize());
+    return fs_configure(b, ctas_per_sm);  // leaves the shape unchanged when it fails
+}
+
 int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_dev, double* resp_dev,
                                  int32_t commit, void* stream) {
     if (!b || !eps0_kappa_dev || !resp_dev) return fail(STRUT_BAD_ARG, "bad arguments");
     if (b->L.T > 0) {
-        fiber_stream_kernel<<<b->grid, kFsThreads, b->smem, (cudaStream_t)stream>>>(
-            b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, b->n_tiles, eps0_kappa_dev, resp_dev, commit ? 1 : 0,
-            b->d_err);
+        if (b->ctas_per_sm == 2)
+            fiber_stream_kernel<kFsThreadsPair, 2><<<b->grid, kFsThreadsPair, b->smem, (cudaStream_t)stream>>>(
+                b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, b->n_tiles, eps0_kappa_dev, resp_dev,
+                commit ? 1 : 0, b->d_err);
+        else
+            fiber_stream_kernel<kFsThreads, 1><<<b->grid, kFsThreads, b->smem, (cudaStream_t)stream>>>(
+                b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, b->n_tiles, eps0_kappa_dev, resp_dev,
+                commit ? 1 : 0, b->d_err);
     } else {
         // a section too large for the streaming kernel's tiles: one warp per instance
         const long long threads = (long long)b->n_inst * 32;

@@ -1,17 +1,18 @@
 """The whole 256-frame batch on the GPU against the CPU oracle, record by record.
 
 tests/golden/batch256_outcomes.json (tests/golden/make_batch_golden.py) holds the oracle's
-outcome of every record at two summation orders of the reference's algorithm (SIMD widths 8 and
-1).  The two orders agree on 255 of the 256 records: the same 28 records stop non-converged at
-the same steps with the same Newton iteration counts, the rest complete.  Record 234 is the
-exception: its forceBeamColumn elements fail their local iteration for much of the record; it
-completes at width 8 and stops at step 1225 at width 1, so rounding alone decides its outcome.
+outcome of every record under four roundings of the reference's algorithm: SIMD widths 8 and 1,
+each with separately rounded and with contracted multiply-adds.  Long strongly nonlinear records
+bifurcate at rounding level: a few stop non-converged at different steps, or not at all, depending
+only on the rounding (record 234 completes at width 8 and stops at step 1225 at width 1; record
+98 stops at step 780 in all separately rounded orders and at steps 376, 788 or 858 with contracted
+multiply-adds).
 
-The GPU (a third summation order, with fused multiply-adds) must give, on every record where the
-two orders agree, the same status and the same failing step; and its per-record Newton
-iteration totals may differ from width 8's on no more records than twice the number on which
-width 1 differs from width 8 (long strongly nonlinear records drift apart at rounding level;
-the test bounds how far)."""
+The GPU (another rounding: warp-tree sums and fused multiply-adds) must give, on every record where
+all the oracle's roundings agree, the same status and the same failing step; and its per-record
+Newton iteration totals may differ from width 8's on no more records than twice the number on
+which the oracle's other roundings differ from width 8 (the test bounds how far the GPU drifts
+relative to the oracle's own spread)."""
 import json
 from pathlib import Path
 
@@ -47,15 +48,17 @@ def test_batch256_outcomes_match_the_oracle(gpu_lib):
     models = [M.Model(c) for c in W.batched_frames(fx["frames"], steps=steps, dt=fx["dt"],
                                                     base_seed=fx["base_seed"])]
     status, failed, its = gpu_outcomes(gpu_lib, models, steps)
-    w8, w1 = fx["orders"]["simd8"], fx["orders"]["simd1"]
-    s8, s1 = np.array(w8["status"]), np.array(w1["status"])
-    f8, f1 = np.array(w8["failed_step"]), np.array(w1["failed_step"])
-    i8, i1 = np.array(w8["newton_iterations"]), np.array(w1["newton_iterations"])
-    agree = (s8 == s1) & (f8 == f1)
-    assert agree.sum() >= 250
-    bad = [int(i) for i in np.nonzero(agree)[0] if status[i] != s8[i] or failed[i] != f8[i]]
+    orders = fx["orders"]
+    st = {k: np.array(v["status"]) for k, v in orders.items()}
+    fs = {k: np.array(v["failed_step"]) for k, v in orders.items()}
+    it = {k: np.array(v["newton_iterations"]) for k, v in orders.items()}
+    agree = np.ones(len(models), dtype=bool)
+    for k in orders:
+        agree &= (st[k] == st["simd8"]) & (fs[k] == fs["simd8"])
+    assert agree.sum() >= 240
+    bad = [int(i) for i in np.nonzero(agree)[0] if status[i] != st["simd8"][i] or failed[i] != fs["simd8"][i]]
     assert not bad, f"records whose outcome differs from the oracle's: {bad}"
-    both_done = agree & (s8 == 0)
-    own = int(np.sum((i1 != i8) & both_done))
-    ours = int(np.sum((its != i8) & both_done))
-    assert ours <= 2 * own, f"{ours} records with other iteration totals (oracle orders: {own})"
+    all_done = agree & (st["simd8"] == 0)
+    own = max(int(np.sum((it[k] != it["simd8"]) & all_done)) for k in orders if k != "simd8")
+    ours = int(np.sum((its != it["simd8"]) & all_done))
+    assert ours <= 2 * own, f"{ours} records with other iteration totals (oracle roundings: {own})"

@@ -6,14 +6,17 @@ fan_out the twelve attempts of an element whose last state determination needed 
 run on twelve CTAs and the first success in Strut's order is kept.  Frames 0, 21 and 37 of the
 256-frame batch subdivide in their first 400 steps (the oracle counts 116, 153 and 121
 cut-back passes there), so their histories exercise the fan-out; they must be bit for bit those
-of the sequential order, with either element CTA size, and within 1e-7 of peak of the
-oracle's."""
+of the sequential order, with either element CTA size, and within 1e-7 of peak of the oracle's
+under one of its roundings: frame 0 bifurcates at rounding level near step 300 (the oracle with
+separately rounded and with contracted multiply-adds differ there by 1.3 % of peak, while its
+SIMD widths 8 and 1 agree to 3e-9), and the GPU, which contracts, follows the contracted
+oracle."""
 import numpy as np
 import pytest
 
 from strut_b200 import model as M
 from strut_b200 import workloads as W
-from tests.test_gpu_records import compare_histories, record_everything
+from tests.test_gpu_records import nearest_order, record_everything
 
 pytestmark = pytest.mark.gpu
 
@@ -53,8 +56,6 @@ def test_fan_out_is_the_sequential_order_bit_for_bit(gpu_lib, oracle):
             assert np.array_equal(d0, d1)
             assert np.array_equal(e0, e1)
     for m, (gd, ge, gi) in zip(models, fan):
-        rd, re, ri, rc, failed = oracle.run_transient(m, STEPS)
-        assert rc == 0
-        worst_d, worst_e, n_diff = compare_histories(gd, ge, gi, rd, re, ri)
-        assert worst_d <= 1e-7 and worst_e <= 1e-7
+        worst_d, worst_e, n_diff, order = nearest_order(oracle, m, STEPS, gd, ge, gi, widths=(8,))[0]
+        assert worst_d <= 1e-7 and worst_e <= 1e-7, (worst_d, worst_e, order)
         assert n_diff <= 0.01 * STEPS

@@ -80,19 +80,34 @@ def test_section_batch_matches_oracle(gpu_lib, oracle):
     ek[:, :, 0] = np.cumsum(rng.normal(0, 2e-4, (npts, n_inst)), axis=0)
     ek[:, :, 1] = np.cumsum(rng.normal(0, 2e-3, (npts, n_inst)), axis=0)
     ref = oracle.section_batch_path(mats, nm, fibs, nf, ek)
-    b = gpu_lib.SectionBatch(mats, nm, fibs, nf, n_inst)
     d_ek = torch.empty((n_inst, 2), dtype=torch.float64, device="cuda")
     d_r = torch.empty((n_inst, 5), dtype=torch.float64, device="cuda")
-    got = np.zeros_like(ref)
-    for p in range(npts):
-        d_ek.copy_(torch.from_numpy(ek[p]))
-        torch.cuda.synchronize()
-        b.eval(d_ek.data_ptr(), d_r.data_ptr(), commit=True)
-        torch.cuda.synchronize()
-        got[p] = d_r.cpu().numpy()
-    b.close()
+
+    def run(shapes):
+        """shapes[p]: the streaming kernel's CTAs per SM at point p (the history carries over)."""
+        b = gpu_lib.SectionBatch(mats, nm, fibs, nf, n_inst)
+        got = np.zeros_like(ref)
+        for p in range(npts):
+            if p == 0 or shapes[p] != shapes[p - 1]:
+                b.set_shape(shapes[p])
+            d_ek.copy_(torch.from_numpy(ek[p]))
+            torch.cuda.synchronize()
+            b.eval(d_ek.data_ptr(), d_r.data_ptr(), commit=True)
+            torch.cuda.synchronize()
+            got[p] = d_r.cpu().numpy()
+        state = b.fiber_state(n_inst - 1)
+        b.close()
+        return got, state
+
+    got, state = run([1] * npts)
     scale = np.abs(ref).max(axis=(0, 1))
     assert np.all(np.abs(got - ref) <= 1e-9 * scale + 1e-12)
+    # the launch shape (512-thread CTAs with larger tiles, pairs of 256-thread CTAs with
+    # smaller tiles, or a switch in mid-history) changes nothing, bit for bit
+    for shapes in ([2] * npts, [1] * (npts // 2) + [2] * (npts - npts // 2)):
+        got2, state2 = run(shapes)
+        assert np.array_equal(got2, got)
+        assert np.array_equal(state2, state)
 
 
 def _random_u(m, seed, scale=0.02):

@@ -52,6 +52,27 @@ def compare_histories(gd, ge, gi, rd, re, ri):
     return worst(gd, rd), worst(ge, re), int(np.sum(gi != ri))
 
 
+def nearest_order(oracle, model, steps, gd, ge, gi, widths=(8, 1)):
+    """The GPU history's errors against the oracle under several roundings of the reference's
+    algorithm (SIMD widths, separately rounded or contracted multiply-adds), nearest first:
+    [(worst_d, worst_e, n_iter_diff, (width, fma))].  A record that bifurcates at rounding level
+    (two roundings of the oracle already differ by more than the tolerance) is held to the
+    rounding it follows."""
+    out = []
+    try:
+        for fma in (False, True):
+            oracle.use_fma(fma)
+            for w in widths:
+                oracle.set_simd_width(w)
+                rd, re, ri, rc, _failed = oracle.run_transient(model, steps)
+                out.append((*compare_histories(gd, ge, gi, rd, re, ri), (w, fma)) if rc == 0
+                           else (float("inf"), float("inf"), steps, (w, fma)))
+    finally:
+        oracle.use_fma(False)
+        oracle.set_simd_width(8)
+    return sorted(out, key=lambda r: max(r[0], r[1]))
+
+
 def test_config0_full_record(gpu_lib, oracle):
     steps = 2000
     m = M.Model(record_everything(W.rc_frame_case(steps=steps)))

@@ -52,7 +52,7 @@ def test_oracle_gradients_match_finite_differences():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n_in,n_out,n", [(29, 3, 300), (32, 16, 128), (5, 1, 1000)])
+@pytest.mark.parametrize("n_in,n_out,n", [(29, 3, 300), (41, 6, 300), (48, 16, 128), (5, 1, 1000)])
 def test_forward_matches_oracle(gpu_lib, n_in, n_out, n):
     rng = np.random.default_rng(n)
     p = random_params(n_in, n_out, seed=n_in)
@@ -72,7 +72,7 @@ def test_forward_matches_oracle(gpu_lib, n_in, n_out, n):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n_in,n_out,n", [(29, 3, 500), (32, 16, 256)])
+@pytest.mark.parametrize("n_in,n_out,n", [(29, 3, 500), (41, 6, 300), (48, 16, 256)])
 def test_gradients_match_oracle(gpu_lib, n_in, n_out, n):
     """The tensor-core backward pass against the oracle's (same bf16 operand roundings): the
     loss and every parameter gradient."""
