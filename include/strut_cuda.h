@@ -330,7 +330,8 @@ void* strut_gpu_stream(const StrutHandle* h);
  *   factor_ctas  CTAs of the cooperative wide-band factorisation (1 .. its resident limit;
  *                0: the default, as many as one panel has trailing tiles).
  *   element_threads  threads of an element CTA: 640 (default, one CTA per SM: the shortest
- *                per-element iteration) or 320 (two CTAs per SM: twice the elements in flight).
+ *                per-element iteration), 320, 224 or 160 (2D only): as many CTAs per SM as
+ *                registers and shared memory allow, more elements in flight.
  * strut_gpu_set_tuning with t = NULL restores the defaults. */
 typedef struct StrutTuning {
     int32_t fan_out;

@@ -7,7 +7,7 @@ class, whatever runs fastest:
   fan_out          forceBeamColumn2d attempts of an element that needed a subdivision: twelve CTAs
                    at once (1) or one after another (0)
   element_threads  640 threads per element CTA (one CTA per SM, the shortest per-element
-                   iteration) or 320 (two CTAs per SM, twice the elements in flight)
+                   iteration), 320, 224 or 160 (2D): more CTAs per SM, more elements in flight
   commit_team      64 or 128 threads per integration point in the commit kernel
   factor_ctas      CTAs of the cooperative wide-band factorisation (wide bands only)
 
@@ -55,7 +55,7 @@ def candidates(models, wide_band: bool, max_nip: int, n_sm: int = 148):
     """Values each knob may take for this batch."""
     has_fbc2d = any(int(e.type) == A.ELEM_FORCE_BEAM_COLUMN_2D for m in models for e in m.elements)
     c = {"fan_out": [1, 0] if has_fbc2d else [1],
-         "element_threads": [640, 320],
+         "element_threads": [640, 320, 224] + ([160] if models[0].ndf == 3 else []),
          "commit_team": [0] + ([64, 128] if max_nip <= 5 else [64]),
          "factor_ctas": [0, n_sm // 4, n_sm // 2, n_sm] if wide_band else [0]}
     return c

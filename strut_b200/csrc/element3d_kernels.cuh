@@ -628,7 +628,8 @@ __device__ void element3d_process(const Geo& g, const DevSection& sd, const DevE
         }
         return;
     }
-    derive_element(g, sd, E, sv, const_cast<double*>(sv.c2d), const_cast<double*>(sv.s2d));
+    derive_element(g, sd, E, sv, fs.c2 + 4 * fs.c2_n + E.c2_off, const_cast<double*>(sv.c2d),
+                   const_cast<double*>(sv.s2d));
     const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     double* ys = const_cast<double*>(sv.s2d) + 12 * E.s2_blk;
     double* zs = ys + ((n_tot + 1) & ~1);

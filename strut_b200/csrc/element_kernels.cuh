@@ -90,7 +90,7 @@ struct ElemScratch {
     double pt_e[kMaxIp], pt_k[kMaxIp];    // points to evaluate
     double resp[kMaxIp][5];
     double raw[kMaxIp][6];                // section sums of the last evaluation
-    double scr[32][12];                   // per-point terms of the element algebra (warp 0)
+    double scr[kMaxIp][12];               // per-point terms of the element algebra (lanes < nip of warp 0)
     double sub_e[kMaxIp], sub_k[kMaxIp], ssr_n[kMaxIp], ssr_m[kMaxIp];
     double fs00[kMaxIp], fs01[kMaxIp], fs11[kMaxIp];
     double best[10];
@@ -111,7 +111,8 @@ struct ElemScratch {
 // Family views of the element's committed history (shared memory, or global memory with the
 // family length as field stride).
 struct StageView {
-    const double* c2;   // 5 fields x c2_blk
+    const double* c2;   // staged: 4 fields x c2_blk (eps sig tan ecmin; dept only enters the
+                        // derived constants, which read it from global memory)
     const double* s2;   // 10 fields x s2_blk
     const int* kon;     // s2_blk
     const double* s1;   // 5 fields x s1_blk
@@ -131,13 +132,15 @@ __device__ __forceinline__ void load_c1(const StageView& sv, int idx, C1State& c
     c.slope = sv.c1[5 * B + idx];
 }
 
+// The staged Concrete02 fields; dept is not staged (set to 0 here: the stress and tangent given
+// the derived constants do not use it).
 __device__ __forceinline__ void load_c2(const StageView& sv, int idx, C2State& c) {
     const int B = sv.c2_blk;
     c.eps = sv.c2[0 * B + idx];
     c.sig = sv.c2[1 * B + idx];
     c.tan = sv.c2[2 * B + idx];
     c.ecmin = sv.c2[3 * B + idx];
-    c.dept = sv.c2[4 * B + idx];
+    c.dept = 0.0;
 }
 
 __device__ __forceinline__ void load_s2(const StageView& sv, int idx, S2State& c) {
@@ -156,13 +159,16 @@ __device__ __forceinline__ void load_s2(const StageView& sv, int idx, S2State& c
 }
 
 // Derived constants of every Concrete02 / Steel02 fiber of the staged element, computed once
-// per launch by the whole CTA (the committed state does not change inside a launch).
+// per launch by the whole CTA (the committed state does not change inside a launch).  A
+// Concrete02 fiber's dept comes from global memory (c2_dept: the element's dept field).
 __device__ __forceinline__ void derive_element(const Geo& g, const DevSection& sd, const DevElem& E,
-                                               const StageView& sv, double* c2d, double* s2d) {
+                                               const StageView& sv, const double* __restrict__ c2_dept,
+                                               double* c2d, double* s2d) {
     const int nc = E.nip * sd.n_c2, ns = E.nip * sd.n_s2;
     for (int idx = threadIdx.x; idx < nc; idx += blockDim.x) {
         C2State c;
         load_c2(sv, idx, c);
+        c.dept = __ldg(c2_dept + idx);
         const int j = idx % sd.n_c2;
         C2Derived d;
         concrete02_derive(g.mats[__ldg(g.m + sd.geo_off + sd.n_s2 + j)], c, d);
@@ -1003,7 +1009,7 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
                                               double* sm, uint64_t* bar, uint32_t& phase,
                                               StageView& sv, int* err) {
     double* c2 = sm;
-    double* s2 = c2 + 5 * E.c2_blk;
+    double* s2 = c2 + 4 * E.c2_blk;
     double* s1 = s2 + 10 * E.s2_blk;
     double* c1 = s1 + 5 * E.s1_blk;
     int* kon = reinterpret_cast<int*>(c1 + 6 * E.c1_blk);
@@ -1019,14 +1025,14 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
     sv.s2_blk = E.s2_blk;
     sv.s1_blk = E.s1_blk;
     sv.c1_blk = E.c1_blk;
-    const uint32_t bytes = (uint32_t)(8 * (5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
+    const uint32_t bytes = (uint32_t)(8 * (4 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
                                       4 * E.s2_blk);
     if (bytes == 0) return true;
     if (threadIdx.x == 0) {
         // the previous element's reads of this buffer (generic proxy) come before the copies
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive_expect_tx(bar, bytes);
-        for (int f = 0; f < 5 && E.c2_blk; ++f)
+        for (int f = 0; f < 4 && E.c2_blk; ++f)
             bulk_g2s(c2 + f * E.c2_blk, fs.c2 + f * fs.c2_n + E.c2_off, 8u * E.c2_blk, bar);
         for (int f = 0; f < 10 && E.s2_blk; ++f)
             bulk_g2s(s2 + f * E.s2_blk, fs.s2 + f * fs.s2_n + E.s2_off, 8u * E.s2_blk, bar);
@@ -1079,6 +1085,18 @@ struct RecPass {
 // Newton iteration of a few slow records launches no idle CTAs and a slow element does not hold
 // up elements queued behind it on the same CTA.
 //
+// Element-level scratch of the element kernel: the 3D scratch exists only in the 3D instance (a
+// smaller static footprint lets more 2D element CTAs share an SM).
+template <int DIM>
+union ElemScratchOf {
+    ElemScratch s2;
+    ElemScratch3 s3;
+};
+template <>
+union ElemScratchOf<2> {
+    ElemScratch s2;
+};
+
 // DIM 2 instantiates the 2D elements' code only, DIM 3 the 3D elements' (a batch holds one kind).
 template <int DIM>
 __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
@@ -1090,10 +1108,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     extern __shared__ __align__(128) double smem_fib[];
     __shared__ DevElem E;
     __shared__ DevSection sd;
-    __shared__ union ScratchU {
-        ElemScratch s2;
-        ElemScratch3 s3;
-    } SU;
+    __shared__ ElemScratchOf<DIM> SU;
     ElemScratch& S = SU.s2;
     const int all_elems = mode != ELEM_MODE_LIST;
     __shared__ __align__(8) uint64_t bar;
@@ -1171,7 +1186,8 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         stop = true;
         return;
     }
-    derive_element(g, sd, E, sv, const_cast<double*>(sv.c2d), const_cast<double*>(sv.s2d));
+    derive_element(g, sd, E, sv, fs.c2 + 4 * fs.c2_n + E.c2_off, const_cast<double*>(sv.c2d),
+                   const_cast<double*>(sv.s2d));
     // the section's fiber y (phase-2 sums) and the per-fiber results of phase 1 follow
     const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
     double* ys = const_cast<double*>(sv.s2d) + 12 * E.s2_blk;

@@ -409,8 +409,15 @@ static int prof_end(StrutHandle* h, int k) {
 // threads per integration point up to 5 points, else 64.
 using CommitKernel = decltype(&commit_kernel<128>);
 using ElemKernel = decltype(&element_state_kernel<2>);
+// Element CTA sizes: 640 (one CTA per SM), 320, 224 and 160 threads (more CTAs per SM where
+// shared memory allows: more elements in flight, each with fewer threads).  The 3D kernel's
+// epilogue needs 172 threads, so 160 is 2D only.
+static bool elem_threads_ok(const StrutHandle* h, int t) {
+    return t == kTeamThreads || t == kTeamThreads / 2 || t == 224 || (t == 160 && h->ndf_all != 6);
+}
 static int elem_threads_of(const StrutHandle* h) {
-    return h->tune.element_threads == kTeamThreads / 2 ? kTeamThreads / 2 : kTeamThreads;
+    return h->tune.element_threads != 0 && elem_threads_ok(h, h->tune.element_threads) ? h->tune.element_threads
+                                                                                        : kTeamThreads;
 }
 static ElemKernel elem_kernel_of(const StrutHandle* h) {
     return h->ndf_all == 6 ? element_state_kernel<3> : element_state_kernel<2>;
@@ -988,10 +995,11 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
             E.c1_blk = round4(E.nip * sd.n_c1);
             c1_total += E.c1_blk;
             h->max_nip = std::max(h->max_nip, E.nip);
-            // staged history + derived constants (Concrete02 5, Steel02 12 doubles per fiber) +
-            // the section's fiber y + per-fiber stress and tangent of every point
+            // staged history (Concrete02 without dept) + derived constants (Concrete02 5, Steel02
+            // 12 doubles per fiber) + the section's fiber y + per-fiber stress and tangent of
+            // every point
             const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
-            const size_t smem = 8 * (size_t)(5 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
+            const size_t smem = 8 * (size_t)(4 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
                                 4 * (size_t)E.s2_blk +
                                 8 * (size_t)(5 * E.c2_blk + 12 * E.s2_blk) +
                                 8 * (size_t)((three_d ? 2 : 1) * ((n_tot + 1) & ~1) + 2 * E.nip * n_tot);
@@ -1863,7 +1871,7 @@ int strut_gpu_set_tuning(StrutHandle* h, const StrutTuning* t) {
     if (t) {
         if ((t->fan_out != 0 && t->fan_out != 1) || (t->commit_team != 0 && t->commit_team != 64 && t->commit_team != 128) ||
             (t->commit_team == 128 && h->max_nip > 5) || t->factor_ctas < 0 ||
-            (t->element_threads != 0 && t->element_threads != kTeamThreads && t->element_threads != kTeamThreads / 2))
+            (t->element_threads != 0 && !elem_threads_ok(h, t->element_threads)))
             return fail(STRUT_BAD_ARG, "tuning value out of range");
         d = *t;
     }
