@@ -244,7 +244,7 @@ def tall_arm(args, device, runtime, A, torch):
     return out
 
 
-def fiber_arm(n_fibers, runtime, torch, peak, steps=20, warmup=3, shape=None):
+def fiber_arm(n_fibers, runtime, torch, peak, steps=20, warmup=3):
     """The streaming fiber-state update kernel alone: one RC column section (140 Concrete02
     and 8 Steel02 fibers) in as many instances as the batch has fibers, each with its own
     committed history; every call reads and rewrites every fiber's history once (80 B per
@@ -261,8 +261,6 @@ def fiber_arm(n_fibers, runtime, torch, peak, steps=20, warmup=3, shape=None):
     mats, nm, fibs, nf = Mo.section_fibers(case["section"], case["materials"])
     n = (n_fibers + nf - 1) // nf
     b = runtime.SectionBatch(mats, nm, fibs, nf, n)
-    if shape is not None:
-        b.set_shape(shape)
     tot = steps + warmup
     gen = torch.Generator(device="cuda")
     gen.manual_seed(0)

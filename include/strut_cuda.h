@@ -392,10 +392,6 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
                                    const StrutFiber* fibers, int32_t num_fibers,
                                    int32_t n_inst, StrutSectionBatch** out);
 int strut_gpu_section_batch_destroy(StrutSectionBatch* b);
-/* Launch shape of the streaming kernel: ctas_per_sm = 1 (one 512-thread CTA per SM, the
- * default) or 2 (two 256-thread CTAs per SM with smaller tiles).  Results do not depend on it.
- * STRUT_UNSUPPORTED (shape unchanged) when the section's tiles do not fit that shape. */
-int strut_gpu_section_batch_set_shape(StrutSectionBatch* b, int32_t ctas_per_sm);
 /* eps0_kappa_dev / resp_dev are DEVICE pointers (n_inst x 2 and n_inst x 5). */
 int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_dev,
                                  double* resp_dev, int32_t commit, void* stream);

@@ -286,7 +286,6 @@ EXPORTS = {
          C.POINTER(C.c_void_p)],
     ),
     "strut_gpu_section_batch_destroy": (C.c_int, [C.c_void_p]),
-    "strut_gpu_section_batch_set_shape": (C.c_int, [C.c_void_p, C.c_int32]),
     "strut_gpu_section_eval_batch": (
         C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
     ),

@@ -89,25 +89,29 @@ struct BatchState {
     int* kon;
     double* s1;
     double* c1;
-    long long n_inst;  // instances with allocated state: the field stride is n_inst x family size
+    long long n_inst;  // instances with allocated state: a field's stride is n_inst x P
+    int p_s2, p_c2, p_s1, p_c1;  // P: each instance's run per family, the family's length padded
+                                 // to a multiple of 4
 };
 
-__global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd, BatchState bs,
+// One warp per instance (n_live instances), for sections whose stages do not fit the streaming
+// kernel's shared memory.
+__global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd, BatchState bs, long long n_live,
                                                             const double* __restrict__ ek,
                                                             double* __restrict__ resp,
                                                             int commit) {
-    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long warp_global = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (warp_global >= bs.n_inst) return;
+    if (warp_global >= n_live) return;
     const long long i = warp_global;
     const double eps0 = ek[2 * i], kappa = ek[2 * i + 1];
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a3el = 0.0;
     int base = sd.geo_off;
     {
-        const long long N = bs.n_inst * sd.n_s2;
+        const long long N = bs.n_inst * bs.p_s2;
         for (int j = lane; j < sd.n_s2; j += 32) {
-            double* F = bs.s2 + i * sd.n_s2 + j;
-            int* K = bs.kon + i * sd.n_s2 + j;
+            double* F = bs.s2 + i * bs.p_s2 + j;
+            int* K = bs.kon + i * bs.p_s2 + j;
             S2State c, t;
             c.eps = F[0 * N]; c.sig = F[1 * N]; c.tan = F[2 * N]; c.epsmin = F[3 * N];
             c.epsmax = F[4 * N]; c.epspl = F[5 * N]; c.epss0 = F[6 * N]; c.sigs0 = F[7 * N];
@@ -125,9 +129,9 @@ __global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd
     }
     base += sd.n_s2;
     {
-        const long long N = bs.n_inst * sd.n_c2;
+        const long long N = bs.n_inst * bs.p_c2;
         for (int j = lane; j < sd.n_c2; j += 32) {
-            double* F = bs.c2 + i * sd.n_c2 + j;
+            double* F = bs.c2 + i * bs.p_c2 + j;
             C2State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.ecmin = F[3 * N]; c.dept = F[4 * N];
             const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
@@ -142,9 +146,9 @@ __global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd
     }
     base += sd.n_c2;
     {
-        const long long N = bs.n_inst * sd.n_s1;
+        const long long N = bs.n_inst * bs.p_s1;
         for (int j = lane; j < sd.n_s1; j += 32) {
-            double* F = bs.s1 + i * sd.n_s1 + j;
+            double* F = bs.s1 + i * bs.p_s1 + j;
             S1State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.epsp = F[3 * N]; c.alpha = F[4 * N];
             const double y = __ldg(g.y + base + j), A = __ldg(g.a + base + j);
@@ -159,9 +163,9 @@ __global__ void __launch_bounds__(256) section_batch_kernel(Geo g, DevSection sd
     }
     base += sd.n_s1;
     {
-        const long long N = bs.n_inst * sd.n_c1;
+        const long long N = bs.n_inst * bs.p_c1;
         for (int j = lane; j < sd.n_c1; j += 32) {
-            double* F = bs.c1 + i * sd.n_c1 + j;
+            double* F = bs.c1 + i * bs.p_c1 + j;
             C1State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.emin = F[3 * N]; c.eend = F[4 * N];
             c.slope = F[5 * N];
@@ -220,7 +224,7 @@ __global__ void section3d_path_kernel(Geo g, DevSection sd, BatchState bs,
         };
         int base = sd.geo_off;
         for (int j = lane; j < sd.n_s2; j += 32) {
-            const long long N = sd.n_s2;
+            const long long N = bs.p_s2;
             double* F = bs.s2 + j;
             S2State c, t;
             c.eps = F[0 * N]; c.sig = F[1 * N]; c.tan = F[2 * N]; c.epsmin = F[3 * N];
@@ -235,7 +239,7 @@ __global__ void section3d_path_kernel(Geo g, DevSection sd, BatchState bs,
         }
         base += sd.n_s2;
         for (int j = lane; j < sd.n_c2; j += 32) {
-            const long long N = sd.n_c2;
+            const long long N = bs.p_c2;
             double* F = bs.c2 + j;
             C2State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.ecmin = F[3 * N]; c.dept = F[4 * N];
@@ -246,7 +250,7 @@ __global__ void section3d_path_kernel(Geo g, DevSection sd, BatchState bs,
         }
         base += sd.n_c2;
         for (int j = lane; j < sd.n_s1; j += 32) {
-            const long long N = sd.n_s1;
+            const long long N = bs.p_s1;
             double* F = bs.s1 + j;
             S1State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.epsp = F[3 * N]; c.alpha = F[4 * N];
@@ -257,7 +261,7 @@ __global__ void section3d_path_kernel(Geo g, DevSection sd, BatchState bs,
         }
         base += sd.n_s1;
         for (int j = lane; j < sd.n_c1; j += 32) {
-            const long long N = sd.n_c1;
+            const long long N = bs.p_c1;
             double* F = bs.c1 + j;
             C1State c, t;
             c.eps = F[0]; c.sig = F[N]; c.tan = F[2 * N]; c.emin = F[3 * N]; c.eend = F[4 * N];

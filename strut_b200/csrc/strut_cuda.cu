@@ -2009,16 +2009,14 @@ int strut_gpu_revert(StrutHandle* h) {
 // ---------------------------------------------------------------------------------------
 struct StrutSectionBatch {
     int n_inst = 0;
-    long long n_alloc = 0;  // instances with allocated state (a whole number of tiles)
     std::vector<void*> allocs;
     Geo geo;
     DevSection sd;
-    BatchState bs;
-    // streaming kernel: instances per tile (L.T 0: the section does not fit, one warp per instance)
+    BatchState bs;  // bs.n_inst == n_inst (the field stride), family runs padded to 4
+    // streaming kernel: stage geometry, persistent grid (0: the stages do not fit, one warp per
+    // instance instead)
     FsLayout L{};
-    long long n_tiles = 0;
-    int grid = 1;
-    int ctas_per_sm = 1;  // 1: 512-thread CTAs, 2: pairs of 256-thread CTAs
+    int grid = 0;
     size_t smem = 0;
     int* d_err = nullptr;
     ~StrutSectionBatch() {
@@ -2054,8 +2052,8 @@ static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>
                                 std::vector<double>& s2, std::vector<double>& c2, std::vector<double>& s1,
                                 std::vector<double>& c1, std::vector<int>& kon) {
     const DevSection& sd = sp.secs[0];
-    const long long n2 = n_inst * sd.n_s2, n3 = n_inst * sd.n_c2, n1 = n_inst * sd.n_s1,
-                    n4 = n_inst * sd.n_c1;
+    const int P2 = fs_pad4(sd.n_s2), P3 = fs_pad4(sd.n_c2), P1 = fs_pad4(sd.n_s1), P4 = fs_pad4(sd.n_c1);
+    const long long n2 = n_inst * P2, n3 = n_inst * P3, n1 = n_inst * P1, n4 = n_inst * P4;
     s2.assign(10 * std::max<long long>(n2, 1), 0.0);
     c2.assign(5 * std::max<long long>(n3, 1), 0.0);
     s1.assign(5 * std::max<long long>(n1, 1), 0.0);
@@ -2065,7 +2063,7 @@ static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>
         int base = sd.geo_off;
         for (int j = 0; j < sd.n_s2; ++j) {
             const DevMat& m = mats[sp.m[base + j]];
-            const long long idx = i * sd.n_s2 + j;
+            const long long idx = i * P2 + j;
             s2[2 * n2 + idx] = m.p[1];
             s2[4 * n2 + idx] = m.k[S2K_EPSY];
             s2[3 * n2 + idx] = -m.k[S2K_EPSY];
@@ -2075,51 +2073,33 @@ static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>
             }
         }
         base += sd.n_s2;
-        for (int j = 0; j < sd.n_c2; ++j) c2[2 * n3 + i * sd.n_c2 + j] = mats[sp.m[base + j]].k[C2K_EC0];
+        for (int j = 0; j < sd.n_c2; ++j) c2[2 * n3 + i * P3 + j] = mats[sp.m[base + j]].k[C2K_EC0];
         base += sd.n_c2;
-        for (int j = 0; j < sd.n_s1; ++j) s1[2 * n1 + i * sd.n_s1 + j] = mats[sp.m[base + j]].p[1];
+        for (int j = 0; j < sd.n_s1; ++j) s1[2 * n1 + i * P1 + j] = mats[sp.m[base + j]].p[1];
         base += sd.n_s1;
         for (int j = 0; j < sd.n_c1; ++j) {
-            c1[2 * n4 + i * sd.n_c1 + j] = mats[sp.m[base + j]].k[C1K_EC0];
-            c1[5 * n4 + i * sd.n_c1 + j] = mats[sp.m[base + j]].k[C1K_EC0];
+            c1[2 * n4 + i * P4 + j] = mats[sp.m[base + j]].k[C1K_EC0];
+            c1[5 * n4 + i * P4 + j] = mats[sp.m[base + j]].k[C1K_EC0];
         }
     }
 }
 
-// Shape of the streaming kernel: ctas_per_sm CTAs of 512 / ctas_per_sm threads per SM, each with
-// the largest tile (a multiple of 4, at most 16 instances) whose two stages and per-fiber results
-// fit its share of the SM's shared memory, checked against the occupancy calculator.
-static int fs_configure(StrutSectionBatch* b, int ctas_per_sm) {
-    if (ctas_per_sm != 1 && ctas_per_sm != 2) return fail(STRUT_BAD_ARG, "ctas_per_sm must be 1 or 2");
-    int dev = 0, optin = 0, n_sm = 1, per_sm = 0, reserved = 0;
+// Persistent grid of the streaming kernel: as many one-warp CTAs per SM as the occupancy
+// calculator allows with this section's two stages; 0 when they do not fit at all.
+static int fs_configure(StrutSectionBatch* b) {
+    int dev = 0, optin = 0, n_sm = 1;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-    CK(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-    const long long share = (long long)per_sm / ctas_per_sm - reserved - 256;  // 256: static shared memory
-    const size_t cap = (size_t)std::max(0LL, std::min<long long>(share, (long long)optin - 256));
-    int T = 0;
-    for (int t = 16; t >= 4; t -= 4)
-        if (fs_smem_bytes(fs_layout(b->sd, t)) <= cap) {
-            T = t;
-            break;
-        }
-    if (T == 0) return fail(STRUT_UNSUPPORTED, "the section's tiles do not fit this shape's shared memory");
-    const FsLayout L = fs_layout(b->sd, T);
-    const size_t smem = fs_smem_bytes(L);
-    const int threads = ctas_per_sm == 1 ? kFsThreads : kFsThreadsPair;
-    const void* fn = ctas_per_sm == 1 ? (const void*)fiber_stream_kernel<kFsThreads, 1>
-                                      : (const void*)fiber_stream_kernel<kFsThreadsPair, 2>;
-    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    b->L = fs_layout(b->sd);
+    b->smem = fs_smem_bytes(b->L);
+    b->grid = 0;
+    if (b->smem + 256 > (size_t)optin) return STRUT_OK;
+    CK(cudaFuncSetAttribute(fiber_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
     int resident = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fn, threads, smem));
-    if (resident < ctas_per_sm) return fail(STRUT_UNSUPPORTED, "this shape's CTAs are not co-resident");
-    b->L = L;
-    b->ctas_per_sm = ctas_per_sm;
-    b->smem = smem;
-    b->n_tiles = (b->n_inst + T - 1) / T;
-    b->grid = (int)std::min<long long>(b->n_tiles, (long long)n_sm * ctas_per_sm);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fiber_stream_kernel, 32, b->smem));
+    if (resident < 1) return STRUT_OK;
+    b->grid = (int)std::min<long long>((long long)b->n_inst, (long long)n_sm * resident);
     return STRUT_OK;
 }
 
@@ -2155,16 +2135,21 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
     b->geo.secs = d_secs;
     std::vector<double> s2, c2, s1, c1;
     std::vector<int> kon;
-    // state for a whole number of tiles of every tile size, so the shape can change later
-    b->n_alloc = (n_inst + kFsTileQuantum - 1) / kFsTileQuantum * kFsTileQuantum;
-    if (fs_configure(b, 1) != STRUT_OK) b->L.T = 0;  // the one-warp-per-instance kernel
-    batch_initial_state(sp, mats, b->n_alloc, s2, c2, s1, c1, kon);
+    if ((rc = fs_configure(b)) != STRUT_OK) {
+        delete b;
+        return rc;
+    }
+    batch_initial_state(sp, mats, n_inst, s2, c2, s1, c1, kon);
     if ((rc = upload(&b->bs.s2, s2, al)) || (rc = upload(&b->bs.c2, c2, al)) || (rc = upload(&b->bs.s1, s1, al)) ||
         (rc = upload(&b->bs.c1, c1, al)) || (rc = upload(&b->bs.kon, kon, al))) {
         delete b;
         return rc;
     }
-    b->bs.n_inst = b->n_alloc;
+    b->bs.n_inst = n_inst;
+    b->bs.p_s2 = b->L.p_s2;
+    b->bs.p_c2 = b->L.p_c2;
+    b->bs.p_s1 = b->L.p_s1;
+    b->bs.p_c1 = b->L.p_c1;
     if ((rc = dzeros(&b->d_err, 1, al))) {
         delete b;
         return rc;
@@ -2180,31 +2165,18 @@ int strut_gpu_section_batch_destroy(StrutSectionBatch* b) {
     return STRUT_OK;
 }
 
-int strut_gpu_section_batch_set_shape(StrutSectionBatch* b, int32_t ctas_per_sm) {
-    if (!b) return fail(STRUT_BAD_ARG, "bad arguments");
-    if (b->L.T == 0) return fail(STRUT_UNSUPPORTED, "the section is evaluated one warp per instance");
-    CK(cudaDeviceSynchronize());
-    return fs_configure(b, ctas_per_sm);  // leaves the shape unchanged when it fails
-}
-
 int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_dev, double* resp_dev,
                                  int32_t commit, void* stream) {
     if (!b || !eps0_kappa_dev || !resp_dev) return fail(STRUT_BAD_ARG, "bad arguments");
-    if (b->L.T > 0) {
-        if (b->ctas_per_sm == 2)
-            fiber_stream_kernel<kFsThreadsPair, 2><<<b->grid, kFsThreadsPair, b->smem, (cudaStream_t)stream>>>(
-                b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, b->n_tiles, eps0_kappa_dev, resp_dev,
-                commit ? 1 : 0, b->d_err);
-        else
-            fiber_stream_kernel<kFsThreads, 1><<<b->grid, kFsThreads, b->smem, (cudaStream_t)stream>>>(
-                b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, b->n_tiles, eps0_kappa_dev, resp_dev,
-                commit ? 1 : 0, b->d_err);
+    if (b->grid > 0) {
+        fiber_stream_kernel<<<b->grid, 32, b->smem, (cudaStream_t)stream>>>(
+            b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, eps0_kappa_dev, resp_dev, commit ? 1 : 0, b->d_err);
     } else {
-        // a section too large for the streaming kernel's tiles: one warp per instance
+        // a section whose stages do not fit in shared memory: one warp per instance
         const long long threads = (long long)b->n_inst * 32;
         const int tb = 256;
         section_batch_kernel<<<(unsigned)((threads + tb - 1) / tb), tb, 0, (cudaStream_t)stream>>>(
-            b->geo, b->sd, b->bs, eps0_kappa_dev, resp_dev, commit ? 1 : 0);
+            b->geo, b->sd, b->bs, (long long)b->n_inst, eps0_kappa_dev, resp_dev, commit ? 1 : 0);
     }
     CK(cudaGetLastError());
     return STRUT_OK;
@@ -2224,28 +2196,28 @@ int strut_gpu_section_batch_state(StrutSectionBatch* b, int32_t instance, double
     }
     // 16 doubles per fiber: the family's committed fields in declaration order, kon in slot 15
     std::vector<double> o((size_t)nf * 16, 0.0);
-    const long long n2 = b->n_alloc * sd.n_s2, n3 = b->n_alloc * sd.n_c2,
-                    n1 = b->n_alloc * sd.n_s1, n4 = b->n_alloc * sd.n_c1;
+    const int P2 = b->bs.p_s2, P3 = b->bs.p_c2, P1 = b->bs.p_s1, P4 = b->bs.p_c1;
+    const long long n2 = b->bs.n_inst * P2, n3 = b->bs.n_inst * P3, n1 = b->bs.n_inst * P1, n4 = b->bs.n_inst * P4;
     for (int j = 0; j < sd.n_s2; ++j) {
         for (int f = 0; f < 10; ++f)
-            CK(cudaMemcpy(&o[(size_t)j * 16 + f], b->bs.s2 + f * n2 + (long long)instance * sd.n_s2 + j, sizeof(double),
+            CK(cudaMemcpy(&o[(size_t)j * 16 + f], b->bs.s2 + f * n2 + (long long)instance * P2 + j, sizeof(double),
                           cudaMemcpyDeviceToHost));
         int kon = 0;
-        CK(cudaMemcpy(&kon, b->bs.kon + (long long)instance * sd.n_s2 + j, sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&kon, b->bs.kon + (long long)instance * P2 + j, sizeof(int), cudaMemcpyDeviceToHost));
         o[(size_t)j * 16 + 15] = kon;
     }
     for (int j = 0; j < sd.n_c2; ++j)
         for (int f = 0; f < 5; ++f)
-            CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + j) * 16 + f], b->bs.c2 + f * n3 + (long long)instance * sd.n_c2 + j,
+            CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + j) * 16 + f], b->bs.c2 + f * n3 + (long long)instance * P3 + j,
                           sizeof(double), cudaMemcpyDeviceToHost));
     for (int j = 0; j < sd.n_s1; ++j)
         for (int f = 0; f < 5; ++f)
             CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + sd.n_c2 + j) * 16 + f],
-                          b->bs.s1 + f * n1 + (long long)instance * sd.n_s1 + j, sizeof(double), cudaMemcpyDeviceToHost));
+                          b->bs.s1 + f * n1 + (long long)instance * P1 + j, sizeof(double), cudaMemcpyDeviceToHost));
     for (int j = 0; j < sd.n_c1; ++j)
         for (int f = 0; f < 6; ++f)
             CK(cudaMemcpy(&o[(size_t)(sd.n_s2 + sd.n_c2 + sd.n_s1 + j) * 16 + f],
-                          b->bs.c1 + f * n4 + (long long)instance * sd.n_c1 + j, sizeof(double), cudaMemcpyDeviceToHost));
+                          b->bs.c1 + f * n4 + (long long)instance * P4 + j, sizeof(double), cudaMemcpyDeviceToHost));
     std::memcpy(out, o.data(), o.size() * sizeof(double));
     return STRUT_OK;
 }
@@ -2306,6 +2278,10 @@ int strut_gpu_section3d_path(const StrutUniMaterial* materials, int32_t num_mate
         return rc;
     }
     bs.n_inst = 1;
+    bs.p_s2 = fs_pad4(sp.secs[0].n_s2);
+    bs.p_c2 = fs_pad4(sp.secs[0].n_c2);
+    bs.p_s1 = fs_pad4(sp.secs[0].n_s1);
+    bs.p_c1 = fs_pad4(sp.secs[0].n_c1);
     Geo g;
     std::memset(&g, 0, sizeof(g));
     g.y = d_y;

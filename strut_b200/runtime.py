@@ -218,11 +218,6 @@ class SectionBatch:
         self.b = b
         self.n_inst = n_inst
 
-    def set_shape(self, ctas_per_sm: int):
-        """Streaming kernel launch shape: 1 (512-thread CTAs) or 2 (pairs of 256-thread CTAs)."""
-        _check(lib().strut_gpu_section_batch_set_shape(self.b, int(ctas_per_sm)),
-               "strut_gpu_section_batch_set_shape")
-
     def eval(self, eps0_kappa_dev_ptr: int, resp_dev_ptr: int, commit: bool = True, stream: int = 0):
         _check(lib().strut_gpu_section_eval_batch(self.b, C.c_void_p(eps0_kappa_dev_ptr),
                                                   C.c_void_p(resp_dev_ptr), 1 if commit else 0,
