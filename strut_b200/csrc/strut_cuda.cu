@@ -2012,10 +2012,11 @@ struct StrutSectionBatch {
     std::vector<void*> allocs;
     Geo geo;
     DevSection sd;
-    BatchState bs;  // bs.n_inst == n_inst (the field stride), family runs padded to 4
-    // streaming kernel: stage geometry, persistent grid (0: the stages do not fit, one warp per
-    // instance instead)
+    BatchState bs;  // bs.n_inst: allocated instances (a whole number of tiles), the field stride
+    // streaming kernel: stage geometry, tiles, persistent grid (0: the stages do not fit, one warp
+    // per instance instead)
     FsLayout L{};
+    long long n_tiles = 0;
     int grid = 0;
     size_t smem = 0;
     int* d_err = nullptr;
@@ -2084,8 +2085,8 @@ static void batch_initial_state(const SectionPack& sp, const std::vector<DevMat>
     }
 }
 
-// Persistent grid of the streaming kernel: as many one-warp CTAs per SM as the occupancy
-// calculator allows with this section's two stages; 0 when they do not fit at all.
+// Persistent grid of the streaming kernel: as many CTAs per SM as the occupancy calculator
+// allows with this section's two stages; 0 when they do not fit at all.
 static int fs_configure(StrutSectionBatch* b) {
     int dev = 0, optin = 0, n_sm = 1;
     CK(cudaGetDevice(&dev));
@@ -2093,13 +2094,14 @@ static int fs_configure(StrutSectionBatch* b) {
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     b->L = fs_layout(b->sd);
     b->smem = fs_smem_bytes(b->L);
+    b->n_tiles = (b->n_inst + kFsTile - 1) / kFsTile;
     b->grid = 0;
-    if (b->smem + 256 > (size_t)optin) return STRUT_OK;
+    if (b->smem + 1024 > (size_t)optin) return STRUT_OK;
     CK(cudaFuncSetAttribute(fiber_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
     int resident = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fiber_stream_kernel, 32, b->smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fiber_stream_kernel, fs_threads(b->L), b->smem));
     if (resident < 1) return STRUT_OK;
-    b->grid = (int)std::min<long long>((long long)b->n_inst, (long long)n_sm * resident);
+    b->grid = (int)std::min<long long>(b->n_tiles, (long long)n_sm * resident);
     return STRUT_OK;
 }
 
@@ -2139,13 +2141,14 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
         delete b;
         return rc;
     }
-    batch_initial_state(sp, mats, n_inst, s2, c2, s1, c1, kon);
+    const long long n_alloc = b->n_tiles * kFsTile;  // whole tiles: a tile's copies stay in bounds
+    batch_initial_state(sp, mats, n_alloc, s2, c2, s1, c1, kon);
     if ((rc = upload(&b->bs.s2, s2, al)) || (rc = upload(&b->bs.c2, c2, al)) || (rc = upload(&b->bs.s1, s1, al)) ||
         (rc = upload(&b->bs.c1, c1, al)) || (rc = upload(&b->bs.kon, kon, al))) {
         delete b;
         return rc;
     }
-    b->bs.n_inst = n_inst;
+    b->bs.n_inst = n_alloc;
     b->bs.p_s2 = b->L.p_s2;
     b->bs.p_c2 = b->L.p_c2;
     b->bs.p_s1 = b->L.p_s1;
@@ -2169,8 +2172,9 @@ int strut_gpu_section_eval_batch(StrutSectionBatch* b, const double* eps0_kappa_
                                  int32_t commit, void* stream) {
     if (!b || !eps0_kappa_dev || !resp_dev) return fail(STRUT_BAD_ARG, "bad arguments");
     if (b->grid > 0) {
-        fiber_stream_kernel<<<b->grid, 32, b->smem, (cudaStream_t)stream>>>(
-            b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, eps0_kappa_dev, resp_dev, commit ? 1 : 0, b->d_err);
+        fiber_stream_kernel<<<b->grid, fs_threads(b->L), b->smem, (cudaStream_t)stream>>>(
+            b->geo, b->sd, b->bs, b->L, (long long)b->n_inst, b->n_tiles, eps0_kappa_dev, resp_dev, commit ? 1 : 0,
+            b->d_err);
     } else {
         // a section whose stages do not fit in shared memory: one warp per instance
         const long long threads = (long long)b->n_inst * 32;
