@@ -13,19 +13,20 @@
 // instances, a multiple of the tile), so every field of a tile of kFsTile consecutive instances
 // is one contiguous, 16-byte aligned run: one bulk copy per field and tile.
 //
-// Warp-specialised CTAs, several per SM: kFsTile instance warps, each owning one instance of the
-// tile (its Concrete02, Steel01, Concrete01 and elastic fibers, then its sums), and W_s steel
-// warps that take the Steel02 fibers of all the tile's instances together, so the expensive
-// Menegotto-Pinto branch runs on full warps instead of a few lanes of every instance warp.  Two
-// stages: the TMA unit (cp.async.bulk, mbarrier completion, no multicast) brings tile k + 2 into a
-// stage as soon as every warp has read tile k from it.  The warps hand work to one another through
-// mbarriers only (stage full / stage read / steel results written / sums done), never a CTA-wide
-// barrier, so a warp that finishes its part of a tile goes on to the next one.  Each lane writes
-// its fibers' new state straight back to HBM (consecutive lanes, consecutive fibers), and the
-// per-fiber stress and tangent (times area) go to shared memory, from which eight lanes of the
-// instance warp form the sums in the element kernel's fixed order (eight chunks of the section's
+// Warp-specialised CTAs, several per SM: kFsTile instance warps share the tile's Concrete02,
+// Steel01, Concrete01 and elastic fibers (flattened over the tile's instances, so the warps' last
+// round is nearly full), and W_s steel warps take the Steel02 fibers of all the tile's instances
+// together, so the expensive Menegotto-Pinto branch runs on full warps instead of a few lanes of
+// every warp.  Two stages: the TMA unit (cp.async.bulk, mbarrier completion, no multicast) brings
+// tile k + 2 into a stage as soon as every warp has read tile k from it.  The steel warps hand
+// their results over through mbarriers (stage full / stage read / steel results written / sums
+// done); the instance warps meet at one named barrier per tile (not the steel warps), after which
+// one of them forms the four instances' sums with all 32 lanes while the others go on to the next
+// tile.  Each lane writes its fibers' new state straight back to HBM (consecutive lanes,
+// consecutive fibers), and the per-fiber stress and tangent (times area) go to shared memory, from
+// which the sums are formed in the element kernel's fixed order (eight chunks of the section's
 // fibers, each summed sequentially, then a pairwise tree), so results do not depend on the launch
-// shape.
+// shape.  The section's fiber geometry and materials are copied to shared memory once per CTA.
 #pragma once
 
 #include "element_kernels.cuh"
@@ -35,6 +36,7 @@ namespace strut {
 
 constexpr int kFsTile = 4;        // instances per tile = instance warps per CTA
 constexpr int kFsMaxSteelWarps = 4;
+constexpr int kFsMaxMats = 16;    // materials copied to shared memory (more: read from global)
 
 __host__ __device__ inline int fs_pad4(int n) { return (n + 3) & ~3; }
 
@@ -45,7 +47,9 @@ struct FsLayout {
     int off_s2, off_c2, off_s1, off_c1, off_kon;  // offsets in a stage, in doubles
     int stage_doubles;                            // one stage, kon included, a multiple of 2
     int steel_warps;                              // W_s (0 without Steel02 fibers)
-    float inv_s2;                                 // 1 / n_s2
+    int n_mats;                                   // materials of the batch
+    int n_oth;                                    // non-Steel02 fibers of a section
+    float inv_s2, inv_oth;                        // 1 / n_s2, 1 / n_oth
     uint32_t bytes_s2, bytes_c2, bytes_s1, bytes_c1, bytes_kon, bytes_total;  // per field / tile
 };
 
@@ -70,7 +74,10 @@ __host__ __device__ inline FsLayout fs_layout(const DevSection& sd) {
     L.stage_doubles = L.off_kon + T * L.p_s2 / 2;
     const int ws = (T * sd.n_s2 + 31) / 32;
     L.steel_warps = ws < kFsMaxSteelWarps ? ws : kFsMaxSteelWarps;
+    L.n_mats = 0;
+    L.n_oth = L.n_tot - sd.n_s2;
     L.inv_s2 = sd.n_s2 ? 1.0f / sd.n_s2 : 0.0f;
+    L.inv_oth = L.n_oth ? 1.0f / L.n_oth : 0.0f;
     L.bytes_s2 = 8u * T * L.p_s2;
     L.bytes_c2 = 8u * T * L.p_c2;
     L.bytes_s1 = 8u * T * L.p_s1;
@@ -83,10 +90,15 @@ __host__ __device__ inline FsLayout fs_layout(const DevSection& sd) {
 // Threads of a CTA: the instance warps and the steel warps.
 __host__ __device__ inline int fs_threads(const FsLayout& L) { return 32 * (kFsTile + L.steel_warps); }
 
-// Dynamic shared memory of one CTA: two stages and, per stage, the per-fiber (sig A, tan A) of
-// the tile's instances.
+// Dynamic shared memory of one CTA: two stages; per stage, the per-fiber (sig A, tan A) of the
+// tile's instances; the section's fiber y and area; the materials (when at most kFsMaxMats); the
+// fibers' material indices.
+__host__ __device__ inline size_t fs_fk_doubles(const FsLayout& L) { return 2u * kFsTile * 2u * (size_t)L.n_tot; }
+__host__ __device__ inline size_t fs_geo_doubles(const FsLayout& L) {
+    return 2u * (size_t)L.n_tot + (L.n_mats <= kFsMaxMats ? (sizeof(DevMat) / 8) * (size_t)L.n_mats : 0u);
+}
 __host__ __device__ inline size_t fs_smem_bytes(const FsLayout& L) {
-    return 8u * (2u * (size_t)L.stage_doubles + 2u * (size_t)kFsTile * 2u * (size_t)L.n_tot);
+    return 8u * (2u * (size_t)L.stage_doubles + fs_fk_doubles(L) + fs_geo_doubles(L)) + 4u * (size_t)L.n_tot;
 }
 
 // q = r / n for 0 <= r < 2^22 and n >= 1, from a float estimate corrected to the exact quotient.
@@ -123,16 +135,25 @@ __device__ __forceinline__ void fs_load(const FsLayout& L, const BatchState& bs,
             bulk_g2s(st + L.off_c1 + f * T * L.p_c1, bs.c1 + f * N4 + t * T * L.p_c1, L.bytes_c1, bar);
 }
 
-// One fiber of a non-Steel02 family of instance i (section index j >= n_s2): trial state from the
-// stage at strain e, new committed state to HBM when commit, (sig A, tan A) returned.
-__device__ __forceinline__ void fs_other_fiber(const Geo& g, const DevSection& sd, const BatchState& bs,
-                                               const FsLayout& L, const double* st, int w, long long i, int j,
-                                               double e0, double ka, long long N3, long long N1, long long N4,
-                                               int commit, double& sA, double& tA) {
+
+// The section's fiber geometry as the kernel reads it (shared memory).
+struct FsGeo {
+    const double* y;
+    const double* a;
+    const int* m;
+    const DevMat* mats;
+};
+
+// One fiber of a non-Steel02 family of tile instance w (global instance i, section index
+// j >= n_s2): trial state from the stage at strain e0 - y ka, new committed state to HBM when
+// commit, (sig A, tan A) returned.
+__device__ __forceinline__ void fs_other_fiber(const FsGeo& G, const BatchState& bs, const FsLayout& L,
+                                               const double* st, int w, long long i, int j, double e0, double ka,
+                                               long long N3, long long N1, long long N4, int commit, double& sA,
+                                               double& tA) {
     constexpr int T = kFsTile;
-    const int gi = sd.geo_off + j;
-    const double y = __ldg(g.y + gi), A = __ldg(g.a + gi);
-    const DevMat& mat = g.mats[__ldg(g.m + gi)];
+    const double y = G.y[j], A = G.a[j];
+    const DevMat& mat = G.mats[G.m[j]];
     const double e = e0 - y * ka;
     int jj = j - L.n_s2;
     if (jj < L.n_c2) {
@@ -142,8 +163,8 @@ __device__ __forceinline__ void fs_other_fiber(const Geo& g, const DevSection& s
         c.eps = F[0]; c.sig = F[S]; c.tan = F[2 * S]; c.ecmin = F[3 * S]; c.dept = F[4 * S];
         concrete02_trial(mat, c, e, t);
         if (commit) {
-            double* G = bs.c2 + i * L.p_c2 + jj;
-            G[0] = t.eps; G[N3] = t.sig; G[2 * N3] = t.tan; G[3 * N3] = t.ecmin; G[4 * N3] = t.dept;
+            double* Gp = bs.c2 + i * L.p_c2 + jj;
+            Gp[0] = t.eps; Gp[N3] = t.sig; Gp[2 * N3] = t.tan; Gp[3 * N3] = t.ecmin; Gp[4 * N3] = t.dept;
         }
         sA = t.sig * A;
         tA = t.tan * A;
@@ -157,8 +178,8 @@ __device__ __forceinline__ void fs_other_fiber(const Geo& g, const DevSection& s
         c.eps = F[0]; c.sig = F[S]; c.tan = F[2 * S]; c.epsp = F[3 * S]; c.alpha = F[4 * S];
         steel01_trial(mat, c, e, t);
         if (commit) {
-            double* G = bs.s1 + i * L.p_s1 + jj;
-            G[0] = t.eps; G[N1] = t.sig; G[2 * N1] = t.tan; G[3 * N1] = t.epsp; G[4 * N1] = t.alpha;
+            double* Gp = bs.s1 + i * L.p_s1 + jj;
+            Gp[0] = t.eps; Gp[N1] = t.sig; Gp[2 * N1] = t.tan; Gp[3 * N1] = t.epsp; Gp[4 * N1] = t.alpha;
         }
         sA = t.sig * A;
         tA = t.tan * A;
@@ -172,9 +193,9 @@ __device__ __forceinline__ void fs_other_fiber(const Geo& g, const DevSection& s
         c.eps = F[0]; c.sig = F[S]; c.tan = F[2 * S]; c.emin = F[3 * S]; c.eend = F[4 * S]; c.slope = F[5 * S];
         concrete01_trial(mat, c, e, t);
         if (commit) {
-            double* G = bs.c1 + i * L.p_c1 + jj;
-            G[0] = t.eps; G[N4] = t.sig; G[2 * N4] = t.tan; G[3 * N4] = t.emin; G[4 * N4] = t.eend;
-            G[5 * N4] = t.slope;
+            double* Gp = bs.c1 + i * L.p_c1 + jj;
+            Gp[0] = t.eps; Gp[N4] = t.sig; Gp[2 * N4] = t.tan; Gp[3 * N4] = t.emin; Gp[4 * N4] = t.eend;
+            Gp[5 * N4] = t.slope;
         }
         sA = t.sig * A;
         tA = t.tan * A;
@@ -185,20 +206,22 @@ __device__ __forceinline__ void fs_other_fiber(const Geo& g, const DevSection& s
     tA = ks;
 }
 
-// Sums of one instance from its per-fiber (sig A, tan A): lane b < 8 sums chunk b (running sums
-// over a chunk, the elastic fibers' k12 apart), then a pairwise tree over the eight chunks; lane 0
-// writes N, Mz, k11, k12, k22.  Whole warp.
-__device__ __forceinline__ void fs_sums(const Geo& g, const DevSection& sd, const FsLayout& L, const double* fk,
-                                        int lane, double* out) {
+// Sums of the tile's instances with one warp: lane 8 w + b sums chunk b of instance w (running
+// sums over a chunk, the elastic fibers' k12 apart), then each instance's eight chunks are added
+// by a pairwise tree; lane 8 w writes N, Mz, k11, k12, k22 of instance w (when valid).
+__device__ __forceinline__ void fs_sums(const FsGeo& G, const DevSection& sd, const FsLayout& L, const double* fk,
+                                        int lane, int n_valid, double* out) {
     constexpr unsigned full = 0xffffffffu;
+    const int w = lane >> 3, b = lane & 7;
     const int n_nl = L.n_tot - L.n_el;
+    const double* f = fk + (size_t)w * 2 * L.n_tot;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
-    if (lane < 8) {
+    if (w < n_valid) {
         const int cs = (L.n_tot + 7) >> 3;
-        const int g0 = lane * cs, g1 = min(g0 + cs, L.n_tot);
+        const int g0 = b * cs, g1 = min(g0 + cs, L.n_tot);
         const int gm = min(g1, n_nl);
         for (int gg = g0; gg < gm; ++gg) {
-            const double fs = fk[2 * gg], ks = fk[2 * gg + 1], y = __ldg(g.y + sd.geo_off + gg);
+            const double fs = f[2 * gg], ks = f[2 * gg + 1], y = G.y[gg];
             a0 += fs;
             a1 += -fs * y;
             a2 += ks;
@@ -206,7 +229,7 @@ __device__ __forceinline__ void fs_sums(const Geo& g, const DevSection& sd, cons
             a4 += ks * y * y;
         }
         for (int gg = max(g0, n_nl); gg < g1; ++gg) {
-            const double fs = fk[2 * gg], ks = fk[2 * gg + 1], y = __ldg(g.y + sd.geo_off + gg);
+            const double fs = f[2 * gg], ks = f[2 * gg + 1], y = G.y[gg];
             a0 += fs;
             a1 += -fs * y;
             a2 += ks;
@@ -223,19 +246,20 @@ __device__ __forceinline__ void fs_sums(const Geo& g, const DevSection& sd, cons
         a4 += __shfl_down_sync(full, a4, o);
         a5 += __shfl_down_sync(full, a5, o);
     }
-    if (lane == 0) {
-        out[0] = a0;
-        out[1] = a1;
-        out[2] = a2;
-        out[3] = a3 + (sd.el_uniform ? 0.0 : a5);
-        out[4] = a4;
+    if (b == 0 && w < n_valid) {
+        double* o = out + 5 * w;
+        o[0] = a0;
+        o[1] = a1;
+        o[2] = a2;
+        o[3] = a3 + (sd.el_uniform ? 0.0 : a5);
+        o[4] = a4;
     }
 }
 
 // n_inst instances in n_tiles tiles (state allocated for n_tiles * kFsTile instances); ek:
 // n_inst x 2 (eps0, kappa); resp: n_inst x 5 (N, Mz, k11, k12, k22).  fs_threads(L) threads; CTA c
 // takes tiles c, c + gridDim.x, ...  *err is set when a wait does not complete within its bound
-// (the warps then stop; the loading lane first lets its copies in flight land).
+// (the warps then stop together; the loading lane first lets its copies in flight land).
 __global__ void __launch_bounds__(32 * (kFsTile + kFsMaxSteelWarps), 2)
     fiber_stream_kernel(Geo g, DevSection sd, BatchState bs, FsLayout L, long long n_inst, long long n_tiles,
                         const double* __restrict__ ek, double* __restrict__ resp, int commit,
@@ -244,124 +268,159 @@ __global__ void __launch_bounds__(32 * (kFsTile + kFsMaxSteelWarps), 2)
     constexpr unsigned all = 0xffffffffu;
     extern __shared__ __align__(128) double fs_smem[];
     // per stage: full (bulk copies landed), read (every warp has read the stage), steel (the
-    // Steel02 results of the tile are in fk), summed (every instance warp has read fk)
+    // Steel02 results of the tile are in fk), summed (the tile's sums have read fk)
     __shared__ __align__(8) uint64_t bar_full[2], bar_read[2], bar_steel[2], bar_summed[2];
-    __shared__ double s_ek[kFsMaxSteelWarps][2 * T];  // strains of the tile, per steel warp
+    __shared__ int s_abort;            // the instance warps stop together
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = T + L.steel_warps;
     double* const fkb = fs_smem + 2 * L.stage_doubles;  // [stage][instance] x n_tot x {sig A, tan A}
+    double* const gy = fkb + fs_fk_doubles(L);
+    double* const ga = gy + L.n_tot;
+    DevMat* const gm = reinterpret_cast<DevMat*>(ga + L.n_tot);
+    int* const gmi = reinterpret_cast<int*>(gy + fs_geo_doubles(L));
+    FsGeo G;
+    G.y = gy;
+    G.a = ga;
+    G.m = gmi;
+    G.mats = L.n_mats <= kFsMaxMats ? gm : g.mats;
     const long long N2 = bs.n_inst * L.p_s2, N3 = bs.n_inst * L.p_c2, N1 = bs.n_inst * L.p_s1,
                     N4 = bs.n_inst * L.p_c1;
+    for (int j = threadIdx.x; j < L.n_tot; j += blockDim.x) {
+        gy[j] = __ldg(g.y + sd.geo_off + j);
+        ga[j] = __ldg(g.a + sd.geo_off + j);
+        gmi[j] = __ldg(g.m + sd.geo_off + j);
+    }
+    if (L.n_mats <= kFsMaxMats)
+        for (int q = threadIdx.x; q < L.n_mats * (int)(sizeof(DevMat) / 4); q += blockDim.x)
+            reinterpret_cast<uint32_t*>(gm)[q] = __ldg(reinterpret_cast<const uint32_t*>(g.mats) + q);
     if (threadIdx.x == 0) {
         for (int s = 0; s < 2; ++s) {
             mbar_init(&bar_full[s], 1);
             mbar_init(&bar_read[s], W);
             mbar_init(&bar_steel[s], L.steel_warps > 0 ? L.steel_warps : 1);
-            mbar_init(&bar_summed[s], T);
+            mbar_init(&bar_summed[s], 1);
         }
+        s_abort = 0;
         mbar_fence_init();
     }
-    __syncthreads();  // barrier initialisation: the kernel's only CTA-wide barrier
+    __syncthreads();  // geometry and barrier initialisation: the kernel's only CTA-wide barrier
     const long long t0 = blockIdx.x;
     if (t0 >= n_tiles) return;
-    const long long G = gridDim.x;
+    const long long G_ = gridDim.x;
     // the loading lane (lane 0 of warp 0) tracks the copies it issued and nobody has waited for
     uint32_t pend = 0u, pend_par = 0u;  // bit s: stage s has a copy in flight / its phase parity
     if (threadIdx.x == 0) {
         fs_load(L, bs, N2, N3, N1, N4, t0, fs_smem, &bar_full[0]);
         pend |= 1u;
-        if (t0 + G < n_tiles) {
-            fs_load(L, bs, N2, N3, N1, N4, t0 + G, fs_smem + L.stage_doubles, &bar_full[1]);
+        if (t0 + G_ < n_tiles) {
+            fs_load(L, bs, N2, N3, N1, N4, t0 + G_, fs_smem + L.stage_doubles, &bar_full[1]);
             pend |= 2u;
         }
     }
+    // strains of tile t: thread q < 2T of a warp loads value q (instance q / 2 of the tile)
+    auto strains = [&](long long t) -> double {
+        const long long q = 2 * t * T + lane;
+        return (lane < 2 * T && t < n_tiles && q < 2 * n_inst) ? __ldg(ek + q) : 0.0;
+    };
     bool ok = true;
     if (warp < T) {
-        // ---- instance warp w: its instance's non-Steel02 fibers, then its sums
+        // ---- instance warps: the tile's non-Steel02 fibers, then (one warp per tile) the sums
         const int w = warp;
-        auto strain = [&](long long t) -> double {
-            const long long i = t * T + w;
-            return (lane < 2 && t < n_tiles && i < n_inst) ? __ldg(ek + 2 * i + lane) : 0.0;
-        };
-        double ek_cur = strain(t0);
+        const int n_items = T * L.n_oth;
+        double ek_cur = strains(t0);
         for (int k = 0;; ++k) {
-            const long long t = t0 + k * G;
+            const long long t = t0 + k * G_;
             if (t >= n_tiles) break;
             const int s = k & 1;
             const uint32_t par = (uint32_t)(k >> 1) & 1u;
             const double* st = fs_smem + s * L.stage_doubles;
-            double* fk = fkb + (size_t)(s * T + w) * 2 * L.n_tot;
-            const long long i = t * T + w;
-            const bool valid = i < n_inst;
-            const double e0 = __shfl_sync(all, ek_cur, 0), ka = __shfl_sync(all, ek_cur, 1);
-            ek_cur = strain(t + G);
-            ok = __all_sync(all, mbar_wait_bounded(&bar_full[s], par));
-            if (!ok) break;
-            if (threadIdx.x == 0) pend &= ~(1u << s);
-            if (valid)
-                for (int j = L.n_s2 + lane; j < L.n_tot; j += 32) {
+            double* fk = fkb + (size_t)s * T * 2 * L.n_tot;
+            const int n_valid = (int)min((long long)T, n_inst - t * T);
+            const double ek_here = ek_cur;  // lanes 2q, 2q + 1: eps0, kappa of tile instance q
+            ek_cur = strains(t + G_);
+            if (__all_sync(all, mbar_wait_bounded(&bar_full[s], par))) {
+                if (threadIdx.x == 0) pend &= ~(1u << s);
+                for (int base = w * 32; base < n_items; base += 32 * T) {
+                    const int q = base + lane;
+                    const int inst = q < n_items ? fs_div(q, L.n_oth, L.inv_oth) : 0;
+                    const double e0 = __shfl_sync(all, ek_here, 2 * inst),
+                                 ka = __shfl_sync(all, ek_here, 2 * inst + 1);
+                    if (q >= n_items || inst >= n_valid) continue;
+                    const int j = L.n_s2 + (q - inst * L.n_oth);
                     double sA, tA;
-                    fs_other_fiber(g, sd, bs, L, st, w, i, j, e0, ka, N3, N1, N4, commit, sA, tA);
-                    fk[2 * j] = sA;
-                    fk[2 * j + 1] = tA;
+                    fs_other_fiber(G, bs, L, st, inst, t * T + inst, j, e0, ka, N3, N1, N4, commit, sA, tA);
+                    double* f = fk + (size_t)inst * 2 * L.n_tot;
+                    f[2 * j] = sA;
+                    f[2 * j + 1] = tA;
                 }
-            __syncwarp();
-            if (lane == 0) fs_arrive(&bar_read[s]);
-            if (L.steel_warps) {
-                ok = __all_sync(all, mbar_wait_bounded(&bar_steel[s], par));
-                if (!ok) break;
+                __syncwarp();
+                if (lane == 0) fs_arrive(&bar_read[s]);
+            } else if (lane == 0) {
+                s_abort = 1;
             }
-            if (valid) fs_sums(g, sd, L, fk, lane, resp + 5 * i);
-            __syncwarp();
-            if (lane == 0) fs_arrive(&bar_summed[s]);
+            // the instance warps' fibers of the tile are in fk (and the sums of tile t - G have
+            // read fk of the other stage)
+            asm volatile("bar.sync 1, %0;" ::"r"(32 * T) : "memory");
+            if (s_abort) break;
+            // one warp per tile forms the sums; the others go on to the next tile
+            if (w == (k & (T - 1))) {
+                if (!L.steel_warps || __all_sync(all, mbar_wait_bounded(&bar_steel[s], par))) {
+                    fs_sums(G, sd, L, fk, lane, n_valid, resp + 5 * t * T);
+                    __syncwarp();
+                    if (lane == 0) fs_arrive(&bar_summed[s]);
+                } else if (lane == 0) {
+                    s_abort = 1;
+                }
+            }
             // the loading lane refills stage s with tile t + 2G once every warp has read tile t
-            if (threadIdx.x == 0 && t + 2 * G < n_tiles) {
+            if (threadIdx.x == 0 && t + 2 * G_ < n_tiles) {
                 if (mbar_wait_bounded(&bar_read[s], par)) {
-                    fs_load(L, bs, N2, N3, N1, N4, t + 2 * G, fs_smem + s * L.stage_doubles, &bar_full[s]);
+                    fs_load(L, bs, N2, N3, N1, N4, t + 2 * G_, fs_smem + s * L.stage_doubles, &bar_full[s]);
                     pend |= 1u << s;
                     pend_par = (pend_par & ~(1u << s)) | ((par ^ 1u) << s);
                 } else {
-                    ok = false;
+                    s_abort = 1;
                 }
             }
-            ok = __shfl_sync(all, ok ? 1 : 0, 0) != 0;
-            if (!ok) break;
+            __syncwarp();
         }
+        // a failure in the last tile (no later barrier to meet at) is seen here
+        ok = *reinterpret_cast<volatile int*>(&s_abort) == 0;
     } else {
         // ---- steel warp v: the Steel02 fibers of every instance of the tile
         const int v = warp - T;
         const int n_items = T * L.n_s2;
-        auto strains = [&](long long t) -> double {
-            const long long q = 2 * t * T + lane;
-            return (lane < 2 * T && t < n_tiles && q < 2 * n_inst) ? __ldg(ek + q) : 0.0;
-        };
         double ek_cur = strains(t0);
         for (int k = 0;; ++k) {
-            const long long t = t0 + k * G;
+            const long long t = t0 + k * G_;
             if (t >= n_tiles) break;
             const int s = k & 1;
             const uint32_t par = (uint32_t)(k >> 1) & 1u;
             const double* st = fs_smem + s * L.stage_doubles;
-            if (lane < 2 * T) s_ek[v][lane] = ek_cur;
-            __syncwarp();
-            ek_cur = strains(t + G);
+            double* fk = fkb + (size_t)s * T * 2 * L.n_tot;
+            // the tile's strains, one instance per lane pair; lanes read them by shuffle below
+            const double ek_here = ek_cur;
+            ek_cur = strains(t + G_);
             ok = __all_sync(all, mbar_wait_bounded(&bar_full[s], par));
-            // fk of this stage is free once the instance warps have summed tile t - 2G
+            // fk of this stage is free once the sums of tile t - 2G have read it
             if (ok && k >= 2) ok = __all_sync(all, mbar_wait_bounded(&bar_summed[s], par ^ 1u));
             if (!ok) break;
-            for (int q = v * 32 + lane; q < n_items; q += 32 * L.steel_warps) {
-                const int inst = fs_div(q, L.n_s2, L.inv_s2), j = q - inst * L.n_s2;
+            for (int base = v * 32; base < n_items; base += 32 * L.steel_warps) {
+                const int q = base + lane;
+                const int inst = q < n_items ? fs_div(q, L.n_s2, L.inv_s2) : 0;
+                const double e0 = __shfl_sync(all, ek_here, 2 * inst), ka = __shfl_sync(all, ek_here, 2 * inst + 1);
+                if (q >= n_items) continue;
+                const int j = q - inst * L.n_s2;
                 const long long i = t * T + inst;
                 if (i >= n_inst) continue;
                 const int S = T * L.p_s2, x = inst * L.p_s2 + j;
                 const double* F = st + L.off_s2 + x;
-                const int gi = sd.geo_off + j;
-                const double y = __ldg(g.y + gi), A = __ldg(g.a + gi);
+                const double y = G.y[j], A = G.a[j];
                 S2State c, tr;
                 c.eps = F[0]; c.sig = F[S]; c.tan = F[2 * S]; c.epsmin = F[3 * S]; c.epsmax = F[4 * S];
                 c.epspl = F[5 * S]; c.epss0 = F[6 * S]; c.sigs0 = F[7 * S]; c.epsr = F[8 * S]; c.sigr = F[9 * S];
                 c.kon = reinterpret_cast<const int*>(st + L.off_kon)[x];
-                steel02_trial(g.mats[__ldg(g.m + gi)], c, s_ek[v][2 * inst] - y * s_ek[v][2 * inst + 1], tr);
+                steel02_trial(G.mats[G.m[j]], c, e0 - y * ka, tr);
                 if (commit) {
                     double* Gp = bs.s2 + i * L.p_s2 + j;
                     Gp[0] = tr.eps; Gp[N2] = tr.sig; Gp[2 * N2] = tr.tan; Gp[3 * N2] = tr.epsmin;
@@ -369,9 +428,9 @@ __global__ void __launch_bounds__(32 * (kFsTile + kFsMaxSteelWarps), 2)
                     Gp[8 * N2] = tr.epsr; Gp[9 * N2] = tr.sigr;
                     bs.kon[i * L.p_s2 + j] = tr.kon;
                 }
-                double* fk = fkb + (size_t)(s * T + inst) * 2 * L.n_tot;
-                fk[2 * j] = tr.sig * A;
-                fk[2 * j + 1] = tr.tan * A;
+                double* f = fk + (size_t)inst * 2 * L.n_tot;
+                f[2 * j] = tr.sig * A;
+                f[2 * j + 1] = tr.tan * A;
             }
             __syncwarp();
             if (lane == 0) {

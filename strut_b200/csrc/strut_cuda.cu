@@ -2016,6 +2016,7 @@ struct StrutSectionBatch {
     // streaming kernel: stage geometry, tiles, persistent grid (0: the stages do not fit, one warp
     // per instance instead)
     FsLayout L{};
+    int n_mats = 0;
     long long n_tiles = 0;
     int grid = 0;
     size_t smem = 0;
@@ -2093,6 +2094,7 @@ static int fs_configure(StrutSectionBatch* b) {
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     b->L = fs_layout(b->sd);
+    b->L.n_mats = b->n_mats;
     b->smem = fs_smem_bytes(b->L);
     b->n_tiles = (b->n_inst + kFsTile - 1) / kFsTile;
     b->grid = 0;
@@ -2119,6 +2121,7 @@ int strut_gpu_section_batch_create(const StrutUniMaterial* materials, int32_t nu
     for (int i = 0; i < num_materials; ++i) mats.push_back(make_devmat(materials[i]));
     StrutSectionBatch* b = new StrutSectionBatch();
     b->n_inst = n_inst;
+    b->n_mats = num_materials;
     b->sd = sp.secs[0];
     DevMat* d_mats;
     DevSection* d_secs;
