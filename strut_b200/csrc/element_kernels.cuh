@@ -1085,6 +1085,71 @@ struct RecPass {
 // Newton iteration of a few slow records launches no idle CTAs and a slow element does not hold
 // up elements queued behind it on the same CTA.
 //
+// Saves the accepted state a fanned element's next pass starts from in its round record and posts
+// the pass's twelve attempts to the list's queue (thread 0 of the resolving CTA).
+__device__ __noinline__ void post_next_pass(const ElemList& el, int cur, int fslot, double* R, int round, int guard,
+                                            const ElemScratch& S, int nip) {
+    R[kFRound] = (double)(round + 1);
+    R[kFGuard] = (double)guard;
+    R[kFLocal] = (double)S.local_iters;
+    R[kFEvals] = (double)S.section_evals;
+    R[kFHard] = (double)S.hard;
+    R[kFCValid] = (double)S.c_valid;
+    R[kFBestOk] = (double)S.best_ok;
+    for (int i = 0; i < 3; ++i) {
+        R[kFAccV + i] = S.acc_v[i];
+        R[kFAccQ + i] = S.acc_q[i];
+        R[kFRem + i] = S.att[i];
+    }
+    for (int i = 0; i < 10; ++i) R[kFBest + i] = S.best[i];
+    for (int ip = 0; ip < nip; ++ip) {
+        R[kFSvsE + ip] = S.svs_e[ip];
+        R[kFSvsK + ip] = S.svs_k[ip];
+        R[kFCN + ip] = S.c_n[ip];
+        R[kFCM + ip] = S.c_m[ip];
+        R[kFC00 + ip] = S.c_f00[ip];
+        R[kFC01 + ip] = S.c_f01[ip];
+        R[kFC11 + ip] = S.c_f11[ip];
+    }
+    el.fan_first[cur * kFanCap + fslot] = kFanAttempts;
+    __threadfence();
+    const int d0 = atomicAdd(&el.rq_tail[cur], kFanAttempts);
+    long long* q = el.rq + (size_t)cur * kRoundQ;
+    for (int a = 0; a < kFanAttempts; ++a) {
+        const int d = d0 + a;
+        const long long v = ((long long)d << 16) | (long long)(fslot * kFanAttempts + a);
+        // an entry is free once its previous attempt was taken (bounded wait)
+        int n = 0;
+        while (atomicCAS(reinterpret_cast<unsigned long long*>(q + d % kRoundQ), ~0ull, (unsigned long long)v) !=
+               ~0ull) {
+            if (++n > kQueuePolls) {
+                atomicExch(el.q_err, 1);
+                break;
+            }
+            __nanosleep(128);
+        }
+    }
+}
+
+// Takes the posted attempt with queue ticket d: returns slot x 12 + attempt, or -1 once every
+// fanned element of the list is resolved and no attempt has ticket d (thread 0).
+__device__ __noinline__ int take_posted(const ElemList& el, int cur, int d, int n_slots) {
+    volatile long long* q = el.rq + (size_t)cur * kRoundQ + d % kRoundQ;
+    for (int n = 0; n < kQueuePolls; ++n) {
+        const long long v = *q;
+        if (v >= 0 && (v >> 16) == (long long)d) {
+            __threadfence();
+            *q = -1;  // free the entry
+            return (int)(v & 0xFFFF);
+        }
+        if (*(volatile int*)(el.fan_finished + cur) >= n_slots && *(volatile int*)(el.rq_tail + cur) <= d)
+            return -1;
+        __nanosleep(n < 256 ? 64 : 512);
+    }
+    atomicExch(el.q_err, 1);
+    return -1;
+}
+
 // Element-level scratch of the element kernel: the 3D scratch exists only in the 3D instance (a
 // smaller static footprint lets more 2D element CTAs share an SM).
 template <int DIM>
@@ -1118,7 +1183,9 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         mbar_fence_init();
     }
     __shared__ int s_next;
-    __shared__ int s_fan;  // a fan attempt has already counted itself in (fan_done)
+    __shared__ int s_fan;    // a fan attempt has already counted itself in (fan_done)
+    __shared__ int s_round;  // pass of the fanned element this CTA works on (1: the first)
+    __shared__ int s_item;   // posted attempt taken from the queue (-1: none)
     const int cur = all_elems ? 0 : (ctl->iter & 1);
     // fanned-out elements of this list (their attempts come first in the work order)
     const int n_fan = all_elems ? 0 : min(el.hard_count[cur], (int)kFanCap) * kFanAttempts;
@@ -1126,6 +1193,10 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         el.count[cur ^ 1] = 0;
         el.next[cur ^ 1] = 0;
         el.hard_count[cur ^ 1] = 0;
+        if (el.rq) {
+            el.rq_tail[cur ^ 1] = 0;
+            el.fan_finished[cur ^ 1] = 0;
+        }
     }
     const int total = mode == ELEM_MODE_ALL ? n_elem
                     : mode == ELEM_MODE_RECORD ? rp.n : n_fan + el.count[cur];
@@ -1136,7 +1207,11 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     auto process = [&](const int e, const int fslot, const int fa) -> void {
     copy_struct(&E, elems + e);
     __syncthreads();
-    if (mode == ELEM_MODE_RECORD ? status[E.inst] != 0 : !active[E.inst]) return;
+    if (mode == ELEM_MODE_RECORD ? status[E.inst] != 0 : !active[E.inst]) {
+        // a fanned element that is not run still counts as resolved (its first attempt's CTA)
+        if (fslot >= 0 && fa == 0 && tid == 0 && el.rq) atomicAdd(&el.fan_finished[cur], 1);
+        return;
+    }
     copy_struct(&sd, g.secs + E.sec);
     if constexpr (DIM == 3) {
         __syncthreads();
@@ -1293,6 +1368,31 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         S.best_ok = 0;
         S.loop_ctrl = 0;
     }
+    // a later pass of a fanned-out element starts from the state its previous pass accepted
+    if (fslot >= 0 && tid == 0) {
+        const double* R = el.fan_round + (size_t)(cur * kFanCap + fslot) * kFanRound;
+        s_round = (int)__ldcg(R + kFRound);
+        if (s_round > 1) {
+            for (int i = 0; i < 3; ++i) {
+                S.acc_v[i] = __ldcg(R + kFAccV + i);
+                S.acc_q[i] = __ldcg(R + kFAccQ + i);
+                S.rem[i] = __ldcg(R + kFRem + i);
+                S.att[i] = S.rem[i];
+            }
+            for (int i = 0; i < 10; ++i) S.best[i] = __ldcg(R + kFBest + i);
+            S.best_ok = (int)__ldcg(R + kFBestOk);
+            S.c_valid = (int)__ldcg(R + kFCValid);
+            for (int ip = 0; ip < nip; ++ip) {
+                S.svs_e[ip] = __ldcg(R + kFSvsE + ip);
+                S.svs_k[ip] = __ldcg(R + kFSvsK + ip);
+                S.c_n[ip] = __ldcg(R + kFCN + ip);
+                S.c_m[ip] = __ldcg(R + kFCM + ip);
+                S.c_f00[ip] = __ldcg(R + kFC00 + ip);
+                S.c_f01[ip] = __ldcg(R + kFC01 + ip);
+                S.c_f11[ip] = __ldcg(R + kFC11 + ip);
+            }
+        }
+    }
     __syncthreads();
     int converged = 0;
     if (sd.all_elastic) {
@@ -1377,15 +1477,34 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
                     s_fan = 1;
                     return;  // not the last attempt: the last one finishes the element
                 }
-                if (tid == 0) s_fan = 1;
+                double* R = el.fan_round + (size_t)(cur * kFanCap + fslot) * kFanRound;
+                const int round = s_round;
+                const int guard_before = round > 1 ? (int)__ldcg(R + kFGuard) : 0;
+                if (tid == 0) {
+                    s_fan = 1;
+                    if (round > 1) {  // the passes before this one
+                        S.local_iters += (int)__ldcg(R + kFLocal);
+                        S.section_evals += (int)__ldcg(R + kFEvals);
+                        if (__ldcg(R + kFHard) != 0.0) S.hard = 1;
+                    }
+                }
                 if (best_a < 0) {
                     run_loop = false;  // every attempt failed: the initial-tangent fallback
+                    guard = guard_before + 4;
                 } else {
                     if (S.loop_ctrl == 1) {
                         converged = 1;
                         run_loop = false;
                     }
-                    guard = best_a / 3 + 1;
+                    guard = guard_before + best_a / 3 + 1;
+                    // the next pass over the remainder, fanned out while the guard leaves room
+                    // for all four of its levels
+                    if (run_loop && guard + 4 <= 10000) {
+                        __syncthreads();
+                        if (tid == 0) post_next_pass(el, cur, fslot, R, round, guard, S, nip);
+                        __syncthreads();
+                        return;
+                    }
                 }
             }
             while (run_loop && num_subdivide <= 4 && guard < 10000) {
@@ -1484,7 +1603,10 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         }
         es[kEcv] = S.c_valid ? 1.0 : 0.0;
         if (el.hard_flag && mode == ELEM_MODE_LIST) el.hard_flag[e] = ctl->fan ? S.hard : 0;
-        if (fslot >= 0) atomicAdd(&counters[6], 1ull);
+        if (fslot >= 0) {
+            atomicAdd(&counters[6], 1ull);
+            atomicAdd(&el.fan_finished[cur], 1);  // the fanned element is resolved
+        }
     }
     __syncthreads();
     if (S.flag) {
@@ -1542,30 +1664,44 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     };
     // first element by block index, then dynamically: thread 0 claims the next list entry while
     // the CTA works on the current one (the claim's latency hides behind the element)
+    // Tickets beyond the list are attempts of later passes of fanned elements, posted while the
+    // launch runs (el.rq); a CTA holding such a ticket waits for its attempt while any fanned
+    // element is unresolved.
     int li = blockIdx.x;
-    while (li < total && !stop) {
+    const bool queue = mode == ELEM_MODE_LIST && n_fan > 0 && el.rq != nullptr;
+    while (!stop && (li < total || queue)) {
+        int item = -1;  // slot x 12 + attempt of a fan-out attempt
+        if (li >= total) {
+            if (tid == 0) s_item = take_posted(el, cur, li - total, n_fan / kFanAttempts);
+            __syncthreads();
+            item = s_item;
+            __syncthreads();
+            if (item < 0) break;
+        } else if (mode == ELEM_MODE_LIST && li < n_fan) {
+            item = li;
+        }
         int claimed = li + gridDim.x;
         if (!all_elems && tid == 0) claimed = atomicAdd(&el.next[cur], 1) + gridDim.x;
         int pe = -1;
-        const bool fan_item = mode == ELEM_MODE_LIST && li < n_fan;
+        const bool fan_item = item >= 0;
         if (mode == ELEM_MODE_ALL) {
             pe = li;
         } else if (mode == ELEM_MODE_RECORD) {
             pe = rp.list[li];
         } else if (fan_item) {
-            pe = el.hard[cur][li / kFanAttempts];
+            pe = el.hard[cur][item / kFanAttempts];
         } else {
             const int ent = el.list[cur][li - n_fan];
             if (!(ent & kFanBit)) pe = ent;
         }
         if (tid == 0) s_fan = 0;
-        if (pe >= 0) process(pe, fan_item ? li / kFanAttempts : -1, li % kFanAttempts);
+        if (pe >= 0) process(pe, fan_item ? item / kFanAttempts : -1, fan_item ? item % kFanAttempts : 0);
         if (fan_item) {
             __syncthreads();
             // every attempt counts itself in exactly once, whatever path it took
             if (tid == 0 && !s_fan) {
                 __threadfence();
-                atomicAdd(&el.fan_done[cur * kFanCap + li / kFanAttempts], 1);
+                atomicAdd(&el.fan_done[cur * kFanCap + item / kFanAttempts], 1);
             }
         }
         if (tid == 0) s_next = claimed;

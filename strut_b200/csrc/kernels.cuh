@@ -129,10 +129,28 @@ struct Attempt {
 // reference's order (level by level, scheme 0, 1, 2) and carries on from there as the sequential
 // algorithm would, so the result is the sequential one bit for bit.  Its plain list entry carries
 // kFanBit and is skipped.  At most kFanCap elements are fanned out per list.
+//
+// Later passes fan out too.  When the chosen attempt leaves part of the increment (an accepted
+// subdivision), the sequential algorithm starts a new pass over the remainder from level 1; the
+// resolving CTA saves the element's accepted state in the slot's round record, posts the next
+// pass's twelve attempts to a queue that the persistent CTAs of the same launch take work from,
+// and leaves the element; the pass's last attempt resolves it in turn.  CTAs whose next ticket lies
+// beyond the posted items wait for one while any fanned element is unresolved.  A pass is fanned
+// out only while the sequential loop's guard leaves room for all four levels; otherwise the
+// resolving CTA goes on sequentially, so the result is the sequential one bit for bit.
 constexpr int kFanAttempts = 12;  // 4 subdivision levels x 3 schemes
 constexpr int kFanCap = 512;
 constexpr int kFanRec = 88;       // doubles per attempt record
 constexpr int kFanBit = 0x40000000;
+constexpr int kFanRound = 96;     // doubles per round record (the state a pass starts from)
+constexpr int kRoundQ = 8192;     // queue entries per list buffer (a ring)
+constexpr int kQueuePolls = 1 << 26;  // bound on a queue wait (polls with a short sleep)
+// round record fields
+enum {
+    kFRound = 0, kFGuard = 1, kFLocal = 2, kFEvals = 3, kFHard = 4, kFCValid = 5, kFBestOk = 6,
+    kFAccV = 7, kFAccQ = 10, kFRem = 13, kFBest = 16, kFSvsE = 26, kFSvsK = 36, kFCN = 46, kFCM = 56,
+    kFC00 = 66, kFC01 = 76, kFC11 = 86
+};
 
 struct ElemList {
     int* list[2];
@@ -147,6 +165,12 @@ struct ElemList {
     double* fan_rec;    // 2 x kFanCap x kFanAttempts x kFanRec attempt records
     int* fan_first;     // 2 x kFanCap: the earliest attempt that has succeeded (kFanAttempts:
                         // none yet); a later attempt stops as soon as it sees an earlier success
+    double* fan_round;  // 2 x kFanCap x kFanRound: the state each slot's current pass starts from
+    long long* rq;      // 2 x kRoundQ: posted attempts, (ticket << 16) | (slot x 12 + attempt);
+                        // -1 when free (the taker frees it)
+    int* rq_tail;       // 2 entries: queue tickets handed to posted attempts
+    int* fan_finished;  // 2 entries: fanned elements of the list that are resolved
+    int* q_err;         // a queue wait that ran out
 };
 
 // List entry of element e in list buffer `buf`: a flagged element also gets a fan slot.
@@ -157,6 +181,7 @@ __device__ __forceinline__ int list_entry(const ElemList& el, int buf, int e) {
             el.hard[buf][slot] = e;
             el.fan_done[buf * kFanCap + slot] = 0;
             el.fan_first[buf * kFanCap + slot] = kFanAttempts;
+            if (el.fan_round) el.fan_round[(size_t)(buf * kFanCap + slot) * kFanRound + kFRound] = 1.0;
             return e | kFanBit;
         }
     }

@@ -1437,7 +1437,10 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
                 }
         if (any_fbc2d &&
             ((rc = dzeros(&A.el.hard_flag, (size_t)h->n_elem, al)) ||
-             (rc = dzeros(&A.el.fan_rec, (size_t)2 * kFanCap * kFanAttempts * kFanRec, al))))
+             (rc = dzeros(&A.el.fan_rec, (size_t)2 * kFanCap * kFanAttempts * kFanRec, al)) ||
+             (rc = dzeros(&A.el.fan_round, (size_t)2 * kFanCap * kFanRound, al)) ||
+             (rc = dzeros(&A.el.rq, (size_t)2 * kRoundQ, al)) || (rc = dzeros(&A.el.rq_tail, 2, al)) ||
+             (rc = dzeros(&A.el.fan_finished, 2, al)) || (rc = dzeros(&A.el.q_err, 1, al))))
             return bail(rc);
     }
     if (h->any_modified &&
@@ -1643,6 +1646,12 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
         CK(cudaMemsetAsync(h->A.el.count, 0, 2 * sizeof(int), h->stream));
         CK(cudaMemsetAsync(h->A.el.next, 0, 2 * sizeof(int), h->stream));
         CK(cudaMemsetAsync(h->A.el.hard_count, 0, 2 * sizeof(int), h->stream));
+        if (h->A.el.rq) {
+            // the attempt queue starts empty (-1 entries) for every run
+            CK(cudaMemsetAsync(h->A.el.rq, 0xFF, sizeof(long long) * 2 * kRoundQ, h->stream));
+            CK(cudaMemsetAsync(h->A.el.rq_tail, 0, 2 * sizeof(int), h->stream));
+            CK(cudaMemsetAsync(h->A.el.fan_finished, 0, 2 * sizeof(int), h->stream));
+        }
         CK(cudaStreamSynchronize(h->stream));
     }
     if (n_steps > 0 && !h->prof && h->n_large == 0) {
@@ -1762,6 +1771,14 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
     }
     // fiber updates: per section evaluation, the section's fiber count
     st.fiber_updates = (int64_t)cnt[2];
+    if (h->A.el.q_err) {
+        int qe = 0;
+        CK(cudaMemcpy(&qe, h->A.el.q_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (qe) {
+            rc = fail(STRUT_CUDA_ERROR, "a wait on the element attempt queue ran out");
+            CK(cudaMemset(h->A.el.q_err, 0, sizeof(int)));
+        }
+    }
     st.status = rc;
     if (rc != STRUT_OK) {
         std::vector<int> ee(h->n_elem);
