@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-predictor arm")
     ap.add_argument("--train-frames", type=int, default=64)
-    ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--train-epochs", type=int, default=60)
     ap.add_argument("--learned3d-steps", type=int, default=4000,
                     help="record steps of the 3D learned-predictor arm (config 3)")
     ap.add_argument("--no-learned3d", action="store_true", help="skip the 3D learned-predictor arm")

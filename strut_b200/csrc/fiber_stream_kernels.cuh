@@ -18,10 +18,10 @@
 // round is nearly full), and W_s steel warps take the Steel02 fibers of all the tile's instances
 // together, so the expensive Menegotto-Pinto branch runs on full warps instead of a few lanes of
 // every warp.  Two stages: the TMA unit (cp.async.bulk, mbarrier completion, no multicast) brings
-// tile k + 2 into a stage as soon as every warp has read tile k from it.  The steel warps hand
-// their results over through mbarriers (stage full / stage read / steel results written / sums
-// done); the instance warps meet at one named barrier per tile (not the steel warps), after which
-// one of them forms the four instances' sums with all 32 lanes while the others go on to the next
+// tile k + 2 into a stage as soon as every warp has read tile k from it.  The warps hand work to
+// one another through mbarriers only (stage full / stage read / steel and instance results
+// written / sums done), never a CTA-wide barrier: one instance warp per tile forms the four
+// instances' sums with all 32 lanes once every result is in, while the others go on to the next
 // tile.  Each lane writes its fibers' new state straight back to HBM (consecutive lanes,
 // consecutive fibers), and the per-fiber stress and tangent (times area) go to shared memory, from
 // which the sums are formed in the element kernel's fixed order (eight chunks of the section's
@@ -267,10 +267,10 @@ __global__ void __launch_bounds__(32 * (kFsTile + kFsMaxSteelWarps), 2)
     constexpr int T = kFsTile;
     constexpr unsigned all = 0xffffffffu;
     extern __shared__ __align__(128) double fs_smem[];
-    // per stage: full (bulk copies landed), read (every warp has read the stage), steel (the
-    // Steel02 results of the tile are in fk), summed (the tile's sums have read fk)
-    __shared__ __align__(8) uint64_t bar_full[2], bar_read[2], bar_steel[2], bar_summed[2];
-    __shared__ int s_abort;            // the instance warps stop together
+    // per stage: full (bulk copies landed), read (every warp has read the stage), steel / inst
+    // (the steel / instance warps' results of the tile are in fk), summed (the tile's sums have
+    // read fk)
+    __shared__ __align__(8) uint64_t bar_full[2], bar_read[2], bar_steel[2], bar_inst[2], bar_summed[2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = T + L.steel_warps;
     double* const fkb = fs_smem + 2 * L.stage_doubles;  // [stage][instance] x n_tot x {sig A, tan A}
@@ -298,9 +298,9 @@ __global__ void __launch_bounds__(32 * (kFsTile + kFsMaxSteelWarps), 2)
             mbar_init(&bar_full[s], 1);
             mbar_init(&bar_read[s], W);
             mbar_init(&bar_steel[s], L.steel_warps > 0 ? L.steel_warps : 1);
+            mbar_init(&bar_inst[s], T);
             mbar_init(&bar_summed[s], 1);
         }
-        s_abort = 0;
         mbar_fence_init();
     }
     __syncthreads();  // geometry and barrier initialisation: the kernel's only CTA-wide barrier
@@ -338,39 +338,37 @@ __global__ void __launch_bounds__(32 * (kFsTile + kFsMaxSteelWarps), 2)
             const int n_valid = (int)min((long long)T, n_inst - t * T);
             const double ek_here = ek_cur;  // lanes 2q, 2q + 1: eps0, kappa of tile instance q
             ek_cur = strains(t + G_);
-            if (__all_sync(all, mbar_wait_bounded(&bar_full[s], par))) {
-                if (threadIdx.x == 0) pend &= ~(1u << s);
-                for (int base = w * 32; base < n_items; base += 32 * T) {
-                    const int q = base + lane;
-                    const int inst = q < n_items ? fs_div(q, L.n_oth, L.inv_oth) : 0;
-                    const double e0 = __shfl_sync(all, ek_here, 2 * inst),
-                                 ka = __shfl_sync(all, ek_here, 2 * inst + 1);
-                    if (q >= n_items || inst >= n_valid) continue;
-                    const int j = L.n_s2 + (q - inst * L.n_oth);
-                    double sA, tA;
-                    fs_other_fiber(G, bs, L, st, inst, t * T + inst, j, e0, ka, N3, N1, N4, commit, sA, tA);
-                    double* f = fk + (size_t)inst * 2 * L.n_tot;
-                    f[2 * j] = sA;
-                    f[2 * j + 1] = tA;
-                }
-                __syncwarp();
-                if (lane == 0) fs_arrive(&bar_read[s]);
-            } else if (lane == 0) {
-                s_abort = 1;
+            ok = __all_sync(all, mbar_wait_bounded(&bar_full[s], par));
+            // fk of this stage is free once the sums of tile t - 2G have read it
+            if (ok && k >= 2) ok = __all_sync(all, mbar_wait_bounded(&bar_summed[s], par ^ 1u));
+            if (!ok) break;
+            if (threadIdx.x == 0) pend &= ~(1u << s);
+            for (int base = w * 32; base < n_items; base += 32 * T) {
+                const int q = base + lane;
+                const int inst = q < n_items ? fs_div(q, L.n_oth, L.inv_oth) : 0;
+                const double e0 = __shfl_sync(all, ek_here, 2 * inst), ka = __shfl_sync(all, ek_here, 2 * inst + 1);
+                if (q >= n_items || inst >= n_valid) continue;
+                const int j = L.n_s2 + (q - inst * L.n_oth);
+                double sA, tA;
+                fs_other_fiber(G, bs, L, st, inst, t * T + inst, j, e0, ka, N3, N1, N4, commit, sA, tA);
+                double* f = fk + (size_t)inst * 2 * L.n_tot;
+                f[2 * j] = sA;
+                f[2 * j + 1] = tA;
             }
-            // the instance warps' fibers of the tile are in fk (and the sums of tile t - G have
-            // read fk of the other stage)
-            asm volatile("bar.sync 1, %0;" ::"r"(32 * T) : "memory");
-            if (s_abort) break;
-            // one warp per tile forms the sums; the others go on to the next tile
+            __syncwarp();
+            if (lane == 0) {
+                fs_arrive(&bar_read[s]);
+                fs_arrive(&bar_inst[s]);
+            }
+            // one warp per tile forms the sums once every warp's results are in fk; the others go
+            // on to the next tile
             if (w == (k & (T - 1))) {
-                if (!L.steel_warps || __all_sync(all, mbar_wait_bounded(&bar_steel[s], par))) {
-                    fs_sums(G, sd, L, fk, lane, n_valid, resp + 5 * t * T);
-                    __syncwarp();
-                    if (lane == 0) fs_arrive(&bar_summed[s]);
-                } else if (lane == 0) {
-                    s_abort = 1;
-                }
+                ok = __all_sync(all, mbar_wait_bounded(&bar_inst[s], par));
+                if (ok && L.steel_warps) ok = __all_sync(all, mbar_wait_bounded(&bar_steel[s], par));
+                if (!ok) break;
+                fs_sums(G, sd, L, fk, lane, n_valid, resp + 5 * t * T);
+                __syncwarp();
+                if (lane == 0) fs_arrive(&bar_summed[s]);
             }
             // the loading lane refills stage s with tile t + 2G once every warp has read tile t
             if (threadIdx.x == 0 && t + 2 * G_ < n_tiles) {
@@ -379,13 +377,12 @@ __global__ void __launch_bounds__(32 * (kFsTile + kFsMaxSteelWarps), 2)
                     pend |= 1u << s;
                     pend_par = (pend_par & ~(1u << s)) | ((par ^ 1u) << s);
                 } else {
-                    s_abort = 1;
+                    ok = false;
                 }
             }
-            __syncwarp();
+            ok = __shfl_sync(all, ok ? 1 : 0, 0) != 0;
+            if (!ok) break;
         }
-        // a failure in the last tile (no later barrier to meet at) is seen here
-        ok = *reinterpret_cast<volatile int*>(&s_abort) == 0;
     } else {
         // ---- steel warp v: the Steel02 fibers of every instance of the tile
         const int v = warp - T;

@@ -959,6 +959,12 @@ __global__ void step_end_kernel(DevCtl* ctl, const int* __restrict__ status,
         el.next[1] = 0;
         el.hard_count[0] = 0;
         el.hard_count[1] = 0;
+        if (el.rq) {
+            el.rq_tail[0] = 0;
+            el.rq_tail[1] = 0;
+            el.fan_finished[0] = 0;
+            el.fan_finished[1] = 0;
+        }
         const bool stop = ctl->single && status[0] != 0;
         if (use_cond) cudaGraphSetConditional(outer, (step + 1 < ctl->n_end && !stop) ? 1 : 0);
     }
