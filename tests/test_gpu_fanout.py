@@ -2,8 +2,9 @@
 
 A forceBeamColumn2d element tries an increment with three schemes at up to four subdivision
 levels, each attempt from the accepted state (force_beam_column2d.mojo:1669-1763).  With
-fan_out the twelve attempts of an element whose last state determination needed a subdivision
-run on twelve CTAs and the first success in Strut's order is kept.  Frames 0, 21 and 37 of the
+fan_out the twelve attempts of every pass of an element whose last state determination needed
+a subdivision run on twelve CTAs (later passes through the launch's attempt queue) and the
+first success in Strut's order is kept.  Frames 0, 21 and 37 of the
 256-frame batch subdivide in their first 400 steps (the oracle counts 116, 153 and 121
 cut-back passes there), so their histories exercise the fan-out; they must be bit for bit those
 of the sequential order, with every element CTA size, and within 1e-7 of peak of the oracle's
