@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define STRUT_ABI_VERSION 6
+#define STRUT_ABI_VERSION 7
 #define STRUT_MAX_INT_PTS 10
 
 /* Status codes.  No entry point aborts the process. */
@@ -182,6 +182,29 @@ typedef struct StrutSolverAttempt {
     double tol;
 } StrutSolverAttempt;
 
+/* A section recorder entry (section_force / section_deformation recorders,
+ * transient_nonlinear.mojo:1631-1655, 3537-3605): integration point `section` (0-based) of
+ * element `element`.  Values per step (2D: 2, 3D: 4):
+ *   forceBeamColumn2d  force  q0, (xi - 1) q1 + xi q2          deformation  eps0, kappa
+ *                      (from the element's basic state after the step, helpers.mojo:1974-2040)
+ *   dispBeamColumn2d   force  N, Mz of the section at          deformation  eps0, kappa
+ *                      the displacements' deformation          (helpers.mojo:2043-2156)
+ *   forceBeamColumn3d  force  q0, (xi-1) q1 + xi q2,           deformation  eps0, kappa_z,
+ *                      (xi-1) q3 + xi q4, GJ twist                          kappa_y, twist
+ *                      (after the recorder's state determination at the step's displacements,
+ *                      helpers.mojo:2158-2300; the element is then also a recorded element)
+ *   dispBeamColumn3d   force  N, Mz, -My, GJ twist             deformation  eps0, kappa_z,
+ *                                                                           -kappa_y, twist
+ *                      (beam_column3d_nonlinear.mojo:578-640) */
+#define STRUT_SECTION_FORCE 0
+#define STRUT_SECTION_DEFORMATION 1
+typedef struct StrutSectionRecord {
+    int32_t element;
+    int32_t section;
+    int32_t kind;     /* STRUT_SECTION_FORCE or STRUT_SECTION_DEFORMATION */
+    int32_t reserved;
+} StrutSectionRecord;
+
 /* One analysis instance (one frame + one record). */
 typedef struct StrutModelDesc {
     int32_t ndm;                 /* 2 (ndf 3) or 3 (ndf 6)                               */
@@ -244,6 +267,10 @@ typedef struct StrutModelDesc {
     int32_t num_attempts;          /* 0 .. STRUT_MAX_ATTEMPTS                              */
     int32_t reserved_attempts;
     StrutSolverAttempt attempts[STRUT_MAX_ATTEMPTS];
+    /* section recorders: their values every step (strut_gpu_get_section_history) */
+    int32_t num_record_sections;
+    int32_t reserved_sections;
+    const StrutSectionRecord* record_sections;
 } StrutModelDesc;
 
 /* Per-run statistics (RuntimeProfileMetrics counters, solver/profile.mojo:37-74). */
@@ -306,6 +333,11 @@ int strut_gpu_get_history(StrutHandle* h, int32_t instance, double* disp, double
 /* Same for all instances at once, instance-major, each block sized as for one instance
  * with that instance's recorder counts; offsets are the prefix sums of those sizes. */
 int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int32_t* iters);
+/* Section recorder values of one instance for steps [0, steps_done): steps x
+ * num_record_sections x (2 for a 2D handle, 4 for a 3D one), in the order of the instance's
+ * record_sections (see StrutSectionRecord).  Replaces the section recorder branch of Strut's
+ * transient recorder loop (transient_nonlinear.mojo:3537-3605). */
+int strut_gpu_get_section_history(StrutHandle* h, int32_t instance, double* out);
 /* Status of every instance (STRUT_OK or the code it failed with), n_inst entries. */
 int strut_gpu_instance_status(const StrutHandle* h, int32_t* status);
 /* Current free displacement / velocity / acceleration vectors of one instance. */

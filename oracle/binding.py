@@ -65,6 +65,8 @@ def lib():
                                             C.POINTER(A.StrutFiber), C.c_int, _dp, C.c_int, _dp]
         L.oracle_element_state.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _dp]
         L.oracle_run_transient.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _ip, _ip]
+        L.oracle_run_transient_sections.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, _dp, _dp, _ip,
+                                                    _ip, _dp]
         L.oracle_state_determination.argtypes = [C.POINTER(A.StrutModelDesc), _dp, _dp, _dp, _ip]
         L.oracle_run_transient_batch.argtypes = [C.POINTER(A.StrutModelDesc), C.c_int, C.c_int,
                                                  C.c_int, _ip, _ip, _ip, _ip]
@@ -139,8 +141,9 @@ def section_batch_path(mats, nmat, fibs, nfib, eps0_kappa) -> np.ndarray:
     return out
 
 
-def run_transient(model, steps: int):
-    """(disp (steps, nrec), eforce (steps, nrece, 2*ndf), iters (steps,), rc, failed_step)"""
+def run_transient(model, steps: int, sections: bool = False):
+    """(disp (steps, nrec), eforce (steps, nrece, 2*ndf), iters (steps,), rc, failed_step), and
+    with sections the section recorders' values (steps, nsec, 2 in 2D / 4 in 3D) appended."""
     d = model.desc()
     nrec = d.num_record_dofs
     nrece = d.num_record_elements
@@ -148,9 +151,15 @@ def run_transient(model, steps: int):
     ef = np.zeros((steps, max(nrece, 1), 2 * model.ndf))
     iters = np.zeros(steps, dtype=np.int32)
     failed = C.c_int(-1)
-    rc = lib().oracle_run_transient(C.byref(d), steps, _d(disp), _d(ef),
-                                    iters.ctypes.data_as(_ip), C.byref(failed))
-    return disp[:, :nrec], ef[:, :nrece], iters, rc, failed.value
+    if not sections:
+        rc = lib().oracle_run_transient(C.byref(d), steps, _d(disp), _d(ef),
+                                        iters.ctypes.data_as(_ip), C.byref(failed))
+        return disp[:, :nrec], ef[:, :nrece], iters, rc, failed.value
+    nsec = d.num_record_sections
+    sec = np.zeros((steps, max(nsec, 1), 2 if model.ndf == 3 else 4))
+    rc = lib().oracle_run_transient_sections(C.byref(d), steps, _d(disp), _d(ef),
+                                             iters.ctypes.data_as(_ip), C.byref(failed), _d(sec))
+    return disp[:, :nrec], ef[:, :nrece], iters, rc, failed.value, sec[:, :nsec]
 
 
 def state_determination(model, u_free):

@@ -61,6 +61,10 @@ int oracle_section3d_path(const StrutUniMaterial* mats, int nmat, const StrutFib
  * 2*ndf values per recorded element and step. */
 int oracle_run_transient(const StrutModelDesc* m, int steps, double* disp_hist,
                          double* eforce_hist, int* iters_hist, int* failed_step);
+/* The same with the section recorders' values: steps x num_record_sections x (2 or 4). */
+int oracle_run_transient_sections(const StrutModelDesc* m, int steps, double* disp_hist,
+                                  double* eforce_hist, int* iters_hist, int* failed_step,
+                                  double* section_hist);
 /* One element state determination + assembly at u_free (parity entry). */
 int oracle_state_determination(const StrutModelDesc* m, const double* u_free,
                                double* f_int_free, double* band_out, int* half_bw);

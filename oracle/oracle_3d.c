@@ -340,6 +340,28 @@ static void u_to_local_dense(const double R[9], const double ug[12], double ul[1
     }
 }
 
+/* Section kinematics of a dispBeamColumn3d at integration point ip for the section recorders
+ * (beam_column3d_nonlinear.mojo:578-640): out = eps0, kappa_y, kappa_z, twist. */
+int oracle_dbc3d_section_kinematics(const OElement* e, const double ug[12], int ip, double out[4]) {
+    double dx = e->x2[0] - e->x1[0], dy = e->x2[1] - e->x1[1], dz = e->x2[2] - e->x1[2];
+    double L = sqrt(dx * dx + dy * dy + dz * dz);
+    if (L == 0.0) return STRUT_BAD_ARG;
+    double R[9];
+    int rc = element_rotation(e, ug, R);
+    if (rc != STRUT_OK) return rc;
+    double ul[12];
+    u_to_local_dense(R, ug, ul);
+    double xi = e->xi[ip];
+    double inv_L = 1.0 / L;
+    out[0] = (-inv_L) * ul[0] + inv_L * ul[6];
+    out[1] = ((-6.0 + 12.0 * xi) / (L * L)) * ul[2] + ((4.0 - 6.0 * xi) / L) * ul[4] +
+             ((6.0 - 12.0 * xi) / (L * L)) * ul[8] + ((2.0 - 6.0 * xi) / L) * ul[10];
+    out[2] = ((-6.0 + 12.0 * xi) / (L * L)) * ul[1] + ((-4.0 + 6.0 * xi) / L) * ul[5] +
+             ((6.0 - 12.0 * xi) / (L * L)) * ul[7] + ((-2.0 + 6.0 * xi) / L) * ul[11];
+    out[3] = (ul[9] - ul[3]) / L;
+    return STRUT_OK;
+}
+
 /* ---- dispBeamColumn3d (beam_column3d_nonlinear.mojo:357-575) ---------------------------- */
 
 int oracle_dbc3d(OElement* e, const double ug[12], double k[144], double f[12]) {

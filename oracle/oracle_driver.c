@@ -58,6 +58,7 @@ typedef struct OModel {
     int* kcol;
     double* kval;
     int* epos;         /* num_elements x nd x nd */
+    double* sec_hist;  /* section recorder values, steps x num_record_sections x (2 or 4), or NULL */
     int* epos_sh;      /* num_shells x 24 x 24 */
     double* shell_k;   /* num_shells x 576, constant */
     int* efree_sh;     /* num_shells x 24 */
@@ -873,6 +874,103 @@ static int initial_assembly(OModel* m) {
 
 static double simd_sumsq(const double* x, int n) { return oracle_simd_dot(x, x, n); }
 
+/* Section recorders after the step (transient_nonlinear.mojo:3537-3605).  forceBeamColumn2d:
+ * from the basic state the step left (helpers.mojo:1974-2040); dispBeamColumn2d: the section at
+ * the deformation of the step's displacements (2043-2156); forceBeamColumn3d: from the basic
+ * state of the recorder's state determination, which the element-force pass ran since such an
+ * element is also recorded (2158-2300); dispBeamColumn3d: beam_column3d_nonlinear.mojo:578-640.
+ * Evaluating a section sets its trial state from the committed one only. */
+static int record_sections(OModel* m, int step) {
+    const StrutModelDesc* d = m->d;
+    if (!m->sec_hist || d->num_record_sections <= 0) return STRUT_OK;
+    const int W = m->nd == 6 ? 2 : 4;
+    for (int k = 0; k < d->num_record_sections; ++k) {
+        const StrutSectionRecord* sr = &d->record_sections[k];
+        OElement* el = &m->elems[sr->element];
+        const int ip = sr->section;
+        const int defo = sr->kind == STRUT_SECTION_DEFORMATION;
+        const double xi = el->xi[ip];
+        double* out = m->sec_hist + ((size_t)step * d->num_record_sections + k) * W;
+        double ug[12];
+        for (int a = 0; a < m->nd; ++a) ug[a] = m->u[el->desc->dof[a]];
+        switch (el->desc->type) {
+        case STRUT_ELEM_FORCE_BEAM_COLUMN_2D:
+            if (defo) {
+                out[0] = el->eps0[ip];
+                out[1] = el->kappa[ip];
+            } else {
+                out[0] = el->q[0] + 0.0;
+                out[1] = (xi - 1.0) * el->q[1] + xi * el->q[2] + 0.0;
+            }
+            break;
+        case STRUT_ELEM_DISP_BEAM_COLUMN_2D: {
+            const double c = el->c_div, s = el->s_div, L = el->L, inv_L = 1.0 / L;
+            double ul[6];
+            ul[0] = c * ug[0] + s * ug[1];
+            ul[1] = -s * ug[0] + c * ug[1];
+            ul[2] = ug[2];
+            ul[3] = c * ug[3] + s * ug[4];
+            ul[4] = -s * ug[3] + c * ug[4];
+            ul[5] = ug[5];
+            const double eps0 = (-inv_L) * ul[0] + inv_L * ul[3];
+            const double kappa = ((-6.0 + 12.0 * xi) / (L * L)) * ul[1] + ((-4.0 + 6.0 * xi) / L) * ul[2] +
+                                 ((6.0 - 12.0 * xi) / (L * L)) * ul[4] + ((-2.0 + 6.0 * xi) / L) * ul[5];
+            if (defo) {
+                out[0] = eps0;
+                out[1] = kappa;
+            } else {
+                double r[5];
+                oracle_section_response(el->sec, &el->sst[ip], eps0, kappa, r);
+                out[0] = r[0] + 0.0;
+                out[1] = r[1] + 0.0;
+            }
+            break;
+        }
+        case STRUT_ELEM_FORCE_BEAM_COLUMN_3D: {
+            const double dx = el->x2[0] - el->x1[0], dy = el->x2[1] - el->x1[1], dz = el->x2[2] - el->x1[2];
+            const double L = sqrt(dx * dx + dy * dy + dz * dz);
+            const double rot_i = (dx * ug[3] + dy * ug[4] + dz * ug[5]) / L;
+            const double rot_j = (dx * ug[9] + dy * ug[10] + dz * ug[11]) / L;
+            const double twist = (rot_j - rot_i) / L;
+            if (defo) {
+                out[0] = el->eps0[ip];
+                out[1] = el->kz[ip];
+                out[2] = el->ky[ip];
+                out[3] = twist;
+            } else {
+                out[0] = el->q5[0] + 0.0;
+                out[1] = (xi - 1.0) * el->q5[1] + xi * el->q5[2] + 0.0;
+                out[2] = (xi - 1.0) * el->q5[3] + xi * el->q5[4] + 0.0;
+                out[3] = el->G * el->J * twist;
+            }
+            break;
+        }
+        case STRUT_ELEM_DISP_BEAM_COLUMN_3D: {
+            double kin[4];
+            int rc = oracle_dbc3d_section_kinematics(el, ug, ip, kin);
+            if (rc != STRUT_OK) return rc;
+            if (defo) {
+                out[0] = kin[0];
+                out[1] = kin[2];
+                out[2] = -kin[1];
+                out[3] = kin[3];
+            } else {
+                double r[9];
+                oracle_section3d_response(el->sec3, &el->sst[ip], kin[0], kin[1], kin[2], r);
+                out[0] = r[0];
+                out[1] = r[2];
+                out[2] = -r[1];
+                out[3] = el->G * el->J * kin[3];
+            }
+            break;
+        }
+        default:
+            return STRUT_UNSUPPORTED;
+        }
+    }
+    return STRUT_OK;
+}
+
 /* Recorders after the step's commit (transient_nonlinear.mojo:3225-3300): node displacements,
  * and element forces computed once per element and step.  A 3D beam-column's force comes from
  * a full element state determination at the converged displacements
@@ -909,7 +1007,7 @@ static int record_step(OModel* m, int step, double* disp_hist, double* eforce_hi
         }
         if (out) memcpy(out, f, sizeof(double) * nd);
     }
-    return STRUT_OK;
+    return record_sections(m, step);
 }
 
 /* The step's solver chain (transient_nonlinear.mojo:758-830): the attempts as given, or the
@@ -1178,8 +1276,15 @@ static int run_steps_chain(OModel* m, int steps, double* disp_hist, double* efor
 
 int oracle_run_transient(const StrutModelDesc* d, int steps, double* disp_hist,
                          double* eforce_hist, int* iters_hist, int* failed_step) {
+    return oracle_run_transient_sections(d, steps, disp_hist, eforce_hist, iters_hist, failed_step, 0);
+}
+
+int oracle_run_transient_sections(const StrutModelDesc* d, int steps, double* disp_hist,
+                                  double* eforce_hist, int* iters_hist, int* failed_step,
+                                  double* section_hist) {
     OModel m;
     int rc = model_build(&m, d);
+    m.sec_hist = section_hist;
     if (rc == STRUT_OK) rc = initial_assembly(&m);
     if (rc == STRUT_OK) rc = run_steps(&m, steps, disp_hist, eforce_hist, iters_hist, failed_step);
     model_free(&m);

@@ -108,5 +108,6 @@ int oracle_rotation3d(const double x1[3], const double x2[3], int has_vecxz, con
                       double R[9]);
 int oracle_fbc3d(OElement* e, const double u_global[12], double k[144], double f[12]);
 int oracle_dbc3d(OElement* e, const double u_global[12], double k[144], double f[12]);
+int oracle_dbc3d_section_kinematics(const OElement* e, const double u_global[12], int ip, double out[4]);
 
 #endif

@@ -145,6 +145,14 @@ class StrutSolverAttempt(C.Structure):
     ]
 
 
+SECTION_FORCE = 0
+SECTION_DEFORMATION = 1
+
+
+class StrutSectionRecord(C.Structure):
+    _fields_ = [("element", C.c_int32), ("section", C.c_int32), ("kind", C.c_int32), ("reserved", C.c_int32)]
+
+
 class StrutModelDesc(C.Structure):
     _fields_ = [
         ("ndm", C.c_int32),
@@ -196,6 +204,9 @@ class StrutModelDesc(C.Structure):
         ("num_attempts", C.c_int32),
         ("reserved_attempts", C.c_int32),
         ("attempts", StrutSolverAttempt * MAX_ATTEMPTS),
+        ("num_record_sections", C.c_int32),
+        ("reserved_sections", C.c_int32),
+        ("record_sections", C.POINTER(StrutSectionRecord)),
     ]
 
 
@@ -244,6 +255,7 @@ PROF_ELEMENT_CRITICAL = 5
 # the test that checks the built library exports all of them.
 EXPORTS = {
     "strut_gpu_abi_version": (C.c_int, []),
+    "strut_gpu_get_section_history": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "strut_gpu_last_error": (C.c_char_p, []),
     "strut_gpu_create": (
         C.c_int,

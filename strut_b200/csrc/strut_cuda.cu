@@ -31,6 +31,7 @@
 #include "largeband_kernels.cuh"
 #include "shell_kernels.cuh"
 #include "predictor_kernels.cuh"
+#include "section_record_kernels.cuh"
 
 using namespace strut;
 
@@ -289,6 +290,11 @@ struct StrutHandle {
     int ndf_all = 3;                 // ndf shared by every instance, -1 when mixed
     int* d_rec3 = nullptr;           // recorded 3D elements (record pass after commit)
     int n_rec3 = 0;
+    // section recorders: one slot per (instance, record), instance-major
+    SecRec* d_secrec = nullptr;
+    int n_sec_slots = 0;
+    std::vector<int> sec_off, sec_n;
+    double* d_hist_sec = nullptr;
     long long ek_total = 0, ef_total = 0;
     std::vector<DevShell> shells_h;  // linear shells of all instances
     DevShell* d_shells = nullptr;
@@ -348,7 +354,7 @@ struct StrutHandle {
     int* d_fail_step = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    const void* graph_keys[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    const void* graph_keys[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     double* d_rhs = nullptr;
     std::vector<long long> elem_fibers;  // fibers per element (all families)
     // node table of the learned predictor: nodes with a free dof, instance order then node order
@@ -369,6 +375,7 @@ struct StrutHandle {
         if (d_hist_disp) cudaFree(d_hist_disp);
         if (d_hist_ef) cudaFree(d_hist_ef);
         if (d_hist_iters) cudaFree(d_hist_iters);
+        if (d_hist_sec) cudaFree(d_hist_sec);
         if (d_ag) cudaFree(d_ag);
         if (h_ctrl) cudaFreeHost(h_ctrl);
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -556,6 +563,9 @@ static int ensure_history(StrutHandle* h, int need) {
     double* nd = nullptr;
     double* ne = nullptr;
     int* ni = nullptr;
+    double* ns = nullptr;
+    const int sw = h->ndf_all == 6 ? 4 : 2;
+    CK(cudaMalloc((void**)&ns, (size_t)cap * std::max(h->n_sec_slots, 1) * sw * sizeof(double)));
     CK(cudaMalloc((void**)&nd, (size_t)cap * std::max(h->n_rec_total, 1) * sizeof(double)));
     CK(cudaMalloc((void**)&ne, (size_t)cap * std::max(h->n_rece_slots, 1) * h->ef_w * sizeof(double)));
     CK(cudaMalloc((void**)&ni, (size_t)cap * h->n_inst * sizeof(int)));
@@ -567,7 +577,11 @@ static int ensure_history(StrutHandle* h, int need) {
                       cudaMemcpyDeviceToDevice));
         CK(cudaMemcpy(ni, h->d_hist_iters, (size_t)h->steps_done * h->n_inst * sizeof(int),
                       cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(ns, h->d_hist_sec, (size_t)h->steps_done * std::max(h->n_sec_slots, 1) * sw * sizeof(double),
+                      cudaMemcpyDeviceToDevice));
     }
+    if (h->d_hist_sec) cudaFree(h->d_hist_sec);
+    h->d_hist_sec = ns;
     if (h->d_hist_disp) cudaFree(h->d_hist_disp);
     if (h->d_hist_ef) cudaFree(h->d_hist_ef);
     if (h->d_hist_iters) cudaFree(h->d_hist_iters);
@@ -710,6 +724,14 @@ static int build_graph(StrutHandle* h) {
                             h->d_hist_disp, (const DevCtl*)h->d_ctl));
         last = n_rec;
     }
+    if (h->n_sec_slots > 0) {
+        cudaGraphNode_t n_sec;
+        TRY(add_kernel_node(&n_sec, body, &last, 1, record_sections_kernel, dim3((h->n_sec_slots * 32 + 255) / 256),
+                            dim3(256), 0, (const DevElem*)h->d_elems, h->geo, h->fs, (const double*)h->A.u_full,
+                            (const double*)h->d_estate, (const SecRec*)h->d_secrec, h->n_sec_slots,
+                            h->ndf_all == 6 ? 4 : 2, h->d_hist_sec, (const DevCtl*)h->d_ctl));
+        last = n_sec;
+    }
     TRY(add_kernel_node(&n_end, body, &last, 1, step_end_kernel, dim3(1), dim3(256), 0, h->d_ctl,
                         (const int*)h->A.status, h->d_fail_step, h->n_inst, h->A.nactive, h->A.el, outer, 1));
     CK(cudaGraphInstantiate(&h->gexec, g, 0));
@@ -717,6 +739,7 @@ static int build_graph(StrutHandle* h) {
     h->graph_keys[1] = h->d_hist_ef;
     h->graph_keys[2] = h->d_hist_iters;
     h->graph_keys[3] = h->d_ag;
+    h->graph_keys[5] = h->d_hist_sec;
     h->graph_keys[4] = h->pred;
     h->graph_tune_gen = h->tune_gen;
     return STRUT_OK;
@@ -724,7 +747,8 @@ static int build_graph(StrutHandle* h) {
 
 static int ensure_graph(StrutHandle* h) {
     if (h->gexec && h->graph_tune_gen == h->tune_gen && h->graph_keys[0] == h->d_hist_disp && h->graph_keys[1] == h->d_hist_ef &&
-        h->graph_keys[2] == h->d_hist_iters && h->graph_keys[3] == h->d_ag && h->graph_keys[4] == h->pred)
+        h->graph_keys[2] == h->d_hist_iters && h->graph_keys[3] == h->d_ag && h->graph_keys[4] == h->pred &&
+        h->graph_keys[5] == h->d_hist_sec)
         return STRUT_OK;
     return build_graph(h);
 }
@@ -1345,6 +1369,35 @@ int strut_gpu_create(const StrutModelDesc* models, int32_t num_instances, int32_
         h->n_rec3 = (int)rec3.size();
         if ((rc = upload(&h->d_rec3, rec3, al))) return bail(rc);
     }
+    {
+        // section recorders
+        std::vector<SecRec> secs;
+        h->sec_off.assign(num_instances, 0);
+        h->sec_n.assign(num_instances, 0);
+        for (int i = 0; i < num_instances; ++i) {
+            const StrutModelDesc& d = models[i];
+            h->sec_off[i] = (int)secs.size();
+            h->sec_n[i] = std::max(d.num_record_sections, 0);
+            if (d.num_record_sections > 0 && !d.record_sections)
+                return bail(fail(STRUT_BAD_ARG, "record_sections is NULL"));
+            for (int k = 0; k < d.num_record_sections; ++k) {
+                const StrutSectionRecord& sr = d.record_sections[k];
+                if (sr.element < 0 || sr.element >= d.num_elements)
+                    return bail(fail(STRUT_BAD_ARG, "section recorder element out of range"));
+                const int ge = h->insts[i].elem_off + sr.element;
+                if (sr.section < 0 || sr.section >= elems[ge].nip)
+                    return bail(fail(STRUT_BAD_ARG, "section recorder section index out of range"));
+                if (sr.kind != STRUT_SECTION_FORCE && sr.kind != STRUT_SECTION_DEFORMATION)
+                    return bail(fail(STRUT_BAD_ARG, "section recorder kind must be force or deformation"));
+                if (elems[ge].type == STRUT_ELEM_FORCE_BEAM_COLUMN_3D && elems[ge].rec < 0)
+                    return bail(fail(STRUT_BAD_ARG, "a forceBeamColumn3d section recorder needs its element "
+                                                    "recorded too (Strut's recorder re-runs its state determination)"));
+                secs.push_back(SecRec{ge, sr.section, sr.kind, i});
+            }
+        }
+        h->n_sec_slots = (int)secs.size();
+        if (h->n_sec_slots > 0 && (rc = upload(&h->d_secrec, secs, al))) return bail(rc);
+    }
     h->geo.y = d_y;
     h->geo.z = d_z;
     h->geo.a = d_a;
@@ -1710,6 +1763,12 @@ int strut_gpu_run_steps(StrutHandle* h, int32_t n_steps, StrutStepStats* stats) 
                     h->A.u_full, h->d_rec_dof, h->n_rec_total, h->d_hist_disp, h->d_ctl);
                 CK(cudaGetLastError());
             }
+            if (h->n_sec_slots > 0) {
+                record_sections_kernel<<<(h->n_sec_slots * 32 + 255) / 256, 256, 0, h->stream>>>(
+                    h->d_elems, h->geo, h->fs, h->A.u_full, h->d_estate, h->d_secrec, h->n_sec_slots,
+                    h->ndf_all == 6 ? 4 : 2, h->d_hist_sec, h->d_ctl);
+                CK(cudaGetLastError());
+            }
             step_end_kernel<<<1, 256, 0, h->stream>>>(h->d_ctl, h->A.status, h->d_fail_step, h->n_inst,
                                                       h->A.nactive, h->A.el, none, 0);
             CK(cudaGetLastError());
@@ -1854,6 +1913,21 @@ int strut_gpu_get_history_all(StrutHandle* h, double* disp, double* eforce, int3
         for (int i = 0; i < h->n_inst; ++i)
             for (int s = 0; s < S; ++s) iters[o++] = all[(size_t)s * h->n_inst + i];
     }
+    return STRUT_OK;
+}
+
+int strut_gpu_get_section_history(StrutHandle* h, int32_t instance, double* out) {
+    if (!h || instance < 0 || instance >= h->n_inst) return fail(STRUT_BAD_ARG, "bad arguments");
+    const int S = h->steps_done, n = h->sec_n[instance];
+    if (S == 0 || n == 0) return STRUT_OK;
+    if (!out) return fail(STRUT_BAD_ARG, "bad arguments");
+    const int W = h->ndf_all == 6 ? 4 : 2;
+    std::vector<double> all((size_t)S * h->n_sec_slots * W);
+    CK(cudaMemcpy(all.data(), h->d_hist_sec, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < S; ++s)
+        for (int k = 0; k < n; ++k)
+            for (int c = 0; c < W; ++c)
+                out[((size_t)s * n + k) * W + c] = all[((size_t)s * h->n_sec_slots + h->sec_off[instance] + k) * W + c];
     return STRUT_OK;
 }
 

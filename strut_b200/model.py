@@ -599,6 +599,15 @@ class Model:
                 raise ModelError(f"{what}: dof {d} out of range 1..{self.ndf}")
             return d - 1
 
+        sec_recs, sec_col = [], {}
+
+        def scol(e, ip, kind):
+            key = (e, ip, kind)
+            if key not in sec_col:
+                sec_col[key] = len(sec_recs)
+                sec_recs.append(key)
+            return sec_col[key]
+
         self.recorder_plan = []
         for r in case.get("recorders", []) or []:
             t = r["type"]
@@ -627,10 +636,34 @@ class Model:
                 self.recorder_plan.append({"type": t, "file": f"{out}_i{i_node}_j{j_node}.out",
                                            "i_col": dcol(ii * self.ndf + d), "j_col": dcol(jj * self.ndf + d),
                                            "dx": float(dx)})
+            elif t in ("section_force", "section_deformation"):
+                # one file per element and section (transient_nonlinear.mojo:1631-1655)
+                kind = A.SECTION_FORCE if t == "section_force" else A.SECTION_DEFORMATION
+                for eid in r["elements"]:
+                    if int(eid) not in self.elem_index:
+                        raise ModelError(f"{t}: element {eid} not found")
+                    ei = self.elem_index[int(eid)]
+                    el = self.elements[ei]
+                    nip = int(self.integrations[el.integration].num_int_pts)
+                    for sec_no in r["sections"]:
+                        if int(sec_no) < 1 or int(sec_no) > nip:
+                            raise ModelError("section recorder section index out of range")
+                        if int(el.type) == A.ELEM_FORCE_BEAM_COLUMN_3D:
+                            # Strut's recorder re-runs this element's state determination at
+                            # the step's displacements (helpers.mojo:2223-2246): the element is
+                            # recorded, whose record pass does exactly that
+                            ecol(ei)
+                        c = scol(ei, int(sec_no) - 1, kind)
+                        self.recorder_plan.append({"type": t, "file": f"{out}_ele{int(eid)}_sec{int(sec_no)}.out",
+                                                   "sec_col": c})
             else:
                 raise ModelError(f"recorder type {t!r} is not on this path")
         self.record_dofs = np.asarray(rec_dofs, dtype=np.int32)
         self.record_elements = np.asarray(rec_elems, dtype=np.int32)
+        self.record_sections = (A.StrutSectionRecord * max(len(sec_recs), 1))()
+        for k, (e, ip, kind) in enumerate(sec_recs):
+            self.record_sections[k] = A.StrutSectionRecord(e, ip, kind, 0)
+        self.num_record_sections = len(sec_recs)
 
     def _mp_constraints(self, mpcs, case, constrained):
         """{slave dof: [(retained dof, coefficient), ...]} in constraint order."""
@@ -763,6 +796,8 @@ class Model:
         d.record_dofs = iptr(self.record_dofs)
         d.num_record_elements = len(self.record_elements)
         d.record_elements = iptr(self.record_elements)
+        d.num_record_sections = self.num_record_sections
+        d.record_sections = C.cast(self.record_sections, C.POINTER(A.StrutSectionRecord))
         sl = sorted(self.slaves)
         d.num_slaves = len(sl)
         ptr, mdof, coef = [0], [], []

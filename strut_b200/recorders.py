@@ -9,6 +9,10 @@ device returns (`Analysis.history`: displacements at `Model.record_dofs`, global
 * element_force            `<output>_ele<id>.out`, one row per step: the 2 ndf global end forces
 * drift                    `<output>_i<i>_j<j>.out`, one value per step: (u_j - u_i) / dx, dx the
                            coordinate difference along perp_dirn (helpers.mojo:3113-3142)
+* section_force / section_deformation
+                           `<output>_ele<id>_sec<n>.out`, one row per step: the section's
+                           resultants or deformations (StrutSectionRecord gives their order;
+                           transient_nonlinear.mojo:1631-1655, 3537-3605)
 * envelope_node_displacement / envelope_element_force
                            three rows after the last step: component-wise minima, maxima and
                            absolute maxima, the first step's values as the start
@@ -30,9 +34,10 @@ def format_values_line(values) -> str:
     return " ".join(repr(float(v)) for v in values) + "\n"
 
 
-def recorder_outputs(model, disp: np.ndarray, eforce: np.ndarray) -> dict:
+def recorder_outputs(model, disp: np.ndarray, eforce: np.ndarray, sections=None) -> dict:
     """{file name: text} for the recorders of `model`; disp is steps x len(record_dofs), eforce
-    steps x len(record_elements) x (2 ndf)."""
+    steps x len(record_elements) x (2 ndf), sections steps x model.num_record_sections x width
+    (needed only when the model has section recorders)."""
     disp = np.asarray(disp, dtype=np.float64)
     eforce = np.asarray(eforce, dtype=np.float64)
     steps = disp.shape[0] if disp.ndim == 2 else eforce.shape[0]
@@ -53,6 +58,8 @@ def recorder_outputs(model, disp: np.ndarray, eforce: np.ndarray) -> dict:
                 values = disp[k, rec["disp_cols"]]
             elif t in ("element_force", "envelope_element_force"):
                 values = eforce[k, rec["elem_col"], :]
+            elif t in ("section_force", "section_deformation"):
+                values = np.asarray(sections)[k, rec["sec_col"], :]
             else:  # drift
                 values = np.array([(disp[k, rec["j_col"]] - disp[k, rec["i_col"]]) / rec["dx"]])
             if t.startswith("envelope_"):
@@ -70,12 +77,12 @@ def recorder_outputs(model, disp: np.ndarray, eforce: np.ndarray) -> dict:
     return {name: "".join(parts[name]) for name in order}
 
 
-def write_outputs(model, disp, eforce, outdir) -> list:
+def write_outputs(model, disp, eforce, outdir, sections=None) -> list:
     """Writes the recorder files into outdir; returns their paths."""
     outdir = Path(outdir)
     outdir.mkdir(parents=True, exist_ok=True)
     paths = []
-    for name, text in recorder_outputs(model, disp, eforce).items():
+    for name, text in recorder_outputs(model, disp, eforce, sections).items():
         p = outdir / name
         p.parent.mkdir(parents=True, exist_ok=True)
         p.write_text(text)

@@ -121,6 +121,15 @@ class Analysis:
         )
         return disp[:, : len(m.record_dofs)], ef[:, : len(m.record_elements)], it
 
+    def section_history(self, instance: int = 0) -> np.ndarray:
+        """Section recorder values of one instance: steps x num_record_sections x (2 in 2D, 4
+        in 3D)."""
+        m = self.models[instance]
+        w = 2 if m.ndf == 3 else 4
+        out = np.zeros((self.steps_done, max(m.num_record_sections, 1), w))
+        _check(lib().strut_gpu_get_section_history(self.h, instance, _d(out)), "strut_gpu_get_section_history")
+        return out[:, : m.num_record_sections]
+
     def history_all(self):
         S = self.steps_done
         nd = sum(len(m.record_dofs) for m in self.models)

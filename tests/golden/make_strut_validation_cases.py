@@ -8,8 +8,8 @@ FiberSection3d patches, element type, geomTransf, integration); the conversion r
 analysis block and its point load by: a lumped mass on the free node's translations, 5 % mass-
 proportional damping, a seeded Kanai-Tajimi ground motion along the point load's direction
 (PGA 0.5 g, dt 0.01 s, 300 steps) and Newton with NormDispIncr 1e-8 on BandGeneral.  Recorders
-that this path records (node displacement, element force) are kept; the section force /
-deformation recorders of the 3D files are dropped.
+that this path records (node displacement, element force, section force and deformation) are
+kept.
 
     python tests/golden/make_strut_validation_cases.py [/path/to/reference]
 """
@@ -46,7 +46,8 @@ def convert(case: dict, seed: int) -> dict:
                        "integrator": {"type": "Newmark", "gamma": 0.5, "beta": 0.25},
                        "algorithm": "Newton", "test_type": "NormDispIncr", "tol": 1.0e-8, "max_iters": 20,
                        "system": "BandGeneral"}
-    out["recorders"] = [r for r in case.get("recorders", []) if r["type"] in ("node_displacement", "element_force")]
+    out["recorders"] = [r for r in case.get("recorders", [])
+                        if r["type"] in ("node_displacement", "element_force", "section_force", "section_deformation")]
     return out
 
 

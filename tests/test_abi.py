@@ -29,7 +29,7 @@ def test_library_exports_every_header_symbol(gpu_lib):
 
 def test_abi_version_and_error_text_without_gpu(gpu_lib):
     lib = gpu_lib.lib()
-    assert lib.strut_gpu_abi_version() == 6
+    assert lib.strut_gpu_abi_version() == 7
     assert isinstance(lib.strut_gpu_last_error(), bytes)
 
 
@@ -41,7 +41,7 @@ def test_struct_sizes_match_c_layout(tmp_path):
 
     names = ["StrutUniMaterial", "StrutFiber", "StrutBeamIntegration", "StrutFrameElement",
              "StrutFiberSection", "StrutExcitation", "StrutModelDesc", "StrutStepStats",
-             "StrutTuning", "StrutSolverAttempt"]
+             "StrutTuning", "StrutSolverAttempt", "StrutSectionRecord"]
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
