@@ -47,9 +47,7 @@ def use_fma(on: bool):
 def lib():
     global _lib
     if _lib is None:
-        path = LIB_PATH_FMA if _fma else LIB_PATH
-        if not path.exists():
-            build(fma=_fma)
+        path = build(fma=_fma)  # rebuilt when a source is newer than the library
         L = C.CDLL(str(path))
         L.oracle_set_simd_width.argtypes = [C.c_int]
         L.oracle_subdivisions.restype = C.c_long

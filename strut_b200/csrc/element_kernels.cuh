@@ -160,42 +160,63 @@ __device__ __forceinline__ void load_s2(const StageView& sv, int idx, S2State& c
 
 // Derived constants of every Concrete02 / Steel02 fiber of the staged element, computed once
 // per launch by the whole CTA (the committed state does not change inside a launch).  A
-// Concrete02 fiber's dept comes from global memory (c2_dept: the element's dept field).
+// Concrete02 fiber's dept comes from global memory (c2_dept: the element's dept field).  The two
+// branch curves of a Steel02 fiber (each with its own pow) are two work items, given to the last
+// threads of the CTA, so they run beside the Concrete02 items instead of after them.
+__device__ __forceinline__ void derive_c2(const Geo& g, const DevSection& sd, const StageView& sv,
+                                          const double* __restrict__ c2_dept, double* c2d, int idx) {
+    C2State c;
+    load_c2(sv, idx, c);
+    c.dept = __ldg(c2_dept + idx);
+    const int j = idx % sd.n_c2;
+    C2Derived d;
+    concrete02_derive(g.mats[__ldg(g.m + sd.geo_off + sd.n_s2 + j)], c, d);
+    const int B = sv.c2_blk;
+    c2d[0 * B + idx] = d.sigmm;
+    c2d[1 * B + idx] = d.er;
+    c2d[2 * B + idx] = d.ept;
+    c2d[3 * B + idx] = d.epn;
+    c2d[4 * B + idx] = d.etn;
+}
+
+// Branch curve k (0: strain increasing, 1: decreasing) of Steel02 fiber idx (steel02_derive).
+__device__ __forceinline__ void derive_s2(const Geo& g, const DevSection& sd, const StageView& sv, double* s2d,
+                                          int idx, int k) {
+    S2State c;
+    load_s2(sv, idx, c);
+    const int j = idx % sd.n_s2;
+    const DevMat& m = g.mats[__ldg(g.m + sd.geo_off + j)];
+    S2State t;
+    steel02_branch(m, c, k == 0, t);
+    S2Curve cv;
+    steel02_curve_of(m, t, cv);
+    const int B = sv.s2_blk;
+    s2d[(6 * k + 0) * B + idx] = cv.epsr;
+    s2d[(6 * k + 1) * B + idx] = cv.sigr;
+    s2d[(6 * k + 2) * B + idx] = cv.denom;
+    s2d[(6 * k + 3) * B + idx] = cv.dsig;
+    s2d[(6 * k + 4) * B + idx] = cv.R;
+    s2d[(6 * k + 5) * B + idx] = cv.invR;
+}
+
 __device__ __forceinline__ void derive_element(const Geo& g, const DevSection& sd, const DevElem& E,
                                                const StageView& sv, const double* __restrict__ c2_dept,
                                                double* c2d, double* s2d) {
-    const int nc = E.nip * sd.n_c2, ns = E.nip * sd.n_s2;
-    for (int idx = threadIdx.x; idx < nc; idx += blockDim.x) {
-        C2State c;
-        load_c2(sv, idx, c);
-        c.dept = __ldg(c2_dept + idx);
-        const int j = idx % sd.n_c2;
-        C2Derived d;
-        concrete02_derive(g.mats[__ldg(g.m + sd.geo_off + sd.n_s2 + j)], c, d);
-        const int B = sv.c2_blk;
-        c2d[0 * B + idx] = d.sigmm;
-        c2d[1 * B + idx] = d.er;
-        c2d[2 * B + idx] = d.ept;
-        c2d[3 * B + idx] = d.epn;
-        c2d[4 * B + idx] = d.etn;
-    }
-    for (int idx = threadIdx.x; idx < ns; idx += blockDim.x) {
-        S2State c;
-        load_s2(sv, idx, c);
-        const int j = idx % sd.n_s2;
-        S2Derived d;
-        steel02_derive(g.mats[__ldg(g.m + sd.geo_off + j)], c, d);
-        const int B = sv.s2_blk;
-        const S2Curve* cv[2] = {&d.up, &d.dn};
-        for (int k = 0; k < 2; ++k) {
-            s2d[(6 * k + 0) * B + idx] = cv[k]->epsr;
-            s2d[(6 * k + 1) * B + idx] = cv[k]->sigr;
-            s2d[(6 * k + 2) * B + idx] = cv[k]->denom;
-            s2d[(6 * k + 3) * B + idx] = cv[k]->dsig;
-            s2d[(6 * k + 4) * B + idx] = cv[k]->R;
-            s2d[(6 * k + 5) * B + idx] = cv[k]->invR;
+    const int nc = E.nip * sd.n_c2, ns2 = 2 * E.nip * sd.n_s2;
+    const int nt = blockDim.x, tid = threadIdx.x;
+    if (ns2 > 0 && ns2 <= nt / 2) {
+        // Concrete02 on the first nt - ns2 threads, one Steel02 branch on each of the others
+        const int split = nt - ns2;
+        if (tid < split) {
+            for (int idx = tid; idx < nc; idx += split) derive_c2(g, sd, sv, c2_dept, c2d, idx);
+        } else {
+            const int q = tid - split;
+            derive_s2(g, sd, sv, s2d, q >> 1, q & 1);
         }
+        return;
     }
+    for (int idx = tid; idx < nc; idx += nt) derive_c2(g, sd, sv, c2_dept, c2d, idx);
+    for (int q = tid; q < ns2; q += nt) derive_s2(g, sd, sv, s2d, q >> 1, q & 1);
 }
 
 __device__ __forceinline__ void acc_fiber(double* a, double fs, double ks, double y) {
@@ -1002,12 +1023,13 @@ __device__ __forceinline__ void copy_struct(T* dst, const T* src) {
     for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) d[i] = s[i];
 }
 
-// Stages the element's committed fiber history into shared memory.  bar was initialised once
-// for the CTA; phase is the parity of its next completion (every thread tracks the same value).
-// Returns false (and sets *err) if the bulk copy did not complete within the bounded wait.
-__device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState& fs,
-                                              double* sm, uint64_t* bar, uint32_t& phase,
-                                              StageView& sv, int* err) {
+// Stages the element's committed fiber history into shared memory: stage_issue (the views, and
+// thread 0's bulk copies) then stage_wait; stage_element does both.  bar was initialised once for
+// the CTA; phase is the parity of its next completion (every thread tracks the same value).
+// stage_wait returns false (and sets *err) if the bulk copy did not complete within the bounded
+// wait.
+__device__ __forceinline__ uint32_t stage_issue(const DevElem& E, const FiberState& fs, double* sm,
+                                                uint64_t* bar, StageView& sv) {
     double* c2 = sm;
     double* s2 = c2 + 4 * E.c2_blk;
     double* s1 = s2 + 10 * E.s2_blk;
@@ -1027,7 +1049,7 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
     sv.c1_blk = E.c1_blk;
     const uint32_t bytes = (uint32_t)(8 * (4 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
                                       4 * E.s2_blk);
-    if (bytes == 0) return true;
+    if (bytes == 0) return 0u;
     if (threadIdx.x == 0) {
         // the previous element's reads of this buffer (generic proxy) come before the copies
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1042,6 +1064,11 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
         for (int f = 0; f < 6 && E.c1_blk; ++f)
             bulk_g2s(c1 + f * E.c1_blk, fs.c1 + f * fs.c1_n + E.c1_off, 8u * E.c1_blk, bar);
     }
+    return bytes;
+}
+
+__device__ __forceinline__ bool stage_wait(uint32_t bytes, uint64_t* bar, uint32_t& phase, int* err) {
+    if (bytes == 0) return true;
     const uint32_t ph = phase;
     phase ^= 1u;
     const bool ok = mbar_wait_bounded(bar, ph);
@@ -1053,6 +1080,12 @@ __device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState
         return false;
     }
     return true;
+}
+
+__device__ __forceinline__ bool stage_element(const DevElem& E, const FiberState& fs,
+                                              double* sm, uint64_t* bar, uint32_t& phase,
+                                              StageView& sv, int* err) {
+    return stage_wait(stage_issue(E, fs, sm, bar, sv), bar, phase, err);
 }
 
 }  // namespace strut
@@ -1222,17 +1255,15 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
                           smem_fib, &bar, phase, stop, rec_out);
         return;
     }
-    if (tid == 0) {
-        S.local_iters = 0;
-        S.section_evals = 0;
-        S.hard = 0;
-        for (int i = 0; i < 3; ++i) {
-            S.q[i] = estate[(size_t)e * kEStride + kEq + i];
-            S.acc_v[i] = estate[(size_t)e * kEStride + kEv + i];
-            S.zero3[i] = 0.0;
-        }
+    // the bulk copies of the fiber history go out first; the element state is read by several
+    // warps while they are in flight
+    StageView sv;
+    int err = ELEM_ERR_NONE;
+    const uint32_t stage_bytes = stage_issue(E, fs, smem_fib, &bar, sv);
+    {
         const double* es = estate + (size_t)e * kEStride;
-        for (int ip = 0; ip < E.nip; ++ip) {
+        if (tid < E.nip) {
+            const int ip = tid;
             S.vs_e[ip] = es[kEe + ip];
             S.vs_k[ip] = es[kEk + ip];
             S.c_n[ip] = es[kEcN + ip];
@@ -1240,18 +1271,26 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
             S.c_f00[ip] = es[kEc00 + ip];
             S.c_f01[ip] = es[kEc01 + ip];
             S.c_f11[ip] = es[kEc11 + ip];
+        } else if (tid == 32) {
+            S.local_iters = 0;
+            S.section_evals = 0;
+            S.hard = 0;
+            for (int i = 0; i < 3; ++i) {
+                S.q[i] = es[kEq + i];
+                S.acc_v[i] = es[kEv + i];
+                S.zero3[i] = 0.0;
+            }
+            S.c_valid = E.type == 2 && es[kEcv] != 0.0;
+        } else if (tid == 64) {
+            double ug[6];
+            for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
+            if (E.type == 2)
+                u_to_local(E.c, E.s, ug, S.ul);
+            else
+                u_to_local(E.c_div, E.s_div, ug, S.ul);
         }
-        S.c_valid = E.type == 2 && es[kEcv] != 0.0;
-        double ug[6];
-        for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
-        if (E.type == 2)
-            u_to_local(E.c, E.s, ug, S.ul);
-        else
-            u_to_local(E.c_div, E.s_div, ug, S.ul);
     }
-    StageView sv;
-    int err = ELEM_ERR_NONE;
-    const bool staged = stage_element(E, fs, smem_fib, &bar, phase, sv, &err);
+    const bool staged = stage_wait(stage_bytes, &bar, phase, &err);
     __syncthreads();
     if (!staged) {
         if (tid == 0) {
