@@ -112,7 +112,7 @@ struct ElemScratch {
 // family length as field stride).
 struct StageView {
     const double* c2;   // staged: 4 fields x c2_blk (eps sig tan ecmin; dept only enters the
-                        // derived constants, which read it from global memory)
+                        // derived constants, which read it from a separate buffer)
     const double* s2;   // 10 fields x s2_blk
     const int* kon;     // s2_blk
     const double* s1;   // 5 fields x s1_blk
@@ -160,14 +160,15 @@ __device__ __forceinline__ void load_s2(const StageView& sv, int idx, S2State& c
 
 // Derived constants of every Concrete02 / Steel02 fiber of the staged element, computed once
 // per launch by the whole CTA (the committed state does not change inside a launch).  A
-// Concrete02 fiber's dept comes from global memory (c2_dept: the element's dept field).  The two
+// Concrete02 fiber's dept comes from c2_dept: the element's dept field, in global memory or
+// copied into shared memory beside the staged history.  The two
 // branch curves of a Steel02 fiber (each with its own pow) are two work items, given to the last
 // threads of the CTA, so they run beside the Concrete02 items instead of after them.
 __device__ __forceinline__ void derive_c2(const Geo& g, const DevSection& sd, const StageView& sv,
                                           const double* __restrict__ c2_dept, double* c2d, int idx) {
     C2State c;
     load_c2(sv, idx, c);
-    c.dept = __ldg(c2_dept + idx);
+    c.dept = c2_dept[idx];
     const int j = idx % sd.n_c2;
     C2Derived d;
     concrete02_derive(g.mats[__ldg(g.m + sd.geo_off + sd.n_s2 + j)], c, d);
@@ -1028,8 +1029,7 @@ __device__ __forceinline__ void copy_struct(T* dst, const T* src) {
 // the CTA; phase is the parity of its next completion (every thread tracks the same value).
 // stage_wait returns false (and sets *err) if the bulk copy did not complete within the bounded
 // wait.
-__device__ __forceinline__ uint32_t stage_issue(const DevElem& E, const FiberState& fs, double* sm,
-                                                uint64_t* bar, StageView& sv) {
+__device__ __forceinline__ void stage_layout(const DevElem& E, double* sm, StageView& sv) {
     double* c2 = sm;
     double* s2 = c2 + 4 * E.c2_blk;
     double* s1 = s2 + 10 * E.s2_blk;
@@ -1047,8 +1047,21 @@ __device__ __forceinline__ uint32_t stage_issue(const DevElem& E, const FiberSta
     sv.s2_blk = E.s2_blk;
     sv.s1_blk = E.s1_blk;
     sv.c1_blk = E.c1_blk;
+}
+
+// dept (optional): shared-memory destination of the Concrete02 dept field (E.c2_blk doubles,
+// 16-byte aligned), copied with the history.
+__device__ __forceinline__ uint32_t stage_issue(const DevElem& E, const FiberState& fs, double* sm,
+                                                uint64_t* bar, StageView& sv, double* dept = nullptr) {
+    stage_layout(E, sm, sv);
+    double* c2 = const_cast<double*>(sv.c2);
+    double* s2 = const_cast<double*>(sv.s2);
+    double* s1 = const_cast<double*>(sv.s1);
+    double* c1 = const_cast<double*>(sv.c1);
+    int* kon = const_cast<int*>(sv.kon);
+    if (!E.c2_blk) dept = nullptr;
     const uint32_t bytes = (uint32_t)(8 * (4 * E.c2_blk + 10 * E.s2_blk + 5 * E.s1_blk + 6 * E.c1_blk) +
-                                      4 * E.s2_blk);
+                                      4 * E.s2_blk + (dept ? 8 * E.c2_blk : 0));
     if (bytes == 0) return 0u;
     if (threadIdx.x == 0) {
         // the previous element's reads of this buffer (generic proxy) come before the copies
@@ -1056,6 +1069,7 @@ __device__ __forceinline__ uint32_t stage_issue(const DevElem& E, const FiberSta
         mbar_arrive_expect_tx(bar, bytes);
         for (int f = 0; f < 4 && E.c2_blk; ++f)
             bulk_g2s(c2 + f * E.c2_blk, fs.c2 + f * fs.c2_n + E.c2_off, 8u * E.c2_blk, bar);
+        if (dept) bulk_g2s(dept, fs.c2 + 4 * fs.c2_n + E.c2_off, 8u * E.c2_blk, bar);
         for (int f = 0; f < 10 && E.s2_blk; ++f)
             bulk_g2s(s2 + f * E.s2_blk, fs.s2 + f * fs.s2_n + E.s2_off, 8u * E.s2_blk, bar);
         if (E.s2_blk) bulk_g2s(kon, fs.s2_kon + E.s2_off, 4u * E.s2_blk, bar);
@@ -1240,12 +1254,15 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
     auto process = [&](const int e, const int fslot, const int fa) -> void {
     copy_struct(&E, elems + e);
     __syncthreads();
-    if (mode == ELEM_MODE_RECORD ? status[E.inst] != 0 : !active[E.inst]) {
+    // the instance's flag and the section record are read together (the section of an element
+    // that is not run is read but not used)
+    const bool skip = mode == ELEM_MODE_RECORD ? status[E.inst] != 0 : !active[E.inst];
+    copy_struct(&sd, g.secs + E.sec);
+    if (skip) {
         // a fanned element that is not run still counts as resolved (its first attempt's CTA)
         if (fslot >= 0 && fa == 0 && tid == 0 && el.rq) atomicAdd(&el.fan_finished[cur], 1);
         return;
     }
-    copy_struct(&sd, g.secs + E.sec);
     if constexpr (DIM == 3) {
         __syncthreads();
         double* rec_out = nullptr;
@@ -1255,43 +1272,75 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
                           smem_fib, &bar, phase, stop, rec_out);
         return;
     }
-    // the bulk copies of the fiber history go out first; the element state is read by several
-    // warps while they are in flight
+    __syncthreads();
+    // the bulk copies of the fiber history go out first, with the Concrete02 dept field into the
+    // buffer of the per-fiber results (free until the first evaluation); the element state and
+    // the section's fiber y are read while they are in flight
     StageView sv;
+    stage_layout(E, smem_fib, sv);
+    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
+    double* ys = const_cast<double*>(sv.s2d) + 12 * E.s2_blk;
+    double* fo = ys + ((n_tot + 1) & ~1);
     int err = ELEM_ERR_NONE;
-    const uint32_t stage_bytes = stage_issue(E, fs, smem_fib, &bar, sv);
+    const uint32_t stage_bytes = stage_issue(E, fs, smem_fib, &bar, sv, fo);
     {
         const double* es = estate + (size_t)e * kEStride;
         if (tid < E.nip) {
             const int ip = tid;
-            S.vs_e[ip] = es[kEe + ip];
-            S.vs_k[ip] = es[kEk + ip];
+            const double ve = es[kEe + ip], vk = es[kEk + ip];
+            S.vs_e[ip] = ve;
+            S.vs_k[ip] = vk;
+            if (E.type == 2) {  // the accepted section deformations start as the element's
+                S.svs_e[ip] = ve;
+                S.svs_k[ip] = vk;
+            }
             S.c_n[ip] = es[kEcN + ip];
             S.c_m[ip] = es[kEcM + ip];
             S.c_f00[ip] = es[kEc00 + ip];
             S.c_f01[ip] = es[kEc01 + ip];
             S.c_f11[ip] = es[kEc11 + ip];
         } else if (tid == 32) {
+            // the displacements in the element's frame and (forceBeamColumn2d) the basic
+            // deformations, the accepted state and the increment still to apply
+            double ug[6], ul[6], q[3], av[3];
+            for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
+            for (int i = 0; i < 3; ++i) {
+                q[i] = es[kEq + i];
+                av[i] = es[kEv + i];
+            }
+            const bool cv = es[kEcv] != 0.0;
+            if (E.type == 2)
+                u_to_local(E.c, E.s, ug, ul);
+            else
+                u_to_local(E.c_div, E.s_div, ug, ul);
+            for (int a = 0; a < 6; ++a) S.ul[a] = ul[a];
             S.local_iters = 0;
             S.section_evals = 0;
             S.hard = 0;
             for (int i = 0; i < 3; ++i) {
-                S.q[i] = es[kEq + i];
-                S.acc_v[i] = es[kEv + i];
+                S.q[i] = q[i];
+                S.acc_v[i] = av[i];
                 S.zero3[i] = 0.0;
             }
-            S.c_valid = E.type == 2 && es[kEcv] != 0.0;
-        } else if (tid == 64) {
-            double ug[6];
-            for (int a = 0; a < 6; ++a) ug[a] = u_full[E.dof[a]];
-            if (E.type == 2)
-                u_to_local(E.c, E.s, ug, S.ul);
-            else
-                u_to_local(E.c_div, E.s_div, ug, S.ul);
+            S.c_valid = E.type == 2 && cv;
+            if (E.type == 2) {
+                const double chord = (ul[4] - ul[1]) / E.L;
+                const double v[3] = {ul[3] - ul[0], ul[2] - chord, ul[5] - chord};
+                for (int i = 0; i < 3; ++i) {
+                    S.v[i] = v[i];
+                    S.acc_q[i] = q[i];
+                    const double r = v[i] - av[i];
+                    S.rem[i] = r;
+                    S.att[i] = r;
+                }
+                S.best_ok = 0;
+                S.loop_ctrl = 0;
+            }
         }
     }
-    const bool staged = stage_wait(stage_bytes, &bar, phase, &err);
-    __syncthreads();
+    for (int gg = tid; gg < n_tot; gg += blockDim.x) ys[gg] = __ldg(g.y + sd.geo_off + gg);
+    const bool staged = stage_wait(stage_bytes, &bar, phase, &err);  // a CTA barrier when copies ran
+    if (!stage_bytes) __syncthreads();
     if (!staged) {
         if (tid == 0) {
             elem_err[e] = err;
@@ -1300,13 +1349,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         stop = true;
         return;
     }
-    derive_element(g, sd, E, sv, fs.c2 + 4 * fs.c2_n + E.c2_off, const_cast<double*>(sv.c2d),
-                   const_cast<double*>(sv.s2d));
-    // the section's fiber y (phase-2 sums) and the per-fiber results of phase 1 follow
-    const int n_tot = sd.n_s2 + sd.n_c2 + sd.n_s1 + sd.n_c1 + sd.n_el;
-    double* ys = const_cast<double*>(sv.s2d) + 12 * E.s2_blk;
-    double* fo = ys + ((n_tot + 1) & ~1);
-    for (int gg = tid; gg < n_tot; gg += blockDim.x) ys[gg] = __ldg(g.y + sd.geo_off + gg);
+    derive_element(g, sd, E, sv, fo, const_cast<double*>(sv.c2d), const_cast<double*>(sv.s2d));
     __syncthreads();
     const int nip = E.nip;
     if (E.type == 3) {
@@ -1388,25 +1431,9 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
         return;
     }
     // ---------------- forceBeamColumn2d ----------------
+    // (basic deformations, accepted state and increment were set up while the history was staged)
     const double L = E.L;
     const double inv_L = E.inv_L;
-    if (tid == 0) {
-        const double chord = (S.ul[4] - S.ul[1]) / L;
-        S.v[0] = S.ul[3] - S.ul[0];
-        S.v[1] = S.ul[2] - chord;
-        S.v[2] = S.ul[5] - chord;
-        for (int i = 0; i < 3; ++i) {
-            S.acc_q[i] = S.q[i];
-            S.rem[i] = S.v[i] - S.acc_v[i];
-            S.att[i] = S.rem[i];
-        }
-        for (int ip = 0; ip < nip; ++ip) {
-            S.svs_e[ip] = S.vs_e[ip];
-            S.svs_k[ip] = S.vs_k[ip];
-        }
-        S.best_ok = 0;
-        S.loop_ctrl = 0;
-    }
     // a later pass of a fanned-out element starts from the state its previous pass accepted
     if (fslot >= 0 && tid == 0) {
         const double* R = el.fan_round + (size_t)(cur * kFanCap + fslot) * kFanRound;
@@ -1432,7 +1459,7 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
             }
         }
     }
-    __syncthreads();
+    if (fslot >= 0) __syncthreads();
     int converged = 0;
     if (sd.all_elastic) {
         // _force_beam_column2d_exact_elastic_state (section evaluations there only set trial
@@ -1549,35 +1576,39 @@ __global__ void __launch_bounds__(kTeamThreads) element_state_kernel(
             while (run_loop && num_subdivide <= 4 && guard < 10000) {
                 ++guard;
                 int scheme_success = 0;
-                if (tid == 0)
-                    for (int i = 0; i < 3; ++i) S.tv[i] = S.acc_v[i] + S.att[i];
-                __syncthreads();
                 for (int scheme = 0; scheme < 3; ++scheme) {
-                    if (tid == 0) {
-                        for (int i = 0; i < 3; ++i) S.q[i] = S.acc_q[i];
-                        for (int ip = 0; ip < nip; ++ip) {
-                            S.vs_e[ip] = S.svs_e[ip];
-                            S.vs_k[ip] = S.svs_k[ip];
+                    // warp 0 restores the accepted state (and first forms the trial deformation)
+                    if (tid < 32) {
+                        if (tid < 3) {
+                            if (scheme == 0) S.tv[tid] = S.acc_v[tid] + S.att[tid];
+                            S.q[tid] = S.acc_q[tid];
+                        }
+                        if (tid < nip) {
+                            S.vs_e[tid] = S.svs_e[tid];
+                            S.vs_k[tid] = S.svs_k[tid];
                         }
                     }
                     __syncthreads();
                     if (!fbc_try_increment(g, sd, sv, E, S, S.acc_v, S.att, scheme, ys, fo, nullptr, 0)) continue;
-                    if (tid == 0) {
-                        for (int i = 0; i < 3; ++i) {
-                            S.acc_v[i] = S.tv[i];
-                            S.acc_q[i] = S.best[i];
+                    if (tid < 32) {
+                        // accept the partial step; every lane forms the remainder and its test
+                        double rm[3];
+                        for (int i = 0; i < 3; ++i) rm[i] = S.v[i] - S.tv[i];
+                        const bool done = max_abs3(rm) <= 1.0e-12;
+                        if (tid < 3) {
+                            const double r = tid == 0 ? rm[0] : tid == 1 ? rm[1] : rm[2];
+                            S.acc_v[tid] = S.tv[tid];
+                            S.acc_q[tid] = S.best[tid];
+                            S.rem[tid] = r;
+                            if (!done) S.att[tid] = r;
                         }
-                        for (int ip = 0; ip < nip; ++ip) {
-                            S.svs_e[ip] = S.vs_e[ip];
-                            S.svs_k[ip] = S.vs_k[ip];
+                        if (tid < nip) {
+                            S.svs_e[tid] = S.vs_e[tid];
+                            S.svs_k[tid] = S.vs_k[tid];
                         }
-                        S.best_ok = 1;
-                        for (int i = 0; i < 3; ++i) S.rem[i] = S.v[i] - S.acc_v[i];
-                        if (max_abs3(S.rem) <= 1.0e-12) {
-                            S.loop_ctrl = 1;
-                        } else {
-                            for (int i = 0; i < 3; ++i) S.att[i] = S.rem[i];
-                            S.loop_ctrl = 0;
+                        if (tid == 0) {
+                            S.best_ok = 1;
+                            S.loop_ctrl = done ? 1 : 0;
                         }
                     }
                     __syncthreads();
