@@ -91,6 +91,8 @@ def parse():
                     help="one short analysis (for a profiler launch list); prints no bench line")
     ap.add_argument("--profile-tall", action="store_true",
                     help="with --profile-only: --tall-steps steps of the 20-story 3D frame instead")
+    ap.add_argument("--element-threads", type=int, default=0,
+                    help="with --profile-only: element CTA size (0: the library default)")
     return ap.parse_args()
 
 
@@ -566,6 +568,8 @@ def main():
         # host-driven loop (profiling mode): plain launches a profiler can attribute (kernel
         # nodes of a graph with conditional nodes cannot be profiled one by one)
         with runtime.Analysis(models, device=device) as an:
+            if args.element_threads:
+                an.set_tuning(element_threads=args.element_threads)
             runtime.lib().strut_gpu_set_profiling(an.h, 1)
             an.run(min(50, args.record_steps), check=False)
             P = A.StrutKernelProfile()
