@@ -105,7 +105,7 @@ def tune(models, steps: int, device: int = -1, save: bool = True, table: Path = 
     (class key, best tuning, {tuning: ms}) and, with save, records the winner in the table."""
     import torch
 
-    with runtime.Analysis(models, device=device) as an:
+    with runtime.Analysis(models, device=device, tuned=False) as an:
         wide = any(an.band_info(i)[1] * 8 * models[i].num_free > 220 * 1024 for i in range(len(models)))
         max_nip = max((int(m.integrations[e.integration].num_int_pts) for m in models for e in m.elements),
                       default=1)
@@ -113,7 +113,7 @@ def tune(models, steps: int, device: int = -1, save: bool = True, table: Path = 
     key = workload_class(models, wide)
 
     def trial(t):
-        with runtime.Analysis(models, device=device) as an:
+        with runtime.Analysis(models, device=device, tuned=False) as an:
             an.set_tuning(**t)
             stream = torch.cuda.ExternalStream(runtime.lib().strut_gpu_stream(an.h))
             e0 = torch.cuda.Event(enable_timing=True)

@@ -55,9 +55,13 @@ def _d(a: np.ndarray):
 
 
 class Analysis:
-    """A batch of transient analyses on one GPU (one handle)."""
+    """A batch of transient analyses on one GPU (one handle).
 
-    def __init__(self, models, device: int = -1):
+    tuned: start from the launch shapes the autotuner recorded for this batch's workload class
+    (strut_b200/tuned_shapes.json), if it has an entry; the library's defaults otherwise.  Every
+    launch shape gives the same results bit for bit; set_tuning overrides them."""
+
+    def __init__(self, models, device: int = -1, tuned: bool = True):
         self.models = list(models)
         n = len(self.models)
         self._descs = (A.StrutModelDesc * n)()
@@ -67,6 +71,11 @@ class Analysis:
         _check(lib().strut_gpu_create(self._descs, n, device, C.byref(h)), "strut_gpu_create")
         self.h = h
         self.steps_done = 0
+        self.tuned = None
+        if tuned:
+            from . import autotune
+
+            self.tuned = autotune.apply(self)
 
     def close(self):
         if getattr(self, "h", None):
