@@ -198,8 +198,9 @@ __device__ int band_chol_smem(double* B, int n, int bw, int rw, double* fac) {
 // linear_solver_backend.mojo:735-770).  Forward: column-oriented, so row i receives
 // rhs_i - L_i,j0 w_j0 - L_i,j0+1 w_j0+1 - ... in increasing j, the order of the reference's row
 // loop.  Back: lane 0 runs each row's sum in the reference's order.  w may not alias rhs.
-__device__ void band_solve_lu_warp(const double* B, int n, int bw, int rw, const double* rhs,
-                                   double* w, double* x) {
+__device__ void band_solve_lu_warp(const double* __restrict__ B, int n, int bw, int rw,
+                                   const double* __restrict__ rhs, double* __restrict__ w,
+                                   double* __restrict__ x) {
     const int lane = threadIdx.x & 31;
     for (int i = lane; i < n; i += 32) w[i] = rhs[i];
     __syncwarp();
@@ -266,6 +267,60 @@ __device__ __forceinline__ double gather_slot(const InstArrays& A, long long sp0
         for (long long c = c0; c < c1; ++c) K += A.ek[A.slot_contrib[c]];
     }
     return K;
+}
+
+// The whole band of an instance (n x rw slots, entries outside the matrix zero): gather_slot of
+// every slot, four slots per thread interleaved so that their dependent loads (list bounds,
+// contribution indices, element entries) are in flight together.  Each slot adds its own
+// contributions in list order, as gather_slot does.  The whole CTA.
+__device__ __forceinline__ void gather_band4(const InstArrays& A, long long sp0, int n, int bw, int rw,
+                                             double* __restrict__ Kb) {
+    const int nt = blockDim.x, n_slots = n * rw;
+    const long long* __restrict__ ptr = A.slot_ptr + sp0;
+    const int* __restrict__ con = A.slot_contrib;
+    const double* __restrict__ coef = A.slot_coef;
+    const double* __restrict__ ek = A.ek;
+    for (int s0 = threadIdx.x; s0 < n_slots; s0 += 4 * nt) {
+        long long c[4], e[4];
+        double K[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int slot = s0 + u * nt;
+            c[u] = e[u] = 0;
+            K[u] = 0.0;
+            if (slot < n_slots) {
+                const int i = slot / rw, j = i + (slot - i * rw) - bw;
+                if (j >= 0 && j < n) {
+                    c[u] = ptr[slot];
+                    e[u] = ptr[slot + 1];
+                }
+            }
+        }
+        for (;;) {
+            int idx[4];
+            bool any = false;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                idx[u] = c[u] < e[u] ? con[c[u]] : -1;
+                any |= idx[u] >= 0;
+            }
+            if (!any) break;
+            if (coef) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (idx[u] >= 0) K[u] += coef[c[u]] * ek[idx[u]];
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (idx[u] >= 0) K[u] += ek[idx[u]];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) c[u] += c[u] < e[u] ? 1 : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (s0 + u * nt < n_slots) Kb[s0 + u * nt] = K[u];
+    }
 }
 
 // F_int of free dof i of an instance: its element end forces in element order (times the
@@ -527,6 +582,11 @@ __global__ void __launch_bounds__(256) instance_newton_kernel(const DevInst* __r
         const long long sp0 = I.slot_ptr_off;
         const double* Kinit = A.Kinit + I.band_off;
         const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+        if (!modified) {
+            // four slots per thread at a time, their contribution lists walked side by side
+            // (each slot still sums its own contributions in element order)
+            gather_band4(A, sp0, n, bw, rw, Kb);
+        } else
         for (int i = warp; i < n; i += nw)
             for (int o = lane; o < rw; o += 32) {
                 const int j = i + o - bw;
